@@ -1,0 +1,29 @@
+import os
+import sys
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(REPO, "opticalflow-ri_b200")
+for p in (PKG, os.path.join(REPO, "oracle"), REPO):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+GOLDEN = os.path.join(REPO, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+def golden(name):
+    import numpy as np
+    return np.load(os.path.join(GOLDEN, f"{name}.npz"))
+
+
+@pytest.fixture(scope="session")
+def cuda_ok():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return True

@@ -1,0 +1,94 @@
+"""The CPU oracle against golden vectors produced by the reference itself
+(tests/golden/make_golden.py).  Bit-exact except the spline upsample (<= 1 float32 ulp)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden
+
+
+def test_prefilter_taps():
+    g = golden("taps_prefilter")
+    for i, (s, K) in enumerate(g["params"]):
+        assert np.array_equal(O.prepare_gaussian_kernel(s, int(K)), g[f"k{i}"])
+
+
+def test_bitexact_taps():
+    g = golden("taps_bitexact")
+    for i, (n, s) in enumerate(g["params"]):
+        assert np.array_equal(O.gaussian_kernel_bitexact(int(n), s), g[f"k{i}"]), (n, s)
+
+
+def test_farneback_consts():
+    g = golden("fb_consts")
+    for i in range(3):
+        n, s = g[f"n{i}"]
+        gg, xg, xxg, ig = O.farneback_poly_consts(int(n), s)
+        assert np.array_equal(gg, g[f"g{i}"]) and np.array_equal(xg, g[f"xg{i}"])
+        assert np.array_equal(xxg, g[f"xxg{i}"]) and np.array_equal(ig, g[f"ig{i}"])
+    for i in range(4):
+        n, s = g[f"halfp{i}"]
+        assert np.array_equal(O.fb_half_kernel(int(n), s), g[f"half{i}"])
+
+
+def test_prefilter():
+    g = golden("prefilter")
+    for i, (s, K) in enumerate([(3.4, 3), (2.0, 3), (0.48, 5)]):
+        assert np.array_equal(O.prefilter(g["img"], s, K), g[f"out{i}"])
+
+
+def test_hs():
+    g = golden("hs")
+    fx, fy, ft = O.hs_derivatives(g["f0"], g["f1"])
+    assert np.array_equal(fx, g["fx"]) and np.array_equal(fy, g["fy"]) and np.array_equal(ft, g["ft"])
+    U, V, e = O.hs_solve(g["f0"], g["f1"], g["U0"], g["V0"], float(g["alpha"]), int(g["niter"]))
+    assert np.array_equal(U, g["U"]) and np.array_equal(V, g["V"])
+    assert e == pytest.approx(float(g["err"]), rel=1e-6)
+
+
+def test_ls():
+    g = golden("ls")
+    c = O.ls_coeffs(g["f0"], g["f1"], float(g["h"]))
+    assert np.array_equal(c[5], g["B11"]) and np.array_equal(c[6], g["B12"]) and np.array_equal(c[7], g["B22"])
+    U, V, e, it = O.ls_solve(g["f0"], g["f1"], g["U0"], g["V0"], float(g["h"]))
+    assert np.array_equal(U, g["U"]) and np.array_equal(V, g["V"])
+    assert e == pytest.approx(float(g["err"]), rel=1e-6)
+
+
+def test_warp():
+    g = golden("warp")
+    O0, O1 = O.warp_pair(g["I0"], g["I1"], g["U"], g["V"])
+    assert np.array_equal(O0, g["O0"]) and np.array_equal(O1, g["O1"])
+
+
+def test_resize():
+    g = golden("resize")
+    i = 0
+    while f"src{i}" in g:
+        W, H, f = g[f"spec{i}"]
+        out = O.resize(g[f"src{i}"], (int(W), int(H)), int(f))
+        assert np.array_equal(out, g[f"dst{i}"]), i
+        i += 1
+
+
+def test_spline():
+    g = golden("spline")
+    i = 0
+    while f"src{i}" in g:
+        ref = g[f"dst{i}"]
+        out = O.spline_upsample(g[f"src{i}"], *ref.shape)
+        ulp = np.spacing(np.abs(ref).astype(np.float32))
+        assert np.all(np.abs(out - ref) <= ulp), i
+        i += 1
+
+
+def test_pyramid_hs():
+    g = golden("pyr_hs")
+    U, V = O.pyramid(g["f0"], g["f1"], 3.4, O.HS([21], 600), 1)
+    assert np.array_equal(U, g["U"]) and np.array_equal(V, g["V"])
+
+
+def test_pyramid_hs_ls():
+    g = golden("pyr_hs_ls")
+    U, V = O.pyramid(g["f0"], g["f1"], 3.4, O.HS([21, 45], 100), 2, 1, 0.48, O.LS(10))
+    assert np.abs(U - g["U"]).max() <= 1e-5 and np.abs(V - g["V"]).max() <= 1e-5
