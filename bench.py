@@ -1,0 +1,326 @@
+"""Benchmark of the dense pyramidal optical-flow hot path on B200.
+
+Workload (the headline metric's plain arm): the LiuSE_Farneback_Fs0_0_PyrLvls2 calibration
+(Farneback, 2 pyramid levels, no prefilter, then Liu-Shen refinement with h = 10 on
+FILTER_OPT = 0.48 prefiltered frames) on 1024x1024 uint8 synthetic PIV pairs with a
+divergence-free random-Fourier displacement (max 4 px, 0.05 particles/px, diameter 2-3 px,
+noise 2 DN).  One step = `--pairs` frame pairs through the whole pipeline.
+
+  value : pairs/s with the frames already resident in HBM (device-timed, CUDA events),
+          aggregated over all ranks (pairs / max-over-ranks time).
+  e2e   : pairs/s through the reference-facing API (genericPyramidalOpticalFlow with
+          numpy float32 frames in and numpy U, V out: host<->device copies inside).
+  roofline : the Liu-Shen solve at 1024^2 (the dominant kernel), algorithmic bytes =
+          (24 B x sweeps + 8 B) per pixel, against the measured HBM copy bandwidth.
+  cpu_baseline : the CPU oracle (C restatement of the reference, 1 thread) on one pair.
+
+--impl reference: the CPU restatement of the reference's path (the reference itself needs
+OpenCL for Farneback and cannot run on the box), on all host cores, one pair per worker
+per step.
+
+Multi-GPU (torchrun): pairs are independent; every rank runs its own pairs (weak scaling),
+no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "opticalflow-ri_b200"))
+
+METRIC = "pairs/s @1024^2 Liu-Shen (Farneback pyr2 + Liu-Shen, plain)"
+WORKLOAD = "LiuSE_Farneback_Fs0_0_PyrLvls2 1024x1024 random-Fourier PIV pairs"
+L2_BYTES = 126 * 2 ** 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--pairs", type=int, default=8, help="frame pairs per step per GPU")
+    p.add_argument("--size", type=int, default=1024)
+    p.add_argument("--unique", type=int, default=4, help="distinct synthetic pairs (cycled)")
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_pairs(n, size, seed0=100):
+    from ofb200 import synthetic as S
+    out = []
+    for i in range(n):
+        a, b, U, V = S.config_pair("fbls1024", seed=seed0 + i, size=size)
+        out.append((a, b, U, V))
+    return out
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def pipeline_dev(a, b):
+    """One pair on device tensors through the drop-in driver (no host synchronisation)."""
+    import Farneback_PyCL as F
+    import GenericPyramidalOpticalFlow as G
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    return G.genericPyramidalOpticalFlow(a, b, 0, F.Farneback_PyCL(), 2, 1, 0.48, LS.LiuShenOpticalFlowAlgoAdapter(10))
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from ofb200 import _lib, ops
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    pairs = make_pairs(args.unique, args.size, seed0=100 + 1000 * rank)
+    frames = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _, _ in pairs]
+    host_frames = [(a.astype(np.float32), b.astype(np.float32)) for a, b, _, _ in pairs]
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    N = args.size * args.size
+
+    def step(timing=None):
+        for i in range(args.pairs):
+            a8, b8 = frames[i % len(frames)]
+            a = ops.u8_to_f32(a8)
+            b = ops.u8_to_f32(b8)
+            U, V = pipeline_dev(a, b)
+        return U, V
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+
+    # device-timed steps (L2 flushed between steps, outside the events)
+    clocks = Clocks(local_rank) if rank == 0 else None
+    lc0 = _lib.lib().of_launch_count()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    launches = _lib.lib().of_launch_count() - lc0
+    clk = clocks.stop() if clocks else None
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    barrier()
+
+    # roofline of the dominant kernel: the Liu-Shen solve at full size, timed alone
+    a = ops.u8_to_f32(frames[0][0])
+    b = ops.u8_to_f32(frames[0][1])
+    taps = np.array([1.3824512e-04, 9.2915423e-02, 8.1389272e-01, 9.2915423e-02, 1.3824512e-04], np.float32)
+    from gaussian_filter import prepareGaussianKernel
+    taps = prepareGaussianKernel(0.48, 5)
+    fa, fb = ops.prefilter(a, taps), ops.prefilter(b, taps)
+    U0 = torch.zeros_like(fa)
+    ls_ms, iters = [], None
+    for r in range(4):
+        Uw, Vw = U0.clone(), U0.clone()
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, _, it, _ = ops.ls_solve(fa, fb, Uw, Vw, 10.0)
+        e1.record()
+        e1.synchronize()
+        if r > 0:
+            ls_ms.append(e0.elapsed_time(e1))
+        iters = int(it.item())
+    ls_ms = float(np.mean(ls_ms))
+    alg_bytes = (24.0 * iters + 8.0) * N
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (ls_ms * 1e-3) / 1e9
+
+    # end to end through the reference-facing API, host buffers
+    e2e = None
+    if not args.no_e2e:
+        import Farneback_PyCL as F
+        import GenericPyramidalOpticalFlow as G
+        import PhysicsBasedOpticalFlowLiuShen as LS
+        for i in range(2):
+            G.genericPyramidalOpticalFlow(*host_frames[i % len(host_frames)], 0, F.Farneback_PyCL(), 2, 1, 0.48,
+                                          LS.LiuShenOpticalFlowAlgoAdapter(10))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n_e2e = max(2, args.pairs)
+        for i in range(n_e2e):
+            U, V = G.genericPyramidalOpticalFlow(*host_frames[i % len(host_frames)], 0, F.Farneback_PyCL(), 2, 1,
+                                                 0.48, LS.LiuShenOpticalFlowAlgoAdapter(10))
+        dt = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(dt, op=dist.ReduceOp.MAX)
+        e2e = {"value": n_e2e * world / float(dt.item()), "unit": "pairs/s",
+               "h2d_bytes_per_step": 2 * N * 4 * args.pairs, "d2h_bytes_per_step": 2 * N * 4 * args.pairs}
+
+    if rank != 0:
+        return None
+    pairs_total = args.pairs * args.steps * world
+    line = {
+        "metric": METRIC, "value": pairs_total / (total_ms * 1e-3), "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "pairs_per_step_per_gpu": args.pairs, "size": args.size,
+                   "unique_pairs": args.unique, "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"pairs sharded over {world} rank(s)"},
+        "clocks": clk, "e2e": e2e, "gpu_launches": int(launches),
+        "roofline": {"kernel": "Liu-Shen solve 1024^2 (setup + sweeps)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None, "sweeps": iters, "ms": ls_ms,
+                     "algorithmic_bytes": alg_bytes},
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(pairs[0])
+    return line
+
+
+def _oracle():
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    return O
+
+
+def _oracle_pair(args):
+    a, b = args
+    O = _oracle()
+    return O.pyramid(a, b, 0, O.FB(), 2, 1, 0.48, O.LS(10))
+
+
+def cpu_baseline(pair):
+    """The oracle (scalar C port, 1 thread) on one 1024^2 pair."""
+    a, b = pair[0].astype(np.float32), pair[1].astype(np.float32)
+    t0 = time.perf_counter()
+    _oracle_pair((a, b))
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "pairs/s", "cores": 1, "kind": "port",
+            "sample": f"1 pair {a.shape[0]}x{a.shape[1]}, full pipeline, {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    import multiprocessing as mp
+    try:
+        ncores = len(os.sched_getaffinity(0))
+    except Exception:
+        ncores = os.cpu_count() or 1
+    pairs = make_pairs(min(args.unique, 2), args.size)
+    work = [(p[0].astype(np.float32), p[1].astype(np.float32)) for p in pairs]
+    ctx = mp.get_context("spawn")
+    per_step = ncores
+    with ctx.Pool(ncores) as pool:
+        for _ in range(min(args.warmup, 1)):
+            pool.map(_oracle_pair, [work[i % len(work)] for i in range(per_step)])
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            pool.map(_oracle_pair, [work[i % len(work)] for i in range(per_step)])
+        dt = time.perf_counter() - t0
+    v = per_step * args.steps / dt
+    return {"metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "pairs_per_step": per_step, "size": args.size},
+            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": ncores, "kind": "port",
+                             "sample": f"{per_step} pairs per step, one per process"},
+            "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line:
+            print(json.dumps(line))
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    line = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if line:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,185 @@
+/*
+ * ofb200 — C ABI of the B200 (sm_100a) dense pyramidal optical-flow kernels.
+ *
+ * Conventions
+ *  - Every entry point returns an int status: OF_OK (0) or a negative OF_ERR_* code;
+ *    of_last_error() returns the message of the calling thread's last failure.
+ *  - All image / flow buffers are DEVICE pointers to row-major float32 planes of H rows
+ *    and W columns with a row pitch of `pitch` elements (pitch >= W).  U is the +x
+ *    (column) displacement, V the +y (row) displacement.
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls only enqueue work:
+ *    results are ready when the stream is synchronised.  Values reported "to device"
+ *    (iteration counts, errors) are written to device memory for the same reason.
+ *  - Entry points that need scratch memory take a caller-provided device workspace of at
+ *    least the size returned by the matching *_workspace_size() call; they never
+ *    allocate.  Distinct streams need distinct workspaces.
+ *  - No C++ exception crosses this boundary.  The library holds no state besides the
+ *    per-thread error message.
+ *
+ * Each declaration names the reference interface it replaces (OpticalFlow-RI,
+ * file:line).
+ */
+#ifndef OFB200_H
+#define OFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OF_OK 0
+#define OF_ERR_INVALID (-1)   /* bad argument (size, pointer, pitch, parameter) */
+#define OF_ERR_CUDA (-2)      /* a CUDA launch or runtime call failed */
+#define OF_ERR_WORKSPACE (-3) /* workspace missing or smaller than required */
+#define OF_ERR_UNSUPPORTED (-4)
+
+#define OF_FILTER_BILINEAR 0
+#define OF_FILTER_BICUBIC 1
+
+/* Library version (major*10000 + minor*100 + patch). */
+int of_version(void);
+
+/* Number of CUDA kernels this library has launched in the process (all threads); lets a
+ * caller count the launches of a timed region. */
+unsigned long long of_launch_count(void);
+
+/* Copies the calling thread's last error message into buf (always NUL-terminated);
+ * returns its full length. */
+int of_last_error(char* buf, size_t n);
+
+/* ---------------------------------------------------------------------------------
+ * A1 Gaussian prefilter — replaces gaussian_filterPx / convolveSeparableFilter
+ * (src/gaussian_filter.py:54-94).  Separable K-tap FIR (K odd, 1..15), row pass then
+ * column pass, with the reference's border (left mirrored, right copied in order) and
+ * float32 arithmetic order; bit-exact with the reference.  `taps` is a HOST array of K
+ * floats (e.g. prepareGaussianKernel(sigma, K), src/gaussian_filter.py:47-52).
+ * src and dst may not alias.  of_prefilter_u8 reads uint8 frames (fused cast).
+ * ------------------------------------------------------------------------------- */
+int of_prefilter_f32(const float* src, int src_pitch, float* dst, int dst_pitch, int H, int W,
+                     const float* taps, int K, void* stream);
+int of_prefilter_u8(const uint8_t* src, int src_pitch, float* dst, int dst_pitch, int H, int W,
+                    const float* taps, int K, void* stream);
+
+/* uint8 -> float32 plane conversion (the examples' imread(...).astype(np.float32)). */
+int of_u8_to_f32(const uint8_t* src, int src_pitch, float* dst, int dst_pitch, int H, int W, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * A2 antialiased resize — replaces imresize (src/GenericPyramidalOpticalFlow.py:66-67,
+ * PIL BICUBIC) and the Farneback imresize (src/Farneback_PyCL.py:61-62, PIL BILINEAR):
+ * Pillow Image.resize on a mode 'F' image (horizontal pass into a float32 intermediate,
+ * then vertical pass; double accumulation).  Same size is a copy.
+ * ------------------------------------------------------------------------------- */
+size_t of_resize_workspace_size(int Hs, int Ws, int Hd, int Wd, int filter);
+int of_resize(const float* src, int Hs, int Ws, int src_pitch, float* dst, int Hd, int Wd, int dst_pitch, int filter,
+              void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * A3 flow upsample — replaces the RectBivariateSpline branch of updateNextPyramidalLevel
+ * (src/GenericPyramidalOpticalFlow.py:151-171): cubic interpolating (not-a-knot) spline
+ * of the h x w field on x_i = i/w, y_i = i/h evaluated at X/W, Y/H (clamped to the
+ * last sample), rounded to float32, then multiplied by `scale` (float32) — pass 1.0f
+ * when the level does not scale.  h, w >= 4.
+ * ------------------------------------------------------------------------------- */
+size_t of_spline_workspace_size(int h, int w, int H, int W);
+int of_spline_upsample(const float* src, int h, int w, int src_pitch, float* dst, int H, int W, int dst_pitch,
+                       float scale, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * A4 symmetric bilinear warp — replaces doBiLinearWarping as called at
+ * src/GenericPyramidalOpticalFlow.py:197-200: O0 = I0 sampled at (y - V/2, x - U/2),
+ * O1 = I1 sampled at (y + V/2, x + U/2); round-half-even base, replicate borders.
+ * ------------------------------------------------------------------------------- */
+int of_warp_pair_bilinear(const float* I0, const float* I1, const float* U, const float* V, float* O0, float* O1,
+                          int H, int W, int pitch, void* stream);
+/* doBiLinearWarping(img, coordsY, coordsX) itself (src/GenericPyramidalOpticalFlow.py:69-115)
+ * for arbitrary float32 coordinate planes. */
+int of_warp_bilinear_coords(const float* img, const float* coordsY, const float* coordsX, float* out, int H, int W,
+                            int pitch, void* stream);
+
+/* dst = dst + src (the driver's Uaccum += U, src/GenericPyramidalOpticalFlow.py:412-413),
+ * and dst = src * s (float32). */
+int of_accumulate(float* dst, const float* src, int H, int W, int pitch, void* stream);
+int of_scale(const float* src, float* dst, float s, int H, int W, int pitch, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * A6/A7 Horn-Schunck — replaces HSOpticalFlowAlgoAdapter.compute / HS
+ * (src/HornSchunck.py:28-104): 2x2-cube derivatives, `niter` Jacobi sweeps with the
+ * 3x3 averaging kernel (mirror borders), bit-exact with the reference.  I0 = frame at t0,
+ * I1 = frame at t1.  U, V: initial flow in, result out.  err_out (device, optional):
+ * (||U-U0||_F + ||V-V0||_F) / (H*W) as float64.
+ * ------------------------------------------------------------------------------- */
+size_t of_hs_workspace_size(int H, int W, int pitch);
+/* computeDerivatives (src/HornSchunck.py:106-126) as HS calls it: fx, fy, ft of the pair
+ * (I0 = frame t0, I1 = frame t1). */
+int of_hs_derivatives(const float* I0, const float* I1, float* fx, float* fy, float* ft, int H, int W, int pitch,
+                      void* stream);
+int of_hs_solve(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float alpha,
+                int niter, double* err_out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * A8/A9 Liu-Shen physics-based optimiser — replaces LiuShenOpticalFlowAlgoAdapter.compute /
+ * physicsBasedOpticalFlowLiuShen (src/PhysicsBasedOpticalFlowLiuShen.py:33-158).
+ * Frames are normalised by their maxima; sweeps run while err > tol and k < maxnum
+ * (reference: tol 1e-8, maxnum 60); bit-exact with the reference's float32 fields.
+ * U, V: initial flow in, result out.  iters_out / err_out: DEVICE int / double
+ * (optional): sweeps run and the last sweep's error.
+ * ------------------------------------------------------------------------------- */
+size_t of_ls_workspace_size(int H, int W, int pitch, int maxnum);
+/* The eight per-pixel coefficient planes of the solver (IIx, IIy, II, Ixt, Iyt and
+ * B11, B12, B22 of generate_invmatrix, src/PhysicsBasedOpticalFlowLiuShen.py:47-73,124-128)
+ * from a normalised frame I1n and Et = I2n - I1n; coef holds 8 stacked H x W planes. */
+int of_ls_coefficients(const float* I1n, const float* Et, float* coef, int H, int W, int pitch, float h, void* stream);
+int of_ls_solve(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float h, int maxnum,
+                double tol, int* iters_out, double* err_out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * A10/A11 dense Lucas-Kanade — replaces denseLucasKanade_PyCl.compute
+ * (src/denseLucasKanade_PyCL.py:113-169) and the lkDense kernel
+ * (src/pyrlkDenseLargeW.cl:304-669): per pixel, Scharr gradients over a
+ * (2*half_win+1)^2 window (half_win <= 15), <= niter Newton steps on a bilinear J
+ * (float32 weights), stop at |delta| < 0.01.  asym: {left,right,top,bottom} window
+ * masks (HOST array, may be NULL = all 0).  status (uint8, optional): 1 = tracked,
+ * 0 = singular / left the image.  err (float, optional): the kernel's mean |J-I|.
+ * Pixels with a singular gradient matrix keep their input U, V.
+ * ------------------------------------------------------------------------------- */
+int of_lk_dense(const float* I, const float* J, float* U, float* V, int H, int W, int pitch, int half_win, int niter,
+                const int* asym, uint8_t* status, float* err, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * A12-A19 Farneback — replaces Farneback_PyCL.compute (src/Farneback_PyCL.py:461-603)
+ * and its kernels (src/optical_flow_farneback.cl:72-429).  The planar 5-coefficient
+ * fields (RA, RB, M) are 5*H x W stacks with row pitch `pitch`.
+ * ------------------------------------------------------------------------------- */
+typedef struct {
+  int polyN;           /* 5 or 7 */
+  float g[8], xg[8], xxg[8]; /* polyN+1 taps (centre first), FarnebackPrepareGaussian */
+  float ig[4];         /* invG[1,1], invG[0,3], invG[3,3], invG[5,5] as float32 */
+} of_fb_poly_consts;
+
+/* gaussianBlur / gaussianBlur5 (:160-253): `planes` stacked planes, reflect-101 borders,
+ * half kernel gk[0..kh] (centre first, HOST array, kh <= 32). */
+int of_fb_blur(const float* src, float* dst, int H, int W, int pitch, int planes, const float* gk, int kh,
+               void* stream);
+/* boxFilter5 (:350-406), clamped borders. */
+int of_fb_box5(const float* src, float* dst, int H, int W, int pitch, int kh, void* stream);
+/* polynomialExpansion (:72-133): src H x W -> dst 5H x W. consts: HOST struct. */
+int of_fb_polyexp(const float* src, float* dst, int H, int W, int pitch, const of_fb_poly_consts* consts,
+                  void* stream);
+/* updateMatrices (:256-348): M from the flow and the two expansions. */
+int of_fb_update_matrices(const float* flowx, const float* flowy, const float* R0, const float* R1, float* M, int H,
+                          int W, int pitch, void* stream);
+/* updateFlow (:408-429). */
+int of_fb_update_flow(const float* M, float* flowx, float* flowy, int H, int W, int pitch, void* stream);
+/* One Farneback iteration fused (updateFlowGaussianBlur, src/Farneback_PyCL.py:441-456):
+ * blur5(M_in) with the half kernel wk[0..kh] (HOST array) -> updateFlow -> (if
+ * update_matrices) updateMatrices into M_out.  Same result as the three kernels above.
+ * M_in and M_out must not alias (the blur reads a (2kh+1)^2 neighbourhood). */
+int of_fb_iteration(const float* M_in, float* M_out, const float* R0, const float* R1, float* flowx, float* flowy,
+                    int H, int W, int pitch, const float* wk, int kh, int update_matrices, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OFB200_H */

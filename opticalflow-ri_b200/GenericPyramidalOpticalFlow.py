@@ -1,0 +1,149 @@
+"""Drop-in for the reference's GenericPyramidalOpticalFlow module
+(src/GenericPyramidalOpticalFlow.py): the coarse-to-fine driver that calls a main
+optical-flow adapter and an optional refining adapter per pyramid level.
+
+The whole pyramid runs on the GPU: the frames are uploaded once, each level's resize
+(PIL BICUBIC semantics), flow upsample (RectBivariateSpline semantics), bilinear warp,
+prefilter and the adapters' kernels run on the device, and U, V come back once.  Adapters
+from this package are driven through their device path; any other object implementing
+the reference's adapter protocol (compute / getAlgoName / hasGenericPyramidalDefaults /
+getGenericPyramidalDefaults) is called with numpy arrays, exactly like the reference.
+
+Not supported yet: the Liu-Shen optical-flow-equation warp (biLinear=False,
+:188-220) raises NotImplementedError.  Progress prints are off unless OFB200_VERBOSE=1.
+"""
+import numpy as np
+
+from gaussian_filter import prepareGaussianKernel
+from ofb200 import ops, to_device, is_host, to_host, log, _torch
+
+__all__ = ["genericPyramidalOpticalFlow", "updateNextPyramidalLevel", "doBiLinearWarping", "imresize"]
+
+
+def imresize(im, res):
+    """PIL BICUBIC resize of a float32 image to res = (width, height) (:66-67)."""
+    host = is_host(im)
+    out = ops.resize(to_device(im), res, bicubic=True)
+    return to_host(out) if host else out
+
+
+def doBiLinearWarping(img, coordsY, coordsX, order=1, mode='nearest'):
+    """:69-115: img sampled at float32 (coordsY, coordsX), round-half-even base index."""
+    host = is_host(img)
+    out = ops.warp_coords(to_device(img), to_device(np.float32(coordsY) if host else coordsY),
+                          to_device(np.float32(coordsX) if host else coordsX))
+    return to_host(out) if host else out
+
+
+def _prefilter(img, sigma, K):
+    return ops.prefilter(img, prepareGaussianKernel(sigma, K))
+
+
+def updateNextPyramidalLevel(im1IterNext, im1IterPrev, im2IterNext, Uaccum, Vaccum, U, V, warping=True,
+                             biLinear=True, scale=False):
+    """:117-234 on device tensors (numpy inputs are accepted and returned as numpy)."""
+    host = is_host(im1IterNext)
+    d = to_device
+    n1, n2, Ua, Va = d(im1IterNext), d(im2IterNext), d(Uaccum), d(Vaccum)
+    res = _transition(n1, tuple(im1IterPrev.shape), n2, Ua, Va, warping, biLinear, scale)
+    return tuple(to_host(t) for t in res) if host else res
+
+
+def _transition(n1, prev_shape, n2, Ua, Va, warping, biLinear, scale):
+    torch = _torch()
+    H, W = n1.shape
+    h, w = prev_shape
+    sx = np.float32(np.float32(W) / np.float32(w)) if scale else np.float32(1.0)
+    sy = np.float32(np.float32(H) / np.float32(h)) if scale else np.float32(1.0)
+    if (h, w) != (H, W):
+        us = ops.spline_upsample(Ua, H, W, sx)
+        vs = ops.spline_upsample(Va, H, W, sy)
+    else:
+        us = ops.scale(Ua, sx) if scale else Ua
+        vs = ops.scale(Va, sy) if scale else Va
+    if warping:
+        if not biLinear:
+            raise NotImplementedError("Liu-Shen optical-flow-equation warp (biLinear=False)")
+        O0, O1 = ops.warp_pair(n1, n2, us, vs)
+        return O0, O1, us, vs, torch.zeros_like(n1), torch.zeros_like(n1)
+    return n1, n2, torch.zeros_like(n1), torch.zeros_like(n1), us, vs
+
+
+def _adapter_call(adapter, I0, I1, U, V):
+    if hasattr(adapter, "_compute_dev"):
+        return adapter._compute_dev(I0, I1, U, V)
+    u, v, e = adapter.compute(to_host(I0), to_host(I1), to_host(U), to_host(V))
+    return to_device(u), to_device(v), e
+
+
+def genericPyramidalOpticalFlow(im1, im2, FILTER, mainOFlowAlgoAdapter, pyramidalLevels=1, kLevels=1,
+                                FILTER_OPT=None, optionalOFlowAlgoAdapter=None, warping=True, biLinear=True,
+                                pyramidalIntermediateScaling=True, pyramidalScaling=False):
+    """:237-415.  Returns (Uaccum, Vaccum): numpy arrays for numpy input, CUDA tensors for
+    tensor input."""
+    host = is_host(im1)
+    torch = _torch()
+    dev = getattr(mainOFlowAlgoAdapter, "device", None)
+    I1 = to_device(im1, dev)
+    I2 = to_device(im2, I1.device)
+    scale = 1.0 / (2.0 ** (pyramidalLevels - 1))
+    if mainOFlowAlgoAdapter.hasGenericPyramidalDefaults():
+        dm = mainOFlowAlgoAdapter.getGenericPyramidalDefaults()
+        if dm is not None:
+            warping = dm.get('warping', warping) if dm.get('warping') is not None else warping
+            biLinear = dm.get('biLinear') if dm.get('biLinear') is not None else biLinear
+            if dm.get('intermediateScaling') is not None:
+                pyramidalIntermediateScaling = dm.get('intermediateScaling')
+            if dm.get('scaling') is not None:
+                pyramidalScaling = dm.get('scaling')
+    U = V = Uacc = Vacc = None
+    work1 = None
+    for level in range(1, pyramidalLevels + 1):
+        lscale = pyramidalScaling if level == pyramidalLevels else pyramidalIntermediateScaling
+        prev_shape = None if work1 is None else tuple(work1.shape)
+        if scale < 1.0 and level != pyramidalLevels:
+            size = (int(np.round(I1.shape[1] * scale)), int(np.round(I1.shape[0] * scale)))
+            n1 = ops.resize(I1, size, bicubic=True)
+            n2 = ops.resize(I2, size, bicubic=True)
+        elif scale > 1.0:
+            raise Exception('Invalid scale level: ' + str(scale))
+        else:
+            n1, n2 = I1, I2
+        if level > 1:
+            w1, w2, Uacc, Vacc, U, V = _transition(n1, prev_shape, n2, Uacc, Vacc, warping, biLinear, lscale)
+        else:
+            w1, w2 = n1, n2
+            U = torch.zeros_like(n1)
+            V = torch.zeros_like(n1)
+            Uacc = torch.zeros_like(n1)
+            Vacc = torch.zeros_like(n1)
+        if FILTER > 1e-3:
+            work1, work2 = _prefilter(w1, FILTER, 3), _prefilter(w2, FILTER, 3)
+        else:
+            work1, work2 = w1, w2
+        if optionalOFlowAlgoAdapter is not None and FILTER_OPT is not None and FILTER_OPT > 1e-3:
+            opt1, opt2 = _prefilter(n1, FILTER_OPT, 5), _prefilter(n2, FILTER_OPT, 5)
+        elif optionalOFlowAlgoAdapter is not None:
+            opt1, opt2 = n1, n2
+        for k in range(kLevels):
+            log('Level=', level, ' kIter=', k)
+            if k > 0:
+                if warping:
+                    w1, w2, Uacc, Vacc, U, V = _transition(n1, tuple(n1.shape), n2, Uacc, Vacc, warping, biLinear,
+                                                           False)
+                    if FILTER > 1:
+                        work1, work2 = _prefilter(w1, FILTER, 3), _prefilter(w2, FILTER, 3)
+                    else:
+                        work1, work2 = w1, w2
+                else:
+                    work1, work2, Uacc, Vacc, U, V = _transition(work1, tuple(work1.shape), work2, Uacc, Vacc,
+                                                                 warping, biLinear, False)
+            U, V, error = _adapter_call(mainOFlowAlgoAdapter, work1, work2, U, V)
+            if optionalOFlowAlgoAdapter is not None:
+                U, V, errorOptional = _adapter_call(optionalOFlowAlgoAdapter, opt1, opt2, U, V)
+            Uacc = ops.accumulate(Uacc.clone(), U)
+            Vacc = ops.accumulate(Vacc.clone(), V)
+        scale *= 2
+    if host:
+        return to_host(Uacc), to_host(Vacc)
+    return Uacc, Vacc

@@ -1,0 +1,88 @@
+// Error reporting, version and the small elementwise entry points of the C ABI.
+#include <string.h>
+
+#include <atomic>
+
+#include "common.cuh"
+
+namespace ofb {
+
+static thread_local char g_err[1024] = "";
+static std::atomic<unsigned long long> g_launches{0};
+
+int set_error(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int check_launch(const char* what, long long nlaunch) {
+  g_launches.fetch_add((unsigned long long)nlaunch, std::memory_order_relaxed);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return OF_OK;
+}
+
+__global__ void u8_to_f32_kernel(const uint8_t* __restrict__ src, int sp, float* __restrict__ dst, int dp, int H,
+                                 int W) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x < W) dst[(size_t)y * dp + x] = (float)src[(size_t)y * sp + x];
+}
+
+__global__ void accumulate_kernel(float* __restrict__ dst, const float* __restrict__ src, int pitch, int W) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x < W) {
+    size_t i = (size_t)y * pitch + x;
+    dst[i] = __fadd_rn(dst[i], src[i]);
+  }
+}
+
+__global__ void scale_kernel(const float* __restrict__ src, float* __restrict__ dst, float s, int pitch, int W) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x < W) {
+    size_t i = (size_t)y * pitch + x;
+    dst[i] = __fmul_rn(src[i], s);
+  }
+}
+
+}  // namespace ofb
+
+using namespace ofb;
+
+extern "C" int of_version(void) { return 100; }
+
+extern "C" unsigned long long of_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+extern "C" int of_last_error(char* buf, size_t n) {
+  size_t len = strlen(g_err);
+  if (buf && n) {
+    size_t c = len < n - 1 ? len : n - 1;
+    memcpy(buf, g_err, c);
+    buf[c] = 0;
+  }
+  return (int)len;
+}
+
+extern "C" int of_u8_to_f32(const uint8_t* src, int src_pitch, float* dst, int dst_pitch, int H, int W,
+                            void* stream) {
+  OF_REQUIRE(!bad_plane(src, H, W, src_pitch) && !bad_plane(dst, H, W, dst_pitch), "of_u8_to_f32: bad plane");
+  dim3 grid((W + 255) / 256, H);
+  u8_to_f32_kernel<<<grid, 256, 0, as_stream(stream)>>>(src, src_pitch, dst, dst_pitch, H, W);
+  return check_launch("of_u8_to_f32");
+}
+
+extern "C" int of_accumulate(float* dst, const float* src, int H, int W, int pitch, void* stream) {
+  OF_REQUIRE(!bad_plane(dst, H, W, pitch) && src, "of_accumulate: bad plane");
+  dim3 grid((W + 255) / 256, H);
+  accumulate_kernel<<<grid, 256, 0, as_stream(stream)>>>(dst, src, pitch, W);
+  return check_launch("of_accumulate");
+}
+
+extern "C" int of_scale(const float* src, float* dst, float s, int H, int W, int pitch, void* stream) {
+  OF_REQUIRE(!bad_plane(dst, H, W, pitch) && src, "of_scale: bad plane");
+  dim3 grid((W + 255) / 256, H);
+  scale_kernel<<<grid, 256, 0, as_stream(stream)>>>(src, dst, s, pitch, W);
+  return check_launch("of_scale");
+}

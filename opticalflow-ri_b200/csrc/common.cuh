@@ -1,0 +1,69 @@
+// Shared helpers for the ofb200 kernels (sm_100a).
+//
+// The library is compiled with -fmad=false: every float/double multiply-add that the
+// kernels fuse is written as an explicit __fmaf_rn / __fma_rn, so the arithmetic order is
+// fixed by the source and matches the CPU oracle bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/ofb200.h"
+
+namespace ofb {
+
+int set_error(int code, const char* fmt, ...);
+// Reports the first launch error of an entry point; `nlaunch` kernel launches are added
+// to the process-wide counter behind of_launch_count().
+int check_launch(const char* what, long long nlaunch = 1);
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+__host__ __device__ inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// scipy.ndimage 'mirror' / OpenCV reflect-101 index for |i| < n (one reflection).
+__host__ __device__ inline int mirror1(int i, int n) {
+  if (n == 1) return 0;
+  if (i < 0) i = -i;
+  if (i >= n) i = 2 * n - 2 - i;
+  return i;
+}
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Carves typed sub-buffers out of a caller workspace.
+struct Carver {
+  char* base;
+  size_t cap, off;
+  Carver(void* b, size_t c) : base(static_cast<char*>(b)), cap(c), off(0) {}
+  template <class T>
+  T* take(size_t count) {
+    off = align_up(off, 256);
+    T* p = reinterpret_cast<T*>(base + off);
+    off += count * sizeof(T);
+    return p;
+  }
+  bool ok() const { return off <= cap; }
+};
+
+// Size bookkeeping with the same alignment rule as Carver.
+struct Sizer {
+  size_t off = 0;
+  template <class T>
+  void take(size_t count) {
+    off = align_up(off, 256);
+    off += count * sizeof(T);
+  }
+};
+
+inline bool bad_plane(const void* p, int H, int W, int pitch) { return !p || H <= 0 || W <= 0 || pitch < W; }
+
+constexpr int kNumSMs = 148;
+
+}  // namespace ofb
+
+#define OF_REQUIRE(cond, ...)                                        \
+  do {                                                               \
+    if (!(cond)) return ::ofb::set_error(OF_ERR_INVALID, __VA_ARGS__); \
+  } while (0)

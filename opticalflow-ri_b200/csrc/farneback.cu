@@ -1,0 +1,370 @@
+// A12-A19 Farneback kernels (src/optical_flow_farneback.cl:72-429).
+//
+// Arithmetic follows the OpenCL source with its multiply-adds fused the way the CPU
+// oracle fixes them (`acc += a*b` -> fmaf(a, b, acc); `a*b + c*d` -> fmaf(a, b, c*d)),
+// so GPU and oracle agree bit for bit.  Planar 5-coefficient fields are 5 stacked H x W
+// planes sharing one pitch.
+//
+// Kernels
+//  - fb_blur_kernel: separable Gaussian (vertical then horizontal, reflect-101), one plane
+//    per blockIdx.z; the input tile with its halo is staged in shared memory once.
+//  - fb_polyexp_kernel: 7- (or 5-) tap vertical moments of the clamped neighbourhood into
+//    shared memory, then the horizontal combination into the 5 coefficient planes.
+//  - fb_iter_kernel: one solver iteration fused — blur5 of M, updateFlow, and
+//    updateMatrices into the other M buffer — so M is read once per iteration and the
+//    blurred M never leaves the SM.
+#include "common.cuh"
+
+namespace ofb {
+
+constexpr int FB_MAXKH = 32;
+struct FbTaps {
+  float g[FB_MAXKH + 1];
+};
+
+__host__ __device__ __forceinline__ int fb_low(int y, int last) { return abs(y) % (last + 1); }
+__host__ __device__ __forceinline__ int fb_high(int y, int last) { return abs(last - abs(last - y)) % (last + 1); }
+// reflect-101 mapping of the gaussianBlur kernels (idx_row_low / idx_row_high / idx_col)
+__device__ __forceinline__ int fb_row(int y, int rows) {
+  if (y < 0) return fb_low(y, rows - 1);
+  if (y > rows - 1) return fb_high(y, rows - 1);
+  return y;
+}
+__device__ __forceinline__ int fb_col(int x, int cols) { return fb_low(fb_high(x, cols - 1), cols - 1); }
+
+constexpr int FBB_TW = 64, FBB_TH = 16;
+
+// Blur of plane blockIdx.z: out = H(V(src)).  smem: input (TH+2kh) x (TW+2kh), vertical
+// result TH x (TW+2kh).
+__global__ void __launch_bounds__(256) fb_blur_kernel(const float* __restrict__ src, float* __restrict__ dst, int H,
+                                                      int W, int pitch, FbTaps t, int kh) {
+  extern __shared__ float sm[];
+  const int iw = FBB_TW + 2 * kh, ih = FBB_TH + 2 * kh;
+  float* tin = sm;
+  float* tv = sm + ih * iw;
+  const size_t plane = (size_t)H * pitch * blockIdx.z;
+  const float* s = src + plane;
+  const int x0 = blockIdx.x * FBB_TW, y0 = blockIdx.y * FBB_TH;
+  for (int i = threadIdx.x; i < ih * iw; i += blockDim.x) {
+    int ly = i / iw, lx = i - ly * iw;
+    tin[i] = s[(size_t)fb_row(y0 - kh + ly, H) * pitch + fb_col(x0 - kh + lx, W)];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < FBB_TH * iw; i += blockDim.x) {
+    int ly = i / iw, lx = i - ly * iw;
+    const float* c = tin + (ly + kh) * iw + lx;
+    float acc = __fmul_rn(c[0], t.g[0]);
+    for (int j = 1; j <= kh; j++) acc = __fmaf_rn(__fadd_rn(c[-j * iw], c[j * iw]), t.g[j], acc);
+    tv[i] = acc;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < FBB_TH * FBB_TW; i += blockDim.x) {
+    int ly = i / FBB_TW, lx = i - ly * FBB_TW;
+    int y = y0 + ly, x = x0 + lx;
+    if (y >= H || x >= W) continue;
+    const float* r = tv + ly * iw + lx + kh;
+    float res = __fmul_rn(r[0], t.g[0]);
+    for (int j = 1; j <= kh; j++) res = __fmaf_rn(__fadd_rn(r[-j], r[j]), t.g[j], res);
+    dst[plane + (size_t)y * pitch + x] = res;
+  }
+}
+
+// boxFilter5 (:350-406): clamped borders, plain sums, one plane per blockIdx.z
+__global__ void __launch_bounds__(256) fb_box_kernel(const float* __restrict__ src, float* __restrict__ dst, int H,
+                                                     int W, int pitch, int kh, float inv) {
+  extern __shared__ float sm[];
+  const int iw = FBB_TW + 2 * kh, ih = FBB_TH + 2 * kh;
+  float* tin = sm;
+  float* tv = sm + ih * iw;
+  const size_t plane = (size_t)H * pitch * blockIdx.z;
+  const float* s = src + plane;
+  const int x0 = blockIdx.x * FBB_TW, y0 = blockIdx.y * FBB_TH;
+  for (int i = threadIdx.x; i < ih * iw; i += blockDim.x) {
+    int ly = i / iw, lx = i - ly * iw;
+    tin[i] = s[(size_t)clampi(y0 - kh + ly, 0, H - 1) * pitch + clampi(x0 - kh + lx, 0, W - 1)];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < FBB_TH * iw; i += blockDim.x) {
+    int ly = i / iw, lx = i - ly * iw;
+    const float* c = tin + (ly + kh) * iw + lx;
+    float acc = c[0];
+    for (int j = 1; j <= kh; j++) acc = __fadd_rn(acc, __fadd_rn(c[-j * iw], c[j * iw]));
+    tv[i] = acc;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < FBB_TH * FBB_TW; i += blockDim.x) {
+    int ly = i / FBB_TW, lx = i - ly * FBB_TW;
+    int y = y0 + ly, x = x0 + lx;
+    if (y >= H || x >= W) continue;
+    const float* r = tv + ly * iw + lx + kh;
+    float res = r[0];
+    for (int j = 1; j <= kh; j++) res = __fadd_rn(res, __fadd_rn(r[-j], r[j]));
+    dst[plane + (size_t)y * pitch + x] = __fmul_rn(res, inv);
+  }
+}
+
+struct FbPoly {
+  float g[8], xg[8], xxg[8], ig[4];
+  int n;
+};
+
+// polynomialExpansion: one CTA = 1 row segment of 256-2n outputs (the reference's
+// (256,1) work-group shape), vertical moments for 256 clamped columns in smem.
+constexpr int FBP_T = 256;
+__global__ void __launch_bounds__(FBP_T) fb_polyexp_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                                                           int H, int W, int pitch, FbPoly P) {
+  __shared__ float row[3][FBP_T];
+  const int n = P.n;
+  const int y = blockIdx.y, tx = threadIdx.x;
+  const int x = blockIdx.x * (FBP_T - 2 * n) + tx - n;
+  const int xw = clampi(x, 0, W - 1);
+  float r0 = __fmul_rn(src[(size_t)y * pitch + xw], P.g[0]), r1 = 0.f, r2 = 0.f;
+  for (int k = 1; k <= n; k++) {
+    float t0 = src[(size_t)max(y - k, 0) * pitch + xw];
+    float t1 = src[(size_t)min(y + k, H - 1) * pitch + xw];
+    r0 = __fmaf_rn(P.g[k], __fadd_rn(t0, t1), r0);
+    r1 = __fmaf_rn(P.xg[k], __fsub_rn(t1, t0), r1);
+    r2 = __fmaf_rn(P.xxg[k], __fadd_rn(t0, t1), r2);
+  }
+  row[0][tx] = r0;
+  row[1][tx] = r1;
+  row[2][tx] = r2;
+  __syncthreads();
+  if (tx >= n && tx + n < FBP_T && x < W) {
+    float b1 = __fmul_rn(P.g[0], row[0][tx]), b3 = __fmul_rn(P.g[0], row[1][tx]), b5 = __fmul_rn(P.g[0], row[2][tx]);
+    float b2 = 0.f, b4 = 0.f, b6 = 0.f;
+    for (int k = 1; k <= n; k++) {
+      float sp = __fadd_rn(row[0][tx + k], row[0][tx - k]), sm_ = __fsub_rn(row[0][tx + k], row[0][tx - k]);
+      b1 = __fmaf_rn(sp, P.g[k], b1);
+      b4 = __fmaf_rn(sp, P.xxg[k], b4);
+      b2 = __fmaf_rn(sm_, P.xg[k], b2);
+      b3 = __fmaf_rn(__fadd_rn(row[1][tx + k], row[1][tx - k]), P.g[k], b3);
+      b6 = __fmaf_rn(__fsub_rn(row[1][tx + k], row[1][tx - k]), P.xg[k], b6);
+      b5 = __fmaf_rn(__fadd_rn(row[2][tx + k], row[2][tx - k]), P.g[k], b5);
+    }
+    const size_t pl = (size_t)H * pitch, i = (size_t)y * pitch + x;
+    dst[i] = __fmul_rn(b3, P.ig[0]);
+    dst[pl + i] = __fmul_rn(b2, P.ig[0]);
+    dst[2 * pl + i] = __fmaf_rn(b1, P.ig[1], __fmul_rn(b5, P.ig[2]));
+    dst[3 * pl + i] = __fmaf_rn(b1, P.ig[1], __fmul_rn(b4, P.ig[2]));
+    dst[4 * pl + i] = __fmul_rn(b6, P.ig[3]);
+  }
+}
+
+__constant__ float c_border[6] = {0.14f, 0.14f, 0.4472f, 0.4472f, 0.4472f, 1.f};
+
+// updateMatrices for pixel (y, x) given its flow; writes the 5 M planes.
+__device__ __forceinline__ void fb_matrices_at(int y, int x, float dx, float dy, const float* __restrict__ R0,
+                                               const float* __restrict__ R1, float* __restrict__ M, int H, int W,
+                                               int pitch) {
+  const size_t pl = (size_t)H * pitch, i = (size_t)y * pitch + x;
+  float fx = __fadd_rn((float)x, dx), fy = __fadd_rn((float)y, dy);
+  float flx = floorf(fx), fly = floorf(fy);
+  int x1 = (int)flx, y1 = (int)fly;
+  fx = __fsub_rn(fx, (float)x1);
+  fy = __fsub_rn(fy, (float)y1);
+  float r2, r3, r4, r5, r6;
+  if (x1 >= 0 && y1 >= 0 && x1 < W - 1 && y1 < H - 1) {
+    float a00 = __fmul_rn(__fsub_rn(1.f, fx), __fsub_rn(1.f, fy)), a01 = __fmul_rn(fx, __fsub_rn(1.f, fy));
+    float a10 = __fmul_rn(__fsub_rn(1.f, fx), fy), a11 = __fmul_rn(fx, fy);
+    float rr[5];
+    const size_t j = (size_t)y1 * pitch + x1;
+#pragma unroll
+    for (int p = 0; p < 5; p++) {
+      const float* R = R1 + p * pl;
+      float tt = __fmaf_rn(a00, R[j], __fmul_rn(a01, R[j + 1]));
+      tt = __fmaf_rn(a10, R[j + pitch], tt);
+      tt = __fmaf_rn(a11, R[j + pitch + 1], tt);
+      rr[p] = tt;
+    }
+    r2 = rr[0];
+    r3 = rr[1];
+    r4 = __fmul_rn(__fadd_rn(R0[2 * pl + i], rr[2]), 0.5f);
+    r5 = __fmul_rn(__fadd_rn(R0[3 * pl + i], rr[3]), 0.5f);
+    r6 = __fmul_rn(__fadd_rn(R0[4 * pl + i], rr[4]), 0.25f);
+  } else {
+    r2 = r3 = 0.f;
+    r4 = R0[2 * pl + i];
+    r5 = R0[3 * pl + i];
+    r6 = __fmul_rn(R0[4 * pl + i], 0.5f);
+  }
+  r2 = __fmul_rn(__fsub_rn(R0[i], r2), 0.5f);
+  r3 = __fmul_rn(__fsub_rn(R0[pl + i], r3), 0.5f);
+  r2 = __fadd_rn(r2, __fmaf_rn(r4, dy, __fmul_rn(r6, dx)));
+  r3 = __fadd_rn(r3, __fmaf_rn(r6, dy, __fmul_rn(r5, dx)));
+  float scale = __fmul_rn(c_border[min(x, 5)], c_border[min(y, 5)]);
+  scale = __fmul_rn(scale, c_border[min(W - x - 1, 5)]);
+  scale = __fmul_rn(scale, c_border[min(H - y - 1, 5)]);
+  r2 = __fmul_rn(r2, scale);
+  r3 = __fmul_rn(r3, scale);
+  r4 = __fmul_rn(r4, scale);
+  r5 = __fmul_rn(r5, scale);
+  r6 = __fmul_rn(r6, scale);
+  M[i] = __fmaf_rn(r4, r4, __fmul_rn(r6, r6));
+  M[pl + i] = __fmul_rn(__fadd_rn(r4, r5), r6);
+  M[2 * pl + i] = __fmaf_rn(r5, r5, __fmul_rn(r6, r6));
+  M[3 * pl + i] = __fmaf_rn(r4, r2, __fmul_rn(r6, r3));
+  M[4 * pl + i] = __fmaf_rn(r6, r2, __fmul_rn(r5, r3));
+}
+
+__device__ __forceinline__ void fb_flow_from(float g11, float g12, float g22, float h1, float h2, float* fx,
+                                             float* fy) {
+  float detInv = __fdiv_rn(1.f, __fadd_rn(__fmaf_rn(g11, g22, -__fmul_rn(g12, g12)), 1e-3f));
+  *fx = __fmul_rn(__fmaf_rn(g11, h2, -__fmul_rn(g12, h1)), detInv);
+  *fy = __fmul_rn(__fmaf_rn(g22, h1, -__fmul_rn(g12, h2)), detInv);
+}
+
+__global__ void fb_update_matrices_kernel(const float* __restrict__ flowx, const float* __restrict__ flowy,
+                                          const float* __restrict__ R0, const float* __restrict__ R1,
+                                          float* __restrict__ M, int H, int W, int pitch) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  size_t i = (size_t)y * pitch + x;
+  fb_matrices_at(y, x, flowx[i], flowy[i], R0, R1, M, H, W, pitch);
+}
+
+__global__ void fb_update_flow_kernel(const float* __restrict__ M, float* __restrict__ flowx, float* __restrict__ flowy,
+                                      int H, int W, int pitch) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  const size_t pl = (size_t)H * pitch, i = (size_t)y * pitch + x;
+  float fx, fy;
+  fb_flow_from(M[i], M[pl + i], M[2 * pl + i], M[3 * pl + i], M[4 * pl + i], &fx, &fy);
+  flowx[i] = fx;
+  flowy[i] = fy;
+}
+
+// Fused iteration.  CTA tile: FBI_TW x FBI_TH outputs, all 5 planes.  Per plane the input
+// tile (+kh halo) is staged, blurred vertically into tv, horizontally into registers; the
+// 5 blurred values of each output pixel then feed updateFlow and updateMatrices.
+constexpr int FBI_TW = 32, FBI_TH = 16;
+__global__ void __launch_bounds__(256) fb_iter_kernel(const float* __restrict__ Min, float* __restrict__ Mout,
+                                                      const float* __restrict__ R0, const float* __restrict__ R1,
+                                                      float* __restrict__ flowx, float* __restrict__ flowy, int H,
+                                                      int W, int pitch, FbTaps t, int kh, int upd) {
+  extern __shared__ float sm[];
+  const int iw = FBI_TW + 2 * kh, ih = FBI_TH + 2 * kh;
+  float* tin = sm;
+  float* tv = sm + ih * iw;
+  const size_t pl = (size_t)H * pitch;
+  const int x0 = blockIdx.x * FBI_TW, y0 = blockIdx.y * FBI_TH;
+  // each thread owns 2 output pixels of the 32x16 tile
+  float res[2][5];
+#pragma unroll
+  for (int p = 0; p < 5; p++) {
+    const float* s = Min + p * pl;
+    for (int i = threadIdx.x; i < ih * iw; i += blockDim.x) {
+      int ly = i / iw, lx = i - ly * iw;
+      tin[i] = s[(size_t)fb_row(y0 - kh + ly, H) * pitch + fb_col(x0 - kh + lx, W)];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < FBI_TH * iw; i += blockDim.x) {
+      int ly = i / iw, lx = i - ly * iw;
+      const float* c = tin + (ly + kh) * iw + lx;
+      float acc = __fmul_rn(c[0], t.g[0]);
+      for (int j = 1; j <= kh; j++) acc = __fmaf_rn(__fadd_rn(c[-j * iw], c[j * iw]), t.g[j], acc);
+      tv[i] = acc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      int o = threadIdx.x + q * 256;
+      int ly = o / FBI_TW, lx = o - ly * FBI_TW;
+      const float* r = tv + ly * iw + lx + kh;
+      float v = __fmul_rn(r[0], t.g[0]);
+      for (int j = 1; j <= kh; j++) v = __fmaf_rn(__fadd_rn(r[-j], r[j]), t.g[j], v);
+      res[q][p] = v;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    int o = threadIdx.x + q * 256;
+    int ly = o / FBI_TW, lx = o - ly * FBI_TW;
+    int y = y0 + ly, x = x0 + lx;
+    if (y >= H || x >= W) continue;
+    float fx, fy;
+    fb_flow_from(res[q][0], res[q][1], res[q][2], res[q][3], res[q][4], &fx, &fy);
+    size_t i = (size_t)y * pitch + x;
+    flowx[i] = fx;
+    flowy[i] = fy;
+    if (upd) fb_matrices_at(y, x, fx, fy, R0, R1, Mout, H, W, pitch);
+  }
+}
+
+static FbTaps make_taps(const float* gk, int kh) {
+  FbTaps t{};
+  for (int j = 0; j <= kh; j++) t.g[j] = gk[j];
+  return t;
+}
+
+}  // namespace ofb
+
+using namespace ofb;
+
+extern "C" int of_fb_blur(const float* src, float* dst, int H, int W, int pitch, int planes, const float* gk, int kh,
+                          void* stream) {
+  OF_REQUIRE(!bad_plane(src, H, W, pitch) && dst && src != dst, "of_fb_blur: bad plane");
+  OF_REQUIRE(gk && kh >= 0 && kh <= FB_MAXKH && planes >= 1 && planes <= 65535, "of_fb_blur: bad kernel");
+  size_t smem = sizeof(float) * ((size_t)(FBB_TH + 2 * kh) * (FBB_TW + 2 * kh) + (size_t)FBB_TH * (FBB_TW + 2 * kh));
+  if (smem > 48 * 1024) cudaFuncSetAttribute(fb_blur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+  dim3 grid((W + FBB_TW - 1) / FBB_TW, (H + FBB_TH - 1) / FBB_TH, planes);
+  fb_blur_kernel<<<grid, 256, smem, as_stream(stream)>>>(src, dst, H, W, pitch, make_taps(gk, kh), kh);
+  return check_launch("of_fb_blur");
+}
+
+extern "C" int of_fb_box5(const float* src, float* dst, int H, int W, int pitch, int kh, void* stream) {
+  OF_REQUIRE(!bad_plane(src, H, W, pitch) && dst && src != dst, "of_fb_box5: bad plane");
+  OF_REQUIRE(kh >= 0 && kh <= FB_MAXKH, "of_fb_box5: bad kernel");
+  size_t smem = sizeof(float) * ((size_t)(FBB_TH + 2 * kh) * (FBB_TW + 2 * kh) + (size_t)FBB_TH * (FBB_TW + 2 * kh));
+  if (smem > 48 * 1024) cudaFuncSetAttribute(fb_box_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+  dim3 grid((W + FBB_TW - 1) / FBB_TW, (H + FBB_TH - 1) / FBB_TH, 5);
+  float inv = 1.f / (float)((1 + 2 * kh) * (1 + 2 * kh));
+  fb_box_kernel<<<grid, 256, smem, as_stream(stream)>>>(src, dst, H, W, pitch, kh, inv);
+  return check_launch("of_fb_box5");
+}
+
+extern "C" int of_fb_polyexp(const float* src, float* dst, int H, int W, int pitch, const of_fb_poly_consts* c,
+                             void* stream) {
+  OF_REQUIRE(!bad_plane(src, H, W, pitch) && dst && c, "of_fb_polyexp: bad plane");
+  OF_REQUIRE(c->polyN >= 1 && c->polyN <= 7, "of_fb_polyexp: polyN must be in 1..7");
+  FbPoly P{};
+  P.n = c->polyN;
+  for (int k = 0; k <= P.n; k++) {
+    P.g[k] = c->g[k];
+    P.xg[k] = c->xg[k];
+    P.xxg[k] = c->xxg[k];
+  }
+  for (int k = 0; k < 4; k++) P.ig[k] = c->ig[k];
+  dim3 grid((W + (FBP_T - 2 * P.n) - 1) / (FBP_T - 2 * P.n), H);
+  fb_polyexp_kernel<<<grid, FBP_T, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P);
+  return check_launch("of_fb_polyexp");
+}
+
+extern "C" int of_fb_update_matrices(const float* flowx, const float* flowy, const float* R0, const float* R1, float* M,
+                                     int H, int W, int pitch, void* stream) {
+  OF_REQUIRE(!bad_plane(flowx, H, W, pitch) && flowy && R0 && R1 && M, "of_fb_update_matrices: bad plane");
+  dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8);
+  fb_update_matrices_kernel<<<grd, blk, 0, as_stream(stream)>>>(flowx, flowy, R0, R1, M, H, W, pitch);
+  return check_launch("of_fb_update_matrices");
+}
+
+extern "C" int of_fb_update_flow(const float* M, float* flowx, float* flowy, int H, int W, int pitch, void* stream) {
+  OF_REQUIRE(!bad_plane(M, H, W, pitch) && flowx && flowy, "of_fb_update_flow: bad plane");
+  dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8);
+  fb_update_flow_kernel<<<grd, blk, 0, as_stream(stream)>>>(M, flowx, flowy, H, W, pitch);
+  return check_launch("of_fb_update_flow");
+}
+
+extern "C" int of_fb_iteration(const float* M_in, float* M_out, const float* R0, const float* R1, float* flowx,
+                               float* flowy, int H, int W, int pitch, const float* wk, int kh, int update_matrices,
+                               void* stream) {
+  OF_REQUIRE(!bad_plane(M_in, H, W, pitch) && R0 && R1 && flowx && flowy, "of_fb_iteration: bad plane");
+  OF_REQUIRE(!update_matrices || (M_out && M_out != M_in), "of_fb_iteration: M_out missing or aliases M_in");
+  OF_REQUIRE(wk && kh >= 0 && kh <= FB_MAXKH, "of_fb_iteration: bad kernel");
+  size_t smem = sizeof(float) * ((size_t)(FBI_TH + 2 * kh) * (FBI_TW + 2 * kh) + (size_t)FBI_TH * (FBI_TW + 2 * kh));
+  dim3 grid((W + FBI_TW - 1) / FBI_TW, (H + FBI_TH - 1) / FBI_TH);
+  fb_iter_kernel<<<grid, 256, smem, as_stream(stream)>>>(M_in, M_out, R0, R1, flowx, flowy, H, W, pitch,
+                                                         make_taps(wk, kh), kh, update_matrices);
+  return check_launch("of_fb_iteration");
+}

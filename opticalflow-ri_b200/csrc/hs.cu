@@ -1,0 +1,169 @@
+// A6/A7 Horn-Schunck (src/HornSchunck.py:28-126), bit-exact with the reference.
+//
+// Derivatives: the 2x2 correlations of computeDerivatives(frame1, frame0) with scipy's
+// 'mirror' border, each accumulated in double over the non-zero weights in C order and
+// rounded to float32.  Sweep: the 3x3 averaging kernel (weights float32(1/12),
+// float32(1/6)) accumulated the same way, then HS_helper2's float32 update.
+// Layout: U, V, fx, fy, ft are H x W float32 planes with a shared pitch.  A sweep reads
+// 3 coefficient planes and the two 3x3 neighbourhoods (served by L1) and writes U, V:
+// 28 B per pixel of HBM/L2 traffic.
+#include "common.cuh"
+
+namespace ofb {
+
+__device__ __forceinline__ double dacc(double a, float v, double w) { return __dadd_rn(a, __dmul_rn((double)v, w)); }
+
+__global__ void hs_deriv_kernel(const float* __restrict__ f0, const float* __restrict__ f1, float* __restrict__ fx,
+                                float* __restrict__ fy, float* __restrict__ ft, int H, int W, int pitch) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  int y1 = mirror1(y + 1, H), x1 = mirror1(x + 1, W);
+  size_t i00 = (size_t)y * pitch + x, i01 = (size_t)y * pitch + x1, i10 = (size_t)y1 * pitch + x, i11 = (size_t)y1 * pitch + x1;
+  float a00 = f1[i00], a01 = f1[i01], a10 = f1[i10], a11 = f1[i11];  // frame t1
+  float b00 = f0[i00], b01 = f0[i01], b10 = f0[i10], b11 = f0[i11];  // frame t0
+  // kernelX flipped: +.25 -.25 / +.25 -.25 ; kernelY flipped: +.25 +.25 / -.25 -.25
+  double t;
+  t = dacc(dacc(dacc(dacc(0.0, a00, 0.25), a01, -0.25), a10, 0.25), a11, -0.25);
+  float gx1 = (float)t;
+  t = dacc(dacc(dacc(dacc(0.0, b00, 0.25), b01, -0.25), b10, 0.25), b11, -0.25);
+  float gx0 = (float)t;
+  t = dacc(dacc(dacc(dacc(0.0, a00, 0.25), a01, 0.25), a10, -0.25), a11, -0.25);
+  float gy1 = (float)t;
+  t = dacc(dacc(dacc(dacc(0.0, b00, 0.25), b01, 0.25), b10, -0.25), b11, -0.25);
+  float gy0 = (float)t;
+  t = dacc(dacc(dacc(dacc(0.0, b00, 0.25), b01, 0.25), b10, 0.25), b11, 0.25);
+  float gt0 = (float)t;
+  t = dacc(dacc(dacc(dacc(0.0, a00, -0.25), a01, -0.25), a10, -0.25), a11, -0.25);
+  float gt1 = (float)t;
+  fx[i00] = __fadd_rn(gx1, gx0);
+  fy[i00] = __fadd_rn(gy1, gy0);
+  ft[i00] = __fadd_rn(gt0, gt1);
+}
+
+__global__ void hs_sweep_kernel(const float* __restrict__ fx, const float* __restrict__ fy,
+                                const float* __restrict__ ft, const float* __restrict__ U, const float* __restrict__ V,
+                                float* __restrict__ Un, float* __restrict__ Vn, int H, int W, int pitch, float a2) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  const double wc = (double)(1.0f / 12.0f), we = (double)(1.0f / 6.0f);
+  int ym = mirror1(y - 1, H), yp = mirror1(y + 1, H), xm = mirror1(x - 1, W), xp = mirror1(x + 1, W);
+  const size_t rm = (size_t)ym * pitch, r0 = (size_t)y * pitch, rp = (size_t)yp * pitch;
+  double su = 0.0, sv = 0.0;
+  su = dacc(su, U[rm + xm], wc); sv = dacc(sv, V[rm + xm], wc);
+  su = dacc(su, U[rm + x], we);  sv = dacc(sv, V[rm + x], we);
+  su = dacc(su, U[rm + xp], wc); sv = dacc(sv, V[rm + xp], wc);
+  su = dacc(su, U[r0 + xm], we); sv = dacc(sv, V[r0 + xm], we);
+  su = dacc(su, U[r0 + xp], we); sv = dacc(sv, V[r0 + xp], we);
+  su = dacc(su, U[rp + xm], wc); sv = dacc(sv, V[rp + xm], wc);
+  su = dacc(su, U[rp + x], we);  sv = dacc(sv, V[rp + x], we);
+  su = dacc(su, U[rp + xp], wc); sv = dacc(sv, V[rp + xp], wc);
+  float ua = (float)su, va = (float)sv;
+  size_t i = r0 + x;
+  float gx = fx[i], gy = fy[i];
+  float num = __fadd_rn(__fadd_rn(__fmul_rn(gx, ua), __fmul_rn(gy, va)), ft[i]);
+  float den = __fadd_rn(__fadd_rn(a2, __fmul_rn(gx, gx)), __fmul_rn(gy, gy));
+  float der = __fdiv_rn(num, den);
+  Un[i] = __fsub_rn(ua, __fmul_rn(gx, der));
+  Vn[i] = __fsub_rn(va, __fmul_rn(gy, der));
+}
+
+__global__ void copy2_kernel(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ ao,
+                             float* __restrict__ bo, int W, int pitch) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x < W) {
+    size_t i = (size_t)y * pitch + x;
+    ao[i] = a[i];
+    bo[i] = b[i];
+  }
+}
+
+// sum of squared differences of two plane pairs into acc[0], acc[1] (double atomics)
+__global__ void sqdiff2_kernel(const float* __restrict__ a, const float* __restrict__ a0, const float* __restrict__ b,
+                               const float* __restrict__ b0, int H, int W, int pitch, double* acc) {
+  double sa = 0.0, sb = 0.0;
+  for (int y = blockIdx.y; y < H; y += gridDim.y)
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x) {
+      size_t i = (size_t)y * pitch + x;
+      double da = (double)a[i] - (double)a0[i], db = (double)b[i] - (double)b0[i];
+      sa += da * da;
+      sb += db * db;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    sa += __shfl_down_sync(0xffffffffu, sa, o);
+    sb += __shfl_down_sync(0xffffffffu, sb, o);
+  }
+  __shared__ double ra[32], rb[32];
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { ra[w] = sa; rb[w] = sb; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); k++) { sa += ra[k]; sb += rb[k]; }
+    atomicAdd(acc, sa);
+    atomicAdd(acc + 1, sb);
+  }
+}
+
+__global__ void hs_err_kernel(const double* acc, double n, double* err_out) {
+  *err_out = (sqrt(acc[0]) + sqrt(acc[1])) / n;
+}
+
+}  // namespace ofb
+
+using namespace ofb;
+
+extern "C" int of_hs_derivatives(const float* I0, const float* I1, float* fx, float* fy, float* ft, int H, int W,
+                                 int pitch, void* stream) {
+  OF_REQUIRE(!bad_plane(I0, H, W, pitch) && I1 && fx && fy && ft, "of_hs_derivatives: bad plane");
+  dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8);
+  hs_deriv_kernel<<<grd, blk, 0, as_stream(stream)>>>(I0, I1, fx, fy, ft, H, W, pitch);
+  return check_launch("of_hs_derivatives");
+}
+
+extern "C" size_t of_hs_workspace_size(int H, int W, int pitch) {
+  Sizer s;
+  size_t N = (size_t)H * pitch;
+  for (int i = 0; i < 7; i++) s.take<float>(N);
+  s.take<double>(2);
+  return s.off;
+}
+
+extern "C" int of_hs_solve(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float alpha,
+                           int niter, double* err_out, void* workspace, size_t workspace_bytes, void* stream) {
+  OF_REQUIRE(!bad_plane(I0, H, W, pitch) && I1 && U && V, "of_hs_solve: bad plane");
+  OF_REQUIRE(niter >= 0, "of_hs_solve: niter < 0");
+  if (!workspace || workspace_bytes < of_hs_workspace_size(H, W, pitch))
+    return set_error(OF_ERR_WORKSPACE, "of_hs_solve: workspace too small (%zu < %zu)", workspace_bytes,
+                     of_hs_workspace_size(H, W, pitch));
+  cudaStream_t st = as_stream(stream);
+  size_t N = (size_t)H * pitch;
+  Carver c(workspace, workspace_bytes);
+  float *fx = c.take<float>(N), *fy = c.take<float>(N), *ft = c.take<float>(N);
+  float *U0 = c.take<float>(N), *V0 = c.take<float>(N), *Ub = c.take<float>(N), *Vb = c.take<float>(N);
+  double* acc = c.take<double>(2);
+  dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8);
+  dim3 rgrid((W + 255) / 256, H);
+  hs_deriv_kernel<<<grd, blk, 0, st>>>(I0, I1, fx, fy, ft, H, W, pitch);
+  copy2_kernel<<<rgrid, 256, 0, st>>>(U, V, U0, V0, W, pitch);
+  float a2 = alpha * alpha;
+  for (int k = 0; k < niter; k++) {
+    const float *su, *sv;
+    float *du, *dv;
+    if (k == 0) { su = U0; sv = V0; du = U; dv = V; }
+    else if (k & 1) { su = U; sv = V; du = Ub; dv = Vb; }
+    else { su = Ub; sv = Vb; du = U; dv = V; }
+    hs_sweep_kernel<<<grd, blk, 0, st>>>(fx, fy, ft, su, sv, du, dv, H, W, pitch, a2);
+  }
+  long long n = 2 + niter;
+  if (niter > 0 && ((niter - 1) & 1)) {
+    copy2_kernel<<<rgrid, 256, 0, st>>>(Ub, Vb, U, V, W, pitch);
+    n += 1;
+  }
+  if (err_out) {
+    cudaMemsetAsync(acc, 0, 2 * sizeof(double), st);
+    dim3 g2((W + 255) / 256 < 4 ? (W + 255) / 256 : 4, H < 256 ? H : 256);
+    sqdiff2_kernel<<<g2, 256, 0, st>>>(U, U0, V, V0, H, W, pitch, acc);
+    hs_err_kernel<<<1, 1, 0, st>>>(acc, (double)H * (double)W, err_out);
+    n += 2;
+  }
+  return check_launch("of_hs_solve", n);
+}

@@ -1,0 +1,250 @@
+// A10/A11 dense pyramidal Lucas-Kanade (src/pyrlkDenseLargeW.cl:304-669 with
+// -DWSX/-DWSY as set by src/denseLucasKanade_PyCL.py:57-71).
+//
+// The reference runs one 64-work-item group per pixel.  Here one WARP handles one pixel
+// and a CTA handles an 8x8 pixel tile whose window data is shared: the intensity patch
+// (41x41 with the Scharr border, clamp-to-edge) and its unweighted Scharr gradients
+// (39x39) are staged once per CTA in shared memory.  Lane l plays the reference's work
+// items l and l+32 (xid = l&7, yid = l>>3 and yid+4), so the first level of the
+// reference's 64->1 reduction tree is an in-lane add and the rest are warp shuffles in
+// the same pairing: A, b and the error are reduced in exactly the reference's order.
+// J is sampled with exact float32 bilinear weights (pixel-centre convention, clamp to
+// edge) through L1.  Compute bound: ~7e4 FP32 flops per pixel at a 27x27 window and
+// 5 Newton steps.
+#include <float.h>
+
+#include "common.cuh"
+
+namespace ofb {
+
+constexpr int LK_PT = 8;            // pixel tile edge
+constexpr int LK_G = LK_PT + 31;    // gradient positions per axis
+constexpr int LK_I = LK_G + 2;      // intensity positions per axis
+
+struct LkParams {
+  int ws, hw, aL, aR, aT, aB, niter;
+};
+
+// per-axis tile weights of work item `id` (:339-373); base[] feeds the error guards
+__device__ __forceinline__ void lk_weights(int id, int ws, int lo, int hi, float w[4], int base[2]) {
+  if (ws >= 16) {
+    base[0] = 16 + id;
+    base[1] = 24 + id;
+    w[0] = 1.f;
+    w[1] = id == 0 ? (float)(1 - lo) : 1.f;
+    w[2] = base[0] < ws - hi ? 1.f : 0.f;
+    w[3] = base[1] < ws - hi ? 1.f : 0.f;
+  } else {
+    base[0] = 8 + id;
+    base[1] = 16 + id;
+    w[0] = 1.f;
+    w[1] = id == 0 ? (float)(1 - lo) : (base[0] < ws - hi ? 1.f : 0.f);
+    w[2] = 0.f;
+    w[3] = 0.f;
+  }
+}
+
+__device__ __forceinline__ float lk_bilinear(const float* __restrict__ J, int H, int W, int pitch, float x, float y) {
+  float xs = __fsub_rn(x, 0.5f), ys = __fsub_rn(y, 0.5f);
+  float fx0 = floorf(xs), fy0 = floorf(ys);
+  float a = __fsub_rn(xs, fx0), b = __fsub_rn(ys, fy0);
+  int i0 = (int)fx0, j0 = (int)fy0;
+  int xa = clampi(i0, 0, W - 1), xb = clampi(i0 + 1, 0, W - 1);
+  int ya = clampi(j0, 0, H - 1), yb = clampi(j0 + 1, 0, H - 1);
+  float t00 = __ldg(J + (size_t)ya * pitch + xa), t10 = __ldg(J + (size_t)ya * pitch + xb);
+  float t01 = __ldg(J + (size_t)yb * pitch + xa), t11 = __ldg(J + (size_t)yb * pitch + xb);
+  float oa = __fsub_rn(1.f, a), ob = __fsub_rn(1.f, b);
+  float r = __fmul_rn(__fmul_rn(oa, ob), t00);
+  r = __fmaf_rn(__fmul_rn(a, ob), t10, r);
+  r = __fmaf_rn(__fmul_rn(oa, b), t01, r);
+  r = __fmaf_rn(__fmul_rn(a, b), t11, r);
+  return r;
+}
+
+// the reference's reduce tree: (t, t+32) in-lane, then 16, 8, 4, (0+1)+(2+3)
+__device__ __forceinline__ float lk_tree(float lo, float hi) {
+  float q = __fadd_rn(lo, hi);
+  q = __fadd_rn(q, __shfl_down_sync(0xffffffffu, q, 16));
+  q = __fadd_rn(q, __shfl_down_sync(0xffffffffu, q, 8));
+  q = __fadd_rn(q, __shfl_down_sync(0xffffffffu, q, 4));
+  float a = __fadd_rn(q, __shfl_down_sync(0xffffffffu, q, 1));
+  float t = __fadd_rn(a, __shfl_down_sync(0xffffffffu, a, 2));
+  return __shfl_sync(0xffffffffu, t, 0);
+}
+
+__global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__ I, const float* __restrict__ J,
+                                                       float* __restrict__ U, float* __restrict__ V, int H, int W,
+                                                       int pitch, LkParams p, uint8_t* __restrict__ status,
+                                                       float* __restrict__ err) {
+  __shared__ float sI[LK_I * LK_I];
+  __shared__ float sDx[LK_G * LK_G], sDy[LK_G * LK_G];
+  const int i0 = blockIdx.y * LK_PT, j0 = blockIdx.x * LK_PT;
+  const int oy = i0 - p.hw - 1, ox = j0 - p.hw - 1;  // image position of sI[0][0]
+  for (int t = threadIdx.x; t < LK_I * LK_I; t += blockDim.x) {
+    int ly = t / LK_I, lx = t - ly * LK_I;
+    sI[t] = I[(size_t)clampi(oy + ly, 0, H - 1) * pitch + clampi(ox + lx, 0, W - 1)];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < LK_G * LK_G; t += blockDim.x) {
+    int gy = t / LK_G, gx = t - gy * LK_G;
+    const float* c = sI + (gy + 1) * LK_I + gx + 1;
+#define P(dy, dx) c[(dy) * LK_I + (dx)]
+    sDx[t] = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(-1, 1), P(1, 1)), P(-1, -1)), P(1, -1)), 3.0f,
+                       __fmul_rn(__fsub_rn(P(0, 1), P(0, -1)), 10.0f));
+    sDy[t] = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(1, -1), P(1, 1)), P(-1, -1)), P(-1, 1)), 3.0f,
+                       __fmul_rn(__fsub_rn(P(1, 0), P(-1, 0)), 10.0f));
+#undef P
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int xid = lane & 7, yid = lane >> 3;
+  float wx[4], wy0[4], wy1[4];
+  int bx[2], by0[2], by1[2];
+  lk_weights(xid, p.ws, p.aL, p.aR, wx, bx);
+  lk_weights(yid, p.ws, p.aT, p.aB, wy0, by0);
+  lk_weights(yid + 4, p.ws, p.aT, p.aB, wy1, by1);
+  const float hw = (float)p.hw;
+  const int i = i0 + warp;
+  if (i >= H) return;
+  for (int c = 0; c < LK_PT; c++) {
+    const int j = j0 + c;
+    if (j >= W) break;
+    const int gyb = warp, gxb = c;  // gradient-tile origin of this pixel's window
+    float a11[2] = {0.f, 0.f}, a12[2] = {0.f, 0.f}, a22[2] = {0.f, 0.f};
+#pragma unroll
+    for (int v = 0; v < 2; v++) {
+      const float* wy = v ? wy1 : wy0;
+      const int yy = yid + 4 * v;
+#pragma unroll
+      for (int ty = 0; ty < 4; ty++)
+#pragma unroll
+        for (int tx = 0; tx < 4; tx++) {
+          float w = __fmul_rn(wx[tx], wy[ty]);
+          if (w == 0.f) continue;
+          int g = (gyb + ty * 8 + yy) * LK_G + gxb + tx * 8 + xid;
+          float dx = __fmul_rn(sDx[g], w), dy = __fmul_rn(sDy[g], w);
+          a11[v] = __fmaf_rn(dx, dx, a11[v]);
+          a12[v] = __fmaf_rn(dx, dy, a12[v]);
+          a22[v] = __fmaf_rn(dy, dy, a22[v]);
+        }
+    }
+    float A11 = lk_tree(a11[0], a11[1]), A12 = lk_tree(a12[0], a12[1]), A22 = lk_tree(a22[0], a22[1]);
+    const size_t gid = (size_t)i * pitch + j;
+    float D = __fmaf_rn(A11, A22, -__fmul_rn(A12, A12));
+    if (D < 1.192092896e-07f) {
+      if (lane == 0) {
+        if (status) status[gid] = 0;
+        if (err) err[gid] = 0.f;
+      }
+      continue;
+    }
+    A11 = __fdiv_rn(A11, D);
+    A12 = __fdiv_rn(A12, D);
+    A22 = __fdiv_rn(A22, D);
+    float ptx = __fsub_rn(__fadd_rn((float)j, U[gid]), hw), pty = __fsub_rn(__fadd_rn((float)i, V[gid]), hw);
+    float lx[4], ly[2][4];
+    lx[0] = __fadd_rn(ptx, __fadd_rn((float)xid, 0.5f));
+    ly[0][0] = __fadd_rn(pty, __fadd_rn((float)yid, 0.5f));
+    ly[1][0] = __fadd_rn(pty, __fadd_rn((float)(yid + 4), 0.5f));
+#pragma unroll
+    for (int t = 1; t < 4; t++) {
+      lx[t] = __fadd_rn(lx[t - 1], 8.0f);
+      ly[0][t] = __fadd_rn(ly[0][t - 1], 8.0f);
+      ly[1][t] = __fadd_rn(ly[1][t - 1], 8.0f);
+    }
+    uint8_t st = 1;
+    for (int k = 0; k < p.niter; k++) {
+      if (ptx < -hw || ptx >= (float)W || pty < -hw || pty >= (float)H) {
+        st = 0;
+        break;
+      }
+      float b1[2] = {0.f, 0.f}, b2[2] = {0.f, 0.f};
+#pragma unroll
+      for (int v = 0; v < 2; v++) {
+        const float* wy = v ? wy1 : wy0;
+        const int yy = yid + 4 * v;
+#pragma unroll
+        for (int ty = 0; ty < 4; ty++)
+#pragma unroll
+          for (int tx = 0; tx < 4; tx++) {
+            float w = __fmul_rn(wx[tx], wy[ty]);
+            if (w == 0.f) continue;
+            int g = (gyb + ty * 8 + yy) * LK_G + gxb + tx * 8 + xid;
+            float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_I + gxb + tx * 8 + xid + 1];
+            float Jv = lk_bilinear(J, H, W, pitch, lx[tx], ly[v][ty]);
+            float diff = __fmul_rn(__fsub_rn(Jv, Iv), w);
+            b1[v] = __fmaf_rn(diff, __fmul_rn(sDx[g], w), b1[v]);
+            b2[v] = __fmaf_rn(diff, __fmul_rn(sDy[g], w), b2[v]);
+          }
+      }
+      float B1 = lk_tree(b1[0], b1[1]), B2 = lk_tree(b2[0], b2[1]);
+      float dx = __fmul_rn(__fmaf_rn(A12, B2, -__fmul_rn(A22, B1)), 32.0f);
+      float dy = __fmul_rn(__fmaf_rn(A12, B1, -__fmul_rn(A11, B2)), 32.0f);
+      ptx = __fadd_rn(ptx, dx);
+      pty = __fadd_rn(pty, dy);
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        lx[t] = __fadd_rn(lx[t], dx);
+        ly[0][t] = __fadd_rn(ly[0][t], dy);
+        ly[1][t] = __fadd_rn(ly[1][t], dy);
+      }
+      if (fabsf(dx) < 0.01f && fabsf(dy) < 0.01f) break;
+    }
+    if (err) {
+      // GetError visiting order and guards (:620-653); bits: 1 xBase, 2 yBase, 4 xBase2, 8 yBase2
+      const int ord[16] = {0x000, 0x010, 0x100, 0x110, 0x021, 0x121, 0x202, 0x212,
+                           0x223, 0x034, 0x134, 0x234, 0x308, 0x318, 0x328, 0x33c};
+      float e[2] = {0.f, 0.f};
+#pragma unroll
+      for (int v = 0; v < 2; v++) {
+        const float* wy = v ? wy1 : wy0;
+        const int* by = v ? by1 : by0;
+        const int yy = yid + 4 * v;
+#pragma unroll
+        for (int o = 0; o < 16; o++) {
+          int ty = ord[o] >> 8, tx = (ord[o] >> 4) & 15, gb = ord[o] & 15;
+          if ((gb & 1) && !(bx[0] < p.ws)) continue;
+          if ((gb & 2) && !(by[0] < p.ws)) continue;
+          if ((gb & 4) && !(bx[1] < p.ws)) continue;
+          if ((gb & 8) && !(by[1] < p.ws)) continue;
+          float w = __fmul_rn(wx[tx], wy[ty]);
+          float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_I + gxb + tx * 8 + xid + 1];
+          float Jv = lk_bilinear(J, H, W, pitch, lx[tx], ly[v][ty]);
+          float d = __fmul_rn(__fsub_rn(__fdiv_rn(__fmaf_rn(Jv, 16384.f, 256.f), 512.f),
+                                        __fdiv_rn(__fmaf_rn(Iv, 16384.f, 256.f), 512.f)),
+                              w);
+          e[v] = __fadd_rn(e[v], fabsf(d));
+        }
+      }
+      float E = lk_tree(e[0], e[1]);
+      if (lane == 0) err[gid] = __fdiv_rn(E, (float)(32 * p.ws * p.ws));
+    }
+    if (lane == 0) {
+      U[gid] = __fsub_rn(__fadd_rn(ptx, hw), (float)j);
+      V[gid] = __fsub_rn(__fadd_rn(pty, hw), (float)i);
+      if (status) status[gid] = st;
+    }
+  }
+}
+
+}  // namespace ofb
+
+using namespace ofb;
+
+extern "C" int of_lk_dense(const float* I, const float* J, float* U, float* V, int H, int W, int pitch, int half_win,
+                           int niter, const int* asym, uint8_t* status, float* err, void* stream) {
+  OF_REQUIRE(!bad_plane(I, H, W, pitch) && J && U && V, "of_lk_dense: bad plane");
+  OF_REQUIRE(half_win >= 1 && half_win <= 15, "of_lk_dense: half_win must be in 1..15");
+  OF_REQUIRE(niter >= 0, "of_lk_dense: niter < 0");
+  LkParams p;
+  p.ws = 2 * half_win + 1;
+  p.hw = (p.ws - 1) >> 1;
+  p.aL = asym ? asym[0] : 0;
+  p.aR = asym ? asym[1] : 0;
+  p.aT = asym ? asym[2] : 0;
+  p.aB = asym ? asym[3] : 0;
+  p.niter = niter;
+  dim3 grid((W + LK_PT - 1) / LK_PT, (H + LK_PT - 1) / LK_PT);
+  lk_dense_kernel<<<grid, 256, 0, as_stream(stream)>>>(I, J, U, V, H, W, pitch, p, status, err);
+  return check_launch("of_lk_dense");
+}

@@ -1,0 +1,343 @@
+// Level-transition kernels of the pyramid driver (src/GenericPyramidalOpticalFlow.py).
+//
+//  A2 of_resize: Pillow's antialiased two-pass resample of a float32 image.  The
+//     per-output-coordinate kernels (bounds + normalised double weights) are built on the
+//     device by one thread per output coordinate with the same double operations as the
+//     published algorithm; the horizontal pass writes a float32 intermediate, the vertical
+//     pass reads it; both accumulate in double.  Bit-exact with Pillow.
+//  A3 of_spline_upsample: not-a-knot cubic interpolant (the s=0 RectBivariateSpline),
+//     separable: moments along y per coarse column, evaluation at the fine rows, moments
+//     along x per fine row, evaluation at the fine columns; double throughout.
+//  A4 of_warp_pair_bilinear: doBiLinearWarping's round-half-even base, float64 weights.
+#include "common.cuh"
+
+namespace ofb {
+
+// ----------------------------------------------------------------------------- resize
+__device__ __forceinline__ double filt(double x, int bicubic) {
+  if (x < 0.0) x = -x;
+  if (!bicubic) return x < 1.0 ? __dadd_rn(1.0, -x) : 0.0;
+  const double a = -0.5;
+  if (x < 1.0) return __dadd_rn(__dmul_rn(__dmul_rn(__dadd_rn(__dmul_rn(a + 2.0, x), -(a + 3.0)), x), x), 1.0);
+  if (x < 2.0) {
+    double t = __dmul_rn(__dadd_rn(x, -5.0), x);
+    t = __dmul_rn(__dadd_rn(t, 8.0), x);
+    return __dmul_rn(__dadd_rn(t, -4.0), a);
+  }
+  return 0.0;
+}
+
+__host__ __device__ inline void resize_geom(int inSize, int outSize, int bicubic, double* scale, double* fscale,
+                                            double* support, int* ksize) {
+  double s = (double)((float)inSize - 0.0f) / outSize;
+  double fs = s < 1.0 ? 1.0 : s;
+  double sup = (bicubic ? 2.0 : 1.0) * fs;
+  *scale = s;
+  *fscale = fs;
+  *support = sup;
+  *ksize = (int)ceil(sup) * 2 + 1;
+}
+
+__global__ void resize_coeff_kernel(int inSize, int outSize, int bicubic, int ksize, int* bounds, double* kk) {
+  int xx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (xx >= outSize) return;
+  double scale, fscale, support;
+  int ks;
+  resize_geom(inSize, outSize, bicubic, &scale, &fscale, &support, &ks);
+  double center = __dadd_rn(0.0, __dmul_rn(__dadd_rn((double)xx, 0.5), scale));
+  double ww = 0.0, ss = __ddiv_rn(1.0, fscale);
+  int xmin = (int)__dadd_rn(__dadd_rn(center, -support), 0.5);
+  if (xmin < 0) xmin = 0;
+  int xmax = (int)__dadd_rn(__dadd_rn(center, support), 0.5);
+  if (xmax > inSize) xmax = inSize;
+  xmax -= xmin;
+  double* k = kk + (size_t)xx * ksize;
+  int x;
+  for (x = 0; x < xmax; x++) {
+    double w = filt(__dmul_rn(__dadd_rn(__dadd_rn((double)(x + xmin), -center), 0.5), ss), bicubic);
+    k[x] = w;
+    ww = __dadd_rn(ww, w);
+  }
+  for (x = 0; x < xmax; x++)
+    if (ww != 0.0) k[x] = __ddiv_rn(k[x], ww);
+  for (; x < ksize; x++) k[x] = 0.0;
+  bounds[2 * xx] = xmin;
+  bounds[2 * xx + 1] = xmax;
+}
+
+__global__ void resize_h_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst, int dp, int Hs, int Wd,
+                                const int* __restrict__ bounds, const double* __restrict__ kk, int ksize) {
+  int xx = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (xx >= Wd) return;
+  int xmin = bounds[2 * xx], xmax = bounds[2 * xx + 1];
+  const double* k = kk + (size_t)xx * ksize;
+  const float* row = src + (size_t)y * sp + xmin;
+  double ss = 0.0;
+  for (int x = 0; x < xmax; x++) ss = __dadd_rn(ss, __dmul_rn((double)row[x], k[x]));
+  dst[(size_t)y * dp + xx] = (float)ss;
+}
+
+__global__ void resize_v_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst, int dp, int Wd,
+                                const int* __restrict__ bounds, const double* __restrict__ kk, int ksize) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, yy = blockIdx.y;
+  if (x >= Wd) return;
+  int ymin = bounds[2 * yy], ymax = bounds[2 * yy + 1];
+  const double* k = kk + (size_t)yy * ksize;
+  double ss = 0.0;
+  for (int y = 0; y < ymax; y++) ss = __dadd_rn(ss, __dmul_rn((double)src[(size_t)(y + ymin) * sp + x], k[y]));
+  dst[(size_t)yy * dp + x] = (float)ss;
+}
+
+__global__ void copy_plane_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst, int dp, int W) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x < W) dst[(size_t)y * dp + x] = src[(size_t)y * sp + x];
+}
+
+static int ksize_of(int in, int out, int bicubic) {
+  double a, b, c;
+  int k;
+  resize_geom(in, out, bicubic, &a, &b, &c, &k);
+  return k;
+}
+
+// ----------------------------------------------------------------------------- spline
+// Thomas-algorithm moments of the not-a-knot spline through n >= 4 samples with unit
+// spacing; sample i of line l is y[i*ls + l*ss_], scratch/moments use the same layout.
+__device__ void nak_moments(const double* y, const float* yf, size_t ls, double* M, double* cp, double* dp, int n) {
+#define YV(i) (y ? y[(size_t)(i) * ls] : (double)yf[(size_t)(i) * ls])
+#define MV(i) M[(size_t)(i) * ls]
+  double d1 = __dadd_rn(__dadd_rn(YV(2), -__dmul_rn(2.0, YV(1))), YV(0));
+  double dl = __dadd_rn(__dadd_rn(YV(n - 1), -__dmul_rn(2.0, YV(n - 2))), YV(n - 3));
+  MV(1) = d1;
+  MV(n - 2) = dl;
+  int m = n - 4;
+  if (m > 0) {
+    for (int r = 0; r < m; r++) {
+      int i = r + 2;
+      double rhs = __dmul_rn(6.0, __dadd_rn(__dadd_rn(YV(i + 1), -__dmul_rn(2.0, YV(i))), YV(i - 1)));
+      if (r == 0) rhs = __dadd_rn(rhs, -MV(1));
+      if (r == m - 1) rhs = __dadd_rn(rhs, -MV(n - 2));
+      if (r == 0) {
+        cp[0] = __ddiv_rn(1.0, 4.0);
+        dp[0] = __ddiv_rn(rhs, 4.0);
+      } else {
+        double den = __dadd_rn(4.0, -cp[(size_t)(r - 1) * ls]);
+        cp[(size_t)r * ls] = __ddiv_rn(1.0, den);
+        dp[(size_t)r * ls] = __ddiv_rn(__dadd_rn(rhs, -dp[(size_t)(r - 1) * ls]), den);
+      }
+    }
+    MV(m + 1) = dp[(size_t)(m - 1) * ls];
+    for (int r = m - 2; r >= 0; r--) MV(r + 2) = __dadd_rn(dp[(size_t)r * ls], -__dmul_rn(cp[(size_t)r * ls], MV(r + 3)));
+  }
+  MV(0) = __dadd_rn(__dmul_rn(2.0, MV(1)), -MV(2));
+  MV(n - 1) = __dadd_rn(__dmul_rn(2.0, MV(n - 2)), -MV(n - 3));
+#undef YV
+#undef MV
+}
+
+__device__ __forceinline__ double nak_eval(double yi, double yi1, double Mi, double Mi1, double t) {
+  double u = __dadd_rn(1.0, -t);
+  double a = __dadd_rn(__dmul_rn(u, yi), __dmul_rn(t, yi1));
+  double cu = __dadd_rn(__dmul_rn(__dmul_rn(u, u), u), -u);
+  double ct = __dadd_rn(__dmul_rn(__dmul_rn(t, t), t), -t);
+  double b = __dadd_rn(__dmul_rn(cu, Mi), __dmul_rn(ct, Mi1));
+  return __dadd_rn(a, __ddiv_rn(b, 6.0));
+}
+
+__device__ __forceinline__ void fine_index(int j, int N, int n, int* i, double* t) {
+  double s = __dmul_rn(__ddiv_rn((double)j, (double)N), (double)n);
+  if (s < 0.0) s = 0.0;
+  if (s > n - 1) s = n - 1;
+  int k = (int)floor(s);
+  if (k > n - 2) k = n - 2;
+  *i = k;
+  *t = __dadd_rn(s, -(double)k);
+}
+
+// moments along y for each coarse column x
+__global__ void spline_my_kernel(const float* __restrict__ src, int sp, int h, int w, double* M, double* Y0,
+                                 double* S) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= w) return;
+  // the column (pitch sp) is copied into Y0, laid out [i][x] like the moments and scratch
+  for (int i = 0; i < h; i++) Y0[(size_t)i * w + x] = (double)src[(size_t)i * sp + x];
+  nak_moments(Y0 + x, nullptr, w, M + x, S + x, S + (size_t)h * w + x, h);
+}
+
+// T[Y][x] = column spline at fine row Y
+__global__ void spline_ey_kernel(const double* __restrict__ Y0, const double* __restrict__ M, double* __restrict__ T,
+                                 int h, int w, int H) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y;
+  if (x >= w) return;
+  int i;
+  double t;
+  fine_index(Y, H, h, &i, &t);
+  T[(size_t)Y * w + x] =
+      nak_eval(Y0[(size_t)i * w + x], Y0[(size_t)(i + 1) * w + x], M[(size_t)i * w + x], M[(size_t)(i + 1) * w + x], t);
+}
+
+// moments along x for each fine row Y of T (layout [k][Y], stride H)
+__global__ void spline_mx_kernel(const double* __restrict__ T, int w, int H, double* M, double* cp, double* dp,
+                                 double* Tt) {
+  int Y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (Y >= H) return;
+  for (int k = 0; k < w; k++) Tt[(size_t)k * H + Y] = T[(size_t)Y * w + k];
+  nak_moments(Tt + Y, nullptr, H, M + Y, cp + Y, dp + Y, w);
+}
+
+__global__ void spline_ex_kernel(const double* __restrict__ Tt, const double* __restrict__ M, float* __restrict__ dst,
+                                 int dpitch, int w, int H, int W, float scale) {
+  int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y;
+  if (X >= W) return;
+  int i;
+  double t;
+  fine_index(X, W, w, &i, &t);
+  double v = nak_eval(Tt[(size_t)i * H + Y], Tt[(size_t)(i + 1) * H + Y], M[(size_t)i * H + Y],
+                      M[(size_t)(i + 1) * H + Y], t);
+  dst[(size_t)Y * dpitch + X] = __fmul_rn((float)v, scale);
+}
+
+// ----------------------------------------------------------------------------- warp
+__device__ __forceinline__ float warp_sample(const float* __restrict__ img, int H, int W, int pitch, float cy,
+                                             float cx) {
+  int iy = (int)rintf(cy), ix = (int)rintf(cx);
+  double dy = __dadd_rn((double)cy, -(double)iy), dx = __dadd_rn((double)cx, -(double)ix);
+  int ny = dy < 0 ? iy - 1 : iy + 1, nx = dx < 0 ? ix - 1 : ix + 1;
+  dy = fabs(dy);
+  dx = fabs(dx);
+  iy = clampi(iy, 0, H - 1);
+  ny = clampi(ny, 0, H - 1);
+  ix = clampi(ix, 0, W - 1);
+  nx = clampi(nx, 0, W - 1);
+  double oy = __dadd_rn(1.0, -dy), ox = __dadd_rn(1.0, -dx);
+  double a = __dmul_rn(__dmul_rn(oy, ox), (double)img[(size_t)iy * pitch + ix]);
+  a = __dadd_rn(a, __dmul_rn(__dmul_rn(oy, dx), (double)img[(size_t)iy * pitch + nx]));
+  a = __dadd_rn(a, __dmul_rn(__dmul_rn(dy, ox), (double)img[(size_t)ny * pitch + ix]));
+  a = __dadd_rn(a, __dmul_rn(__dmul_rn(dy, dx), (double)img[(size_t)ny * pitch + nx]));
+  return (float)a;
+}
+
+__global__ void warp_pair_kernel(const float* __restrict__ I0, const float* __restrict__ I1,
+                                 const float* __restrict__ U, const float* __restrict__ V, float* __restrict__ O0,
+                                 float* __restrict__ O1, int H, int W, int pitch) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  size_t i = (size_t)y * pitch + x;
+  float hv = __fdiv_rn(V[i], 2.0f), hu = __fdiv_rn(U[i], 2.0f);
+  float cy0 = (float)__dadd_rn((double)y, -(double)hv), cx0 = (float)__dadd_rn((double)x, -(double)hu);
+  float cy1 = (float)__dadd_rn((double)y, (double)hv), cx1 = (float)__dadd_rn((double)x, (double)hu);
+  O0[i] = warp_sample(I0, H, W, pitch, cy0, cx0);
+  O1[i] = warp_sample(I1, H, W, pitch, cy1, cx1);
+}
+
+__global__ void warp_coords_kernel(const float* __restrict__ img, const float* __restrict__ cy,
+                                   const float* __restrict__ cx, float* __restrict__ out, int H, int W, int pitch) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  size_t i = (size_t)y * pitch + x;
+  out[i] = warp_sample(img, H, W, pitch, cy[i], cx[i]);
+}
+
+}  // namespace ofb
+
+using namespace ofb;
+
+extern "C" int of_warp_bilinear_coords(const float* img, const float* coordsY, const float* coordsX, float* out, int H,
+                                       int W, int pitch, void* stream) {
+  OF_REQUIRE(!bad_plane(img, H, W, pitch) && coordsY && coordsX && out, "of_warp_bilinear_coords: bad plane");
+  warp_coords_kernel<<<dim3((W + 255) / 256, H), 256, 0, as_stream(stream)>>>(img, coordsY, coordsX, out, H, W, pitch);
+  return check_launch("of_warp_bilinear_coords");
+}
+
+extern "C" size_t of_resize_workspace_size(int Hs, int Ws, int Hd, int Wd, int filter) {
+  Sizer s;
+  int bic = filter == OF_FILTER_BICUBIC;
+  s.take<int>(2 * (size_t)(Wd > 0 ? Wd : 1));
+  s.take<double>((size_t)ksize_of(Ws, Wd > 0 ? Wd : 1, bic) * (Wd > 0 ? Wd : 1));
+  s.take<int>(2 * (size_t)(Hd > 0 ? Hd : 1));
+  s.take<double>((size_t)ksize_of(Hs, Hd > 0 ? Hd : 1, bic) * (Hd > 0 ? Hd : 1));
+  s.take<float>((size_t)Hs * (Wd > 0 ? Wd : 1));
+  return s.off;
+}
+
+extern "C" int of_resize(const float* src, int Hs, int Ws, int src_pitch, float* dst, int Hd, int Wd, int dst_pitch,
+                         int filter, void* workspace, size_t workspace_bytes, void* stream) {
+  OF_REQUIRE(!bad_plane(src, Hs, Ws, src_pitch) && !bad_plane(dst, Hd, Wd, dst_pitch), "of_resize: bad plane");
+  OF_REQUIRE(filter == OF_FILTER_BILINEAR || filter == OF_FILTER_BICUBIC, "of_resize: unknown filter");
+  cudaStream_t st = as_stream(stream);
+  if (Hs == Hd && Ws == Wd) {
+    copy_plane_kernel<<<dim3((Wd + 255) / 256, Hd), 256, 0, st>>>(src, src_pitch, dst, dst_pitch, Wd);
+    return check_launch("of_resize");
+  }
+  size_t need = of_resize_workspace_size(Hs, Ws, Hd, Wd, filter);
+  if (!workspace || workspace_bytes < need)
+    return set_error(OF_ERR_WORKSPACE, "of_resize: workspace too small (%zu < %zu)", workspace_bytes, need);
+  int bic = filter == OF_FILTER_BICUBIC;
+  int kh = ksize_of(Ws, Wd, bic), kv = ksize_of(Hs, Hd, bic);
+  Carver c(workspace, workspace_bytes);
+  int* bh = c.take<int>(2 * (size_t)Wd);
+  double* kkh = c.take<double>((size_t)kh * Wd);
+  int* bv = c.take<int>(2 * (size_t)Hd);
+  double* kkv = c.take<double>((size_t)kv * Hd);
+  float* tmp = c.take<float>((size_t)Hs * Wd);
+  bool need_h = Wd != Ws, need_v = Hd != Hs;
+  const float* cur = src;
+  int cur_pitch = src_pitch;
+  if (need_h) {
+    resize_coeff_kernel<<<(Wd + 127) / 128, 128, 0, st>>>(Ws, Wd, bic, kh, bh, kkh);
+    float* out = need_v ? tmp : dst;
+    int op = need_v ? Wd : dst_pitch;
+    resize_h_kernel<<<dim3((Wd + 127) / 128, Hs), 128, 0, st>>>(src, src_pitch, out, op, Hs, Wd, bh, kkh, kh);
+    cur = out;
+    cur_pitch = op;
+  }
+  if (need_v) {
+    resize_coeff_kernel<<<(Hd + 127) / 128, 128, 0, st>>>(Hs, Hd, bic, kv, bv, kkv);
+    resize_v_kernel<<<dim3((Wd + 127) / 128, Hd), 128, 0, st>>>(cur, cur_pitch, dst, dst_pitch, Wd, bv, kkv, kv);
+  }
+  return check_launch("of_resize", 2 * (int)need_h + 2 * (int)need_v);
+}
+
+extern "C" size_t of_spline_workspace_size(int h, int w, int H, int W) {
+  Sizer s;
+  size_t a = (size_t)h * w, b = (size_t)H * w;
+  s.take<double>(a);      // column samples (double)
+  s.take<double>(a);      // moments along y
+  s.take<double>(2 * a);  // Thomas scratch along y
+  s.take<double>(b);      // T (fine rows x coarse columns)
+  s.take<double>(b);      // T transposed
+  s.take<double>(b);      // moments along x
+  s.take<double>(2 * b);  // Thomas scratch along x
+  return s.off;
+}
+
+extern "C" int of_spline_upsample(const float* src, int h, int w, int src_pitch, float* dst, int H, int W,
+                                  int dst_pitch, float scale, void* workspace, size_t workspace_bytes, void* stream) {
+  OF_REQUIRE(!bad_plane(src, h, w, src_pitch) && !bad_plane(dst, H, W, dst_pitch), "of_spline_upsample: bad plane");
+  OF_REQUIRE(h >= 4 && w >= 4, "of_spline_upsample: the coarse field needs at least 4x4 samples");
+  size_t need = of_spline_workspace_size(h, w, H, W);
+  if (!workspace || workspace_bytes < need)
+    return set_error(OF_ERR_WORKSPACE, "of_spline_upsample: workspace too small (%zu < %zu)", workspace_bytes, need);
+  cudaStream_t st = as_stream(stream);
+  size_t a = (size_t)h * w, b = (size_t)H * w;
+  Carver c(workspace, workspace_bytes);
+  double* Y0 = c.take<double>(a);
+  double* My = c.take<double>(a);
+  double* Sy = c.take<double>(2 * a);
+  double* T = c.take<double>(b);
+  double* Tt = c.take<double>(b);
+  double* Mx = c.take<double>(b);
+  double* Sx = c.take<double>(2 * b);
+  spline_my_kernel<<<(w + 127) / 128, 128, 0, st>>>(src, src_pitch, h, w, My, Y0, Sy);
+  spline_ey_kernel<<<dim3((w + 127) / 128, H), 128, 0, st>>>(Y0, My, T, h, w, H);
+  spline_mx_kernel<<<(H + 127) / 128, 128, 0, st>>>(T, w, H, Mx, Sx, Sx + b, Tt);
+  spline_ex_kernel<<<dim3((W + 127) / 128, H), 128, 0, st>>>(Tt, Mx, dst, dst_pitch, w, H, W, scale);
+  return check_launch("of_spline_upsample", 4);
+}
+
+extern "C" int of_warp_pair_bilinear(const float* I0, const float* I1, const float* U, const float* V, float* O0,
+                                     float* O1, int H, int W, int pitch, void* stream) {
+  OF_REQUIRE(!bad_plane(I0, H, W, pitch) && I1 && U && V && O0 && O1, "of_warp_pair_bilinear: bad plane");
+  warp_pair_kernel<<<dim3((W + 255) / 256, H), 256, 0, as_stream(stream)>>>(I0, I1, U, V, O0, O1, H, W, pitch);
+  return check_launch("of_warp_pair_bilinear");
+}

@@ -1,0 +1,69 @@
+"""ofb200: B200-native (sm_100a) kernels of OpticalFlow-RI's dense pyramidal optical-flow
+hot path, behind the reference's Python module / class API.
+
+The drop-in modules sit next to this package (``GenericPyramidalOpticalFlow``,
+``HornSchunck``, ``PhysicsBasedOpticalFlowLiuShen``, ``denseLucasKanade_PyCL``,
+``Farneback_PyCL``, ``gaussian_filter``, ``GaussianKernelBitExact``); put the directory
+that holds them on ``sys.path`` exactly as the reference's examples do with its ``src``.
+
+Inputs may be numpy arrays (copied to the device, results copied back as new numpy
+arrays) or CUDA tensors (used in place, results returned as tensors).
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+__version__ = "0.1.0"
+
+VERBOSE = os.environ.get("OFB200_VERBOSE", "0") not in ("", "0")
+
+
+def log(*args):
+    if VERBOSE:
+        print(*args)
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("ofb200 needs a CUDA device (B200, sm_100a); there is no CPU fallback")
+    return torch
+
+
+def device_of(platformID=0, deviceID=0):
+    """The reference selects an OpenCL platform/device; here deviceID is the CUDA index."""
+    torch = _torch()
+    n = torch.cuda.device_count()
+    if deviceID < 0 or deviceID >= n:
+        raise ValueError(f"deviceID {deviceID} out of range (0..{n - 1})")
+    return torch.device("cuda", int(deviceID))
+
+
+def to_device(a, device=None):
+    """float32 CUDA plane from a numpy array or tensor (uint8 frames are cast like the
+    reference examples' astype(np.float32))."""
+    torch = _torch()
+    if isinstance(a, torch.Tensor):
+        t = a if a.is_cuda else a.to(device or torch.device("cuda", torch.cuda.current_device()))
+        if t.dtype != torch.float32:
+            t = t.float()
+        if t.dim() != 2 or t.stride(1) != 1:
+            t = t.contiguous()
+        return t
+    arr = np.ascontiguousarray(a)
+    if arr.ndim != 2:
+        raise ValueError("expected a 2-D image")
+    if arr.dtype != np.float32:
+        arr = arr.astype(np.float32)
+    dev = device or torch.device("cuda", torch.cuda.current_device())
+    return torch.from_numpy(arr).to(dev, non_blocking=False)
+
+
+def is_host(a) -> bool:
+    return isinstance(a, np.ndarray)
+
+
+def to_host(t):
+    return t.detach().cpu().numpy()

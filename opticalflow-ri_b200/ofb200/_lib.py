@@ -1,0 +1,101 @@
+"""ctypes binding of libofb200.so (the sm_100a kernels behind include/ofb200.h).
+
+The library is built in-tree by ``opticalflow-ri_b200/csrc/Makefile``.  There is no
+fallback: if the library is missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libofb200.so")
+CSRC = os.path.join(os.path.dirname(_HERE), "csrc")
+
+OF_OK = 0
+OF_FILTER_BILINEAR = 0
+OF_FILTER_BICUBIC = 1
+
+
+class OfError(RuntimeError):
+    """A C-ABI entry point returned a negative status."""
+
+
+class FbPolyConsts(ctypes.Structure):
+    _fields_ = [("polyN", ctypes.c_int), ("g", ctypes.c_float * 8), ("xg", ctypes.c_float * 8),
+                ("xxg", ctypes.c_float * 8), ("ig", ctypes.c_float * 4)]
+
+
+_lib = None
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+_D = ctypes.c_double
+_Z = ctypes.c_size_t
+
+_SIGS = {
+    "of_version": ([], _I),
+    "of_last_error": ([ctypes.c_char_p, _Z], _I),
+    "of_launch_count": ([], ctypes.c_ulonglong),
+    "of_prefilter_f32": ([_P, _I, _P, _I, _I, _I, _P, _I, _P], _I),
+    "of_prefilter_u8": ([_P, _I, _P, _I, _I, _I, _P, _I, _P], _I),
+    "of_u8_to_f32": ([_P, _I, _P, _I, _I, _I, _P], _I),
+    "of_resize_workspace_size": ([_I, _I, _I, _I, _I], _Z),
+    "of_resize": ([_P, _I, _I, _I, _P, _I, _I, _I, _I, _P, _Z, _P], _I),
+    "of_spline_workspace_size": ([_I, _I, _I, _I], _Z),
+    "of_spline_upsample": ([_P, _I, _I, _I, _P, _I, _I, _I, _F, _P, _Z, _P], _I),
+    "of_warp_pair_bilinear": ([_P, _P, _P, _P, _P, _P, _I, _I, _I, _P], _I),
+    "of_warp_bilinear_coords": ([_P, _P, _P, _P, _I, _I, _I, _P], _I),
+    "of_accumulate": ([_P, _P, _I, _I, _I, _P], _I),
+    "of_scale": ([_P, _P, _F, _I, _I, _I, _P], _I),
+    "of_hs_workspace_size": ([_I, _I, _I], _Z),
+    "of_hs_derivatives": ([_P, _P, _P, _P, _P, _I, _I, _I, _P], _I),
+    "of_ls_coefficients": ([_P, _P, _P, _I, _I, _I, _F, _P], _I),
+    "of_hs_solve": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _P, _P, _Z, _P], _I),
+    "of_ls_workspace_size": ([_I, _I, _I, _I], _Z),
+    "of_ls_solve": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P, _Z, _P], _I),
+    "of_lk_dense": ([_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P], _I),
+    "of_fb_blur": ([_P, _P, _I, _I, _I, _I, _P, _I, _P], _I),
+    "of_fb_box5": ([_P, _P, _I, _I, _I, _I, _P], _I),
+    "of_fb_polyexp": ([_P, _P, _I, _I, _I, ctypes.POINTER(FbPolyConsts), _P], _I),
+    "of_fb_update_matrices": ([_P, _P, _P, _P, _P, _I, _I, _I, _P], _I),
+    "of_fb_update_flow": ([_P, _P, _P, _I, _I, _I, _P], _I),
+    "of_fb_iteration": ([_P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _I, _I, _P], _I),
+}
+
+
+def exported_symbols():
+    """Names of every entry point the binding declares (the header's ABI)."""
+    return sorted(_SIGS)
+
+
+def lib():
+    """Loads libofb200.so (raises if it is absent: there is no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"ofb200: {LIB_PATH} is not built; run `make -C {CSRC}` "
+                              "(or __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    lib().of_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, name: str) -> None:
+    if rc != OF_OK:
+        raise OfError(f"{name} failed (status {rc}): {last_error()}")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args), name)
