@@ -52,7 +52,31 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls"],
+                   help="ls: only the Liu-Shen solve of one pair, --steps times (for profiling)")
     return p.parse_args()
+
+
+def run_ls_only(args):
+    """Liu-Shen solve on one prefiltered --size pair, --warmup + --steps times."""
+    import torch
+    from gaussian_filter import prepareGaussianKernel
+    from ofb200 import ops
+    a, b, _, _ = make_pairs(1, args.size)[0]
+    taps = prepareGaussianKernel(0.48, 5)
+    fa = ops.prefilter(torch.from_numpy(a).cuda(), taps)
+    fb = ops.prefilter(torch.from_numpy(b).cuda(), taps)
+    ms = []
+    for r in range(args.warmup + args.steps):
+        U, V = torch.zeros_like(fa), torch.zeros_like(fa)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, _, it, _ = ops.ls_solve(fa, fb, U, V, 10.0)
+        e1.record()
+        e1.synchronize()
+        if r >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+    print(json.dumps({"mode": "ls", "size": args.size, "sweeps": int(it.item()), "ms": float(np.mean(ms))}))
 
 
 def peaks():
@@ -157,7 +181,8 @@ def run_ours(args, rank, world, local_rank):
 
     # device-timed steps (L2 flushed between steps, outside the events)
     clocks = Clocks(local_rank) if rank == 0 else None
-    lc0 = _lib.lib().of_launch_count()
+    from ofb200 import graph as _graph
+    lc0 = _lib.lib().of_launch_count() + _graph.replayed_kernels()
     total_ms = 0.0
     for _ in range(args.steps):
         flush.zero_()
@@ -168,7 +193,7 @@ def run_ours(args, rank, world, local_rank):
         e1.record()
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
-    launches = _lib.lib().of_launch_count() - lc0
+    launches = _lib.lib().of_launch_count() + _graph.replayed_kernels() - lc0
     clk = clocks.stop() if clocks else None
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -176,25 +201,29 @@ def run_ours(args, rank, world, local_rank):
     total_ms = float(t.item())
     barrier()
 
-    # roofline of the dominant kernel: the Liu-Shen solve at full size, timed alone
+    # roofline of the dominant kernel: the Liu-Shen solve at full size, graph-replayed alone
+    from gaussian_filter import prepareGaussianKernel
+    from ofb200 import graph as _graph
     a = ops.u8_to_f32(frames[0][0])
     b = ops.u8_to_f32(frames[0][1])
-    taps = np.array([1.3824512e-04, 9.2915423e-02, 8.1389272e-01, 9.2915423e-02, 1.3824512e-04], np.float32)
-    from gaussian_filter import prepareGaussianKernel
     taps = prepareGaussianKernel(0.48, 5)
     fa, fb = ops.prefilter(a, taps), ops.prefilter(b, taps)
     U0 = torch.zeros_like(fa)
+
+    def ls_fn(x, y, u0):
+        U, V = u0.clone(), u0.clone()
+        return ops.ls_solve(x, y, U, V, 10.0)
+
     ls_ms, iters = [], None
-    for r in range(4):
-        Uw, Vw = U0.clone(), U0.clone()
+    for r in range(6):
         flush.zero_()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        _, _, it, _ = ops.ls_solve(fa, fb, Uw, Vw, 10.0)
+        _, _, it, _ = _graph.CACHE.run(("bench-ls", args.size), ls_fn, [fa, fb, U0])
         e1.record()
         e1.synchronize()
-        if r > 0:
+        if r > 1:
             ls_ms.append(e0.elapsed_time(e1))
         iters = int(it.item())
     ls_ms = float(np.mean(ls_ms))
@@ -305,6 +334,9 @@ def main():
         line = run_reference(args, rank, world)
         if line:
             print(json.dumps(line))
+        return
+    if args.mode == "ls":
+        run_ls_only(args)
         return
     if world > 1:
         import datetime

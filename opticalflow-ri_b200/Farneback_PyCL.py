@@ -8,6 +8,8 @@ deviceID selects the CUDA device.  The per-kernel methods (gaussianBlur, polynom
 updateMatrices, ...) are kept with the reference's signatures and accept numpy arrays or
 CUDA tensors.
 """
+import functools
+
 import numpy as np
 
 from GaussianKernelBitExact import getGaussianKernelBitExact
@@ -21,6 +23,38 @@ def imresize(im, res):
     host = is_host(im)
     out = ops.resize(to_device(im), res, bicubic=False)
     return to_host(out) if host else out
+
+
+@functools.lru_cache(maxsize=64)
+def _prepare_gaussian(n, sigma):
+    """src/Farneback_PyCL.py:123-171: g, xg, xxg (2n+1 float32 taps) and invG[1,1], invG[0,3],
+    invG[3,3], invG[5,5] of the 6x6 moment matrix (float64)."""
+    if sigma < 1.19209289550781250000000000000000000e-7:
+        sigma = n * 0.3
+    g = np.zeros([2 * n + 1], dtype=np.float32)
+    xg = np.zeros([2 * n + 1], dtype=np.float32)
+    xxg = np.zeros([2 * n + 1], dtype=np.float32)
+    s = np.float64(0.0)
+    for x in range(-n, n + 1):
+        g[x + n] = np.exp(-x * x / (2 * sigma * sigma))
+        s += g[x + n]
+    s = 1.0 / s
+    for x in range(-n, n + 1):
+        g[x + n] = np.float32(g[x + n] * s)
+        xg[x + n] = np.float32(x * g[x + n])
+        xxg[x + n] = np.float32(x * x * g[x + n])
+    G = np.zeros((6, 6), np.float64)
+    for y in range(-n, n + 1):
+        for x in range(-n, n + 1):
+            G[0, 0] += g[y + n] * g[x + n]
+            G[1, 1] += g[y + n] * g[x + n] * x * x
+            G[3, 3] += g[y + n] * g[x + n] * x * x * x * x
+            G[5, 5] += g[y + n] * g[x + n] * x * x * y * y
+    G[2, 2] = G[0, 3] = G[0, 4] = G[3, 0] = G[4, 0] = G[1, 1]
+    G[4, 4] = G[3, 3]
+    G[3, 4] = G[4, 3] = G[5, 5]
+    invG = np.linalg.inv(G)
+    return g, xg, xxg, invG[1, 1], invG[0, 3], invG[3, 3], invG[5, 5]
 
 
 class Farneback_PyCL(object):
@@ -47,35 +81,10 @@ class Farneback_PyCL(object):
 
     # ---------------------------------------------------------------- host constants
     def FarnebackPrepareGaussian(self):
-        """src/Farneback_PyCL.py:123-171."""
-        n = self.polyN
-        sigma = self.polySigma
-        if sigma < 1.19209289550781250000000000000000000e-7:
-            sigma = n * 0.3
-        g = np.zeros([2 * n + 1], dtype=np.float32)
-        xg = np.zeros([2 * n + 1], dtype=np.float32)
-        xxg = np.zeros([2 * n + 1], dtype=np.float32)
-        s = np.float64(0.0)
-        for x in range(-n, n + 1):
-            g[x + n] = np.exp(-x * x / (2 * sigma * sigma))
-            s += g[x + n]
-        s = 1.0 / s
-        for x in range(-n, n + 1):
-            g[x + n] = np.float32(g[x + n] * s)
-            xg[x + n] = np.float32(x * g[x + n])
-            xxg[x + n] = np.float32(x * x * g[x + n])
-        G = np.zeros((6, 6), np.float64)
-        for y in range(-n, n + 1):
-            for x in range(-n, n + 1):
-                G[0, 0] += g[y + n] * g[x + n]
-                G[1, 1] += g[y + n] * g[x + n] * x * x
-                G[3, 3] += g[y + n] * g[x + n] * x * x * x * x
-                G[5, 5] += g[y + n] * g[x + n] * x * x * y * y
-        G[2, 2] = G[0, 3] = G[0, 4] = G[3, 0] = G[4, 0] = G[1, 1]
-        G[4, 4] = G[3, 3]
-        G[3, 4] = G[4, 3] = G[5, 5]
-        invG = np.linalg.inv(G)
-        return g, xg, xxg, invG[1, 1], invG[0, 3], invG[3, 3], invG[5, 5]
+        """src/Farneback_PyCL.py:123-171 (memoised per (polyN, polySigma))."""
+        g, xg, xxg, a, b, c, d = _prepare_gaussian(self.polyN, float(self.polySigma))
+        return g.copy(), xg.copy(), xxg.copy(), a, b, c, d
+
 
     def setPolynomialExpansionConsts(self):
         n = self.polyN
@@ -193,6 +202,16 @@ class Farneback_PyCL(object):
         if host:
             return to_host(Ud), to_host(Vd), e
         return Ud, Vd, e
+
+    def _graph_key(self, n):
+        return ("FB", self.windowSize, self.numIters, self.polyN, float(self.polySigma), bool(self.useGaussianFilter),
+                float(self.pyrScale), self.pyramidalLevels, str(self.device))
+
+    def _graph_clone(self, n):
+        return self
+
+    def _graph_consume(self, n):
+        pass
 
     def getAlgoName(self):
         return 'Farneback CL'

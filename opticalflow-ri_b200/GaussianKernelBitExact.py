@@ -6,6 +6,7 @@ Quirk kept from the reference (:102-106): a positive sigma is ignored and
 sigma = 0.15 * n + 0.35 is used; sigma <= 0 with n in {1,3,5,7,9} uses fixed tables.
 Returns (sum, kernel) with both as float64, like the reference.
 """
+import functools
 from decimal import Decimal
 
 import numpy as np
@@ -20,6 +21,12 @@ _FIXED = {
 
 
 def getGaussianKernelBitExact(n, sigma):
+    s, k = _bitexact_cached(int(n), float(sigma))
+    return s, k.copy()
+
+
+@functools.lru_cache(maxsize=256)
+def _bitexact_cached(n, sigma):
     assert n > 0
     if sigma <= 0 and n in _FIXED:
         k = np.array(_FIXED[n], dtype=np.float64)

@@ -15,6 +15,7 @@ Not supported yet: the Liu-Shen optical-flow-equation warp (biLinear=False,
 import numpy as np
 
 from gaussian_filter import prepareGaussianKernel
+from ofb200 import graph as _graph
 from ofb200 import ops, to_device, is_host, to_host, log, _torch
 
 __all__ = ["genericPyramidalOpticalFlow", "updateNextPyramidalLevel", "doBiLinearWarping", "imresize"]
@@ -80,22 +81,61 @@ def genericPyramidalOpticalFlow(im1, im2, FILTER, mainOFlowAlgoAdapter, pyramida
                                 FILTER_OPT=None, optionalOFlowAlgoAdapter=None, warping=True, biLinear=True,
                                 pyramidalIntermediateScaling=True, pyramidalScaling=False):
     """:237-415.  Returns (Uaccum, Vaccum): numpy arrays for numpy input, CUDA tensors for
-    tensor input."""
+    tensor input.
+
+    With this package's adapters the whole pyramid is captured once per configuration
+    into a CUDA graph and replayed on later calls (ofb200.graph); the adapters' visible
+    state changes exactly as in the reference (Horn-Schunck pops one alpha per level)."""
     host = is_host(im1)
-    torch = _torch()
     dev = getattr(mainOFlowAlgoAdapter, "device", None)
     I1 = to_device(im1, dev)
     I2 = to_device(im2, I1.device)
-    scale = 1.0 / (2.0 ** (pyramidalLevels - 1))
     if mainOFlowAlgoAdapter.hasGenericPyramidalDefaults():
         dm = mainOFlowAlgoAdapter.getGenericPyramidalDefaults()
         if dm is not None:
-            warping = dm.get('warping', warping) if dm.get('warping') is not None else warping
-            biLinear = dm.get('biLinear') if dm.get('biLinear') is not None else biLinear
+            if dm.get('warping') is not None:
+                warping = dm.get('warping')
+            if dm.get('biLinear') is not None:
+                biLinear = dm.get('biLinear')
             if dm.get('intermediateScaling') is not None:
                 pyramidalIntermediateScaling = dm.get('intermediateScaling')
             if dm.get('scaling') is not None:
                 pyramidalScaling = dm.get('scaling')
+    cfg = (float(FILTER), int(pyramidalLevels), int(kLevels), None if FILTER_OPT is None else float(FILTER_OPT),
+           bool(warping), bool(biLinear), bool(pyramidalIntermediateScaling), bool(pyramidalScaling))
+    main, opt = mainOFlowAlgoAdapter, optionalOFlowAlgoAdapter
+    ncalls = int(pyramidalLevels) * int(kLevels)
+    keyable = all(a is None or hasattr(a, "_graph_key") for a in (main, opt))
+    mk = main._graph_key(ncalls) if keyable else None
+    ok = opt._graph_key(ncalls) if keyable and opt is not None else None
+    if keyable and mk is not None and (opt is None or ok is not None) and _graph.ENABLED \
+            and I1.stride(0) == I1.shape[1]:
+        key = ("pyramid", tuple(I1.shape), I1.device.index, cfg, mk, ok)
+        m2 = main._graph_clone(ncalls)
+        o2 = None if opt is None else opt._graph_clone(ncalls)
+
+        def fn(a, b):
+            return _pyramid_dev(a, b, cfg, m2._graph_clone(ncalls), None if o2 is None else o2._graph_clone(ncalls))
+
+        Uacc, Vacc = _graph.CACHE.run(key, fn, [I1, I2])
+        main._graph_consume(ncalls)
+        if opt is not None:
+            opt._graph_consume(ncalls)
+        if host:
+            return to_host(Uacc), to_host(Vacc)
+        return Uacc.clone(), Vacc.clone()
+    Uacc, Vacc = _pyramid_dev(I1, I2, cfg, main, opt)
+    if host:
+        return to_host(Uacc), to_host(Vacc)
+    return Uacc, Vacc
+
+
+def _pyramid_dev(I1, I2, cfg, mainOFlowAlgoAdapter, optionalOFlowAlgoAdapter):
+    """The pyramid loop on device tensors (no host synchronisation for package adapters)."""
+    torch = _torch()
+    FILTER, pyramidalLevels, kLevels, FILTER_OPT, warping, biLinear, pyramidalIntermediateScaling, \
+        pyramidalScaling = cfg
+    scale = 1.0 / (2.0 ** (pyramidalLevels - 1))
     U = V = Uacc = Vacc = None
     work1 = None
     for level in range(1, pyramidalLevels + 1):
@@ -144,6 +184,4 @@ def genericPyramidalOpticalFlow(im1, im2, FILTER, mainOFlowAlgoAdapter, pyramida
             Uacc = ops.accumulate(Uacc.clone(), U)
             Vacc = ops.accumulate(Vacc.clone(), V)
         scale *= 2
-    if host:
-        return to_host(Uacc), to_host(Vacc)
     return Uacc, Vacc

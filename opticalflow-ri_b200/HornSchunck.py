@@ -29,6 +29,19 @@ class HSOpticalFlowAlgoAdapter(object):
         U, V = U.clone(), V.clone()
         return ops.hs_solve(im1, im2, U, V, alpha, self.Niter)
 
+    # CUDA-graph support (ofb200.graph): the key holds the alphas the next `n` calls pop
+    def _graph_key(self, n):
+        if len(self.alphas) < n:
+            raise IndexError('pop from empty list')
+        return ("HS", int(self.Niter), tuple(float(a) for a in self.alphas[len(self.alphas) - n:]))
+
+    def _graph_clone(self, n):
+        return HSOpticalFlowAlgoAdapter(list(self.alphas), self.Niter, self.provideGenericPyramidalDefaults)
+
+    def _graph_consume(self, n):
+        for _ in range(n):
+            self.alphas.pop()
+
     def getAlgoName(self):
         return 'Horn-Schunck'
 

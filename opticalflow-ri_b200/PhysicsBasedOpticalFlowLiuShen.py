@@ -37,6 +37,15 @@ class LiuShenOpticalFlowAlgoAdapter(object):
         self.last_iterations = it
         return U, V, err
 
+    def _graph_key(self, n):
+        return ("LS", float(self.alpha))
+
+    def _graph_clone(self, n):
+        return LiuShenOpticalFlowAlgoAdapter(self.alpha)
+
+    def _graph_consume(self, n):
+        pass
+
     def getAlgoName(self):
         return 'Liu-Shen Physics based OF'
 

@@ -4,6 +4,7 @@
 #include <atomic>
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace ofb {
 
@@ -16,6 +17,38 @@ int set_error(int code, const char* fmt, ...) {
   vsnprintf(g_err, sizeof(g_err), fmt, ap);
   va_end(ap);
   return code;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int tmap_f32(CUtensorMap* map, const void* base, int rank, const uint64_t* dims, const uint64_t* strides_bytes,
+             const uint32_t* box) {
+  static EncodeTiledFn encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+      return set_error(OF_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    encode = reinterpret_cast<EncodeTiledFn>(fn);
+  }
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0) return set_error(OF_ERR_INVALID, "tensor base not 16-byte aligned");
+  cuuint64_t d[3], s[2];
+  cuuint32_t b[3], e[3] = {1, 1, 1};
+  for (int i = 0; i < rank; i++) {
+    d[i] = dims[i];
+    b[i] = box[i];
+  }
+  for (int i = 0; i + 1 < rank; i++) {
+    if (strides_bytes[i] % 16) return set_error(OF_ERR_INVALID, "tensor stride not a multiple of 16 bytes");
+    s[i] = strides_bytes[i];
+  }
+  CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, const_cast<void*>(base), d, s, b, e,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(OF_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return OF_OK;
 }
 
 int check_launch(const char* what, long long nlaunch) {

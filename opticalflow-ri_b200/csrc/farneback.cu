@@ -292,6 +292,91 @@ __global__ void __launch_bounds__(256) fb_iter_kernel(const float* __restrict__ 
   }
 }
 
+// Fused iteration for a compile-time half window KH (the default windowSize 33 -> KH 16).
+// CTA: 64 x 32 outputs, 256 threads.  Per plane: the (32+2KH) x (64+2KH) input tile is
+// staged once; the vertical pass gives each thread 8 consecutive rows of one column
+// (8+2KH values read once, 8 outputs), the horizontal pass 8 consecutive columns of one
+// row; taps fully unrolled in the reference order.  The thread's 8 pixels x 5 blurred
+// planes stay in registers for updateFlow / updateMatrices.
+constexpr int FBK_TW = 64, FBK_TH = 32, FBK_R = 8;
+template <int KH>
+__global__ void __launch_bounds__(256, 2) fb_iter_fixed_kernel(const float* __restrict__ Min, float* __restrict__ Mout,
+                                                               const float* __restrict__ R0,
+                                                               const float* __restrict__ R1, float* __restrict__ flowx,
+                                                               float* __restrict__ flowy, int H, int W, int pitch,
+                                                               FbTaps t, int upd) {
+  constexpr int IW = FBK_TW + 2 * KH, IH = FBK_TH + 2 * KH;
+  extern __shared__ float sm[];
+  float* tin = sm;             // IH x IW
+  float* tv = sm + IH * IW;    // FBK_TH x IW
+  const size_t pl = (size_t)H * pitch;
+  const int x0 = blockIdx.x * FBK_TW, y0 = blockIdx.y * FBK_TH;
+  const bool interior = x0 >= KH && y0 >= KH && x0 + FBK_TW + KH <= W && y0 + FBK_TH + KH <= H;
+  const int hx = (threadIdx.x & 7) * FBK_R, hy = threadIdx.x >> 3;  // horizontal-pass assignment
+  float g[KH + 1];
+#pragma unroll
+  for (int j = 0; j <= KH; j++) g[j] = t.g[j];
+  float res[5][FBK_R];
+#pragma unroll
+  for (int p = 0; p < 5; p++) {
+    const float* s = Min + p * pl;
+    if (interior) {
+      const float* base = s + (size_t)(y0 - KH) * pitch + (x0 - KH);
+      for (int i = threadIdx.x; i < IH * IW; i += 256) {
+        int ly = i / IW, lx = i - ly * IW;
+        tin[i] = __ldg(base + (size_t)ly * pitch + lx);
+      }
+    } else {
+      for (int i = threadIdx.x; i < IH * IW; i += 256) {
+        int ly = i / IW, lx = i - ly * IW;
+        tin[i] = __ldg(s + (size_t)fb_row(y0 - KH + ly, H) * pitch + fb_col(x0 - KH + lx, W));
+      }
+    }
+    __syncthreads();
+    // vertical: work item = (column, 8-row group)
+    for (int it = threadIdx.x; it < IW * (FBK_TH / FBK_R); it += 256) {
+      const int col = it % IW, r0 = (it / IW) * FBK_R;
+      float c[FBK_R + 2 * KH];
+#pragma unroll
+      for (int q = 0; q < FBK_R + 2 * KH; q++) c[q] = tin[(r0 + q) * IW + col];
+#pragma unroll
+      for (int r = 0; r < FBK_R; r++) {
+        float acc = __fmul_rn(c[r + KH], g[0]);
+#pragma unroll
+        for (int j = 1; j <= KH; j++) acc = __fmaf_rn(__fadd_rn(c[r + KH - j], c[r + KH + j]), g[j], acc);
+        tv[(r0 + r) * IW + col] = acc;
+      }
+    }
+    __syncthreads();
+    {
+      float c[FBK_R + 2 * KH];
+#pragma unroll
+      for (int q = 0; q < FBK_R + 2 * KH; q++) c[q] = tv[hy * IW + hx + q];
+#pragma unroll
+      for (int r = 0; r < FBK_R; r++) {
+        float acc = __fmul_rn(c[r + KH], g[0]);
+#pragma unroll
+        for (int j = 1; j <= KH; j++) acc = __fmaf_rn(__fadd_rn(c[r + KH - j], c[r + KH + j]), g[j], acc);
+        res[p][r] = acc;
+      }
+    }
+    __syncthreads();
+  }
+  const int y = y0 + hy;
+  if (y >= H) return;
+#pragma unroll
+  for (int r = 0; r < FBK_R; r++) {
+    const int x = x0 + hx + r;
+    if (x >= W) continue;
+    float fx, fy;
+    fb_flow_from(res[0][r], res[1][r], res[2][r], res[3][r], res[4][r], &fx, &fy);
+    const size_t i = (size_t)y * pitch + x;
+    flowx[i] = fx;
+    flowy[i] = fy;
+    if (upd) fb_matrices_at(y, x, fx, fy, R0, R1, Mout, H, W, pitch);
+  }
+}
+
 static FbTaps make_taps(const float* gk, int kh) {
   FbTaps t{};
   for (int j = 0; j <= kh; j++) t.g[j] = gk[j];
@@ -362,6 +447,14 @@ extern "C" int of_fb_iteration(const float* M_in, float* M_out, const float* R0,
   OF_REQUIRE(!bad_plane(M_in, H, W, pitch) && R0 && R1 && flowx && flowy, "of_fb_iteration: bad plane");
   OF_REQUIRE(!update_matrices || (M_out && M_out != M_in), "of_fb_iteration: M_out missing or aliases M_in");
   OF_REQUIRE(wk && kh >= 0 && kh <= FB_MAXKH, "of_fb_iteration: bad kernel");
+  if (kh == 16) {  // windowSize 33, the reference default: the unrolled kernel
+    constexpr int KH = 16;
+    size_t smem = sizeof(float) * ((size_t)(FBK_TH + 2 * KH) * (FBK_TW + 2 * KH) + (size_t)FBK_TH * (FBK_TW + 2 * KH));
+    dim3 grid((W + FBK_TW - 1) / FBK_TW, (H + FBK_TH - 1) / FBK_TH);
+    fb_iter_fixed_kernel<KH><<<grid, 256, smem, as_stream(stream)>>>(M_in, M_out, R0, R1, flowx, flowy, H, W, pitch,
+                                                                     make_taps(wk, kh), update_matrices);
+    return check_launch("of_fb_iteration");
+  }
   size_t smem = sizeof(float) * ((size_t)(FBI_TH + 2 * kh) * (FBI_TW + 2 * kh) + (size_t)FBI_TH * (FBI_TW + 2 * kh));
   dim3 grid((W + FBI_TW - 1) / FBI_TW, (H + FBI_TH - 1) / FBI_TH);
   fb_iter_kernel<<<grid, 256, smem, as_stream(stream)>>>(M_in, M_out, R0, R1, flowx, flowy, H, W, pitch,

@@ -13,6 +13,7 @@
 // synchronisation and the sequence can be captured in a CUDA graph.
 // Inside the solver u is the row (y) component and v the column (x) component (:38-39).
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace ofb {
 
@@ -53,15 +54,26 @@ __global__ void ls_max_kernel(const float* __restrict__ a, const float* __restri
 
 __global__ void ls_normalize_kernel(const float* __restrict__ a, const float* __restrict__ b,
                                     const unsigned int* __restrict__ keys, float* __restrict__ I1,
-                                    float* __restrict__ I2, float* __restrict__ Et, int W, int pitch) {
+                                    float* __restrict__ I2, float* __restrict__ Et, int W, int sp, int dp) {
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
   if (x >= W) return;
   float ma = key2f(keys[0]), mb = key2f(keys[1]);
-  size_t i = (size_t)y * pitch + x;
+  size_t i = (size_t)y * sp + x, o = (size_t)y * dp + x;
   float i1 = __fdiv_rn(a[i], ma), i2 = __fdiv_rn(b[i], mb);
-  I1[i] = i1;
-  I2[i] = i2;
-  Et[i] = __fsub_rn(i2, i1);
+  I1[o] = i1;
+  I2[o] = i2;
+  Et[o] = __fsub_rn(i2, i1);
+}
+
+// (a, b) -> (ao, bo) plane copy between pitches
+__global__ void ls_copy2_kernel(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ ao,
+                                float* __restrict__ bo, int W, int sp, int dp, const int* __restrict__ gate) {
+  if (gate && !(*gate & 1)) return;
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  size_t i = (size_t)y * sp + x, o = (size_t)y * dp + x;
+  ao[o] = a[i];
+  bo[o] = b[i];
 }
 
 __device__ __forceinline__ double dacc(double a, float v, double w) { return __dadd_rn(a, __dmul_rn((double)v, w)); }
@@ -144,52 +156,176 @@ __device__ __forceinline__ double ls_err(const double* ss, int k, double inv_n) 
   return (sqrt(ss[2 * k]) + sqrt(ss[2 * k + 1])) * inv_n;
 }
 
-__global__ void __launch_bounds__(256) ls_sweep_kernel(const float* __restrict__ coef, size_t plane,
-                                                       const float* __restrict__ u, const float* __restrict__ v,
-                                                       float* __restrict__ un, float* __restrict__ vn, int H, int W,
-                                                       int pitch, float h, double* ss, int* run,
-                                                       unsigned int* done, int k, double inv_n, double tol) {
-  if (k > 0 && *(volatile int*)(run + k) == 0) return;  // the stop rule ended the loop earlier
-  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-  double du2 = 0.0, dv2 = 0.0;
-  if (x < W && y < H) {
-    Nb3 U, V;
-    U.load(u, y, x, H, W, pitch);
-    V.load(v, y, x, H, W, pitch);
-    size_t i = (size_t)y * pitch + x;
-    float a = coef[i], b = coef[plane + i], c = coef[2 * plane + i];
-    float Du = U.dy(), DTu = U.dx(), Dv = V.dy(), DTv = V.dx();
-    float Fu = U.fy(), FTv = V.fx(), Mu = U.m(), Mv = V.m();
-    float Hu = hsum(u, y, x, H, W, pitch), Hv = hsum(v, y, x, H, W, pitch);
+// Sweep kernel.  CTA tile: 32 columns x 64 rows, 32x8 threads, each thread an 8-row strip
+// of one column with a sliding 3x3 window (float32 and double copies), so every u, v value
+// is read from shared memory and converted to double once per thread.
+// Data movement (one mbarrier, one elected thread): a 3-D TMA copy brings the 8 coefficient
+// planes of the tile (32 x 64 x 8 floats = 64 KB) and two 2-D TMA copies the u, v tiles
+// with their 1-pixel halo (40 x 66 floats each, x starting 4 floats left of the tile so the
+// copy stays 16-byte aligned).  Out-of-image cells (zero-filled by TMA) are replaced by
+// their clamped neighbours ('nearest') on tiles that touch the border.
+// Arithmetic:
+//  - 2-term stencils (D, D^T, F, F^T) in float32 as 0 + w0*a + w1*b: with exact operand
+//    halves, one float32 rounding of the exact value equals the reference's double
+//    accumulation rounded to float32 (including the sign of zero);
+//  - M (4 terms) and H (8 terms) keep the reference's double accumulation order; H uses
+//    'constant' 0 outside the image (selected on border tiles).
+constexpr int LS_TW = 32, LS_TH = 64, LS_RPT = LS_TH / 8;
+constexpr int LS_UW = LS_TW + 8, LS_UH = LS_TH + 2;  // u/v tile: x from x0-4, y from y0-1
+constexpr int LS_COEF_BYTES = 8 * LS_TW * LS_TH * 4, LS_UV_BYTES = LS_UW * LS_UH * 4;
+constexpr int LS_UV_STRIDE = (LS_UV_BYTES + 127) / 128 * 128;  // keeps every TMA destination 128-byte aligned
+constexpr size_t LS_SMEM = LS_COEF_BYTES + 2 * LS_UV_STRIDE + 128 + 128;  // + barrier + alignment slack
+constexpr long long LS_WAIT_LIMIT = 1ll << 22;
+
+__device__ __forceinline__ float st2(float a, float b, float wa, float wb) {
+  return __fadd_rn(__fadd_rn(0.0f, __fmul_rn(a, wa)), __fmul_rn(b, wb));
+}
+__device__ __forceinline__ float st_m(const double d[3][3]) {
+  double t = __dadd_rn(0.0, __dmul_rn(d[0][0], 0.25));
+  t = __dadd_rn(t, __dmul_rn(d[0][2], -0.25));
+  t = __dadd_rn(t, __dmul_rn(d[2][0], -0.25));
+  t = __dadd_rn(t, __dmul_rn(d[2][2], 0.25));
+  return (float)t;
+}
+template <bool EDGE>
+__device__ __forceinline__ float st_h(const double d[3][3], bool T, bool B, bool L, bool R) {
+  double t = 0.0;
+  t = __dadd_rn(t, (EDGE && (T || L)) ? 0.0 : d[0][0]);
+  t = __dadd_rn(t, (EDGE && T) ? 0.0 : d[0][1]);
+  t = __dadd_rn(t, (EDGE && (T || R)) ? 0.0 : d[0][2]);
+  t = __dadd_rn(t, (EDGE && L) ? 0.0 : d[1][0]);
+  t = __dadd_rn(t, (EDGE && R) ? 0.0 : d[1][2]);
+  t = __dadd_rn(t, (EDGE && (B || L)) ? 0.0 : d[2][0]);
+  t = __dadd_rn(t, (EDGE && B) ? 0.0 : d[2][1]);
+  t = __dadd_rn(t, (EDGE && (B || R)) ? 0.0 : d[2][2]);
+  return (float)t;
+}
+
+template <bool EDGE>
+__device__ __forceinline__ void ls_strip(const float (*su)[LS_UW], const float (*sv)[LS_UW],
+                                         const float (*sc)[LS_TH][LS_TW], float* __restrict__ un,
+                                         float* __restrict__ vn, int H, int W, int pitch, float h, int x, int y0,
+                                         int r0, int tx, double& du2, double& dv2) {
+  const int c = tx + 4;  // tile column of x
+  float fu[3][3], fv[3][3];
+  double du[3][3], dv[3][3];
+#pragma unroll
+  for (int r = 0; r < 2; r++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      fu[r + 1][j] = su[r0 + r][c - 1 + j];
+      fv[r + 1][j] = sv[r0 + r][c - 1 + j];
+      du[r + 1][j] = (double)fu[r + 1][j];
+      dv[r + 1][j] = (double)fv[r + 1][j];
+    }
+#pragma unroll
+  for (int r = 0; r < LS_RPT; r++) {
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      fu[0][j] = fu[1][j]; fu[1][j] = fu[2][j];
+      fv[0][j] = fv[1][j]; fv[1][j] = fv[2][j];
+      du[0][j] = du[1][j]; du[1][j] = du[2][j];
+      dv[0][j] = dv[1][j]; dv[1][j] = dv[2][j];
+      fu[2][j] = su[r0 + r + 2][c - 1 + j];
+      fv[2][j] = sv[r0 + r + 2][c - 1 + j];
+      du[2][j] = (double)fu[2][j];
+      dv[2][j] = (double)fv[2][j];
+    }
+    const int y = y0 + r;
+    if (y >= H || x >= W) continue;
+    const int ly = r0 + r;
+    const bool T = y == 0, B = y == H - 1, L = x == 0, R = x == W - 1;
+    const float a = sc[0][ly][tx], b = sc[1][ly][tx], cc = sc[2][ly][tx];
+    float Du = st2(fu[0][1], fu[2][1], -0.5f, 0.5f), DTu = st2(fu[1][0], fu[1][2], -0.5f, 0.5f);
+    float Dv = st2(fv[0][1], fv[2][1], -0.5f, 0.5f), DTv = st2(fv[1][0], fv[1][2], -0.5f, 0.5f);
+    float Fu = st2(fu[0][1], fu[2][1], 1.0f, 1.0f), FTv = st2(fv[1][0], fv[1][2], 1.0f, 1.0f);
+    float Mu = st_m(du), Mv = st_m(dv);
+    float Hu = st_h<EDGE>(du, T, B, L, R), Hv = st_h<EDGE>(dv, T, B, L, R);
     float bu = __fmul_rn(__fmul_rn(2.0f, a), Du);
     bu = __fadd_rn(bu, __fmul_rn(a, DTv));
     bu = __fadd_rn(bu, __fmul_rn(b, Dv));
-    bu = __fadd_rn(bu, __fmul_rn(c, Fu));
-    bu = __fadd_rn(bu, __fmul_rn(c, Mv));
+    bu = __fadd_rn(bu, __fmul_rn(cc, Fu));
+    bu = __fadd_rn(bu, __fmul_rn(cc, Mv));
     bu = __fadd_rn(bu, __fmul_rn(h, Hu));
-    bu = __fadd_rn(bu, coef[3 * plane + i]);
+    bu = __fadd_rn(bu, sc[3][ly][tx]);
     float bv = __fmul_rn(b, Du);
     bv = __fadd_rn(bv, __fmul_rn(a, DTu));
     bv = __fadd_rn(bv, __fmul_rn(__fmul_rn(2.0f, b), DTv));
-    bv = __fadd_rn(bv, __fmul_rn(c, Mu));
-    bv = __fadd_rn(bv, __fmul_rn(c, FTv));
+    bv = __fadd_rn(bv, __fmul_rn(cc, Mu));
+    bv = __fadd_rn(bv, __fmul_rn(cc, FTv));
     bv = __fadd_rn(bv, __fmul_rn(h, Hv));
-    bv = __fadd_rn(bv, coef[4 * plane + i]);
-    float B11 = coef[5 * plane + i], B12 = coef[6 * plane + i], B22 = coef[7 * plane + i];
+    bv = __fadd_rn(bv, sc[4][ly][tx]);
+    const float B11 = sc[5][ly][tx], B12 = sc[6][ly][tx], B22 = sc[7][ly][tx];
     float nu = -__fadd_rn(__fmul_rn(B11, bu), __fmul_rn(B12, bv));
     float nv = -__fadd_rn(__fmul_rn(B12, bu), __fmul_rn(B22, bv));
+    const size_t i = (size_t)y * pitch + x;
     un[i] = nu;
     vn[i] = nv;
-    double a1 = (double)nu - (double)U.p[1][1], a2 = (double)nv - (double)V.p[1][1];
-    du2 = a1 * a1;
-    dv2 = a2 * a2;
+    // squared change for the stop rule, in double
+    double eu = __dadd_rn((double)nu, -du[1][1]), ev = __dadd_rn((double)nv, -dv[1][1]);
+    du2 = __fma_rn(eu, eu, du2);
+    dv2 = __fma_rn(ev, ev, dv2);
+  }
+}
+
+// One sweep.  `err_flag` receives 1 if a TMA wait timed out (the CTA then skips its tile).
+__global__ void __launch_bounds__(256) ls_sweep_kernel(const __grid_constant__ CUtensorMap tm_coef,
+                                                       const __grid_constant__ CUtensorMap tm_u,
+                                                       const __grid_constant__ CUtensorMap tm_v,
+                                                       float* __restrict__ un, float* __restrict__ vn, int H, int W,
+                                                       int pitch, float h, double* ss, int* run,
+                                                       unsigned int* done, int k, double inv_n, double tol,
+                                                       int* err_flag) {
+  if (k > 0 && *(volatile int*)(run + k) == 0) return;  // the stop rule ended the loop earlier
+  extern __shared__ __align__(128) unsigned char ls_smem_raw[];
+  unsigned char* ls_smem = ls_smem_raw + ((128 - (smem_u32(ls_smem_raw) & 127)) & 127);
+  float(*sc)[LS_TH][LS_TW] = reinterpret_cast<float(*)[LS_TH][LS_TW]>(ls_smem);
+  float(*su)[LS_UW] = reinterpret_cast<float(*)[LS_UW]>(ls_smem + LS_COEF_BYTES);
+  float(*sv)[LS_UW] = reinterpret_cast<float(*)[LS_UW]>(ls_smem + LS_COEF_BYTES + LS_UV_STRIDE);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ls_smem + LS_COEF_BYTES + 2 * LS_UV_STRIDE);
+  const int x0 = blockIdx.x * LS_TW, y0 = blockIdx.y * LS_TH;
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  if (t == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (t == 0) {
+    mbar_expect_tx(bar, LS_COEF_BYTES + 2 * LS_UV_BYTES);
+    tma_load_3d(sc, &tm_coef, x0, y0, 0, bar);
+    tma_load_2d(su, &tm_u, x0 - 4, y0 - 1, bar);
+    tma_load_2d(sv, &tm_v, x0 - 4, y0 - 1, bar);
+  }
+  bool ok = mbar_wait(bar, 0, LS_WAIT_LIMIT);
+  if (!ok) {  // record the timeout, give the copies one more bounded wait, skip the tile
+    if (t == 0) atomicExch(err_flag, 1);
+    mbar_wait(bar, 0, LS_WAIT_LIMIT);
+  }
+  const bool edge = x0 == 0 || y0 == 0 || x0 + LS_TW >= W || y0 + LS_TH >= H;
+  if (edge) {
+    __syncthreads();
+    // out-of-image cells of the u/v halo tiles take their clamped ('nearest') value
+    for (int e = t; e < LS_UH * LS_UW; e += 256) {
+      int r = e / LS_UW, cl = e - r * LS_UW;
+      int gy = y0 - 1 + r, gx = x0 - 4 + cl;
+      if (gy >= 0 && gy < H && gx >= 0 && gx < W) continue;
+      int cy = clampi(gy, 0, H - 1) - (y0 - 1), cx = clampi(gx, 0, W - 1) - (x0 - 4);
+      if (cy < 0 || cy >= LS_UH || cx < 0 || cx >= LS_UW) continue;  // cell outside every stencil
+      su[r][cl] = su[cy][cx];
+      sv[r][cl] = sv[cy][cx];
+    }
+  }
+  __syncthreads();
+  double du2 = 0.0, dv2 = 0.0;
+  const int x = x0 + threadIdx.x, r0 = threadIdx.y * LS_RPT, ys = y0 + r0;
+  if (ok) {
+    if (edge)
+      ls_strip<true>(su, sv, sc, un, vn, H, W, pitch, h, x, ys, r0, threadIdx.x, du2, dv2);
+    else
+      ls_strip<false>(su, sv, sc, un, vn, H, W, pitch, h, x, ys, r0, threadIdx.x, du2, dv2);
   }
   for (int o = 16; o > 0; o >>= 1) {
     du2 += __shfl_down_sync(0xffffffffu, du2, o);
     dv2 += __shfl_down_sync(0xffffffffu, dv2, o);
   }
   __shared__ double ru[8], rv[8];
-  int t = threadIdx.y * blockDim.x + threadIdx.x;
   if ((t & 31) == 0) {
     ru[t >> 5] = du2;
     rv[t >> 5] = dv2;
@@ -213,8 +349,10 @@ __global__ void __launch_bounds__(256) ls_sweep_kernel(const float* __restrict__
   }
 }
 
+// Sweeps run (and the last sweep's error); a TMA wait timeout in any sweep is reported as
+// iters = -1, err = NaN.
 __global__ void ls_count_kernel(LsCtrl* ctrl, const int* run, const double* ss, int maxnum, double inv_n,
-                                int* iters_out, double* err_out) {
+                                const int* err_flag, int* iters_out, double* err_out) {
   int K = maxnum;
   for (int k = 1; k < maxnum; k++)
     if (!run[k]) {
@@ -222,25 +360,28 @@ __global__ void ls_count_kernel(LsCtrl* ctrl, const int* run, const double* ss, 
       break;
     }
   ctrl->K = K;
-  if (iters_out) *iters_out = K;
-  if (err_out) *err_out = K > 0 ? ls_err(ss, K - 1, inv_n) : 0.0;
+  bool failed = *err_flag != 0;
+  if (iters_out) *iters_out = failed ? -1 : K;
+  if (err_out) *err_out = failed ? __longlong_as_double(0x7ff8000000000000ll) : (K > 0 ? ls_err(ss, K - 1, inv_n) : 0.0);
 }
 
-// The last sweep wrote the ping-pong buffers when the sweep count is odd.
-__global__ void ls_finalize_kernel(const float* __restrict__ bu, const float* __restrict__ bv, float* __restrict__ V,
-                                   float* __restrict__ U, int W, int pitch, const LsCtrl* ctrl) {
-  if (!(ctrl->K & 1)) return;
+// Result of the last sweep (buffer K mod 2) -> caller's V (row component) and U.
+__global__ void ls_finalize_kernel(const float* __restrict__ u0, const float* __restrict__ v0,
+                                   const float* __restrict__ u1, const float* __restrict__ v1, float* __restrict__ V,
+                                   float* __restrict__ U, int W, int sp, int dp, const LsCtrl* ctrl) {
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-  if (x < W) {
-    size_t i = (size_t)y * pitch + x;
-    V[i] = bu[i];
-    U[i] = bv[i];
-  }
+  if (x >= W) return;
+  const bool odd = ctrl->K & 1;
+  size_t i = (size_t)y * sp + x, o = (size_t)y * dp + x;
+  V[o] = odd ? u1[i] : u0[i];
+  U[o] = odd ? v1[i] : v0[i];
 }
 
 }  // namespace ofb
 
 using namespace ofb;
+
+static inline int ls_pitch(int W) { return (W + 31) / 32 * 32; }
 
 extern "C" int of_ls_coefficients(const float* I1n, const float* Et, float* coef, int H, int W, int pitch, float h,
                                   void* stream) {
@@ -252,12 +393,12 @@ extern "C" int of_ls_coefficients(const float* I1n, const float* Et, float* coef
 
 extern "C" size_t of_ls_workspace_size(int H, int W, int pitch, int maxnum) {
   Sizer s;
-  size_t N = (size_t)H * pitch;
+  size_t N = (size_t)H * ls_pitch(W);
   s.take<float>(3 * N);  // I1, I2, Et
   s.take<float>(8 * N);  // coefficient planes
-  s.take<float>(2 * N);  // ping-pong u, v
+  s.take<float>(4 * N);  // u0, v0, u1, v1
   s.take<LsCtrl>(1);
-  s.take<int>((size_t)maxnum + 1);
+  s.take<int>((size_t)maxnum + 2);  // run[] and the TMA error flag
   s.take<unsigned int>((size_t)maxnum + 1);
   s.take<double>(2 * (size_t)(maxnum > 0 ? maxnum : 1));
   return s.off;
@@ -272,31 +413,56 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   if (!workspace || workspace_bytes < need)
     return set_error(OF_ERR_WORKSPACE, "of_ls_solve: workspace too small (%zu < %zu)", workspace_bytes, need);
   cudaStream_t st = as_stream(stream);
-  size_t N = (size_t)H * pitch;
+  const int P = ls_pitch(W);
+  const size_t N = (size_t)H * P;
   Carver c(workspace, workspace_bytes);
   float* nrm = c.take<float>(3 * N);
   float* coef = c.take<float>(8 * N);
-  float* pp = c.take<float>(2 * N);
+  float* uv = c.take<float>(4 * N);
   LsCtrl* ctrl = c.take<LsCtrl>(1);
-  int* run = c.take<int>((size_t)maxnum + 1);
+  int* run = c.take<int>((size_t)maxnum + 2);
   unsigned int* done = c.take<unsigned int>((size_t)maxnum + 1);
   double* ss = c.take<double>(2 * (size_t)(maxnum > 0 ? maxnum : 1));
-  float *n1 = nrm, *n2 = nrm + N, *et = nrm + 2 * N, *bu = pp, *bv = pp + N;
+  int* err_flag = run + maxnum + 1;
+  float *n1 = nrm, *n2 = nrm + N, *et = nrm + 2 * N;
+  float* ub[2] = {uv, uv + 2 * N};
+  float* vb[2] = {uv + N, uv + 3 * N};
+  // tensor maps: 8 coefficient planes (3-D) and the four u / v planes (2-D)
+  CUtensorMap tm_coef, tm_u[2], tm_v[2];
+  {
+    uint64_t d3[3] = {(uint64_t)W, (uint64_t)H, 8}, s3[2] = {(uint64_t)P * 4, (uint64_t)N * 4};
+    uint32_t b3[3] = {LS_TW, LS_TH, 8};
+    int rc = tmap_f32(&tm_coef, coef, 3, d3, s3, b3);
+    if (rc) return rc;
+    uint64_t d2[2] = {(uint64_t)W, (uint64_t)H}, s2[1] = {(uint64_t)P * 4};
+    uint32_t b2[2] = {LS_UW, LS_UH};
+    for (int q = 0; q < 2; q++) {
+      if ((rc = tmap_f32(&tm_u[q], ub[q], 2, d2, s2, b2))) return rc;
+      if ((rc = tmap_f32(&tm_v[q], vb[q], 2, d2, s2, b2))) return rc;
+    }
+  }
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(ls_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LS_SMEM);
+    attr = true;
+  }
   // control block, flags, counters and sums are contiguous: one memset clears them
   cudaMemsetAsync(ctrl, 0, (size_t)((char*)(ss + 2 * (size_t)(maxnum > 0 ? maxnum : 1)) - (char*)ctrl), st);
   dim3 mg((W + 255) / 256 < 8 ? (W + 255) / 256 : 8, H < 512 ? H : 512);
   ls_max_kernel<<<mg, 256, 0, st>>>(I0, I1, H, W, pitch, ctrl->maxkey);
   dim3 rg((W + 255) / 256, H);
-  ls_normalize_kernel<<<rg, 256, 0, st>>>(I0, I1, ctrl->maxkey, n1, n2, et, W, pitch);
+  ls_normalize_kernel<<<rg, 256, 0, st>>>(I0, I1, ctrl->maxkey, n1, n2, et, W, pitch, P);
   dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8);
-  ls_coef_kernel<<<grd, blk, 0, st>>>(n1, et, coef, N, H, W, pitch, h);
+  ls_coef_kernel<<<grd, blk, 0, st>>>(n1, et, coef, N, H, W, P, h);
+  ls_copy2_kernel<<<rg, 256, 0, st>>>(V, U, ub[0], vb[0], W, pitch, P, nullptr);
   double inv_n = 1.0 / ((double)H * (double)W);
+  dim3 sgrd((W + LS_TW - 1) / LS_TW, (H + LS_TH - 1) / LS_TH);
   for (int k = 0; k < maxnum; k++) {
-    const float *su = (k & 1) ? bu : V, *sv = (k & 1) ? bv : U;
-    float *du = (k & 1) ? V : bu, *dv = (k & 1) ? U : bv;
-    ls_sweep_kernel<<<grd, blk, 0, st>>>(coef, N, su, sv, du, dv, H, W, pitch, h, ss, run, done, k, inv_n, tol);
+    int s = k & 1;
+    ls_sweep_kernel<<<sgrd, blk, LS_SMEM, st>>>(tm_coef, tm_u[s], tm_v[s], ub[s ^ 1], vb[s ^ 1], H, W, P, h, ss, run,
+                                                done, k, inv_n, tol, err_flag);
   }
-  ls_count_kernel<<<1, 1, 0, st>>>(ctrl, run, ss, maxnum, inv_n, iters_out, err_out);
-  ls_finalize_kernel<<<rg, 256, 0, st>>>(bu, bv, V, U, W, pitch, ctrl);
-  return check_launch("of_ls_solve", 5 + (long long)maxnum);
+  ls_count_kernel<<<1, 1, 0, st>>>(ctrl, run, ss, maxnum, inv_n, err_flag, iters_out, err_out);
+  ls_finalize_kernel<<<rg, 256, 0, st>>>(ub[0], vb[0], ub[1], vb[1], V, U, W, P, pitch, ctrl);
+  return check_launch("of_ls_solve", 6 + (long long)maxnum);
 }

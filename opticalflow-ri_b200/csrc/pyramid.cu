@@ -102,35 +102,58 @@ static int ksize_of(int in, int out, int bicubic) {
 
 // ----------------------------------------------------------------------------- spline
 // Thomas-algorithm moments of the not-a-knot spline through n >= 4 samples with unit
-// spacing; sample i of line l is y[i*ls + l*ss_], scratch/moments use the same layout.
-__device__ void nak_moments(const double* y, const float* yf, size_t ls, double* M, double* cp, double* dp, int n) {
-#define YV(i) (y ? y[(size_t)(i) * ls] : (double)yf[(size_t)(i) * ls])
+// spacing; sample i of the line is y[i*ls]; moments and scratch use the same stride.
+// The recurrences carry their previous terms in registers (the line data is the only
+// memory traffic), so one line costs O(n) dependent double operations, not O(n) memory
+// round trips.
+__device__ void nak_moments(const double* __restrict__ y, size_t ls, double* __restrict__ M, double* __restrict__ cp,
+                            double* __restrict__ dp, int n) {
+#define YV(i) y[(size_t)(i) * ls]
 #define MV(i) M[(size_t)(i) * ls]
-  double d1 = __dadd_rn(__dadd_rn(YV(2), -__dmul_rn(2.0, YV(1))), YV(0));
-  double dl = __dadd_rn(__dadd_rn(YV(n - 1), -__dmul_rn(2.0, YV(n - 2))), YV(n - 3));
-  MV(1) = d1;
-  MV(n - 2) = dl;
+  double M1 = __dadd_rn(__dadd_rn(YV(2), -__dmul_rn(2.0, YV(1))), YV(0));
+  double Ml = __dadd_rn(__dadd_rn(YV(n - 1), -__dmul_rn(2.0, YV(n - 2))), YV(n - 3));
+  MV(1) = M1;
+  MV(n - 2) = Ml;
+  double M2 = Ml, M3 = Ml;  // M[2], M[n-3] for the end conditions
   int m = n - 4;
   if (m > 0) {
+    double ym = YV(1), y0 = YV(2), cprev = 0.0, dprev = 0.0;
     for (int r = 0; r < m; r++) {
       int i = r + 2;
-      double rhs = __dmul_rn(6.0, __dadd_rn(__dadd_rn(YV(i + 1), -__dmul_rn(2.0, YV(i))), YV(i - 1)));
-      if (r == 0) rhs = __dadd_rn(rhs, -MV(1));
-      if (r == m - 1) rhs = __dadd_rn(rhs, -MV(n - 2));
+      double yp = YV(i + 1);
+      double rhs = __dmul_rn(6.0, __dadd_rn(__dadd_rn(yp, -__dmul_rn(2.0, y0)), ym));
+      if (r == 0) rhs = __dadd_rn(rhs, -M1);
+      if (r == m - 1) rhs = __dadd_rn(rhs, -Ml);
+      double c, d;
       if (r == 0) {
-        cp[0] = __ddiv_rn(1.0, 4.0);
-        dp[0] = __ddiv_rn(rhs, 4.0);
+        c = __ddiv_rn(1.0, 4.0);
+        d = __ddiv_rn(rhs, 4.0);
       } else {
-        double den = __dadd_rn(4.0, -cp[(size_t)(r - 1) * ls]);
-        cp[(size_t)r * ls] = __ddiv_rn(1.0, den);
-        dp[(size_t)r * ls] = __ddiv_rn(__dadd_rn(rhs, -dp[(size_t)(r - 1) * ls]), den);
+        double den = __dadd_rn(4.0, -cprev);
+        c = __ddiv_rn(1.0, den);
+        d = __ddiv_rn(__dadd_rn(rhs, -dprev), den);
       }
+      cp[(size_t)r * ls] = c;
+      dp[(size_t)r * ls] = d;
+      cprev = c;
+      dprev = d;
+      ym = y0;
+      y0 = yp;
     }
-    MV(m + 1) = dp[(size_t)(m - 1) * ls];
-    for (int r = m - 2; r >= 0; r--) MV(r + 2) = __dadd_rn(dp[(size_t)r * ls], -__dmul_rn(cp[(size_t)r * ls], MV(r + 3)));
+    double next = dprev;
+    MV(m + 1) = next;
+    M3 = next;  // M[n-3] = M[m+1]
+    for (int r = m - 2; r >= 0; r--) {
+      next = __dadd_rn(dp[(size_t)r * ls], -__dmul_rn(cp[(size_t)r * ls], next));
+      MV(r + 2) = next;
+    }
+    M2 = next;  // M[2]
+  } else {
+    M2 = Ml;  // n == 4: M[2] = M[n-2], M[n-3] = M[1]
+    M3 = M1;
   }
-  MV(0) = __dadd_rn(__dmul_rn(2.0, MV(1)), -MV(2));
-  MV(n - 1) = __dadd_rn(__dmul_rn(2.0, MV(n - 2)), -MV(n - 3));
+  MV(0) = __dadd_rn(__dmul_rn(2.0, M1), -M2);
+  MV(n - 1) = __dadd_rn(__dmul_rn(2.0, Ml), -M3);
 #undef YV
 #undef MV
 }
@@ -161,7 +184,7 @@ __global__ void spline_my_kernel(const float* __restrict__ src, int sp, int h, i
   if (x >= w) return;
   // the column (pitch sp) is copied into Y0, laid out [i][x] like the moments and scratch
   for (int i = 0; i < h; i++) Y0[(size_t)i * w + x] = (double)src[(size_t)i * sp + x];
-  nak_moments(Y0 + x, nullptr, w, M + x, S + x, S + (size_t)h * w + x, h);
+  nak_moments(Y0 + x, w, M + x, S + x, S + (size_t)h * w + x, h);
 }
 
 // T[Y][x] = column spline at fine row Y
@@ -182,7 +205,7 @@ __global__ void spline_mx_kernel(const double* __restrict__ T, int w, int H, dou
   int Y = blockIdx.x * blockDim.x + threadIdx.x;
   if (Y >= H) return;
   for (int k = 0; k < w; k++) Tt[(size_t)k * H + Y] = T[(size_t)Y * w + k];
-  nak_moments(Tt + Y, nullptr, H, M + Y, cp + Y, dp + Y, w);
+  nak_moments(Tt + Y, H, M + Y, cp + Y, dp + Y, w);
 }
 
 __global__ void spline_ex_kernel(const double* __restrict__ Tt, const double* __restrict__ M, float* __restrict__ dst,

@@ -1,0 +1,67 @@
+// Tensor Memory Accelerator helpers: host-side tiled tensor maps (float32) and the
+// device-side mbarrier / cp.async.bulk.tensor sequence.  No multicast anywhere.
+//
+// Rules these helpers rely on (checked by the callers):
+//  - global base address 16-byte aligned, every stride a multiple of 16 bytes;
+//  - box inner extent x element size a multiple of 16 bytes, every box dimension <= 256;
+//  - the x coordinate of every copy a multiple of 4 floats (16 bytes); other coordinates
+//    may be negative or beyond the tensor (those elements are filled with zeros);
+//  - shared-memory destinations 128-byte aligned.
+#pragma once
+#include <cuda.h>  // CUtensorMap and its enums (header only; the encoder is fetched at run time)
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ofb {
+
+// Encodes a float32 tiled tensor map of rank 2 or 3.  dims / box are innermost first;
+// strides_bytes holds rank-1 byte strides.  Returns 0 or an OF_ERR_* code (message set).
+int tmap_f32(CUtensorMap* map, const void* base, int rank, const uint64_t* dims, const uint64_t* strides_bytes,
+             const uint32_t* box);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Waits for phase `parity` of the barrier with an iteration limit; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long max_iters) {
+  uint32_t addr = smem_u32(bar);
+  for (long long it = 0; it < max_iters; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+}  // namespace ofb

@@ -82,6 +82,17 @@ class denseLucasKanade_PyCl(object):
         Ud, Vd, _, _ = self._run(im1, im2, U, V, False)
         return Ud, Vd, True
 
+    def _graph_key(self, n):
+        if self.enableVorticityEnhancement:
+            return None  # the window masks are chosen on the host from the current flow
+        return ("LK", int(self.Niter), int(self.windowHalfWidth), str(self.device))
+
+    def _graph_clone(self, n):
+        return self
+
+    def _graph_consume(self, n):
+        pass
+
     def getAlgoName(self):
         return 'OpenCL Dense LK'
 
