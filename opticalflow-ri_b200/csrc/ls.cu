@@ -170,11 +170,12 @@ __device__ __forceinline__ double ls_err(const double* ss, int k, double inv_n) 
 //    accumulation rounded to float32 (including the sign of zero);
 //  - M (4 terms) and H (8 terms) keep the reference's double accumulation order; H uses
 //    'constant' 0 outside the image (selected on border tiles).
-constexpr int LS_TW = 32, LS_TH = 64, LS_RPT = LS_TH / 8;
+constexpr int LS_TW = 32, LS_TH = 64, LS_TY = 16, LS_RPT = LS_TH / LS_TY, LS_THREADS = LS_TW * LS_TY;
 constexpr int LS_UW = LS_TW + 8, LS_UH = LS_TH + 2;  // u/v tile: x from x0-4, y from y0-1
 constexpr int LS_COEF_BYTES = 8 * LS_TW * LS_TH * 4, LS_UV_BYTES = LS_UW * LS_UH * 4;
 constexpr int LS_UV_STRIDE = (LS_UV_BYTES + 127) / 128 * 128;  // keeps every TMA destination 128-byte aligned
-constexpr size_t LS_SMEM = LS_COEF_BYTES + 2 * LS_UV_STRIDE + 128 + 128;  // + barrier + alignment slack
+constexpr int LS_STAGE = LS_COEF_BYTES + 2 * LS_UV_STRIDE;               // one tile: coefficients + u + v
+constexpr size_t LS_SMEM = 2 * LS_STAGE + 128 + 128;  // two stages + barriers + alignment slack
 constexpr long long LS_WAIT_LIMIT = 1ll << 22;
 
 __device__ __forceinline__ float st2(float a, float b, float wa, float wb) {
@@ -268,79 +269,105 @@ __device__ __forceinline__ void ls_strip(const float (*su)[LS_UW], const float (
   }
 }
 
-// One sweep.  `err_flag` receives 1 if a TMA wait timed out (the CTA then skips its tile).
-__global__ void __launch_bounds__(256) ls_sweep_kernel(const __grid_constant__ CUtensorMap tm_coef,
-                                                       const __grid_constant__ CUtensorMap tm_u,
-                                                       const __grid_constant__ CUtensorMap tm_v,
-                                                       float* __restrict__ un, float* __restrict__ vn, int H, int W,
-                                                       int pitch, float h, double* ss, int* run,
-                                                       unsigned int* done, int k, double inv_n, double tol,
-                                                       int* err_flag) {
+// One sweep, persistent: gridDim.x CTAs (one per SM) walk the tiles with a two-stage TMA
+// pipeline - while a tile is computed the next one is already in flight into the other
+// stage.  `err_flag` receives 1 if a TMA wait times out (the CTA then stops early).
+struct LsStage {
+  float (*sc)[LS_TH][LS_TW];
+  float (*su)[LS_UW];
+  float (*sv)[LS_UW];
+};
+
+__device__ __forceinline__ LsStage ls_stage(unsigned char* base, int s) {
+  unsigned char* p = base + s * LS_STAGE;
+  return {reinterpret_cast<float(*)[LS_TH][LS_TW]>(p), reinterpret_cast<float(*)[LS_UW]>(p + LS_COEF_BYTES),
+          reinterpret_cast<float(*)[LS_UW]>(p + LS_COEF_BYTES + LS_UV_STRIDE)};
+}
+
+__device__ __forceinline__ void ls_issue(const LsStage& S, uint64_t* bar, const CUtensorMap* tc, const CUtensorMap* tu,
+                                         const CUtensorMap* tv, int x0, int y0) {
+  mbar_expect_tx(bar, LS_COEF_BYTES + 2 * LS_UV_BYTES);
+  tma_load_3d(S.sc, tc, x0, y0, 0, bar);
+  tma_load_2d(S.su, tu, x0 - 4, y0 - 1, bar);
+  tma_load_2d(S.sv, tv, x0 - 4, y0 - 1, bar);
+}
+
+__global__ void __launch_bounds__(LS_THREADS, 1) ls_sweep_kernel(const __grid_constant__ CUtensorMap tm_coef,
+                                                                 const __grid_constant__ CUtensorMap tm_u,
+                                                                 const __grid_constant__ CUtensorMap tm_v,
+                                                                 float* __restrict__ un, float* __restrict__ vn, int H,
+                                                                 int W, int pitch, float h, double* ss, int* run,
+                                                                 unsigned int* done, int k, double inv_n, double tol,
+                                                                 int* err_flag) {
   if (k > 0 && *(volatile int*)(run + k) == 0) return;  // the stop rule ended the loop earlier
   extern __shared__ __align__(128) unsigned char ls_smem_raw[];
-  unsigned char* ls_smem = ls_smem_raw + ((128 - (smem_u32(ls_smem_raw) & 127)) & 127);
-  float(*sc)[LS_TH][LS_TW] = reinterpret_cast<float(*)[LS_TH][LS_TW]>(ls_smem);
-  float(*su)[LS_UW] = reinterpret_cast<float(*)[LS_UW]>(ls_smem + LS_COEF_BYTES);
-  float(*sv)[LS_UW] = reinterpret_cast<float(*)[LS_UW]>(ls_smem + LS_COEF_BYTES + LS_UV_STRIDE);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(ls_smem + LS_COEF_BYTES + 2 * LS_UV_STRIDE);
-  const int x0 = blockIdx.x * LS_TW, y0 = blockIdx.y * LS_TH;
+  unsigned char* base = ls_smem_raw + ((128 - (smem_u32(ls_smem_raw) & 127)) & 127);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + 2 * LS_STAGE);
+  const int tilesx = (W + LS_TW - 1) / LS_TW, ntiles = tilesx * ((H + LS_TH - 1) / LS_TH);
   const int t = threadIdx.y * blockDim.x + threadIdx.x;
-  if (t == 0) mbar_init(bar, 1);
-  __syncthreads();
   if (t == 0) {
-    mbar_expect_tx(bar, LS_COEF_BYTES + 2 * LS_UV_BYTES);
-    tma_load_3d(sc, &tm_coef, x0, y0, 0, bar);
-    tma_load_2d(su, &tm_u, x0 - 4, y0 - 1, bar);
-    tma_load_2d(sv, &tm_v, x0 - 4, y0 - 1, bar);
-  }
-  bool ok = mbar_wait(bar, 0, LS_WAIT_LIMIT);
-  if (!ok) {  // record the timeout, give the copies one more bounded wait, skip the tile
-    if (t == 0) atomicExch(err_flag, 1);
-    mbar_wait(bar, 0, LS_WAIT_LIMIT);
-  }
-  const bool edge = x0 == 0 || y0 == 0 || x0 + LS_TW >= W || y0 + LS_TH >= H;
-  if (edge) {
-    __syncthreads();
-    // out-of-image cells of the u/v halo tiles take their clamped ('nearest') value
-    for (int e = t; e < LS_UH * LS_UW; e += 256) {
-      int r = e / LS_UW, cl = e - r * LS_UW;
-      int gy = y0 - 1 + r, gx = x0 - 4 + cl;
-      if (gy >= 0 && gy < H && gx >= 0 && gx < W) continue;
-      int cy = clampi(gy, 0, H - 1) - (y0 - 1), cx = clampi(gx, 0, W - 1) - (x0 - 4);
-      if (cy < 0 || cy >= LS_UH || cx < 0 || cx >= LS_UW) continue;  // cell outside every stencil
-      su[r][cl] = su[cy][cx];
-      sv[r][cl] = sv[cy][cx];
-    }
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
   }
   __syncthreads();
+  int tile = blockIdx.x;
+  if (t == 0 && tile < ntiles) ls_issue(ls_stage(base, 0), &bar[0], &tm_coef, &tm_u, &tm_v, (tile % tilesx) * LS_TW,
+                                        (tile / tilesx) * LS_TH);
   double du2 = 0.0, dv2 = 0.0;
-  const int x = x0 + threadIdx.x, r0 = threadIdx.y * LS_RPT, ys = y0 + r0;
-  if (ok) {
+  for (int i = 0; tile < ntiles; i++, tile += gridDim.x) {
+    const int s = i & 1;
+    const int next = tile + gridDim.x;
+    if (t == 0 && next < ntiles)  // the other stage was released by the barrier that ended iteration i-1
+      ls_issue(ls_stage(base, s ^ 1), &bar[s ^ 1], &tm_coef, &tm_u, &tm_v, (next % tilesx) * LS_TW,
+               (next / tilesx) * LS_TH);
+    const LsStage S = ls_stage(base, s);
+    if (!mbar_wait(&bar[s], (i >> 1) & 1, LS_WAIT_LIMIT)) {
+      if (t == 0) atomicExch(err_flag, 1);
+      mbar_wait(&bar[s], (i >> 1) & 1, LS_WAIT_LIMIT);  // one more bounded wait for the copies in flight
+      if (next < ntiles) mbar_wait(&bar[s ^ 1], ((i + 1) >> 1) & 1, LS_WAIT_LIMIT);
+      break;
+    }
+    const int x0 = (tile % tilesx) * LS_TW, y0 = (tile / tilesx) * LS_TH;
+    const bool edge = x0 == 0 || y0 == 0 || x0 + LS_TW >= W || y0 + LS_TH >= H;
+    if (edge) {
+      // out-of-image cells of the u/v halo tiles take their clamped ('nearest') value
+      for (int e = t; e < LS_UH * LS_UW; e += LS_THREADS) {
+        int r = e / LS_UW, cl = e - r * LS_UW;
+        int gy = y0 - 1 + r, gx = x0 - 4 + cl;
+        if (gy >= 0 && gy < H && gx >= 0 && gx < W) continue;
+        int cy = clampi(gy, 0, H - 1) - (y0 - 1), cx = clampi(gx, 0, W - 1) - (x0 - 4);
+        if (cy < 0 || cy >= LS_UH || cx < 0 || cx >= LS_UW) continue;  // cell outside every stencil
+        S.su[r][cl] = S.su[cy][cx];
+        S.sv[r][cl] = S.sv[cy][cx];
+      }
+      __syncthreads();
+    }
+    const int x = x0 + threadIdx.x, r0 = threadIdx.y * LS_RPT, ys = y0 + r0;
     if (edge)
-      ls_strip<true>(su, sv, sc, un, vn, H, W, pitch, h, x, ys, r0, threadIdx.x, du2, dv2);
+      ls_strip<true>(S.su, S.sv, S.sc, un, vn, H, W, pitch, h, x, ys, r0, threadIdx.x, du2, dv2);
     else
-      ls_strip<false>(su, sv, sc, un, vn, H, W, pitch, h, x, ys, r0, threadIdx.x, du2, dv2);
+      ls_strip<false>(S.su, S.sv, S.sc, un, vn, H, W, pitch, h, x, ys, r0, threadIdx.x, du2, dv2);
+    __syncthreads();  // stage s is free for the load issued at iteration i+1
   }
   for (int o = 16; o > 0; o >>= 1) {
     du2 += __shfl_down_sync(0xffffffffu, du2, o);
     dv2 += __shfl_down_sync(0xffffffffu, dv2, o);
   }
-  __shared__ double ru[8], rv[8];
+  __shared__ double ru[LS_THREADS / 32], rv[LS_THREADS / 32];
   if ((t & 31) == 0) {
     ru[t >> 5] = du2;
     rv[t >> 5] = dv2;
   }
   __syncthreads();
   if (t == 0) {
-    for (int w = 1; w < 8; w++) {
+    for (int w = 1; w < LS_THREADS / 32; w++) {
       du2 += ru[w];
       dv2 += rv[w];
     }
     atomicAdd(ss + 2 * k, du2);
     atomicAdd(ss + 2 * k + 1, dv2);
     __threadfence();
-    unsigned int nblk = gridDim.x * gridDim.y;
-    if (atomicAdd(done + k, 1u) == nblk - 1) {  // last block of this sweep decides the next one
+    if (atomicAdd(done + k, 1u) == gridDim.x - 1) {  // last CTA of this sweep decides the next one
       __threadfence();
       double s0 = atomicAdd(ss + 2 * k, 0.0), s1 = atomicAdd(ss + 2 * k + 1, 0.0);
       double e = (sqrt(s0) + sqrt(s1)) * inv_n;
@@ -349,8 +376,6 @@ __global__ void __launch_bounds__(256) ls_sweep_kernel(const __grid_constant__ C
   }
 }
 
-// Sweeps run (and the last sweep's error); a TMA wait timeout in any sweep is reported as
-// iters = -1, err = NaN.
 __global__ void ls_count_kernel(LsCtrl* ctrl, const int* run, const double* ss, int maxnum, double inv_n,
                                 const int* err_flag, int* iters_out, double* err_out) {
   int K = maxnum;
@@ -456,10 +481,12 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   ls_coef_kernel<<<grd, blk, 0, st>>>(n1, et, coef, N, H, W, P, h);
   ls_copy2_kernel<<<rg, 256, 0, st>>>(V, U, ub[0], vb[0], W, pitch, P, nullptr);
   double inv_n = 1.0 / ((double)H * (double)W);
-  dim3 sgrd((W + LS_TW - 1) / LS_TW, (H + LS_TH - 1) / LS_TH);
+  int ntiles = ((W + LS_TW - 1) / LS_TW) * ((H + LS_TH - 1) / LS_TH);
+  int sgrd = ntiles < kNumSMs ? ntiles : kNumSMs;
+  dim3 sblk(LS_TW, LS_TY);
   for (int k = 0; k < maxnum; k++) {
     int s = k & 1;
-    ls_sweep_kernel<<<sgrd, blk, LS_SMEM, st>>>(tm_coef, tm_u[s], tm_v[s], ub[s ^ 1], vb[s ^ 1], H, W, P, h, ss, run,
+    ls_sweep_kernel<<<sgrd, sblk, LS_SMEM, st>>>(tm_coef, tm_u[s], tm_v[s], ub[s ^ 1], vb[s ^ 1], H, W, P, h, ss, run,
                                                 done, k, inv_n, tol, err_flag);
   }
   ls_count_kernel<<<1, 1, 0, st>>>(ctrl, run, ss, maxnum, inv_n, err_flag, iters_out, err_out);
