@@ -14,6 +14,7 @@
 //    updateMatrices into the other M buffer — so M is read once per iteration and the
 //    blurred M never leaves the SM.
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace ofb {
 
@@ -299,40 +300,76 @@ __global__ void __launch_bounds__(256) fb_iter_kernel(const float* __restrict__ 
 // row; taps fully unrolled in the reference order.  The thread's 8 pixels x 5 blurred
 // planes stay in registers for updateFlow / updateMatrices.
 constexpr int FBK_TW = 64, FBK_TH = 32, FBK_R = 8;
+constexpr long long FBK_WAIT_LIMIT = 1ll << 22;
 template <int KH>
-__global__ void __launch_bounds__(256, 2) fb_iter_fixed_kernel(const float* __restrict__ Min, float* __restrict__ Mout,
-                                                               const float* __restrict__ R0,
+struct FbkGeom {
+  static constexpr int IW = FBK_TW + 2 * KH, IH = FBK_TH + 2 * KH;
+  static constexpr int STAGE = IW * IH * 4;  // bytes of one staged input plane tile
+  static constexpr size_t SMEM = 2 * STAGE + (size_t)FBK_TH * IW * 4 + 128 + 128;
+};
+
+// reflect-101 fix-up of a staged tile: cells outside the image take their mirror image
+template <int KH>
+__device__ __forceinline__ void fbk_reflect(float* tin, int x0, int y0, int H, int W) {
+  constexpr int IW = FbkGeom<KH>::IW, IH = FbkGeom<KH>::IH;
+  for (int i = threadIdx.x; i < IH * IW; i += 256) {
+    int ly = i / IW, lx = i - ly * IW;
+    int gy = y0 - KH + ly, gx = x0 - KH + lx;
+    if (gy >= 0 && gy < H && gx >= 0 && gx < W) continue;
+    int sy = fb_row(gy, H) - (y0 - KH), sx = fb_col(gx, W) - (x0 - KH);
+    if (sy < 0 || sy >= IH || sx < 0 || sx >= IW) continue;  // only outside every used window
+    tin[i] = tin[sy * IW + sx];
+  }
+}
+
+// Fused iteration for a compile-time half window KH (windowSize 33 -> KH 16).
+// CTA: 64 x 32 outputs, 256 threads.  The 5 planes' (32+2KH) x (64+2KH) input tiles arrive
+// by TMA (a 3-D map over the 5 stacked planes, one plane per box) into two stages, so plane
+// p+1 is in flight while plane p is blurred; border tiles get their reflect-101 cells
+// filled in shared memory (one reflection: H, W >= KH + 1).  The vertical pass gives each
+// thread 8 consecutive rows of one column, the horizontal pass 8 consecutive columns of one
+// row; taps fully unrolled in the reference order.  The 8 pixels x 5 blurred planes of a
+// thread stay in registers for updateFlow / updateMatrices.
+template <int KH>
+__global__ void __launch_bounds__(256, 2) fb_iter_fixed_kernel(const __grid_constant__ CUtensorMap tm_m,
+                                                               float* __restrict__ Mout, const float* __restrict__ R0,
                                                                const float* __restrict__ R1, float* __restrict__ flowx,
                                                                float* __restrict__ flowy, int H, int W, int pitch,
                                                                FbTaps t, int upd) {
-  constexpr int IW = FBK_TW + 2 * KH, IH = FBK_TH + 2 * KH;
-  extern __shared__ float sm[];
-  float* tin = sm;             // IH x IW
-  float* tv = sm + IH * IW;    // FBK_TH x IW
-  const size_t pl = (size_t)H * pitch;
+  using G = FbkGeom<KH>;
+  constexpr int IW = G::IW;
+  extern __shared__ __align__(128) unsigned char fbk_raw[];
+  unsigned char* base = fbk_raw + ((128 - (smem_u32(fbk_raw) & 127)) & 127);
+  float* stage[2] = {reinterpret_cast<float*>(base), reinterpret_cast<float*>(base + G::STAGE)};
+  float* tv = reinterpret_cast<float*>(base + 2 * G::STAGE);  // FBK_TH x IW
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + 2 * G::STAGE + FBK_TH * IW * 4);
   const int x0 = blockIdx.x * FBK_TW, y0 = blockIdx.y * FBK_TH;
-  const bool interior = x0 >= KH && y0 >= KH && x0 + FBK_TW + KH <= W && y0 + FBK_TH + KH <= H;
+  const bool border = x0 < KH || y0 < KH || x0 + FBK_TW + KH > W || y0 + FBK_TH + KH > H;
   const int hx = (threadIdx.x & 7) * FBK_R, hy = threadIdx.x >> 3;  // horizontal-pass assignment
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < 2; q++) {
+      mbar_expect_tx(&bar[q], G::STAGE);
+      tma_load_3d(stage[q], &tm_m, x0 - KH, y0 - KH, q, &bar[q]);
+    }
+  }
   float g[KH + 1];
 #pragma unroll
   for (int j = 0; j <= KH; j++) g[j] = t.g[j];
   float res[5][FBK_R];
+  bool ok = true;
 #pragma unroll
   for (int p = 0; p < 5; p++) {
-    const float* s = Min + p * pl;
-    if (interior) {
-      const float* base = s + (size_t)(y0 - KH) * pitch + (x0 - KH);
-      for (int i = threadIdx.x; i < IH * IW; i += 256) {
-        int ly = i / IW, lx = i - ly * IW;
-        tin[i] = __ldg(base + (size_t)ly * pitch + lx);
-      }
-    } else {
-      for (int i = threadIdx.x; i < IH * IW; i += 256) {
-        int ly = i / IW, lx = i - ly * IW;
-        tin[i] = __ldg(s + (size_t)fb_row(y0 - KH + ly, H) * pitch + fb_col(x0 - KH + lx, W));
-      }
+    float* tin = stage[p & 1];
+    if (ok && !mbar_wait(&bar[p & 1], (p >> 1) & 1, FBK_WAIT_LIMIT)) ok = false;
+    if (border) {
+      fbk_reflect<KH>(tin, x0, y0, H, W);
+      __syncthreads();
     }
-    __syncthreads();
     // vertical: work item = (column, 8-row group)
     for (int it = threadIdx.x; it < IW * (FBK_TH / FBK_R); it += 256) {
       const int col = it % IW, r0 = (it / IW) * FBK_R;
@@ -348,6 +385,11 @@ __global__ void __launch_bounds__(256, 2) fb_iter_fixed_kernel(const float* __re
       }
     }
     __syncthreads();
+    // the stage is free again: bring plane p+2 into it while the horizontal pass runs
+    if (threadIdx.x == 0 && p + 2 < 5 && ok) {
+      mbar_expect_tx(&bar[p & 1], G::STAGE);
+      tma_load_3d(tin, &tm_m, x0 - KH, y0 - KH, p + 2, &bar[p & 1]);
+    }
     {
       float c[FBK_R + 2 * KH];
 #pragma unroll
@@ -364,6 +406,15 @@ __global__ void __launch_bounds__(256, 2) fb_iter_fixed_kernel(const float* __re
   }
   const int y = y0 + hy;
   if (y >= H) return;
+  if (!ok) {  // a tile copy never arrived: the tile's flow is reported as NaN
+#pragma unroll
+    for (int r = 0; r < FBK_R; r++)
+      if (x0 + hx + r < W) {
+        flowx[(size_t)y * pitch + x0 + hx + r] = __int_as_float(0x7fc00000);
+        flowy[(size_t)y * pitch + x0 + hx + r] = __int_as_float(0x7fc00000);
+      }
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < FBK_R; r++) {
     const int x = x0 + hx + r;
@@ -447,12 +498,24 @@ extern "C" int of_fb_iteration(const float* M_in, float* M_out, const float* R0,
   OF_REQUIRE(!bad_plane(M_in, H, W, pitch) && R0 && R1 && flowx && flowy, "of_fb_iteration: bad plane");
   OF_REQUIRE(!update_matrices || (M_out && M_out != M_in), "of_fb_iteration: M_out missing or aliases M_in");
   OF_REQUIRE(wk && kh >= 0 && kh <= FB_MAXKH, "of_fb_iteration: bad kernel");
-  if (kh == 16) {  // windowSize 33, the reference default: the unrolled kernel
+  // windowSize 33 (the reference default) on images with a single reflect-101 border and
+  // TMA-compatible strides: the unrolled, TMA-staged kernel
+  if (kh == 16 && H > 16 && W > 16 && (pitch % 4) == 0 && (reinterpret_cast<uintptr_t>(M_in) & 15) == 0) {
     constexpr int KH = 16;
-    size_t smem = sizeof(float) * ((size_t)(FBK_TH + 2 * KH) * (FBK_TW + 2 * KH) + (size_t)FBK_TH * (FBK_TW + 2 * KH));
+    using G = FbkGeom<KH>;
+    CUtensorMap tm;
+    uint64_t dims[3] = {(uint64_t)W, (uint64_t)H, 5}, strides[2] = {(uint64_t)pitch * 4, (uint64_t)H * pitch * 4};
+    uint32_t box[3] = {G::IW, G::IH, 1};
+    int rc = tmap_f32(&tm, M_in, 3, dims, strides, box);
+    if (rc) return rc;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(fb_iter_fixed_kernel<KH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
+      attr = true;
+    }
     dim3 grid((W + FBK_TW - 1) / FBK_TW, (H + FBK_TH - 1) / FBK_TH);
-    fb_iter_fixed_kernel<KH><<<grid, 256, smem, as_stream(stream)>>>(M_in, M_out, R0, R1, flowx, flowy, H, W, pitch,
-                                                                     make_taps(wk, kh), update_matrices);
+    fb_iter_fixed_kernel<KH><<<grid, 256, G::SMEM, as_stream(stream)>>>(tm, M_out, R0, R1, flowx, flowy, H, W, pitch,
+                                                                        make_taps(wk, kh), update_matrices);
     return check_launch("of_fb_iteration");
   }
   size_t smem = sizeof(float) * ((size_t)(FBI_TH + 2 * kh) * (FBI_TW + 2 * kh) + (size_t)FBI_TH * (FBI_TW + 2 * kh));

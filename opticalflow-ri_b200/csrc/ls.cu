@@ -19,8 +19,8 @@ namespace ofb {
 
 struct LsCtrl {
   unsigned int maxkey[2];
-  int K;  // sweeps run, written by ls_count_kernel
-  int pad;
+  int K;          // sweeps run (written by the pass that ends the loop)
+  int final_buf;  // ping-pong buffer holding the last pass's result
 };
 // Workspace after LsCtrl: int run[maxnum+1] (run[k] != 0: sweep k runs; run[0] is unused),
 // unsigned done[maxnum] (blocks finished per sweep), double ss[maxnum][2] (squared changes).
@@ -156,26 +156,12 @@ __device__ __forceinline__ double ls_err(const double* ss, int k, double inv_n) 
   return (sqrt(ss[2 * k]) + sqrt(ss[2 * k + 1])) * inv_n;
 }
 
-// Sweep kernel.  CTA tile: 32 columns x 64 rows, 32x8 threads, each thread an 8-row strip
-// of one column with a sliding 3x3 window (float32 and double copies), so every u, v value
-// is read from shared memory and converted to double once per thread.
-// Data movement (one mbarrier, one elected thread): a 3-D TMA copy brings the 8 coefficient
-// planes of the tile (32 x 64 x 8 floats = 64 KB) and two 2-D TMA copies the u, v tiles
-// with their 1-pixel halo (40 x 66 floats each, x starting 4 floats left of the tile so the
-// copy stays 16-byte aligned).  Out-of-image cells (zero-filled by TMA) are replaced by
-// their clamped neighbours ('nearest') on tiles that touch the border.
-// Arithmetic:
+// Stencil helpers of the sweep.
 //  - 2-term stencils (D, D^T, F, F^T) in float32 as 0 + w0*a + w1*b: with exact operand
 //    halves, one float32 rounding of the exact value equals the reference's double
 //    accumulation rounded to float32 (including the sign of zero);
 //  - M (4 terms) and H (8 terms) keep the reference's double accumulation order; H uses
-//    'constant' 0 outside the image (selected on border tiles).
-constexpr int LS_TW = 32, LS_TH = 64, LS_TY = 16, LS_RPT = LS_TH / LS_TY, LS_THREADS = LS_TW * LS_TY;
-constexpr int LS_UW = LS_TW + 8, LS_UH = LS_TH + 2;  // u/v tile: x from x0-4, y from y0-1
-constexpr int LS_COEF_BYTES = 8 * LS_TW * LS_TH * 4, LS_UV_BYTES = LS_UW * LS_UH * 4;
-constexpr int LS_UV_STRIDE = (LS_UV_BYTES + 127) / 128 * 128;  // keeps every TMA destination 128-byte aligned
-constexpr int LS_STAGE = LS_COEF_BYTES + 2 * LS_UV_STRIDE;               // one tile: coefficients + u + v
-constexpr size_t LS_SMEM = 2 * LS_STAGE + 128 + 128;  // two stages + barriers + alignment slack
+//    'constant' 0 outside the image (the EDGE variant selects +0.0 there).
 constexpr long long LS_WAIT_LIMIT = 1ll << 22;
 
 __device__ __forceinline__ float st2(float a, float b, float wa, float wb) {
@@ -202,204 +188,283 @@ __device__ __forceinline__ float st_h(const double d[3][3], bool T, bool B, bool
   return (float)t;
 }
 
-template <bool EDGE>
-__device__ __forceinline__ void ls_strip(const float (*su)[LS_UW], const float (*sv)[LS_UW],
-                                         const float (*sc)[LS_TH][LS_TW], float* __restrict__ un,
-                                         float* __restrict__ vn, int H, int W, int pitch, float h, int x, int y0,
-                                         int r0, int tx, double& du2, double& dv2) {
-  const int c = tx + 4;  // tile column of x
-  float fu[3][3], fv[3][3];
-  double du[3][3], dv[3][3];
-#pragma unroll
-  for (int r = 0; r < 2; r++)
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      fu[r + 1][j] = su[r0 + r][c - 1 + j];
-      fv[r + 1][j] = sv[r0 + r][c - 1 + j];
-      du[r + 1][j] = (double)fu[r + 1][j];
-      dv[r + 1][j] = (double)fv[r + 1][j];
-    }
-#pragma unroll
-  for (int r = 0; r < LS_RPT; r++) {
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      fu[0][j] = fu[1][j]; fu[1][j] = fu[2][j];
-      fv[0][j] = fv[1][j]; fv[1][j] = fv[2][j];
-      du[0][j] = du[1][j]; du[1][j] = du[2][j];
-      dv[0][j] = dv[1][j]; dv[1][j] = dv[2][j];
-      fu[2][j] = su[r0 + r + 2][c - 1 + j];
-      fv[2][j] = sv[r0 + r + 2][c - 1 + j];
-      du[2][j] = (double)fu[2][j];
-      dv[2][j] = (double)fv[2][j];
-    }
-    const int y = y0 + r;
-    if (y >= H || x >= W) continue;
-    const int ly = r0 + r;
-    const bool T = y == 0, B = y == H - 1, L = x == 0, R = x == W - 1;
-    const float a = sc[0][ly][tx], b = sc[1][ly][tx], cc = sc[2][ly][tx];
-    float Du = st2(fu[0][1], fu[2][1], -0.5f, 0.5f), DTu = st2(fu[1][0], fu[1][2], -0.5f, 0.5f);
-    float Dv = st2(fv[0][1], fv[2][1], -0.5f, 0.5f), DTv = st2(fv[1][0], fv[1][2], -0.5f, 0.5f);
-    float Fu = st2(fu[0][1], fu[2][1], 1.0f, 1.0f), FTv = st2(fv[1][0], fv[1][2], 1.0f, 1.0f);
-    float Mu = st_m(du), Mv = st_m(dv);
-    float Hu = st_h<EDGE>(du, T, B, L, R), Hv = st_h<EDGE>(dv, T, B, L, R);
-    float bu = __fmul_rn(__fmul_rn(2.0f, a), Du);
-    bu = __fadd_rn(bu, __fmul_rn(a, DTv));
-    bu = __fadd_rn(bu, __fmul_rn(b, Dv));
-    bu = __fadd_rn(bu, __fmul_rn(cc, Fu));
-    bu = __fadd_rn(bu, __fmul_rn(cc, Mv));
-    bu = __fadd_rn(bu, __fmul_rn(h, Hu));
-    bu = __fadd_rn(bu, sc[3][ly][tx]);
-    float bv = __fmul_rn(b, Du);
-    bv = __fadd_rn(bv, __fmul_rn(a, DTu));
-    bv = __fadd_rn(bv, __fmul_rn(__fmul_rn(2.0f, b), DTv));
-    bv = __fadd_rn(bv, __fmul_rn(cc, Mu));
-    bv = __fadd_rn(bv, __fmul_rn(cc, FTv));
-    bv = __fadd_rn(bv, __fmul_rn(h, Hv));
-    bv = __fadd_rn(bv, sc[4][ly][tx]);
-    const float B11 = sc[5][ly][tx], B12 = sc[6][ly][tx], B22 = sc[7][ly][tx];
-    float nu = -__fadd_rn(__fmul_rn(B11, bu), __fmul_rn(B12, bv));
-    float nv = -__fadd_rn(__fmul_rn(B12, bu), __fmul_rn(B22, bv));
-    const size_t i = (size_t)y * pitch + x;
-    un[i] = nu;
-    vn[i] = nv;
-    // squared change for the stop rule, in double
-    double eu = __dadd_rn((double)nu, -du[1][1]), ev = __dadd_rn((double)nv, -dv[1][1]);
-    du2 = __fma_rn(eu, eu, du2);
-    dv2 = __fma_rn(ev, ev, dv2);
-  }
-}
+// Temporally blocked sweeps: one pass runs up to LB_T sweeps on a tile held in shared
+// memory, so the 8 coefficient planes and (u, v) cross HBM/L2 once per LB_T sweeps.
+// Tile: 24 x 64 owned pixels plus a 4-pixel halo = a 32 x 72 region, loaded by one 3-D TMA
+// (8 coefficient planes, 72 KB) and two 2-D TMAs (u, v) starting at (x0-4, y0-4): x stays
+// 16-byte aligned.  Each sweep computes every cell of the region that has its full 3x3
+// neighbourhood in the tile; after sweep s only the cells at least s+1 from the region's
+// edge are exact, so after LB_T = 4 sweeps exactly the owned 24 x 64 pixels are, and those
+// are written back.  Out-of-image cells hold their clamped ('nearest') neighbour and are
+// refreshed after every sweep; H uses 'constant' 0 through the border flags.
+// The squared change of every sweep is accumulated over owned pixels only, so each pixel is
+// counted once per sweep.  The stop rule: the last CTA of a pass finds the first sweep
+// whose error is <= tol; if that is not the pass's last sweep, the pass ran too far and the
+// rollback launch recomputes the pass from its (unchanged) input with the right count.
+constexpr int LB_T = 4, LB_TW = 24, LB_TH = 64, LB_RW = LB_TW + 2 * LB_T, LB_RH = LB_TH + 2 * LB_T;  // 32 x 72
+constexpr int LB_PLANE = LB_RW * LB_RH * 4;                  // 9216 B, a multiple of 128
+constexpr int LB_COEF_BYTES = 8 * LB_PLANE;
+constexpr size_t LB_SMEM = LB_COEF_BYTES + 4 * LB_PLANE + 128 + 128;  // coef + 2 x (u, v) + barrier + slack
+constexpr int LB_ROWS = (LB_RH + 7) / 8;                       // rows per thread (9)
 
-// One sweep, persistent: gridDim.x CTAs (one per SM) walk the tiles with a two-stage TMA
-// pipeline - while a tile is computed the next one is already in flight into the other
-// stage.  `err_flag` receives 1 if a TMA wait times out (the CTA then stops early).
-struct LsStage {
-  float (*sc)[LS_TH][LS_TW];
-  float (*su)[LS_UW];
-  float (*sv)[LS_UW];
+typedef float LbPlane[LB_RW];
+
+struct LbPass {  // per-launch description of a pass
+  int k0;        // first sweep index
+  int nsweep;    // sweeps in this pass (<= LB_T)
+  int pass;      // pass index
+  int redo;      // 1: rollback launch (sweep count read from redo[pass])
 };
 
-__device__ __forceinline__ LsStage ls_stage(unsigned char* base, int s) {
-  unsigned char* p = base + s * LS_STAGE;
-  return {reinterpret_cast<float(*)[LS_TH][LS_TW]>(p), reinterpret_cast<float(*)[LS_UW]>(p + LS_COEF_BYTES),
-          reinterpret_cast<float(*)[LS_UW]>(p + LS_COEF_BYTES + LS_UV_STRIDE)};
+__device__ __forceinline__ void lb_refresh(LbPlane* u, LbPlane* v, int x0, int y0, int H, int W, int t) {
+  for (int e = t; e < LB_RH * LB_RW; e += 256) {
+    int r = e / LB_RW, c = e - r * LB_RW;
+    int gy = y0 - LB_T + r, gx = x0 - LB_T + c;
+    if (gy >= 0 && gy < H && gx >= 0 && gx < W) continue;
+    int sy = clampi(gy, 0, H - 1) - (y0 - LB_T), sx = clampi(gx, 0, W - 1) - (x0 - LB_T);
+    if (sy < 0 || sy >= LB_RH || sx < 0 || sx >= LB_RW) continue;
+    u[r][c] = u[sy][sx];
+    v[r][c] = v[sy][sx];
+  }
 }
 
-__device__ __forceinline__ void ls_issue(const LsStage& S, uint64_t* bar, const CUtensorMap* tc, const CUtensorMap* tu,
-                                         const CUtensorMap* tv, int x0, int y0) {
-  mbar_expect_tx(bar, LS_COEF_BYTES + 2 * LS_UV_BYTES);
-  tma_load_3d(S.sc, tc, x0, y0, 0, bar);
-  tma_load_2d(S.su, tu, x0 - 4, y0 - 1, bar);
-  tma_load_2d(S.sv, tv, x0 - 4, y0 - 1, bar);
+// One row of a thread's 3x3 window: the three u, v values as float32 and float64.
+struct LbRow {
+  float fu[3], fv[3];
+  double du[3], dv[3];
+};
+
+__device__ __forceinline__ void lb_load(LbRow& R, const LbPlane* su, const LbPlane* sv, int row, int c) {
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    R.fu[j] = su[row][c - 1 + j];
+    R.fv[j] = sv[row][c - 1 + j];
+    R.du[j] = (double)R.fu[j];
+    R.dv[j] = (double)R.fv[j];
+  }
 }
 
-__global__ void __launch_bounds__(LS_THREADS, 1) ls_sweep_kernel(const __grid_constant__ CUtensorMap tm_coef,
-                                                                 const __grid_constant__ CUtensorMap tm_u,
-                                                                 const __grid_constant__ CUtensorMap tm_v,
-                                                                 float* __restrict__ un, float* __restrict__ vn, int H,
-                                                                 int W, int pitch, float h, double* ss, int* run,
-                                                                 unsigned int* done, int k, double inv_n, double tol,
-                                                                 int* err_flag) {
-  if (k > 0 && *(volatile int*)(run + k) == 0) return;  // the stop rule ended the loop earlier
-  extern __shared__ __align__(128) unsigned char ls_smem_raw[];
-  unsigned char* base = ls_smem_raw + ((128 - (smem_u32(ls_smem_raw) & 127)) & 127);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(base + 2 * LS_STAGE);
-  const int tilesx = (W + LS_TW - 1) / LS_TW, ntiles = tilesx * ((H + LS_TH - 1) / LS_TH);
+// Update of the cell (row, c) from its window rows U (above), C (centre), D (below).
+template <bool EDGE>
+__device__ __forceinline__ void lb_cell(const LbRow& U, const LbRow& C, const LbRow& D, LbPlane* du_, LbPlane* dv_,
+                                        const float* sc, int row, int c, int gx, int gy, int H, int W, float h,
+                                        bool own, double& acc_u, double& acc_v) {
+  if (EDGE && (gy < 0 || gy >= H || gx < 0 || gx >= W)) return;  // refreshed from its clamp source
+  const bool T = gy == 0, B = gy == H - 1, L = gx == 0, R = gx == W - 1;
+  const double du[3][3] = {{U.du[0], U.du[1], U.du[2]}, {C.du[0], C.du[1], C.du[2]}, {D.du[0], D.du[1], D.du[2]}};
+  const double dv[3][3] = {{U.dv[0], U.dv[1], U.dv[2]}, {C.dv[0], C.dv[1], C.dv[2]}, {D.dv[0], D.dv[1], D.dv[2]}};
+  const int o = row * LB_RW + c;
+  const int PL = LB_RW * LB_RH;
+  const float a = sc[o], b = sc[PL + o], cc = sc[2 * PL + o];
+  float Du = st2(U.fu[1], D.fu[1], -0.5f, 0.5f), DTu = st2(C.fu[0], C.fu[2], -0.5f, 0.5f);
+  float Dv = st2(U.fv[1], D.fv[1], -0.5f, 0.5f), DTv = st2(C.fv[0], C.fv[2], -0.5f, 0.5f);
+  float Fu = st2(U.fu[1], D.fu[1], 1.0f, 1.0f), FTv = st2(C.fv[0], C.fv[2], 1.0f, 1.0f);
+  float Mu = st_m(du), Mv = st_m(dv);
+  float Hu = st_h<EDGE>(du, T, B, L, R), Hv = st_h<EDGE>(dv, T, B, L, R);
+  float bu = __fmul_rn(__fmul_rn(2.0f, a), Du);
+  bu = __fadd_rn(bu, __fmul_rn(a, DTv));
+  bu = __fadd_rn(bu, __fmul_rn(b, Dv));
+  bu = __fadd_rn(bu, __fmul_rn(cc, Fu));
+  bu = __fadd_rn(bu, __fmul_rn(cc, Mv));
+  bu = __fadd_rn(bu, __fmul_rn(h, Hu));
+  bu = __fadd_rn(bu, sc[3 * PL + o]);
+  float bv = __fmul_rn(b, Du);
+  bv = __fadd_rn(bv, __fmul_rn(a, DTu));
+  bv = __fadd_rn(bv, __fmul_rn(__fmul_rn(2.0f, b), DTv));
+  bv = __fadd_rn(bv, __fmul_rn(cc, Mu));
+  bv = __fadd_rn(bv, __fmul_rn(cc, FTv));
+  bv = __fadd_rn(bv, __fmul_rn(h, Hv));
+  bv = __fadd_rn(bv, sc[4 * PL + o]);
+  const float B11 = sc[5 * PL + o], B12 = sc[6 * PL + o], B22 = sc[7 * PL + o];
+  float nu = -__fadd_rn(__fmul_rn(B11, bu), __fmul_rn(B12, bv));
+  float nv = -__fadd_rn(__fmul_rn(B12, bu), __fmul_rn(B22, bv));
+  du_[row][c] = nu;
+  dv_[row][c] = nv;
+  if (own) {
+    double eu = __dadd_rn((double)nu, -C.du[1]), ev = __dadd_rn((double)nv, -C.dv[1]);
+    acc_u = __fma_rn(eu, eu, acc_u);
+    acc_v = __fma_rn(ev, ev, acc_v);
+  }
+}
+
+// One sweep of one thread's column strip: rows [r0, r0+n) of column c (1 <= c <= RW-2).
+// The three window rows rotate through three register sets (3-row steps), so sliding the
+// window costs loads only.
+template <bool EDGE>
+__device__ __forceinline__ void lb_strip(const LbPlane* su, const LbPlane* sv, LbPlane* du_, LbPlane* dv_,
+                                         const float* sc, int c, int r0, int n, int gx, int gy0, int H, int W, float h,
+                                         bool own_col, double& acc_u, double& acc_v) {
+  LbRow A, B, C;
+  lb_load(A, su, sv, r0 - 1, c);
+  lb_load(B, su, sv, r0, c);
+#define LB_OWN(row) (own_col && (row) >= LB_T && (row) < LB_T + LB_TH)
+#pragma unroll 1
+  for (int r = 0; r < n; r += 3) {
+    const int row = r0 + r;
+    lb_load(C, su, sv, row + 1, c);
+    lb_cell<EDGE>(A, B, C, du_, dv_, sc, row, c, gx, gy0 + r, H, W, h, LB_OWN(row), acc_u, acc_v);
+    if (r + 1 < n) {
+      lb_load(A, su, sv, row + 2, c);
+      lb_cell<EDGE>(B, C, A, du_, dv_, sc, row + 1, c, gx, gy0 + r + 1, H, W, h, LB_OWN(row + 1), acc_u, acc_v);
+    }
+    if (r + 2 < n) {
+      lb_load(B, su, sv, row + 3, c);
+      lb_cell<EDGE>(C, A, B, du_, dv_, sc, row + 2, c, gx, gy0 + r + 2, H, W, h, LB_OWN(row + 2), acc_u, acc_v);
+    }
+  }
+#undef LB_OWN
+}
+
+__global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__ CUtensorMap tm_coef,
+                                                         const __grid_constant__ CUtensorMap tm_u,
+                                                         const __grid_constant__ CUtensorMap tm_v,
+                                                         float* __restrict__ un, float* __restrict__ vn, int H, int W,
+                                                         int pitch, float h, LbPass P, LsCtrl* ctrl, double* ss,
+                                                         int* run, unsigned int* done, int* redo, double inv_n,
+                                                         double tol, int* err_flag, int final_buf) {
+  int nsw = P.nsweep;
+  if (P.redo) {
+    nsw = *(volatile int*)(redo + P.pass);
+    if (nsw == 0) return;
+  } else if (P.k0 > 0 && *(volatile int*)(run + P.k0) == 0) {
+    return;  // the stop rule ended the loop in an earlier pass
+  }
+  extern __shared__ __align__(128) unsigned char lb_smem_raw[];
+  unsigned char* base = lb_smem_raw + ((128 - (smem_u32(lb_smem_raw) & 127)) & 127);
+  const float* sc = reinterpret_cast<const float*>(base);
+  // ping-pong buffer q: u at base + COEF + 2q planes, v right after it
+#define LB_U(q) reinterpret_cast<LbPlane*>(base + LB_COEF_BYTES + (2 * (q)) * LB_PLANE)
+#define LB_V(q) reinterpret_cast<LbPlane*>(base + LB_COEF_BYTES + (2 * (q) + 1) * LB_PLANE)
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + LB_COEF_BYTES + 4 * LB_PLANE);
+  const int x0 = blockIdx.x * LB_TW, y0 = blockIdx.y * LB_TH;
   const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  if (t == 0) mbar_init(bar, 1);
+  __syncthreads();
   if (t == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    mbar_expect_tx(bar, LB_COEF_BYTES + 2 * LB_PLANE);
+    tma_load_3d((void*)sc, &tm_coef, x0 - LB_T, y0 - LB_T, 0, bar);
+    tma_load_2d(LB_U(0), &tm_u, x0 - LB_T, y0 - LB_T, bar);
+    tma_load_2d(LB_V(0), &tm_v, x0 - LB_T, y0 - LB_T, bar);
+  }
+  if (!mbar_wait(bar, 0, LS_WAIT_LIMIT)) {
+    if (t == 0) atomicExch(err_flag, 1);
+    mbar_wait(bar, 0, LS_WAIT_LIMIT);  // one more bounded wait for the copies in flight
+    nsw = 0;
+  }
+  const bool edge = x0 < LB_T || y0 < LB_T || x0 + LB_TW + LB_T > W || y0 + LB_TH + LB_T > H;
+  if (edge) {
+    __syncthreads();
+    lb_refresh(LB_U(0), LB_V(0), x0, y0, H, W, t);
   }
   __syncthreads();
-  int tile = blockIdx.x;
-  if (t == 0 && tile < ntiles) ls_issue(ls_stage(base, 0), &bar[0], &tm_coef, &tm_u, &tm_v, (tile % tilesx) * LS_TW,
-                                        (tile / tilesx) * LS_TH);
-  double du2 = 0.0, dv2 = 0.0;
-  for (int i = 0; tile < ntiles; i++, tile += gridDim.x) {
-    const int s = i & 1;
-    const int next = tile + gridDim.x;
-    if (t == 0 && next < ntiles)  // the other stage was released by the barrier that ended iteration i-1
-      ls_issue(ls_stage(base, s ^ 1), &bar[s ^ 1], &tm_coef, &tm_u, &tm_v, (next % tilesx) * LS_TW,
-               (next / tilesx) * LS_TH);
-    const LsStage S = ls_stage(base, s);
-    if (!mbar_wait(&bar[s], (i >> 1) & 1, LS_WAIT_LIMIT)) {
-      if (t == 0) atomicExch(err_flag, 1);
-      mbar_wait(&bar[s], (i >> 1) & 1, LS_WAIT_LIMIT);  // one more bounded wait for the copies in flight
-      if (next < ntiles) mbar_wait(&bar[s ^ 1], ((i + 1) >> 1) & 1, LS_WAIT_LIMIT);
-      break;
+  const int c = threadIdx.x;  // region column
+  const int gx = x0 - LB_T + c;
+  const bool own_col = c >= LB_T && c < LB_T + LB_TW;
+  int r0 = threadIdx.y * LB_ROWS, r1 = r0 + LB_ROWS;
+  if (r0 < 1) r0 = 1;
+  if (r1 > LB_RH - 1) r1 = LB_RH - 1;
+  __shared__ double red[LB_T][2][8];
+#pragma unroll 1
+  for (int s = 0; s < nsw; s++) {
+    const int in = s & 1, out = in ^ 1;
+    double au = 0.0, av = 0.0;
+    if (c >= 1 && c <= LB_RW - 2 && r1 > r0) {
+      if (edge)
+        lb_strip<true>(LB_U(in), LB_V(in), LB_U(out), LB_V(out), sc, c, r0, r1 - r0, gx, y0 - LB_T + r0, H, W, h,
+                       own_col, au, av);
+      else
+        lb_strip<false>(LB_U(in), LB_V(in), LB_U(out), LB_V(out), sc, c, r0, r1 - r0, gx, y0 - LB_T + r0, H, W,
+                        h, own_col, au, av);
     }
-    const int x0 = (tile % tilesx) * LS_TW, y0 = (tile / tilesx) * LS_TH;
-    const bool edge = x0 == 0 || y0 == 0 || x0 + LS_TW >= W || y0 + LS_TH >= H;
-    if (edge) {
-      // out-of-image cells of the u/v halo tiles take their clamped ('nearest') value
-      for (int e = t; e < LS_UH * LS_UW; e += LS_THREADS) {
-        int r = e / LS_UW, cl = e - r * LS_UW;
-        int gy = y0 - 1 + r, gx = x0 - 4 + cl;
-        if (gy >= 0 && gy < H && gx >= 0 && gx < W) continue;
-        int cy = clampi(gy, 0, H - 1) - (y0 - 1), cx = clampi(gx, 0, W - 1) - (x0 - 4);
-        if (cy < 0 || cy >= LS_UH || cx < 0 || cx >= LS_UW) continue;  // cell outside every stencil
-        S.su[r][cl] = S.su[cy][cx];
-        S.sv[r][cl] = S.sv[cy][cx];
+    if (!P.redo) {
+      for (int o = 16; o > 0; o >>= 1) {
+        au += __shfl_down_sync(0xffffffffu, au, o);
+        av += __shfl_down_sync(0xffffffffu, av, o);
       }
+      if ((t & 31) == 0) {
+        red[s][0][t >> 5] = au;
+        red[s][1][t >> 5] = av;
+      }
+    }
+    __syncthreads();
+    if (edge) {
+      lb_refresh(LB_U(out), LB_V(out), x0, y0, H, W, t);
       __syncthreads();
     }
-    const int x = x0 + threadIdx.x, r0 = threadIdx.y * LS_RPT, ys = y0 + r0;
-    if (edge)
-      ls_strip<true>(S.su, S.sv, S.sc, un, vn, H, W, pitch, h, x, ys, r0, threadIdx.x, du2, dv2);
-    else
-      ls_strip<false>(S.su, S.sv, S.sc, un, vn, H, W, pitch, h, x, ys, r0, threadIdx.x, du2, dv2);
-    __syncthreads();  // stage s is free for the load issued at iteration i+1
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    du2 += __shfl_down_sync(0xffffffffu, du2, o);
-    dv2 += __shfl_down_sync(0xffffffffu, dv2, o);
-  }
-  __shared__ double ru[LS_THREADS / 32], rv[LS_THREADS / 32];
-  if ((t & 31) == 0) {
-    ru[t >> 5] = du2;
-    rv[t >> 5] = dv2;
-  }
-  __syncthreads();
-  if (t == 0) {
-    for (int w = 1; w < LS_THREADS / 32; w++) {
-      du2 += ru[w];
-      dv2 += rv[w];
+  // owned pixels of the last sweep -> global
+  if (nsw > 0) {
+    const LbPlane* fu = LB_U(nsw & 1);
+    const LbPlane* fv = LB_V(nsw & 1);
+    for (int e = t; e < LB_TW * LB_TH; e += 256) {
+      int r = e / LB_TW, cl = e - r * LB_TW;
+      int y = y0 + r, x = x0 + cl;
+      if (y < H && x < W) {
+        size_t i = (size_t)y * pitch + x;
+        un[i] = fu[r + LB_T][cl + LB_T];
+        vn[i] = fv[r + LB_T][cl + LB_T];
+      }
     }
-    atomicAdd(ss + 2 * k, du2);
-    atomicAdd(ss + 2 * k + 1, dv2);
+  }
+  if (P.redo) return;
+  // per-sweep squared changes -> ss[k0 + s]; the last CTA applies the stop rule
+  if (t == 0) {
+    for (int s = 0; s < nsw; s++) {
+      double a = 0.0, b = 0.0;
+      for (int w = 0; w < 8; w++) {
+        a += red[s][0][w];
+        b += red[s][1][w];
+      }
+      atomicAdd(ss + 2 * (P.k0 + s), a);
+      atomicAdd(ss + 2 * (P.k0 + s) + 1, b);
+    }
     __threadfence();
-    if (atomicAdd(done + k, 1u) == gridDim.x - 1) {  // last CTA of this sweep decides the next one
+    if (atomicAdd(done + P.pass, 1u) == gridDim.x * gridDim.y - 1) {
       __threadfence();
-      double s0 = atomicAdd(ss + 2 * k, 0.0), s1 = atomicAdd(ss + 2 * k + 1, 0.0);
-      double e = (sqrt(s0) + sqrt(s1)) * inv_n;
-      run[k + 1] = (e > tol) ? 1 : 0;
+      int stop = -1;
+      for (int s = 0; s < nsw; s++) {
+        double s0 = atomicAdd(ss + 2 * (P.k0 + s), 0.0), s1 = atomicAdd(ss + 2 * (P.k0 + s) + 1, 0.0);
+        if (!((sqrt(s0) + sqrt(s1)) * inv_n > tol)) {
+          stop = s;
+          break;
+        }
+      }
+      if (stop < 0) {
+        run[P.k0 + nsw] = 1;
+        ctrl->K = P.k0 + nsw;
+      } else {
+        run[P.k0 + nsw] = 0;
+        ctrl->K = P.k0 + stop + 1;
+        redo[P.pass] = (stop < nsw - 1) ? stop + 1 : 0;
+      }
+      ctrl->final_buf = final_buf;
     }
   }
 }
 
-__global__ void ls_count_kernel(LsCtrl* ctrl, const int* run, const double* ss, int maxnum, double inv_n,
-                                const int* err_flag, int* iters_out, double* err_out) {
-  int K = maxnum;
-  for (int k = 1; k < maxnum; k++)
-    if (!run[k]) {
-      K = k;
-      break;
-    }
-  ctrl->K = K;
+#undef LB_U
+#undef LB_V
+
+// Sweeps run (and the last sweep's error); a TMA wait timeout in any pass is reported as
+// iters = -1, err = NaN.
+__global__ void ls_count_kernel(LsCtrl* ctrl, const double* ss, double inv_n, const int* err_flag, int* iters_out,
+                                double* err_out) {
+  int K = ctrl->K;
   bool failed = *err_flag != 0;
   if (iters_out) *iters_out = failed ? -1 : K;
   if (err_out) *err_out = failed ? __longlong_as_double(0x7ff8000000000000ll) : (K > 0 ? ls_err(ss, K - 1, inv_n) : 0.0);
 }
 
-// Result of the last sweep (buffer K mod 2) -> caller's V (row component) and U.
+// Result (ping-pong buffer ctrl->final_buf) -> caller's V (row component) and U.
 __global__ void ls_finalize_kernel(const float* __restrict__ u0, const float* __restrict__ v0,
                                    const float* __restrict__ u1, const float* __restrict__ v1, float* __restrict__ V,
                                    float* __restrict__ U, int W, int sp, int dp, const LsCtrl* ctrl) {
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
   if (x >= W) return;
-  const bool odd = ctrl->K & 1;
+  const bool one = ctrl->final_buf & 1;
   size_t i = (size_t)y * sp + x, o = (size_t)y * dp + x;
-  V[o] = odd ? u1[i] : u0[i];
-  U[o] = odd ? v1[i] : v0[i];
+  V[o] = one ? u1[i] : u0[i];
+  U[o] = one ? v1[i] : v0[i];
 }
 
 }  // namespace ofb
@@ -424,7 +489,8 @@ extern "C" size_t of_ls_workspace_size(int H, int W, int pitch, int maxnum) {
   s.take<float>(4 * N);  // u0, v0, u1, v1
   s.take<LsCtrl>(1);
   s.take<int>((size_t)maxnum + 2);  // run[] and the TMA error flag
-  s.take<unsigned int>((size_t)maxnum + 1);
+  s.take<unsigned int>((size_t)maxnum + 1);  // done[] per pass
+  s.take<int>((size_t)maxnum + 1);           // redo[] per pass
   s.take<double>(2 * (size_t)(maxnum > 0 ? maxnum : 1));
   return s.off;
 }
@@ -447,20 +513,22 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   LsCtrl* ctrl = c.take<LsCtrl>(1);
   int* run = c.take<int>((size_t)maxnum + 2);
   unsigned int* done = c.take<unsigned int>((size_t)maxnum + 1);
+  int* redo = c.take<int>((size_t)maxnum + 1);
   double* ss = c.take<double>(2 * (size_t)(maxnum > 0 ? maxnum : 1));
   int* err_flag = run + maxnum + 1;
   float *n1 = nrm, *n2 = nrm + N, *et = nrm + 2 * N;
   float* ub[2] = {uv, uv + 2 * N};
   float* vb[2] = {uv + N, uv + 3 * N};
-  // tensor maps: 8 coefficient planes (3-D) and the four u / v planes (2-D)
+  // tensor maps over the whole solve: the 8 coefficient planes (3-D) and the four u / v
+  // planes (2-D), all with the 32 x 72 region box of a pass
   CUtensorMap tm_coef, tm_u[2], tm_v[2];
   {
     uint64_t d3[3] = {(uint64_t)W, (uint64_t)H, 8}, s3[2] = {(uint64_t)P * 4, (uint64_t)N * 4};
-    uint32_t b3[3] = {LS_TW, LS_TH, 8};
+    uint32_t b3[3] = {LB_RW, LB_RH, 8};
     int rc = tmap_f32(&tm_coef, coef, 3, d3, s3, b3);
     if (rc) return rc;
     uint64_t d2[2] = {(uint64_t)W, (uint64_t)H}, s2[1] = {(uint64_t)P * 4};
-    uint32_t b2[2] = {LS_UW, LS_UH};
+    uint32_t b2[2] = {LB_RW, LB_RH};
     for (int q = 0; q < 2; q++) {
       if ((rc = tmap_f32(&tm_u[q], ub[q], 2, d2, s2, b2))) return rc;
       if ((rc = tmap_f32(&tm_v[q], vb[q], 2, d2, s2, b2))) return rc;
@@ -468,10 +536,10 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   }
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(ls_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LS_SMEM);
+    cudaFuncSetAttribute(ls_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LB_SMEM);
     attr = true;
   }
-  // control block, flags, counters and sums are contiguous: one memset clears them
+  // control block, flags, counters, redo counts and sums are contiguous: one memset
   cudaMemsetAsync(ctrl, 0, (size_t)((char*)(ss + 2 * (size_t)(maxnum > 0 ? maxnum : 1)) - (char*)ctrl), st);
   dim3 mg((W + 255) / 256 < 8 ? (W + 255) / 256 : 8, H < 512 ? H : 512);
   ls_max_kernel<<<mg, 256, 0, st>>>(I0, I1, H, W, pitch, ctrl->maxkey);
@@ -481,15 +549,20 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   ls_coef_kernel<<<grd, blk, 0, st>>>(n1, et, coef, N, H, W, P, h);
   ls_copy2_kernel<<<rg, 256, 0, st>>>(V, U, ub[0], vb[0], W, pitch, P, nullptr);
   double inv_n = 1.0 / ((double)H * (double)W);
-  int ntiles = ((W + LS_TW - 1) / LS_TW) * ((H + LS_TH - 1) / LS_TH);
-  int sgrd = ntiles < kNumSMs ? ntiles : kNumSMs;
-  dim3 sblk(LS_TW, LS_TY);
-  for (int k = 0; k < maxnum; k++) {
-    int s = k & 1;
-    ls_sweep_kernel<<<sgrd, sblk, LS_SMEM, st>>>(tm_coef, tm_u[s], tm_v[s], ub[s ^ 1], vb[s ^ 1], H, W, P, h, ss, run,
-                                                done, k, inv_n, tol, err_flag);
+  dim3 pgrd((W + LB_TW - 1) / LB_TW, (H + LB_TH - 1) / LB_TH), pblk(32, 8);
+  long long nl = 5;
+  for (int k0 = 0, p = 0; k0 < maxnum; k0 += LB_T, p++) {
+    const int in = p & 1, out = in ^ 1;
+    LbPass P0{k0, maxnum - k0 < LB_T ? maxnum - k0 : LB_T, p, 0};
+    ls_pass_kernel<<<pgrd, pblk, LB_SMEM, st>>>(tm_coef, tm_u[in], tm_v[in], ub[out], vb[out], H, W, P, h, P0, ctrl, ss,
+                                               run, done, redo, inv_n, tol, err_flag, out);
+    LbPass P1 = P0;
+    P1.redo = 1;  // rollback: recompute this pass with the sweep count the stop rule chose
+    ls_pass_kernel<<<pgrd, pblk, LB_SMEM, st>>>(tm_coef, tm_u[in], tm_v[in], ub[out], vb[out], H, W, P, h, P1, ctrl, ss,
+                                               run, done, redo, inv_n, tol, err_flag, out);
+    nl += 2;
   }
-  ls_count_kernel<<<1, 1, 0, st>>>(ctrl, run, ss, maxnum, inv_n, err_flag, iters_out, err_out);
+  ls_count_kernel<<<1, 1, 0, st>>>(ctrl, ss, inv_n, err_flag, iters_out, err_out);
   ls_finalize_kernel<<<rg, 256, 0, st>>>(ub[0], vb[0], ub[1], vb[1], V, U, W, P, pitch, ctrl);
-  return check_launch("of_ls_solve", 6 + (long long)maxnum);
+  return check_launch("of_ls_solve", nl + 1);
 }
