@@ -14,7 +14,8 @@
  *    least the size returned by the matching *_workspace_size() call; they never
  *    allocate.  Distinct streams need distinct workspaces.
  *  - No C++ exception crosses this boundary.  The library holds no state besides the
- *    per-thread error message.
+ *    per-thread error message, a launch counter and the fixed scratch array of
+ *    of_ls_solve_noalloc.
  *
  * Each declaration names the reference interface it replaces (OpticalFlow-RI,
  * file:line).
@@ -133,6 +134,19 @@ size_t of_ls_workspace_size(int H, int W, int pitch, int maxnum);
 int of_ls_coefficients(const float* I1n, const float* Et, float* coef, int H, int W, int pitch, float h, void* stream);
 int of_ls_solve(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float h, int maxnum,
                 double tol, int* iters_out, double* err_out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* The same Liu-Shen solve for callers that cannot allocate device memory at call time
+ * (a framework that owns all allocations, a plugin that must not touch the process's
+ * allocator, a real-time loop that cannot afford cudaMalloc's synchronisation).  It has no
+ * counterpart in the reference.  Its scratch is a fixed OF_LS_NOALLOC_SCRATCH_BYTES array
+ * inside the library (held by every GPU that loads it), so it takes no workspace and
+ * rejects, with OF_ERR_INVALID, any size whose of_ls_workspace_size exceeds that array
+ * (256 x 256 with 60 sweeps fits).  The first call on each device looks up the array's
+ * device address; make it before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race.  Results equal of_ls_solve's. */
+#define OF_LS_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
+int of_ls_solve_noalloc(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float h,
+                        int maxnum, double tol, int* iters_out, double* err_out, void* stream);
 
 /* ---------------------------------------------------------------------------------
  * A10/A11 dense Lucas-Kanade — replaces denseLucasKanade_PyCl.compute

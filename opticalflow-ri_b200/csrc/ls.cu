@@ -566,3 +566,66 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   ls_finalize_kernel<<<rg, 256, 0, st>>>(ub[0], vb[0], ub[1], vb[1], V, U, W, P, pitch, ctrl);
   return check_launch("of_ls_solve", nl + 1);
 }
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free Liu-Shen solve.
+//
+// Some callers cannot allocate device memory when they run the solver: a host framework
+// that owns every allocation through its own pool, a plugin loaded into a process whose
+// allocator must not be touched, or a real-time loop where cudaMalloc's implicit device
+// synchronisation is not allowed.  This variant needs no workspace argument: its scratch
+// is a fixed array compiled into the library (OF_LS_NOALLOC_SCRATCH_BYTES, 4 MiB), which
+// every GPU that loads the library holds until the process exits.  That bounds the image:
+// of_ls_workspace_size(H, W, pitch, maxnum) must not exceed the array (256 x 256 with the
+// reference's 60 sweeps fits).
+//
+// Host code cannot pass the array's name to a kernel (on the host it only stands for the
+// symbol), so the first call on each device looks up its device address with
+// cudaGetSymbolAddress while that device is current and caches it; make that first call
+// before capturing any stream.  All calls share the one array and it keeps the previous
+// call's contents; the solver clears its control words itself.  Calls that overlap on the
+// GPU (other streams, other host threads) race on the array.
+// ---------------------------------------------------------------------------------------
+#include <mutex>
+
+static __device__ __align__(256) unsigned char g_ls_noalloc_scratch[OF_LS_NOALLOC_SCRATCH_BYTES];
+
+static void* ls_noalloc_scratch_ptr(int* rc) {
+  static std::mutex mu;
+  static void* ptrs[64] = {nullptr};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    *rc = set_error(OF_ERR_CUDA, "of_ls_solve_noalloc: cudaGetDevice failed (%s)", cudaGetErrorString(e));
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_ls_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      *rc = set_error(OF_ERR_CUDA, "of_ls_solve_noalloc: cudaGetSymbolAddress failed (%s)", cudaGetErrorString(e));
+      return nullptr;
+    }
+    ptrs[dev] = p;
+  }
+  *rc = OF_OK;
+  return ptrs[dev];
+}
+
+extern "C" int of_ls_solve_noalloc(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch,
+                                   float h, int maxnum, double tol, int* iters_out, double* err_out, void* stream) {
+  OF_REQUIRE(!bad_plane(I0, H, W, pitch) && I1 && U && V, "of_ls_solve_noalloc: bad plane");
+  OF_REQUIRE(maxnum >= 0 && maxnum <= 100000, "of_ls_solve_noalloc: maxnum out of range");
+  size_t need = of_ls_workspace_size(H, W, pitch, maxnum);
+  if (need > (size_t)OF_LS_NOALLOC_SCRATCH_BYTES)
+    return set_error(OF_ERR_INVALID,
+                     "of_ls_solve_noalloc: a %d x %d solve with %d sweeps needs %zu bytes of scratch, more than the "
+                     "library's fixed %d-byte array; use of_ls_solve with a workspace",
+                     H, W, maxnum, need, OF_LS_NOALLOC_SCRATCH_BYTES);
+  int rc = OF_OK;
+  void* scratch = ls_noalloc_scratch_ptr(&rc);
+  if (!scratch) return rc;
+  return of_ls_solve(I0, I1, U, V, H, W, pitch, h, maxnum, tol, iters_out, err_out, scratch,
+                     (size_t)OF_LS_NOALLOC_SCRATCH_BYTES, stream);
+}

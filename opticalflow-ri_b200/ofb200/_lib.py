@@ -55,6 +55,7 @@ _SIGS = {
     "of_hs_solve": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _P, _P, _Z, _P], _I),
     "of_ls_workspace_size": ([_I, _I, _I, _I], _Z),
     "of_ls_solve": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P, _Z, _P], _I),
+    "of_ls_solve_noalloc": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P], _I),
     "of_lk_dense": ([_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P], _I),
     "of_fb_blur": ([_P, _P, _I, _I, _I, _I, _P, _I, _P], _I),
     "of_fb_box5": ([_P, _P, _I, _I, _I, _I, _P], _I),
