@@ -46,7 +46,17 @@ __global__ void ls_max_kernel(const float* __restrict__ a, const float* __restri
     ka = max(ka, __shfl_down_sync(0xffffffffu, ka, o));
     kb = max(kb, __shfl_down_sync(0xffffffffu, kb, o));
   }
+  __shared__ unsigned int ra[8], rb[8];
   if ((threadIdx.x & 31) == 0) {
+    ra[threadIdx.x >> 5] = ka;
+    rb[threadIdx.x >> 5] = kb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {  // one atomic per block
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+      ka = max(ka, ra[w]);
+      kb = max(kb, rb[w]);
+    }
     atomicMax(keys, ka);
     atomicMax(keys + 1, kb);
   }
@@ -541,7 +551,7 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   }
   // control block, flags, counters, redo counts and sums are contiguous: one memset
   cudaMemsetAsync(ctrl, 0, (size_t)((char*)(ss + 2 * (size_t)(maxnum > 0 ? maxnum : 1)) - (char*)ctrl), st);
-  dim3 mg((W + 255) / 256 < 8 ? (W + 255) / 256 : 8, H < 512 ? H : 512);
+  dim3 mg((W + 255) / 256 < 2 ? (W + 255) / 256 : 2, H < 148 ? H : 148);
   ls_max_kernel<<<mg, 256, 0, st>>>(I0, I1, H, W, pitch, ctrl->maxkey);
   dim3 rg((W + 255) / 256, H);
   ls_normalize_kernel<<<rg, 256, 0, st>>>(I0, I1, ctrl->maxkey, n1, n2, et, W, pitch, P);

@@ -101,14 +101,45 @@ static int ksize_of(int in, int out, int bicubic) {
 }
 
 // ----------------------------------------------------------------------------- spline
+// Reciprocal pivots of the constant (1, 4, 1) tridiagonal elimination, shared by every
+// line: c[0] = 1/4, c[r] = 1/(4 - c[r-1]) until the fixed point (2 - sqrt 3) repeats in
+// double.  One thread runs the short division chain (about 20 steps); the block fills the
+// constant tail.
+__global__ void spline_recip_kernel(double* c, int m) {
+  __shared__ double tail;
+  __shared__ int rc;
+  if (threadIdx.x == 0) {
+    int r = 0;
+    double v = 0.0;
+    if (m > 0) {
+      v = __ddiv_rn(1.0, 4.0);
+      c[0] = v;
+      for (r = 1; r < m; r++) {
+        double nv = __ddiv_rn(1.0, __dadd_rn(4.0, -v));
+        c[r] = nv;
+        if (nv == v) break;
+        v = nv;
+      }
+    }
+    tail = v;
+    rc = r;
+  }
+  __syncthreads();
+  for (int r = rc + 1 + threadIdx.x; r < m; r += blockDim.x) c[r] = tail;
+}
+
 // Thomas-algorithm moments of the not-a-knot spline through n >= 4 samples with unit
-// spacing; sample i of the line is y[i*ls]; moments and scratch use the same stride.
-// The recurrences carry their previous terms in registers (the line data is the only
-// memory traffic), so one line costs O(n) dependent double operations, not O(n) memory
-// round trips.
-__device__ void nak_moments(const double* __restrict__ y, size_t ls, double* __restrict__ M, double* __restrict__ cp,
-                            double* __restrict__ dp, int n) {
-#define YV(i) y[(size_t)(i) * ls]
+// spacing; sample i of the line is y[i*ys] (float or double), moment and scratch i are
+// M[i*ls] and dp[i*ls] (double).  The elimination multiplies by the shared pivots, so a
+// step is one add and one multiply.  Each line is one thread, and the recurrence is
+// serial; samples, pivots and scratch are fetched NAK_CH steps ahead into registers so a
+// chunk of steps waits on one memory latency instead of one per step.  Lanes of a warp
+// hold neighbouring lines (stride-1 in memory), so each chunk load is coalesced.
+#define NAK_CH 32
+template <typename TY>
+__device__ void nak_moments(const TY* __restrict__ y, size_t ys, size_t ls, double* __restrict__ M,
+                            const double* __restrict__ cp, double* __restrict__ dp, int n) {
+#define YV(i) ((double)y[(size_t)(i) * ys])
 #define MV(i) M[(size_t)(i) * ls]
   double M1 = __dadd_rn(__dadd_rn(YV(2), -__dmul_rn(2.0, YV(1))), YV(0));
   double Ml = __dadd_rn(__dadd_rn(YV(n - 1), -__dmul_rn(2.0, YV(n - 2))), YV(n - 3));
@@ -117,35 +148,50 @@ __device__ void nak_moments(const double* __restrict__ y, size_t ls, double* __r
   double M2 = Ml, M3 = Ml;  // M[2], M[n-3] for the end conditions
   int m = n - 4;
   if (m > 0) {
-    double ym = YV(1), y0 = YV(2), cprev = 0.0, dprev = 0.0;
-    for (int r = 0; r < m; r++) {
-      int i = r + 2;
-      double yp = YV(i + 1);
-      double rhs = __dmul_rn(6.0, __dadd_rn(__dadd_rn(yp, -__dmul_rn(2.0, y0)), ym));
-      if (r == 0) rhs = __dadd_rn(rhs, -M1);
-      if (r == m - 1) rhs = __dadd_rn(rhs, -Ml);
-      double c, d;
-      if (r == 0) {
-        c = __ddiv_rn(1.0, 4.0);
-        d = __ddiv_rn(rhs, 4.0);
-      } else {
-        double den = __dadd_rn(4.0, -cprev);
-        c = __ddiv_rn(1.0, den);
-        d = __ddiv_rn(__dadd_rn(rhs, -dprev), den);
+    double ym = YV(1), y0 = YV(2), dprev = 0.0;
+    for (int r0 = 0; r0 < m; r0 += NAK_CH) {
+      double yb[NAK_CH], cb[NAK_CH];
+#pragma unroll
+      for (int j = 0; j < NAK_CH; j++) {
+        bool in = r0 + j < m;
+        yb[j] = in ? YV(r0 + j + 3) : 0.0;
+        cb[j] = in ? cp[r0 + j] : 0.0;
       }
-      cp[(size_t)r * ls] = c;
-      dp[(size_t)r * ls] = d;
-      cprev = c;
-      dprev = d;
-      ym = y0;
-      y0 = yp;
+#pragma unroll
+      for (int j = 0; j < NAK_CH; j++) {
+        int r = r0 + j;
+        if (r < m) {
+          double yp = yb[j];
+          double rhs = __dmul_rn(6.0, __dadd_rn(__dadd_rn(yp, -__dmul_rn(2.0, y0)), ym));
+          if (r == 0) rhs = __dadd_rn(rhs, -M1);
+          if (r == m - 1) rhs = __dadd_rn(rhs, -Ml);
+          double d = (r == 0) ? __dmul_rn(rhs, cb[j]) : __dmul_rn(__dadd_rn(rhs, -dprev), cb[j]);
+          dp[(size_t)r * ls] = d;
+          dprev = d;
+          ym = y0;
+          y0 = yp;
+        }
+      }
     }
     double next = dprev;
     MV(m + 1) = next;
     M3 = next;  // M[n-3] = M[m+1]
-    for (int r = m - 2; r >= 0; r--) {
-      next = __dadd_rn(dp[(size_t)r * ls], -__dmul_rn(cp[(size_t)r * ls], next));
-      MV(r + 2) = next;
+    for (int r1 = m - 2; r1 >= 0; r1 -= NAK_CH) {
+      double db[NAK_CH], cb[NAK_CH];
+#pragma unroll
+      for (int j = 0; j < NAK_CH; j++) {
+        int r = r1 - j;
+        db[j] = r >= 0 ? dp[(size_t)r * ls] : 0.0;
+        cb[j] = r >= 0 ? cp[r] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < NAK_CH; j++) {
+        int r = r1 - j;
+        if (r >= 0) {
+          next = __dadd_rn(db[j], -__dmul_rn(cb[j], next));
+          MV(r + 2) = next;
+        }
+      }
     }
     M2 = next;  // M[2]
   } else {
@@ -177,47 +223,92 @@ __device__ __forceinline__ void fine_index(int j, int N, int n, int* i, double* 
   *t = __dadd_rn(s, -(double)k);
 }
 
-// moments along y for each coarse column x
-__global__ void spline_my_kernel(const float* __restrict__ src, int sp, int h, int w, double* M, double* Y0,
-                                 double* S) {
+// moments along y for each coarse column x, read straight from the float field (pitch sp)
+__global__ void __launch_bounds__(128) spline_my_kernel(const float* __restrict__ src, int sp, int h, int w,
+                                                        double* M, double* S, const double* __restrict__ cp) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= w) return;
-  // the column (pitch sp) is copied into Y0, laid out [i][x] like the moments and scratch
-  for (int i = 0; i < h; i++) Y0[(size_t)i * w + x] = (double)src[(size_t)i * sp + x];
-  nak_moments(Y0 + x, w, M + x, S + x, S + (size_t)h * w + x, h);
+  // moments and scratch are laid out [i][x] with stride w
+  nak_moments<float>(src + x, (size_t)sp, (size_t)w, M + x, cp, S + x, h);
 }
 
-// T[Y][x] = column spline at fine row Y
-__global__ void spline_ey_kernel(const double* __restrict__ Y0, const double* __restrict__ M, double* __restrict__ T,
-                                 int h, int w, int H) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y;
-  if (x >= w) return;
-  int i;
-  double t;
-  fine_index(Y, H, h, &i, &t);
-  T[(size_t)Y * w + x] =
-      nak_eval(Y0[(size_t)i * w + x], Y0[(size_t)(i + 1) * w + x], M[(size_t)i * w + x], M[(size_t)(i + 1) * w + x], t);
+// Tt[x][Y] = column spline of coarse column x at fine row Y.  A 32x32 tile goes through
+// shared memory so the reads (along x) and the transposed writes (along Y) both coalesce.
+__global__ void __launch_bounds__(256) spline_ey_kernel(const float* __restrict__ src, int sp,
+                                                        const double* __restrict__ M, double* __restrict__ Tt,
+                                                        int h, int w, int H) {
+  __shared__ double tile[32][33];
+  int x0 = blockIdx.x * 32, Y0 = blockIdx.y * 32;
+  int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int k = ty; k < 32; k += 8) {
+    int Y = Y0 + k, x = x0 + tx;
+    if (Y < H && x < w) {
+      int i;
+      double t;
+      fine_index(Y, H, h, &i, &t);
+      tile[k][tx] = nak_eval((double)src[(size_t)i * sp + x], (double)src[(size_t)(i + 1) * sp + x],
+                             M[(size_t)i * w + x], M[(size_t)(i + 1) * w + x], t);
+    }
+  }
+  __syncthreads();
+  for (int k = ty; k < 32; k += 8) {
+    int x = x0 + k, Y = Y0 + tx;
+    if (x < w && Y < H) Tt[(size_t)x * H + Y] = tile[tx][k];
+  }
 }
 
-// moments along x for each fine row Y of T (layout [k][Y], stride H)
-__global__ void spline_mx_kernel(const double* __restrict__ T, int w, int H, double* M, double* cp, double* dp,
-                                 double* Tt) {
+// moments along x for each fine row Y of Tt (layout [k][Y], stride H)
+__global__ void __launch_bounds__(128) spline_mx_kernel(const double* __restrict__ Tt, int w, int H, double* M,
+                                                        const double* __restrict__ cp, double* dp) {
   int Y = blockIdx.x * blockDim.x + threadIdx.x;
   if (Y >= H) return;
-  for (int k = 0; k < w; k++) Tt[(size_t)k * H + Y] = T[(size_t)Y * w + k];
-  nak_moments(Tt + Y, H, M + Y, cp + Y, dp + Y, w);
+  nak_moments<double>(Tt + Y, (size_t)H, (size_t)H, M + Y, cp, dp + Y, w);
 }
 
-__global__ void spline_ex_kernel(const double* __restrict__ Tt, const double* __restrict__ M, float* __restrict__ dst,
-                                 int dpitch, int w, int H, int W, float scale) {
-  int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y;
+// dst[Y][X] = row spline of fine row Y at fine column X (times scale).  The coarse
+// samples and moments a 32x32 output tile needs (columns i..i+1 of Tt/M for each X, all
+// along Y) are staged through shared memory with loads that coalesce along Y.
+#define EX_SPAN 40
+__global__ void __launch_bounds__(256) spline_ex_kernel(const double* __restrict__ Tt, const double* __restrict__ M,
+                                                        float* __restrict__ dst, int dpitch, int w, int H, int W,
+                                                        float scale) {
+  __shared__ double sT[EX_SPAN][33], sM[EX_SPAN][33];
+  int X0 = blockIdx.x * 32, Y0 = blockIdx.y * 32;
+  int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  int Xl = min(X0 + 31, W - 1);
+  int ilo, ihi;
+  double tt;
+  fine_index(X0, W, w, &ilo, &tt);
+  fine_index(Xl, W, w, &ihi, &tt);
+  ihi += 1;  // the interval's right sample
+  bool staged = ihi - ilo + 1 <= EX_SPAN;  // false only for strong downsampling
+  if (staged) {
+    for (int k = ty; k <= ihi - ilo; k += 8) {
+      int Y = Y0 + tx;
+      if (Y < H) {
+        sT[k][tx] = Tt[(size_t)(ilo + k) * H + Y];
+        sM[k][tx] = M[(size_t)(ilo + k) * H + Y];
+      }
+    }
+  }
+  __syncthreads();
+  int X = X0 + tx;
   if (X >= W) return;
   int i;
   double t;
   fine_index(X, W, w, &i, &t);
-  double v = nak_eval(Tt[(size_t)i * H + Y], Tt[(size_t)(i + 1) * H + Y], M[(size_t)i * H + Y],
-                      M[(size_t)(i + 1) * H + Y], t);
-  dst[(size_t)Y * dpitch + X] = __fmul_rn((float)v, scale);
+  for (int k = ty; k < 32; k += 8) {
+    int Y = Y0 + k;
+    if (Y >= H) break;
+    double v;
+    if (staged) {
+      v = nak_eval(sT[i - ilo][k], sT[i - ilo + 1][k], sM[i - ilo][k], sM[i - ilo + 1][k], t);
+    } else {
+      v = nak_eval(Tt[(size_t)i * H + Y], Tt[(size_t)(i + 1) * H + Y], M[(size_t)i * H + Y],
+                   M[(size_t)(i + 1) * H + Y], t);
+    }
+    dst[(size_t)Y * dpitch + X] = __fmul_rn((float)v, scale);
+  }
 }
 
 // ----------------------------------------------------------------------------- warp
@@ -324,13 +415,13 @@ extern "C" int of_resize(const float* src, int Hs, int Ws, int src_pitch, float*
 extern "C" size_t of_spline_workspace_size(int h, int w, int H, int W) {
   Sizer s;
   size_t a = (size_t)h * w, b = (size_t)H * w;
-  s.take<double>(a);      // column samples (double)
   s.take<double>(a);      // moments along y
-  s.take<double>(2 * a);  // Thomas scratch along y
-  s.take<double>(b);      // T (fine rows x coarse columns)
-  s.take<double>(b);      // T transposed
+  s.take<double>(a);      // Thomas scratch along y
+  s.take<double>((size_t)(h > w ? h : w));  // shared reciprocal pivots
+  s.take<double>(b);      // column splines at the fine rows, layout [x][Y]
   s.take<double>(b);      // moments along x
-  s.take<double>(2 * b);  // Thomas scratch along x
+  s.take<double>(b);      // Thomas scratch along x
+  (void)W;
   return s.off;
 }
 
@@ -344,18 +435,19 @@ extern "C" int of_spline_upsample(const float* src, int h, int w, int src_pitch,
   cudaStream_t st = as_stream(stream);
   size_t a = (size_t)h * w, b = (size_t)H * w;
   Carver c(workspace, workspace_bytes);
-  double* Y0 = c.take<double>(a);
   double* My = c.take<double>(a);
-  double* Sy = c.take<double>(2 * a);
-  double* T = c.take<double>(b);
+  double* Sy = c.take<double>(a);
+  double* piv = c.take<double>((size_t)(h > w ? h : w));
   double* Tt = c.take<double>(b);
   double* Mx = c.take<double>(b);
-  double* Sx = c.take<double>(2 * b);
-  spline_my_kernel<<<(w + 127) / 128, 128, 0, st>>>(src, src_pitch, h, w, My, Y0, Sy);
-  spline_ey_kernel<<<dim3((w + 127) / 128, H), 128, 0, st>>>(Y0, My, T, h, w, H);
-  spline_mx_kernel<<<(H + 127) / 128, 128, 0, st>>>(T, w, H, Mx, Sx, Sx + b, Tt);
-  spline_ex_kernel<<<dim3((W + 127) / 128, H), 128, 0, st>>>(Tt, Mx, dst, dst_pitch, w, H, W, scale);
-  return check_launch("of_spline_upsample", 4);
+  double* Sx = c.take<double>(b);
+  spline_recip_kernel<<<1, 256, 0, st>>>(piv, (h > w ? h : w) - 4);
+  spline_my_kernel<<<(w + 127) / 128, 128, 0, st>>>(src, src_pitch, h, w, My, Sy, piv);
+  spline_ey_kernel<<<dim3((w + 31) / 32, (H + 31) / 32), dim3(32, 8), 0, st>>>(src, src_pitch, My, Tt, h, w, H);
+  spline_mx_kernel<<<(H + 127) / 128, 128, 0, st>>>(Tt, w, H, Mx, piv, Sx);
+  spline_ex_kernel<<<dim3((W + 31) / 32, (H + 31) / 32), dim3(32, 8), 0, st>>>(Tt, Mx, dst, dst_pitch, w, H, W,
+                                                                              scale);
+  return check_launch("of_spline_upsample", 5);
 }
 
 extern "C" int of_warp_pair_bilinear(const float* I0, const float* I1, const float* U, const float* V, float* O0,

@@ -507,28 +507,39 @@ EXPORT void ofo_resize(const float* src, int Hs, int Ws, float* dst, int Hd, int
  * (moment) form on unit spacing, in double, rows then columns; result rounded to f32.
  * ------------------------------------------------------------------------------------------ */
 /* moments of the not-a-knot spline through y[0..n-1] (n >= 4), unit spacing */
+/* Reciprocal pivots of the constant (1, 4, 1) tridiagonal elimination:
+ * c[0] = 1/4, c[r] = 1/(4 - c[r-1]); the sequence reaches its fixed point (2 - sqrt 3) in
+ * double after a few tens of steps, after which every entry repeats it. */
+static void nak_recip(double* c, int m) {
+  if (m <= 0) return;
+  c[0] = 1.0 / 4.0;
+  int r = 1;
+  for (; r < m; r++) {
+    c[r] = 1.0 / (4.0 - c[r - 1]);
+    if (c[r] == c[r - 1]) break;
+  }
+  for (; r < m; r++) c[r] = c[r - 1];
+}
+
 static void nak_moments(const double* y, int n, double* M, double* cp, double* dp) {
-  /* M1 = d1, M_{n-2} = d_{n-2}; interior rows i=2..n-3: M_{i-1}+4M_i+M_{i+1} = 6 d_i */
+  /* M1 = d1, M_{n-2} = d_{n-2}; interior rows i=2..n-3: M_{i-1}+4M_i+M_{i+1} = 6 d_i,
+   * eliminated with the pivots of nak_recip (cp) as multiplications */
   double d1 = y[2] - 2.0 * y[1] + y[0];
   double dl = y[n - 1] - 2.0 * y[n - 2] + y[n - 3];
   M[1] = d1;
   M[n - 2] = dl;
   int m = n - 4; /* unknowns M_2 .. M_{n-3} */
   if (m > 0) {
+    nak_recip(cp, m);
     for (int r = 0; r < m; r++) {
       int i = r + 2;
       double rhs = 6.0 * (y[i + 1] - 2.0 * y[i] + y[i - 1]);
       if (r == 0) rhs -= M[1];
       if (r == m - 1) rhs -= M[n - 2];
-      double b = 4.0;
-      if (r == 0) {
-        cp[r] = 1.0 / b;
-        dp[r] = rhs / b;
-      } else {
-        double den = b - cp[r - 1];
-        cp[r] = 1.0 / den;
-        dp[r] = (rhs - dp[r - 1]) / den;
-      }
+      if (r == 0)
+        dp[r] = rhs * cp[r];
+      else
+        dp[r] = (rhs - dp[r - 1]) * cp[r];
     }
     M[m + 1] = dp[m - 1];
     for (int r = m - 2; r >= 0; r--) M[r + 2] = dp[r] - cp[r] * M[r + 3];

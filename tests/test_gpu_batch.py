@@ -1,0 +1,101 @@
+"""Concurrent multi-stream batches (ofb200.batch) give, pair for pair, the single-pair
+result of the drop-in driver, for mixed sizes and methods, eager and graph-replayed."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _pair(size, seed):
+    from ofb200 import synthetic as S
+    a, b, _, _ = S.config_pair("fbls1024", seed=seed, size=size)
+    return a.astype(np.float32), b.astype(np.float32)
+
+
+def _specs():
+    import Farneback_PyCL as F
+    import HornSchunck as HS
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    from ofb200.batch import PairSpec
+    return [
+        PairSpec(0, lambda: F.Farneback_PyCL(), 2, 1, 0.48, lambda: LS.LiuShenOpticalFlowAlgoAdapter(10),
+                 key=("fbls",)),
+        PairSpec(3.4, lambda: HS.HSOpticalFlowAlgoAdapter([7, 21, 45], 50), 2, 1, key=("hs",)),
+        PairSpec(0, lambda: F.Farneback_PyCL(), 2, 1, 0.48, lambda: LS.LiuShenOpticalFlowAlgoAdapter(10),
+                 key=("fbls",)),
+        PairSpec(1.0, lambda: LS.LiuShenOpticalFlowAlgoAdapter(20), 1, 1, key=("ls",)),
+    ], [(256, 1), (192, 2), (320, 3), (128, 4)]
+
+
+def _single(spec, a, b):
+    import GenericPyramidalOpticalFlow as G
+    opt = spec.make_opt() if spec.make_opt is not None else None
+    return G.genericPyramidalOpticalFlow(a, b, spec.FILTER, spec.make_main(), spec.pyramidalLevels, spec.kLevels,
+                                         spec.FILTER_OPT, opt)
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batch_matches_single(torch_cuda, use_graph):
+    torch = torch_cuda
+    from ofb200 import graph
+    from ofb200.batch import PairBatch
+    specs, shapes = _specs()
+    host = [_pair(s, seed) for s, seed in shapes]
+    graph.ENABLED = False
+    want = [_single(sp, a, b) for sp, (a, b) in zip(specs, host)]
+    graph.ENABLED = True
+    batch = PairBatch(specs, streams=3, use_graph=use_graph)
+    dev = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in host]
+    for _ in range(2):  # second run replays the captured graph
+        got = batch.run(dev)
+        torch.cuda.synchronize()
+        for (Ug, Vg), (Uw, Vw) in zip(got, want):
+            assert np.array_equal(Ug.cpu().numpy(), Uw)
+            assert np.array_equal(Vg.cpu().numpy(), Vw)
+
+
+def test_batch_new_inputs_replay(torch_cuda):
+    """A replay on new frames of the same shapes gives those frames' results."""
+    torch = torch_cuda
+    from ofb200 import graph
+    from ofb200.batch import PairBatch
+    specs, shapes = _specs()
+    batch = PairBatch(specs, streams=2)
+    first = [_pair(s, seed) for s, seed in shapes]
+    second = [_pair(s, seed + 50) for s, seed in shapes]
+    batch.run([(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in first])
+    got = batch.run([(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in second])
+    got = [(u.cpu().numpy(), v.cpu().numpy()) for u, v in got]
+    graph.ENABLED = False
+    try:
+        for sp, (a, b), (Ug, Vg) in zip(specs, second, got):
+            Uw, Vw = _single(sp, a, b)
+            assert np.array_equal(Ug, Uw) and np.array_equal(Vg, Vw)
+    finally:
+        graph.ENABLED = True
+
+
+def test_batch_u8_frames(torch_cuda):
+    torch = torch_cuda
+    from ofb200 import synthetic as S
+    from ofb200.batch import PairBatch
+    specs, _ = _specs()
+    a, b, _, _ = S.config_pair("fbls1024", seed=5, size=256)
+    got = PairBatch(specs[:1], streams=1).run([(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda())])
+    Uw, Vw = _single(specs[0], a.astype(np.float32), b.astype(np.float32))
+    assert np.array_equal(got[0][0].cpu().numpy(), Uw) and np.array_equal(got[0][1].cpu().numpy(), Vw)
+
+
+def test_batch_rejects_count_mismatch(torch_cuda):
+    from ofb200.batch import PairBatch
+    specs, _ = _specs()
+    with pytest.raises(ValueError):
+        PairBatch(specs).run([])
