@@ -41,6 +41,9 @@ METRIC = "pairs/s @1024^2 Liu-Shen (Farneback pyr2 + Liu-Shen, plain)"
 WORKLOAD = "LiuSE_Farneback_Fs0_0_PyrLvls2 1024x1024 random-Fourier PIV pairs"
 L2_BYTES = 126 * 2 ** 20
 REF_BUDGET_S = 90.0
+# DRAM bytes (read + write) of one 60-sweep Liu-Shen solve at 1024^2, summed over its
+# launches from one ncu capture (profiles/ls_solve_traffic_1024.txt; cold cache per launch)
+NCU_LS_TRAFFIC = {1024: 672.27e6}
 
 
 def parse():
@@ -280,7 +283,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk, "e2e": e2e, "gpu_launches": int(launches),
         "roofline": {"kernel": "Liu-Shen solve 1024^2 (setup + sweeps)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": None, "sweeps": iters, "ms": ls_ms,
+                     "peak_kind": peak_kind,
+                     "traffic": NCU_LS_TRAFFIC.get(args.size) if iters == 60 else None, "sweeps": iters, "ms": ls_ms,
                      "algorithmic_bytes": alg_bytes},
     }
     if not args.no_cpu_baseline:
