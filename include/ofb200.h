@@ -193,6 +193,57 @@ int of_fb_update_flow(const float* M, float* flowx, float* flowy, int H, int W, 
 int of_fb_iteration(const float* M_in, float* M_out, const float* R0, const float* R1, float* flowx, float* flowy,
                     int H, int W, int pitch, const float* wk, int kh, int update_matrices, void* stream);
 
+/* ---------------------------------------------------------------------------------
+ * Learned warm start for Liu-Shen (no reference counterpart: the reference has no
+ * learned component).  An encoder-decoder CNN over bfloat16 NHWC activations
+ * ([image][y][x][channel], a tensor may be a channel slice [coff, coff + C) of a wider
+ * one with ctot channels per pixel; for bf16 tensors ctot and coff multiples of 8), f32
+ * accumulation.
+ * `err` is a device word; the conv kernel ORs a nonzero code into it when one of its
+ * bounded waits gives up (its output is then incomplete).
+ * ------------------------------------------------------------------------------- */
+#define OF_CNN_RELU 1 /* apply max(0, .) after the bias */
+#define OF_CNN_F32 2  /* store float32 instead of bfloat16 */
+/* y = conv3x3(x, w) + bias, zero padding, tensor cores (tcgen05, TMEM accumulator).
+ * x: n x H x W x cin slice (cin 16 or a multiple of 32); w: bf16 [9][cout][cin] (tap =
+ * 3 * (dy + 1) + (dx + 1)); cout a multiple of 16, <= 512; W a divisor or a multiple of
+ * 128, H a multiple of 128 / min(W, 128) or a divisor of it, and then n a multiple of
+ * 128 / (W * H).  Channels [0, cout_store) are written. */
+int of_cnn_conv3x3(const void* x, int n, int H, int W, int cin, int x_ctot, int x_coff, const void* w, int cout,
+                   const float* bias, int flags, void* y, int y_ctot, int y_coff, int cout_store, unsigned* err,
+                   void* stream);
+/* dw[tap][co][ci] += sum_p dy[p][co] * x[p + tap][ci]   (f32, CUDA cores). */
+int of_cnn_conv3x3_wgrad(const void* x, int x_ctot, int x_coff, const void* dy, int dy_ctot, int dy_coff, int n,
+                         int H, int W, int cin, int cout, float* dw, void* stream);
+/* db[c] += sum_p dy[p][c] over P pixels. */
+int of_cnn_bias_grad(const void* dy, int dy_ctot, int dy_coff, long long P, int cout, float* db, void* stream);
+/* out[y][x] = (I0 / max I0, I1 / max I1, 0 ...) over cpad channels; max2: 2 device words. */
+int of_cnn_pack_pair(const float* I0, const float* I1, int H, int W, int pitch, unsigned* max2, void* out, int cpad,
+                     void* stream);
+int of_cnn_avgpool2(const void* x, int x_ctot, int x_coff, int n, int H, int W, int C, void* y, int y_ctot,
+                    int y_coff, void* stream);
+int of_cnn_avgpool2_bwd(const void* dy, int dy_ctot, int dy_coff, int n, int H, int W, int C, void* dx, int dx_ctot,
+                        int dx_coff, int accumulate, void* stream);
+int of_cnn_upsample2(const void* x, int x_ctot, int x_coff, int n, int h, int w, int C, void* y, int y_ctot,
+                     int y_coff, void* stream);
+int of_cnn_upsample2_bwd(const void* dy, int dy_ctot, int dy_coff, int n, int h, int w, int C, void* dx, int dx_ctot,
+                         int dx_coff, void* stream);
+/* g *= (y > 0) over P pixels x C channels. */
+int of_cnn_relu_bwd(void* g, int g_ctot, int g_coff, const void* y, int y_ctot, int y_coff, long long P, int C,
+                    void* stream);
+/* loss += sum |pred - label|^2 / (2P) over P two-channel f32 pixels; dpred (bf16, g_ctot
+ * channels, padding zeroed; may be NULL) = (pred - label) / P. */
+int of_cnn_flow_mse(const float* pred, const float* label, long long P, void* dpred, int g_ctot, double* loss,
+                    void* stream);
+int of_cnn_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+                int step, void* stream);
+/* master w[tap][co][ci] (f32) -> bf16 [9][cout_pad][cin_pad], or with transpose_flip
+ * the input-gradient operand [9][cin_pad][cout_pad] with the taps mirrored. */
+int of_cnn_pack_weights(const float* w, int cout, int cin, int cout_pad, int cin_pad, int transpose_flip, void* out,
+                        void* stream);
+/* (h, w, 2) interleaved f32 flow -> u, v planes (row pitch `pitch`). */
+int of_cnn_split_flow(const float* flow, int h, int w, float* u, float* v, int pitch, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

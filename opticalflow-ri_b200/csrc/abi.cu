@@ -23,8 +23,8 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-int tmap_f32(CUtensorMap* map, const void* base, int rank, const uint64_t* dims, const uint64_t* strides_bytes,
-             const uint32_t* box) {
+static int tmap_encode(CUtensorMap* map, CUtensorMapDataType dtype, const void* base, int rank, const uint64_t* dims,
+                       const uint64_t* strides_bytes, const uint32_t* box, CUtensorMapSwizzle swz) {
   static EncodeTiledFn encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
@@ -34,8 +34,9 @@ int tmap_f32(CUtensorMap* map, const void* base, int rank, const uint64_t* dims,
     encode = reinterpret_cast<EncodeTiledFn>(fn);
   }
   if ((reinterpret_cast<uintptr_t>(base) & 15) != 0) return set_error(OF_ERR_INVALID, "tensor base not 16-byte aligned");
-  cuuint64_t d[3], s[2];
-  cuuint32_t b[3], e[3] = {1, 1, 1};
+  if (rank < 1 || rank > 5) return set_error(OF_ERR_INVALID, "tensor map rank %d", rank);
+  cuuint64_t d[5], s[4];
+  cuuint32_t b[5], e[5] = {1, 1, 1, 1, 1};
   for (int i = 0; i < rank; i++) {
     d[i] = dims[i];
     b[i] = box[i];
@@ -44,11 +45,33 @@ int tmap_f32(CUtensorMap* map, const void* base, int rank, const uint64_t* dims,
     if (strides_bytes[i] % 16) return set_error(OF_ERR_INVALID, "tensor stride not a multiple of 16 bytes");
     s[i] = strides_bytes[i];
   }
-  CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, const_cast<void*>(base), d, s, b, e,
-                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r = encode(map, dtype, (cuuint32_t)rank, const_cast<void*>(base), d, s, b, e, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      swz, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_error(OF_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return OF_OK;
+}
+
+int tmap_f32(CUtensorMap* map, const void* base, int rank, const uint64_t* dims, const uint64_t* strides_bytes,
+             const uint32_t* box) {
+  if (rank > 3) return set_error(OF_ERR_INVALID, "tmap_f32: rank %d", rank);
+  return tmap_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, base, rank, dims, strides_bytes, box,
+                     CU_TENSOR_MAP_SWIZZLE_NONE);
+}
+
+int tmap_bf16(CUtensorMap* map, const void* base, int rank, const uint64_t* dims, const uint64_t* strides_bytes,
+              const uint32_t* box, int swizzle_bytes) {
+  CUtensorMapSwizzle swz;
+  switch (swizzle_bytes) {
+    case 0: swz = CU_TENSOR_MAP_SWIZZLE_NONE; break;
+    case 32: swz = CU_TENSOR_MAP_SWIZZLE_32B; break;
+    case 64: swz = CU_TENSOR_MAP_SWIZZLE_64B; break;
+    case 128: swz = CU_TENSOR_MAP_SWIZZLE_128B; break;
+    default: return set_error(OF_ERR_INVALID, "tmap_bf16: swizzle %d", swizzle_bytes);
+  }
+  if (swizzle_bytes && box[0] * 2u != (uint32_t)swizzle_bytes)
+    return set_error(OF_ERR_INVALID, "tmap_bf16: inner box of %u B does not match the %d B swizzle", box[0] * 2u,
+                     swizzle_bytes);
+  return tmap_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, base, rank, dims, strides_bytes, box, swz);
 }
 
 int check_launch(const char* what, long long nlaunch) {

@@ -33,6 +33,7 @@ _I = ctypes.c_int
 _F = ctypes.c_float
 _D = ctypes.c_double
 _Z = ctypes.c_size_t
+_L = ctypes.c_longlong
 
 _SIGS = {
     "of_version": ([], _I),
@@ -56,6 +57,19 @@ _SIGS = {
     "of_ls_workspace_size": ([_I, _I, _I, _I], _Z),
     "of_ls_solve": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P, _Z, _P], _I),
     "of_ls_solve_noalloc": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P], _I),
+    "of_cnn_conv3x3": ([_P, _I, _I, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, _P, _P], _I),
+    "of_cnn_conv3x3_wgrad": ([_P, _I, _I, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P], _I),
+    "of_cnn_bias_grad": ([_P, _I, _I, _L, _I, _P, _P], _I),
+    "of_cnn_pack_pair": ([_P, _P, _I, _I, _I, _P, _P, _I, _P], _I),
+    "of_cnn_avgpool2": ([_P, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P], _I),
+    "of_cnn_avgpool2_bwd": ([_P, _I, _I, _I, _I, _I, _I, _P, _I, _I, _I, _P], _I),
+    "of_cnn_upsample2": ([_P, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P], _I),
+    "of_cnn_upsample2_bwd": ([_P, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P], _I),
+    "of_cnn_relu_bwd": ([_P, _I, _I, _P, _I, _I, _L, _I, _P], _I),
+    "of_cnn_flow_mse": ([_P, _P, _L, _P, _I, _P, _P], _I),
+    "of_cnn_adam": ([_P, _P, _P, _P, _L, _F, _F, _F, _F, _I, _P], _I),
+    "of_cnn_pack_weights": ([_P, _I, _I, _I, _I, _I, _P, _P], _I),
+    "of_cnn_split_flow": ([_P, _I, _I, _P, _P, _I, _P], _I),
     "of_lk_dense": ([_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P], _I),
     "of_fb_blur": ([_P, _P, _I, _I, _I, _I, _P, _I, _P], _I),
     "of_fb_box5": ([_P, _P, _I, _I, _I, _I, _P], _I),

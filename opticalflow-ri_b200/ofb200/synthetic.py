@@ -41,8 +41,7 @@ class Flow:
             self.k = np.array(kk, dtype=np.float64) * (2 * np.pi / L)
             self.phi = rng.uniform(0, 2 * np.pi, modes)
             self.amp = rng.normal(0, 1, modes) / np.maximum(np.hypot(self.k[:, 0], self.k[:, 1]), 1e-9)
-            yy, xx = np.mgrid[0:H, 0:W].astype(np.float64)
-            u, v = self._fourier_raw(xx, yy)
+            u, v = self._fourier_grid()
             self.scale = self.max_disp / max(np.max(np.hypot(u, v)), 1e-12)
         elif kind not in ("poiseuille", "lamb_oseen", "uniform"):
             raise ValueError(kind)
@@ -55,6 +54,19 @@ class Flow:
             u += c * ky      # d psi / d y
             v -= c * kx      # -d psi / d x
         return u, v
+
+    def _fourier_grid(self):
+        """The unscaled field on the pixel grid, separably: cos(kx x + ky y + p) =
+        cos(kx x) cos(ky y + p) - sin(kx x) sin(ky y + p), one matrix product per component."""
+        x = np.arange(self.W, dtype=np.float64)
+        y = np.arange(self.H, dtype=np.float64)
+        ax = np.outer(self.k[:, 0], x)                      # modes x W
+        by = np.outer(self.k[:, 1], y) + self.phi[:, None]  # modes x H
+        L = np.concatenate([np.cos(by), np.sin(by)]).T      # H x 2M
+        R = np.concatenate([np.cos(ax), -np.sin(ax)])       # 2M x W
+        wu = np.concatenate([self.amp * self.k[:, 1]] * 2)
+        wv = np.concatenate([-self.amp * self.k[:, 0]] * 2)
+        return (L * wu) @ R, (L * wv) @ R
 
     def __call__(self, x, y):
         x = np.asarray(x, np.float64)
@@ -73,6 +85,9 @@ class Flow:
         return u * self.scale, v * self.scale
 
     def ground_truth(self):
+        if self.kind == "fourier":
+            u, v = self._fourier_grid()
+            return (u * self.scale).astype(np.float32), (v * self.scale).astype(np.float32)
         yy, xx = np.mgrid[0:self.H, 0:self.W].astype(np.float64)
         u, v = self(xx, yy)
         return u.astype(np.float32), v.astype(np.float32)
@@ -86,11 +101,13 @@ def _render(H, W, px, py, amp, diam, radius):
     keep = (ix >= -radius - 1) & (ix <= W + radius) & (iy >= -radius - 1) & (iy <= H + radius)
     px, py, amp, diam, ix, iy = px[keep], py[keep], amp[keep], diam[keep], ix[keep], iy[keep]
     inv = -8.0 / (diam * diam)
-    for oy in range(-radius, radius + 2):
-        for ox in range(-radius, radius + 2):
-            jx, jy = ix + ox, iy + oy
-            val = amp * np.exp(inv * ((jx - px) ** 2 + (jy - py) ** 2))
-            np.add.at(img, (jy + off, jx + off), val)
+    Wp = W + 2 * off
+    o = np.arange(-radius, radius + 2)
+    jx = ix[:, None, None] + o[None, None, :]
+    jy = iy[:, None, None] + o[None, :, None]
+    val = amp[:, None, None] * np.exp(inv[:, None, None] * ((jx - px[:, None, None]) ** 2 +
+                                                            (jy - py[:, None, None]) ** 2))
+    img += np.bincount(((jy + off) * Wp + jx + off).ravel(), weights=val.ravel(), minlength=img.size).reshape(img.shape)
     return img[off:off + H, off:off + W]
 
 

@@ -1,0 +1,202 @@
+"""Training and calibration of the learned Liu-Shen warm start.
+
+    python -m ofb200.warmstart_train --pairs 2000 --steps 3000 --out warmstart.npz
+
+1. Training pairs (1024^2, seeded; random-Fourier or Lamb-Oseen flow with a random core
+   radius, 0.02-0.1 particles/px, noise sigma 0-5 DN, diameter 2-3 px, max 4 px) are
+   rendered on the host cores by a spawn process pool.
+2. Each pair is labelled by the plain pipeline on the GPU (Farneback pyr2 + Liu-Shen h = 10,
+   the package's converged output); frames and label are taken to the 512^2 level (the
+   pyramid's bicubic downsample; the label also halved in magnitude).
+3. The network is trained on random 256^2 crops (Adam, mean squared flow error) with the
+   package's own forward / backward kernels.
+4. On held-out pairs of the 1024^2 benchmark workload (disjoint seeds) the plain pipeline
+   and the learned start followed by K Liu-Shen sweeps are compared by interior endpoint
+   error against the analytic ground truth; the smallest K whose mean EPE is at most the
+   plain mean is kept, and the fallback threshold on the solve's last update norm is
+   set from the pairs that met the plain EPE.
+Weights, K, the threshold and the evaluation table go to one .npz.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+if PKG not in sys.path:
+    sys.path.insert(0, PKG)
+
+TRAIN_SEED0 = 10_000
+EVAL_SEED0 = 900_000
+LEVEL = 512
+CROP = 256
+
+
+def _train_pair(seed):
+    from ofb200 import synthetic as S
+    rng = np.random.default_rng(seed)
+    kind = "fourier" if rng.uniform() < 0.5 else "lamb_oseen"
+    kw = {"core_radius": float(rng.uniform(40, 160))} if kind == "lamb_oseen" else {}
+    a, b, U, V = S.piv_pair(1024, 1024, kind, seed=seed, density=float(rng.uniform(0.02, 0.1)), diameter=(2.0, 3.0),
+                            noise=float(rng.uniform(0.0, 5.0)), **kw)
+    return a, b
+
+
+def _eval_pair(seed):
+    from ofb200 import synthetic as S
+    return S.config_pair("fbls1024", seed=seed)
+
+
+def generate(fn, seeds, workers):
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers) as pool:
+        return pool.map(fn, seeds, chunksize=max(1, len(seeds) // (4 * workers)))
+
+
+def plain(a, b):
+    import Farneback_PyCL as F
+    import GenericPyramidalOpticalFlow as G
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    return G.genericPyramidalOpticalFlow(a, b, 0, F.Farneback_PyCL(), 2, 1, 0.48, LS.LiuShenOpticalFlowAlgoAdapter(10))
+
+
+def build_level_data(pairs, dev):
+    """(N, 512, 512, 2) bf16 inputs (each frame / its max) and (N, 512, 512, 2) f32 labels."""
+    import torch
+    from ofb200 import ops
+    from ofb200._lib import call
+    from ofb200.warmstart import _p, _sp
+    N = len(pairs)
+    X = torch.empty((N, LEVEL, LEVEL, 2), dtype=torch.bfloat16, device=dev)
+    Y = torch.empty((N, LEVEL, LEVEL, 2), dtype=torch.float32, device=dev)
+    tmp = torch.empty((LEVEL, LEVEL, 16), dtype=torch.bfloat16, device=dev)
+    mx = torch.zeros(2, dtype=torch.int32, device=dev)
+    for i, (a, b) in enumerate(pairs):
+        A = ops.u8_to_f32(torch.from_numpy(a).to(dev))
+        B = ops.u8_to_f32(torch.from_numpy(b).to(dev))
+        U, V = plain(A, B)
+        a2 = ops.resize(A, (LEVEL, LEVEL), bicubic=True)
+        b2 = ops.resize(B, (LEVEL, LEVEL), bicubic=True)
+        call("of_cnn_pack_pair", _p(a2), _p(b2), LEVEL, LEVEL, LEVEL, _p(mx), _p(tmp), 16, _sp())
+        X[i] = tmp[..., :2]
+        Y[i, ..., 0] = ops.scale(ops.resize(U, (LEVEL, LEVEL), bicubic=True), 0.5)
+        Y[i, ..., 1] = ops.scale(ops.resize(V, (LEVEL, LEVEL), bicubic=True), 0.5)
+    torch.cuda.synchronize()
+    return X, Y
+
+
+def train(net, X, Y, steps, batch=16, lr=1e-3, seed=0, log=print):
+    import torch
+    N = X.shape[0]
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    b = net.buffers(batch, CROP)
+    gb = net.grad_buffers(batch, CROP)
+    b["x0"].zero_()
+    lab = torch.empty((batch, CROP, CROP, 2), dtype=torch.float32, device=X.device)
+    hist = []
+    t0 = time.time()
+    for s in range(steps):
+        idx = torch.randint(0, N, (batch,), generator=g)
+        oy = torch.randint(0, LEVEL - CROP + 1, (batch,), generator=g)
+        ox = torch.randint(0, LEVEL - CROP + 1, (batch,), generator=g)
+        for j in range(batch):
+            i, y, x = int(idx[j]), int(oy[j]), int(ox[j])
+            b["x0"][j, ..., :2] = X[i, y:y + CROP, x:x + CROP]
+            lab[j] = Y[i, y:y + CROP, x:x + CROP]
+        net.forward(b)
+        loss = net.loss(b, gb, lab)
+        net.backward(b, gb)
+        cur = lr * 0.5 * (1 + np.cos(np.pi * s / steps))  # cosine decay
+        net.adam(cur)
+        if s % 100 == 0 or s == steps - 1:
+            lv = float(loss.item())
+            hist.append((s, lv))
+            log(f"step {s} loss {lv:.5f} lr {cur:.2e} {time.time() - t0:.1f}s")
+    net.check()
+    return hist
+
+
+def evaluate(net, pairs, sweeps_list, dev, log=print):
+    """Interior EPE (16 px crop) of plain vs learned + K sweeps; the solve's update norms."""
+    import torch
+    from ofb200 import synthetic as S
+    from ofb200.warmstart import LearnedLiuShen
+    rows = []
+    for a, b, Ug, Vg in pairs:
+        A = torch.from_numpy(a.astype(np.float32)).to(dev)
+        B = torch.from_numpy(b.astype(np.float32)).to(dev)
+        Up, Vp = plain(A, B)
+        row = {"plain": S.epe(Up.cpu().numpy(), Vp.cpu().numpy(), Ug, Vg, crop=16)}
+        for K in sweeps_list:
+            for mode in ("ls", "fb"):
+                U, V, it, err = LearnedLiuShen(net, sweeps=K, mode=mode).run(A, B)
+                row[(mode, K)] = (S.epe(U.cpu().numpy(), V.cpu().numpy(), Ug, Vg, crop=16), float(err.item()))
+        U0, V0 = LearnedLiuShen(net).predict(A, B)
+        row["cnn"] = S.epe(U0.cpu().numpy(), V0.cpu().numpy(), Ug, Vg, crop=16)
+        rows.append(row)
+    plain_m = float(np.mean([r["plain"] for r in rows]))
+    table = {"plain_epe": plain_m, "cnn_epe": float(np.mean([r["cnn"] for r in rows])), "modes": {}}
+    best = None
+    for mode in ("ls", "fb"):
+        table["modes"][mode] = {}
+        for K in sweeps_list:
+            e = [r[(mode, K)][0] for r in rows]
+            table["modes"][mode][K] = {"epe": float(np.mean(e)),
+                                       "err_max": float(np.max([r[(mode, K)][1] for r in rows])),
+                                       "worse_pairs": int(sum(x > r["plain"] for x, r in zip(e, rows)))}
+            log(f"{mode} K={K}: EPE {np.mean(e):.4f} (plain {plain_m:.4f})")
+            if np.mean(e) <= plain_m and best is None:
+                best = (mode, K)  # "ls" before "fb": the cheaper mode first, then fewer sweeps
+    mode, K = best if best is not None else ("fb", max(sweeps_list))
+    good = [r[(mode, K)][1] for r in rows if r[(mode, K)][0] <= r["plain"] * 1.02]
+    thr = float(np.max(good)) * 1.5 if good else 0.0
+    return mode, K, thr, table, rows
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--pairs", type=int, default=2000)
+    ap.add_argument("--eval", type=int, default=16)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--workers", type=int, default=0)
+    ap.add_argument("--sweeps", default="4,8,12,16,24,32,60")
+    ap.add_argument("--out", default="warmstart.npz")
+    args = ap.parse_args()
+    workers = args.workers or max(1, min(64, len(os.sched_getaffinity(0))))
+    t0 = time.time()
+    # host rendering first, in spawned workers, before this process touches CUDA
+    train_pairs = generate(_train_pair, [TRAIN_SEED0 + i for i in range(args.pairs)], workers)
+    eval_pairs = generate(_eval_pair, [EVAL_SEED0 + i for i in range(args.eval)], workers)
+    print(f"generated {len(train_pairs)} + {len(eval_pairs)} pairs on {workers} workers in {time.time() - t0:.0f}s",
+          flush=True)
+    import torch
+    from ofb200.warmstart import WarmStartNet
+    dev = torch.device("cuda", 0)
+    t1 = time.time()
+    X, Y = build_level_data(train_pairs, dev)
+    del train_pairs
+    print(f"labelled in {time.time() - t1:.0f}s", flush=True)
+    net = WarmStartNet(seed=0)
+    t2 = time.time()
+    hist = train(net, X, Y, args.steps, args.batch, args.lr, log=lambda m: print(m, flush=True))
+    print(f"trained in {time.time() - t2:.0f}s", flush=True)
+    sweeps = [int(s) for s in args.sweeps.split(",")]
+    mode, K, thr, table, rows = evaluate(net, eval_pairs, sweeps, dev, log=lambda m: print(m, flush=True))
+    meta = {"mode": mode, "sweeps": K, "threshold": thr, "table": table, "train_pairs": args.pairs, "steps": args.steps,
+            "batch": args.batch, "crop": CROP, "level": LEVEL, "eval_pairs": args.eval,
+            "train_seed0": TRAIN_SEED0, "eval_seed0": EVAL_SEED0, "loss_history": hist}
+    np.savez(args.out, meta=json.dumps(meta), **net.state())
+    print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}), flush=True)
+
+
+if __name__ == "__main__":
+    main()
