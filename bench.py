@@ -59,6 +59,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
     p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls"],
                    help="ls: only the Liu-Shen solve of one pair, --steps times (for profiling)")
     return p.parse_args()
@@ -269,6 +270,8 @@ def run_ours(args, rank, world, local_rank):
         e2e = {"value": n_e2e * world / float(dt.item()), "unit": "pairs/s",
                "h2d_bytes_per_step": 2 * N * 4 * args.pairs, "d2h_bytes_per_step": 2 * N * 4 * args.pairs}
 
+    learned = None if args.no_learned else run_learned(args, step_frames, pairs, dev, flush, world,
+                                                           pairs_total_ms=total_ms)
     if rank != 0:
         return None
     pairs_total = args.pairs * args.steps * world
@@ -280,7 +283,7 @@ def run_ours(args, rank, world, local_rank):
                    "unique_pairs": args.unique, "streams": args.streams,
                    "l2": "flushed between steps (256 MB write)",
                    "parallelism": f"pairs sharded over {world} rank(s)"},
-        "clocks": clk, "e2e": e2e, "gpu_launches": int(launches),
+        "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "learned": learned,
         "roofline": {"kernel": "Liu-Shen solve 1024^2 (setup + sweeps)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,
@@ -290,6 +293,75 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pairs[0])
     return line
+
+
+def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
+    """The learned warm start on the same frames: one network forward over the step's
+    pairs (512^2 level), Farneback at full size from that start, then the calibrated number
+    of Liu-Shen sweeps; pairs whose last update norm exceeds the calibrated threshold are
+    recomputed by the plain pyramid inside the timed region.  Endpoint errors of both arms
+    against the analytic ground truth (16 px interior) on the distinct pairs."""
+    import torch
+    import torch.distributed as dist
+    from ofb200 import ops, synthetic as S
+    from ofb200.warmstart import LearnedBatch, load_trained
+    net, meta = load_trained(device=dev)
+    nu = min(len(pairs), args.pairs)
+    plain_value = args.pairs * args.steps * world / (pairs_total_ms * 1e-3)
+    epe_p = []
+    for i in range(nu):
+        a, b, Ug, Vg = pairs[i]
+        Up, Vp = pipeline_dev(ops.u8_to_f32(step_frames[i][0]), ops.u8_to_f32(step_frames[i][1]))
+        epe_p.append(S.epe(Up.cpu().numpy(), Vp.cpu().numpy(), Ug, Vg, crop=16))
+
+    def arm(start):
+        lb = LearnedBatch(net, meta, args.pairs, args.size, streams=args.streams, start=start)
+
+        def step():
+            f32 = [(ops.u8_to_f32(a8), ops.u8_to_f32(b8)) for a8, b8 in step_frames]
+            res, errs = lb.run(f32)
+            if start == "zero":
+                return list(res), 0
+            return lb.fallback(f32, res, errs.cpu())
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        total_ms, fallbacks = 0.0, 0
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _, nfb = step()
+            e1.record()
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            fallbacks += nfb
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        out, _ = step()  # accuracy on the distinct pairs, outside the timed region
+        epe = [S.epe(out[i][0].cpu().numpy(), out[i][1].cpu().numpy(), pairs[i][2], pairs[i][3], crop=16)
+               for i in range(nu)]
+        value = args.pairs * args.steps * world / (total_ms * 1e-3)
+        ll = lb.ll
+        return {"value": value, "unit": "pairs/s", "ms_per_step": total_ms / args.steps,
+                "speedup_vs_plain": value / plain_value, "fb_iters": ll.fb_iters if ll.mode == "fb" else 0,
+                "sweeps": ll.sweeps, "fallback_pairs": fallbacks, "epe": float(np.mean(epe))}
+
+    learned = arm("cnn")
+    ablation = arm("zero")
+    net.check()
+    learned.update({"mode": meta["mode"], "threshold": meta["threshold"], "epe_plain": float(np.mean(epe_p)),
+                    "epe_pairs": nu, "epe_crop_px": 16,
+                    "network": "encoder-decoder CNN at the 512^2 level, 1.75M params, bf16 tcgen05 convs, f32 accumulate",
+                    "trained": {k: meta[k] for k in ("train_pairs", "steps", "batch", "crop", "level", "eval_pairs")},
+                    "no_network_ablation": ablation})
+    return learned
 
 
 def _oracle():

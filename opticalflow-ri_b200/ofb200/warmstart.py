@@ -27,6 +27,7 @@ points.  torch provides device memory and the stream only.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -34,7 +35,9 @@ import torch
 from . import ops
 from ._lib import call, lib
 
-__all__ = ["LAYERS", "WarmStartNet", "LearnedLiuShen", "n_params"]
+__all__ = ["LAYERS", "WarmStartNet", "LearnedLiuShen", "LearnedBatch", "load_trained", "n_params"]
+
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "warmstart_weights.npz")
 
 LAYERS = [  # name, cin, cout
     ("c0a", 2, 32), ("c0b", 32, 32),
@@ -309,45 +312,157 @@ class WarmStartNet:
 
 class LearnedLiuShen:
     """CNN warm start at the 512^2 level, spline upsample, then at full size either
-    Liu-Shen alone (mode "ls") or the pyramid's last level, Farneback then Liu-Shen
-    (mode "fb"), with `sweeps` Liu-Shen sweeps.
+    Liu-Shen alone (mode "ls") or the pyramid's last level, Farneback (`fb_iters`
+    iterations) then Liu-Shen (mode "fb"), with `sweeps` Liu-Shen sweeps.
 
     run() returns (U, V, iters, err): err is the solve's last update norm (device scalar);
     accept(err) tells whether it is within the calibrated threshold."""
 
-    def __init__(self, net: WarmStartNet, sweeps=16, h=10.0, filter_opt=0.48, threshold=None, mode="ls"):
+    def __init__(self, net: WarmStartNet, sweeps=16, h=10.0, filter_opt=0.48, threshold=None, mode="ls", fb_iters=5):
         self.net, self.sweeps, self.h, self.filter_opt, self.threshold = net, int(sweeps), float(h), filter_opt, threshold
         if mode not in ("ls", "fb"):
             raise ValueError(mode)
-        self.mode = mode
+        self.mode, self.fb_iters = mode, int(fb_iters)
         from gaussian_filter import prepareGaussianKernel
         self.taps = prepareGaussianKernel(filter_opt, 5)
 
-    def predict(self, I0, I1):
-        """Initial (U, V) at the frames' size from the CNN at half size."""
+    def pack(self, b, i, I0, I1):
+        """The pyramid's half-size level of pair i into the network input."""
         H, W = I0.shape
-        h, w = H // 2, W // 2
-        n0 = ops.resize(I0, (w, h), bicubic=True)
-        n1 = ops.resize(I1, (w, h), bicubic=True)
-        b = self.net.buffers(1, h)
-        self.net.pack_input(b, 0, n0, n1)
-        out = self.net.forward(b)[0]
-        u = torch.empty((h, w), dtype=torch.float32, device=I0.device)
+        n0 = ops.resize(I0, (W // 2, H // 2), bicubic=True)
+        n1 = ops.resize(I1, (W // 2, H // 2), bicubic=True)
+        self.net.pack_input(b, i, n0, n1)
+
+    @staticmethod
+    def upsample(out_i, H, W):
+        """The network's (h, w, 2) flow at half size -> the initial (U, V) at H x W."""
+        h, w = out_i.shape[0], out_i.shape[1]
+        u = torch.empty((h, w), dtype=torch.float32, device=out_i.device)
         v = torch.empty_like(u)
-        call("of_cnn_split_flow", _p(out), h, w, _p(u), _p(v), w, _sp())
+        call("of_cnn_split_flow", _p(out_i), h, w, _p(u), _p(v), w, _sp())
         U = ops.spline_upsample(u, H, W, np.float32(W) / np.float32(w))
         V = ops.spline_upsample(v, H, W, np.float32(H) / np.float32(h))
         return U, V
 
-    def run(self, I0, I1):
-        U, V = self.predict(I0, I1)
+    def predict(self, I0, I1):
+        """Initial (U, V) at the frames' size from the CNN at half size."""
+        H, W = I0.shape
+        b = self.net.buffers(1, H // 2)
+        self.pack(b, 0, I0, I1)
+        return self.upsample(self.net.forward(b)[0], H, W)
+
+    def refine(self, I0, I1, U, V):
+        """The full-size stage from the initial field: (Farneback,) then Liu-Shen."""
         if self.mode == "fb":
             import Farneback_PyCL as F
-            U, V, _ = F.Farneback_PyCL()._compute_dev(I0, I1, U, V)
+            U, V, _ = F.Farneback_PyCL(Niters=self.fb_iters)._compute_dev(I0, I1, U, V)
         f0 = ops.prefilter(I0, self.taps)
         f1 = ops.prefilter(I1, self.taps)
-        U, V, it, err = ops.ls_solve(f0, f1, U, V, self.h, self.sweeps, 1e-8)
-        return U, V, it, err
+        return ops.ls_solve(f0, f1, U, V, self.h, self.sweeps, 1e-8)
+
+    def run(self, I0, I1):
+        U, V = self.predict(I0, I1)
+        return self.refine(I0, I1, U, V)
 
     def accept(self, err) -> bool:
         return self.threshold is None or float(err) <= self.threshold
+
+
+def load_trained(path=WEIGHTS, device="cuda"):
+    """The packaged network and its calibration (mode, sweeps, threshold, evaluation)."""
+    import json
+    d = np.load(path)
+    meta = json.loads(str(d["meta"]))
+    return WarmStartNet(device=device).load(path), meta
+
+
+class LearnedBatch:
+    """n frame pairs of one size through the learned pipeline: one network forward over
+    the batch, then each pair's full-size stage on one of `streams` CUDA streams; the
+    whole step is captured into a CUDA graph on its first call and replayed afterwards.
+
+    run() returns the per-pair (U, V) (graph-owned, overwritten by the next run) and a
+    device vector of the Liu-Shen update norms; pairs whose norm exceeds the calibrated
+    threshold are recomputed by the plain pyramid in fallback().
+
+    start="zero" is the same full-size stage from a zero field with no network (the
+    ablation the calibration compares against); it uses the calibration's zero-start
+    Farneback iteration count."""
+
+    def __init__(self, net, meta, n, size=1024, streams=4, use_graph=True, start="cnn"):
+        if start not in ("cnn", "zero"):
+            raise ValueError(start)
+        fb_iters = meta.get("fb_iters", 5) if start == "cnn" else meta.get("zero_fb_iters", 5)
+        self.ll = LearnedLiuShen(net, sweeps=meta["sweeps"], threshold=meta["threshold"],
+                                 mode=meta["mode"] if start == "cnn" else "fb", fb_iters=fb_iters)
+        self.start = start
+        self.net, self.n, self.size, self.nstreams, self.use_graph = net, int(n), int(size), max(1, streams), use_graph
+        self._graph = None
+        self._streams = None
+
+    def _step(self, frames):
+        cur = torch.cuda.current_stream()
+        if self._streams is None:
+            self._streams = [torch.cuda.Stream() for _ in range(self.nstreams)]
+        out = None
+        if self.start == "cnn":
+            b = self.net.buffers(self.n, self.size // 2)
+            for i, (A, B) in enumerate(frames):
+                self.ll.pack(b, i, A, B)
+            out = self.net.forward(b)
+        errs = torch.empty(self.n, dtype=torch.float64, device=frames[0][0].device)
+        res = [None] * self.n
+        for s in self._streams:
+            s.wait_stream(cur)
+        for i, (A, B) in enumerate(frames):
+            with torch.cuda.stream(self._streams[i % self.nstreams]):
+                if out is not None:
+                    U, V = self.ll.upsample(out[i], self.size, self.size)
+                else:
+                    U, V = torch.zeros_like(A), torch.zeros_like(A)
+                U, V, _, err = self.ll.refine(A, B, U, V)
+                errs[i:i + 1].copy_(err.reshape(1))
+                res[i] = (U, V)
+        for s in self._streams:
+            cur.wait_stream(s)
+        return res, errs
+
+    def run(self, frames):
+        """frames: n (frame1, frame2) float32 CUDA tensors of size x size."""
+        if len(frames) != self.n:
+            raise ValueError("one frame pair per batch slot")
+        if not self.use_graph:
+            return self._step(frames)
+        if self._graph is None:
+            static_in = [(a.clone(), b.clone()) for a, b in frames]
+            self._step(static_in)  # eager warm-up: sizes the buffers and workspaces
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.graph(g, stream=side):
+                static_out = self._step(static_in)
+            self._graph = (g, static_in, static_out)
+        g, static_in, static_out = self._graph
+        for (sa, sb), (a, b) in zip(static_in, frames):
+            sa.copy_(a)
+            sb.copy_(b)
+        g.replay()
+        return static_out
+
+    def fallback(self, frames, res, errs):
+        """Replaces the pairs whose update norm exceeds the threshold by the plain pyramid;
+        returns the list of results and the number of pairs that fell back."""
+        import Farneback_PyCL as F
+        import GenericPyramidalOpticalFlow as G
+        import PhysicsBasedOpticalFlowLiuShen as LS
+        thr = self.ll.threshold
+        if thr is None:
+            return list(res), 0
+        bad = (errs > thr).nonzero().flatten().tolist()
+        out = list(res)
+        for i in bad:
+            A, B = frames[i]
+            out[i] = G.genericPyramidalOpticalFlow(A, B, 0, F.Farneback_PyCL(), 2, 1, 0.48,
+                                                   LS.LiuShenOpticalFlowAlgoAdapter(10))
+        return out, len(bad)

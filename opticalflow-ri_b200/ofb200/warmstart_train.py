@@ -10,12 +10,15 @@
    pyramid's bicubic downsample; the label also halved in magnitude).
 3. The network is trained on random 256^2 crops (Adam, mean squared flow error) with the
    package's own forward / backward kernels.
-4. On held-out pairs of the 1024^2 benchmark workload (disjoint seeds) the plain pipeline
-   and the learned start followed by K Liu-Shen sweeps are compared by interior endpoint
-   error against the analytic ground truth; the smallest K whose mean EPE is at most the
-   plain mean is kept, and the fallback threshold on the solve's last update norm is
-   set from the pairs that met the plain EPE.
-Weights, K, the threshold and the evaluation table go to one .npz.
+4. On held-out pairs of the 1024^2 benchmark workload (disjoint seeds) the plain pipeline,
+   the network's start followed by each full-size stage (Liu-Shen alone with K sweeps, or
+   Farneback with 1-5 iterations then K sweeps), and the same stages from a zero field
+   (the no-network ablation) are compared by interior endpoint error against the analytic
+   ground truth.  The cheapest network configuration whose mean EPE is at most the plain
+   mean is kept, with a fallback threshold on the solve's last update norm set from the
+   pairs that met the plain EPE; the cheapest such zero-start stage is recorded too.
+Weights, the configuration, the threshold and the evaluation table go to one .npz;
+--calibrate redoes step 4 for existing weights.
 """
 from __future__ import annotations
 
@@ -123,41 +126,85 @@ def train(net, X, Y, steps, batch=16, lr=1e-3, seed=0, log=print):
     return hist
 
 
+FB_ITERS = (1, 2, 3, 5)
+FB_SWEEPS = (4, 8)
+
+
+def _configs(sweeps_list):
+    """Full-size stages in increasing cost: Liu-Shen alone (by sweeps), then Farneback
+    (by iterations, then sweeps) followed by Liu-Shen."""
+    cfg = [("ls", 0, K) for K in sorted(sweeps_list)]
+    cfg += [("fb", it, K) for it in FB_ITERS for K in FB_SWEEPS]
+    return cfg
+
+
 def evaluate(net, pairs, sweeps_list, dev, log=print):
-    """Interior EPE (16 px crop) of plain vs learned + K sweeps; the solve's update norms."""
+    """Interior EPE (16 px crop) against the analytic ground truth of the plain pyramid,
+    of the network's start followed by each full-size stage, and of the same stages from
+    a zero field (no network).  The cheapest network configuration whose mean EPE is at
+    most the plain mean is kept; its fallback threshold is 1.5 x the largest update norm
+    among the pairs within 2% of their plain EPE."""
     import torch
     from ofb200 import synthetic as S
     from ofb200.warmstart import LearnedLiuShen
+    cfgs = _configs(sweeps_list)
     rows = []
     for a, b, Ug, Vg in pairs:
         A = torch.from_numpy(a.astype(np.float32)).to(dev)
         B = torch.from_numpy(b.astype(np.float32)).to(dev)
         Up, Vp = plain(A, B)
         row = {"plain": S.epe(Up.cpu().numpy(), Vp.cpu().numpy(), Ug, Vg, crop=16)}
-        for K in sweeps_list:
-            for mode in ("ls", "fb"):
-                U, V, it, err = LearnedLiuShen(net, sweeps=K, mode=mode).run(A, B)
-                row[(mode, K)] = (S.epe(U.cpu().numpy(), V.cpu().numpy(), Ug, Vg, crop=16), float(err.item()))
-        U0, V0 = LearnedLiuShen(net).predict(A, B)
+        base = LearnedLiuShen(net)
+        U0, V0 = base.predict(A, B)
         row["cnn"] = S.epe(U0.cpu().numpy(), V0.cpu().numpy(), Ug, Vg, crop=16)
+        for mode, it, K in cfgs:
+            ll = LearnedLiuShen(net, sweeps=K, mode=mode, fb_iters=max(it, 1))
+            U, V, _, err = ll.refine(A, B, U0.clone(), V0.clone())
+            row[("cnn", mode, it, K)] = (S.epe(U.cpu().numpy(), V.cpu().numpy(), Ug, Vg, crop=16), float(err.item()))
+            if mode == "fb":
+                Z = torch.zeros_like(A)
+                U, V, _, err = ll.refine(A, B, Z, Z.clone())
+                row[("zero", mode, it, K)] = (S.epe(U.cpu().numpy(), V.cpu().numpy(), Ug, Vg, crop=16),
+                                              float(err.item()))
         rows.append(row)
     plain_m = float(np.mean([r["plain"] for r in rows]))
-    table = {"plain_epe": plain_m, "cnn_epe": float(np.mean([r["cnn"] for r in rows])), "modes": {}}
-    best = None
-    for mode in ("ls", "fb"):
-        table["modes"][mode] = {}
-        for K in sweeps_list:
-            e = [r[(mode, K)][0] for r in rows]
-            table["modes"][mode][K] = {"epe": float(np.mean(e)),
-                                       "err_max": float(np.max([r[(mode, K)][1] for r in rows])),
-                                       "worse_pairs": int(sum(x > r["plain"] for x, r in zip(e, rows)))}
-            log(f"{mode} K={K}: EPE {np.mean(e):.4f} (plain {plain_m:.4f})")
-            if np.mean(e) <= plain_m and best is None:
-                best = (mode, K)  # "ls" before "fb": the cheaper mode first, then fewer sweeps
-    mode, K = best if best is not None else ("fb", max(sweeps_list))
-    good = [r[(mode, K)][1] for r in rows if r[(mode, K)][0] <= r["plain"] * 1.02]
+    table = {"plain_epe": plain_m, "cnn_epe": float(np.mean([r["cnn"] for r in rows])), "configs": {}}
+    best = {"cnn": None, "zero": None}
+    for start in ("cnn", "zero"):
+        for mode, it, K in cfgs:
+            key = (start, mode, it, K)
+            if key not in rows[0]:
+                continue
+            e = [r[key][0] for r in rows]
+            name = f"{start}:{mode}:fb{it}:ls{K}"
+            table["configs"][name] = {"epe": float(np.mean(e)), "err_max": float(np.max([r[key][1] for r in rows])),
+                                      "worse_pairs": int(sum(x > r["plain"] for x, r in zip(e, rows)))}
+            log(f"{name}: EPE {np.mean(e):.4f} (plain {plain_m:.4f})")
+            if best[start] is None and np.mean(e) <= plain_m:
+                best[start] = key
+    key = best["cnn"] or ("cnn", "fb", FB_ITERS[-1], FB_SWEEPS[-1])
+    good = [r[key][1] for r in rows if r[key][0] <= r["plain"] * 1.02]
     thr = float(np.max(good)) * 1.5 if good else 0.0
-    return mode, K, thr, table, rows
+    zkey = best["zero"] or ("zero", "fb", FB_ITERS[-1], FB_SWEEPS[-1])
+    sel = {"mode": key[1], "fb_iters": key[2], "sweeps": key[3], "threshold": thr, "zero_fb_iters": zkey[2],
+           "zero_sweeps": zkey[3]}
+    return sel, table, rows
+
+
+def calibrate_only(args):
+    """New calibration (configuration, threshold, table) for existing weights."""
+    workers = args.workers or max(1, min(64, len(os.sched_getaffinity(0))))
+    eval_pairs = generate(_eval_pair, [EVAL_SEED0 + i for i in range(args.eval)], workers)
+    import torch
+    from ofb200.warmstart import WarmStartNet
+    d = np.load(args.calibrate)
+    old = json.loads(str(d["meta"]))
+    net = WarmStartNet(seed=0).load(args.calibrate)
+    sweeps = [int(s) for s in args.sweeps.split(",")]
+    sel, table, _ = evaluate(net, eval_pairs, sweeps, torch.device("cuda", 0), log=lambda m: print(m, flush=True))
+    meta = {**{k: v for k, v in old.items() if k not in ("table",)}, **sel, "table": table, "eval_pairs": args.eval}
+    np.savez_compressed(args.out, meta=json.dumps(meta), params=d["params"], layers=d["layers"])
+    print(json.dumps({k: v for k, v in meta.items() if k not in ("loss_history", "table")}), flush=True)
 
 
 def main():
@@ -170,7 +217,10 @@ def main():
     ap.add_argument("--workers", type=int, default=0)
     ap.add_argument("--sweeps", default="4,8,12,16,24,32,60")
     ap.add_argument("--out", default="warmstart.npz")
+    ap.add_argument("--calibrate", default=None, help="recalibrate the weights in this .npz (no training)")
     args = ap.parse_args()
+    if args.calibrate:
+        return calibrate_only(args)
     workers = args.workers or max(1, min(64, len(os.sched_getaffinity(0))))
     t0 = time.time()
     # host rendering first, in spawned workers, before this process touches CUDA
@@ -190,8 +240,8 @@ def main():
     hist = train(net, X, Y, args.steps, args.batch, args.lr, log=lambda m: print(m, flush=True))
     print(f"trained in {time.time() - t2:.0f}s", flush=True)
     sweeps = [int(s) for s in args.sweeps.split(",")]
-    mode, K, thr, table, rows = evaluate(net, eval_pairs, sweeps, dev, log=lambda m: print(m, flush=True))
-    meta = {"mode": mode, "sweeps": K, "threshold": thr, "table": table, "train_pairs": args.pairs, "steps": args.steps,
+    sel, table, rows = evaluate(net, eval_pairs, sweeps, dev, log=lambda m: print(m, flush=True))
+    meta = {**sel, "table": table, "train_pairs": args.pairs, "steps": args.steps,
             "batch": args.batch, "crop": CROP, "level": LEVEL, "eval_pairs": args.eval,
             "train_seed0": TRAIN_SEED0, "eval_seed0": EVAL_SEED0, "loss_history": hist}
     np.savez(args.out, meta=json.dumps(meta), **net.state())

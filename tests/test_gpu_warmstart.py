@@ -1,0 +1,82 @@
+"""The learned Liu-Shen warm start end to end: the batched, graph-replayed pipeline equals
+the single-pair one, and on held-out pairs of the 1024^2 workload (seeds outside both the
+training and the calibration sets) the packaged network gives a lower interior endpoint
+error than the plain pyramid and than the same full-size stage started from zero."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HELD_OUT = (950_000, 950_001)
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+@pytest.fixture(scope="module")
+def trained(torch_cuda):
+    from ofb200.warmstart import load_trained
+    return load_trained()
+
+
+def _f32(torch, a):
+    return torch.from_numpy(a.astype(np.float32)).cuda()
+
+
+def test_batch_matches_single_pair(torch_cuda, trained):
+    torch = torch_cuda
+    from ofb200 import synthetic as S
+    from ofb200.warmstart import LearnedBatch, LearnedLiuShen
+    net, meta = trained
+    frames = []
+    for seed in (1, 2, 3):
+        a, b, _, _ = S.config_pair("fbls1024", seed=seed, size=256)
+        frames.append((_f32(torch, a), _f32(torch, b)))
+    ll = LearnedLiuShen(net, sweeps=meta["sweeps"], mode=meta["mode"], fb_iters=meta["fb_iters"])
+    want = [ll.run(A, B) for A, B in frames]
+    want = [(U.cpu().numpy(), V.cpu().numpy(), float(e.item())) for U, V, _, e in want]
+    lb = LearnedBatch(net, meta, 3, size=256, streams=2)
+    for _ in range(2):  # capture, then replay
+        res, errs = lb.run(frames)
+        torch.cuda.synchronize()
+        for (U, V), e, (Uw, Vw, ew) in zip(res, errs.cpu().tolist(), want):
+            assert np.array_equal(U.cpu().numpy(), Uw) and np.array_equal(V.cpu().numpy(), Vw)
+            assert e == pytest.approx(ew, rel=1e-9)  # summed with float64 atomics in any order
+    net.check()
+
+
+def test_trained_start_gain(torch_cuda, trained):
+    """With the calibrated configuration (one Farneback iteration at full size, then a few
+    Liu-Shen sweeps) the network's start is at least as accurate as the plain pyramid and
+    far better than the same stage from zero, which needs a second Farneback iteration to
+    come close: that iteration is what the network saves."""
+    torch = torch_cuda
+    import Farneback_PyCL as F
+    import GenericPyramidalOpticalFlow as G
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    from ofb200 import synthetic as S
+    from ofb200.warmstart import LearnedLiuShen
+    net, meta = trained
+    assert meta["mode"] == "fb" and meta["fb_iters"] < meta["zero_fb_iters"]
+    ll = LearnedLiuShen(net, sweeps=meta["sweeps"], mode="fb", fb_iters=meta["fb_iters"])
+    e_plain, e_learned, e_zero = [], [], []
+    for seed in HELD_OUT:
+        a, b, Ug, Vg = S.config_pair("fbls1024", seed=seed)
+        A, B = _f32(torch, a), _f32(torch, b)
+        Up, Vp = G.genericPyramidalOpticalFlow(A, B, 0, F.Farneback_PyCL(), 2, 1, 0.48,
+                                               LS.LiuShenOpticalFlowAlgoAdapter(10))
+        e_plain.append(S.epe(Up.cpu().numpy(), Vp.cpu().numpy(), Ug, Vg, crop=16))
+        U, V, _, err = ll.run(A, B)
+        e_learned.append(S.epe(U.cpu().numpy(), V.cpu().numpy(), Ug, Vg, crop=16))
+        assert float(err.item()) <= meta["threshold"]  # the calibrated judge accepts it
+        Z = torch.zeros_like(A)
+        Uz, Vz, _, _ = ll.refine(A, B, Z, Z.clone())
+        e_zero.append(S.epe(Uz.cpu().numpy(), Vz.cpu().numpy(), Ug, Vg, crop=16))
+    net.check()
+    assert np.mean(e_learned) <= np.mean(e_plain), (e_learned, e_plain)
+    assert np.mean(e_learned) < 0.5 * np.mean(e_zero), (e_learned, e_zero)
