@@ -95,7 +95,9 @@ def build_level_data(pairs, dev):
     return X, Y
 
 
-def train(net, X, Y, steps, batch=16, lr=1e-3, seed=0, log=print):
+def train(net, X, Y, steps, batch=16, lr=1e-3, seed=0, log=print, sync=None):
+    """Adam on random crops.  `sync(grads)` (data-parallel training) averages the flat
+    gradient vector over the ranks between backward and the optimizer step."""
     import torch
     N = X.shape[0]
     g = torch.Generator(device="cpu").manual_seed(seed)
@@ -116,6 +118,8 @@ def train(net, X, Y, steps, batch=16, lr=1e-3, seed=0, log=print):
         net.forward(b)
         loss = net.loss(b, gb, lab)
         net.backward(b, gb)
+        if sync is not None:
+            sync(net.grads)
         cur = lr * 0.5 * (1 + np.cos(np.pi * s / steps))  # cosine decay
         net.adam(cur)
         if s % 100 == 0 or s == steps - 1:
@@ -221,27 +225,46 @@ def main():
     args = ap.parse_args()
     if args.calibrate:
         return calibrate_only(args)
-    workers = args.workers or max(1, min(64, len(os.sched_getaffinity(0))))
+    # data-parallel under torchrun: each rank renders and labels its share of the pairs
+    # and the gradients are averaged every step (one all-reduce of the flat vector)
+    from ofb200.shard import average_gradients, shard_range
+    rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    workers = args.workers or max(1, min(64, len(os.sched_getaffinity(0)) // world))
     t0 = time.time()
     # host rendering first, in spawned workers, before this process touches CUDA
-    train_pairs = generate(_train_pair, [TRAIN_SEED0 + i for i in range(args.pairs)], workers)
-    eval_pairs = generate(_eval_pair, [EVAL_SEED0 + i for i in range(args.eval)], workers)
-    print(f"generated {len(train_pairs)} + {len(eval_pairs)} pairs on {workers} workers in {time.time() - t0:.0f}s",
-          flush=True)
+    mine = [TRAIN_SEED0 + i for i in shard_range(args.pairs, rank, world)]
+    train_pairs = generate(_train_pair, mine, workers)
+    eval_pairs = generate(_eval_pair, [EVAL_SEED0 + i for i in range(args.eval)], workers) if rank == 0 else []
+    print(f"rank {rank}: generated {len(train_pairs)} + {len(eval_pairs)} pairs on {workers} workers in "
+          f"{time.time() - t0:.0f}s", flush=True)
     import torch
     from ofb200.warmstart import WarmStartNet
-    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     t1 = time.time()
     X, Y = build_level_data(train_pairs, dev)
     del train_pairs
-    print(f"labelled in {time.time() - t1:.0f}s", flush=True)
-    net = WarmStartNet(seed=0)
+    print(f"rank {rank}: labelled in {time.time() - t1:.0f}s", flush=True)
+    net = WarmStartNet(seed=0, device=dev)  # the same initial weights on every rank
     t2 = time.time()
-    hist = train(net, X, Y, args.steps, args.batch, args.lr, log=lambda m: print(m, flush=True))
-    print(f"trained in {time.time() - t2:.0f}s", flush=True)
+    hist = train(net, X, Y, args.steps, args.batch, args.lr, seed=rank,
+                 log=(lambda m: print(m, flush=True)) if rank == 0 else (lambda m: None),
+                 sync=average_gradients if world > 1 else None)
+    print(f"rank {rank}: trained in {time.time() - t2:.0f}s", flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
     sweeps = [int(s) for s in args.sweeps.split(",")]
     sel, table, rows = evaluate(net, eval_pairs, sweeps, dev, log=lambda m: print(m, flush=True))
-    meta = {**sel, "table": table, "train_pairs": args.pairs, "steps": args.steps,
+    meta = {**sel, "table": table, "train_pairs": args.pairs, "steps": args.steps, "ranks": world,
             "batch": args.batch, "crop": CROP, "level": LEVEL, "eval_pairs": args.eval,
             "train_seed0": TRAIN_SEED0, "eval_seed0": EVAL_SEED0, "loss_history": hist}
     np.savez(args.out, meta=json.dumps(meta), **net.state())
