@@ -60,7 +60,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
-    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls"],
+    p.add_argument("--batch-pairs", type=int, default=256, help="--mode batch: pairs in the manifest")
+    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch"],
                    help="ls: only the Liu-Shen solve of one pair, --steps times (for profiling)")
     return p.parse_args()
 
@@ -364,6 +365,74 @@ def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
     return learned
 
 
+def run_batch(args, rank, world, local_rank):
+    """Config 4: a seeded manifest of pairs of uneven sizes (128^2-2048^2), methods (HS,
+    LK pyr2, Farneback pyr2, Farneback pyr2 + Liu-Shen) and flows, sharded over the ranks by
+    cost, rendered on the host cores, run as autotuned chunks of multi-stream CUDA graphs.
+    value = pairs of the whole manifest / max-over-ranks time of one pass."""
+    import multiprocessing as mp
+    from ofb200.batch import config4_manifest, pair_cost_of, render_entry
+    from ofb200.shard import gather_objects, max_over_ranks, shard_by_cost
+    manifest = config4_manifest(args.batch_pairs, seed=0)
+    mine = shard_by_cost([pair_cost_of(e) for e in manifest], world)[rank]
+    entries = [manifest[i] for i in mine]
+    try:
+        ncores = len(os.sched_getaffinity(0))
+    except Exception:
+        ncores = os.cpu_count() or 1
+    with mp.get_context("spawn").Pool(max(1, min(32, ncores // world))) as pool:  # before CUDA is touched
+        rendered = pool.map(render_entry, entries)
+    import torch
+    import torch.distributed as dist
+    from ofb200 import synthetic as S
+    from ofb200.batch import autotune
+    dev = torch.device("cuda", local_rank)
+    frames = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _, _ in rendered]
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    runner, table = autotune(entries, frames)
+    for _ in range(args.warmup):
+        runner.run(frames)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local_rank) if rank == 0 else None
+    total = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        outs = runner.run(frames)
+        e1.record()
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    clk = clocks.stop() if clocks else None
+    total = max_over_ranks(total, dev)
+    per = {}
+    for e, (U, V), (_, _, Ug, Vg) in zip(entries, outs, rendered):
+        ep = S.epe(U.cpu().numpy(), V.cpu().numpy(), Ug, Vg, crop=16 if e["size"] > 64 else 0)
+        per.setdefault(e["method"], []).append(ep)
+    per = gather_objects(per)
+    if rank != 0:
+        return None
+    merged = {}
+    for d in per:
+        for k, v in d.items():
+            merged.setdefault(k, []).extend(v)
+    epe = {k: {"mean": float(np.nanmean(v)) if np.isfinite(v).any() else None, "pairs": len(v),
+               "nonfinite": int(np.sum(~np.isfinite(v)))} for k, v in merged.items()}
+    return {"metric": "pairs/s, batched uneven pairs (config 4)", "value": len(manifest) * args.steps / (total * 1e-3),
+            "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{len(manifest)} pairs, sizes 128^2-2048^2, HS / LK pyr2 / FB pyr2 / FB pyr2 + LS, "
+                                   "Poiseuille / Lamb-Oseen / random-Fourier, max 4 px",
+                       "l2": "flushed between steps (256 MB write)", "parallelism": f"pairs sharded by cost over {world}",
+                       "autotuned": {"chunk": runner.key[0], "streams": runner.key[1],
+                                     "candidates_ms": {f"{c}x{s}": round(v, 2) for (c, s), v in table.items()}}},
+            "clocks": clk, "epe_interior": epe}
+
+
 def _oracle():
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as O
@@ -431,6 +500,22 @@ def main():
         return
     if args.mode == "ls":
         run_ls_only(args)
+        return
+    if args.mode == "batch":
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        line = run_batch(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        if line:
+            print(json.dumps(line))
         return
     if world > 1:
         import datetime

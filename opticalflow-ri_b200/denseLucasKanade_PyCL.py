@@ -65,6 +65,12 @@ class denseLucasKanade_PyCl(object):
         ops.lk_dense(I, J, Ud, Vd, self.windowHalfWidth, self.Niter, asym, st, er)
         return Ud, Vd, st, er
 
+    def _compute_dev(self, im1, im2, U, V):
+        """compute() on device tensors; enqueues only (no host synchronisation) unless the
+        vorticity enhancement has to read the mean vorticity back."""
+        Ud, Vd, _, _ = self._run(im1, im2, U, V, False)
+        return Ud, Vd, True
+
     def compute(self, im1, im2, U, V):
         Ud, Vd, _, _ = self._run(im1, im2, U, V, False)
         if is_host(im1):

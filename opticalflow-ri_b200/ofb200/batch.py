@@ -19,7 +19,8 @@ import torch
 from . import graph as _graph
 from . import ops
 
-__all__ = ["PairSpec", "PairBatch"]
+__all__ = ["PairSpec", "PairBatch", "method_spec", "config4_manifest", "render_entry", "pair_cost_of", "BatchRunner",
+           "autotune"]
 
 
 @dataclass
@@ -58,13 +59,17 @@ def _cfg_for(spec: PairSpec, main):
 class PairBatch:
     """Runs len(specs) pairs concurrently on `streams` CUDA streams (graph-captured)."""
 
-    def __init__(self, specs, streams: int = 4, use_graph: bool = True):
+    def __init__(self, specs, streams=4, use_graph: bool = True):
+        """streams: a count, or a list of torch.cuda.Stream to share with other batches
+        (their workspaces are shared too: batches sharing streams must not overlap)."""
         self.specs = list(specs)
-        self.nstreams = max(1, int(streams))
+        if isinstance(streams, (list, tuple)):
+            self._streams, self.nstreams = list(streams), len(streams)
+        else:
+            self._streams, self.nstreams = None, max(1, int(streams))
         self.use_graph = use_graph
         self._graphs = {}
         self._lock = threading.Lock()
-        self._streams = None
 
     def _pipelines(self, frames):
         import GenericPyramidalOpticalFlow as G
@@ -117,3 +122,109 @@ class PairBatch:
             g.replay()
             _graph._replayed_kernels += nk
             return static_out
+
+
+# ----------------------------------------------------------------------------- config 4
+# The batched workload: pairs of uneven sizes and methods, each method with its reference
+# calibration (examples/PyHSchunck_Fs3_4.py, denseLK_Fs2_0_PyrLvls2.py,
+# Farneback_Fs0_0_PyrLvls2.py, LiuSE_Farneback_Fs0_0_PyrLvls2.py).
+CONFIG4_SIZES = (128, 256, 512, 1024, 2048)
+CONFIG4_METHODS = ("hs", "lk", "fb", "ls")
+CONFIG4_FLOWS = ("poiseuille", "lamb_oseen", "fourier")
+
+
+def method_spec(method: str) -> PairSpec:
+    import Farneback_PyCL as F
+    import HornSchunck as HS
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    import denseLucasKanade_PyCL as LK
+    if method == "hs":
+        return PairSpec(3.4, lambda: HS.HSOpticalFlowAlgoAdapter([21], 600), 1, 1, key=("hs",))
+    if method == "lk":
+        return PairSpec(2.0, lambda: LK.denseLucasKanade_PyCl(), 2, 1, key=("lk",))
+    if method == "fb":
+        return PairSpec(0, lambda: F.Farneback_PyCL(), 2, 1, key=("fb",))
+    if method == "ls":  # Liu-Shen as the refiner of Farneback pyr2 (it cannot be the main adapter)
+        return PairSpec(0, lambda: F.Farneback_PyCL(), 2, 1, 0.48, lambda: LS.LiuShenOpticalFlowAlgoAdapter(10),
+                        key=("ls",))
+    raise ValueError(method)
+
+
+def config4_manifest(n=256, seed=0):
+    """n entries {size, method, flow, seed}, each field drawn uniformly from its set."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        out.append({"size": int(rng.choice(CONFIG4_SIZES)), "method": str(rng.choice(CONFIG4_METHODS)),
+                    "flow": str(rng.choice(CONFIG4_FLOWS)), "seed": int(seed * 100_000 + i)})
+    return out
+
+
+def pair_cost_of(e) -> float:
+    from .shard import pair_cost
+    return pair_cost(e["size"], e["method"])
+
+
+def render_entry(e):
+    """(frame1 u8, frame2 u8, U_gt, V_gt) of one manifest entry (max 4 px displacement;
+    the vortex core scales with the image, 60 px at 512^2)."""
+    from . import synthetic as S
+    n = e["size"]
+    density, diameter = {"hs": (0.05, 2.5), "lk": (0.08, 2.5)}.get(e["method"], (0.05, (2.0, 3.0)))
+    kw = {"core_radius": 60.0 * n / 512.0} if e["flow"] == "lamb_oseen" else {}
+    return S.piv_pair(n, n, e["flow"], e["seed"], density=density, diameter=diameter, noise=2.0, **kw)
+
+
+class BatchRunner:
+    """A manifest in chunks of `chunk` pairs, ordered by decreasing cost, each chunk one
+    multi-stream CUDA graph (PairBatch) on `streams` shared streams.  run() replays the
+    chunks in turn and returns every pair's (U, V) in manifest order."""
+
+    def __init__(self, entries, chunk=32, streams=4):
+        self.entries = list(entries)
+        self.order = sorted(range(len(self.entries)), key=lambda i: (-pair_cost_of(self.entries[i]), i))
+        self.chunk, self.nstreams = int(chunk), int(streams)
+        self._streams = [torch.cuda.Stream() for _ in range(self.nstreams)]
+        self._batches = []
+        for c in range(0, len(self.order), self.chunk):
+            idx = self.order[c:c + self.chunk]
+            specs = [method_spec(self.entries[i]["method"]) for i in idx]
+            self._batches.append((idx, PairBatch(specs, streams=self._streams)))
+
+    def run(self, frames):
+        outs = [None] * len(self.entries)
+        for idx, pb in self._batches:
+            res = pb.run([frames[i] for i in idx])
+            for i, r in zip(idx, res):
+                outs[i] = r
+        return outs
+
+
+def autotune(entries, frames, chunks=(16, 64, 256), streams=(2, 4, 8), reps=2, log=None):
+    """Times every (chunk, streams) candidate on the manifest (after its capture run) and
+    returns (best runner, {candidate: ms})."""
+    import gc
+    best, table = None, {}
+    for c in chunks:
+        for s in streams:
+            r = BatchRunner(entries, chunk=min(c, len(entries)), streams=s)
+            r.key = (c, s)
+            r.run(frames)  # capture
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                r.run(frames)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            table[(c, s)] = ms
+            if log:
+                log(f"chunk {c} streams {s}: {ms:.1f} ms")
+            if best is None or ms < table[best.key]:
+                best = r
+            else:
+                del r
+                gc.collect()
+    return best, table

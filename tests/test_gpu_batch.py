@@ -99,3 +99,33 @@ def test_batch_rejects_count_mismatch(torch_cuda):
     specs, _ = _specs()
     with pytest.raises(ValueError):
         PairBatch(specs).run([])
+
+
+def test_config4_runner_matches_single_pairs(torch_cuda):
+    """A small mixed manifest (all four methods, three sizes) through the chunked,
+    autotuned runner gives each pair's single-call result."""
+    torch = torch_cuda
+    import GenericPyramidalOpticalFlow as G
+    from ofb200 import graph
+    from ofb200.batch import autotune, method_spec, render_entry
+    entries = [{"size": s, "method": m, "flow": f, "seed": 70 + i}
+               for i, (s, m, f) in enumerate([(128, "hs", "poiseuille"), (256, "lk", "lamb_oseen"),
+                                              (256, "fb", "fourier"), (192, "ls", "fourier"),
+                                              (128, "lk", "fourier"), (256, "hs", "lamb_oseen")])]
+    rendered = [render_entry(e) for e in entries]
+    frames = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b, _, _ in rendered]
+    runner, table = autotune(entries, frames, chunks=(2, 6), streams=(1, 3), reps=1)
+    assert len(table) == 4
+    outs = runner.run(frames)
+    torch.cuda.synchronize()
+    graph.ENABLED = False
+    try:
+        for e, (a, b, _, _), (U, V) in zip(entries, rendered, outs):
+            sp = method_spec(e["method"])
+            opt = sp.make_opt() if sp.make_opt is not None else None
+            Uw, Vw = G.genericPyramidalOpticalFlow(a.astype(np.float32), b.astype(np.float32), sp.FILTER,
+                                                   sp.make_main(), sp.pyramidalLevels, sp.kLevels, sp.FILTER_OPT, opt)
+            assert np.array_equal(U.cpu().numpy(), Uw, equal_nan=True), e
+            assert np.array_equal(V.cpu().numpy(), Vw, equal_nan=True), e
+    finally:
+        graph.ENABLED = True
