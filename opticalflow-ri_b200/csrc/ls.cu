@@ -169,19 +169,22 @@ __device__ __forceinline__ double ls_err(const double* ss, int k, double inv_n) 
 // Stencil helpers of the sweep.
 //  - 2-term stencils (D, D^T, F, F^T) in float32 as 0 + w0*a + w1*b: with exact operand
 //    halves, one float32 rounding of the exact value equals the reference's double
-//    accumulation rounded to float32 (including the sign of zero);
+//    accumulation rounded to float32 (including the sign of zero; double rounding through
+//    53 bits is innocuous for a sum of two 24-bit values);
 //  - M (4 terms) and H (8 terms) keep the reference's double accumulation order; H uses
 //    'constant' 0 outside the image (the EDGE variant selects +0.0 there).
 constexpr long long LS_WAIT_LIMIT = 1ll << 22;
 
+// The weights (+-0.5, 1, +-0.25) are powers of two, so every product is exact and an add of
+// the product rounds exactly as a fused multiply-add does: each term is one FMA.
 __device__ __forceinline__ float st2(float a, float b, float wa, float wb) {
-  return __fadd_rn(__fadd_rn(0.0f, __fmul_rn(a, wa)), __fmul_rn(b, wb));
+  return __fmaf_rn(b, wb, __fmaf_rn(a, wa, 0.0f));
 }
 __device__ __forceinline__ float st_m(const double d[3][3]) {
-  double t = __dadd_rn(0.0, __dmul_rn(d[0][0], 0.25));
-  t = __dadd_rn(t, __dmul_rn(d[0][2], -0.25));
-  t = __dadd_rn(t, __dmul_rn(d[2][0], -0.25));
-  t = __dadd_rn(t, __dmul_rn(d[2][2], 0.25));
+  double t = __fma_rn(d[0][0], 0.25, 0.0);
+  t = __fma_rn(d[0][2], -0.25, t);
+  t = __fma_rn(d[2][0], -0.25, t);
+  t = __fma_rn(d[2][2], 0.25, t);
   return (float)t;
 }
 template <bool EDGE>
@@ -378,12 +381,15 @@ __global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__
   for (int s = 0; s < nsw; s++) {
     const int in = s & 1, out = in ^ 1;
     double au = 0.0, av = 0.0;
-    if (c >= 1 && c <= LB_RW - 2 && r1 > r0) {
+    // sweep s only needs the rows at least s + 1 from the region's edge (later sweeps
+    // read no others)
+    const int ra = r0 > 1 + s ? r0 : 1 + s, rb = r1 < LB_RH - 1 - s ? r1 : LB_RH - 1 - s;
+    if (c >= 1 && c <= LB_RW - 2 && rb > ra) {
       if (edge)
-        lb_strip<true>(LB_U(in), LB_V(in), LB_U(out), LB_V(out), sc, c, r0, r1 - r0, gx, y0 - LB_T + r0, H, W, h,
+        lb_strip<true>(LB_U(in), LB_V(in), LB_U(out), LB_V(out), sc, c, ra, rb - ra, gx, y0 - LB_T + ra, H, W, h,
                        own_col, au, av);
       else
-        lb_strip<false>(LB_U(in), LB_V(in), LB_U(out), LB_V(out), sc, c, r0, r1 - r0, gx, y0 - LB_T + r0, H, W,
+        lb_strip<false>(LB_U(in), LB_V(in), LB_U(out), LB_V(out), sc, c, ra, rb - ra, gx, y0 - LB_T + ra, H, W,
                         h, own_col, au, av);
     }
     if (!P.redo) {
