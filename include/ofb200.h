@@ -52,7 +52,7 @@ int of_last_error(char* buf, size_t n);
 
 /* ---------------------------------------------------------------------------------
  * A1 Gaussian prefilter — replaces gaussian_filterPx / convolveSeparableFilter
- * (src/gaussian_filter.py:54-94).  Separable K-tap FIR (K odd, 1..15), row pass then
+ * (src/gaussian_filter.py:54-94).  Separable K-tap FIR (K odd, 1..81; H, W >= K/2), row pass then
  * column pass, with the reference's border (left mirrored, right copied in order) and
  * float32 arithmetic order; bit-exact with the reference.  `taps` is a HOST array of K
  * floats (e.g. prepareGaussianKernel(sigma, K), src/gaussian_filter.py:47-52).
@@ -192,6 +192,27 @@ int of_fb_update_flow(const float* M, float* flowx, float* flowy, int H, int W, 
  * M_in and M_out must not alias (the blur reads a (2kh+1)^2 neighbourhood). */
 int of_fb_iteration(const float* M_in, float* M_out, const float* R0, const float* R1, float* flowx, float* flowy,
                     int H, int W, int pitch, const float* wk, int kh, int update_matrices, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * The Liu-Shen optical-flow-equation warp of the pyramid's level transition
+ * (updateNextPyramidalLevel with biLinear=False, src/GenericPyramidalOpticalFlow.py:
+ * 184-218).  Step 1 (of_warp_liushen_scatter): the integer shift
+ * out[y + floor(v + 0.5)][x + floor(u + 0.5)] = I[y][x] with numpy's rules (negative
+ * destinations wrap once; when several sources land on one pixel the last in row-major
+ * order wins; pixels nobody lands on keep I), and the sub-pixel parts du = u - floor(u +
+ * 0.5), dv likewise.  bad[0] / bad[1] (device ints) receive the row-major position of the
+ * first source whose destination row / column lies outside [-H, H) / [-W, W), or INT_MAX:
+ * the reference raises IndexError there.  Step 2: du, dv are smoothed with the reference's
+ * 73-tap gaussian_filter (of_prefilter_f32, prepareGaussianKernel(0.6 * 3, 73)).  Step 3
+ * (of_warp_liushen_ofe): out[y][x] = I - ((I[y][x+1] du[y][x+1] - I du) + (I[y+1][x]
+ * dv[y+1][x] - I dv)) for y < H-1, x < W-1 (float32, the reference's order); the last row
+ * and column are copied.  I is step 1's output.
+ * ------------------------------------------------------------------------------- */
+size_t of_warp_liushen_workspace_size(int H, int W);
+int of_warp_liushen_scatter(const float* I, const float* u, const float* v, float* out, float* du, float* dv, int H,
+                            int W, int pitch, int* bad, void* workspace, size_t workspace_bytes, void* stream);
+int of_warp_liushen_ofe(const float* I, const float* du, const float* dv, float* out, int H, int W, int pitch,
+                        void* stream);
 
 /* ---------------------------------------------------------------------------------
  * Learned warm start for Liu-Shen (no reference counterpart: the reference has no

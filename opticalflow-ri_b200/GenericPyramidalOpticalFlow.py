@@ -9,8 +9,10 @@ from this package are driven through their device path; any other object impleme
 the reference's adapter protocol (compute / getAlgoName / hasGenericPyramidalDefaults /
 getGenericPyramidalDefaults) is called with numpy arrays, exactly like the reference.
 
-Not supported yet: the Liu-Shen optical-flow-equation warp (biLinear=False,
-:188-220) raises NotImplementedError.  Progress prints are off unless OFB200_VERBOSE=1.
+Both warps of the level transition are supported: bilinear (biLinear=True) and Liu-Shen's
+optical-flow-equation warp (biLinear=False, :184-218), which, like the reference, edits
+the level's first frame in place (the caller's frame at the last level) and raises
+IndexError where the reference does.  Progress prints are off unless OFB200_VERBOSE=1.
 """
 import numpy as np
 
@@ -46,7 +48,12 @@ def updateNextPyramidalLevel(im1IterNext, im1IterPrev, im2IterNext, Uaccum, Vacc
     host = is_host(im1IterNext)
     d = to_device
     n1, n2, Ua, Va = d(im1IterNext), d(im2IterNext), d(Uaccum), d(Vaccum)
-    res = _transition(n1, tuple(im1IterPrev.shape), n2, Ua, Va, warping, biLinear, scale)
+    try:
+        res = _transition(n1, tuple(im1IterPrev.shape), n2, Ua, Va, warping, biLinear, scale)
+    finally:  # the Liu-Shen warp edits im1IterNext in place, as the reference does
+        if warping and not biLinear and host and isinstance(im1IterNext, np.ndarray) \
+                and im1IterNext.dtype == np.float32 and im1IterNext.flags.writeable:
+            np.copyto(im1IterNext, to_host(n1))
     return tuple(to_host(t) for t in res) if host else res
 
 
@@ -64,10 +71,40 @@ def _transition(n1, prev_shape, n2, Ua, Va, warping, biLinear, scale):
         vs = ops.scale(Va, sy) if scale else Va
     if warping:
         if not biLinear:
-            raise NotImplementedError("Liu-Shen optical-flow-equation warp (biLinear=False)")
+            _liushen_warp(n1, us, vs)
+            return n1, n2, us, vs, torch.zeros_like(n1), torch.zeros_like(n1)
         O0, O1 = ops.warp_pair(n1, n2, us, vs)
         return O0, O1, us, vs, torch.zeros_like(n1), torch.zeros_like(n1)
     return n1, n2, torch.zeros_like(n1), torch.zeros_like(n1), us, vs
+
+
+# the warp's smoothing: gaussian_filter(d, 0.6 * mask_size, truncate=4.0 / 0.6 * mask_size)
+# with mask_size 3 (:207-208), the reference's own separable filter (src/gaussian_filter.py:87-90)
+_LSW_SIGMA = 0.6 * 3
+_LSW_K = 2 * int(4.0 / 0.6 * 3 * _LSW_SIGMA + 0.5) + 1
+
+
+def _liushen_warp(n1, us, vs):
+    """:184-218 in place on n1: the integer scatter (IndexError beyond the image, as numpy
+    reports it), the 73-tap smoothing of the sub-pixel parts (IndexError below 36 pixels),
+    the optical-flow-equation correction.  Reads two ints back from the device."""
+    H, W = n1.shape
+    out, du, dv, bad = ops.warp_liushen_scatter(n1, us, vs)
+    bv, bu = (int(b) for b in bad.cpu().tolist())
+    for pos, axis, size, shift in ((bv, 0, H, vs), (bu, 1, W, us)):
+        if pos != 2 ** 31 - 1:  # the first out-of-range index, row-major, axis 0 first
+            y, x = divmod(pos, W)
+            f = float(np.floor(np.float32(float(shift[y, x])) + np.float32(0.5)))
+            idx = (y if axis == 0 else x) + int(f) if np.isfinite(f) else f
+            raise IndexError(f"index {idx} is out of bounds for axis {axis} with size {size}")
+    h = _LSW_K // 2
+    if W < h or H < h:  # convolveSeparableFilter reads image[i, j] for j < K // 2
+        n1.copy_(out)
+        ax, sz = (1, W) if W < h else (0, H)
+        raise IndexError(f"index {sz} is out of bounds for axis {ax} with size {sz}")
+    taps = prepareGaussianKernel(_LSW_SIGMA, _LSW_K)
+    n1.copy_(ops.warp_liushen_ofe(out, ops.prefilter(du, taps), ops.prefilter(dv, taps)))
+    return n1
 
 
 def _adapter_call(adapter, I0, I1, U, V):
@@ -108,8 +145,9 @@ def genericPyramidalOpticalFlow(im1, im2, FILTER, mainOFlowAlgoAdapter, pyramida
     keyable = all(a is None or hasattr(a, "_graph_key") for a in (main, opt))
     mk = main._graph_key(ncalls) if keyable else None
     ok = opt._graph_key(ncalls) if keyable and opt is not None else None
+    lswarp = bool(warping) and not bool(biLinear) and int(pyramidalLevels) * int(kLevels) > 1
     if keyable and mk is not None and (opt is None or ok is not None) and _graph.ENABLED \
-            and I1.stride(0) == I1.shape[1]:
+            and I1.stride(0) == I1.shape[1] and not lswarp:
         key = ("pyramid", tuple(I1.shape), I1.device.index, cfg, mk, ok)
         m2 = main._graph_clone(ncalls)
         o2 = None if opt is None else opt._graph_clone(ncalls)
@@ -124,7 +162,13 @@ def genericPyramidalOpticalFlow(im1, im2, FILTER, mainOFlowAlgoAdapter, pyramida
         if host:
             return to_host(Uacc), to_host(Vacc)
         return Uacc.clone(), Vacc.clone()
-    Uacc, Vacc = _pyramid_dev(I1, I2, cfg, main, opt)
+    try:
+        Uacc, Vacc = _pyramid_dev(I1, I2, cfg, main, opt)
+    finally:
+        # the Liu-Shen warp edits the last level's first frame, the caller's im1, in place
+        if lswarp and host and int(pyramidalLevels) > 1 and isinstance(im1, np.ndarray) \
+                and im1.dtype == np.float32 and im1.flags.writeable:
+            np.copyto(im1, to_host(I1))
     if host:
         return to_host(Uacc), to_host(Vacc)
     return Uacc, Vacc
@@ -168,9 +212,9 @@ def _pyramid_dev(I1, I2, cfg, mainOFlowAlgoAdapter, optionalOFlowAlgoAdapter):
         for k in range(kLevels):
             log('Level=', level, ' kIter=', k)
             if k > 0:
-                if warping:
-                    w1, w2, Uacc, Vacc, U, V = _transition(n1, tuple(n1.shape), n2, Uacc, Vacc, warping, biLinear,
-                                                           False)
+                if warping:  # on a copy of the level frame (:393)
+                    w1, w2, Uacc, Vacc, U, V = _transition(n1.clone(), tuple(n1.shape), n2, Uacc, Vacc, warping,
+                                                           biLinear, False)
                     if FILTER > 1:
                         work1, work2 = _prefilter(w1, FILTER, 3), _prefilter(w2, FILTER, 3)
                     else:

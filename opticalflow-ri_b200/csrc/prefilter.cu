@@ -11,10 +11,11 @@
 
 namespace ofb {
 
-constexpr int PF_TW = 64, PF_TH = 32, PF_MAXK = 15;
+constexpr int PF_TW = 64, PF_TH = 32, PF_MAXK = 15;  // the pyramid's prefilters (3 and 5 taps)
+constexpr int PF_MAXK_LARGE = 81;                     // the Liu-Shen warp's 73-tap smoothing
 
 struct PfTaps {
-  float k[PF_MAXK];
+  float k[PF_MAXK_LARGE];
 };
 
 // Border of convolveSeparableFilter (:62-66): coordinate c of a line of length n with
@@ -25,9 +26,9 @@ __device__ __forceinline__ int pf_map(int c, int n, int h) {
   return clampi(c, 0, n - 1);  // only reached for outputs outside the image
 }
 
-template <typename Tin>
+template <typename Tin, int MAXK>
 __global__ void __launch_bounds__(256) prefilter_kernel(const Tin* __restrict__ src, int sp, float* __restrict__ dst,
-                                                        int dp, int H, int W, PfTaps taps, int K) {
+                                                        int dp, int H, int W, const PfTaps taps, int K) {
   extern __shared__ float sm[];
   const int h = K >> 1;
   const int iw = PF_TW + 2 * h, ih = PF_TH + 2 * h;
@@ -46,8 +47,8 @@ __global__ void __launch_bounds__(256) prefilter_kernel(const Tin* __restrict__ 
     int ly = i / PF_TW, lx = i - ly * PF_TW;
     const float* t = tin + ly * iw + lx + 2 * h;
     float acc = 0.0f;
-#pragma unroll
-    for (int j = 0; j < PF_MAXK; j++)
+#pragma unroll(MAXK <= PF_MAXK ? MAXK : 8)
+    for (int j = 0; j < MAXK; j++)
       if (j < K) acc = __fadd_rn(acc, __fmul_rn(t[-j], taps.k[j]));
     trow[i] = acc;
   }
@@ -58,8 +59,8 @@ __global__ void __launch_bounds__(256) prefilter_kernel(const Tin* __restrict__ 
     if (y >= H || x >= W) continue;
     const float* t = trow + (ly + 2 * h) * PF_TW + lx;
     float acc = 0.0f;
-#pragma unroll
-    for (int j = 0; j < PF_MAXK; j++)
+#pragma unroll(MAXK <= PF_MAXK ? MAXK : 8)
+    for (int j = 0; j < MAXK; j++)
       if (j < K) acc = __fadd_rn(acc, __fmul_rn(t[-j * PF_TW], taps.k[j]));
     dst[(size_t)y * dp + x] = acc;
   }
@@ -69,7 +70,7 @@ template <typename Tin>
 static int launch_prefilter(const Tin* src, int sp, float* dst, int dp, int H, int W, const float* taps, int K,
                             void* stream, const char* name) {
   OF_REQUIRE(!bad_plane(src, H, W, sp) && !bad_plane(dst, H, W, dp), "%s: bad plane", name);
-  OF_REQUIRE(taps && K >= 1 && K <= PF_MAXK && (K & 1), "%s: K must be odd and <= %d", name, PF_MAXK);
+  OF_REQUIRE(taps && K >= 1 && K <= PF_MAXK_LARGE && (K & 1), "%s: K must be odd and <= %d", name, PF_MAXK_LARGE);
   OF_REQUIRE(H >= K / 2 && W >= K / 2, "%s: image smaller than the half kernel", name);
   OF_REQUIRE((const void*)src != (const void*)dst, "%s: src and dst alias", name);
   PfTaps t{};
@@ -77,7 +78,18 @@ static int launch_prefilter(const Tin* src, int sp, float* dst, int dp, int H, i
   int h = K / 2;
   size_t smem = sizeof(float) * ((size_t)(PF_TH + 2 * h) * (PF_TW + 2 * h) + (size_t)(PF_TH + 2 * h) * PF_TW);
   dim3 grid((W + PF_TW - 1) / PF_TW, (H + PF_TH - 1) / PF_TH);
-  prefilter_kernel<Tin><<<grid, 256, smem, as_stream(stream)>>>(src, sp, dst, dp, H, W, t, K);
+  if (K <= PF_MAXK) {
+    prefilter_kernel<Tin, PF_MAXK><<<grid, 256, smem, as_stream(stream)>>>(src, sp, dst, dp, H, W, t, K);
+  } else {
+    static bool attr = false;  // up to 83 KB of staged tile for 81 taps
+    if (!attr) {
+      cudaError_t e = cudaFuncSetAttribute(prefilter_kernel<Tin, PF_MAXK_LARGE>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+      if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "%s: %s", name, cudaGetErrorString(e));
+      attr = true;
+    }
+    prefilter_kernel<Tin, PF_MAXK_LARGE><<<grid, 256, smem, as_stream(stream)>>>(src, sp, dst, dp, H, W, t, K);
+  }
   return check_launch(name);
 }
 

@@ -9,6 +9,11 @@
 //     separable: moments along y per coarse column, evaluation at the fine rows, moments
 //     along x per fine row, evaluation at the fine columns; double throughout.
 //  A4 of_warp_pair_bilinear: doBiLinearWarping's round-half-even base, float64 weights.
+//  of_warp_liushen_*: the optical-flow-equation warp (biLinear=False): a last-writer-wins
+//     integer scatter (atomicMax of the source's row-major position per destination, then
+//     a gather) and the float32 optical-flow-equation correction.
+#include <climits>
+
 #include "common.cuh"
 
 namespace ofb {
@@ -311,6 +316,57 @@ __global__ void __launch_bounds__(256) spline_ex_kernel(const double* __restrict
   }
 }
 
+// ----------------------------------------------------------------------------- Liu-Shen warp
+__global__ void lsw_init_kernel(int* owner, int n, int* bad) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) owner[i] = -1;
+  if (i < 2) bad[i] = INT_MAX;
+}
+
+// numpy: usSwap = int32(xsMesh + floor(usNew + 0.5)) (float32 add and floor, exact
+// integer sum); dUsNew = usNew - floor(usNew + float32(0.5)).
+__global__ void lsw_owner_kernel(const float* __restrict__ u, const float* __restrict__ v, int H, int W, int pitch,
+                                 int* __restrict__ owner, float* __restrict__ du, float* __restrict__ dv,
+                                 int* __restrict__ bad) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  size_t i = (size_t)y * pitch + x;
+  const float fu = floorf(__fadd_rn(u[i], 0.5f)), fv = floorf(__fadd_rn(v[i], 0.5f));
+  du[i] = __fsub_rn(u[i], fu);
+  dv[i] = __fsub_rn(v[i], fv);
+  const int p = y * W + x;
+  // destinations beyond +-2^30 (or non-finite shifts) are out of range for any image
+  const bool okv = fv > -1073741824.0f && fv < 1073741824.0f, oku = fu > -1073741824.0f && fu < 1073741824.0f;
+  const int ty = okv ? y + (int)fv : INT_MIN, tx = oku ? x + (int)fu : INT_MIN;
+  const bool inv = okv && ty >= -H && ty < H, inu = oku && tx >= -W && tx < W;
+  if (!inv) atomicMin(&bad[0], p);
+  if (!inu) atomicMin(&bad[1], p);
+  if (inv && inu) atomicMax(&owner[(ty < 0 ? ty + H : ty) * W + (tx < 0 ? tx + W : tx)], p);
+}
+
+__global__ void lsw_gather_kernel(const float* __restrict__ I, const int* __restrict__ owner, float* __restrict__ out,
+                                  int H, int W, int pitch) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  const int o = owner[y * W + x];
+  out[(size_t)y * pitch + x] = o >= 0 ? I[(size_t)(o / W) * pitch + (o % W)] : I[(size_t)y * pitch + x];
+}
+
+__global__ void lsw_ofe_kernel(const float* __restrict__ I, const float* __restrict__ du, const float* __restrict__ dv,
+                               float* __restrict__ out, int H, int W, int pitch) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  size_t i = (size_t)y * pitch + x;
+  if (y == H - 1 || x == W - 1) {
+    out[i] = I[i];
+    return;
+  }
+  const float c = __fmul_rn(I[i], du[i]), cy = __fmul_rn(I[i], dv[i]);
+  const float tdx = __fsub_rn(__fmul_rn(I[i + 1], du[i + 1]), c);
+  const float tdy = __fsub_rn(__fmul_rn(I[i + pitch], dv[i + pitch]), cy);
+  out[i] = __fsub_rn(I[i], __fadd_rn(tdx, tdy));
+}
+
 // ----------------------------------------------------------------------------- warp
 __device__ __forceinline__ float warp_sample(const float* __restrict__ img, int H, int W, int pitch, float cy,
                                              float cx) {
@@ -455,4 +511,38 @@ extern "C" int of_warp_pair_bilinear(const float* I0, const float* I1, const flo
   OF_REQUIRE(!bad_plane(I0, H, W, pitch) && I1 && U && V && O0 && O1, "of_warp_pair_bilinear: bad plane");
   warp_pair_kernel<<<dim3((W + 255) / 256, H), 256, 0, as_stream(stream)>>>(I0, I1, U, V, O0, O1, H, W, pitch);
   return check_launch("of_warp_pair_bilinear");
+}
+
+extern "C" size_t of_warp_liushen_workspace_size(int H, int W) {
+  Sizer s;
+  s.take<int>((size_t)H * W);  // owner of each destination
+  return s.off;
+}
+
+extern "C" int of_warp_liushen_scatter(const float* I, const float* u, const float* v, float* out, float* du, float* dv,
+                                       int H, int W, int pitch, int* bad, void* workspace, size_t workspace_bytes,
+                                       void* stream) {
+  OF_REQUIRE(!bad_plane(I, H, W, pitch) && u && v && out && du && dv && bad, "of_warp_liushen_scatter: bad arguments");
+  OF_REQUIRE(out != I, "of_warp_liushen_scatter: out and I alias");
+  OF_REQUIRE((long long)H * W < INT_MAX, "of_warp_liushen_scatter: image too large");
+  size_t need = of_warp_liushen_workspace_size(H, W);
+  if (!workspace || workspace_bytes < need)
+    return set_error(OF_ERR_WORKSPACE, "of_warp_liushen_scatter: workspace too small (%zu < %zu)", workspace_bytes,
+                     need);
+  cudaStream_t st = as_stream(stream);
+  int* owner = Carver(workspace, workspace_bytes).take<int>((size_t)H * W);
+  const int n = H * W;
+  lsw_init_kernel<<<(n + 255) / 256, 256, 0, st>>>(owner, n, bad);
+  dim3 g((W + 127) / 128, H);
+  lsw_owner_kernel<<<g, 128, 0, st>>>(u, v, H, W, pitch, owner, du, dv, bad);
+  lsw_gather_kernel<<<g, 128, 0, st>>>(I, owner, out, H, W, pitch);
+  return check_launch("of_warp_liushen_scatter", 3);
+}
+
+extern "C" int of_warp_liushen_ofe(const float* I, const float* du, const float* dv, float* out, int H, int W,
+                                   int pitch, void* stream) {
+  OF_REQUIRE(!bad_plane(I, H, W, pitch) && du && dv && out && out != I, "of_warp_liushen_ofe: bad arguments");
+  dim3 g((W + 127) / 128, H);
+  lsw_ofe_kernel<<<g, 128, 0, as_stream(stream)>>>(I, du, dv, out, H, W, pitch);
+  return check_launch("of_warp_liushen_ofe");
 }

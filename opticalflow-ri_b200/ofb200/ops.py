@@ -19,7 +19,7 @@ from ._lib import FbPolyConsts, call, lib
 __all__ = [
     "prefilter", "u8_to_f32", "resize", "spline_upsample", "warp_pair", "accumulate", "scale", "hs_solve",
     "ls_solve", "lk_dense", "fb_blur", "fb_box5", "fb_polyexp", "fb_update_matrices", "fb_update_flow",
-    "fb_iteration", "workspace", "stream_ptr",
+    "fb_iteration", "workspace", "stream_ptr", "warp_liushen_scatter", "warp_liushen_ofe",
 ]
 
 _WS = {}
@@ -126,6 +126,30 @@ def warp_coords(img, coordsY, coordsX):
     out = torch.empty_like(img)
     call("of_warp_bilinear_coords", _plane(img, "img")[0], _plane(coordsY, "coordsY")[0],
          _plane(coordsX, "coordsX")[0], _plane(out, "out")[0], H, W, p, stream_ptr())
+    return out
+
+
+def warp_liushen_scatter(I, us, vs):
+    """Step 1 of the optical-flow-equation warp: (scattered image, du, dv, bad) with bad a
+    device int32[2] (first out-of-range destination row / column position, INT_MAX)."""
+    p = _same_pitch(I, us, vs)
+    H, W = I.shape
+    out, du, dv = torch.empty_like(I), torch.empty_like(I), torch.empty_like(I)
+    bad = torch.empty(2, dtype=torch.int32, device=I.device)
+    ws, wn = workspace(lib().of_warp_liushen_workspace_size(H, W), "lswarp")
+    call("of_warp_liushen_scatter", _plane(I, "I")[0], _plane(us, "us")[0], _plane(vs, "vs")[0],
+         _plane(out, "out")[0], _plane(du, "du")[0], _plane(dv, "dv")[0], H, W, p, ctypes.c_void_p(bad.data_ptr()),
+         ws, wn, stream_ptr())
+    return out, du, dv, bad
+
+
+def warp_liushen_ofe(I, du, dv):
+    """Step 3: the float32 optical-flow-equation correction of the scattered image."""
+    p = _same_pitch(I, du, dv)
+    H, W = I.shape
+    out = torch.empty_like(I)
+    call("of_warp_liushen_ofe", _plane(I, "I")[0], _plane(du, "du")[0], _plane(dv, "dv")[0], _plane(out, "out")[0],
+         H, W, p, stream_ptr())
     return out
 
 

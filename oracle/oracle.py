@@ -346,8 +346,10 @@ def lk_dense(I, J, U, V, halfWindow=13, Niter=5, asym=(0, 0, 0, 0), want_status=
 class HS:
     defaults = {"warping": True, "biLinear": True, "scaling": True}
 
-    def __init__(self, alphas, Niter):
+    def __init__(self, alphas, Niter, provideGenericPyramidalDefaults=True):
         self.alphas, self.Niter = list(alphas), Niter
+        if not provideGenericPyramidalDefaults:
+            self.defaults = None
 
     def compute(self, im1, im2, U, V):
         return hs_solve(im1, im2, U, V, self.alphas.pop(), self.Niter)
@@ -386,8 +388,38 @@ class FB:
         return farneback(im1, im2, U, V, **self.kw)
 
 
+def liushen_warp(im1, us, vs):
+    """The optical-flow-equation warp, in place on im1 (src/GenericPyramidalOpticalFlow.py:
+    184-218): numpy's scatter (IndexError beyond the image, negative destinations wrap,
+    the last source in row-major order wins), the sub-pixel parts smoothed by the
+    reference's own 73-tap gaussian_filter (src/gaussian_filter.py:87-90, which raises
+    IndexError below 36 pixels), then the float32 optical-flow-equation correction."""
+    H, W = im1.shape
+    ym, xm = np.meshgrid(np.arange(H, dtype=np.int32), np.arange(W, dtype=np.int32), indexing="ij")
+    usSwap = np.int32(xm + np.floor(us + 0.5))
+    vsSwap = np.int32(ym + np.floor(vs + 0.5))
+    dU = us - np.floor(us + np.float32(0.5))
+    dV = vs - np.floor(vs + np.float32(0.5))
+    im1[vsSwap, usSwap] = im1[ym, xm]
+    sigma, truncate = 0.6 * 3, 4.0 / 0.6 * 3
+    K = 2 * int(truncate * sigma + 0.5) + 1
+    h = K // 2
+    for P in (dU, dV):
+        if P.shape[1] < h:
+            raise IndexError(f"index {P.shape[1]} is out of bounds for axis 1 with size {P.shape[1]}")
+        if P.shape[0] < h:
+            raise IndexError(f"index {P.shape[0]} is out of bounds for axis 0 with size {P.shape[0]}")
+    taps = prepare_gaussian_kernel(sigma, K)
+    dU, dV = prefilter_taps(dU, taps), prefilter_taps(dV, taps)
+    tdx = im1[:-1, 1:] * dU[:-1, 1:] - im1[:-1, :-1] * dU[:-1, :-1]
+    tdy = im1[1:, :-1] * dV[1:, :-1] - im1[:-1, :-1] * dV[:-1, :-1]
+    im1[:-1, :-1] = im1[:-1, :-1] - (tdx + tdy)
+    return im1
+
+
 def _level_transition(im1_next, prev_shape, im2_next, Uacc, Vacc, warping, biLinear, scale):
-    """src/GenericPyramidalOpticalFlow.py:117-234 (bilinear-warp and no-warp branches)."""
+    """src/GenericPyramidalOpticalFlow.py:117-234.  The Liu-Shen warp (biLinear=False)
+    modifies im1_next in place, as the reference does."""
     H, W = im1_next.shape
     h, w = prev_shape
     if (h, w) != (H, W):
@@ -400,7 +432,9 @@ def _level_transition(im1_next, prev_shape, im2_next, Uacc, Vacc, warping, biLin
         vs *= np.float32(np.float32(H) / np.float32(h))
     if warping:
         if not biLinear:
-            raise NotImplementedError("Liu-Shen optical-flow-equation warp")
+            liushen_warp(im1_next, us, vs)
+            z = np.zeros((H, W), np.float32)
+            return im1_next, im2_next, us, vs, z, z.copy()
         O0, O1 = warp_pair(im1_next, im2_next, us, vs)
         z = np.zeros((H, W), np.float32)
         return O0, O1, us, vs, z, z.copy()
@@ -410,8 +444,7 @@ def _level_transition(im1_next, prev_shape, im2_next, Uacc, Vacc, warping, biLin
 
 def pyramid(im1, im2, FILTER, main, pyramidalLevels=1, kLevels=1, FILTER_OPT=None, opt=None, warping=True,
             biLinear=True, pyramidalIntermediateScaling=True, pyramidalScaling=False):
-    """genericPyramidalOpticalFlow (src/GenericPyramidalOpticalFlow.py:237-415), kLevels == 1."""
-    assert kLevels == 1
+    """genericPyramidalOpticalFlow (src/GenericPyramidalOpticalFlow.py:237-415)."""
     im1, im2 = _c32(im1), _c32(im2)
     d = main.defaults or {}
     warping = d.get("warping", warping)
@@ -445,10 +478,22 @@ def pyramid(im1, im2, FILTER, main, pyramidalLevels=1, kLevels=1, FILTER_OPT=Non
         elif opt is not None:
             o1, o2 = n1.copy(), n2
         prev_shape = k1.shape
-        U, V, _ = main.compute(k1, k2, U, V)
-        if opt is not None:
-            U, V, _ = opt.compute(o1.copy(), o2.copy(), U, V)
-        Uacc = Uacc + U
-        Vacc = Vacc + V
+        for k in range(kLevels):
+            if k > 0:  # :391-403 (note FILTER > 1 here, FILTER > 1e-3 above)
+                if warping:
+                    w1, w2, Uacc, Vacc, U, V = _level_transition(n1.copy(), n1.shape, n2, Uacc, Vacc, warping,
+                                                                 biLinear, False)
+                    if FILTER > 1:
+                        k1, k2 = prefilter(w1, FILTER, 3), prefilter(w2, FILTER, 3)
+                    else:
+                        k1, k2 = w1.copy(), w2
+                else:
+                    k1, k2, Uacc, Vacc, U, V = _level_transition(k1, k1.shape, k2, Uacc, Vacc, warping, biLinear,
+                                                                 False)
+            U, V, _ = main.compute(k1, k2, U, V)
+            if opt is not None:
+                U, V, _ = opt.compute(o1.copy(), o2.copy(), U, V)
+            Uacc = Uacc + U
+            Vacc = Vacc + V
         scale *= 2
     return Uacc, Vacc

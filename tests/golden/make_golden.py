@@ -181,9 +181,85 @@ def main():
                    ls.LiuShenOpticalFlowAlgoAdapter(10))
     out["pyr_hs_ls"] = dict(f0=a, f1=b, U=Ur, V=Vr)
 
+    out.update(liushen_warp_cases(R, rng))
+    only = sys.argv[sys.argv.index("--only") + 1].split(",") if "--only" in sys.argv else None
     for name, d in out.items():
+        if only and name not in only:
+            continue
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **d)
         print("wrote", name, os.path.getsize(os.path.join(HERE, f"{name}.npz")))
+
+
+def _in_bounds_field(rng, H, W, lo, hi):
+    """Random displacements whose rounded destinations stay below the last row / column
+    (the reference's scatter raises IndexError beyond them; negative ones wrap)."""
+    us = np.float32(rng.uniform(lo, hi, (H, W)))
+    vs = np.float32(rng.uniform(lo, hi, (H, W)))
+    xm, ym = np.meshgrid(np.arange(W), np.arange(H))
+    us = np.where(xm + np.floor(us + np.float32(0.5)) > W - 1, np.float32(W - 1 - xm) - np.float32(0.25), us)
+    vs = np.where(ym + np.floor(vs + np.float32(0.5)) > H - 1, np.float32(H - 1 - ym) - np.float32(0.25), vs)
+    return np.float32(us), np.float32(vs)
+
+
+def liushen_warp_cases(R, rng):
+    """The optical-flow-equation warp (biLinear=False, src/GenericPyramidalOpticalFlow.py:184-218)."""
+    from ofb200 import synthetic as S
+    G, hs, ls = R["GenericPyramidalOpticalFlow"], R["HornSchunck"], R["PhysicsBasedOpticalFlowLiuShen"]
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    out = {}
+    # the level transition: same size, and upsampled from half size with scaling
+    d = {}
+    for i, (H, W, h, w, scale) in enumerate([(40, 48, 40, 48, False), (48, 56, 24, 28, True), (36, 36, 36, 36, False)]):
+        I1 = f32(rng.uniform(0, 255, (H, W)))
+        I2 = f32(rng.uniform(0, 255, (H, W)))
+        if (h, w) == (H, W):
+            Ua, Va = _in_bounds_field(rng, H, W, -3.0, 3.0)
+        else:  # an accumulated field at half size whose upsampled, scaled copy stays in bounds
+            Ua, Va = _in_bounds_field(rng, h, w, -0.7, 0.7)
+            Ua = f32(np.where(np.arange(w)[None, :] >= w - 3, np.float32(-0.2), Ua))
+            Va = f32(np.where(np.arange(h)[:, None] >= h - 3, np.float32(-0.2), Va))
+        Z = np.zeros((h, w), np.float32)
+        prev = np.zeros((h, w), np.float32)
+        n1 = I1.copy()
+        o1, o2, ua, va, u0, v0 = quiet(G.updateNextPyramidalLevel, n1, prev, I2, Ua.copy(), Va.copy(), Z, Z, True,
+                                       False, scale)
+        d.update({f"I1_{i}": I1, f"I2_{i}": I2, f"Ua_{i}": Ua, f"Va_{i}": Va, f"O1_{i}": o1, f"O2_{i}": o2,
+                  f"ua_{i}": ua, f"va_{i}": va, f"spec_{i}": np.array([H, W, h, w, int(scale)])})
+    # a destination beyond the last column raises IndexError in the reference
+    I1 = f32(rng.uniform(0, 255, (8, 8)))
+    Ua = np.zeros((8, 8), np.float32)
+    Ua[3, 7] = 0.75
+    try:
+        quiet(G.updateNextPyramidalLevel, I1.copy(), I1, I1.copy(), Ua, np.zeros_like(Ua), Ua, Ua, True, False, False)
+        d["raises"] = np.array(0)
+    except IndexError:
+        d["raises"] = np.array(1)
+    d["bad_I1"], d["bad_Ua"] = I1, Ua
+    # images smaller than the 73-tap filter's half width raise IndexError after the scatter
+    I1 = f32(rng.uniform(0, 255, (40, 30)))
+    n1 = I1.copy()
+    Z = np.zeros_like(I1)
+    try:
+        quiet(G.updateNextPyramidalLevel, n1, I1, I1.copy(), Z, Z, Z, Z, True, False, False)
+        d["small_raises"] = np.array(0)
+    except IndexError as e:
+        d["small_raises"] = np.array(1)
+        d["small_msg"] = np.array(str(e))
+    out["warp_liushen"] = d
+    # full pipeline: HS (adapter defaults off) with the Liu-Shen warp, 2 levels, kLevels 2, LS refine
+    for seed in range(20, 60):
+        a, b, Ug, Vg = S.piv_pair(128, 128, "lamb_oseen", seed=seed, core_radius=12, max_disp=1.5)
+        a, b = f32(a), f32(b)
+        a_in = a.copy()
+        try:
+            Ur, Vr = quiet(G.genericPyramidalOpticalFlow, a_in, b, 3.4,
+                           hs.HSOpticalFlowAlgoAdapter([21, 45, 33, 17], 50, provideGenericPyramidalDefaults=False), 2,
+                           2, 0.48, ls.LiuShenOpticalFlowAlgoAdapter(10), True, False, True, True)
+        except IndexError:
+            continue
+        out["pyr_hs_lswarp"] = dict(f0=a, f1=b, U=Ur, V=Vr, f0_after=a_in, seed=np.array(seed))
+        break
+    return out
 
 
 if __name__ == "__main__":

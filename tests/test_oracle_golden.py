@@ -92,3 +92,40 @@ def test_pyramid_hs_ls():
     g = golden("pyr_hs_ls")
     U, V = O.pyramid(g["f0"], g["f1"], 3.4, O.HS([21, 45], 100), 2, 1, 0.48, O.LS(10))
     assert np.abs(U - g["U"]).max() <= 1e-5 and np.abs(V - g["V"]).max() <= 1e-5
+
+
+def test_liushen_warp_transition():
+    """updateNextPyramidalLevel with biLinear=False: the warp alone is bit-exact on the
+    reference's upsampled fields; the whole transition (spline within 1 ulp) to 1e-3."""
+    g = golden("warp_liushen")
+    for i in range(3):
+        H, W, h, w, scale = (int(x) for x in g[f"spec_{i}"])
+        out = O.liushen_warp(g[f"I1_{i}"].copy(), g[f"ua_{i}"], g[f"va_{i}"])
+        assert np.array_equal(out, g[f"O1_{i}"]), i
+        o1, o2, ua, va, u0, v0 = O._level_transition(g[f"I1_{i}"].copy(), (h, w), g[f"I2_{i}"], g[f"Ua_{i}"],
+                                                     g[f"Va_{i}"], True, False, bool(scale))
+        assert np.abs(ua - g[f"ua_{i}"]).max() <= 1e-5 and np.abs(o1 - g[f"O1_{i}"]).max() <= 1e-3, i
+        assert np.array_equal(o2, g[f"I2_{i}"]) and not u0.any() and not v0.any()
+
+
+def test_liushen_warp_index_errors():
+    g = golden("warp_liushen")
+    assert int(g["raises"]) == 1 and int(g["small_raises"]) == 1
+    Ua = g["bad_Ua"]
+    with pytest.raises(IndexError, match="out of bounds for axis 1 with size 8"):
+        O.liushen_warp(g["bad_I1"].copy(), Ua, np.zeros_like(Ua))
+    z = np.zeros((40, 30), np.float32)
+    with pytest.raises(IndexError) as e:
+        O.liushen_warp(np.ones((40, 30), np.float32), z, z)
+    assert str(e.value) == str(g["small_msg"])
+
+
+def test_pyramid_hs_liushen_warp_klevels():
+    """HS without adapter defaults, the Liu-Shen warp, 2 levels x 2 iterations, LS refine;
+    the caller's first frame is edited in place as in the reference."""
+    g = golden("pyr_hs_lswarp")
+    f0 = g["f0"].copy()
+    U, V = O.pyramid(f0, g["f1"], 3.4, O.HS([21, 45, 33, 17], 50, provideGenericPyramidalDefaults=False), 2, 2, 0.48,
+                     O.LS(10), True, False, True, True)
+    assert np.abs(U - g["U"]).max() <= 1e-3 and np.abs(V - g["V"]).max() <= 1e-3
+    assert np.abs(f0 - g["f0_after"]).max() <= 1e-3 * np.abs(g["f0_after"]).max()
