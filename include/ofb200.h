@@ -63,8 +63,10 @@ int of_prefilter_f32(const float* src, int src_pitch, float* dst, int dst_pitch,
 int of_prefilter_u8(const uint8_t* src, int src_pitch, float* dst, int dst_pitch, int H, int W,
                     const float* taps, int K, void* stream);
 
-/* uint8 -> float32 plane conversion (the examples' imread(...).astype(np.float32)). */
+/* uint8 / uint16 -> float32 plane conversion (the examples' imread(...).astype(np.float32);
+ * 10- and 12-bit PIV frames arrive in 16-bit containers). */
 int of_u8_to_f32(const uint8_t* src, int src_pitch, float* dst, int dst_pitch, int H, int W, void* stream);
+int of_u16_to_f32(const uint16_t* src, int src_pitch, float* dst, int dst_pitch, int H, int W, void* stream);
 
 /* ---------------------------------------------------------------------------------
  * A2 antialiased resize — replaces imresize (src/GenericPyramidalOpticalFlow.py:66-67,

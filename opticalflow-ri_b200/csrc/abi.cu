@@ -81,8 +81,8 @@ int check_launch(const char* what, long long nlaunch) {
   return OF_OK;
 }
 
-__global__ void u8_to_f32_kernel(const uint8_t* __restrict__ src, int sp, float* __restrict__ dst, int dp, int H,
-                                 int W) {
+template <typename T>
+__global__ void to_f32_kernel(const T* __restrict__ src, int sp, float* __restrict__ dst, int dp, int H, int W) {
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
   if (x < W) dst[(size_t)y * dp + x] = (float)src[(size_t)y * sp + x];
 }
@@ -125,8 +125,16 @@ extern "C" int of_u8_to_f32(const uint8_t* src, int src_pitch, float* dst, int d
                             void* stream) {
   OF_REQUIRE(!bad_plane(src, H, W, src_pitch) && !bad_plane(dst, H, W, dst_pitch), "of_u8_to_f32: bad plane");
   dim3 grid((W + 255) / 256, H);
-  u8_to_f32_kernel<<<grid, 256, 0, as_stream(stream)>>>(src, src_pitch, dst, dst_pitch, H, W);
+  to_f32_kernel<uint8_t><<<grid, 256, 0, as_stream(stream)>>>(src, src_pitch, dst, dst_pitch, H, W);
   return check_launch("of_u8_to_f32");
+}
+
+extern "C" int of_u16_to_f32(const uint16_t* src, int src_pitch, float* dst, int dst_pitch, int H, int W,
+                             void* stream) {
+  OF_REQUIRE(!bad_plane(src, H, W, src_pitch) && !bad_plane(dst, H, W, dst_pitch), "of_u16_to_f32: bad plane");
+  dim3 grid((W + 255) / 256, H);
+  to_f32_kernel<uint16_t><<<grid, 256, 0, as_stream(stream)>>>(src, src_pitch, dst, dst_pitch, H, W);
+  return check_launch("of_u16_to_f32");
 }
 
 extern "C" int of_accumulate(float* dst, const float* src, int H, int W, int pitch, void* stream) {

@@ -42,6 +42,7 @@ _SIGS = {
     "of_prefilter_f32": ([_P, _I, _P, _I, _I, _I, _P, _I, _P], _I),
     "of_prefilter_u8": ([_P, _I, _P, _I, _I, _I, _P, _I, _P], _I),
     "of_u8_to_f32": ([_P, _I, _P, _I, _I, _I, _P], _I),
+    "of_u16_to_f32": ([_P, _I, _P, _I, _I, _I, _P], _I),
     "of_resize_workspace_size": ([_I, _I, _I, _I, _I], _Z),
     "of_resize": ([_P, _I, _I, _I, _P, _I, _I, _I, _I, _P, _Z, _P], _I),
     "of_spline_workspace_size": ([_I, _I, _I, _I], _Z),

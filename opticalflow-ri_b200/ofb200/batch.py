@@ -84,7 +84,7 @@ class PairBatch:
             with torch.cuda.stream(st):
                 main = spec.make_main()
                 opt = spec.make_opt() if spec.make_opt is not None else None
-                if a.dtype == torch.uint8:
+                if a.dtype in (torch.uint8, torch.uint16):
                     a, b = ops.u8_to_f32(a), ops.u8_to_f32(b)
                 outs[i] = G._pyramid_dev(a, b, _cfg_for(spec, main), main, opt)
         for s in self._streams:

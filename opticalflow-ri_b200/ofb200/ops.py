@@ -82,10 +82,15 @@ def prefilter(src: torch.Tensor, taps, out: torch.Tensor | None = None) -> torch
 
 
 def u8_to_f32(src: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """uint8 or uint16 (10/12-bit frames) plane -> float32 plane."""
     H, W = src.shape
     out = _new(H, W, src) if out is None else out
-    s, _, _, sp = _plane(src, "u8_to_f32.src", torch.uint8)
     d, _, _, dp = _plane(out, "u8_to_f32.out")
+    if src.dtype == torch.uint16:
+        s, _, _, sp = _plane(src, "u16_to_f32.src", torch.uint16)
+        call("of_u16_to_f32", s, sp, d, dp, H, W, stream_ptr())
+        return out
+    s, _, _, sp = _plane(src, "u8_to_f32.src", torch.uint8)
     call("of_u8_to_f32", s, sp, d, dp, H, W, stream_ptr())
     return out
 

@@ -129,3 +129,11 @@ def test_config4_runner_matches_single_pairs(torch_cuda):
             assert np.array_equal(V.cpu().numpy(), Vw, equal_nan=True), e
     finally:
         graph.ENABLED = True
+
+
+def test_u16_frames_convert_on_device(torch_cuda):
+    torch = torch_cuda
+    from ofb200 import ops
+    a = np.random.default_rng(3).integers(0, 4096, (33, 70)).astype(np.uint16)
+    got = ops.u8_to_f32(torch.from_numpy(a).cuda())
+    assert np.array_equal(got.cpu().numpy(), a.astype(np.float32))
