@@ -235,6 +235,11 @@ int of_warp_liushen_ofe(const float* I, const float* du, const float* dv, float*
 int of_cnn_conv3x3(const void* x, int n, int H, int W, int cin, int x_ctot, int x_coff, const void* w, int cout,
                    const float* bias, int flags, void* y, int y_ctot, int y_coff, int cout_store, unsigned* err,
                    void* stream);
+/* dw[tap][co][ci] += sum_p dy[p][co] * x[p + tap][ci] on the tensor cores (tcgen05, both
+ * operands MN-major from NHWC, f32 accumulate, split over pixel ranges and added with
+ * atomics).  W a divisor or a multiple of 64, H likewise for 64 / min(W, 64); cin, cout <= 512. */
+int of_cnn_conv3x3_wgrad_tc(const void* x, int x_ctot, int x_coff, const void* dy, int dy_ctot, int dy_coff, int n,
+                            int H, int W, int cin, int cout, float* dw, unsigned* err, void* stream);
 /* dw[tap][co][ci] += sum_p dy[p][co] * x[p + tap][ci]   (f32, CUDA cores). */
 int of_cnn_conv3x3_wgrad(const void* x, int x_ctot, int x_coff, const void* dy, int dy_ctot, int dy_coff, int n,
                          int H, int W, int cin, int cout, float* dw, void* stream);

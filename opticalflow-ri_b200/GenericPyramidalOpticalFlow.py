@@ -18,7 +18,7 @@ import numpy as np
 
 from gaussian_filter import prepareGaussianKernel
 from ofb200 import graph as _graph
-from ofb200 import ops, to_device, is_host, to_host, log, _torch
+from ofb200 import ops, to_device, is_host, to_host, to_host_pair, log, _torch
 
 __all__ = ["genericPyramidalOpticalFlow", "updateNextPyramidalLevel", "doBiLinearWarping", "imresize"]
 
@@ -125,8 +125,18 @@ def genericPyramidalOpticalFlow(im1, im2, FILTER, mainOFlowAlgoAdapter, pyramida
     state changes exactly as in the reference (Horn-Schunck pops one alpha per level)."""
     host = is_host(im1)
     dev = getattr(mainOFlowAlgoAdapter, "device", None)
-    I1 = to_device(im1, dev)
-    I2 = to_device(im2, I1.device)
+    if host:  # uploaded below: straight into the graph's inputs, or to_device on the eager path
+        torch = _torch()
+        a1 = np.ascontiguousarray(im1, np.float32)
+        a2 = np.ascontiguousarray(im2, np.float32)
+        if a1.ndim != 2 or a1.shape != a2.shape:
+            raise ValueError("expected two 2-D images of one shape")
+        gdev = dev or torch.device("cuda", torch.cuda.current_device())
+        shape, devidx, dense = a1.shape, gdev.index, True
+    else:
+        I1 = to_device(im1, dev)
+        I2 = to_device(im2, I1.device)
+        shape, devidx, dense = tuple(I1.shape), I1.device.index, I1.stride(0) == I1.shape[1]
     if mainOFlowAlgoAdapter.hasGenericPyramidalDefaults():
         dm = mainOFlowAlgoAdapter.getGenericPyramidalDefaults()
         if dm is not None:
@@ -146,22 +156,24 @@ def genericPyramidalOpticalFlow(im1, im2, FILTER, mainOFlowAlgoAdapter, pyramida
     mk = main._graph_key(ncalls) if keyable else None
     ok = opt._graph_key(ncalls) if keyable and opt is not None else None
     lswarp = bool(warping) and not bool(biLinear) and int(pyramidalLevels) * int(kLevels) > 1
-    if keyable and mk is not None and (opt is None or ok is not None) and _graph.ENABLED \
-            and I1.stride(0) == I1.shape[1] and not lswarp:
-        key = ("pyramid", tuple(I1.shape), I1.device.index, cfg, mk, ok)
+    if keyable and mk is not None and (opt is None or ok is not None) and _graph.ENABLED and dense and not lswarp:
+        key = ("pyramid", tuple(shape), devidx, cfg, mk, ok)
         m2 = main._graph_clone(ncalls)
         o2 = None if opt is None else opt._graph_clone(ncalls)
 
         def fn(a, b):
             return _pyramid_dev(a, b, cfg, m2._graph_clone(ncalls), None if o2 is None else o2._graph_clone(ncalls))
 
-        Uacc, Vacc = _graph.CACHE.run(key, fn, [I1, I2])
+        Uacc, Vacc = _graph.CACHE.run(key, fn, [a1, a2] if host else [I1, I2], device=devidx)
         main._graph_consume(ncalls)
         if opt is not None:
             opt._graph_consume(ncalls)
         if host:
-            return to_host(Uacc), to_host(Vacc)
+            return to_host_pair(Uacc, Vacc)
         return Uacc.clone(), Vacc.clone()
+    if host:
+        I1 = to_device(a1 if a1 is not im1 else im1, dev)
+        I2 = to_device(a2, I1.device)
     try:
         Uacc, Vacc = _pyramid_dev(I1, I2, cfg, main, opt)
     finally:

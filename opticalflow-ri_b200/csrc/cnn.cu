@@ -248,6 +248,152 @@ __global__ void __launch_bounds__(CV_THREADS, 1)
   }
 }
 
+// ----------------------------------------------------------------------------- wgrad, tensor cores
+// dW[tap] = sum over pixels of dY[p] (x) X[p + tap]: per tap a GEMM whose K is the pixel
+// count.  NHWC keeps the channels contiguous, so both operands are MN-major: a TMA box of
+// 64 channels x 64 pixels lands as 64 rows of 128 B (128-byte swizzle), which is the
+// canonical MN-major layout (8-row groups 1024 B apart, 64-channel atoms 8 KB apart).
+// A is the wider channel side (M = 128, channels past its end are zero-filled by TMA and
+// their rows ignored), B the narrower (N <= 256).  X is shifted by the tap through the box
+// coordinates (zero padding from TMA's out-of-bounds fill).  CTAs split the pixel range;
+// each adds its 128 x N partial sums into dW with atomics.
+constexpr int WT_KP = 64;  // pixels per K chunk
+constexpr int WT_STAGES = 4;
+
+struct WgParams {
+  int n, H, W, bw, bh, nb, tiles_x, tiles_per_group, nchunk;  // pixel chunk geometry
+  int chunks_per_cta, mtiles, ntiles;
+  int a_is_dy, a_ch, b_ch;   // channel counts of the A and B sides
+  int nmma, batoms;          // MMA N and 64-channel atoms loaded for B
+  int cin, cout;
+  float* dw;
+  unsigned* err;
+  uint32_t a_bytes, b_bytes, stage_bytes, tmem_cols;
+};
+
+// Shared-memory descriptor of a MN-major operand with the 128-byte swizzle: 64-element atoms
+// `lbo` bytes apart along M/N, 8-row K groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t umma_desc_mn128(uint32_t saddr, uint32_t lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
+}
+
+__host__ __device__ inline uint32_t umma_idesc_bf16_mn(int m, int n) {
+  return umma_idesc_bf16(m, n) | (1u << 15) | (1u << 16);  // A and B MN-major
+}
+
+__global__ void __launch_bounds__(CV_THREADS, 1)
+    wgrad_tc_kernel(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
+                    const WgParams p) {
+  extern __shared__ uint8_t wg_smem_raw[];
+  __shared__ __align__(8) uint64_t full[WT_STAGES], empty[WT_STAGES], accf;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(wg_smem_raw) + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tap = blockIdx.z, mt = blockIdx.y / p.ntiles, nt = blockIdx.y - mt * p.ntiles;
+  const int m0 = mt * 128, n0 = nt * 256;
+  const int c0 = blockIdx.x * p.chunks_per_cta;
+  const int c1 = c0 + p.chunks_per_cta < p.nchunk ? c0 + p.chunks_per_cta : p.nchunk;
+  const int kiters = c1 > c0 ? c1 - c0 : 0;
+  const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < WT_STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&accf, 1);
+    abort_flag = *reinterpret_cast<volatile unsigned*>(p.err) != 0u;
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(p.tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int it = 0; it < kiters && !abort_flag; it++) {
+        const int s = it % WT_STAGES;
+        if (!cv_wait(&empty[s], ((uint32_t)(it / WT_STAGES) & 1u) ^ 1u, &abort_flag)) {
+          atomicOr(p.err, 1u);
+          abort_flag = 1;
+          break;
+        }
+        const int ch = c0 + it, grp = ch / p.tiles_per_group, t_in = ch - grp * p.tiles_per_group;
+        const int ty = t_in / p.tiles_x, tx = t_in - ty * p.tiles_x;
+        const int x0 = tx * p.bw, y0 = ty * p.bh, img0 = grp * p.nb;
+        // the A side is dY (unshifted) or X (shifted), the B side the other
+        const int ax = p.a_is_dy ? x0 : x0 + dx, ay = p.a_is_dy ? y0 : y0 + dy;
+        const int bx = p.a_is_dy ? x0 + dx : x0, by = p.a_is_dy ? y0 + dy : y0;
+        uint8_t* a = smem + (size_t)s * p.stage_bytes;
+        mbar_expect_tx(&full[s], p.a_bytes + p.b_bytes);
+        tma_load_4d(a, &tm_a, m0, ax, ay, img0, &full[s]);
+        tma_load_4d(a + 8192, &tm_a, m0 + 64, ax, ay, img0, &full[s]);
+        for (int j = 0; j < p.batoms; j++)
+          tma_load_4d(a + p.a_bytes + j * 8192, &tm_b, n0 + 64 * j, bx, by, img0, &full[s]);
+        issued = it + 1;
+      }
+      for (int it = issued > WT_STAGES ? issued - WT_STAGES : 0; it < issued; it++)
+        if (!cv_wait(&full[it % WT_STAGES], (uint32_t)(it / WT_STAGES) & 1u, nullptr)) atomicOr(p.err, 2u);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_bf16_mn(128, p.nmma);
+      for (int it = 0; it < kiters; it++) {
+        const int s = it % WT_STAGES;
+        if (!cv_wait(&full[s], (uint32_t)(it / WT_STAGES) & 1u, &abort_flag)) {
+          atomicOr(p.err, 4u);
+          abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t a = smem_u32(smem + (size_t)s * p.stage_bytes), b = a + p.a_bytes;
+        const uint64_t ad = umma_desc_mn128(a, 8192), bd = umma_desc_mn128(b, 8192);
+        for (int kk = 0; kk < WT_KP / 16; kk++)  // 16 pixels = two 8-row groups: +2048 B (128 descriptor units)
+          umma_bf16(tmem, ad + 128ull * kk, bd + 128ull * kk, idesc, (it | kk) != 0);
+        umma_commit(&empty[s]);
+      }
+      umma_commit(&accf);
+    }
+    __syncwarp();
+  } else {
+    const int q = warp & 3;
+    const int m = q * 32 + lane;
+    const bool ok = cv_wait(&accf, 0u, nullptr);
+    if (!ok) atomicOr(p.err, 8u);
+    tc_fence_after();
+    const int am = m0 + m;  // this thread's A-side channel
+    if (ok && !abort_flag && kiters > 0) {
+      for (int c = 0; c < p.nmma; c += 16) {
+        uint32_t r[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, r);
+        if (am >= p.a_ch) continue;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const int bn = n0 + c + j;
+          if (bn >= p.b_ch) break;
+          const int co = p.a_is_dy ? am : bn, ci = p.a_is_dy ? bn : am;
+          atomicAdd(&p.dw[((size_t)tap * p.cout + co) * p.cin + ci], __uint_as_float(r[j]));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(p.tmem_cols) : "memory");
+  }
+}
+
 // ----------------------------------------------------------------------------- wgrad
 // dW[tap][co][ci] += sum over pixels p of dY[p][co] * X[p + tap][ci]  (zero outside the
 // image).  A CTA owns a 32 (co) x 32 (ci) block of all 9 taps and walks 64-pixel row
@@ -670,4 +816,85 @@ extern "C" int of_cnn_split_flow(const float* flow, int h, int w, float* u, floa
   OF_REQUIRE(flow && u && v && h > 0 && w > 0 && pitch >= w, "of_cnn_split_flow: bad arguments");
   split_flow_kernel<<<blocks_for((long long)h * w), 256, 0, as_stream(stream)>>>(flow, h, w, u, v, pitch);
   return check_launch("of_cnn_split_flow");
+}
+
+extern "C" int of_cnn_conv3x3_wgrad_tc(const void* x, int x_ctot, int x_coff, const void* dy, int dy_ctot, int dy_coff,
+                                       int n, int H, int W, int cin, int cout, float* dw, unsigned* err, void* stream) {
+  OF_REQUIRE(x && dy && dw && err && n > 0 && H > 0 && W > 0 && cin > 0 && cout > 0 && cin <= 512 && cout <= 512,
+             "of_cnn_conv3x3_wgrad_tc: bad arguments");
+  OF_REQUIRE(x_ctot % 8 == 0 && x_coff % 8 == 0 && dy_ctot % 8 == 0 && dy_coff % 8 == 0 && x_coff + cin <= x_ctot &&
+                 dy_coff + cout <= dy_ctot,
+             "of_cnn_conv3x3_wgrad_tc: channel slices");
+  int bw = W < WT_KP ? W : WT_KP;
+  OF_REQUIRE(WT_KP % bw == 0 && W % bw == 0, "of_cnn_conv3x3_wgrad_tc: width %d", W);
+  int bh = WT_KP / bw < H ? WT_KP / bw : H;
+  OF_REQUIRE(H % bh == 0 && (WT_KP / bw) % bh == 0, "of_cnn_conv3x3_wgrad_tc: height %d", H);
+  int nb = WT_KP / (bw * bh);
+  OF_REQUIRE(n % nb == 0, "of_cnn_conv3x3_wgrad_tc: %d images of %d x %d", n, H, W);
+  WgParams p;
+  p.n = n;
+  p.H = H;
+  p.W = W;
+  p.bw = bw;
+  p.bh = bh;
+  p.nb = nb;
+  p.tiles_x = W / bw;
+  p.tiles_per_group = (W / bw) * (H / bh);
+  p.nchunk = (n / nb) * p.tiles_per_group;
+  p.a_is_dy = cout >= cin;
+  p.a_ch = p.a_is_dy ? cout : cin;
+  p.b_ch = p.a_is_dy ? cin : cout;
+  p.mtiles = (p.a_ch + 127) / 128;
+  p.ntiles = (p.b_ch + 255) / 256;
+  int nb_last = p.b_ch - (p.ntiles - 1) * 256;  // every N tile uses the same MMA N: the largest needed
+  int nmax = p.ntiles > 1 ? 256 : nb_last;
+  p.nmma = (nmax + 15) / 16 * 16;
+  p.batoms = (p.nmma + 63) / 64;
+  p.cin = cin;
+  p.cout = cout;
+  p.dw = dw;
+  p.err = err;
+  p.a_bytes = 2 * 8192;
+  p.b_bytes = (uint32_t)p.batoms * 8192;
+  p.stage_bytes = p.a_bytes + p.b_bytes;
+  p.tmem_cols = p.nmma <= 32 ? 32 : (p.nmma <= 64 ? 64 : (p.nmma <= 128 ? 128 : 256));
+  // split the pixel chunks so that about 4 CTAs per SM run, at least 8 chunks each
+  const long long tiles = 9LL * p.mtiles * p.ntiles;
+  long long ks = (4LL * kNumSMs + tiles - 1) / tiles;
+  if (ks > p.nchunk / 8) ks = p.nchunk / 8;
+  if (ks < 1) ks = 1;
+  p.chunks_per_cta = (int)((p.nchunk + ks - 1) / ks);
+  ks = (p.nchunk + p.chunks_per_cta - 1) / p.chunks_per_cta;
+  CUtensorMap tma, tmb;
+  {
+    const void* ap = p.a_is_dy ? dy : x;
+    int act = p.a_is_dy ? dy_ctot : x_ctot, aco = p.a_is_dy ? dy_coff : x_coff;
+    uint64_t dims[4] = {(uint64_t)p.a_ch, (uint64_t)W, (uint64_t)H, (uint64_t)n};
+    uint64_t st[3] = {(uint64_t)act * 2, (uint64_t)W * act * 2, (uint64_t)H * W * act * 2};
+    uint32_t box[4] = {64, (uint32_t)bw, (uint32_t)bh, (uint32_t)nb};
+    int rc = tmap_bf16(&tma, static_cast<const bf16*>(ap) + aco, 4, dims, st, box, 128);
+    if (rc) return rc;
+  }
+  {
+    const void* bp = p.a_is_dy ? x : dy;
+    int bct = p.a_is_dy ? x_ctot : dy_ctot, bco = p.a_is_dy ? x_coff : dy_coff;
+    uint64_t dims[4] = {(uint64_t)p.b_ch, (uint64_t)W, (uint64_t)H, (uint64_t)n};
+    uint64_t st[3] = {(uint64_t)bct * 2, (uint64_t)W * bct * 2, (uint64_t)H * W * bct * 2};
+    uint32_t box[4] = {64, (uint32_t)bw, (uint32_t)bh, (uint32_t)nb};
+    int rc = tmap_bf16(&tmb, static_cast<const bf16*>(bp) + bco, 4, dims, st, box, 128);
+    if (rc) return rc;
+  }
+  size_t smem = 1024 + (size_t)WT_STAGES * p.stage_bytes;
+  size_t floor_smem = (size_t)p.tmem_cols * 456 + 1024;  // resident CTAs never exceed 512 TMEM columns
+  if (smem < floor_smem) smem = floor_smem;
+  static size_t attr_smem = 0;
+  if (smem > attr_smem) {
+    cudaError_t e = cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+      return set_error(OF_ERR_CUDA, "of_cnn_conv3x3_wgrad_tc: %zu B of shared memory: %s", smem, cudaGetErrorString(e));
+    attr_smem = smem;
+  }
+  dim3 grid((unsigned)ks, p.mtiles * p.ntiles, 9);
+  wgrad_tc_kernel<<<grid, CV_THREADS, smem, as_stream(stream)>>>(tma, tmb, p);
+  return check_launch("of_cnn_conv3x3_wgrad_tc");
 }

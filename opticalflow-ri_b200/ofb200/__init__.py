@@ -67,3 +67,22 @@ def is_host(a) -> bool:
 
 def to_host(t):
     return t.detach().cpu().numpy()
+
+
+_PINNED_OUT = {}
+
+
+def to_host_pair(a, b):
+    """Two same-shape float32 CUDA planes -> two new numpy arrays: asynchronous copies into
+    cached pinned buffers and one synchronisation."""
+    torch = _torch()
+    key = (tuple(a.shape), a.device.index)
+    if a.shape != b.shape or a.dtype != torch.float32 or b.dtype != torch.float32:
+        return to_host(a), to_host(b)
+    buf = _PINNED_OUT.get(key)
+    if buf is None:
+        buf = _PINNED_OUT[key] = tuple(torch.empty(a.shape, dtype=torch.float32, pin_memory=True) for _ in range(2))
+    buf[0].copy_(a, non_blocking=True)
+    buf[1].copy_(b, non_blocking=True)
+    torch.cuda.current_stream(a.device).synchronize()
+    return buf[0].numpy().copy(), buf[1].numpy().copy()

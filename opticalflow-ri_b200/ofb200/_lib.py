@@ -62,6 +62,7 @@ _SIGS = {
     "of_warp_liushen_scatter": ([_P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P, _Z, _P], _I),
     "of_warp_liushen_ofe": ([_P, _P, _P, _P, _I, _I, _I, _P], _I),
     "of_cnn_conv3x3": ([_P, _I, _I, _I, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, _P, _P], _I),
+    "of_cnn_conv3x3_wgrad_tc": ([_P, _I, _I, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P, _P], _I),
     "of_cnn_conv3x3_wgrad": ([_P, _I, _I, _P, _I, _I, _I, _I, _I, _I, _I, _P, _P], _I),
     "of_cnn_bias_grad": ([_P, _I, _I, _L, _I, _P, _P], _I),
     "of_cnn_pack_pair": ([_P, _P, _I, _I, _I, _P, _P, _I, _P], _I),

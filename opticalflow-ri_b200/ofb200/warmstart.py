@@ -20,9 +20,9 @@ Network (bf16 NHWC activations, f32 accumulation; ~1.75 M parameters):
     head  conv 32->2 (f32, no ReLU)
 
 All 3x3 convolutions with ReLU except the head; pooling is 2x2 average, upsampling nearest.
-Every convolution (forward and input gradient) runs on the tensor cores through
-of_cnn_conv3x3; weight gradients, pooling and the rest through the other of_cnn_* entry
-points.  torch provides device memory and the stream only.
+Every convolution runs on the tensor cores: forward and input gradient through
+of_cnn_conv3x3, weight gradient through of_cnn_conv3x3_wgrad_tc; pooling and the rest
+through the other of_cnn_* entry points.  torch provides device memory and the stream only.
 """
 from __future__ import annotations
 
@@ -240,7 +240,8 @@ class WarmStartNet:
 
     def _wgrad(self, name, x, xct, xco, dy, dct, dco, n, H, W):
         _, _, ci, co = self.off[name]
-        call("of_cnn_conv3x3_wgrad", _p(x), xct, xco, _p(dy), dct, dco, n, H, W, ci, co, self._gw(name), _sp())
+        call("of_cnn_conv3x3_wgrad_tc", _p(x), xct, xco, _p(dy), dct, dco, n, H, W, ci, co, self._gw(name),
+             _p(self.err), _sp())
         call("of_cnn_bias_grad", _p(dy), dct, dco, n * H * W, co, self._gb(name), _sp())
 
     def _relu_bwd(self, gt, gct, gco, yt, yct, yco, P, C):
