@@ -111,6 +111,48 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// TMEM accumulator row (this thread's pixel) -> bias, ReLU, bf16 / f32 store of the N tile
+// starting at channel n0.  taddr: the warp's TMEM lane quarter, column 0.
+__device__ __forceinline__ void cv_epilogue(const ConvParams& p, uint32_t taddr, size_t pix, int n0) {
+  for (int c = 0; c < p.bn; c += 16) {
+    uint32_t r[16];
+    tmem_ld16(taddr + (uint32_t)c, r);
+    const int co = n0 + c;
+    if (co >= p.cout_store) continue;
+    float v[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      float a = __uint_as_float(r[j]);
+      if (p.bias && co + j < p.cout_store) a = __fadd_rn(a, p.bias[co + j]);
+      if (p.flags & CV_RELU) a = fmaxf(a, 0.f);
+      v[j] = a;
+    }
+    const int nvalid = p.cout_store - co < 16 ? p.cout_store - co : 16;
+    if (p.flags & CV_F32) {
+      float* yo = static_cast<float*>(p.y) + pix * p.y_ctot + p.y_coff + co;
+#pragma unroll
+      for (int j = 0; j < 16; j++)
+        if (j < nvalid) yo[j] = v[j];
+    } else {
+      bf16* yo = static_cast<bf16*>(p.y) + pix * p.y_ctot + p.y_coff + co;
+      if (nvalid == 16) {
+        uint32_t w[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+          w[j] = *reinterpret_cast<uint32_t*>(&h2);
+        }
+        reinterpret_cast<uint4*>(yo)[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        reinterpret_cast<uint4*>(yo)[1] = make_uint4(w[4], w[5], w[6], w[7]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+          if (j < nvalid) yo[j] = __float2bfloat16_rn(v[j]);
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(CV_THREADS, 1)
     conv3x3_tc_kernel(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_w,
                       const ConvParams p) {
@@ -199,46 +241,7 @@ __global__ void __launch_bounds__(CV_THREADS, 1)
     const bool ok = cv_wait(&accf, 0u, nullptr);
     if (!ok) atomicOr(p.err, 8u);
     tc_fence_after();
-    if (ok && !abort_flag) {
-      const size_t pix = ((size_t)img * p.H + py) * p.W + px;
-      for (int c = 0; c < p.bn; c += 16) {
-        uint32_t r[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, r);
-        const int co = n0 + c;
-        if (co >= p.cout_store) continue;
-        float v[16];
-#pragma unroll
-        for (int j = 0; j < 16; j++) {
-          float a = __uint_as_float(r[j]);
-          if (p.bias && co + j < p.cout_store) a = __fadd_rn(a, p.bias[co + j]);
-          if (p.flags & CV_RELU) a = fmaxf(a, 0.f);
-          v[j] = a;
-        }
-        const int nvalid = p.cout_store - co < 16 ? p.cout_store - co : 16;
-        if (p.flags & CV_F32) {
-          float* yo = static_cast<float*>(p.y) + pix * p.y_ctot + p.y_coff + co;
-#pragma unroll
-          for (int j = 0; j < 16; j++)
-            if (j < nvalid) yo[j] = v[j];
-        } else {
-          bf16* yo = static_cast<bf16*>(p.y) + pix * p.y_ctot + p.y_coff + co;
-          if (nvalid == 16) {
-            uint32_t w[8];
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-              __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
-              w[j] = *reinterpret_cast<uint32_t*>(&h2);
-            }
-            reinterpret_cast<uint4*>(yo)[0] = make_uint4(w[0], w[1], w[2], w[3]);
-            reinterpret_cast<uint4*>(yo)[1] = make_uint4(w[4], w[5], w[6], w[7]);
-          } else {
-#pragma unroll
-            for (int j = 0; j < 16; j++)
-              if (j < nvalid) yo[j] = __float2bfloat16_rn(v[j]);
-          }
-        }
-      }
-    }
+    if (ok && !abort_flag) cv_epilogue(p, tmem + ((uint32_t)(q * 32) << 16), ((size_t)img * p.H + py) * p.W + px, n0);
   }
   tc_fence_before();
   __syncthreads();
@@ -626,6 +629,30 @@ __global__ void split_flow_kernel(const float* __restrict__ f, int h, int w, flo
   v[(size_t)y * pitch + x] = f[2 * e + 1];
 }
 
+// (h, w, 2) interleaved f32 flow at half size -> U, V planes at (2h, 2w), bilinear with
+// pixel-centre alignment (fine pixel X samples coarse position (X + 0.5) / 2 - 0.5, clamped)
+// and the displacement scaled by `scale`.
+__global__ void flow_up2_kernel(const float* __restrict__ f, int h, int w, float* __restrict__ U,
+                                float* __restrict__ V, int pitch, float scale) {
+  const int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y;
+  if (X >= 2 * w) return;
+  const float sx = fmaxf(__fsub_rn(__fmul_rn(__fadd_rn((float)X, 0.5f), 0.5f), 0.5f), 0.f);
+  const float sy = fmaxf(__fsub_rn(__fmul_rn(__fadd_rn((float)Y, 0.5f), 0.5f), 0.5f), 0.f);
+  int x0 = (int)sx, y0 = (int)sy;
+  x0 = x0 < w - 1 ? x0 : w - 1;
+  y0 = y0 < h - 1 ? y0 : h - 1;
+  const int x1 = x0 + 1 < w ? x0 + 1 : w - 1, y1 = y0 + 1 < h ? y0 + 1 : h - 1;
+  const float ax = __fsub_rn(sx, (float)x0), ay = __fsub_rn(sy, (float)y0);
+#pragma unroll
+  for (int c = 0; c < 2; c++) {
+    const float a = f[((size_t)y0 * w + x0) * 2 + c], b = f[((size_t)y0 * w + x1) * 2 + c];
+    const float d = f[((size_t)y1 * w + x0) * 2 + c], e = f[((size_t)y1 * w + x1) * 2 + c];
+    const float top = __fmaf_rn(ax, __fsub_rn(b, a), a), bot = __fmaf_rn(ax, __fsub_rn(e, d), d);
+    const float v = __fmul_rn(__fmaf_rn(ay, __fsub_rn(bot, top), top), scale);
+    (c == 0 ? U : V)[(size_t)Y * pitch + X] = v;
+  }
+}
+
 static int blocks_for(long long n, int t = 256) { return (int)((n + t - 1) / t); }
 
 }  // namespace ofb
@@ -897,4 +924,12 @@ extern "C" int of_cnn_conv3x3_wgrad_tc(const void* x, int x_ctot, int x_coff, co
   dim3 grid((unsigned)ks, p.mtiles * p.ntiles, 9);
   wgrad_tc_kernel<<<grid, CV_THREADS, smem, as_stream(stream)>>>(tma, tmb, p);
   return check_launch("of_cnn_conv3x3_wgrad_tc");
+}
+
+extern "C" int of_cnn_flow_up2(const float* flow, int h, int w, float* U, float* V, int pitch, float scale,
+                               void* stream) {
+  OF_REQUIRE(flow && U && V && h > 0 && w > 0 && pitch >= 2 * w, "of_cnn_flow_up2: bad arguments");
+  dim3 g((2 * w + 255) / 256, 2 * h);
+  flow_up2_kernel<<<g, 256, 0, as_stream(stream)>>>(flow, h, w, U, V, pitch, scale);
+  return check_launch("of_cnn_flow_up2");
 }

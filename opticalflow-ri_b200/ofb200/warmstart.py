@@ -336,13 +336,15 @@ class LearnedLiuShen:
 
     @staticmethod
     def upsample(out_i, H, W):
-        """The network's (h, w, 2) flow at half size -> the initial (U, V) at H x W."""
+        """The network's (h, w, 2) flow at half size -> the initial (U, V) at H x W: one fused
+        bilinear x2 kernel (the full-size stage refines it, so the pyramid's spline is not
+        needed here)."""
         h, w = out_i.shape[0], out_i.shape[1]
-        u = torch.empty((h, w), dtype=torch.float32, device=out_i.device)
-        v = torch.empty_like(u)
-        call("of_cnn_split_flow", _p(out_i), h, w, _p(u), _p(v), w, _sp())
-        U = ops.spline_upsample(u, H, W, np.float32(W) / np.float32(w))
-        V = ops.spline_upsample(v, H, W, np.float32(H) / np.float32(h))
+        if (H, W) != (2 * h, 2 * w):
+            raise ValueError("the network runs at half the frame size")
+        U = torch.empty((H, W), dtype=torch.float32, device=out_i.device)
+        V = torch.empty_like(U)
+        call("of_cnn_flow_up2", _p(out_i), h, w, _p(U), _p(V), W, 2.0, _sp())
         return U, V
 
     def predict(self, I0, I1):

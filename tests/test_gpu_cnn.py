@@ -73,6 +73,14 @@ CONV_CASES = [  # n, H, W, cin, cout, relu
     (3, 16, 32, 192, 64, True),
     (4, 8, 8, 256, 256, True),
     (2, 8, 16, 128, 64, False),
+    # rows of 128 pixels: the 9 taps as views of one 3 x 130 halo box
+    (2, 16, 128, 16, 32, True),
+    (1, 8, 128, 32, 32, False),
+    (1, 6, 128, 64, 64, True),
+    (1, 4, 256, 96, 32, True),
+    (1, 4, 128, 384, 384, False),
+    (1, 4, 128, 256, 256, True),
+    (2, 3, 128, 192, 64, True),
 ]
 
 
@@ -339,3 +347,30 @@ def test_weight_gradient_tensor_cores(torch_cuda, case):
     want = C.conv3x3_wgrad(x[..., coff:coff + cin], dy[..., :cout])
     got = dw.cpu().numpy()
     assert np.max(np.abs(got - want)) <= 1e-4 * np.max(np.abs(want)), float(np.max(np.abs(got - want)))
+
+
+def test_flow_up2_bilinear(torch_cuda):
+    """The learned start's fused x2 upsample against a float64 restatement (pixel-centre
+    bilinear, clamped edges, times 2)."""
+    from ofb200._lib import call
+    torch = torch_cuda
+    rng = np.random.default_rng(13)
+    h, w = 12, 20
+    f = rng.normal(0, 1, (h, w, 2)).astype(np.float32)
+    ft = torch.from_numpy(f).cuda()
+    U = torch.empty((2 * h, 2 * w), dtype=torch.float32, device="cuda")
+    V = torch.empty_like(U)
+    call("of_cnn_flow_up2", _P(ft), h, w, _P(U), _P(V), 2 * w, 2.0, _sp())
+    torch.cuda.synchronize()
+    sy = np.maximum((np.arange(2 * h) + 0.5) / 2 - 0.5, 0)
+    sx = np.maximum((np.arange(2 * w) + 0.5) / 2 - 0.5, 0)
+    y0 = np.minimum(np.floor(sy).astype(int), h - 1)
+    x0 = np.minimum(np.floor(sx).astype(int), w - 1)
+    y1, x1 = np.minimum(y0 + 1, h - 1), np.minimum(x0 + 1, w - 1)
+    ay, ax = (sy - y0)[:, None], (sx - x0)[None, :]
+    for c, got in ((0, U), (1, V)):
+        g = f[..., c].astype(np.float64)
+        top = g[y0][:, x0] + ax * (g[y0][:, x1] - g[y0][:, x0])
+        bot = g[y1][:, x0] + ax * (g[y1][:, x1] - g[y1][:, x0])
+        want = 2.0 * (top + ay * (bot - top))
+        assert np.max(np.abs(got.cpu().numpy() - want)) <= 1e-5
