@@ -60,6 +60,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
+    p.add_argument("--learned-weights", default=None, help="weights + calibration .npz (default: packaged)")
     p.add_argument("--batch-pairs", type=int, default=256, help="--mode batch: pairs in the manifest")
     p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch"],
                    help="ls: only the Liu-Shen solve of one pair, --steps times (for profiling)")
@@ -306,7 +307,7 @@ def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
     import torch.distributed as dist
     from ofb200 import ops, synthetic as S
     from ofb200.warmstart import LearnedBatch, load_trained
-    net, meta = load_trained(device=dev)
+    net, meta = load_trained(**({"path": args.learned_weights} if args.learned_weights else {}), device=dev)
     nu = min(len(pairs), args.pairs)
     plain_value = args.pairs * args.steps * world / (pairs_total_ms * 1e-3)
     epe_p = []
@@ -359,7 +360,8 @@ def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
     net.check()
     learned.update({"mode": meta["mode"], "threshold": meta["threshold"], "epe_plain": float(np.mean(epe_p)),
                     "epe_pairs": nu, "epe_crop_px": 16,
-                    "network": "encoder-decoder CNN at the 512^2 level, 1.75M params, bf16 tcgen05 convs, f32 accumulate",
+                    "network": f"encoder-decoder CNN at the {meta.get('level', 512)}^2 level, 1.75M params, bf16 tcgen05 convs, "
+                               "f32 accumulate",
                     "trained": {k: meta[k] for k in ("train_pairs", "steps", "batch", "crop", "level", "eval_pairs")},
                     "no_network_ablation": ablation})
     return learned

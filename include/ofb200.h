@@ -269,9 +269,10 @@ int of_cnn_adam(float* w, const float* g, float* m, float* v, long long n, float
  * the input-gradient operand [9][cin_pad][cout_pad] with the taps mirrored. */
 int of_cnn_pack_weights(const float* w, int cout, int cin, int cout_pad, int cin_pad, int transpose_flip, void* out,
                         void* stream);
-/* (h, w, 2) interleaved f32 flow at half size -> U, V planes at (2h, 2w) (row pitch
+/* (h, w, 2) interleaved f32 flow -> U, V planes at (factor h, factor w) (row pitch
  * `pitch`): bilinear, pixel-centre aligned, edges clamped, displacements times `scale`. */
-int of_cnn_flow_up2(const float* flow, int h, int w, float* U, float* V, int pitch, float scale, void* stream);
+int of_cnn_flow_up(const float* flow, int h, int w, int factor, float* U, float* V, int pitch, float scale,
+                   void* stream);
 /* (h, w, 2) interleaved f32 flow -> u, v planes (row pitch `pitch`). */
 int of_cnn_split_flow(const float* flow, int h, int w, float* u, float* v, int pitch, void* stream);
 

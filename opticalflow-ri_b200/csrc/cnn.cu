@@ -629,15 +629,16 @@ __global__ void split_flow_kernel(const float* __restrict__ f, int h, int w, flo
   v[(size_t)y * pitch + x] = f[2 * e + 1];
 }
 
-// (h, w, 2) interleaved f32 flow at half size -> U, V planes at (2h, 2w), bilinear with
-// pixel-centre alignment (fine pixel X samples coarse position (X + 0.5) / 2 - 0.5, clamped)
-// and the displacement scaled by `scale`.
-__global__ void flow_up2_kernel(const float* __restrict__ f, int h, int w, float* __restrict__ U,
-                                float* __restrict__ V, int pitch, float scale) {
+// (h, w, 2) interleaved f32 flow -> U, V planes at (f h, f w), bilinear with pixel-centre
+// alignment (fine pixel X samples coarse position (X + 0.5) / f - 0.5, clamped) and the
+// displacement scaled by `scale`.
+__global__ void flow_up_kernel(const float* __restrict__ fl, int h, int w, int f, float* __restrict__ U,
+                               float* __restrict__ V, int pitch, float scale) {
   const int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y;
-  if (X >= 2 * w) return;
-  const float sx = fmaxf(__fsub_rn(__fmul_rn(__fadd_rn((float)X, 0.5f), 0.5f), 0.5f), 0.f);
-  const float sy = fmaxf(__fsub_rn(__fmul_rn(__fadd_rn((float)Y, 0.5f), 0.5f), 0.5f), 0.f);
+  if (X >= f * w) return;
+  const float inv = __frcp_rn((float)f);
+  const float sx = fmaxf(__fsub_rn(__fmul_rn(__fadd_rn((float)X, 0.5f), inv), 0.5f), 0.f);
+  const float sy = fmaxf(__fsub_rn(__fmul_rn(__fadd_rn((float)Y, 0.5f), inv), 0.5f), 0.f);
   int x0 = (int)sx, y0 = (int)sy;
   x0 = x0 < w - 1 ? x0 : w - 1;
   y0 = y0 < h - 1 ? y0 : h - 1;
@@ -645,8 +646,8 @@ __global__ void flow_up2_kernel(const float* __restrict__ f, int h, int w, float
   const float ax = __fsub_rn(sx, (float)x0), ay = __fsub_rn(sy, (float)y0);
 #pragma unroll
   for (int c = 0; c < 2; c++) {
-    const float a = f[((size_t)y0 * w + x0) * 2 + c], b = f[((size_t)y0 * w + x1) * 2 + c];
-    const float d = f[((size_t)y1 * w + x0) * 2 + c], e = f[((size_t)y1 * w + x1) * 2 + c];
+    const float a = fl[((size_t)y0 * w + x0) * 2 + c], b = fl[((size_t)y0 * w + x1) * 2 + c];
+    const float d = fl[((size_t)y1 * w + x0) * 2 + c], e = fl[((size_t)y1 * w + x1) * 2 + c];
     const float top = __fmaf_rn(ax, __fsub_rn(b, a), a), bot = __fmaf_rn(ax, __fsub_rn(e, d), d);
     const float v = __fmul_rn(__fmaf_rn(ay, __fsub_rn(bot, top), top), scale);
     (c == 0 ? U : V)[(size_t)Y * pitch + X] = v;
@@ -926,10 +927,11 @@ extern "C" int of_cnn_conv3x3_wgrad_tc(const void* x, int x_ctot, int x_coff, co
   return check_launch("of_cnn_conv3x3_wgrad_tc");
 }
 
-extern "C" int of_cnn_flow_up2(const float* flow, int h, int w, float* U, float* V, int pitch, float scale,
-                               void* stream) {
-  OF_REQUIRE(flow && U && V && h > 0 && w > 0 && pitch >= 2 * w, "of_cnn_flow_up2: bad arguments");
-  dim3 g((2 * w + 255) / 256, 2 * h);
-  flow_up2_kernel<<<g, 256, 0, as_stream(stream)>>>(flow, h, w, U, V, pitch, scale);
-  return check_launch("of_cnn_flow_up2");
+extern "C" int of_cnn_flow_up(const float* flow, int h, int w, int factor, float* U, float* V, int pitch, float scale,
+                              void* stream) {
+  OF_REQUIRE(flow && U && V && h > 0 && w > 0 && factor >= 1 && factor <= 16 && pitch >= factor * w,
+             "of_cnn_flow_up: bad arguments");
+  dim3 g((factor * w + 255) / 256, factor * h);
+  flow_up_kernel<<<g, 256, 0, as_stream(stream)>>>(flow, h, w, factor, U, V, pitch, scale);
+  return check_launch("of_cnn_flow_up");
 }

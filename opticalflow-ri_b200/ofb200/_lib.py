@@ -74,7 +74,7 @@ _SIGS = {
     "of_cnn_flow_mse": ([_P, _P, _L, _P, _I, _P, _P], _I),
     "of_cnn_adam": ([_P, _P, _P, _P, _L, _F, _F, _F, _F, _I, _P], _I),
     "of_cnn_pack_weights": ([_P, _I, _I, _I, _I, _I, _P, _P], _I),
-    "of_cnn_flow_up2": ([_P, _I, _I, _P, _P, _I, _F, _P], _I),
+    "of_cnn_flow_up": ([_P, _I, _I, _I, _P, _P, _I, _F, _P], _I),
     "of_cnn_split_flow": ([_P, _I, _I, _P, _P, _I, _P], _I),
     "of_lk_dense": ([_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P], _I),
     "of_fb_blur": ([_P, _P, _I, _I, _I, _I, _P, _I, _P], _I),

@@ -319,38 +319,49 @@ class LearnedLiuShen:
     run() returns (U, V, iters, err): err is the solve's last update norm (device scalar);
     accept(err) tells whether it is within the calibrated threshold."""
 
-    def __init__(self, net: WarmStartNet, sweeps=16, h=10.0, filter_opt=0.48, threshold=None, mode="ls", fb_iters=5):
+    def __init__(self, net: WarmStartNet, sweeps=16, h=10.0, filter_opt=0.48, threshold=None, mode="ls", fb_iters=5,
+                 factor=2):
         self.net, self.sweeps, self.h, self.filter_opt, self.threshold = net, int(sweeps), float(h), filter_opt, threshold
         if mode not in ("ls", "fb"):
             raise ValueError(mode)
-        self.mode, self.fb_iters = mode, int(fb_iters)
+        self.mode, self.fb_iters, self.factor = mode, int(fb_iters), int(factor)  # frame size / network size
         from gaussian_filter import prepareGaussianKernel
         self.taps = prepareGaussianKernel(filter_opt, 5)
 
+    @classmethod
+    def from_meta(cls, net, meta, start="cnn"):
+        """The calibrated configuration.  The network was trained at meta["level"] for
+        meta["frame"] (1024) frames; other frame sizes keep that ratio."""
+        factor = int(meta.get("frame", 1024)) // int(meta.get("level", 512))
+        if start == "cnn":
+            return cls(net, sweeps=meta["sweeps"], threshold=meta["threshold"], mode=meta["mode"],
+                       fb_iters=meta.get("fb_iters", 5), factor=factor)
+        return cls(net, sweeps=meta.get("zero_sweeps", meta["sweeps"]), threshold=meta["threshold"], mode="fb",
+                   fb_iters=meta.get("zero_fb_iters", 5), factor=factor)
+
     def pack(self, b, i, I0, I1):
-        """The pyramid's half-size level of pair i into the network input."""
+        """The pyramid level the network runs at (1 / factor of the frames) of pair i into
+        the network input (PIL bicubic, as the pyramid resizes)."""
         H, W = I0.shape
-        n0 = ops.resize(I0, (W // 2, H // 2), bicubic=True)
-        n1 = ops.resize(I1, (W // 2, H // 2), bicubic=True)
+        n0 = ops.resize(I0, (W // self.factor, H // self.factor), bicubic=True)
+        n1 = ops.resize(I1, (W // self.factor, H // self.factor), bicubic=True)
         self.net.pack_input(b, i, n0, n1)
 
-    @staticmethod
-    def upsample(out_i, H, W):
-        """The network's (h, w, 2) flow at half size -> the initial (U, V) at H x W: one fused
-        bilinear x2 kernel (the full-size stage refines it, so the pyramid's spline is not
-        needed here)."""
-        h, w = out_i.shape[0], out_i.shape[1]
-        if (H, W) != (2 * h, 2 * w):
-            raise ValueError("the network runs at half the frame size")
+    def upsample(self, out_i, H, W):
+        """The network's (h, w, 2) flow -> the initial (U, V) at H x W: one fused bilinear
+        kernel (the full-size stage refines it, so the pyramid's spline is not needed here)."""
+        h, w, f = out_i.shape[0], out_i.shape[1], self.factor
+        if (H, W) != (f * h, f * w):
+            raise ValueError("frame and network sizes do not match the factor")
         U = torch.empty((H, W), dtype=torch.float32, device=out_i.device)
         V = torch.empty_like(U)
-        call("of_cnn_flow_up2", _p(out_i), h, w, _p(U), _p(V), W, 2.0, _sp())
+        call("of_cnn_flow_up", _p(out_i), h, w, f, _p(U), _p(V), W, float(f), _sp())
         return U, V
 
     def predict(self, I0, I1):
-        """Initial (U, V) at the frames' size from the CNN at half size."""
+        """Initial (U, V) at the frames' size from the CNN at 1 / factor of it."""
         H, W = I0.shape
-        b = self.net.buffers(1, H // 2)
+        b = self.net.buffers(1, H // self.factor)
         self.pack(b, 0, I0, I1)
         return self.upsample(self.net.forward(b)[0], H, W)
 
@@ -395,9 +406,7 @@ class LearnedBatch:
     def __init__(self, net, meta, n, size=1024, streams=4, use_graph=True, start="cnn"):
         if start not in ("cnn", "zero"):
             raise ValueError(start)
-        fb_iters = meta.get("fb_iters", 5) if start == "cnn" else meta.get("zero_fb_iters", 5)
-        self.ll = LearnedLiuShen(net, sweeps=meta["sweeps"], threshold=meta["threshold"],
-                                 mode=meta["mode"] if start == "cnn" else "fb", fb_iters=fb_iters)
+        self.ll = LearnedLiuShen.from_meta(net, meta, start)
         self.start = start
         self.net, self.n, self.size, self.nstreams, self.use_graph = net, int(n), int(size), max(1, streams), use_graph
         self._graph = None
@@ -409,7 +418,7 @@ class LearnedBatch:
             self._streams = [torch.cuda.Stream() for _ in range(self.nstreams)]
         out = None
         if self.start == "cnn":
-            b = self.net.buffers(self.n, self.size // 2)
+            b = self.net.buffers(self.n, self.size // self.ll.factor)
             for i, (A, B) in enumerate(frames):
                 self.ll.pack(b, i, A, B)
             out = self.net.forward(b)

@@ -70,51 +70,53 @@ def plain(a, b):
     return G.genericPyramidalOpticalFlow(a, b, 0, F.Farneback_PyCL(), 2, 1, 0.48, LS.LiuShenOpticalFlowAlgoAdapter(10))
 
 
-def build_level_data(pairs, dev):
-    """(N, 512, 512, 2) bf16 inputs (each frame / its max) and (N, 512, 512, 2) f32 labels."""
+def build_level_data(pairs, dev, level=LEVEL):
+    """(N, level, level, 2) bf16 inputs (each frame / its max) and (N, level, level, 2) f32
+    labels (the plain output resized to the level, displacements scaled by level / 1024)."""
     import torch
     from ofb200 import ops
     from ofb200._lib import call
     from ofb200.warmstart import _p, _sp
     N = len(pairs)
-    X = torch.empty((N, LEVEL, LEVEL, 2), dtype=torch.bfloat16, device=dev)
-    Y = torch.empty((N, LEVEL, LEVEL, 2), dtype=torch.float32, device=dev)
-    tmp = torch.empty((LEVEL, LEVEL, 16), dtype=torch.bfloat16, device=dev)
+    X = torch.empty((N, level, level, 2), dtype=torch.bfloat16, device=dev)
+    Y = torch.empty((N, level, level, 2), dtype=torch.float32, device=dev)
+    tmp = torch.empty((level, level, 16), dtype=torch.bfloat16, device=dev)
     mx = torch.zeros(2, dtype=torch.int32, device=dev)
     for i, (a, b) in enumerate(pairs):
         A = ops.u8_to_f32(torch.from_numpy(a).to(dev))
         B = ops.u8_to_f32(torch.from_numpy(b).to(dev))
         U, V = plain(A, B)
-        a2 = ops.resize(A, (LEVEL, LEVEL), bicubic=True)
-        b2 = ops.resize(B, (LEVEL, LEVEL), bicubic=True)
-        call("of_cnn_pack_pair", _p(a2), _p(b2), LEVEL, LEVEL, LEVEL, _p(mx), _p(tmp), 16, _sp())
+        a2 = ops.resize(A, (level, level), bicubic=True)
+        b2 = ops.resize(B, (level, level), bicubic=True)
+        call("of_cnn_pack_pair", _p(a2), _p(b2), level, level, level, _p(mx), _p(tmp), 16, _sp())
         X[i] = tmp[..., :2]
-        Y[i, ..., 0] = ops.scale(ops.resize(U, (LEVEL, LEVEL), bicubic=True), 0.5)
-        Y[i, ..., 1] = ops.scale(ops.resize(V, (LEVEL, LEVEL), bicubic=True), 0.5)
+        sc = level / float(A.shape[0])
+        Y[i, ..., 0] = ops.scale(ops.resize(U, (level, level), bicubic=True), sc)
+        Y[i, ..., 1] = ops.scale(ops.resize(V, (level, level), bicubic=True), sc)
     torch.cuda.synchronize()
     return X, Y
 
 
-def train(net, X, Y, steps, batch=16, lr=1e-3, seed=0, log=print, sync=None):
+def train(net, X, Y, steps, batch=16, lr=1e-3, seed=0, log=print, sync=None, crop=CROP):
     """Adam on random crops.  `sync(grads)` (data-parallel training) averages the flat
     gradient vector over the ranks between backward and the optimizer step."""
     import torch
-    N = X.shape[0]
+    N, level = X.shape[0], X.shape[1]
     g = torch.Generator(device="cpu").manual_seed(seed)
-    b = net.buffers(batch, CROP)
-    gb = net.grad_buffers(batch, CROP)
+    b = net.buffers(batch, crop)
+    gb = net.grad_buffers(batch, crop)
     b["x0"].zero_()
-    lab = torch.empty((batch, CROP, CROP, 2), dtype=torch.float32, device=X.device)
+    lab = torch.empty((batch, crop, crop, 2), dtype=torch.float32, device=X.device)
     hist = []
     t0 = time.time()
     for s in range(steps):
         idx = torch.randint(0, N, (batch,), generator=g)
-        oy = torch.randint(0, LEVEL - CROP + 1, (batch,), generator=g)
-        ox = torch.randint(0, LEVEL - CROP + 1, (batch,), generator=g)
+        oy = torch.randint(0, level - crop + 1, (batch,), generator=g)
+        ox = torch.randint(0, level - crop + 1, (batch,), generator=g)
         for j in range(batch):
             i, y, x = int(idx[j]), int(oy[j]), int(ox[j])
-            b["x0"][j, ..., :2] = X[i, y:y + CROP, x:x + CROP]
-            lab[j] = Y[i, y:y + CROP, x:x + CROP]
+            b["x0"][j, ..., :2] = X[i, y:y + crop, x:x + crop]
+            lab[j] = Y[i, y:y + crop, x:x + crop]
         net.forward(b)
         loss = net.loss(b, gb, lab)
         net.backward(b, gb)
@@ -142,7 +144,7 @@ def _configs(sweeps_list):
     return cfg
 
 
-def evaluate(net, pairs, sweeps_list, dev, log=print):
+def evaluate(net, pairs, sweeps_list, dev, log=print, level=LEVEL):
     """Interior EPE (16 px crop) against the analytic ground truth of the plain pyramid,
     of the network's start followed by each full-size stage, and of the same stages from
     a zero field (no network).  The cheapest network configuration whose mean EPE is at
@@ -158,11 +160,12 @@ def evaluate(net, pairs, sweeps_list, dev, log=print):
         B = torch.from_numpy(b.astype(np.float32)).to(dev)
         Up, Vp = plain(A, B)
         row = {"plain": S.epe(Up.cpu().numpy(), Vp.cpu().numpy(), Ug, Vg, crop=16)}
-        base = LearnedLiuShen(net)
+        f = A.shape[0] // level
+        base = LearnedLiuShen(net, factor=f)
         U0, V0 = base.predict(A, B)
         row["cnn"] = S.epe(U0.cpu().numpy(), V0.cpu().numpy(), Ug, Vg, crop=16)
         for mode, it, K in cfgs:
-            ll = LearnedLiuShen(net, sweeps=K, mode=mode, fb_iters=max(it, 1))
+            ll = LearnedLiuShen(net, sweeps=K, mode=mode, fb_iters=max(it, 1), factor=f)
             U, V, _, err = ll.refine(A, B, U0.clone(), V0.clone())
             row[("cnn", mode, it, K)] = (S.epe(U.cpu().numpy(), V.cpu().numpy(), Ug, Vg, crop=16), float(err.item()))
             if mode == "fb":
@@ -205,7 +208,8 @@ def calibrate_only(args):
     old = json.loads(str(d["meta"]))
     net = WarmStartNet(seed=0).load(args.calibrate)
     sweeps = [int(s) for s in args.sweeps.split(",")]
-    sel, table, _ = evaluate(net, eval_pairs, sweeps, torch.device("cuda", 0), log=lambda m: print(m, flush=True))
+    sel, table, _ = evaluate(net, eval_pairs, sweeps, torch.device("cuda", 0), log=lambda m: print(m, flush=True),
+                             level=int(old.get("level", LEVEL)))
     meta = {**{k: v for k, v in old.items() if k not in ("table",)}, **sel, "table": table, "eval_pairs": args.eval}
     np.savez_compressed(args.out, meta=json.dumps(meta), params=d["params"], layers=d["layers"])
     print(json.dumps({k: v for k, v in meta.items() if k not in ("loss_history", "table")}), flush=True)
@@ -222,6 +226,8 @@ def main():
     ap.add_argument("--sweeps", default="4,8,12,16,24,32,60")
     ap.add_argument("--out", default="warmstart.npz")
     ap.add_argument("--calibrate", default=None, help="recalibrate the weights in this .npz (no training)")
+    ap.add_argument("--level", type=int, default=LEVEL, help="size the network runs at (1024 / 2^k)")
+    ap.add_argument("--crop", type=int, default=CROP, help="training crop (<= level)")
     args = ap.parse_args()
     if args.calibrate:
         return calibrate_only(args)
@@ -248,14 +254,14 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     t1 = time.time()
-    X, Y = build_level_data(train_pairs, dev)
+    X, Y = build_level_data(train_pairs, dev, args.level)
     del train_pairs
     print(f"rank {rank}: labelled in {time.time() - t1:.0f}s", flush=True)
     net = WarmStartNet(seed=0, device=dev)  # the same initial weights on every rank
     t2 = time.time()
     hist = train(net, X, Y, args.steps, args.batch, args.lr, seed=rank,
                  log=(lambda m: print(m, flush=True)) if rank == 0 else (lambda m: None),
-                 sync=average_gradients if world > 1 else None)
+                 sync=average_gradients if world > 1 else None, crop=min(args.crop, args.level))
     print(f"rank {rank}: trained in {time.time() - t2:.0f}s", flush=True)
     if world > 1:
         dist.barrier()
@@ -263,9 +269,9 @@ def main():
     if rank != 0:
         return
     sweeps = [int(s) for s in args.sweeps.split(",")]
-    sel, table, rows = evaluate(net, eval_pairs, sweeps, dev, log=lambda m: print(m, flush=True))
+    sel, table, rows = evaluate(net, eval_pairs, sweeps, dev, log=lambda m: print(m, flush=True), level=args.level)
     meta = {**sel, "table": table, "train_pairs": args.pairs, "steps": args.steps, "ranks": world,
-            "batch": args.batch, "crop": CROP, "level": LEVEL, "eval_pairs": args.eval,
+            "batch": args.batch, "crop": min(args.crop, args.level), "level": args.level, "eval_pairs": args.eval,
             "train_seed0": TRAIN_SEED0, "eval_seed0": EVAL_SEED0, "loss_history": hist}
     np.savez(args.out, meta=json.dumps(meta), **net.state())
     print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}), flush=True)

@@ -349,28 +349,29 @@ def test_weight_gradient_tensor_cores(torch_cuda, case):
     assert np.max(np.abs(got - want)) <= 1e-4 * np.max(np.abs(want)), float(np.max(np.abs(got - want)))
 
 
-def test_flow_up2_bilinear(torch_cuda):
-    """The learned start's fused x2 upsample against a float64 restatement (pixel-centre
-    bilinear, clamped edges, times 2)."""
+@pytest.mark.parametrize("factor", [2, 4])
+def test_flow_upsample_bilinear(torch_cuda, factor):
+    """The learned start's fused upsample against a float64 restatement (pixel-centre
+    bilinear, clamped edges, displacements times the factor)."""
     from ofb200._lib import call
     torch = torch_cuda
     rng = np.random.default_rng(13)
-    h, w = 12, 20
-    f = rng.normal(0, 1, (h, w, 2)).astype(np.float32)
-    ft = torch.from_numpy(f).cuda()
-    U = torch.empty((2 * h, 2 * w), dtype=torch.float32, device="cuda")
+    h, w, f = 12, 20, factor
+    fl = rng.normal(0, 1, (h, w, 2)).astype(np.float32)
+    ft = torch.from_numpy(fl).cuda()
+    U = torch.empty((f * h, f * w), dtype=torch.float32, device="cuda")
     V = torch.empty_like(U)
-    call("of_cnn_flow_up2", _P(ft), h, w, _P(U), _P(V), 2 * w, 2.0, _sp())
+    call("of_cnn_flow_up", _P(ft), h, w, f, _P(U), _P(V), f * w, float(f), _sp())
     torch.cuda.synchronize()
-    sy = np.maximum((np.arange(2 * h) + 0.5) / 2 - 0.5, 0)
-    sx = np.maximum((np.arange(2 * w) + 0.5) / 2 - 0.5, 0)
+    sy = np.maximum((np.arange(f * h) + 0.5) / f - 0.5, 0)
+    sx = np.maximum((np.arange(f * w) + 0.5) / f - 0.5, 0)
     y0 = np.minimum(np.floor(sy).astype(int), h - 1)
     x0 = np.minimum(np.floor(sx).astype(int), w - 1)
     y1, x1 = np.minimum(y0 + 1, h - 1), np.minimum(x0 + 1, w - 1)
     ay, ax = (sy - y0)[:, None], (sx - x0)[None, :]
     for c, got in ((0, U), (1, V)):
-        g = f[..., c].astype(np.float64)
+        g = fl[..., c].astype(np.float64)
         top = g[y0][:, x0] + ax * (g[y0][:, x1] - g[y0][:, x0])
         bot = g[y1][:, x0] + ax * (g[y1][:, x1] - g[y1][:, x0])
-        want = 2.0 * (top + ay * (bot - top))
-        assert np.max(np.abs(got.cpu().numpy() - want)) <= 1e-5
+        want = f * (top + ay * (bot - top))
+        assert np.max(np.abs(got.cpu().numpy() - want)) <= 1e-5 * f

@@ -35,12 +35,12 @@ def test_batch_matches_single_pair(torch_cuda, trained):
     net, meta = trained
     frames = []
     for seed in (1, 2, 3):
-        a, b, _, _ = S.config_pair("fbls1024", seed=seed, size=256)
+        a, b, _, _ = S.config_pair("fbls1024", seed=seed, size=512)
         frames.append((_f32(torch, a), _f32(torch, b)))
-    ll = LearnedLiuShen(net, sweeps=meta["sweeps"], mode=meta["mode"], fb_iters=meta["fb_iters"])
+    ll = LearnedLiuShen.from_meta(net, meta)
     want = [ll.run(A, B) for A, B in frames]
     want = [(U.cpu().numpy(), V.cpu().numpy(), float(e.item())) for U, V, _, e in want]
-    lb = LearnedBatch(net, meta, 3, size=256, streams=2)
+    lb = LearnedBatch(net, meta, 3, size=512, streams=2)
     for _ in range(2):  # capture, then replay
         res, errs = lb.run(frames)
         torch.cuda.synchronize()
@@ -63,7 +63,7 @@ def test_trained_start_gain(torch_cuda, trained):
     from ofb200.warmstart import LearnedLiuShen
     net, meta = trained
     assert meta["mode"] == "fb" and meta["fb_iters"] < meta["zero_fb_iters"]
-    ll = LearnedLiuShen(net, sweeps=meta["sweeps"], mode="fb", fb_iters=meta["fb_iters"])
+    ll = LearnedLiuShen.from_meta(net, meta)
     e_plain, e_learned, e_zero = [], [], []
     for seed in HELD_OUT:
         a, b, Ug, Vg = S.config_pair("fbls1024", seed=seed)
