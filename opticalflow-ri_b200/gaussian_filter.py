@@ -22,9 +22,23 @@ def prepareGaussianKernel(sigma, kernelSizePx):
     return kernel
 
 
+def _reference_errors(K, H, W):
+    """The exceptions src/gaussian_filter.py:54-85 raises before filtering anything: the
+    line buffer's slice assignment for K == 1 or an even K, then the border copy reading
+    image[i, j] for j < K // 2 (columns first, in the row pass)."""
+    h = K // 2
+    if K == 1 or K % 2 == 0:
+        raise ValueError(f"could not broadcast input array from shape ({W},) into shape ({W + K - 1 - 2 * h if h else 0},)")
+    if h > W:
+        raise IndexError(f"index {W} is out of bounds for axis 1 with size {W}")
+    if h > H:  # the reference has filtered the rows in place when the column pass raises
+        raise IndexError(f"index {H} is out of bounds for axis 0 with size {H}")
+
+
 def convolveSeparableFilter(kernel, image):
     """Row pass then column pass with the reference's border (src/gaussian_filter.py:54-85)."""
     kernel = np.ascontiguousarray(kernel, dtype=np.float32)
+    _reference_errors(int(kernel.shape[0]), int(image.shape[0]), int(image.shape[1]))
     if is_host(image):
         src = to_device(image)
         out = ops.prefilter(src, kernel)

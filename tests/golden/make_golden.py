@@ -182,6 +182,16 @@ def main():
     out["pyr_hs_ls"] = dict(f0=a, f1=b, U=Ur, V=Vr)
 
     out.update(liushen_warp_cases(R, rng))
+    # the prefilter's own exceptions on images smaller than half the kernel, K = 1, even K
+    d = {}
+    for i, (shape, K) in enumerate([((1, 7), 3), ((5, 3), 9), ((3, 20), 9), ((7, 40), 15), ((6, 6), 1), ((6, 6), 4)]):
+        try:
+            R["gaussian_filter"].gaussian_filterPx(np.ones(shape, np.float32), 1.0, K)
+            d[f"msg{i}"] = np.array("")
+        except (IndexError, ValueError) as e:
+            d[f"msg{i}"] = np.array(f"{type(e).__name__}: {e}")
+        d[f"case{i}"] = np.array([shape[0], shape[1], K])
+    out["prefilter_errors"] = d
     only = sys.argv[sys.argv.index("--only") + 1].split(",") if "--only" in sys.argv else None
     for name, d in out.items():
         if only and name not in only:

@@ -129,3 +129,19 @@ def test_pyramid_hs_liushen_warp_klevels():
                      O.LS(10), True, False, True, True)
     assert np.abs(U - g["U"]).max() <= 1e-3 and np.abs(V - g["V"]).max() <= 1e-3
     assert np.abs(f0 - g["f0_after"]).max() <= 1e-3 * np.abs(g["f0_after"]).max()
+
+
+def test_prefilter_reference_errors():
+    """The drop-in raises what the reference's gaussian_filterPx raises (before any GPU
+    work): IndexError below half the kernel (columns checked first), ValueError for K == 1
+    or an even K."""
+    import gaussian_filter as GF
+    g = golden("prefilter_errors")
+    for i in range(6):
+        H, W, K = (int(x) for x in g[f"case{i}"])
+        want = str(g[f"msg{i}"])
+        if not want:
+            continue
+        with pytest.raises((IndexError, ValueError)) as e:
+            GF._reference_errors(K, H, W)
+        assert f"{type(e.value).__name__}: {e.value}" == want, i
