@@ -62,7 +62,7 @@ def parse():
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
     p.add_argument("--learned-weights", default=None, help="weights + calibration .npz (default: packaged)")
     p.add_argument("--batch-pairs", type=int, default=256, help="--mode batch: pairs in the manifest")
-    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch"],
+    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn"],
                    help="ls: only the Liu-Shen solve of one pair, --steps times (for profiling)")
     return p.parse_args()
 
@@ -87,6 +87,47 @@ def run_ls_only(args):
         if r >= args.warmup:
             ms.append(e0.elapsed_time(e1))
     print(json.dumps({"mode": "ls", "size": args.size, "sweeps": int(it.item()), "ms": float(np.mean(ms))}))
+
+
+def run_cnn(args):
+    """The warm-start network alone: forward of --pairs frames at --size (the level it runs
+    at), and one training step (16 x 256^2: forward, loss, backward, Adam), CUDA events."""
+    import torch
+    from ofb200.warmstart import LAYERS, WarmStartNet
+    net = WarmStartNet(seed=0)
+
+    def timeit(fn, reps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    n, S = args.pairs, args.size
+    b = net.buffers(n, S)
+    b["x0"][..., :2] = torch.rand((n, S, S, 2), device="cuda").to(torch.bfloat16)
+    fwd = timeit(lambda: net.forward(b), args.steps)
+    flops = sum(2 * 9 * ci * co * n * (S >> lvl) ** 2 for (name, ci, co), lvl in
+                zip(LAYERS, [0, 0, 1, 1, 2, 2, 3, 3, 2, 1, 0, 0]))
+    bt, gt = net.buffers(16, 256), net.grad_buffers(16, 256)
+    bt["x0"][..., :2] = torch.rand((16, 256, 256, 2), device="cuda").to(torch.bfloat16)
+    lab = torch.randn((16, 256, 256, 2), device="cuda")
+
+    def train_step():
+        net.forward(bt)
+        net.loss(bt, gt, lab)
+        net.backward(bt, gt)
+        net.adam(1e-4)
+
+    step = timeit(train_step, args.steps)
+    net.check()
+    print(json.dumps({"mode": "cnn", "size": S, "batch": n, "forward_ms": fwd, "forward_ms_per_pair": fwd / n,
+                      "forward_tflops": flops / fwd / 1e9, "train_step_ms_16x256": step}))
 
 
 def peaks():
@@ -502,6 +543,9 @@ def main():
         return
     if args.mode == "ls":
         run_ls_only(args)
+        return
+    if args.mode == "cnn":
+        run_cnn(args)
         return
     if args.mode == "batch":
         if world > 1:
