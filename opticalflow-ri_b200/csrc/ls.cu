@@ -173,52 +173,107 @@ __device__ __forceinline__ double ls_err(const double* ss, int k, double inv_n) 
 //    53 bits is innocuous for a sum of two 24-bit values);
 //  - M (4 terms) and H (8 terms) keep the reference's double accumulation order; H uses
 //    'constant' 0 outside the image (the EDGE variant selects +0.0 there).
-constexpr long long LS_WAIT_LIMIT = 1ll << 22;
-
 // The weights (+-0.5, 1, +-0.25) are powers of two, so every product is exact and an add of
 // the product rounds exactly as a fused multiply-add does: each term is one FMA.
-__device__ __forceinline__ float st2(float a, float b, float wa, float wb) {
-  return __fmaf_rn(b, wb, __fmaf_rn(a, wa, 0.0f));
+// The float32 arithmetic of a lane's two cells runs as packed f32x2 operations (sm_100
+// fma / add / mul .rn.f32x2): each half rounds exactly as the scalar operation does.
+constexpr long long LS_WAIT_LIMIT = 1ll << 22;
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
+// Packed f32x2 arithmetic.  The assembler contracts a packed multiply feeding a packed add
+// into one fused multiply-add even when both carry .rn (measured on sm_100a with CUDA 12.9;
+// scalar .rn operations are left alone), and it sees through literal ones and zeros.  So a
+// sum of products is written as fma(product, one, sum) with `one` a kernel argument equal
+// to 1.0f: that rounds exactly as product + sum, and a multiplier whose value the assembler
+// does not know cannot be folded away or fused with the product.
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) {
+  float2 d;
+  asm("{.reg .b64 ra, rb, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\t"
+      "mov.b64 rb, {%4, %5};\n\t"
+      "mul.rn.f32x2 rd, ra, rb;\n\t"
+      "mov.b64 {%0, %1}, rd;}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
 }
-__device__ __forceinline__ float st_m(const double d[3][3]) {
-  double t = __fma_rn(d[0][0], 0.25, 0.0);
-  t = __fma_rn(d[0][2], -0.25, t);
-  t = __fma_rn(d[2][0], -0.25, t);
-  t = __fma_rn(d[2][2], 0.25, t);
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+  float2 d;
+  asm("{.reg .b64 ra, rb, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\t"
+      "mov.b64 rb, {%4, %5};\n\t"
+      "add.rn.f32x2 rd, ra, rb;\n\t"
+      "mov.b64 {%0, %1}, rd;}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{.reg .b64 ra, rb, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\t"
+      "mov.b64 rb, {%4, %5};\n\t"
+      "mov.b64 rc, {%6, %7};\n\t"
+      "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+      "mov.b64 {%0, %1}, rd;}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+__device__ __forceinline__ float2 st2x2(float2 a, float2 b, float wa, float wb) {
+  return pfma(b, f2s(wb), pfma(a, f2s(wa), f2s(0.0f)));
+}
+// M at column j of the lane's 4-column window (j = 1: the even cell, 2: the odd cell)
+__device__ __forceinline__ float st_m(const double* U, const double* D, int j) {
+  double t = __fma_rn(U[j - 1], 0.25, 0.0);
+  t = __fma_rn(U[j + 1], -0.25, t);
+  t = __fma_rn(D[j - 1], -0.25, t);
+  t = __fma_rn(D[j + 1], 0.25, t);
   return (float)t;
 }
+// H at column j; on an image border the out-of-image neighbours count as +0.0
 template <bool EDGE>
-__device__ __forceinline__ float st_h(const double d[3][3], bool T, bool B, bool L, bool R) {
+__device__ __forceinline__ float st_h(const double* U, const double* C, const double* D, int j, bool T, bool B,
+                                      bool L, bool R) {
   double t = 0.0;
-  t = __dadd_rn(t, (EDGE && (T || L)) ? 0.0 : d[0][0]);
-  t = __dadd_rn(t, (EDGE && T) ? 0.0 : d[0][1]);
-  t = __dadd_rn(t, (EDGE && (T || R)) ? 0.0 : d[0][2]);
-  t = __dadd_rn(t, (EDGE && L) ? 0.0 : d[1][0]);
-  t = __dadd_rn(t, (EDGE && R) ? 0.0 : d[1][2]);
-  t = __dadd_rn(t, (EDGE && (B || L)) ? 0.0 : d[2][0]);
-  t = __dadd_rn(t, (EDGE && B) ? 0.0 : d[2][1]);
-  t = __dadd_rn(t, (EDGE && (B || R)) ? 0.0 : d[2][2]);
+  t = __dadd_rn(t, (EDGE && (T || L)) ? 0.0 : U[j - 1]);
+  t = __dadd_rn(t, (EDGE && T) ? 0.0 : U[j]);
+  t = __dadd_rn(t, (EDGE && (T || R)) ? 0.0 : U[j + 1]);
+  t = __dadd_rn(t, (EDGE && L) ? 0.0 : C[j - 1]);
+  t = __dadd_rn(t, (EDGE && R) ? 0.0 : C[j + 1]);
+  t = __dadd_rn(t, (EDGE && (B || L)) ? 0.0 : D[j - 1]);
+  t = __dadd_rn(t, (EDGE && B) ? 0.0 : D[j]);
+  t = __dadd_rn(t, (EDGE && (B || R)) ? 0.0 : D[j + 1]);
   return (float)t;
 }
 
 // Temporally blocked sweeps: one pass runs up to LB_T sweeps on a tile held in shared
 // memory, so the 8 coefficient planes and (u, v) cross HBM/L2 once per LB_T sweeps.
-// Tile: 24 x 64 owned pixels plus a 4-pixel halo = a 32 x 72 region, loaded by one 3-D TMA
-// (8 coefficient planes, 72 KB) and two 2-D TMAs (u, v) starting at (x0-4, y0-4): x stays
-// 16-byte aligned.  Each sweep computes every cell of the region that has its full 3x3
-// neighbourhood in the tile; after sweep s only the cells at least s+1 from the region's
-// edge are exact, so after LB_T = 4 sweeps exactly the owned 24 x 64 pixels are, and those
-// are written back.  Out-of-image cells hold their clamped ('nearest') neighbour and are
-// refreshed after every sweep; H uses 'constant' 0 through the border flags.
+// Tile: 56 x 24 owned pixels plus a 4-pixel halo = a 64 x 32 region, loaded by one 3-D TMA
+// (8 coefficient planes, 64 KB) and two 2-D TMAs (u, v) starting at (x0-4, y0-4): x stays
+// 16-byte aligned.  Each lane owns a column pair (2 lane, 2 lane + 1) of the region and
+// walks it down a band of rows (its warp's share of the sweep's rows), so every float32
+// step of the two cells is one packed instruction and the centre pair, the coefficient
+// pairs and the results move as 64-bit shared-memory accesses.  Sweep s computes the rows
+// at least s + 1 from the region's top and bottom edge (all later sweeps need) and every
+// column; a cell's value is exact after sweep s only if it lies at least s + 1 from the
+// region's edge, so after LB_T = 4 sweeps exactly the owned 56 x 24 pixels are, and the
+// last sweep stores those straight to global memory.  The region's outermost columns use
+// their own value as the missing neighbour (inexact, like the rest of the halo).
+// Image borders: every neighbour index is clamped into the image ('nearest'), H uses
+// 'constant' 0 through the border flags, and out-of-image rows are not computed; the cells
+// of out-of-image columns are computed from clamped values but never read.
 // The squared change of every sweep is accumulated over owned pixels only, so each pixel is
 // counted once per sweep.  The stop rule: the last CTA of a pass finds the first sweep
 // whose error is <= tol; if that is not the pass's last sweep, the pass ran too far and the
 // rollback launch recomputes the pass from its (unchanged) input with the right count.
-constexpr int LB_T = 4, LB_TW = 24, LB_TH = 64, LB_RW = LB_TW + 2 * LB_T, LB_RH = LB_TH + 2 * LB_T;  // 32 x 72
-constexpr int LB_PLANE = LB_RW * LB_RH * 4;                  // 9216 B, a multiple of 128
+constexpr int LB_T = 4, LB_TW = 56, LB_TH = 24, LB_RW = LB_TW + 2 * LB_T, LB_RH = LB_TH + 2 * LB_T;  // 64 x 32
+constexpr int LB_PLANE = LB_RW * LB_RH * 4;                  // 8192 B, a multiple of 128
+constexpr int LB_PL = LB_RW * LB_RH;                         // floats per plane
 constexpr int LB_COEF_BYTES = 8 * LB_PLANE;
 constexpr size_t LB_SMEM = LB_COEF_BYTES + 4 * LB_PLANE + 128 + 128;  // coef + 2 x (u, v) + barrier + slack
-constexpr int LB_ROWS = (LB_RH + 7) / 8;                       // rows per thread (9)
+constexpr int LB_WARPS = 8;
 
 typedef float LbPlane[LB_RW];
 
@@ -229,103 +284,151 @@ struct LbPass {  // per-launch description of a pass
   int redo;      // 1: rollback launch (sweep count read from redo[pass])
 };
 
-__device__ __forceinline__ void lb_refresh(LbPlane* u, LbPlane* v, int x0, int y0, int H, int W, int t) {
-  for (int e = t; e < LB_RH * LB_RW; e += 256) {
-    int r = e / LB_RW, c = e - r * LB_RW;
-    int gy = y0 - LB_T + r, gx = x0 - LB_T + c;
-    if (gy >= 0 && gy < H && gx >= 0 && gx < W) continue;
-    int sy = clampi(gy, 0, H - 1) - (y0 - LB_T), sx = clampi(gx, 0, W - 1) - (x0 - LB_T);
-    if (sy < 0 || sy >= LB_RH || sx < 0 || sx >= LB_RW) continue;
-    u[r][c] = u[sy][sx];
-    v[r][c] = v[sy][sx];
-  }
-}
-
-// One row of a thread's 3x3 window: the three u, v values as float32 and float64.
+// One window row of a lane: the float32 centre pair and the float64 values of the four
+// columns 2 lane - 1 .. 2 lane + 2 (clamped), for u and v.
 struct LbRow {
-  float fu[3], fv[3];
-  double du[3], dv[3];
+  float2 cu, cv;
+  double du[4], dv[4];
 };
 
-__device__ __forceinline__ void lb_load(LbRow& R, const LbPlane* su, const LbPlane* sv, int row, int c) {
-#pragma unroll
-  for (int j = 0; j < 3; j++) {
-    R.fu[j] = su[row][c - 1 + j];
-    R.fv[j] = sv[row][c - 1 + j];
-    R.du[j] = (double)R.fu[j];
-    R.dv[j] = (double)R.fv[j];
+// Columns of a lane's window: k[0..3] for 2 lane - 1 .. 2 lane + 2.  EDGE tiles clamp all
+// four into the image; interior tiles only the two outside the region (lanes 0 and 31).
+struct LbCols {
+  int k[4];
+};
+
+template <bool EDGE>
+__device__ __forceinline__ void lb_load(LbRow& R, const LbPlane* su, const LbPlane* sv, int row, const LbCols& c) {
+  if (EDGE) {
+    R.cu = f2(su[row][c.k[1]], su[row][c.k[2]]);
+    R.cv = f2(sv[row][c.k[1]], sv[row][c.k[2]]);
+  } else {
+    R.cu = *reinterpret_cast<const float2*>(&su[row][c.k[1]]);
+    R.cv = *reinterpret_cast<const float2*>(&sv[row][c.k[1]]);
+  }
+  R.du[0] = (double)su[row][c.k[0]];
+  R.du[1] = (double)R.cu.x;
+  R.du[2] = (double)R.cu.y;
+  R.du[3] = (double)su[row][c.k[3]];
+  R.dv[0] = (double)sv[row][c.k[0]];
+  R.dv[1] = (double)R.cv.x;
+  R.dv[2] = (double)R.cv.y;
+  R.dv[3] = (double)sv[row][c.k[3]];
+}
+
+struct LbStrip {  // what a lane needs beyond the window rows
+  const float* sc;  // coefficient planes
+  const LbPlane *su, *sv;  // input buffers of the sweep
+  int kl, kr;       // the window's outer columns (clamped 2 lane - 1, 2 lane + 2)
+  LbPlane *ou, *ov;  // output buffers of the sweep (null on the last sweep)
+  float *gu, *gv;   // global output of the last sweep, at the lane's even column, row 0 of the region
+  int pitch;
+  int c0;           // the lane's even region column
+  int gx0, gy0;     // global x of column c0, global y of the strip's first row
+  int H, W;
+  float h;
+  float one;        // 1.0f, unknown to the assembler (see pfma)
+  bool own_col;     // the pair lies in the owned columns
+};
+
+// Update of the lane's cell pair in region row `row` from window rows U (above), C, D (below).
+template <bool EDGE>
+__device__ __forceinline__ void lb_pair(const LbRow& U, const LbRow& C, const LbRow& D, const LbStrip& S, int row,
+                                        int gy, bool own_row, double& acc_u, double& acc_v) {
+  const bool T = gy == 0, B = gy == S.H - 1;
+  const bool L0 = S.gx0 == 0, R0 = S.gx0 == S.W - 1, L1 = S.gx0 + 1 == 0, R1 = S.gx0 + 1 == S.W - 1;
+  const int o = row * LB_RW + S.c0;
+  const float* sc = S.sc;
+  const float2 a = *reinterpret_cast<const float2*>(sc + o);
+  const float2 b = *reinterpret_cast<const float2*>(sc + LB_PL + o);
+  const float2 cc = *reinterpret_cast<const float2*>(sc + 2 * LB_PL + o);
+  // the outer columns of the centre row again as float32 (cheaper than keeping them live)
+  const float2 Lu = f2(S.su[row][S.kl], C.cu.x), Ru = f2(C.cu.y, S.su[row][S.kr]);
+  const float2 Lv = f2(S.sv[row][S.kl], C.cv.x), Rv = f2(C.cv.y, S.sv[row][S.kr]);
+  const float2 Du = st2x2(U.cu, D.cu, -0.5f, 0.5f), DTu = st2x2(Lu, Ru, -0.5f, 0.5f);
+  const float2 Dv = st2x2(U.cv, D.cv, -0.5f, 0.5f), DTv = st2x2(Lv, Rv, -0.5f, 0.5f);
+  const float2 Fu = st2x2(U.cu, D.cu, 1.0f, 1.0f), FTv = st2x2(Lv, Rv, 1.0f, 1.0f);
+  const float2 Mu = f2(st_m(U.du, D.du, 1), st_m(U.du, D.du, 2));
+  const float2 Mv = f2(st_m(U.dv, D.dv, 1), st_m(U.dv, D.dv, 2));
+  const float2 Hu = f2(st_h<EDGE>(U.du, C.du, D.du, 1, T, B, L0, R0), st_h<EDGE>(U.du, C.du, D.du, 2, T, B, L1, R1));
+  const float2 Hv = f2(st_h<EDGE>(U.dv, C.dv, D.dv, 1, T, B, L0, R0), st_h<EDGE>(U.dv, C.dv, D.dv, 2, T, B, L1, R1));
+  const float2 h2 = f2s(S.h), two = f2s(2.0f), one = f2s(S.one);
+  // acc + x * y with two roundings: fma(x * y, one, acc)
+#define LB_MAC(acc, x, y) pfma(pmul((x), (y)), one, (acc))
+  float2 bu = pmul(pmul(two, a), Du);
+  bu = LB_MAC(bu, a, DTv);
+  bu = LB_MAC(bu, b, Dv);
+  bu = LB_MAC(bu, cc, Fu);
+  bu = LB_MAC(bu, cc, Mv);
+  bu = LB_MAC(bu, h2, Hu);
+  bu = padd(bu, *reinterpret_cast<const float2*>(sc + 3 * LB_PL + o));
+  float2 bv = pmul(b, Du);
+  bv = LB_MAC(bv, a, DTu);
+  bv = LB_MAC(bv, pmul(two, b), DTv);
+  bv = LB_MAC(bv, cc, Mu);
+  bv = LB_MAC(bv, cc, FTv);
+  bv = LB_MAC(bv, h2, Hv);
+  bv = padd(bv, *reinterpret_cast<const float2*>(sc + 4 * LB_PL + o));
+  const float2 B11 = *reinterpret_cast<const float2*>(sc + 5 * LB_PL + o);
+  const float2 B12 = *reinterpret_cast<const float2*>(sc + 6 * LB_PL + o);
+  const float2 B22 = *reinterpret_cast<const float2*>(sc + 7 * LB_PL + o);
+  const float2 m1 = f2s(-S.one);  // exact negation, the sign of zero included
+  const float2 nu = pmul(LB_MAC(pmul(B11, bu), B12, bv), m1);
+  const float2 nv = pmul(LB_MAC(pmul(B12, bu), B22, bv), m1);
+#undef LB_MAC
+  const bool in0 = S.gx0 < S.W, in1 = S.gx0 + 1 < S.W;
+  if (S.ou) {
+    *reinterpret_cast<float2*>(&S.ou[row][S.c0]) = nu;
+    *reinterpret_cast<float2*>(&S.ov[row][S.c0]) = nv;
+  } else if (own_row && S.own_col) {  // last sweep: owned cells straight to global
+    const size_t gi = (size_t)row * S.pitch;
+    if (in1) {
+      *reinterpret_cast<float2*>(S.gu + gi) = nu;
+      *reinterpret_cast<float2*>(S.gv + gi) = nv;
+    } else if (in0) {
+      S.gu[gi] = nu.x;
+      S.gv[gi] = nv.x;
+    }
+  }
+  if (own_row && S.own_col) {
+    // float32 change, as the reference's unew - u; squares summed in double
+    const float2 eu = pfma(C.cu, m1, nu), ev = pfma(C.cv, m1, nv);
+    const float eu0 = in0 ? eu.x : 0.0f, ev0 = in0 ? ev.x : 0.0f;
+    const float eu1 = in1 ? eu.y : 0.0f, ev1 = in1 ? ev.y : 0.0f;
+    acc_u = __fma_rn((double)eu0, (double)eu0, acc_u);
+    acc_u = __fma_rn((double)eu1, (double)eu1, acc_u);
+    acc_v = __fma_rn((double)ev0, (double)ev0, acc_v);
+    acc_v = __fma_rn((double)ev1, (double)ev1, acc_v);
   }
 }
 
-// Update of the cell (row, c) from its window rows U (above), C (centre), D (below).
+// One sweep of a lane's band: rows [r0, r0 + n) of its column pair.  The three window rows
+// rotate through three register sets (3-row steps), so sliding the window costs loads only.
+// EDGE tiles clamp the window rows into [rlo, rhi].
 template <bool EDGE>
-__device__ __forceinline__ void lb_cell(const LbRow& U, const LbRow& C, const LbRow& D, LbPlane* du_, LbPlane* dv_,
-                                        const float* sc, int row, int c, int gx, int gy, int H, int W, float h,
-                                        bool own, double& acc_u, double& acc_v) {
-  if (EDGE && (gy < 0 || gy >= H || gx < 0 || gx >= W)) return;  // refreshed from its clamp source
-  const bool T = gy == 0, B = gy == H - 1, L = gx == 0, R = gx == W - 1;
-  const double du[3][3] = {{U.du[0], U.du[1], U.du[2]}, {C.du[0], C.du[1], C.du[2]}, {D.du[0], D.du[1], D.du[2]}};
-  const double dv[3][3] = {{U.dv[0], U.dv[1], U.dv[2]}, {C.dv[0], C.dv[1], C.dv[2]}, {D.dv[0], D.dv[1], D.dv[2]}};
-  const int o = row * LB_RW + c;
-  const int PL = LB_RW * LB_RH;
-  const float a = sc[o], b = sc[PL + o], cc = sc[2 * PL + o];
-  float Du = st2(U.fu[1], D.fu[1], -0.5f, 0.5f), DTu = st2(C.fu[0], C.fu[2], -0.5f, 0.5f);
-  float Dv = st2(U.fv[1], D.fv[1], -0.5f, 0.5f), DTv = st2(C.fv[0], C.fv[2], -0.5f, 0.5f);
-  float Fu = st2(U.fu[1], D.fu[1], 1.0f, 1.0f), FTv = st2(C.fv[0], C.fv[2], 1.0f, 1.0f);
-  float Mu = st_m(du), Mv = st_m(dv);
-  float Hu = st_h<EDGE>(du, T, B, L, R), Hv = st_h<EDGE>(dv, T, B, L, R);
-  float bu = __fmul_rn(__fmul_rn(2.0f, a), Du);
-  bu = __fadd_rn(bu, __fmul_rn(a, DTv));
-  bu = __fadd_rn(bu, __fmul_rn(b, Dv));
-  bu = __fadd_rn(bu, __fmul_rn(cc, Fu));
-  bu = __fadd_rn(bu, __fmul_rn(cc, Mv));
-  bu = __fadd_rn(bu, __fmul_rn(h, Hu));
-  bu = __fadd_rn(bu, sc[3 * PL + o]);
-  float bv = __fmul_rn(b, Du);
-  bv = __fadd_rn(bv, __fmul_rn(a, DTu));
-  bv = __fadd_rn(bv, __fmul_rn(__fmul_rn(2.0f, b), DTv));
-  bv = __fadd_rn(bv, __fmul_rn(cc, Mu));
-  bv = __fadd_rn(bv, __fmul_rn(cc, FTv));
-  bv = __fadd_rn(bv, __fmul_rn(h, Hv));
-  bv = __fadd_rn(bv, sc[4 * PL + o]);
-  const float B11 = sc[5 * PL + o], B12 = sc[6 * PL + o], B22 = sc[7 * PL + o];
-  float nu = -__fadd_rn(__fmul_rn(B11, bu), __fmul_rn(B12, bv));
-  float nv = -__fadd_rn(__fmul_rn(B12, bu), __fmul_rn(B22, bv));
-  du_[row][c] = nu;
-  dv_[row][c] = nv;
-  if (own) {
-    double eu = __dadd_rn((double)nu, -C.du[1]), ev = __dadd_rn((double)nv, -C.dv[1]);
-    acc_u = __fma_rn(eu, eu, acc_u);
-    acc_v = __fma_rn(ev, ev, acc_v);
-  }
-}
-
-// One sweep of one thread's column strip: rows [r0, r0+n) of column c (1 <= c <= RW-2).
-// The three window rows rotate through three register sets (3-row steps), so sliding the
-// window costs loads only.
-template <bool EDGE>
-__device__ __forceinline__ void lb_strip(const LbPlane* su, const LbPlane* sv, LbPlane* du_, LbPlane* dv_,
-                                         const float* sc, int c, int r0, int n, int gx, int gy0, int H, int W, float h,
-                                         bool own_col, double& acc_u, double& acc_v) {
+__device__ __forceinline__ void lb_strip(const LbPlane* su, const LbPlane* sv, const LbStrip& S, const LbCols& cols,
+                                         int r0, int n, int rlo, int rhi, double& acc_u, double& acc_v) {
   LbRow A, B, C;
-  lb_load(A, su, sv, r0 - 1, c);
-  lb_load(B, su, sv, r0, c);
-#define LB_OWN(row) (own_col && (row) >= LB_T && (row) < LB_T + LB_TH)
+#define LB_ROW(r) (EDGE ? clampi((r), rlo, rhi) : (r))
+#define LB_OWN(row) ((row) >= LB_T && (row) < LB_T + LB_TH)
+  lb_load<EDGE>(A, su, sv, LB_ROW(r0 - 1), cols);
+  lb_load<EDGE>(B, su, sv, r0, cols);
 #pragma unroll 1
   for (int r = 0; r < n; r += 3) {
     const int row = r0 + r;
-    lb_load(C, su, sv, row + 1, c);
-    lb_cell<EDGE>(A, B, C, du_, dv_, sc, row, c, gx, gy0 + r, H, W, h, LB_OWN(row), acc_u, acc_v);
+    lb_load<EDGE>(C, su, sv, LB_ROW(row + 1), cols);
+    lb_pair<EDGE>(A, B, C, S, row, S.gy0 + r, LB_OWN(row), acc_u, acc_v);
     if (r + 1 < n) {
-      lb_load(A, su, sv, row + 2, c);
-      lb_cell<EDGE>(B, C, A, du_, dv_, sc, row + 1, c, gx, gy0 + r + 1, H, W, h, LB_OWN(row + 1), acc_u, acc_v);
+      lb_load<EDGE>(A, su, sv, LB_ROW(row + 2), cols);
+      lb_pair<EDGE>(B, C, A, S, row + 1, S.gy0 + r + 1, LB_OWN(row + 1), acc_u, acc_v);
     }
     if (r + 2 < n) {
-      lb_load(B, su, sv, row + 3, c);
-      lb_cell<EDGE>(C, A, B, du_, dv_, sc, row + 2, c, gx, gy0 + r + 2, H, W, h, LB_OWN(row + 2), acc_u, acc_v);
+      lb_load<EDGE>(B, su, sv, LB_ROW(row + 3), cols);
+      lb_pair<EDGE>(C, A, B, S, row + 2, S.gy0 + r + 2, LB_OWN(row + 2), acc_u, acc_v);
     }
   }
 #undef LB_OWN
+#undef LB_ROW
 }
 
 __global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__ CUtensorMap tm_coef,
@@ -334,7 +437,7 @@ __global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__
                                                          float* __restrict__ un, float* __restrict__ vn, int H, int W,
                                                          int pitch, float h, LbPass P, LsCtrl* ctrl, double* ss,
                                                          int* run, unsigned int* done, int* redo, double inv_n,
-                                                         double tol, int* err_flag, int final_buf) {
+                                                         double tol, int* err_flag, int final_buf, float one) {
   int nsw = P.nsweep;
   if (P.redo) {
     nsw = *(volatile int*)(redo + P.pass);
@@ -350,7 +453,8 @@ __global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__
 #define LB_V(q) reinterpret_cast<LbPlane*>(base + LB_COEF_BYTES + (2 * (q) + 1) * LB_PLANE)
   uint64_t* bar = reinterpret_cast<uint64_t*>(base + LB_COEF_BYTES + 4 * LB_PLANE);
   const int x0 = blockIdx.x * LB_TW, y0 = blockIdx.y * LB_TH;
-  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x, warp = threadIdx.y;
+  const int t = warp * 32 + lane;
   if (t == 0) mbar_init(bar, 1);
   __syncthreads();
   if (t == 0) {
@@ -364,70 +468,77 @@ __global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__
     mbar_wait(bar, 0, LS_WAIT_LIMIT);  // one more bounded wait for the copies in flight
     nsw = 0;
   }
-  const bool edge = x0 < LB_T || y0 < LB_T || x0 + LB_TW + LB_T > W || y0 + LB_TH + LB_T > H;
+  // in-image region rows / columns (region row r <-> y0 - 4 + r, column c <-> x0 - 4 + c)
+  const int rlo = max(0, LB_T - y0), rhi = min(LB_RH - 1, H - 1 + LB_T - y0);
+  const int clo = max(0, LB_T - x0), chi = min(LB_RW - 1, W - 1 + LB_T - x0);
+  const bool edge = rlo > 0 || clo > 0 || rhi < LB_RH - 1 || chi < LB_RW - 1;
+  const int c0 = 2 * lane;
+  LbCols cols;
   if (edge) {
-    __syncthreads();
-    lb_refresh(LB_U(0), LB_V(0), x0, y0, H, W, t);
+#pragma unroll
+    for (int j = 0; j < 4; j++) cols.k[j] = clampi(c0 - 1 + j, clo, chi);
+  } else {
+    cols.k[0] = max(c0 - 1, 0);
+    cols.k[1] = c0;
+    cols.k[2] = c0 + 1;
+    cols.k[3] = min(c0 + 2, LB_RW - 1);
   }
+  LbStrip S;
+  S.sc = sc;
+  S.kl = cols.k[0];
+  S.kr = cols.k[3];
+  S.pitch = pitch;
+  S.c0 = c0;
+  S.gx0 = x0 - LB_T + c0;
+  S.H = H;
+  S.W = W;
+  S.h = h;
+  S.one = one;
+  S.own_col = c0 >= LB_T && c0 < LB_T + LB_TW;
+  __shared__ double red[LB_T][2][LB_WARPS];
   __syncthreads();
-  const int c = threadIdx.x;  // region column
-  const int gx = x0 - LB_T + c;
-  const bool own_col = c >= LB_T && c < LB_T + LB_TW;
-  int r0 = threadIdx.y * LB_ROWS, r1 = r0 + LB_ROWS;
-  if (r0 < 1) r0 = 1;
-  if (r1 > LB_RH - 1) r1 = LB_RH - 1;
-  __shared__ double red[LB_T][2][8];
 #pragma unroll 1
   for (int s = 0; s < nsw; s++) {
     const int in = s & 1, out = in ^ 1;
+    const bool last = s == nsw - 1;
     double au = 0.0, av = 0.0;
-    // sweep s only needs the rows at least s + 1 from the region's edge (later sweeps
-    // read no others)
-    const int ra = r0 > 1 + s ? r0 : 1 + s, rb = r1 < LB_RH - 1 - s ? r1 : LB_RH - 1 - s;
-    if (c >= 1 && c <= LB_RW - 2 && rb > ra) {
+    // sweep s computes the rows at least s + 1 from the region's edge (later sweeps read no
+    // others) that lie in the image, split evenly over the warps
+    const int lo = max(1 + s, rlo), hi = min(LB_RH - 1 - s, rhi + 1);
+    const int n = hi - lo;
+    const int ra = lo + (n * warp) / LB_WARPS, rb = lo + (n * (warp + 1)) / LB_WARPS;
+    if (rb > ra) {
+      S.su = LB_U(in);
+      S.sv = LB_V(in);
+      S.ou = last ? nullptr : LB_U(out);
+      S.ov = last ? nullptr : LB_V(out);
+      // global address of (row 0, column c0) of the region; only owned cells are stored
+      S.gu = un + ((ptrdiff_t)(y0 - LB_T) * pitch + S.gx0);
+      S.gv = vn + ((ptrdiff_t)(y0 - LB_T) * pitch + S.gx0);
+      S.gy0 = y0 - LB_T + ra;
       if (edge)
-        lb_strip<true>(LB_U(in), LB_V(in), LB_U(out), LB_V(out), sc, c, ra, rb - ra, gx, y0 - LB_T + ra, H, W, h,
-                       own_col, au, av);
+        lb_strip<true>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
       else
-        lb_strip<false>(LB_U(in), LB_V(in), LB_U(out), LB_V(out), sc, c, ra, rb - ra, gx, y0 - LB_T + ra, H, W,
-                        h, own_col, au, av);
+        lb_strip<false>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
     }
     if (!P.redo) {
       for (int o = 16; o > 0; o >>= 1) {
         au += __shfl_down_sync(0xffffffffu, au, o);
         av += __shfl_down_sync(0xffffffffu, av, o);
       }
-      if ((t & 31) == 0) {
-        red[s][0][t >> 5] = au;
-        red[s][1][t >> 5] = av;
+      if (lane == 0) {
+        red[s][0][warp] = au;
+        red[s][1][warp] = av;
       }
     }
     __syncthreads();
-    if (edge) {
-      lb_refresh(LB_U(out), LB_V(out), x0, y0, H, W, t);
-      __syncthreads();
-    }
-  }
-  // owned pixels of the last sweep -> global
-  if (nsw > 0) {
-    const LbPlane* fu = LB_U(nsw & 1);
-    const LbPlane* fv = LB_V(nsw & 1);
-    for (int e = t; e < LB_TW * LB_TH; e += 256) {
-      int r = e / LB_TW, cl = e - r * LB_TW;
-      int y = y0 + r, x = x0 + cl;
-      if (y < H && x < W) {
-        size_t i = (size_t)y * pitch + x;
-        un[i] = fu[r + LB_T][cl + LB_T];
-        vn[i] = fv[r + LB_T][cl + LB_T];
-      }
-    }
   }
   if (P.redo) return;
   // per-sweep squared changes -> ss[k0 + s]; the last CTA applies the stop rule
   if (t == 0) {
     for (int s = 0; s < nsw; s++) {
       double a = 0.0, b = 0.0;
-      for (int w = 0; w < 8; w++) {
+      for (int w = 0; w < LB_WARPS; w++) {
         a += red[s][0][w];
         b += red[s][1][w];
       }
@@ -571,11 +682,11 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
     const int in = p & 1, out = in ^ 1;
     LbPass P0{k0, maxnum - k0 < LB_T ? maxnum - k0 : LB_T, p, 0};
     ls_pass_kernel<<<pgrd, pblk, LB_SMEM, st>>>(tm_coef, tm_u[in], tm_v[in], ub[out], vb[out], H, W, P, h, P0, ctrl, ss,
-                                               run, done, redo, inv_n, tol, err_flag, out);
+                                               run, done, redo, inv_n, tol, err_flag, out, 1.0f);
     LbPass P1 = P0;
     P1.redo = 1;  // rollback: recompute this pass with the sweep count the stop rule chose
     ls_pass_kernel<<<pgrd, pblk, LB_SMEM, st>>>(tm_coef, tm_u[in], tm_v[in], ub[out], vb[out], H, W, P, h, P1, ctrl, ss,
-                                               run, done, redo, inv_n, tol, err_flag, out);
+                                               run, done, redo, inv_n, tol, err_flag, out, 1.0f);
     nl += 2;
   }
   ls_count_kernel<<<1, 1, 0, st>>>(ctrl, ss, inv_n, err_flag, iters_out, err_out);

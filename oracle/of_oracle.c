@@ -326,7 +326,8 @@ EXPORT void ofo_ls_sweep(const float* coef, const float* u, const float* v, floa
       bv = bv + Iyt[i];
       float nu = -(B11[i] * bu + B12[i] * bv);
       float nv = -(B12[i] * bu + B22[i] * bv);
-      double du = (double)nu - u[i], dv = (double)nv - v[i];
+      /* float32 change as the reference's unew - u (:79); squares summed in double */
+      double du = (double)(float)(nu - u[i]), dv = (double)(float)(nv - v[i]);
       su += du * du;
       sv += dv * dv;
       un[i] = nu;

@@ -175,6 +175,25 @@ def test_ls_vs_oracle(torch_cuda, n):
     assert np.array_equal(host(U), Uo) and np.array_equal(host(V), Vo)
 
 
+@pytest.mark.parametrize("shape,maxnum", [((1, 9), 5), ((7, 5), 9), ((25, 57), 9), ((49, 113), 13),
+                                           ((130, 171), 7), ((24, 56), 4), ((97, 1), 6)])
+def test_ls_ragged_vs_oracle(torch_cuda, shape, maxnum):
+    """Shapes that are not multiples of the 56 x 24 pass tile (odd widths, single rows and
+    columns, images smaller than one tile) and sweep counts that end mid-pass."""
+    from ofb200 import ops
+    r = rng(sum(shape) + maxnum)
+    a = r.uniform(1, 255, shape).astype(np.float32)
+    b = r.uniform(1, 255, shape).astype(np.float32)
+    U0 = r.normal(0, 0.5, shape).astype(np.float32)
+    V0 = r.normal(0, 0.5, shape).astype(np.float32)
+    U, V, it, e = ops.ls_solve(dev(torch_cuda, a), dev(torch_cuda, b), dev(torch_cuda, U0), dev(torch_cuda, V0), 10,
+                               maxnum, 1e-30)
+    Uo, Vo, eo, ito = O.ls_solve(a, b, U0, V0, 10, maxnum, 1e-30)
+    assert int(it.item()) == ito == maxnum
+    assert np.array_equal(host(U), Uo) and np.array_equal(host(V), Vo)
+    assert float(e.item()) == pytest.approx(eo, rel=1e-9)
+
+
 @pytest.mark.parametrize("tol", [1e-3, 1e-5, 1e-30])
 def test_ls_stop_rule(torch_cuda, tol):
     """The device-side stop rule ends at the same sweep as the reference loop."""
