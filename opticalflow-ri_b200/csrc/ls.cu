@@ -250,15 +250,16 @@ __device__ __forceinline__ float st_h(const double* U, const double* C, const do
 
 // Temporally blocked sweeps: one pass runs up to LB_T sweeps on a tile held in shared
 // memory, so the 8 coefficient planes and (u, v) cross HBM/L2 once per LB_T sweeps.
-// Tile: 56 x 24 owned pixels plus a 4-pixel halo = a 64 x 32 region, loaded by one 3-D TMA
-// (8 coefficient planes, 64 KB) and two 2-D TMAs (u, v) starting at (x0-4, y0-4): x stays
-// 16-byte aligned.  Each lane owns a column pair (2 lane, 2 lane + 1) of the region and
+// Tile: 56 x 23 owned pixels plus a 4-pixel halo = a 64 x 31 region, loaded by one 3-D TMA
+// (8 coefficient planes, 62 KB) and two 2-D TMAs (u, v) starting at (x0-4, y0-4): x stays
+// 16-byte aligned.  (23 rows: a 1024 x 1024 image is 19 x 45 tiles, 2.9 waves of 2 CTAs
+// on 148 SMs.)  Each lane owns a column pair (2 lane, 2 lane + 1) of the region and
 // walks it down a band of rows (its warp's share of the sweep's rows), so every float32
 // step of the two cells is one packed instruction and the centre pair, the coefficient
 // pairs and the results move as 64-bit shared-memory accesses.  Sweep s computes the rows
 // at least s + 1 from the region's top and bottom edge (all later sweeps need) and every
 // column; a cell's value is exact after sweep s only if it lies at least s + 1 from the
-// region's edge, so after LB_T = 4 sweeps exactly the owned 56 x 24 pixels are, and the
+// region's edge, so after LB_T = 4 sweeps exactly the owned 56 x 23 pixels are, and the
 // last sweep stores those straight to global memory.  The region's outermost columns use
 // their own value as the missing neighbour (inexact, like the rest of the halo).
 // Image borders: every neighbour index is clamped into the image ('nearest'), H uses
@@ -267,13 +268,18 @@ __device__ __forceinline__ float st_h(const double* U, const double* C, const do
 // The squared change of every sweep is accumulated over owned pixels only, so each pixel is
 // counted once per sweep.  The stop rule: the last CTA of a pass finds the first sweep
 // whose error is <= tol; if that is not the pass's last sweep, the pass ran too far and the
-// rollback launch recomputes the pass from its (unchanged) input with the right count.
-constexpr int LB_T = 4, LB_TW = 56, LB_TH = 24, LB_RW = LB_TW + 2 * LB_T, LB_RH = LB_TH + 2 * LB_T;  // 64 x 32
-constexpr int LB_PLANE = LB_RW * LB_RH * 4;                  // 8192 B, a multiple of 128
+// next launch (which the stop rule has cancelled as a pass) recomputes it from its
+// unchanged input with the right count.
+constexpr int LB_T = 4, LB_TW = 56, LB_TH = 23, LB_RW = LB_TW + 2 * LB_T, LB_RH = LB_TH + 2 * LB_T;  // 64 x 31
+constexpr int LB_PLANE = LB_RW * LB_RH * 4;                  // 7936 B, a multiple of 128 (TMA destinations)
+static_assert(LB_PLANE % 128 == 0, "each staged plane must start 128-byte aligned");
 constexpr int LB_PL = LB_RW * LB_RH;                         // floats per plane
 constexpr int LB_COEF_BYTES = 8 * LB_PLANE;
 constexpr size_t LB_SMEM = LB_COEF_BYTES + 4 * LB_PLANE + 128 + 128;  // coef + 2 x (u, v) + barrier + slack
-constexpr int LB_WARPS = 8;
+#ifndef OF_LS_PASS_WARPS
+#define OF_LS_PASS_WARPS 6
+#endif
+constexpr int LB_WARPS = OF_LS_PASS_WARPS;  // warps per CTA, each a band of the region's rows
 
 typedef float LbPlane[LB_RW];
 
@@ -281,7 +287,7 @@ struct LbPass {  // per-launch description of a pass
   int k0;        // first sweep index
   int nsweep;    // sweeps in this pass (<= LB_T)
   int pass;      // pass index
-  int redo;      // 1: rollback launch (sweep count read from redo[pass])
+  int last;      // 1: the launch after the last pass, which only rolls that pass back
 };
 
 // One window row of a lane: the float32 centre pair and the float64 values of the four
@@ -431,20 +437,34 @@ __device__ __forceinline__ void lb_strip(const LbPlane* su, const LbPlane* sv, c
 #undef LB_ROW
 }
 
-__global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__ CUtensorMap tm_coef,
-                                                         const __grid_constant__ CUtensorMap tm_u,
-                                                         const __grid_constant__ CUtensorMap tm_v,
-                                                         float* __restrict__ un, float* __restrict__ vn, int H, int W,
+__global__ void __launch_bounds__(32 * LB_WARPS, 2) ls_pass_kernel(const __grid_constant__ CUtensorMap tm_coef,
+                                                         const __grid_constant__ CUtensorMap tm_u0,
+                                                         const __grid_constant__ CUtensorMap tm_v0,
+                                                         const __grid_constant__ CUtensorMap tm_u1,
+                                                         const __grid_constant__ CUtensorMap tm_v1,
+                                                         float* ub0, float* vb0, float* ub1, float* vb1, int H, int W,
                                                          int pitch, float h, LbPass P, LsCtrl* ctrl, double* ss,
                                                          int* run, unsigned int* done, int* redo, double inv_n,
-                                                         double tol, int* err_flag, int final_buf, float one) {
-  int nsw = P.nsweep;
-  if (P.redo) {
-    nsw = *(volatile int*)(redo + P.pass);
-    if (nsw == 0) return;
-  } else if (P.k0 > 0 && *(volatile int*)(run + P.k0) == 0) {
-    return;  // the stop rule ended the loop in an earlier pass
+                                                         double tol, int* err_flag, float one) {
+  // Pass p reads ping-pong buffer p & 1 and writes the other.  A pass that the stop rule
+  // cancelled (and the launch after the last pass) instead rolls the previous pass back
+  // when that pass ran past its stopping sweep: it recomputes it from the same input with
+  // the sweep count the stop rule chose (redo[p - 1]) and keeps no error sums.
+  int k0 = P.k0, nsw = P.nsweep, pass = P.pass;
+  bool rollback = false;
+  if (P.last || (k0 > 0 && *(volatile int*)(run + k0) == 0)) {
+    const int r = pass > 0 ? *(volatile int*)(redo + pass - 1) : 0;
+    if (r == 0) return;
+    rollback = true;
+    pass -= 1;
+    k0 -= LB_T;
+    nsw = r;
   }
+  const int in = pass & 1, out = in ^ 1;
+  const CUtensorMap* tm_u = in ? &tm_u1 : &tm_u0;
+  const CUtensorMap* tm_v = in ? &tm_v1 : &tm_v0;
+  float* un = out ? ub1 : ub0;
+  float* vn = out ? vb1 : vb0;
   extern __shared__ __align__(128) unsigned char lb_smem_raw[];
   unsigned char* base = lb_smem_raw + ((128 - (smem_u32(lb_smem_raw) & 127)) & 127);
   const float* sc = reinterpret_cast<const float*>(base);
@@ -460,8 +480,8 @@ __global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__
   if (t == 0) {
     mbar_expect_tx(bar, LB_COEF_BYTES + 2 * LB_PLANE);
     tma_load_3d((void*)sc, &tm_coef, x0 - LB_T, y0 - LB_T, 0, bar);
-    tma_load_2d(LB_U(0), &tm_u, x0 - LB_T, y0 - LB_T, bar);
-    tma_load_2d(LB_V(0), &tm_v, x0 - LB_T, y0 - LB_T, bar);
+    tma_load_2d(LB_U(0), tm_u, x0 - LB_T, y0 - LB_T, bar);
+    tma_load_2d(LB_V(0), tm_v, x0 - LB_T, y0 - LB_T, bar);
   }
   if (!mbar_wait(bar, 0, LS_WAIT_LIMIT)) {
     if (t == 0) atomicExch(err_flag, 1);
@@ -521,7 +541,7 @@ __global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__
       else
         lb_strip<false>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
     }
-    if (!P.redo) {
+    if (!rollback) {
       for (int o = 16; o > 0; o >>= 1) {
         au += __shfl_down_sync(0xffffffffu, au, o);
         av += __shfl_down_sync(0xffffffffu, av, o);
@@ -533,7 +553,7 @@ __global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__
     }
     __syncthreads();
   }
-  if (P.redo) return;
+  if (rollback) return;
   // per-sweep squared changes -> ss[k0 + s]; the last CTA applies the stop rule
   if (t == 0) {
     for (int s = 0; s < nsw; s++) {
@@ -542,29 +562,29 @@ __global__ void __launch_bounds__(256, 2) ls_pass_kernel(const __grid_constant__
         a += red[s][0][w];
         b += red[s][1][w];
       }
-      atomicAdd(ss + 2 * (P.k0 + s), a);
-      atomicAdd(ss + 2 * (P.k0 + s) + 1, b);
+      atomicAdd(ss + 2 * (k0 + s), a);
+      atomicAdd(ss + 2 * (k0 + s) + 1, b);
     }
     __threadfence();
-    if (atomicAdd(done + P.pass, 1u) == gridDim.x * gridDim.y - 1) {
+    if (atomicAdd(done + pass, 1u) == gridDim.x * gridDim.y - 1) {
       __threadfence();
       int stop = -1;
       for (int s = 0; s < nsw; s++) {
-        double s0 = atomicAdd(ss + 2 * (P.k0 + s), 0.0), s1 = atomicAdd(ss + 2 * (P.k0 + s) + 1, 0.0);
+        double s0 = atomicAdd(ss + 2 * (k0 + s), 0.0), s1 = atomicAdd(ss + 2 * (k0 + s) + 1, 0.0);
         if (!((sqrt(s0) + sqrt(s1)) * inv_n > tol)) {
           stop = s;
           break;
         }
       }
       if (stop < 0) {
-        run[P.k0 + nsw] = 1;
-        ctrl->K = P.k0 + nsw;
+        run[k0 + nsw] = 1;
+        ctrl->K = k0 + nsw;
       } else {
-        run[P.k0 + nsw] = 0;
-        ctrl->K = P.k0 + stop + 1;
-        redo[P.pass] = (stop < nsw - 1) ? stop + 1 : 0;
+        run[k0 + nsw] = 0;
+        ctrl->K = k0 + stop + 1;
+        redo[pass] = (stop < nsw - 1) ? stop + 1 : 0;
       }
-      ctrl->final_buf = final_buf;
+      ctrl->final_buf = out;
     }
   }
 }
@@ -676,18 +696,22 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   ls_coef_kernel<<<grd, blk, 0, st>>>(n1, et, coef, N, H, W, P, h);
   ls_copy2_kernel<<<rg, 256, 0, st>>>(V, U, ub[0], vb[0], W, pitch, P, nullptr);
   double inv_n = 1.0 / ((double)H * (double)W);
-  dim3 pgrd((W + LB_TW - 1) / LB_TW, (H + LB_TH - 1) / LB_TH), pblk(32, 8);
+  dim3 pgrd((W + LB_TW - 1) / LB_TW, (H + LB_TH - 1) / LB_TH), pblk(32, LB_WARPS);
   long long nl = 5;
-  for (int k0 = 0, p = 0; k0 < maxnum; k0 += LB_T, p++) {
-    const int in = p & 1, out = in ^ 1;
+  int p = 0, k0 = 0;
+  for (; k0 < maxnum; k0 += LB_T, p++) {
     LbPass P0{k0, maxnum - k0 < LB_T ? maxnum - k0 : LB_T, p, 0};
-    ls_pass_kernel<<<pgrd, pblk, LB_SMEM, st>>>(tm_coef, tm_u[in], tm_v[in], ub[out], vb[out], H, W, P, h, P0, ctrl, ss,
-                                               run, done, redo, inv_n, tol, err_flag, out, 1.0f);
-    LbPass P1 = P0;
-    P1.redo = 1;  // rollback: recompute this pass with the sweep count the stop rule chose
-    ls_pass_kernel<<<pgrd, pblk, LB_SMEM, st>>>(tm_coef, tm_u[in], tm_v[in], ub[out], vb[out], H, W, P, h, P1, ctrl, ss,
-                                               run, done, redo, inv_n, tol, err_flag, out, 1.0f);
-    nl += 2;
+    ls_pass_kernel<<<pgrd, pblk, LB_SMEM, st>>>(tm_coef, tm_u[0], tm_v[0], tm_u[1], tm_v[1], ub[0], vb[0], ub[1],
+                                               vb[1], H, W, P, h, P0, ctrl, ss, run, done, redo, inv_n, tol,
+                                               err_flag, 1.0f);
+    nl++;
+  }
+  if (p > 0) {  // rolls the last pass back if it ran past the stopping sweep
+    LbPass PL{k0, 0, p, 1};
+    ls_pass_kernel<<<pgrd, pblk, LB_SMEM, st>>>(tm_coef, tm_u[0], tm_v[0], tm_u[1], tm_v[1], ub[0], vb[0], ub[1],
+                                               vb[1], H, W, P, h, PL, ctrl, ss, run, done, redo, inv_n, tol,
+                                               err_flag, 1.0f);
+    nl++;
   }
   ls_count_kernel<<<1, 1, 0, st>>>(ctrl, ss, inv_n, err_flag, iters_out, err_out);
   ls_finalize_kernel<<<rg, 256, 0, st>>>(ub[0], vb[0], ub[1], vb[1], V, U, W, P, pitch, ctrl);
