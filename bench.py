@@ -62,7 +62,7 @@ def parse():
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
     p.add_argument("--learned-weights", default=None, help="weights + calibration .npz (default: packaged)")
     p.add_argument("--batch-pairs", type=int, default=256, help="--mode batch: pairs in the manifest")
-    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn"],
+    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn", "fb"],
                    help="ls: only the Liu-Shen solve of one pair, --steps times (for profiling)")
     return p.parse_args()
 
@@ -87,6 +87,35 @@ def run_ls_only(args):
         if r >= args.warmup:
             ms.append(e0.elapsed_time(e1))
     print(json.dumps({"mode": "ls", "size": args.size, "sweeps": int(it.item()), "ms": float(np.mean(ms))}))
+
+
+def run_fb_only(args):
+    """One fused Farneback iteration (33-tap window, all 5 planes, updateFlow + updateMatrices)
+    at --size on a synthetic pair's polynomial expansions, --warmup + --steps times."""
+    import torch
+    import Farneback_PyCL as F
+    from ofb200 import ops
+    a, b, _, _ = make_pairs(1, args.size)[0]
+    fb = F.Farneback_PyCL()
+    A, B = ops.u8_to_f32(torch.from_numpy(a).cuda()), ops.u8_to_f32(torch.from_numpy(b).cuda())
+    RA, RB = ops.fb_polyexp(A, fb._poly), ops.fb_polyexp(B, fb._poly)
+    cx, cy = torch.zeros_like(A), torch.zeros_like(A)
+    M = ops.fb_update_matrices(cx, cy, RA, RB)
+    Mb = torch.empty_like(M)
+    fb.setGaussianBlurKernel(fb.windowSize, fb.windowSize / 2 * 0.3)
+    wk = fb.matrixGKernel[0]
+    ms = []
+    for r in range(args.warmup + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ops.fb_iteration(M, Mb, RA, RB, cx, cy, wk, True)
+        e1.record()
+        e1.synchronize()
+        if r >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+    px = args.size * args.size
+    print(json.dumps({"mode": "fb", "size": args.size, "ms": float(np.mean(ms)),
+                      "gbs_88B_per_px": 88.0 * px / (float(np.mean(ms)) * 1e-3) / 1e9}))
 
 
 def run_cnn(args):
@@ -546,6 +575,9 @@ def main():
         return
     if args.mode == "cnn":
         run_cnn(args)
+        return
+    if args.mode == "fb":
+        run_fb_only(args)
         return
     if args.mode == "batch":
         if world > 1:

@@ -306,6 +306,7 @@ struct FbkGeom {
   static constexpr int IW = FBK_TW + 2 * KH, IH = FBK_TH + 2 * KH;
   static constexpr int STAGE = IW * IH * 4;  // bytes of one staged input plane tile
   static constexpr size_t SMEM = 2 * STAGE + (size_t)FBK_TH * IW * 4 + 128 + 128;
+  static_assert(2 * STAGE >= 5 * FBK_TH * FBK_TW * 4, "the epilogue's plane transpose reuses the stages");
 };
 
 // reflect-101 fix-up of a staged tile: cells outside the image take their mirror image
@@ -404,24 +405,32 @@ __global__ void __launch_bounds__(256, 2) fb_iter_fixed_kernel(const __grid_cons
     }
     __syncthreads();
   }
-  const int y = y0 + hy;
-  if (y >= H) return;
-  if (!ok) {  // a tile copy never arrived: the tile's flow is reported as NaN
+  // The blurred planes go through shared memory (the staging buffers are free now) so the
+  // epilogue runs one pixel per lane: its flow / R0 / M accesses and the R1 gathers of
+  // neighbouring lanes fall on neighbouring addresses.
+  float* rs = stage[0];  // [plane][FBK_TH][FBK_TW], 40 KB of the two 24 KB stages
 #pragma unroll
-    for (int r = 0; r < FBK_R; r++)
-      if (x0 + hx + r < W) {
-        flowx[(size_t)y * pitch + x0 + hx + r] = __int_as_float(0x7fc00000);
-        flowy[(size_t)y * pitch + x0 + hx + r] = __int_as_float(0x7fc00000);
-      }
-    return;
+  for (int p = 0; p < 5; p++) {
+    float4* d = reinterpret_cast<float4*>(rs + (p * FBK_TH + hy) * FBK_TW + hx);
+    d[0] = make_float4(res[p][0], res[p][1], res[p][2], res[p][3]);
+    d[1] = make_float4(res[p][4], res[p][5], res[p][6], res[p][7]);
   }
-#pragma unroll
-  for (int r = 0; r < FBK_R; r++) {
-    const int x = x0 + hx + r;
-    if (x >= W) continue;
-    float fx, fy;
-    fb_flow_from(res[0][r], res[1][r], res[2][r], res[3][r], res[4][r], &fx, &fy);
+  __syncthreads();
+#pragma unroll 1
+  for (int o = threadIdx.x; o < FBK_TH * FBK_TW; o += 256) {
+    const int ly = o / FBK_TW, lx = o - ly * FBK_TW;
+    const int y = y0 + ly, x = x0 + lx;
+    if (y >= H || x >= W) continue;
     const size_t i = (size_t)y * pitch + x;
+    if (!ok) {  // a tile copy never arrived: the tile's flow is reported as NaN
+      flowx[i] = __int_as_float(0x7fc00000);
+      flowy[i] = __int_as_float(0x7fc00000);
+      continue;
+    }
+    const float* q = rs + ly * FBK_TW + lx;
+    float fx, fy;
+    fb_flow_from(q[0], q[FBK_TH * FBK_TW], q[2 * FBK_TH * FBK_TW], q[3 * FBK_TH * FBK_TW], q[4 * FBK_TH * FBK_TW], &fx,
+                 &fy);
     flowx[i] = fx;
     flowy[i] = fy;
     if (upd) fb_matrices_at(y, x, fx, fy, R0, R1, Mout, H, W, pitch);
