@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--pairs", type=int, default=8, help="frame pairs per step per GPU")
     p.add_argument("--size", type=int, default=1024)
     p.add_argument("--unique", type=int, default=4, help="distinct synthetic pairs (cycled)")
-    p.add_argument("--streams", type=int, default=4,
+    p.add_argument("--streams", type=int, default=8,
                    help="concurrent CUDA streams per step (1: pairs one after another)")
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -369,7 +369,7 @@ def run_ours(args, rank, world, local_rank):
 
 def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
     """The learned warm start on the same frames: one network forward over the step's
-    pairs (512^2 level), Farneback at full size from that start, then the calibrated number
+    pairs (at the network's level), Farneback at full size from that start, then the calibrated number
     of Liu-Shen sweeps; pairs whose last update norm exceeds the calibrated threshold are
     recomputed by the plain pyramid inside the timed region.  Endpoint errors of both arms
     against the analytic ground truth (16 px interior) on the distinct pairs."""
@@ -390,11 +390,10 @@ def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
         lb = LearnedBatch(net, meta, args.pairs, args.size, streams=args.streams, start=start)
 
         def step():
-            f32 = [(ops.u8_to_f32(a8), ops.u8_to_f32(b8)) for a8, b8 in step_frames]
-            res, errs = lb.run(f32)
+            res, errs = lb.run(step_frames)  # uint8 frames, converted inside the graph
             if start == "zero":
                 return list(res), 0
-            return lb.fallback(f32, res, errs.cpu())
+            return lb.fallback(step_frames, res, errs.cpu())
 
         for _ in range(args.warmup):
             step()

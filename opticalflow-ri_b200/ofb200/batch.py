@@ -116,9 +116,8 @@ class PairBatch:
                 e = (g, static_in, static_out, nk)
                 self._graphs[key] = e
             g, static_in, static_out, nk = e
-            for (sa, sb), (a, b) in zip(static_in, frames):
-                sa.copy_(a)
-                sb.copy_(b)
+            # all inputs into the graph's buffers with one multi-tensor copy
+            torch._foreach_copy_([t for p in static_in for t in p], [t for p in frames for t in p])
             g.replay()
             _graph._replayed_kernels += nk
             return static_out

@@ -390,6 +390,11 @@ def load_trained(path=WEIGHTS, device="cuda"):
     return WarmStartNet(device=device).load(path), meta
 
 
+def _as_f32(t):
+    """A float32 frame (uint8 / uint16 frames through the conversion kernel)."""
+    return t if t.dtype == torch.float32 else ops.u8_to_f32(t)
+
+
 class LearnedBatch:
     """n frame pairs of one size through the learned pipeline: one network forward over
     the batch, then each pair's full-size stage on one of `streams` CUDA streams; the
@@ -416,6 +421,7 @@ class LearnedBatch:
         cur = torch.cuda.current_stream()
         if self._streams is None:
             self._streams = [torch.cuda.Stream() for _ in range(self.nstreams)]
+        frames = [(_as_f32(A), _as_f32(B)) for A, B in frames]  # uint8 / uint16 frames converted in the graph
         out = None
         if self.start == "cnn":
             b = self.net.buffers(self.n, self.size // self.ll.factor)
@@ -440,7 +446,7 @@ class LearnedBatch:
         return res, errs
 
     def run(self, frames):
-        """frames: n (frame1, frame2) float32 CUDA tensors of size x size."""
+        """frames: n (frame1, frame2) CUDA tensors of size x size (float32, uint8 or uint16)."""
         if len(frames) != self.n:
             raise ValueError("one frame pair per batch slot")
         if not self.use_graph:
@@ -456,9 +462,8 @@ class LearnedBatch:
                 static_out = self._step(static_in)
             self._graph = (g, static_in, static_out)
         g, static_in, static_out = self._graph
-        for (sa, sb), (a, b) in zip(static_in, frames):
-            sa.copy_(a)
-            sb.copy_(b)
+        # all inputs into the graph's buffers with one multi-tensor copy
+        torch._foreach_copy_([t for p in static_in for t in p], [t for p in frames for t in p])
         g.replay()
         return static_out
 
@@ -474,7 +479,7 @@ class LearnedBatch:
         bad = (errs > thr).nonzero().flatten().tolist()
         out = list(res)
         for i in bad:
-            A, B = frames[i]
+            A, B = _as_f32(frames[i][0]), _as_f32(frames[i][1])
             out[i] = G.genericPyramidalOpticalFlow(A, B, 0, F.Farneback_PyCL(), 2, 1, 0.48,
                                                    LS.LiuShenOpticalFlowAlgoAdapter(10))
         return out, len(bad)

@@ -1,5 +1,5 @@
 """The learned Liu-Shen warm start end to end: the batched, graph-replayed pipeline equals
-the single-pair one, and on held-out pairs of the 1024^2 workload (seeds outside both the
+the single-pair one (1024^2 frames), and on held-out pairs of the 1024^2 workload (seeds outside both the
 training and the calibration sets) the packaged network gives a lower interior endpoint
 error than the plain pyramid and than the same full-size stage started from zero."""
 import numpy as np
@@ -34,13 +34,13 @@ def test_batch_matches_single_pair(torch_cuda, trained):
     from ofb200.warmstart import LearnedBatch, LearnedLiuShen
     net, meta = trained
     frames = []
-    for seed in (1, 2, 3):
-        a, b, _, _ = S.config_pair("fbls1024", seed=seed, size=512)
+    for seed in (1, 2, 3):  # the benchmark's frame size: the network's deepest scale fills its tiles
+        a, b, _, _ = S.config_pair("fbls1024", seed=seed)
         frames.append((_f32(torch, a), _f32(torch, b)))
     ll = LearnedLiuShen.from_meta(net, meta)
     want = [ll.run(A, B) for A, B in frames]
     want = [(U.cpu().numpy(), V.cpu().numpy(), float(e.item())) for U, V, _, e in want]
-    lb = LearnedBatch(net, meta, 3, size=512, streams=2)
+    lb = LearnedBatch(net, meta, 3, size=1024, streams=2)
     for _ in range(2):  # capture, then replay
         res, errs = lb.run(frames)
         torch.cuda.synchronize()
