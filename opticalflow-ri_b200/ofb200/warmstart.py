@@ -2,11 +2,12 @@
 
 The plain pipeline (Farneback at 512^2 and 1024^2, each followed by 60 Liu-Shen sweeps)
 spends most of its time getting a good initial field for the last Liu-Shen solve.  Here an
-encoder-decoder CNN maps the 512^2 level's frame pair (the pyramid's bicubic downsample,
-each frame divided by its maximum) to a flow at 512^2; the spline upsample (x2) turns it
-into the initial field of a Liu-Shen solve at 1024^2 with fewer sweeps.  The solve's last
-update norm (its convergence residual) judges the result: above a threshold calibrated on
-held-out pairs, the pair falls back to the plain pyramid.
+encoder-decoder CNN maps a pyramid level's frame pair (the bicubic downsample by `factor`,
+each frame divided by its maximum; the packaged weights run at 128^2 for 1024^2 frames) to
+a flow at that level; one fused bilinear upsample turns it into the initial field of a
+short full-size stage (one Farneback iteration and a few Liu-Shen sweeps for the packaged
+calibration).  The solve's last update norm (its convergence residual) judges the result:
+above a threshold calibrated on held-out pairs, the pair falls back to the plain pyramid.
 
 Network (bf16 NHWC activations, f32 accumulation; ~1.75 M parameters):
 
@@ -312,7 +313,7 @@ class WarmStartNet:
 
 
 class LearnedLiuShen:
-    """CNN warm start at the 512^2 level, spline upsample, then at full size either
+    """CNN warm start at the level 1/`factor` of the frame size, bilinear upsample, then at full size either
     Liu-Shen alone (mode "ls") or the pyramid's last level, Farneback (`fb_iters`
     iterations) then Liu-Shen (mode "fb"), with `sweeps` Liu-Shen sweeps.
 

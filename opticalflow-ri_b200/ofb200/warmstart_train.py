@@ -6,9 +6,10 @@
    radius, 0.02-0.1 particles/px, noise sigma 0-5 DN, diameter 2-3 px, max 4 px) are
    rendered on the host cores by a spawn process pool.
 2. Each pair is labelled by the plain pipeline on the GPU (Farneback pyr2 + Liu-Shen h = 10,
-   the package's converged output); frames and label are taken to the 512^2 level (the
-   pyramid's bicubic downsample; the label also halved in magnitude).
-3. The network is trained on random 256^2 crops (Adam, mean squared flow error) with the
+   the package's converged output); frames and label are taken to the --level size (the
+   pyramid's bicubic downsample; the label scaled by level / 1024 in magnitude).  The
+   packaged weights: --level 128 --crop 128.
+3. The network is trained on random --crop crops (Adam, mean squared flow error) with the
    package's own forward / backward kernels.
 4. On held-out pairs of the 1024^2 benchmark workload (disjoint seeds) the plain pipeline,
    the network's start followed by each full-size stage (Liu-Shen alone with K sweeps, or
