@@ -62,7 +62,7 @@ def parse():
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
     p.add_argument("--learned-weights", default=None, help="weights + calibration .npz (default: packaged)")
     p.add_argument("--batch-pairs", type=int, default=256, help="--mode batch: pairs in the manifest")
-    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn", "fb"],
+    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn", "fb", "e2e"],
                    help="ls: only the Liu-Shen solve of one pair, --steps times (for profiling)")
     return p.parse_args()
 
@@ -87,6 +87,27 @@ def run_ls_only(args):
         if r >= args.warmup:
             ms.append(e0.elapsed_time(e1))
     print(json.dumps({"mode": "ls", "size": args.size, "sweeps": int(it.item()), "ms": float(np.mean(ms))}))
+
+
+def run_e2e_only(args):
+    """The drop-in call alone (genericPyramidalOpticalFlow with numpy float32 frames in and
+    numpy U, V out), --warmup + --steps calls, wall clock per call."""
+    import torch
+    pairs = make_pairs(args.unique, args.size)
+    host = [(a.astype(np.float32), b.astype(np.float32)) for a, b, _, _ in pairs]
+    import Farneback_PyCL as F
+    import GenericPyramidalOpticalFlow as G
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    ms = []
+    for r in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        G.genericPyramidalOpticalFlow(*host[r % len(host)], 0, F.Farneback_PyCL(), 2, 1, 0.48,
+                                      LS.LiuShenOpticalFlowAlgoAdapter(10))
+        if r >= args.warmup:
+            ms.append((time.perf_counter() - t0) * 1e3)
+    print(json.dumps({"mode": "e2e", "size": args.size, "ms_per_call": float(np.mean(ms)),
+                      "pairs_per_s": 1e3 / float(np.mean(ms))}))
 
 
 def run_fb_only(args):
@@ -577,6 +598,9 @@ def main():
         return
     if args.mode == "fb":
         run_fb_only(args)
+        return
+    if args.mode == "e2e":
+        run_e2e_only(args)
         return
     if args.mode == "batch":
         if world > 1:

@@ -50,6 +50,12 @@ unsigned long long of_launch_count(void);
  * returns its full length. */
 int of_last_error(char* buf, size_t n);
 
+/* Host memcpy of `bytes` between two non-overlapping HOST buffers, split over a small
+ * persistent pool of threads when it is 1 MiB or more (the staging copies of host-buffer
+ * calls: numpy frame -> pinned upload buffer, pinned download buffer -> numpy result).
+ * Blocking; one pooled copy runs at a time; a forked child copies on its own thread. */
+int of_host_copy(void* dst, const void* src, size_t bytes);
+
 /* ---------------------------------------------------------------------------------
  * A1 Gaussian prefilter — replaces gaussian_filterPx / convolveSeparableFilter
  * (src/gaussian_filter.py:54-94).  Separable K-tap FIR (K odd, 1..81; H, W >= K/2), row pass then
@@ -88,6 +94,12 @@ int of_resize(const float* src, int Hs, int Ws, int src_pitch, float* dst, int H
 size_t of_spline_workspace_size(int h, int w, int H, int W);
 int of_spline_upsample(const float* src, int h, int w, int src_pitch, float* dst, int H, int W, int dst_pitch,
                        float scale, void* workspace, size_t workspace_bytes, void* stream);
+/* Both flow components of one level transition in the same launches (twice the lines in
+ * flight for the serial spline recurrences): results equal two of_spline_upsample calls.
+ * Workspace: 2 * of_spline_workspace_size(h, w, H, W) bytes. */
+int of_spline_upsample_pair(const float* src_u, const float* src_v, int h, int w, int src_pitch, float* dst_u,
+                            float* dst_v, int H, int W, int dst_pitch, float scale_u, float scale_v, void* workspace,
+                            size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------------
  * A4 symmetric bilinear warp — replaces doBiLinearWarping as called at

@@ -173,8 +173,11 @@ class Farneback_PyCL(object):
                 cy = ops.scale(ops.resize(prev[1], (width, height), bicubic=False), 1.0 / self.pyrScale)
             self.setGaussianBlurKernel(smoothSize, sigma)
             gk = self.matrixGKernel[0]
-            RA = ops.fb_polyexp(ops.resize(ops.fb_blur(im1, gk, 1), (width, height), bicubic=False), self._poly)
-            RB = ops.fb_polyexp(ops.resize(ops.fb_blur(im2, gk, 1), (width, height), bicubic=False), self._poly)
+            # the blurred frame is only read by the expansion: no copy at the full-size level
+            RA = ops.fb_polyexp(ops.resize(ops.fb_blur(im1, gk, 1), (width, height), bicubic=False, copy=False),
+                                self._poly)
+            RB = ops.fb_polyexp(ops.resize(ops.fb_blur(im2, gk, 1), (width, height), bicubic=False, copy=False),
+                                self._poly)
             M = ops.fb_update_matrices(cx, cy, RA, RB)
             if self.useGaussianFilter:
                 self.setGaussianBlurKernel(self.windowSize, self.windowSize / 2 * 0.3)

@@ -64,8 +64,11 @@ def _transition(n1, prev_shape, n2, Ua, Va, warping, biLinear, scale):
     sx = np.float32(np.float32(W) / np.float32(w)) if scale else np.float32(1.0)
     sy = np.float32(np.float32(H) / np.float32(h)) if scale else np.float32(1.0)
     if (h, w) != (H, W):
-        us = ops.spline_upsample(Ua, H, W, sx)
-        vs = ops.spline_upsample(Va, H, W, sy)
+        if Ua.shape == Va.shape and Ua.stride(0) == Va.stride(0):
+            us, vs = ops.spline_upsample_pair(Ua, Va, H, W, sx, sy)
+        else:
+            us = ops.spline_upsample(Ua, H, W, sx)
+            vs = ops.spline_upsample(Va, H, W, sy)
     else:
         us = ops.scale(Ua, sx) if scale else Ua
         vs = ops.scale(Va, sy) if scale else Va

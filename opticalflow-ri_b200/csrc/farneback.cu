@@ -309,17 +309,33 @@ struct FbkGeom {
   static_assert(2 * STAGE >= 5 * FBK_TH * FBK_TW * 4, "the epilogue's plane transpose reuses the stages");
 };
 
-// reflect-101 fix-up of a staged tile: cells outside the image take their mirror image
+// reflect-101 fix-up of a staged tile: cells outside the image take their mirror image.
+// Only those cells are visited: the out-of-image rows [0, rt) and [rb, IH) in full, and
+// the out-of-image columns [0, cl) and [cr, IW) of the rows in between.
 template <int KH>
 __device__ __forceinline__ void fbk_reflect(float* tin, int x0, int y0, int H, int W) {
   constexpr int IW = FbkGeom<KH>::IW, IH = FbkGeom<KH>::IH;
-  for (int i = threadIdx.x; i < IH * IW; i += 256) {
-    int ly = i / IW, lx = i - ly * IW;
-    int gy = y0 - KH + ly, gx = x0 - KH + lx;
-    if (gy >= 0 && gy < H && gx >= 0 && gx < W) continue;
-    int sy = fb_row(gy, H) - (y0 - KH), sx = fb_col(gx, W) - (x0 - KH);
+  const int rt = min(max(KH - y0, 0), IH), rb = max(min(H - (y0 - KH), IH), rt);
+  const int cl = min(max(KH - x0, 0), IW), cr = max(min(W - (x0 - KH), IW), cl);
+  const int nt = rt * IW, nb = (IH - rb) * IW, side = cl + (IW - cr), n = nt + nb + (rb - rt) * side;
+  for (int i = threadIdx.x; i < n; i += 256) {
+    int ly, lx;
+    if (i < nt) {
+      ly = i / IW;
+      lx = i - ly * IW;
+    } else if (i < nt + nb) {
+      const int k = i - nt;
+      ly = rb + k / IW;
+      lx = k - (ly - rb) * IW;
+    } else {
+      const int k = i - nt - nb, r = k / side, c = k - r * side;
+      ly = rt + r;
+      lx = c < cl ? c : cr + (c - cl);
+    }
+    const int gy = y0 - KH + ly, gx = x0 - KH + lx;
+    const int sy = fb_row(gy, H) - (y0 - KH), sx = fb_col(gx, W) - (x0 - KH);
     if (sy < 0 || sy >= IH || sx < 0 || sx >= IW) continue;  // only outside every used window
-    tin[i] = tin[sy * IW + sx];
+    tin[ly * IW + lx] = tin[sy * IW + sx];
   }
 }
 

@@ -228,21 +228,33 @@ __device__ __forceinline__ void fine_index(int j, int N, int n, int* i, double* 
   *t = __dadd_rn(s, -(double)k);
 }
 
+// One or two planes (blockIdx of the plane dimension) upsampled by the same launches; plane
+// p's workspace arrays sit `pstride` doubles after plane 0's, and both use plane 0's pivots.
+struct SplinePlanes {
+  const float* src[2];
+  float* dst[2];
+  float scale[2];
+  size_t pstride;
+};
+
 // moments along y for each coarse column x, read straight from the float field (pitch sp)
-__global__ void __launch_bounds__(128) spline_my_kernel(const float* __restrict__ src, int sp, int h, int w,
-                                                        double* M, double* S, const double* __restrict__ cp) {
+__global__ void __launch_bounds__(128) spline_my_kernel(SplinePlanes P, int sp, int h, int w, double* M, double* S,
+                                                        const double* __restrict__ cp) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= w) return;
+  const int q = blockIdx.y;
   // moments and scratch are laid out [i][x] with stride w
-  nak_moments<float>(src + x, (size_t)sp, (size_t)w, M + x, cp, S + x, h);
+  nak_moments<float>((q ? P.src[1] : P.src[0]) + x, (size_t)sp, (size_t)w, M + q * P.pstride + x, cp, S + q * P.pstride + x, h);
 }
 
 // Tt[x][Y] = column spline of coarse column x at fine row Y.  A 32x32 tile goes through
 // shared memory so the reads (along x) and the transposed writes (along Y) both coalesce.
-__global__ void __launch_bounds__(256) spline_ey_kernel(const float* __restrict__ src, int sp,
-                                                        const double* __restrict__ M, double* __restrict__ Tt,
-                                                        int h, int w, int H) {
+__global__ void __launch_bounds__(256) spline_ey_kernel(SplinePlanes P, int sp, const double* __restrict__ M,
+                                                        double* __restrict__ Tt, int h, int w, int H) {
   __shared__ double tile[32][33];
+  const float* __restrict__ src = blockIdx.z ? P.src[1] : P.src[0];
+  M += blockIdx.z * P.pstride;
+  Tt += blockIdx.z * P.pstride;
   int x0 = blockIdx.x * 32, Y0 = blockIdx.y * 32;
   int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
   for (int k = ty; k < 32; k += 8) {
@@ -264,10 +276,11 @@ __global__ void __launch_bounds__(256) spline_ey_kernel(const float* __restrict_
 
 // moments along x for each fine row Y of Tt (layout [k][Y], stride H)
 __global__ void __launch_bounds__(128) spline_mx_kernel(const double* __restrict__ Tt, int w, int H, double* M,
-                                                        const double* __restrict__ cp, double* dp) {
+                                                        const double* __restrict__ cp, double* dp, size_t pstride) {
   int Y = blockIdx.x * blockDim.x + threadIdx.x;
   if (Y >= H) return;
-  nak_moments<double>(Tt + Y, (size_t)H, (size_t)H, M + Y, cp, dp + Y, w);
+  const size_t o = blockIdx.y * pstride;
+  nak_moments<double>(Tt + o + Y, (size_t)H, (size_t)H, M + o + Y, cp, dp + o + Y, w);
 }
 
 // dst[Y][X] = row spline of fine row Y at fine column X (times scale).  The coarse
@@ -275,9 +288,12 @@ __global__ void __launch_bounds__(128) spline_mx_kernel(const double* __restrict
 // along Y) are staged through shared memory with loads that coalesce along Y.
 #define EX_SPAN 40
 __global__ void __launch_bounds__(256) spline_ex_kernel(const double* __restrict__ Tt, const double* __restrict__ M,
-                                                        float* __restrict__ dst, int dpitch, int w, int H, int W,
-                                                        float scale) {
+                                                        SplinePlanes P, int dpitch, int w, int H, int W) {
   __shared__ double sT[EX_SPAN][33], sM[EX_SPAN][33];
+  Tt += blockIdx.z * P.pstride;
+  M += blockIdx.z * P.pstride;
+  float* __restrict__ dst = blockIdx.z ? P.dst[1] : P.dst[0];
+  const float scale = blockIdx.z ? P.scale[1] : P.scale[0];
   int X0 = blockIdx.x * 32, Y0 = blockIdx.y * 32;
   int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
   int Xl = min(X0 + 31, W - 1);
@@ -481,6 +497,26 @@ extern "C" size_t of_spline_workspace_size(int h, int w, int H, int W) {
   return s.off;
 }
 
+static int spline_run(const SplinePlanes& P0, int np, int h, int w, int src_pitch, int H, int W, int dst_pitch,
+                      void* workspace, size_t single, cudaStream_t st) {
+  size_t a = (size_t)h * w, b = (size_t)H * w;
+  Carver c(workspace, single);
+  double* My = c.take<double>(a);
+  double* Sy = c.take<double>(a);
+  double* piv = c.take<double>((size_t)(h > w ? h : w));
+  double* Tt = c.take<double>(b);
+  double* Mx = c.take<double>(b);
+  double* Sx = c.take<double>(b);
+  SplinePlanes P = P0;
+  P.pstride = single / sizeof(double);
+  spline_recip_kernel<<<1, 256, 0, st>>>(piv, (h > w ? h : w) - 4);
+  spline_my_kernel<<<dim3((w + 127) / 128, np), 128, 0, st>>>(P, src_pitch, h, w, My, Sy, piv);
+  spline_ey_kernel<<<dim3((w + 31) / 32, (H + 31) / 32, np), dim3(32, 8), 0, st>>>(P, src_pitch, My, Tt, h, w, H);
+  spline_mx_kernel<<<dim3((H + 127) / 128, np), 128, 0, st>>>(Tt, w, H, Mx, piv, Sx, P.pstride);
+  spline_ex_kernel<<<dim3((W + 31) / 32, (H + 31) / 32, np), dim3(32, 8), 0, st>>>(Tt, Mx, P, dst_pitch, w, H, W);
+  return check_launch("of_spline_upsample", 5);
+}
+
 extern "C" int of_spline_upsample(const float* src, int h, int w, int src_pitch, float* dst, int H, int W,
                                   int dst_pitch, float scale, void* workspace, size_t workspace_bytes, void* stream) {
   OF_REQUIRE(!bad_plane(src, h, w, src_pitch) && !bad_plane(dst, H, W, dst_pitch), "of_spline_upsample: bad plane");
@@ -488,22 +524,24 @@ extern "C" int of_spline_upsample(const float* src, int h, int w, int src_pitch,
   size_t need = of_spline_workspace_size(h, w, H, W);
   if (!workspace || workspace_bytes < need)
     return set_error(OF_ERR_WORKSPACE, "of_spline_upsample: workspace too small (%zu < %zu)", workspace_bytes, need);
-  cudaStream_t st = as_stream(stream);
-  size_t a = (size_t)h * w, b = (size_t)H * w;
-  Carver c(workspace, workspace_bytes);
-  double* My = c.take<double>(a);
-  double* Sy = c.take<double>(a);
-  double* piv = c.take<double>((size_t)(h > w ? h : w));
-  double* Tt = c.take<double>(b);
-  double* Mx = c.take<double>(b);
-  double* Sx = c.take<double>(b);
-  spline_recip_kernel<<<1, 256, 0, st>>>(piv, (h > w ? h : w) - 4);
-  spline_my_kernel<<<(w + 127) / 128, 128, 0, st>>>(src, src_pitch, h, w, My, Sy, piv);
-  spline_ey_kernel<<<dim3((w + 31) / 32, (H + 31) / 32), dim3(32, 8), 0, st>>>(src, src_pitch, My, Tt, h, w, H);
-  spline_mx_kernel<<<(H + 127) / 128, 128, 0, st>>>(Tt, w, H, Mx, piv, Sx);
-  spline_ex_kernel<<<dim3((W + 31) / 32, (H + 31) / 32), dim3(32, 8), 0, st>>>(Tt, Mx, dst, dst_pitch, w, H, W,
-                                                                              scale);
-  return check_launch("of_spline_upsample", 5);
+  SplinePlanes P{{src, src}, {dst, dst}, {scale, scale}, 0};
+  return spline_run(P, 1, h, w, src_pitch, H, W, dst_pitch, workspace, need, as_stream(stream));
+}
+
+extern "C" int of_spline_upsample_pair(const float* src_u, const float* src_v, int h, int w, int src_pitch,
+                                       float* dst_u, float* dst_v, int H, int W, int dst_pitch, float scale_u,
+                                       float scale_v, void* workspace, size_t workspace_bytes, void* stream) {
+  OF_REQUIRE(!bad_plane(src_u, h, w, src_pitch) && !bad_plane(src_v, h, w, src_pitch) &&
+                 !bad_plane(dst_u, H, W, dst_pitch) && !bad_plane(dst_v, H, W, dst_pitch),
+             "of_spline_upsample_pair: bad plane");
+  OF_REQUIRE(dst_u != dst_v, "of_spline_upsample_pair: the two outputs alias");
+  OF_REQUIRE(h >= 4 && w >= 4, "of_spline_upsample_pair: the coarse field needs at least 4x4 samples");
+  size_t single = of_spline_workspace_size(h, w, H, W);
+  if (!workspace || workspace_bytes < 2 * single)
+    return set_error(OF_ERR_WORKSPACE, "of_spline_upsample_pair: workspace too small (%zu < %zu)", workspace_bytes,
+                     2 * single);
+  SplinePlanes P{{src_u, src_v}, {dst_u, dst_v}, {scale_u, scale_v}, 0};
+  return spline_run(P, 2, h, w, src_pitch, H, W, dst_pitch, workspace, single, as_stream(stream));
 }
 
 extern "C" int of_warp_pair_bilinear(const float* I0, const float* I1, const float* U, const float* V, float* O0,

@@ -72,17 +72,38 @@ def to_host(t):
 _PINNED_OUT = {}
 
 
+def par_copyto(dst: np.ndarray, src: np.ndarray) -> None:
+    """np.copyto(dst, src) for the staging copies of host-buffer calls.  Same-dtype
+    C-contiguous planes go through of_host_copy, which splits a large copy over a small
+    pool of native threads (ctypes releases the interpreter lock for the call); anything
+    else (a cast, a strided view) through numpy."""
+    if (dst.dtype == src.dtype and dst.shape == src.shape and dst.flags.c_contiguous and src.flags.c_contiguous
+            and dst.nbytes >= (1 << 20)):
+        from ._lib import call
+        call("of_host_copy", dst.ctypes.data, src.ctypes.data, dst.nbytes)
+        return
+    np.copyto(dst, src)
+
+
 def to_host_pair(a, b):
     """Two same-shape float32 CUDA planes -> two new numpy arrays: asynchronous copies into
-    cached pinned buffers and one synchronisation."""
+    cached pinned buffers; the first plane leaves the pinned buffer (threaded host copy)
+    while the second is still being downloaded."""
     torch = _torch()
     key = (tuple(a.shape), a.device.index)
     if a.shape != b.shape or a.dtype != torch.float32 or b.dtype != torch.float32:
         return to_host(a), to_host(b)
     buf = _PINNED_OUT.get(key)
     if buf is None:
-        buf = _PINNED_OUT[key] = tuple(torch.empty(a.shape, dtype=torch.float32, pin_memory=True) for _ in range(2))
+        buf = _PINNED_OUT[key] = (torch.empty(a.shape, dtype=torch.float32, pin_memory=True),
+                                  torch.empty(a.shape, dtype=torch.float32, pin_memory=True), torch.cuda.Event())
+    stream = torch.cuda.current_stream(a.device)
     buf[0].copy_(a, non_blocking=True)
+    buf[2].record(stream)
     buf[1].copy_(b, non_blocking=True)
-    torch.cuda.current_stream(a.device).synchronize()
-    return buf[0].numpy().copy(), buf[1].numpy().copy()
+    out = (np.empty(a.shape, dtype=np.float32), np.empty(b.shape, dtype=np.float32))
+    buf[2].synchronize()
+    par_copyto(out[0], buf[0].numpy())
+    stream.synchronize()
+    par_copyto(out[1], buf[1].numpy())
+    return out

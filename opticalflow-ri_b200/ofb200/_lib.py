@@ -39,6 +39,7 @@ _SIGS = {
     "of_version": ([], _I),
     "of_last_error": ([ctypes.c_char_p, _Z], _I),
     "of_launch_count": ([], ctypes.c_ulonglong),
+    "of_host_copy": ([_P, _P, _Z], _I),
     "of_prefilter_f32": ([_P, _I, _P, _I, _I, _I, _P, _I, _P], _I),
     "of_prefilter_u8": ([_P, _I, _P, _I, _I, _I, _P, _I, _P], _I),
     "of_u8_to_f32": ([_P, _I, _P, _I, _I, _I, _P], _I),
@@ -47,6 +48,7 @@ _SIGS = {
     "of_resize": ([_P, _I, _I, _I, _P, _I, _I, _I, _I, _P, _Z, _P], _I),
     "of_spline_workspace_size": ([_I, _I, _I, _I], _Z),
     "of_spline_upsample": ([_P, _I, _I, _I, _P, _I, _I, _I, _F, _P, _Z, _P], _I),
+    "of_spline_upsample_pair": ([_P, _P, _I, _I, _I, _P, _P, _I, _I, _I, _F, _F, _P, _Z, _P], _I),
     "of_warp_pair_bilinear": ([_P, _P, _P, _P, _P, _P, _I, _I, _I, _P], _I),
     "of_warp_bilinear_coords": ([_P, _P, _P, _P, _I, _I, _I, _P], _I),
     "of_accumulate": ([_P, _P, _I, _I, _I, _P], _I),

@@ -15,6 +15,8 @@ import threading
 import numpy as np
 import torch
 
+from . import par_copyto
+
 ENABLED = True
 
 _lock = threading.Lock()
@@ -66,7 +68,7 @@ class GraphCache:
                         pinned[i] = (torch.empty(s.shape, dtype=s.dtype, pin_memory=True), torch.cuda.Event())
                     p, done = pinned[i]
                     done.synchronize()  # the previous asynchronous copy out of this buffer has finished
-                    np.copyto(p.numpy(), t)
+                    par_copyto(p.numpy(), t)
                     s.copy_(p, non_blocking=True)
                     done.record()
                 else:

@@ -17,7 +17,7 @@ from . import _lib
 from ._lib import FbPolyConsts, call, lib
 
 __all__ = [
-    "prefilter", "u8_to_f32", "resize", "spline_upsample", "warp_pair", "accumulate", "scale", "hs_solve",
+    "prefilter", "u8_to_f32", "resize", "spline_upsample", "spline_upsample_pair", "warp_pair", "accumulate", "scale", "hs_solve",
     "ls_solve", "lk_dense", "fb_blur", "fb_box5", "fb_polyexp", "fb_update_matrices", "fb_update_flow",
     "fb_iteration", "workspace", "stream_ptr", "warp_liushen_scatter", "warp_liushen_ofe",
 ]
@@ -96,8 +96,13 @@ def u8_to_f32(src: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tenso
 
 
 # --------------------------------------------------------------------------- A2/A3/A4
-def resize(src: torch.Tensor, size_wh, bicubic: bool, out: torch.Tensor | None = None) -> torch.Tensor:
+def resize(src: torch.Tensor, size_wh, bicubic: bool, out: torch.Tensor | None = None,
+           copy: bool = True) -> torch.Tensor:
+    """copy=False: a same-size resize returns `src` itself (for results that are only read,
+    as the Farneback level's blurred frames are by the polynomial expansion)."""
     Wd, Hd = int(size_wh[0]), int(size_wh[1])
+    if not copy and out is None and tuple(src.shape) == (Hd, Wd):
+        return src
     s, Hs, Ws, sp = _plane(src, "resize.src")
     out = _new(Hd, Wd, src) if out is None else out
     d, _, _, dp = _plane(out, "resize.out")
@@ -114,6 +119,24 @@ def spline_upsample(src: torch.Tensor, H: int, W: int, scale: float = 1.0, out=N
     ws, wn = workspace(lib().of_spline_workspace_size(h, w, H, W), "spline")
     call("of_spline_upsample", s, h, w, sp, d, H, W, dp, float(np.float32(scale)), ws, wn, stream_ptr())
     return out
+
+
+def spline_upsample_pair(su: torch.Tensor, sv: torch.Tensor, H: int, W: int, scale_u: float = 1.0,
+                         scale_v: float = 1.0):
+    """spline_upsample of both flow components in the same launches (bit-identical)."""
+    s0, h, w, sp = _plane(su, "spline.src_u")
+    s1, _, _, sp1 = _plane(sv, "spline.src_v")
+    if sv.shape != su.shape or sp1 != sp:
+        raise ValueError("spline_upsample_pair: the two components must share shape and pitch")
+    ou, ov = _new(H, W, su), _new(H, W, su)
+    d0, _, _, dp = _plane(ou, "spline.out_u")
+    d1, _, _, dp1 = _plane(ov, "spline.out_v")
+    if dp1 != dp:
+        raise ValueError("spline_upsample_pair: output pitches differ")
+    ws, wn = workspace(2 * lib().of_spline_workspace_size(h, w, H, W), "spline")
+    call("of_spline_upsample_pair", s0, s1, h, w, sp, d0, d1, H, W, dp, float(np.float32(scale_u)),
+         float(np.float32(scale_v)), ws, wn, stream_ptr())
+    return ou, ov
 
 
 def warp_pair(I0, I1, U, V):

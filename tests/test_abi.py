@@ -49,3 +49,31 @@ def test_version_and_error_string_without_gpu():
     buf = ctypes.create_string_buffer(256)
     L.of_last_error(buf, 256)
     assert b"of_prefilter_f32" in buf.value
+
+
+def test_host_copy_without_gpu():
+    """of_host_copy (the staging copy of host-buffer calls) is host code: byte-exact for
+    sizes below and above the 1 MiB pool threshold, including lengths that do not split
+    into whole pages, and it rejects overlapping buffers."""
+    if not os.path.exists(LIB):
+        pytest.skip("libofb200.so not built")
+    import numpy as np
+    from ofb200 import _lib, par_copyto
+    L = _lib.lib()
+    rng = np.random.default_rng(3)
+    for n in (0, 1, 4095, 1 << 20, (1 << 20) + 13, 4 * 1024 * 1024 + 4097, 9 * 1024 * 1024 + 1):
+        src = rng.integers(0, 256, n, dtype=np.uint8)
+        dst = np.zeros(n, dtype=np.uint8)
+        assert L.of_host_copy(dst.ctypes.data, src.ctypes.data, n) == 0
+        assert np.array_equal(dst, src)
+    buf = np.zeros(1 << 21, dtype=np.uint8)
+    assert L.of_host_copy(buf.ctypes.data + 16, buf.ctypes.data, 1 << 20) == -1
+    # the Python helper: same-dtype planes natively, casts through numpy
+    a = rng.random((1024, 1024), dtype=np.float32)
+    b = np.empty_like(a)
+    par_copyto(b, a)
+    assert np.array_equal(a, b)
+    u8 = rng.integers(0, 256, (1024, 1024), dtype=np.uint8)
+    f = np.empty((1024, 1024), dtype=np.float32)
+    par_copyto(f, u8)
+    assert np.array_equal(f, u8.astype(np.float32))

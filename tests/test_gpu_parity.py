@@ -114,6 +114,22 @@ def test_spline_vs_oracle_scaled(torch_cuda, h, w):
     assert np.array_equal(out, O.spline_upsample(a, 2 * h, 2 * w) * np.float32(2.0))
 
 
+@pytest.mark.parametrize("h,w,H,W", [(512, 512, 1024, 1024), (64, 128, 128, 256), (4, 4, 8, 8), (5, 9, 11, 17),
+                                     (37, 50, 75, 101)])
+def test_spline_pair_equals_single(torch_cuda, h, w, H, W):
+    """Both components in the same launches give the single-plane results bit for bit
+    (and the oracle's), with different scales per component."""
+    from ofb200 import ops
+    r = rng(h + w)
+    a = r.normal(0, 2, (h, w)).astype(np.float32)
+    b = r.normal(0, 2, (h, w)).astype(np.float32)
+    su, sv = np.float32(W / w), np.float32(H / h)
+    ou, ov = ops.spline_upsample_pair(dev(torch_cuda, a), dev(torch_cuda, b), H, W, su, sv)
+    assert np.array_equal(host(ou), host(ops.spline_upsample(dev(torch_cuda, a), H, W, su)))
+    assert np.array_equal(host(ov), host(ops.spline_upsample(dev(torch_cuda, b), H, W, sv)))
+    assert np.array_equal(host(ov), O.spline_upsample(b, H, W) * sv)
+
+
 def test_warp_golden(torch_cuda):
     from ofb200 import ops
     g = golden("warp")
