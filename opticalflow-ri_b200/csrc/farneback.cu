@@ -152,6 +152,100 @@ __global__ void __launch_bounds__(FBP_T) fb_polyexp_kernel(const float* __restri
   }
 }
 
+// Tiled polynomial expansion for a compile-time half width N (polyN 5 and 7, the
+// reference's two settings).  The row kernel above loads 2N+1 samples per output from
+// global memory; here a CTA covers FBQ_R rows x FBQ_OW columns.  Each thread walks one
+// column down the tile with a register window (FBQ_R + 2N loads for FBQ_R outputs) and
+// leaves the three vertical moments in shared memory; then each thread takes 8 consecutive
+// outputs of one row with a register window along the row.  The arithmetic of every
+// output is the row kernel's, in the same order.  The moment rows are padded by one float
+// per 8 columns, so the 8-column segments of a warp's lanes fall in distinct banks.
+constexpr int FBQ_OW = 240, FBQ_R = 8, FBQ_SEG = 8;
+__device__ __forceinline__ int fbq_col(int c) { return c + (c >> 3); }
+template <int N>
+__global__ void __launch_bounds__(256) fb_polyexp_tile_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                                                              int H, int W, int pitch, FbPoly P, int vec) {
+  constexpr int CW = FBQ_OW + 2 * N;          // columns that get vertical moments
+  constexpr int CWP = CW + (CW >> 3) + 1;     // padded row length
+  constexpr int WIN = FBQ_SEG + 2 * N;
+  __shared__ float mom[3][FBQ_R][CWP];
+  const int x0 = blockIdx.x * FBQ_OW, y0 = blockIdx.y * FBQ_R, tx = threadIdx.x;
+  if (tx < CW) {
+    const int xw = clampi(x0 - N + tx, 0, W - 1);
+    float c[FBQ_R + 2 * N];
+#pragma unroll
+    for (int q = 0; q < FBQ_R + 2 * N; q++) c[q] = src[(size_t)clampi(y0 - N + q, 0, H - 1) * pitch + xw];
+#pragma unroll
+    for (int r = 0; r < FBQ_R; r++) {
+      float r0 = __fmul_rn(c[r + N], P.g[0]), r1 = 0.f, r2 = 0.f;
+#pragma unroll
+      for (int k = 1; k <= N; k++) {
+        const float t0 = c[r + N - k], t1 = c[r + N + k];
+        r0 = __fmaf_rn(P.g[k], __fadd_rn(t0, t1), r0);
+        r1 = __fmaf_rn(P.xg[k], __fsub_rn(t1, t0), r1);
+        r2 = __fmaf_rn(P.xxg[k], __fadd_rn(t0, t1), r2);
+      }
+      mom[0][r][fbq_col(tx)] = r0;
+      mom[1][r][fbq_col(tx)] = r1;
+      mom[2][r][fbq_col(tx)] = r2;
+    }
+  }
+  __syncthreads();
+  constexpr int NSEG = FBQ_OW / FBQ_SEG;
+  if (tx >= FBQ_R * NSEG) return;
+  const int r = tx / NSEG, sg = tx - r * NSEG;
+  const int y = y0 + r, xs = x0 + sg * FBQ_SEG;
+  if (y >= H || xs >= W) return;
+  // output column xs + i is moment column sg*8 + i + N; its window is sg*8 .. sg*8 + 7 + 2N
+  float a0[WIN], a1[WIN], a2[WIN];
+#pragma unroll
+  for (int q = 0; q < WIN; q++) {
+    const int cc = sg * (FBQ_SEG + 1) + q + (q >> 3);  // fbq_col(sg * 8 + q)
+    a0[q] = mom[0][r][cc];
+    a1[q] = mom[1][r][cc];
+    a2[q] = mom[2][r][cc];
+  }
+  const size_t pl = (size_t)H * pitch;
+  float o[5][FBQ_SEG];
+#pragma unroll
+  for (int i = 0; i < FBQ_SEG; i++) {
+    const int t = i + N;
+    float b1 = __fmul_rn(P.g[0], a0[t]), b3 = __fmul_rn(P.g[0], a1[t]), b5 = __fmul_rn(P.g[0], a2[t]);
+    float b2 = 0.f, b4 = 0.f, b6 = 0.f;
+#pragma unroll
+    for (int k = 1; k <= N; k++) {
+      const float sp = __fadd_rn(a0[t + k], a0[t - k]), sm_ = __fsub_rn(a0[t + k], a0[t - k]);
+      b1 = __fmaf_rn(sp, P.g[k], b1);
+      b4 = __fmaf_rn(sp, P.xxg[k], b4);
+      b2 = __fmaf_rn(sm_, P.xg[k], b2);
+      b3 = __fmaf_rn(__fadd_rn(a1[t + k], a1[t - k]), P.g[k], b3);
+      b6 = __fmaf_rn(__fsub_rn(a1[t + k], a1[t - k]), P.xg[k], b6);
+      b5 = __fmaf_rn(__fadd_rn(a2[t + k], a2[t - k]), P.g[k], b5);
+    }
+    o[0][i] = __fmul_rn(b3, P.ig[0]);
+    o[1][i] = __fmul_rn(b2, P.ig[0]);
+    o[2][i] = __fmaf_rn(b1, P.ig[1], __fmul_rn(b5, P.ig[2]));
+    o[3][i] = __fmaf_rn(b1, P.ig[1], __fmul_rn(b4, P.ig[2]));
+    o[4][i] = __fmul_rn(b6, P.ig[3]);
+  }
+  const size_t i0 = (size_t)y * pitch + xs;
+  if (vec && xs + FBQ_SEG <= W) {
+#pragma unroll
+    for (int p = 0; p < 5; p++) {
+      float4* d = reinterpret_cast<float4*>(dst + p * pl + i0);
+      d[0] = make_float4(o[p][0], o[p][1], o[p][2], o[p][3]);
+      d[1] = make_float4(o[p][4], o[p][5], o[p][6], o[p][7]);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < FBQ_SEG; i++)
+      if (xs + i < W) {
+#pragma unroll
+        for (int p = 0; p < 5; p++) dst[p * pl + i0 + i] = o[p][i];
+      }
+  }
+}
+
 __constant__ float c_border[6] = {0.14f, 0.14f, 0.4472f, 0.4472f, 0.4472f, 1.f};
 
 // updateMatrices for pixel (y, x) given its flow; writes the 5 M planes.
@@ -497,6 +591,15 @@ extern "C" int of_fb_polyexp(const float* src, float* dst, int H, int W, int pit
     P.xxg[k] = c->xxg[k];
   }
   for (int k = 0; k < 4; k++) P.ig[k] = c->ig[k];
+  if (P.n == 5 || P.n == 7) {  // the reference's polyN settings: the tiled kernel
+    const int vec = (pitch % 4) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
+    dim3 grid((W + FBQ_OW - 1) / FBQ_OW, (H + FBQ_R - 1) / FBQ_R);
+    if (P.n == 7)
+      fb_polyexp_tile_kernel<7><<<grid, 256, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P, vec);
+    else
+      fb_polyexp_tile_kernel<5><<<grid, 256, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P, vec);
+    return check_launch("of_fb_polyexp");
+  }
   dim3 grid((W + (FBP_T - 2 * P.n) - 1) / (FBP_T - 2 * P.n), H);
   fb_polyexp_kernel<<<grid, FBP_T, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P);
   return check_launch("of_fb_polyexp");

@@ -136,16 +136,27 @@ __global__ void spline_recip_kernel(double* c, int m) {
 // Thomas-algorithm moments of the not-a-knot spline through n >= 4 samples with unit
 // spacing; sample i of the line is y[i*ys] (float or double), moment and scratch i are
 // M[i*ls] and dp[i*ls] (double).  The elimination multiplies by the shared pivots, so a
-// step is one add and one multiply.  Each line is one thread, and the recurrence is
-// serial; samples, pivots and scratch are fetched NAK_CH steps ahead into registers so a
-// chunk of steps waits on one memory latency instead of one per step.  Lanes of a warp
-// hold neighbouring lines (stride-1 in memory), so each chunk load is coalesced.
+// step is one add and one multiply.  Each line is one thread and the recurrence is serial,
+// with few lines in flight, so every instruction on the serial chain costs its full
+// latency: per chunk of NAK_CH steps the samples are loaded one chunk ahead, the right-hand
+// sides (independent of the chain) are formed first, and the chain itself is then only the
+// add and the multiply of each step.  The pivots come from shared memory (`sp`, the first
+// `nsp` of them; the rest from `cp`).  Lanes of a warp hold neighbouring lines (stride-1 in
+// memory), so each load is coalesced.
 #define NAK_CH 32
+#define NAK_SPIV 4096  // pivots staged in shared memory (32 KB)
+template <typename TY>
+__device__ __forceinline__ void nak_load(double (&b)[NAK_CH], const TY* __restrict__ y, size_t ys, int r0, int m) {
+#pragma unroll
+  for (int j = 0; j < NAK_CH; j++) b[j] = r0 + j < m ? (double)y[(size_t)(r0 + j + 3) * ys] : 0.0;
+}
 template <typename TY>
 __device__ void nak_moments(const TY* __restrict__ y, size_t ys, size_t ls, double* __restrict__ M,
-                            const double* __restrict__ cp, double* __restrict__ dp, int n) {
+                            const double* __restrict__ cp, const double* sp, int nsp, double* __restrict__ dp,
+                            int n) {
 #define YV(i) ((double)y[(size_t)(i) * ys])
 #define MV(i) M[(size_t)(i) * ls]
+#define PIV(r) ((r) < nsp ? sp[r] : cp[r])
   double M1 = __dadd_rn(__dadd_rn(YV(2), -__dmul_rn(2.0, YV(1))), YV(0));
   double Ml = __dadd_rn(__dadd_rn(YV(n - 1), -__dmul_rn(2.0, YV(n - 2))), YV(n - 3));
   MV(1) = M1;
@@ -154,49 +165,78 @@ __device__ void nak_moments(const TY* __restrict__ y, size_t ys, size_t ls, doub
   int m = n - 4;
   if (m > 0) {
     double ym = YV(1), y0 = YV(2), dprev = 0.0;
+    double yb[NAK_CH];
+    nak_load<TY>(yb, y, ys, 0, m);
+#pragma unroll 1
     for (int r0 = 0; r0 < m; r0 += NAK_CH) {
-      double yb[NAK_CH], cb[NAK_CH];
+      double yn[NAK_CH];
+      nak_load<TY>(yn, y, ys, r0 + NAK_CH, m);  // the next chunk, in flight during this one
+      double rhs[NAK_CH], cb[NAK_CH];
 #pragma unroll
       for (int j = 0; j < NAK_CH; j++) {
-        bool in = r0 + j < m;
-        yb[j] = in ? YV(r0 + j + 3) : 0.0;
-        cb[j] = in ? cp[r0 + j] : 0.0;
+        const int r = r0 + j;
+        const double yp = yb[j];
+        double v = __dmul_rn(6.0, __dadd_rn(__dadd_rn(yp, -__dmul_rn(2.0, y0)), ym));
+        if (r == 0) v = __dadd_rn(v, -M1);
+        if (r == m - 1) v = __dadd_rn(v, -Ml);
+        rhs[j] = v;
+        cb[j] = r < m ? PIV(r) : 0.0;
+        ym = y0;
+        y0 = yp;
       }
+      if (r0 + NAK_CH <= m) {  // a whole chunk: the chain alone
 #pragma unroll
-      for (int j = 0; j < NAK_CH; j++) {
-        int r = r0 + j;
-        if (r < m) {
-          double yp = yb[j];
-          double rhs = __dmul_rn(6.0, __dadd_rn(__dadd_rn(yp, -__dmul_rn(2.0, y0)), ym));
-          if (r == 0) rhs = __dadd_rn(rhs, -M1);
-          if (r == m - 1) rhs = __dadd_rn(rhs, -Ml);
-          double d = (r == 0) ? __dmul_rn(rhs, cb[j]) : __dmul_rn(__dadd_rn(rhs, -dprev), cb[j]);
-          dp[(size_t)r * ls] = d;
+        for (int j = 0; j < NAK_CH; j++) {
+          const double d = (r0 + j == 0) ? __dmul_rn(rhs[j], cb[j]) : __dmul_rn(__dadd_rn(rhs[j], -dprev), cb[j]);
+          dp[(size_t)(r0 + j) * ls] = d;
           dprev = d;
-          ym = y0;
-          y0 = yp;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < NAK_CH; j++) {
+          if (r0 + j < m) {
+            const double d = (r0 + j == 0) ? __dmul_rn(rhs[j], cb[j]) : __dmul_rn(__dadd_rn(rhs[j], -dprev), cb[j]);
+            dp[(size_t)(r0 + j) * ls] = d;
+            dprev = d;
+          }
         }
       }
+#pragma unroll
+      for (int j = 0; j < NAK_CH; j++) yb[j] = yn[j];
     }
     double next = dprev;
     MV(m + 1) = next;
     M3 = next;  // M[n-3] = M[m+1]
+    // back substitution, r = m-2 .. 0, in chunks loaded one ahead
+    double db[NAK_CH];
+#pragma unroll
+    for (int j = 0; j < NAK_CH; j++) db[j] = m - 2 - j >= 0 ? dp[(size_t)(m - 2 - j) * ls] : 0.0;
+#pragma unroll 1
     for (int r1 = m - 2; r1 >= 0; r1 -= NAK_CH) {
-      double db[NAK_CH], cb[NAK_CH];
+      double dn[NAK_CH], cb[NAK_CH];
 #pragma unroll
       for (int j = 0; j < NAK_CH; j++) {
-        int r = r1 - j;
-        db[j] = r >= 0 ? dp[(size_t)r * ls] : 0.0;
-        cb[j] = r >= 0 ? cp[r] : 0.0;
+        const int r = r1 - NAK_CH - j;
+        dn[j] = r >= 0 ? dp[(size_t)r * ls] : 0.0;
+        cb[j] = r1 - j >= 0 ? PIV(r1 - j) : 0.0;
       }
+      if (r1 - NAK_CH + 1 >= 0) {
 #pragma unroll
-      for (int j = 0; j < NAK_CH; j++) {
-        int r = r1 - j;
-        if (r >= 0) {
+        for (int j = 0; j < NAK_CH; j++) {
           next = __dadd_rn(db[j], -__dmul_rn(cb[j], next));
-          MV(r + 2) = next;
+          MV(r1 - j + 2) = next;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < NAK_CH; j++) {
+          if (r1 - j >= 0) {
+            next = __dadd_rn(db[j], -__dmul_rn(cb[j], next));
+            MV(r1 - j + 2) = next;
+          }
         }
       }
+#pragma unroll
+      for (int j = 0; j < NAK_CH; j++) db[j] = dn[j];
     }
     M2 = next;  // M[2]
   } else {
@@ -205,8 +245,17 @@ __device__ void nak_moments(const TY* __restrict__ y, size_t ys, size_t ls, doub
   }
   MV(0) = __dadd_rn(__dmul_rn(2.0, M1), -M2);
   MV(n - 1) = __dadd_rn(__dmul_rn(2.0, Ml), -M3);
+#undef PIV
 #undef YV
 #undef MV
+}
+
+// The first min(m, NAK_SPIV) pivots into shared memory (before any thread leaves).
+__device__ __forceinline__ int nak_stage_pivots(double* sp, const double* __restrict__ cp, int m) {
+  const int nsp = m < NAK_SPIV ? (m > 0 ? m : 0) : NAK_SPIV;
+  for (int i = threadIdx.x; i < nsp; i += blockDim.x) sp[i] = cp[i];
+  __syncthreads();
+  return nsp;
 }
 
 __device__ __forceinline__ double nak_eval(double yi, double yi1, double Mi, double Mi1, double t) {
@@ -240,11 +289,14 @@ struct SplinePlanes {
 // moments along y for each coarse column x, read straight from the float field (pitch sp)
 __global__ void __launch_bounds__(128) spline_my_kernel(SplinePlanes P, int sp, int h, int w, double* M, double* S,
                                                         const double* __restrict__ cp) {
+  extern __shared__ double s_piv[];
+  const int nsp = nak_stage_pivots(s_piv, cp, h - 4);
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= w) return;
   const int q = blockIdx.y;
   // moments and scratch are laid out [i][x] with stride w
-  nak_moments<float>((q ? P.src[1] : P.src[0]) + x, (size_t)sp, (size_t)w, M + q * P.pstride + x, cp, S + q * P.pstride + x, h);
+  nak_moments<float>((q ? P.src[1] : P.src[0]) + x, (size_t)sp, (size_t)w, M + q * P.pstride + x, cp, s_piv, nsp,
+                     S + q * P.pstride + x, h);
 }
 
 // Tt[x][Y] = column spline of coarse column x at fine row Y.  A 32x32 tile goes through
@@ -277,10 +329,12 @@ __global__ void __launch_bounds__(256) spline_ey_kernel(SplinePlanes P, int sp, 
 // moments along x for each fine row Y of Tt (layout [k][Y], stride H)
 __global__ void __launch_bounds__(128) spline_mx_kernel(const double* __restrict__ Tt, int w, int H, double* M,
                                                         const double* __restrict__ cp, double* dp, size_t pstride) {
+  extern __shared__ double s_piv[];
+  const int nsp = nak_stage_pivots(s_piv, cp, w - 4);
   int Y = blockIdx.x * blockDim.x + threadIdx.x;
   if (Y >= H) return;
   const size_t o = blockIdx.y * pstride;
-  nak_moments<double>(Tt + o + Y, (size_t)H, (size_t)H, M + o + Y, cp, dp + o + Y, w);
+  nak_moments<double>(Tt + o + Y, (size_t)H, (size_t)H, M + o + Y, cp, s_piv, nsp, dp + o + Y, w);
 }
 
 // dst[Y][X] = row spline of fine row Y at fine column X (times scale).  The coarse
@@ -510,9 +564,10 @@ static int spline_run(const SplinePlanes& P0, int np, int h, int w, int src_pitc
   SplinePlanes P = P0;
   P.pstride = single / sizeof(double);
   spline_recip_kernel<<<1, 256, 0, st>>>(piv, (h > w ? h : w) - 4);
-  spline_my_kernel<<<dim3((w + 127) / 128, np), 128, 0, st>>>(P, src_pitch, h, w, My, Sy, piv);
+  auto piv_smem = [](int m) { return sizeof(double) * (size_t)(m < NAK_SPIV ? (m > 0 ? m : 0) : NAK_SPIV); };
+  spline_my_kernel<<<dim3((w + 127) / 128, np), 128, piv_smem(h - 4), st>>>(P, src_pitch, h, w, My, Sy, piv);
   spline_ey_kernel<<<dim3((w + 31) / 32, (H + 31) / 32, np), dim3(32, 8), 0, st>>>(P, src_pitch, My, Tt, h, w, H);
-  spline_mx_kernel<<<dim3((H + 127) / 128, np), 128, 0, st>>>(Tt, w, H, Mx, piv, Sx, P.pstride);
+  spline_mx_kernel<<<dim3((H + 127) / 128, np), 128, piv_smem(w - 4), st>>>(Tt, w, H, Mx, piv, Sx, P.pstride);
   spline_ex_kernel<<<dim3((W + 31) / 32, (H + 31) / 32, np), dim3(32, 8), 0, st>>>(Tt, Mx, P, dst_pitch, w, H, W);
   return check_launch("of_spline_upsample", 5);
 }

@@ -292,6 +292,18 @@ def test_fb_kernels_vs_oracle(torch_cuda, fb_inputs):
     assert np.array_equal(host(Mout), O.fb_update_matrices(uxo, uyo, host(RA), host(RB)))
 
 
+@pytest.mark.parametrize("shape,polyN,sigma", [((37, 250), 7, 1.5), ((130, 491), 7, 1.5), ((257, 480), 5, 1.1),
+                                               ((9, 1000), 5, 1.1), ((3, 17), 7, 1.5), ((61, 77), 3, 0.9)])
+def test_fb_polyexp_shapes_vs_oracle(torch_cuda, shape, polyN, sigma):
+    """The tiled expansion (polyN 5 and 7) across tile edges, image borders and both store
+    paths (widths that are and are not multiples of 4), and the row kernel (other polyN)."""
+    from ofb200 import ops
+    a = rng(shape[0] * 7 + shape[1]).uniform(0, 255, shape).astype(np.float32)
+    g, xg, xxg, ig = O.farneback_poly_consts(polyN, sigma)
+    R = ops.fb_polyexp(dev(torch_cuda, a), ops.poly_consts(g, xg, xxg, ig, polyN))
+    assert np.array_equal(host(R), O.fb_polyexp(a, polyN, sigma))
+
+
 @pytest.mark.parametrize("kw", [{}, {"useGaussian": False}, {"polyN": 5, "polySigma": 1.1},
                                 {"pyramidalLevels": 2}])
 def test_farneback_compute_vs_oracle(torch_cuda, fb_inputs, kw):
