@@ -134,60 +134,69 @@ __global__ void spline_recip_kernel(double* c, int m) {
 }
 
 // Thomas-algorithm moments of the not-a-knot spline through n >= 4 samples with unit
-// spacing; sample i of the line is y[i*ys] (float or double), moment and scratch i are
+// spacing; sample i of a line is y[i*ys] (float or double), moment and scratch i are
 // M[i*ls] and dp[i*ls] (double).  The elimination multiplies by the shared pivots, so a
-// step is one add and one multiply.  Each line is one thread and the recurrence is serial,
-// with few lines in flight, so every instruction on the serial chain costs its full
-// latency: per chunk of NAK_CH steps the samples are loaded one chunk ahead, the right-hand
-// sides (independent of the chain) are formed first, and the chain itself is then only the
-// add and the multiply of each step.  The pivots come from shared memory (`sp`, the first
-// `nsp` of them; the rest from `cp`).  Lanes of a warp hold neighbouring lines (stride-1 in
-// memory), so each load is coalesced.
+// step is one add and one multiply.
+//
+// Each line is one thread and the recurrence is serial, with few lines in flight (one warp
+// per scheduler), so every instruction on a line's thread costs close to its full latency.
+// The work of a step that does not depend on the previous step -- its right-hand side
+// 6 (y[r+3] - 2 y[r+2] + y[r+1]), with the end corrections of the first and last step --
+// is done first by a fully parallel kernel (nak_rhs, one thread per line and step) into
+// the scratch array; the serial kernel (nak_solve) then reads it back a chunk ahead and
+// does only the add, the multiply and the store of each step, overwriting the right-hand
+// side with the eliminated value.  The arithmetic is the same, in the same order.
 #define NAK_CH 32
 #define NAK_SPIV 4096  // pivots staged in shared memory (32 KB)
 template <typename TY>
-__device__ __forceinline__ void nak_load(double (&b)[NAK_CH], const TY* __restrict__ y, size_t ys, int r0, int m) {
-#pragma unroll
-  for (int j = 0; j < NAK_CH; j++) b[j] = r0 + j < m ? (double)y[(size_t)(r0 + j + 3) * ys] : 0.0;
+__device__ __forceinline__ double nak_m1(const TY* __restrict__ y, size_t ys) {
+  return __dadd_rn(__dadd_rn((double)y[2 * ys], -__dmul_rn(2.0, (double)y[ys])), (double)y[0]);
 }
 template <typename TY>
-__device__ void nak_moments(const TY* __restrict__ y, size_t ys, size_t ls, double* __restrict__ M,
-                            const double* __restrict__ cp, const double* sp, int nsp, double* __restrict__ dp,
-                            int n) {
-#define YV(i) ((double)y[(size_t)(i) * ys])
+__device__ __forceinline__ double nak_ml(const TY* __restrict__ y, size_t ys, int n) {
+  return __dadd_rn(__dadd_rn((double)y[(size_t)(n - 1) * ys], -__dmul_rn(2.0, (double)y[(size_t)(n - 2) * ys])),
+                   (double)y[(size_t)(n - 3) * ys]);
+}
+// right-hand side of step r (0 <= r < m = n - 4) of one line into dp[r*ls]
+template <typename TY>
+__device__ __forceinline__ void nak_rhs(const TY* __restrict__ y, size_t ys, double* __restrict__ dp, size_t ls,
+                                        int r, int n) {
+  const int m = n - 4;
+  const double yp = (double)y[(size_t)(r + 3) * ys], y0 = (double)y[(size_t)(r + 2) * ys];
+  const double ym = (double)y[(size_t)(r + 1) * ys];
+  double v = __dmul_rn(6.0, __dadd_rn(__dadd_rn(yp, -__dmul_rn(2.0, y0)), ym));
+  if (r == 0) v = __dadd_rn(v, -nak_m1<TY>(y, ys));
+  if (r == m - 1) v = __dadd_rn(v, -nak_ml<TY>(y, ys, n));
+  dp[(size_t)r * ls] = v;
+}
+template <typename TY>
+__device__ void nak_solve(const TY* __restrict__ y, size_t ys, size_t ls, double* __restrict__ M,
+                          const double* __restrict__ cp, const double* sp, int nsp, double* __restrict__ dp, int n) {
 #define MV(i) M[(size_t)(i) * ls]
 #define PIV(r) ((r) < nsp ? sp[r] : cp[r])
-  double M1 = __dadd_rn(__dadd_rn(YV(2), -__dmul_rn(2.0, YV(1))), YV(0));
-  double Ml = __dadd_rn(__dadd_rn(YV(n - 1), -__dmul_rn(2.0, YV(n - 2))), YV(n - 3));
+  const double M1 = nak_m1<TY>(y, ys), Ml = nak_ml<TY>(y, ys, n);
   MV(1) = M1;
   MV(n - 2) = Ml;
   double M2 = Ml, M3 = Ml;  // M[2], M[n-3] for the end conditions
-  int m = n - 4;
+  const int m = n - 4;
   if (m > 0) {
-    double ym = YV(1), y0 = YV(2), dprev = 0.0;
-    double yb[NAK_CH];
-    nak_load<TY>(yb, y, ys, 0, m);
+    double dprev = 0.0;
+    double rb[NAK_CH];
+#pragma unroll
+    for (int j = 0; j < NAK_CH; j++) rb[j] = j < m ? dp[(size_t)j * ls] : 0.0;
 #pragma unroll 1
     for (int r0 = 0; r0 < m; r0 += NAK_CH) {
-      double yn[NAK_CH];
-      nak_load<TY>(yn, y, ys, r0 + NAK_CH, m);  // the next chunk, in flight during this one
-      double rhs[NAK_CH], cb[NAK_CH];
+      double rn[NAK_CH], cb[NAK_CH];
 #pragma unroll
       for (int j = 0; j < NAK_CH; j++) {
-        const int r = r0 + j;
-        const double yp = yb[j];
-        double v = __dmul_rn(6.0, __dadd_rn(__dadd_rn(yp, -__dmul_rn(2.0, y0)), ym));
-        if (r == 0) v = __dadd_rn(v, -M1);
-        if (r == m - 1) v = __dadd_rn(v, -Ml);
-        rhs[j] = v;
-        cb[j] = r < m ? PIV(r) : 0.0;
-        ym = y0;
-        y0 = yp;
+        const int r = r0 + NAK_CH + j;
+        rn[j] = r < m ? dp[(size_t)r * ls] : 0.0;  // the next chunk, in flight during this one
+        cb[j] = r0 + j < m ? PIV(r0 + j) : 0.0;
       }
       if (r0 + NAK_CH <= m) {  // a whole chunk: the chain alone
 #pragma unroll
         for (int j = 0; j < NAK_CH; j++) {
-          const double d = (r0 + j == 0) ? __dmul_rn(rhs[j], cb[j]) : __dmul_rn(__dadd_rn(rhs[j], -dprev), cb[j]);
+          const double d = (r0 + j == 0) ? __dmul_rn(rb[j], cb[j]) : __dmul_rn(__dadd_rn(rb[j], -dprev), cb[j]);
           dp[(size_t)(r0 + j) * ls] = d;
           dprev = d;
         }
@@ -195,14 +204,14 @@ __device__ void nak_moments(const TY* __restrict__ y, size_t ys, size_t ls, doub
 #pragma unroll
         for (int j = 0; j < NAK_CH; j++) {
           if (r0 + j < m) {
-            const double d = (r0 + j == 0) ? __dmul_rn(rhs[j], cb[j]) : __dmul_rn(__dadd_rn(rhs[j], -dprev), cb[j]);
+            const double d = (r0 + j == 0) ? __dmul_rn(rb[j], cb[j]) : __dmul_rn(__dadd_rn(rb[j], -dprev), cb[j]);
             dp[(size_t)(r0 + j) * ls] = d;
             dprev = d;
           }
         }
       }
 #pragma unroll
-      for (int j = 0; j < NAK_CH; j++) yb[j] = yn[j];
+      for (int j = 0; j < NAK_CH; j++) rb[j] = rn[j];
     }
     double next = dprev;
     MV(m + 1) = next;
@@ -246,7 +255,6 @@ __device__ void nak_moments(const TY* __restrict__ y, size_t ys, size_t ls, doub
   MV(0) = __dadd_rn(__dmul_rn(2.0, M1), -M2);
   MV(n - 1) = __dadd_rn(__dmul_rn(2.0, Ml), -M3);
 #undef PIV
-#undef YV
 #undef MV
 }
 
@@ -286,6 +294,14 @@ struct SplinePlanes {
   size_t pstride;
 };
 
+// right-hand sides along y: one thread per coarse column x and step r (grid.y = steps,
+// grid.z = plane)
+__global__ void __launch_bounds__(128) spline_ry_kernel(SplinePlanes P, int sp, int h, int w, double* S) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y, q = blockIdx.z;
+  if (x >= w) return;
+  nak_rhs<float>((q ? P.src[1] : P.src[0]) + x, (size_t)sp, S + q * P.pstride + x, (size_t)w, r, h);
+}
+
 // moments along y for each coarse column x, read straight from the float field (pitch sp)
 __global__ void __launch_bounds__(128) spline_my_kernel(SplinePlanes P, int sp, int h, int w, double* M, double* S,
                                                         const double* __restrict__ cp) {
@@ -295,8 +311,8 @@ __global__ void __launch_bounds__(128) spline_my_kernel(SplinePlanes P, int sp, 
   if (x >= w) return;
   const int q = blockIdx.y;
   // moments and scratch are laid out [i][x] with stride w
-  nak_moments<float>((q ? P.src[1] : P.src[0]) + x, (size_t)sp, (size_t)w, M + q * P.pstride + x, cp, s_piv, nsp,
-                     S + q * P.pstride + x, h);
+  nak_solve<float>((q ? P.src[1] : P.src[0]) + x, (size_t)sp, (size_t)w, M + q * P.pstride + x, cp, s_piv, nsp,
+                   S + q * P.pstride + x, h);
 }
 
 // Tt[x][Y] = column spline of coarse column x at fine row Y.  A 32x32 tile goes through
@@ -327,6 +343,15 @@ __global__ void __launch_bounds__(256) spline_ey_kernel(SplinePlanes P, int sp, 
 }
 
 // moments along x for each fine row Y of Tt (layout [k][Y], stride H)
+// right-hand sides along x for each fine row Y: one thread per Y and step r
+__global__ void __launch_bounds__(128) spline_rx_kernel(const double* __restrict__ Tt, int w, int H, double* dp,
+                                                        size_t pstride) {
+  const int Y = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+  if (Y >= H) return;
+  const size_t o = blockIdx.z * pstride;
+  nak_rhs<double>(Tt + o + Y, (size_t)H, dp + o + Y, (size_t)H, r, w);
+}
+
 __global__ void __launch_bounds__(128) spline_mx_kernel(const double* __restrict__ Tt, int w, int H, double* M,
                                                         const double* __restrict__ cp, double* dp, size_t pstride) {
   extern __shared__ double s_piv[];
@@ -334,7 +359,7 @@ __global__ void __launch_bounds__(128) spline_mx_kernel(const double* __restrict
   int Y = blockIdx.x * blockDim.x + threadIdx.x;
   if (Y >= H) return;
   const size_t o = blockIdx.y * pstride;
-  nak_moments<double>(Tt + o + Y, (size_t)H, (size_t)H, M + o + Y, cp, s_piv, nsp, dp + o + Y, w);
+  nak_solve<double>(Tt + o + Y, (size_t)H, (size_t)H, M + o + Y, cp, s_piv, nsp, dp + o + Y, w);
 }
 
 // dst[Y][X] = row spline of fine row Y at fine column X (times scale).  The coarse
@@ -565,11 +590,13 @@ static int spline_run(const SplinePlanes& P0, int np, int h, int w, int src_pitc
   P.pstride = single / sizeof(double);
   spline_recip_kernel<<<1, 256, 0, st>>>(piv, (h > w ? h : w) - 4);
   auto piv_smem = [](int m) { return sizeof(double) * (size_t)(m < NAK_SPIV ? (m > 0 ? m : 0) : NAK_SPIV); };
+  if (h > 4) spline_ry_kernel<<<dim3((w + 127) / 128, h - 4, np), 128, 0, st>>>(P, src_pitch, h, w, Sy);
   spline_my_kernel<<<dim3((w + 127) / 128, np), 128, piv_smem(h - 4), st>>>(P, src_pitch, h, w, My, Sy, piv);
   spline_ey_kernel<<<dim3((w + 31) / 32, (H + 31) / 32, np), dim3(32, 8), 0, st>>>(P, src_pitch, My, Tt, h, w, H);
+  if (w > 4) spline_rx_kernel<<<dim3((H + 127) / 128, w - 4, np), 128, 0, st>>>(Tt, w, H, Sx, P.pstride);
   spline_mx_kernel<<<dim3((H + 127) / 128, np), 128, piv_smem(w - 4), st>>>(Tt, w, H, Mx, piv, Sx, P.pstride);
   spline_ex_kernel<<<dim3((W + 31) / 32, (H + 31) / 32, np), dim3(32, 8), 0, st>>>(Tt, Mx, P, dst_pitch, w, H, W);
-  return check_launch("of_spline_upsample", 5);
+  return check_launch("of_spline_upsample", 5 + (h > 4) + (w > 4));
 }
 
 extern "C" int of_spline_upsample(const float* src, int h, int w, int src_pitch, float* dst, int H, int W,
