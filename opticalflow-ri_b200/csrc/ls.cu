@@ -62,30 +62,6 @@ __global__ void ls_max_kernel(const float* __restrict__ a, const float* __restri
   }
 }
 
-__global__ void ls_normalize_kernel(const float* __restrict__ a, const float* __restrict__ b,
-                                    const unsigned int* __restrict__ keys, float* __restrict__ I1,
-                                    float* __restrict__ I2, float* __restrict__ Et, int W, int sp, int dp) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-  if (x >= W) return;
-  float ma = key2f(keys[0]), mb = key2f(keys[1]);
-  size_t i = (size_t)y * sp + x, o = (size_t)y * dp + x;
-  float i1 = __fdiv_rn(a[i], ma), i2 = __fdiv_rn(b[i], mb);
-  I1[o] = i1;
-  I2[o] = i2;
-  Et[o] = __fsub_rn(i2, i1);
-}
-
-// (a, b) -> (ao, bo) plane copy between pitches
-__global__ void ls_copy2_kernel(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ ao,
-                                float* __restrict__ bo, int W, int sp, int dp, const int* __restrict__ gate) {
-  if (gate && !(*gate & 1)) return;
-  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-  if (x >= W) return;
-  size_t i = (size_t)y * sp + x, o = (size_t)y * dp + x;
-  ao[o] = a[i];
-  bo[o] = b[i];
-}
-
 __device__ __forceinline__ double dacc(double a, float v, double w) { return __dadd_rn(a, __dmul_rn((double)v, w)); }
 __device__ __forceinline__ double dadd(double a, float v) { return __dadd_rn(a, (double)v); }
 
@@ -130,14 +106,10 @@ __device__ __forceinline__ float hsum(const float* __restrict__ P, int y, int x,
   return (float)a;
 }
 
-__global__ void ls_coef_kernel(const float* __restrict__ I1, const float* __restrict__ Et, float* __restrict__ coef,
-                               size_t plane, int H, int W, int pitch, float h) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= W || y >= H) return;
-  Nb3 n, e;
-  n.load(I1, y, x, H, W, pitch);
-  e.load(Et, y, x, H, W, pitch);
-  size_t i = (size_t)y * pitch + x;
+// Coefficient planes of pixel (y, x) (pitch-`pitch` index i) from its 3x3 neighbourhoods
+// of the normalised frame (n) and the temporal difference (e).
+__device__ __forceinline__ void ls_coef_at(const Nb3& n, const Nb3& e, int y, int x, int H, int W, float h,
+                                           float* __restrict__ coef, size_t plane, size_t i) {
   float I = n.p[1][1];
   int cnt = 0;
 #pragma unroll
@@ -160,6 +132,55 @@ __global__ void ls_coef_kernel(const float* __restrict__ I1, const float* __rest
   coef[5 * plane + i] = __fdiv_rn(A22, det);
   coef[6 * plane + i] = __fdiv_rn(-A12, det);
   coef[7 * plane + i] = __fdiv_rn(A11, det);
+}
+
+__global__ void ls_coef_kernel(const float* __restrict__ I1, const float* __restrict__ Et, float* __restrict__ coef,
+                               size_t plane, int H, int W, int pitch, float h) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  Nb3 n, e;
+  n.load(I1, y, x, H, W, pitch);
+  e.load(Et, y, x, H, W, pitch);
+  ls_coef_at(n, e, y, x, H, W, h, coef, plane, (size_t)y * pitch + x);
+}
+
+// The whole set-up of a solve after the frame maxima, in one pass: a 32 x 8 tile of the
+// normalised frame I1 = im1 / max1 and of Et = im2 / max2 - I1 is formed in shared memory
+// with a 1-pixel halo of clamped ('nearest') coordinates -- exactly the neighbourhoods
+// Nb3::load reads -- then each pixel's coefficient planes are computed as in
+// ls_coef_kernel, and the initial field (V, U) is copied into ping-pong buffer 0.  The
+// normalised planes never reach global memory.
+__global__ void __launch_bounds__(256) ls_prep_kernel(const float* __restrict__ a, const float* __restrict__ b,
+                                                      int sp, const unsigned int* __restrict__ keys,
+                                                      const float* __restrict__ V, const float* __restrict__ U,
+                                                      float* __restrict__ coef, size_t plane, float* __restrict__ u0,
+                                                      float* __restrict__ v0, int H, int W, int P, float h) {
+  __shared__ float t1[10][35], te[10][35];
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+  const float ma = key2f(keys[0]), mb = key2f(keys[1]);
+  for (int k = threadIdx.x; k < 10 * 34; k += 256) {
+    const int ly = k / 34, lx = k - ly * 34;
+    const size_t g = (size_t)clampi(y0 - 1 + ly, 0, H - 1) * sp + clampi(x0 - 1 + lx, 0, W - 1);
+    const float i1 = __fdiv_rn(a[g], ma), i2 = __fdiv_rn(b[g], mb);
+    t1[ly][lx] = i1;
+    te[ly][lx] = __fsub_rn(i2, i1);
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int x = x0 + tx, y = y0 + ty;
+  if (x >= W || y >= H) return;
+  Nb3 n, e;
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      n.p[r][c] = t1[ty + r][tx + c];
+      e.p[r][c] = te[ty + r][tx + c];
+    }
+  const size_t i = (size_t)y * P + x, si = (size_t)y * sp + x;
+  ls_coef_at(n, e, y, x, H, W, h, coef, plane, i);
+  u0[i] = V[si];
+  v0[i] = U[si];
 }
 
 __device__ __forceinline__ double ls_err(const double* ss, int k, double inv_n) {
@@ -631,7 +652,7 @@ extern "C" int of_ls_coefficients(const float* I1n, const float* Et, float* coef
 extern "C" size_t of_ls_workspace_size(int H, int W, int pitch, int maxnum) {
   Sizer s;
   size_t N = (size_t)H * ls_pitch(W);
-  s.take<float>(3 * N);  // I1, I2, Et
+  s.take<float>(3 * N);  // reserved (the set-up now forms I1 and Et in shared memory)
   s.take<float>(8 * N);  // coefficient planes
   s.take<float>(4 * N);  // u0, v0, u1, v1
   s.take<LsCtrl>(1);
@@ -663,7 +684,7 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   int* redo = c.take<int>((size_t)maxnum + 1);
   double* ss = c.take<double>(2 * (size_t)(maxnum > 0 ? maxnum : 1));
   int* err_flag = run + maxnum + 1;
-  float *n1 = nrm, *n2 = nrm + N, *et = nrm + 2 * N;
+  (void)nrm;  // normalised frames: formed in shared memory by ls_prep_kernel
   float* ub[2] = {uv, uv + 2 * N};
   float* vb[2] = {uv + N, uv + 3 * N};
   // tensor maps over the whole solve: the 8 coefficient planes (3-D) and the four u / v
@@ -691,13 +712,11 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   dim3 mg((W + 255) / 256 < 2 ? (W + 255) / 256 : 2, H < 148 ? H : 148);
   ls_max_kernel<<<mg, 256, 0, st>>>(I0, I1, H, W, pitch, ctrl->maxkey);
   dim3 rg((W + 255) / 256, H);
-  ls_normalize_kernel<<<rg, 256, 0, st>>>(I0, I1, ctrl->maxkey, n1, n2, et, W, pitch, P);
-  dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8);
-  ls_coef_kernel<<<grd, blk, 0, st>>>(n1, et, coef, N, H, W, P, h);
-  ls_copy2_kernel<<<rg, 256, 0, st>>>(V, U, ub[0], vb[0], W, pitch, P, nullptr);
+  ls_prep_kernel<<<dim3((W + 31) / 32, (H + 7) / 8), 256, 0, st>>>(I0, I1, pitch, ctrl->maxkey, V, U, coef, N,
+                                                                 ub[0], vb[0], H, W, P, h);
   double inv_n = 1.0 / ((double)H * (double)W);
   dim3 pgrd((W + LB_TW - 1) / LB_TW, (H + LB_TH - 1) / LB_TH), pblk(32, LB_WARPS);
-  long long nl = 5;
+  long long nl = 3;
   int p = 0, k0 = 0;
   for (; k0 < maxnum; k0 += LB_T, p++) {
     LbPass P0{k0, maxnum - k0 < LB_T ? maxnum - k0 : LB_T, p, 0};
