@@ -43,7 +43,7 @@ L2_BYTES = 126 * 2 ** 20
 REF_BUDGET_S = 90.0
 # DRAM bytes (read + write) of one 60-sweep Liu-Shen solve at 1024^2, summed over its
 # launches from one ncu capture (profiles/ls_solve_traffic_1024.txt; cold cache per launch)
-NCU_LS_TRAFFIC = {1024: 671.83e6}
+NCU_LS_TRAFFIC = {1024: 663.48e6}
 
 
 def parse():
