@@ -26,10 +26,14 @@ __device__ __forceinline__ int pf_map(int c, int n, int h) {
   return clampi(c, 0, n - 1);  // only reached for outputs outside the image
 }
 
-template <typename Tin, int MAXK>
+// KC > 0: the tap count is the compile-time KC (the pyramid's 3- and 5-tap prefilters), so
+// the tile widths are constants (no integer division per staged element) and the tap loops
+// carry no bound test; KC = 0: K taps at run time, up to MAXK.
+template <typename Tin, int MAXK, int KC = 0>
 __global__ void __launch_bounds__(256) prefilter_kernel(const Tin* __restrict__ src, int sp, float* __restrict__ dst,
-                                                        int dp, int H, int W, const PfTaps taps, int K) {
+                                                        int dp, int H, int W, const PfTaps taps, int Krt) {
   extern __shared__ float sm[];
+  const int K = KC > 0 ? KC : Krt;
   const int h = K >> 1;
   const int iw = PF_TW + 2 * h, ih = PF_TH + 2 * h;
   float* tin = sm;             // ih x iw
@@ -49,7 +53,7 @@ __global__ void __launch_bounds__(256) prefilter_kernel(const Tin* __restrict__ 
     float acc = 0.0f;
 #pragma unroll(MAXK <= PF_MAXK ? MAXK : 8)
     for (int j = 0; j < MAXK; j++)
-      if (j < K) acc = __fadd_rn(acc, __fmul_rn(t[-j], taps.k[j]));
+      if (KC > 0 || j < K) acc = __fadd_rn(acc, __fmul_rn(t[-j], taps.k[j]));
     trow[i] = acc;
   }
   __syncthreads();
@@ -61,7 +65,7 @@ __global__ void __launch_bounds__(256) prefilter_kernel(const Tin* __restrict__ 
     float acc = 0.0f;
 #pragma unroll(MAXK <= PF_MAXK ? MAXK : 8)
     for (int j = 0; j < MAXK; j++)
-      if (j < K) acc = __fadd_rn(acc, __fmul_rn(t[-j * PF_TW], taps.k[j]));
+      if (KC > 0 || j < K) acc = __fadd_rn(acc, __fmul_rn(t[-j * PF_TW], taps.k[j]));
     dst[(size_t)y * dp + x] = acc;
   }
 }
@@ -79,7 +83,12 @@ static int launch_prefilter(const Tin* src, int sp, float* dst, int dp, int H, i
   size_t smem = sizeof(float) * ((size_t)(PF_TH + 2 * h) * (PF_TW + 2 * h) + (size_t)(PF_TH + 2 * h) * PF_TW);
   dim3 grid((W + PF_TW - 1) / PF_TW, (H + PF_TH - 1) / PF_TH);
   if (K <= PF_MAXK) {
-    prefilter_kernel<Tin, PF_MAXK><<<grid, 256, smem, as_stream(stream)>>>(src, sp, dst, dp, H, W, t, K);
+    if (K == 5)
+      prefilter_kernel<Tin, 5, 5><<<grid, 256, smem, as_stream(stream)>>>(src, sp, dst, dp, H, W, t, K);
+    else if (K == 3)
+      prefilter_kernel<Tin, 3, 3><<<grid, 256, smem, as_stream(stream)>>>(src, sp, dst, dp, H, W, t, K);
+    else
+      prefilter_kernel<Tin, PF_MAXK><<<grid, 256, smem, as_stream(stream)>>>(src, sp, dst, dp, H, W, t, K);
   } else {
     static bool attr = false;  // up to 83 KB of staged tile for 81 taps
     if (!attr) {
