@@ -36,26 +36,37 @@ __device__ __forceinline__ int fb_col(int x, int cols) { return fb_low(fb_high(x
 constexpr int FBB_TW = 64, FBB_TH = 16;
 
 // Blur of plane blockIdx.z: out = H(V(src)).  smem: input (TH+2kh) x (TW+2kh), vertical
-// result TH x (TW+2kh).
+// result TH x (TW+2kh).  KHC > 0: the half width is the compile-time KHC (the Farneback
+// levels' frame smoothing uses 1 and 4), so the tile widths are constants and the tap
+// loops unroll; KHC = 0: kh at run time.
+template <int KHC = 0>
 __global__ void __launch_bounds__(256) fb_blur_kernel(const float* __restrict__ src, float* __restrict__ dst, int H,
-                                                      int W, int pitch, FbTaps t, int kh) {
+                                                      int W, int pitch, FbTaps t, int khrt) {
   extern __shared__ float sm[];
+  const int kh = KHC > 0 ? KHC : khrt;
   const int iw = FBB_TW + 2 * kh, ih = FBB_TH + 2 * kh;
   float* tin = sm;
   float* tv = sm + ih * iw;
   const size_t plane = (size_t)H * pitch * blockIdx.z;
   const float* s = src + plane;
   const int x0 = blockIdx.x * FBB_TW, y0 = blockIdx.y * FBB_TH;
+  // interior tiles (halo inside the image) need no reflect-101 mapping
+  const bool inside = x0 >= kh && y0 >= kh && x0 + FBB_TW + kh <= W && y0 + FBB_TH + kh <= H;
   for (int i = threadIdx.x; i < ih * iw; i += blockDim.x) {
     int ly = i / iw, lx = i - ly * iw;
-    tin[i] = s[(size_t)fb_row(y0 - kh + ly, H) * pitch + fb_col(x0 - kh + lx, W)];
+    const int gy = y0 - kh + ly, gx = x0 - kh + lx;
+    tin[i] = inside ? s[(size_t)gy * pitch + gx] : s[(size_t)fb_row(gy, H) * pitch + fb_col(gx, W)];
   }
   __syncthreads();
   for (int i = threadIdx.x; i < FBB_TH * iw; i += blockDim.x) {
     int ly = i / iw, lx = i - ly * iw;
     const float* c = tin + (ly + kh) * iw + lx;
     float acc = __fmul_rn(c[0], t.g[0]);
-    for (int j = 1; j <= kh; j++) acc = __fmaf_rn(__fadd_rn(c[-j * iw], c[j * iw]), t.g[j], acc);
+#pragma unroll
+    for (int j = 1; j <= (KHC > 0 ? KHC : FB_MAXKH); j++) {
+      if (KHC == 0 && j > kh) break;
+      acc = __fmaf_rn(__fadd_rn(c[-j * iw], c[j * iw]), t.g[j], acc);
+    }
     tv[i] = acc;
   }
   __syncthreads();
@@ -65,7 +76,11 @@ __global__ void __launch_bounds__(256) fb_blur_kernel(const float* __restrict__ 
     if (y >= H || x >= W) continue;
     const float* r = tv + ly * iw + lx + kh;
     float res = __fmul_rn(r[0], t.g[0]);
-    for (int j = 1; j <= kh; j++) res = __fmaf_rn(__fadd_rn(r[-j], r[j]), t.g[j], res);
+#pragma unroll
+    for (int j = 1; j <= (KHC > 0 ? KHC : FB_MAXKH); j++) {
+      if (KHC == 0 && j > kh) break;
+      res = __fmaf_rn(__fadd_rn(r[-j], r[j]), t.g[j], res);
+    }
     dst[plane + (size_t)y * pitch + x] = res;
   }
 }
@@ -562,9 +577,16 @@ extern "C" int of_fb_blur(const float* src, float* dst, int H, int W, int pitch,
   OF_REQUIRE(!bad_plane(src, H, W, pitch) && dst && src != dst, "of_fb_blur: bad plane");
   OF_REQUIRE(gk && kh >= 0 && kh <= FB_MAXKH && planes >= 1 && planes <= 65535, "of_fb_blur: bad kernel");
   size_t smem = sizeof(float) * ((size_t)(FBB_TH + 2 * kh) * (FBB_TW + 2 * kh) + (size_t)FBB_TH * (FBB_TW + 2 * kh));
-  if (smem > 48 * 1024) cudaFuncSetAttribute(fb_blur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(fb_blur_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
   dim3 grid((W + FBB_TW - 1) / FBB_TW, (H + FBB_TH - 1) / FBB_TH, planes);
-  fb_blur_kernel<<<grid, 256, smem, as_stream(stream)>>>(src, dst, H, W, pitch, make_taps(gk, kh), kh);
+  const FbTaps tp = make_taps(gk, kh);
+  if (kh == 1)
+    fb_blur_kernel<1><<<grid, 256, smem, as_stream(stream)>>>(src, dst, H, W, pitch, tp, kh);
+  else if (kh == 4)
+    fb_blur_kernel<4><<<grid, 256, smem, as_stream(stream)>>>(src, dst, H, W, pitch, tp, kh);
+  else
+    fb_blur_kernel<0><<<grid, 256, smem, as_stream(stream)>>>(src, dst, H, W, pitch, tp, kh);
   return check_launch("of_fb_blur");
 }
 

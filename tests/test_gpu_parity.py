@@ -292,6 +292,16 @@ def test_fb_kernels_vs_oracle(torch_cuda, fb_inputs):
     assert np.array_equal(host(Mout), O.fb_update_matrices(uxo, uyo, host(RA), host(RB)))
 
 
+@pytest.mark.parametrize("n,sigma", [(3, 0.5), (9, 1.5), (15, 2.2), (33, 4.95)])
+def test_fb_blur_interior_and_border_tiles(torch_cuda, n, sigma):
+    """The Farneback blur on an image with interior tiles (no reflect mapping) and border
+    tiles, for the specialised half widths (1, 4) and run-time ones, over 2 stacked planes."""
+    from ofb200 import ops
+    a = rng(n).uniform(0, 255, (2 * 300, 257)).astype(np.float32)
+    hk = O.fb_half_kernel(n, sigma)
+    assert np.array_equal(host(ops.fb_blur(dev(torch_cuda, a), hk, planes=2)), O.fb_blur(a, hk, planes=2))
+
+
 @pytest.mark.parametrize("shape,polyN,sigma", [((37, 250), 7, 1.5), ((130, 491), 7, 1.5), ((257, 480), 5, 1.1),
                                                ((9, 1000), 5, 1.1), ((3, 17), 7, 1.5), ((61, 77), 3, 0.9)])
 def test_fb_polyexp_shapes_vs_oracle(torch_cuda, shape, polyN, sigma):
