@@ -43,9 +43,10 @@ __host__ __device__ inline void resize_geom(int inSize, int outSize, int bicubic
   *ksize = (int)ceil(sup) * 2 + 1;
 }
 
-__global__ void resize_coeff_kernel(int inSize, int outSize, int bicubic, int ksize, int* bounds, double* kk) {
-  int xx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (xx >= outSize) return;
+// Weights and source window of output index xx along one axis: window [*pmin, *pmin + *pcnt),
+// k[j * kstride] for j < ksize (zero past the window).
+__device__ __forceinline__ void resize_coeff_at(int inSize, int outSize, int bicubic, int ksize, int xx, int* pmin,
+                                                int* pcnt, double* k, int kstride) {
   double scale, fscale, support;
   int ks;
   resize_geom(inSize, outSize, bicubic, &scale, &fscale, &support, &ks);
@@ -56,18 +57,67 @@ __global__ void resize_coeff_kernel(int inSize, int outSize, int bicubic, int ks
   int xmax = (int)__dadd_rn(__dadd_rn(center, support), 0.5);
   if (xmax > inSize) xmax = inSize;
   xmax -= xmin;
-  double* k = kk + (size_t)xx * ksize;
   int x;
   for (x = 0; x < xmax; x++) {
     double w = filt(__dmul_rn(__dadd_rn(__dadd_rn((double)(x + xmin), -center), 0.5), ss), bicubic);
-    k[x] = w;
+    k[x * kstride] = w;
     ww = __dadd_rn(ww, w);
   }
   for (x = 0; x < xmax; x++)
-    if (ww != 0.0) k[x] = __ddiv_rn(k[x], ww);
-  for (; x < ksize; x++) k[x] = 0.0;
-  bounds[2 * xx] = xmin;
-  bounds[2 * xx + 1] = xmax;
+    if (ww != 0.0) k[x * kstride] = __ddiv_rn(k[x * kstride], ww);
+  for (; x < ksize; x++) k[x * kstride] = 0.0;
+  *pmin = xmin;
+  *pcnt = xmax;
+}
+
+__global__ void resize_coeff_kernel(int inSize, int outSize, int bicubic, int ksize, int* bounds, double* kk) {
+  int xx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (xx >= outSize) return;
+  resize_coeff_at(inSize, outSize, bicubic, ksize, xx, &bounds[2 * xx], &bounds[2 * xx + 1], kk + (size_t)xx * ksize,
+                  1);
+}
+
+// Fused passes for kernels of up to RZ_MAXK taps: a CTA computes the weights it needs into
+// shared memory (the horizontal pass: its 128 output columns; the vertical pass: its
+// RZ_RB output rows) and applies them to a band of RZ_RB rows, so a resize is two
+// launches, not four.  Same weights and sums as the table path.
+constexpr int RZ_MAXK = 32, RZ_RB = 16;
+__global__ void __launch_bounds__(128) resize_hf_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst,
+                                                        int dp, int Hs, int Ws, int Wd, int bicubic, int ksize) {
+  __shared__ double kk[RZ_MAXK * 128];
+  const int xx = blockIdx.x * 128 + threadIdx.x;
+  if (xx >= Wd) return;  // no barrier below: every thread uses only its own column's weights
+  int xmin, xcnt;
+  resize_coeff_at(Ws, Wd, bicubic, ksize, xx, &xmin, &xcnt, kk + threadIdx.x, 128);
+  const double* k = kk + threadIdx.x;
+  const int y1 = min(Hs, (blockIdx.y + 1) * RZ_RB);
+  for (int y = blockIdx.y * RZ_RB; y < y1; y++) {
+    const float* row = src + (size_t)y * sp + xmin;
+    double ss = 0.0;
+    for (int x = 0; x < xcnt; x++) ss = __dadd_rn(ss, __dmul_rn((double)row[x], k[x * 128]));
+    dst[(size_t)y * dp + xx] = (float)ss;
+  }
+}
+
+__global__ void __launch_bounds__(128) resize_vf_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst,
+                                                        int dp, int Hs, int Hd, int Wd, int bicubic, int ksize) {
+  __shared__ double kk[RZ_RB * RZ_MAXK];
+  __shared__ int bnd[RZ_RB][2];
+  const int yy0 = blockIdx.y * RZ_RB;
+  if (threadIdx.x < RZ_RB && yy0 + threadIdx.x < Hd)
+    resize_coeff_at(Hs, Hd, bicubic, ksize, yy0 + threadIdx.x, &bnd[threadIdx.x][0], &bnd[threadIdx.x][1],
+                    kk + threadIdx.x * RZ_MAXK, 1);
+  __syncthreads();
+  const int x = blockIdx.x * 128 + threadIdx.x;
+  if (x >= Wd) return;
+  const int n = min(RZ_RB, Hd - yy0);
+  for (int r = 0; r < n; r++) {
+    const int ymin = bnd[r][0], ymax = bnd[r][1];
+    const double* k = kk + r * RZ_MAXK;
+    double ss = 0.0;
+    for (int y = 0; y < ymax; y++) ss = __dadd_rn(ss, __dmul_rn((double)src[(size_t)(y + ymin) * sp + x], k[y]));
+    dst[(size_t)(yy0 + r) * dp + x] = (float)ss;
+  }
 }
 
 __global__ void resize_h_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst, int dp, int Hs, int Wd,
@@ -546,6 +596,17 @@ extern "C" int of_resize(const float* src, int Hs, int Ws, int src_pitch, float*
   double* kkv = c.take<double>((size_t)kv * Hd);
   float* tmp = c.take<float>((size_t)Hs * Wd);
   bool need_h = Wd != Ws, need_v = Hd != Hs;
+  if (kh <= RZ_MAXK && kv <= RZ_MAXK) {  // the fused passes
+    float* mid = need_v ? tmp : dst;
+    const int mp = need_v ? Wd : dst_pitch;
+    if (need_h)
+      resize_hf_kernel<<<dim3((Wd + 127) / 128, (Hs + RZ_RB - 1) / RZ_RB), 128, 0, st>>>(src, src_pitch, mid, mp, Hs,
+                                                                                          Ws, Wd, bic, kh);
+    if (need_v)
+      resize_vf_kernel<<<dim3((Wd + 127) / 128, (Hd + RZ_RB - 1) / RZ_RB), 128, 0, st>>>(
+          need_h ? tmp : src, need_h ? Wd : src_pitch, dst, dst_pitch, Hs, Hd, Wd, bic, kv);
+    return check_launch("of_resize", (int)need_h + (int)need_v);
+  }
   const float* cur = src;
   int cur_pitch = src_pitch;
   if (need_h) {
