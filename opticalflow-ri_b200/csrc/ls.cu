@@ -467,6 +467,35 @@ __global__ void __launch_bounds__(32 * LB_WARPS, 2) ls_pass_kernel(const __grid_
                                                          int pitch, float h, LbPass P, LsCtrl* ctrl, double* ss,
                                                          int* run, unsigned int* done, int* redo, double inv_n,
                                                          double tol, int* err_flag, float one) {
+  // Passes after the first are launched as programmatic dependents of the previous pass:
+  // every CTA lets the next pass be scheduled at once, so its CTAs take the SM slots this
+  // pass's tail frees and prefetch their coefficient tile (the coefficients do not change
+  // during a solve); griddepcontrol.wait then holds them until the previous pass has
+  // completed and its memory (u, v and the stop-rule flags) is visible.  Launched without
+  // the attribute, both instructions have no effect.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  extern __shared__ __align__(128) unsigned char lb_smem_raw[];
+  unsigned char* base = lb_smem_raw + ((128 - (smem_u32(lb_smem_raw) & 127)) & 127);
+  const float* sc = reinterpret_cast<const float*>(base);
+  // ping-pong buffer q: u at base + COEF + 2q planes, v right after it
+#define LB_U(q) reinterpret_cast<LbPlane*>(base + LB_COEF_BYTES + (2 * (q)) * LB_PLANE)
+#define LB_V(q) reinterpret_cast<LbPlane*>(base + LB_COEF_BYTES + (2 * (q) + 1) * LB_PLANE)
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + LB_COEF_BYTES + 4 * LB_PLANE);  // coefficients
+  uint64_t* bar2 = bar + 1;                                                           // u, v
+  const int x0 = blockIdx.x * LB_TW, y0 = blockIdx.y * LB_TH;
+  const int lane = threadIdx.x, warp = threadIdx.y;
+  const int t = warp * 32 + lane;
+  if (t == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar2, 1);
+  }
+  __syncthreads();
+  const bool pre = !P.last;  // the launch after the last pass only rolls back: no prefetch
+  if (pre && t == 0) {
+    mbar_expect_tx(bar, LB_COEF_BYTES);
+    tma_load_3d((void*)sc, &tm_coef, x0 - LB_T, y0 - LB_T, 0, bar);
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   // Pass p reads ping-pong buffer p & 1 and writes the other.  A pass that the stop rule
   // cancelled (and the launch after the last pass) instead rolls the previous pass back
   // when that pass ran past its stopping sweep: it recomputes it from the same input with
@@ -475,7 +504,10 @@ __global__ void __launch_bounds__(32 * LB_WARPS, 2) ls_pass_kernel(const __grid_
   bool rollback = false;
   if (P.last || (k0 > 0 && *(volatile int*)(run + k0) == 0)) {
     const int r = pass > 0 ? *(volatile int*)(redo + pass - 1) : 0;
-    if (r == 0) return;
+    if (r == 0) {
+      if (pre && !mbar_wait(bar, 0, LS_WAIT_LIMIT) && t == 0) atomicExch(err_flag, 1);  // the prefetch lands
+      return;
+    }
     rollback = true;
     pass -= 1;
     k0 -= LB_T;
@@ -486,27 +518,20 @@ __global__ void __launch_bounds__(32 * LB_WARPS, 2) ls_pass_kernel(const __grid_
   const CUtensorMap* tm_v = in ? &tm_v1 : &tm_v0;
   float* un = out ? ub1 : ub0;
   float* vn = out ? vb1 : vb0;
-  extern __shared__ __align__(128) unsigned char lb_smem_raw[];
-  unsigned char* base = lb_smem_raw + ((128 - (smem_u32(lb_smem_raw) & 127)) & 127);
-  const float* sc = reinterpret_cast<const float*>(base);
-  // ping-pong buffer q: u at base + COEF + 2q planes, v right after it
-#define LB_U(q) reinterpret_cast<LbPlane*>(base + LB_COEF_BYTES + (2 * (q)) * LB_PLANE)
-#define LB_V(q) reinterpret_cast<LbPlane*>(base + LB_COEF_BYTES + (2 * (q) + 1) * LB_PLANE)
-  uint64_t* bar = reinterpret_cast<uint64_t*>(base + LB_COEF_BYTES + 4 * LB_PLANE);
-  const int x0 = blockIdx.x * LB_TW, y0 = blockIdx.y * LB_TH;
-  const int lane = threadIdx.x, warp = threadIdx.y;
-  const int t = warp * 32 + lane;
-  if (t == 0) mbar_init(bar, 1);
-  __syncthreads();
   if (t == 0) {
-    mbar_expect_tx(bar, LB_COEF_BYTES + 2 * LB_PLANE);
-    tma_load_3d((void*)sc, &tm_coef, x0 - LB_T, y0 - LB_T, 0, bar);
-    tma_load_2d(LB_U(0), tm_u, x0 - LB_T, y0 - LB_T, bar);
-    tma_load_2d(LB_V(0), tm_v, x0 - LB_T, y0 - LB_T, bar);
+    if (!pre) {
+      mbar_expect_tx(bar, LB_COEF_BYTES);
+      tma_load_3d((void*)sc, &tm_coef, x0 - LB_T, y0 - LB_T, 0, bar);
+    }
+    mbar_expect_tx(bar2, 2 * LB_PLANE);
+    tma_load_2d(LB_U(0), tm_u, x0 - LB_T, y0 - LB_T, bar2);
+    tma_load_2d(LB_V(0), tm_v, x0 - LB_T, y0 - LB_T, bar2);
   }
-  if (!mbar_wait(bar, 0, LS_WAIT_LIMIT)) {
+  const bool ok_c = mbar_wait(bar, 0, LS_WAIT_LIMIT), ok_uv = mbar_wait(bar2, 0, LS_WAIT_LIMIT);
+  if (!ok_c || !ok_uv) {
     if (t == 0) atomicExch(err_flag, 1);
-    mbar_wait(bar, 0, LS_WAIT_LIMIT);  // one more bounded wait for the copies in flight
+    if (!ok_c) mbar_wait(bar, 0, LS_WAIT_LIMIT);  // one more bounded wait for the copies in flight
+    if (!ok_uv) mbar_wait(bar2, 0, LS_WAIT_LIMIT);
     nsw = 0;
   }
   // in-image region rows / columns (region row r <-> y0 - 4 + r, column c <-> x0 - 4 + c)
@@ -718,18 +743,32 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   dim3 pgrd((W + LB_TW - 1) / LB_TW, (H + LB_TH - 1) / LB_TH), pblk(32, LB_WARPS);
   long long nl = 3;
   int p = 0, k0 = 0;
+  // pass 0 waits for the set-up in stream order; later passes (and the rollback launch)
+  // are programmatic dependents of the pass before them
+  cudaLaunchAttribute pdl[1];
+  pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  pdl[0].val.programmaticStreamSerializationAllowed = 1;
+  auto launch_pass = [&](LbPass PP, bool dependent) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = pgrd;
+    cfg.blockDim = pblk;
+    cfg.dynamicSmemBytes = LB_SMEM;
+    cfg.stream = st;
+    cfg.attrs = dependent ? pdl : nullptr;
+    cfg.numAttrs = dependent ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, ls_pass_kernel, tm_coef, tm_u[0], tm_v[0], tm_u[1], tm_v[1], ub[0], vb[0], ub[1],
+                              vb[1], H, W, P, h, PP, ctrl, ss, run, done, redo, inv_n, tol, err_flag, 1.0f);
+  };
   for (; k0 < maxnum; k0 += LB_T, p++) {
     LbPass P0{k0, maxnum - k0 < LB_T ? maxnum - k0 : LB_T, p, 0};
-    ls_pass_kernel<<<pgrd, pblk, LB_SMEM, st>>>(tm_coef, tm_u[0], tm_v[0], tm_u[1], tm_v[1], ub[0], vb[0], ub[1],
-                                               vb[1], H, W, P, h, P0, ctrl, ss, run, done, redo, inv_n, tol,
-                                               err_flag, 1.0f);
+    cudaError_t e = launch_pass(P0, p > 0);
+    if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_ls_solve: pass launch: %s", cudaGetErrorString(e));
     nl++;
   }
   if (p > 0) {  // rolls the last pass back if it ran past the stopping sweep
     LbPass PL{k0, 0, p, 1};
-    ls_pass_kernel<<<pgrd, pblk, LB_SMEM, st>>>(tm_coef, tm_u[0], tm_v[0], tm_u[1], tm_v[1], ub[0], vb[0], ub[1],
-                                               vb[1], H, W, P, h, PL, ctrl, ss, run, done, redo, inv_n, tol,
-                                               err_flag, 1.0f);
+    cudaError_t e = launch_pass(PL, true);
+    if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_ls_solve: pass launch: %s", cudaGetErrorString(e));
     nl++;
   }
   ls_count_kernel<<<1, 1, 0, st>>>(ctrl, ss, inv_n, err_flag, iters_out, err_out);
