@@ -6,7 +6,7 @@ encoder-decoder CNN maps a pyramid level's frame pair (the bicubic downsample by
 each frame divided by its maximum; the packaged weights run at 128^2 for 1024^2 frames) to
 a flow at that level; one fused bilinear upsample turns it into the initial field of a
 short full-size stage (one Farneback iteration and a few Liu-Shen sweeps for the packaged
-calibration).  The solve's last update norm (its convergence residual) judges the result:
+calibration).  The solve's last update norm (its convergence residual) decides the result:
 above a threshold calibrated on held-out pairs, the pair falls back to the plain pyramid.
 
 Network (bf16 NHWC activations, f32 accumulation; ~1.75 M parameters):

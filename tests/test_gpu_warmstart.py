@@ -73,7 +73,7 @@ def test_trained_start_gain(torch_cuda, trained):
         e_plain.append(S.epe(Up.cpu().numpy(), Vp.cpu().numpy(), Ug, Vg, crop=16))
         U, V, _, err = ll.run(A, B)
         e_learned.append(S.epe(U.cpu().numpy(), V.cpu().numpy(), Ug, Vg, crop=16))
-        assert float(err.item()) <= meta["threshold"]  # the calibrated judge accepts it
+        assert float(err.item()) <= meta["threshold"]  # within the calibrated acceptance threshold
         Z = torch.zeros_like(A)
         Uz, Vz, _, _ = ll.refine(A, B, Z, Z.clone())
         e_zero.append(S.epe(Uz.cpu().numpy(), Vz.cpu().numpy(), Ug, Vg, crop=16))
