@@ -67,6 +67,114 @@ __global__ void hs_sweep_kernel(const float* __restrict__ fx, const float* __res
   Vn[i] = __fsub_rn(va, __fmul_rn(gy, der));
 }
 
+// Temporally blocked sweeps: one pass runs up to HB_T sweeps on a tile held in shared
+// memory, so the three derivative planes and (U, V) cross HBM/L2 once per HB_T sweeps
+// instead of once per sweep.  A CTA owns 56 x 32 pixels and stages a 64 x 40 region (halo
+// HB_T): sweep s computes the cells at least s + 1 from the region's edge, which after
+// HB_T sweeps leaves exactly the owned pixels exact; they are written back.  On image
+// borders every neighbour index goes through the same 'mirror' map as hs_sweep_kernel
+// (mapped neighbours stay within one row / column of their cell, so inside the region),
+// and out-of-image cells are neither computed nor read.  Each cell's arithmetic is
+// hs_sweep_kernel's: the averaging weights are float32 values (24-bit mantissas), so every
+// product with a float32 sample is exact in double and fma(v, w, acc) rounds exactly as
+// the separate multiply and add.
+constexpr int HB_T = 4, HB_TW = 56, HB_TH = 32, HB_RW = HB_TW + 2 * HB_T, HB_RH = HB_TH + 2 * HB_T;  // 64 x 40
+constexpr int HB_PL = HB_RW * HB_RH;
+constexpr size_t HB_SMEM = 7 * (size_t)HB_PL * sizeof(float);  // fx, fy, ft, U x2, V x2: 70 KB
+
+template <bool EDGE>
+__device__ __forceinline__ void hb_sweep(const float* __restrict__ sfx, const float* __restrict__ sfy,
+                                         const float* __restrict__ sft, const float* __restrict__ su,
+                                         const float* __restrict__ sv, float* __restrict__ du, float* __restrict__ dv,
+                                         int s, int x0, int y0, int H, int W, float a2) {
+  const double wc = (double)(1.0f / 12.0f), we = (double)(1.0f / 6.0f);
+  const int c = threadIdx.x & (HB_RW - 1), g = threadIdx.x >> 6;
+  if (c < 1 + s || c >= HB_RW - 1 - s) return;
+  const int gx = x0 - HB_T + c;
+  if (EDGE && (gx < 0 || gx >= W)) return;
+  int cm = c - 1, cp = c + 1;
+  if (EDGE) {
+    cm = mirror1(gx - 1, W) - (x0 - HB_T);
+    cp = mirror1(gx + 1, W) - (x0 - HB_T);
+  }
+  for (int r = 1 + s + g; r < HB_RH - 1 - s; r += 4) {
+    const int gy = y0 - HB_T + r;
+    if (EDGE && (gy < 0 || gy >= H)) continue;
+    int rm = r - 1, rp = r + 1;
+    if (EDGE) {
+      rm = mirror1(gy - 1, H) - (y0 - HB_T);
+      rp = mirror1(gy + 1, H) - (y0 - HB_T);
+    }
+    const int om = rm * HB_RW, o0 = r * HB_RW, op = rp * HB_RW;
+    double a = 0.0, b = 0.0;
+    a = __fma_rn((double)su[om + cm], wc, a); b = __fma_rn((double)sv[om + cm], wc, b);
+    a = __fma_rn((double)su[om + c], we, a);  b = __fma_rn((double)sv[om + c], we, b);
+    a = __fma_rn((double)su[om + cp], wc, a); b = __fma_rn((double)sv[om + cp], wc, b);
+    a = __fma_rn((double)su[o0 + cm], we, a); b = __fma_rn((double)sv[o0 + cm], we, b);
+    a = __fma_rn((double)su[o0 + cp], we, a); b = __fma_rn((double)sv[o0 + cp], we, b);
+    a = __fma_rn((double)su[op + cm], wc, a); b = __fma_rn((double)sv[op + cm], wc, b);
+    a = __fma_rn((double)su[op + c], we, a);  b = __fma_rn((double)sv[op + c], we, b);
+    a = __fma_rn((double)su[op + cp], wc, a); b = __fma_rn((double)sv[op + cp], wc, b);
+    const float ua = (float)a, va = (float)b;
+    const int i = o0 + c;
+    const float gxv = sfx[i], gyv = sfy[i];
+    const float num = __fadd_rn(__fadd_rn(__fmul_rn(gxv, ua), __fmul_rn(gyv, va)), sft[i]);
+    const float den = __fadd_rn(__fadd_rn(a2, __fmul_rn(gxv, gxv)), __fmul_rn(gyv, gyv));
+    const float der = __fdiv_rn(num, den);
+    du[i] = __fsub_rn(ua, __fmul_rn(gxv, der));
+    dv[i] = __fsub_rn(va, __fmul_rn(gyv, der));
+  }
+}
+
+__global__ void __launch_bounds__(256) hs_pass_kernel(const float* __restrict__ fx, const float* __restrict__ fy,
+                                                      const float* __restrict__ ft, const float* __restrict__ U,
+                                                      const float* __restrict__ V, float* __restrict__ Un,
+                                                      float* __restrict__ Vn, int H, int W, int pitch, float a2,
+                                                      int nsw) {
+  extern __shared__ float hb_sm[];
+  float* sfx = hb_sm;
+  float* sfy = sfx + HB_PL;
+  float* sft = sfy + HB_PL;
+  // ping-pong buffer q: u at sft + (1 + 2q) planes, v right after it
+#define HB_U(q) (sft + (1 + 2 * (q)) * HB_PL)
+#define HB_V(q) (sft + (2 + 2 * (q)) * HB_PL)
+  const int x0 = blockIdx.x * HB_TW, y0 = blockIdx.y * HB_TH;
+  for (int k = threadIdx.x; k < HB_PL; k += 256) {
+    const int r = k / HB_RW, c = k - r * HB_RW;
+    const int gy = y0 - HB_T + r, gx = x0 - HB_T + c;
+    if (gy < 0 || gy >= H || gx < 0 || gx >= W) continue;  // never read
+    const size_t i = (size_t)gy * pitch + gx;
+    sfx[k] = fx[i];
+    sfy[k] = fy[i];
+    sft[k] = ft[i];
+    HB_U(0)[k] = U[i];
+    HB_V(0)[k] = V[i];
+  }
+  __syncthreads();
+  const bool edge = x0 < HB_T || y0 < HB_T || x0 + HB_TW + HB_T > W || y0 + HB_TH + HB_T > H;
+#pragma unroll 1
+  for (int s = 0; s < nsw; s++) {
+    const int q = s & 1;
+    if (edge)
+      hb_sweep<true>(sfx, sfy, sft, HB_U(q), HB_V(q), HB_U(q ^ 1), HB_V(q ^ 1), s, x0, y0, H, W, a2);
+    else
+      hb_sweep<false>(sfx, sfy, sft, HB_U(q), HB_V(q), HB_U(q ^ 1), HB_V(q ^ 1), s, x0, y0, H, W, a2);
+    __syncthreads();
+  }
+  const float* fu = HB_U(nsw & 1);
+  const float* fv = HB_V(nsw & 1);
+  for (int k = threadIdx.x; k < HB_TW * HB_TH; k += 256) {
+    const int r = k / HB_TW, c = k - r * HB_TW;
+    const int y = y0 + r, x = x0 + c;
+    if (y >= H || x >= W) continue;
+    const int o = (r + HB_T) * HB_RW + c + HB_T;
+    Un[(size_t)y * pitch + x] = fu[o];
+    Vn[(size_t)y * pitch + x] = fv[o];
+  }
+#undef HB_U
+#undef HB_V
+}
+
 __global__ void copy2_kernel(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ ao,
                              float* __restrict__ bo, int W, int pitch) {
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
@@ -145,6 +253,33 @@ extern "C" int of_hs_solve(const float* I0, const float* I1, float* U, float* V,
   hs_deriv_kernel<<<grd, blk, 0, st>>>(I0, I1, fx, fy, ft, H, W, pitch);
   copy2_kernel<<<rgrid, 256, 0, st>>>(U, V, U0, V0, W, pitch);
   float a2 = alpha * alpha;
+  if (H >= 16 && W >= 16 && niter > 0) {  // temporally blocked: HB_T sweeps per launch
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(hs_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HB_SMEM);
+      attr = true;
+    }
+    const int np = (niter + HB_T - 1) / HB_T;
+    dim3 pg((W + HB_TW - 1) / HB_TW, (H + HB_TH - 1) / HB_TH);
+    for (int p = 0; p < np; p++) {
+      // the last pass writes U, V; earlier ones alternate with Ub, Vb; the first reads U0, V0
+      const bool to_uv = ((np - 1 - p) & 1) == 0;
+      const float* su = p == 0 ? U0 : (to_uv ? Ub : U);
+      const float* sv = p == 0 ? V0 : (to_uv ? Vb : V);
+      const int nsw = niter - p * HB_T < HB_T ? niter - p * HB_T : HB_T;
+      hs_pass_kernel<<<pg, 256, HB_SMEM, st>>>(fx, fy, ft, su, sv, to_uv ? U : Ub, to_uv ? V : Vb, H, W, pitch, a2,
+                                              nsw);
+    }
+    long long n = 2 + np;
+    if (err_out) {
+      cudaMemsetAsync(acc, 0, 2 * sizeof(double), st);
+      dim3 g2((W + 255) / 256 < 4 ? (W + 255) / 256 : 4, H < 256 ? H : 256);
+      sqdiff2_kernel<<<g2, 256, 0, st>>>(U, U0, V, V0, H, W, pitch, acc);
+      hs_err_kernel<<<1, 1, 0, st>>>(acc, (double)H * (double)W, err_out);
+      n += 2;
+    }
+    return check_launch("of_hs_solve", n);
+  }
   for (int k = 0; k < niter; k++) {
     const float *su, *sv;
     float *du, *dv;

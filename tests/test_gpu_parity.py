@@ -165,6 +165,24 @@ def test_hs_config1_vs_oracle(torch_cuda):
     assert float(e.item()) == pytest.approx(eo, rel=1e-9)
 
 
+@pytest.mark.parametrize("shape,niter", [((16, 16), 1), ((57, 130), 9), ((300, 201), 13), ((40, 56), 4),
+                                         ((130, 61), 6), ((12, 40), 5), ((1024, 1024), 7)])
+def test_hs_shapes_vs_oracle(torch_cuda, shape, niter):
+    """Horn-Schunck across tile edges, image borders ('mirror'), images smaller than one
+    tile and sweep counts that end mid-pass (the blocked kernel runs 4 sweeps per launch;
+    images under 16 pixels a side take the one-sweep kernel)."""
+    from ofb200 import ops
+    r = rng(shape[0] + 3 * shape[1] + niter)
+    a = r.uniform(0, 255, shape).astype(np.float32)
+    b = r.uniform(0, 255, shape).astype(np.float32)
+    U0 = r.normal(0, 0.5, shape).astype(np.float32)
+    V0 = r.normal(0, 0.5, shape).astype(np.float32)
+    U, V, e = ops.hs_solve(dev(torch_cuda, a), dev(torch_cuda, b), dev(torch_cuda, U0), dev(torch_cuda, V0), 21, niter)
+    Uo, Vo, eo = O.hs_solve(a, b, U0, V0, 21, niter)
+    assert np.array_equal(host(U), Uo) and np.array_equal(host(V), Vo)
+    assert float(e.item()) == pytest.approx(eo, rel=1e-9)
+
+
 # ------------------------------------------------------------------------------ A8/A9
 def test_ls_golden(torch_cuda):
     from ofb200 import ops
