@@ -77,3 +77,20 @@ def test_host_copy_without_gpu():
     f = np.empty((1024, 1024), dtype=np.float32)
     par_copyto(f, u8)
     assert np.array_equal(f, u8.astype(np.float32))
+
+
+def test_spline_pair_argument_checks_without_gpu():
+    """of_spline_upsample_pair validates its arguments on the host before any CUDA call:
+    aliased outputs and a workspace under two single-plane workspaces are rejected with
+    the entry point named in the error message."""
+    if not os.path.exists(LIB):
+        pytest.skip("libofb200.so not built")
+    from ofb200 import _lib
+    L = _lib.lib()
+    fake = ctypes.c_void_p(4096)  # never dereferenced: the checks fail first
+    rc = L.of_spline_upsample_pair(fake, fake, 8, 8, 8, fake, fake, 16, 16, 16, 1.0, 1.0, fake, 1 << 20, None)
+    assert rc == -1 and "alias" in _lib.last_error()
+    other = ctypes.c_void_p(8192)
+    need = 2 * L.of_spline_workspace_size(8, 8, 16, 16)
+    rc = L.of_spline_upsample_pair(fake, fake, 8, 8, 8, fake, other, 16, 16, 16, 1.0, 1.0, fake, need - 8, None)
+    assert rc == -3 and "workspace" in _lib.last_error()
