@@ -571,7 +571,7 @@ def run_reference(args, rank, world):
         dt = time.perf_counter() - t0
     v = per_step * steps / dt
     return {"metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": world, "steps": steps,
-            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "pairs_per_step": per_step, "size": args.size},
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": ncores, "kind": "port",

@@ -30,7 +30,7 @@ def _bitexact_cached(n, sigma):
     assert n > 0
     if sigma <= 0 and n in _FIXED:
         k = np.array(_FIXED[n], dtype=np.float64)
-        return (Decimal("1.0") if n == 1 else Decimal("1.0")), k
+        return Decimal("1.0"), k  # the fixed tables are returned with a unit sum
     one = Decimal("1.0")
     sigx = Decimal(sigma) if sigma < 0 else Decimal(n) * Decimal("0.15") + Decimal("0.35")
     scale2 = Decimal("-0.125") / (sigx * sigx)

@@ -725,12 +725,10 @@ extern "C" int of_cnn_conv3x3(const void* x, int n, int H, int W, int cin, int x
   size_t smem = 1024 + (size_t)CV_STAGES * p.stage_bytes;
   size_t floor_smem = (size_t)p.tmem_cols * 456 + 1024;
   if (smem < floor_smem) smem = floor_smem;
-  static size_t attr_smem = 0;  // the largest dynamic size opted into so far
-  if (smem > attr_smem) {
-    cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  {
+    cudaError_t e = OF_SMEM_OPT_IN(conv3x3_tc_kernel, smem);
     if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_cnn_conv3x3: %zu B of shared memory: %s", smem,
                                            cudaGetErrorString(e));
-    attr_smem = smem;
   }
   dim3 grid((n / nb) * p.tiles_per_group, ntile);
   conv3x3_tc_kernel<<<grid, CV_THREADS, smem, as_stream(stream)>>>(tmx, tmw, p);
@@ -915,12 +913,10 @@ extern "C" int of_cnn_conv3x3_wgrad_tc(const void* x, int x_ctot, int x_coff, co
   size_t smem = 1024 + (size_t)WT_STAGES * p.stage_bytes;
   size_t floor_smem = (size_t)p.tmem_cols * 456 + 1024;  // resident CTAs never exceed 512 TMEM columns
   if (smem < floor_smem) smem = floor_smem;
-  static size_t attr_smem = 0;
-  if (smem > attr_smem) {
-    cudaError_t e = cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  {
+    cudaError_t e = OF_SMEM_OPT_IN(wgrad_tc_kernel, smem);
     if (e != cudaSuccess)
       return set_error(OF_ERR_CUDA, "of_cnn_conv3x3_wgrad_tc: %zu B of shared memory: %s", smem, cudaGetErrorString(e));
-    attr_smem = smem;
   }
   dim3 grid((unsigned)ks, p.mtiles * p.ntiles, 9);
   wgrad_tc_kernel<<<grid, CV_THREADS, smem, as_stream(stream)>>>(tma, tmb, p);

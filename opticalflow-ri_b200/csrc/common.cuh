@@ -9,6 +9,8 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <atomic>
+
 #include "../../include/ofb200.h"
 
 namespace ofb {
@@ -61,7 +63,38 @@ inline bool bad_plane(const void* p, int H, int W, int pitch) { return !p || H <
 
 constexpr int kNumSMs = 148;
 
+// The dynamic shared-memory opt-in (cudaFuncAttributeMaxDynamicSharedMemorySize) is a
+// per-device attribute of a kernel.  Each call site keeps the size it has set on each
+// device (ordinals 0-63; others set the attribute on every call), so a solve on a second
+// GPU of the process opts in there too.  Concurrent first calls both set it: harmless.
+struct SmemOptIn {
+  std::atomic<int> bytes[64];
+};
+
+template <class K>
+inline cudaError_t smem_opt_in(SmemOptIn& s, K* kernel, int bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const bool cached = dev >= 0 && dev < 64;
+  if (cached && s.bytes[dev].load(std::memory_order_acquire) >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && cached) {
+    int cur = s.bytes[dev].load(std::memory_order_relaxed);
+    while (cur < bytes && !s.bytes[dev].compare_exchange_weak(cur, bytes, std::memory_order_release)) {
+    }
+  }
+  return e;
+}
+
 }  // namespace ofb
+
+// smem_opt_in with a call-site-local record (one per template instantiation).
+#define OF_SMEM_OPT_IN(kernel, bytes)                                       \
+  ([&]() {                                                                  \
+    static ::ofb::SmemOptIn of_smem_record_;                                \
+    return ::ofb::smem_opt_in(of_smem_record_, kernel, (int)(bytes));       \
+  }())
 
 #define OF_REQUIRE(cond, ...)                                        \
   do {                                                               \

@@ -577,8 +577,10 @@ extern "C" int of_fb_blur(const float* src, float* dst, int H, int W, int pitch,
   OF_REQUIRE(!bad_plane(src, H, W, pitch) && dst && src != dst, "of_fb_blur: bad plane");
   OF_REQUIRE(gk && kh >= 0 && kh <= FB_MAXKH && planes >= 1 && planes <= 65535, "of_fb_blur: bad kernel");
   size_t smem = sizeof(float) * ((size_t)(FBB_TH + 2 * kh) * (FBB_TW + 2 * kh) + (size_t)FBB_TH * (FBB_TW + 2 * kh));
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(fb_blur_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+  if (smem > 48 * 1024) {
+    cudaError_t e = OF_SMEM_OPT_IN(fb_blur_kernel<0>, 64 * 1024);
+    if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_fb_blur: %s", cudaGetErrorString(e));
+  }
   dim3 grid((W + FBB_TW - 1) / FBB_TW, (H + FBB_TH - 1) / FBB_TH, planes);
   const FbTaps tp = make_taps(gk, kh);
   if (kh == 1)
@@ -594,7 +596,10 @@ extern "C" int of_fb_box5(const float* src, float* dst, int H, int W, int pitch,
   OF_REQUIRE(!bad_plane(src, H, W, pitch) && dst && src != dst, "of_fb_box5: bad plane");
   OF_REQUIRE(kh >= 0 && kh <= FB_MAXKH, "of_fb_box5: bad kernel");
   size_t smem = sizeof(float) * ((size_t)(FBB_TH + 2 * kh) * (FBB_TW + 2 * kh) + (size_t)FBB_TH * (FBB_TW + 2 * kh));
-  if (smem > 48 * 1024) cudaFuncSetAttribute(fb_box_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+  if (smem > 48 * 1024) {
+    cudaError_t e = OF_SMEM_OPT_IN(fb_box_kernel, 64 * 1024);
+    if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_fb_box5: %s", cudaGetErrorString(e));
+  }
   dim3 grid((W + FBB_TW - 1) / FBB_TW, (H + FBB_TH - 1) / FBB_TH, 5);
   float inv = 1.f / (float)((1 + 2 * kh) * (1 + 2 * kh));
   fb_box_kernel<<<grid, 256, smem, as_stream(stream)>>>(src, dst, H, W, pitch, kh, inv);
@@ -658,11 +663,8 @@ extern "C" int of_fb_iteration(const float* M_in, float* M_out, const float* R0,
     uint32_t box[3] = {G::IW, G::IH, 1};
     int rc = tmap_f32(&tm, M_in, 3, dims, strides, box);
     if (rc) return rc;
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(fb_iter_fixed_kernel<KH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
-      attr = true;
-    }
+    cudaError_t e = OF_SMEM_OPT_IN(fb_iter_fixed_kernel<KH>, G::SMEM);
+    if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_fb_iteration: %s", cudaGetErrorString(e));
     dim3 grid((W + FBK_TW - 1) / FBK_TW, (H + FBK_TH - 1) / FBK_TH);
     fb_iter_fixed_kernel<KH><<<grid, 256, G::SMEM, as_stream(stream)>>>(tm, M_out, R0, R1, flowx, flowy, H, W, pitch,
                                                                         make_taps(wk, kh), update_matrices);

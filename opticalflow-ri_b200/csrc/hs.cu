@@ -254,11 +254,8 @@ extern "C" int of_hs_solve(const float* I0, const float* I1, float* U, float* V,
   copy2_kernel<<<rgrid, 256, 0, st>>>(U, V, U0, V0, W, pitch);
   float a2 = alpha * alpha;
   if (H >= 16 && W >= 16 && niter > 0) {  // temporally blocked: HB_T sweeps per launch
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(hs_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HB_SMEM);
-      attr = true;
-    }
+    cudaError_t e = OF_SMEM_OPT_IN(hs_pass_kernel, HB_SMEM);
+    if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_solve: %s", cudaGetErrorString(e));
     const int np = (niter + HB_T - 1) / HB_T;
     dim3 pg((W + HB_TW - 1) / HB_TW, (H + HB_TH - 1) / HB_TH);
     for (int p = 0; p < np; p++) {

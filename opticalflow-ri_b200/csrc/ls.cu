@@ -727,10 +727,9 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
       if ((rc = tmap_f32(&tm_v[q], vb[q], 2, d2, s2, b2))) return rc;
     }
   }
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(ls_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LB_SMEM);
-    attr = true;
+  {
+    cudaError_t e = OF_SMEM_OPT_IN(ls_pass_kernel, LB_SMEM);
+    if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_ls_solve: %s", cudaGetErrorString(e));
   }
   // control block, flags, counters, redo counts and sums are contiguous: one memset
   cudaMemsetAsync(ctrl, 0, (size_t)((char*)(ss + 2 * (size_t)(maxnum > 0 ? maxnum : 1)) - (char*)ctrl), st);
@@ -804,8 +803,12 @@ static void* ls_noalloc_scratch_ptr(int* rc) {
   static void* ptrs[64] = {nullptr};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+  if (e != cudaSuccess) {
     *rc = set_error(OF_ERR_CUDA, "of_ls_solve_noalloc: cudaGetDevice failed (%s)", cudaGetErrorString(e));
+    return nullptr;
+  }
+  if (dev < 0 || dev >= 64) {
+    *rc = set_error(OF_ERR_UNSUPPORTED, "of_ls_solve_noalloc: device ordinal %d; the address cache covers 0-63", dev);
     return nullptr;
   }
   std::lock_guard<std::mutex> lock(mu);

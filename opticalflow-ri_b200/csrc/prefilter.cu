@@ -90,13 +90,9 @@ static int launch_prefilter(const Tin* src, int sp, float* dst, int dp, int H, i
     else
       prefilter_kernel<Tin, PF_MAXK><<<grid, 256, smem, as_stream(stream)>>>(src, sp, dst, dp, H, W, t, K);
   } else {
-    static bool attr = false;  // up to 83 KB of staged tile for 81 taps
-    if (!attr) {
-      cudaError_t e = cudaFuncSetAttribute(prefilter_kernel<Tin, PF_MAXK_LARGE>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-      if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "%s: %s", name, cudaGetErrorString(e));
-      attr = true;
-    }
+    // up to 83 KB of staged tile for 81 taps
+    cudaError_t e = OF_SMEM_OPT_IN((prefilter_kernel<Tin, PF_MAXK_LARGE>), 96 * 1024);
+    if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "%s: %s", name, cudaGetErrorString(e));
     prefilter_kernel<Tin, PF_MAXK_LARGE><<<grid, 256, smem, as_stream(stream)>>>(src, sp, dst, dp, H, W, t, K);
   }
   return check_launch(name);

@@ -84,10 +84,6 @@ class denseLucasKanade_PyCl(object):
             return to_host(Ud), to_host(Vd), to_host(st), to_host(er)
         return Ud, Vd, st, er
 
-    def _compute_dev(self, im1, im2, U, V):
-        Ud, Vd, _, _ = self._run(im1, im2, U, V, False)
-        return Ud, Vd, True
-
     def _graph_key(self, n):
         if self.enableVorticityEnhancement:
             return None  # the window masks are chosen on the host from the current flow

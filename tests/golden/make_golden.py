@@ -1,9 +1,9 @@
 """Generates the golden fixtures in tests/golden/ from the reference implementation.
 
-Run in a container that has the reference source tree (read-only) at REFERENCE_SRC
-(default /root/reference/src):
+Run in a container that has the reference source tree (read-only); pass its src/
+directory as the first argument or in REFERENCE_SRC:
 
-    PYTHONDONTWRITEBYTECODE=1 NUMBA_CACHE_DIR=/tmp/numba python tests/golden/make_golden.py
+    PYTHONDONTWRITEBYTECODE=1 NUMBA_CACHE_DIR=/tmp/numba python tests/golden/make_golden.py <reference>/src
 
 The reference's CPU modules (gaussian_filter, GaussianKernelBitExact, HornSchunck,
 PhysicsBasedOpticalFlowLiuShen, GenericPyramidalOpticalFlow) are imported as-is with
@@ -26,7 +26,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("REFERENCE_SRC", "/root/reference/src")
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_SRC", "")
 sys.dont_write_bytecode = True
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
 sys.path.insert(0, os.path.join(REPO, "opticalflow-ri_b200"))
@@ -58,6 +58,8 @@ def _stub_modules():
 
 
 def load_reference():
+    if not REF or not os.path.isdir(REF):
+        raise SystemExit("make_golden.py: give the reference's src/ directory (argument or REFERENCE_SRC)")
     _stub_modules()
     if REF not in sys.path:
         sys.path.insert(0, REF)

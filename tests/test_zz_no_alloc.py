@@ -10,6 +10,7 @@ counts and errors.  This file is collected last; it also passes on its own.
 """
 import ctypes
 import os
+import re
 
 import numpy as np
 import pytest
@@ -18,7 +19,18 @@ pytestmark = pytest.mark.gpu
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(REPO, "opticalflow-ri_b200", "ofb200", "libofb200.so")
-SCRATCH_BYTES = 4 * 1024 * 1024  # OF_LS_NOALLOC_SCRATCH_BYTES in include/ofb200.h
+
+
+def _header_scratch_bytes():
+    """OF_LS_NOALLOC_SCRATCH_BYTES as include/ofb200.h defines it (the array's size)."""
+    with open(os.path.join(REPO, "include", "ofb200.h")) as f:
+        m = re.search(r"#define\s+OF_LS_NOALLOC_SCRATCH_BYTES\s+([0-9uUlL*+ ()]+)$", f.read(), re.M)
+    assert m, "OF_LS_NOALLOC_SCRATCH_BYTES not found in include/ofb200.h"
+    expr = re.sub(r"(?<=[0-9])[uUlL]+", "", m.group(1))
+    return int(eval(expr, {"__builtins__": {}}))  # digits, *, +, parentheses only
+
+
+SCRATCH_BYTES = _header_scratch_bytes()
 
 
 @pytest.fixture(scope="module")
@@ -98,3 +110,21 @@ def test_noalloc_rejects_sizes_beyond_the_array(env):
     buf = ctypes.create_string_buffer(512)
     L.of_last_error(buf, 512)
     assert b"fixed" in buf.value and b"of_ls_solve" in buf.value
+
+
+def test_noalloc_boundary_of_the_array(env):
+    """The widest 256-row image whose workspace fits is solved; one column more is rejected."""
+    torch, L = env
+    H = 256
+    W = 256
+    while L.of_ls_workspace_size(H, W + 1, W + 1, 60) <= SCRATCH_BYTES:
+        W += 1
+    assert L.of_ls_workspace_size(H, W + 1, W + 1, 60) > SCRATCH_BYTES
+    a, b = _frames(torch, H, W, 21)
+    ref = _solve(torch, L, a, b, noalloc=False)
+    got = _solve(torch, L, a, b, noalloc=True)
+    assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1]) and got[2] == ref[2]
+    a2 = torch.zeros(H, W + 1, device="cuda")
+    rc = L.of_ls_solve_noalloc(a2.data_ptr(), a2.data_ptr(), a2.data_ptr(), a2.data_ptr(), H, W + 1, W + 1, 10.0, 60,
+                               1e-8, None, None, torch.cuda.current_stream().cuda_stream)
+    assert rc == -1
