@@ -16,8 +16,8 @@ host-side pieces in Python:
 * the pyramid driver (src/GenericPyramidalOpticalFlow.py:237-415), with the level
   transition of :117-234.
 
-``pyramid_f64`` is a float64 restatement of the HS / LS pipelines used to separate
-algorithmic error from float32 rounding.
+The float64 restatement of the HS / LS pipelines, used to separate algorithmic error from
+float32 rounding, is ``oracle_f64.py``.
 """
 from __future__ import annotations
 
