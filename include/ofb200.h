@@ -148,6 +148,16 @@ size_t of_ls_workspace_size(int H, int W, int pitch, int maxnum);
 int of_ls_coefficients(const float* I1n, const float* Et, float* coef, int H, int W, int pitch, float h, void* stream);
 int of_ls_solve(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float h, int maxnum,
                 double tol, int* iters_out, double* err_out, void* workspace, size_t workspace_bytes, void* stream);
+/* The same solve (same reference interface, same workspace) with a choice of arithmetic:
+ * OF_LS_EXACT is of_ls_solve (bit-exact with the reference's float32 fields: its stencils
+ * are float64 sums in the reference's order); OF_LS_FAST computes the sweep in float32
+ * with fused multiply-adds (fields within float32 rounding of the reference's, <= 1e-3 px
+ * of the algorithm's float64 answer; the stop rule is evaluated on its own float32 changes). */
+#define OF_LS_EXACT 0
+#define OF_LS_FAST 1
+int of_ls_solve_mode(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float h,
+                     int maxnum, double tol, int mode, int* iters_out, double* err_out, void* workspace,
+                     size_t workspace_bytes, void* stream);
 
 /* The same Liu-Shen solve for callers that cannot allocate device memory at call time
  * (a framework that owns all allocations, a plugin that must not touch the process's

@@ -458,6 +458,171 @@ __device__ __forceinline__ void lb_strip(const LbPlane* su, const LbPlane* sv, c
 #undef LB_ROW
 }
 
+// ---- float32 pass (OF_LS_FAST) ----------------------------------------------------------
+// The same sweep, tile and stop rule with float32 arithmetic throughout: no float64 stencil
+// sums, no conversions, fused multiply-adds.  The stencils share their parts: per field the
+// vertical difference vd = down - up and sum vs = up + down of the lane's four columns give
+// D (= vd / 2), F (= vs), M (= (vd[c+1] - vd[c-1]) / 4) and, with the centre row's
+// neighbours, D^T (= (right - left) / 2), F^T (= left + right) and H (= vs[c-1] + vs[c] +
+// vs[c+1] + left + right in the interior); the constant factors are folded into the
+// coefficients (exact power-of-two scalings).  Results differ from the reference's float32
+// fields by float32 rounding only (<= 1e-3 px of the float64 answer at the configurations).
+struct LbRowF {
+  float2 cu, cv;           // the lane's cell pair
+  float lu, ru, lv, rv;    // the window's outer columns (2 lane - 1, 2 lane + 2)
+};
+
+template <bool EDGE>
+__device__ __forceinline__ void lbf_load(LbRowF& R, const LbPlane* su, const LbPlane* sv, int row, const LbCols& c) {
+  if (EDGE) {
+    R.cu = f2(su[row][c.k[1]], su[row][c.k[2]]);
+    R.cv = f2(sv[row][c.k[1]], sv[row][c.k[2]]);
+  } else {
+    R.cu = *reinterpret_cast<const float2*>(&su[row][c.k[1]]);
+    R.cv = *reinterpret_cast<const float2*>(&sv[row][c.k[1]]);
+  }
+  R.lu = su[row][c.k[0]];
+  R.ru = su[row][c.k[3]];
+  R.lv = sv[row][c.k[0]];
+  R.rv = sv[row][c.k[3]];
+}
+
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return padd(a, pmul(b, f2s(-1.0f))); }
+
+// 8-neighbour sum of the pair with out-of-image neighbours as 0 (H's 'constant' border)
+__device__ __forceinline__ float2 lbf_hsum_edge(const LbRowF& U, const LbRowF& C, const LbRowF& D, bool T, bool B,
+                                                bool L0, bool R0, bool L1, bool R1, bool uv) {
+  const float2 u = uv ? U.cv : U.cu, c = uv ? C.cv : C.cu, d = uv ? D.cv : D.cu;
+  const float ul = uv ? U.lv : U.lu, ur = uv ? U.rv : U.ru, cl = uv ? C.lv : C.lu, cr = uv ? C.rv : C.ru;
+  const float dl = uv ? D.lv : D.lu, dr = uv ? D.rv : D.ru;
+  float h0 = (T || L0) ? 0.f : ul;
+  h0 = __fadd_rn(h0, T ? 0.f : u.x);
+  h0 = __fadd_rn(h0, (T || R0) ? 0.f : u.y);
+  h0 = __fadd_rn(h0, L0 ? 0.f : cl);
+  h0 = __fadd_rn(h0, R0 ? 0.f : c.y);
+  h0 = __fadd_rn(h0, (B || L0) ? 0.f : dl);
+  h0 = __fadd_rn(h0, B ? 0.f : d.x);
+  h0 = __fadd_rn(h0, (B || R0) ? 0.f : d.y);
+  float h1 = (T || L1) ? 0.f : u.x;
+  h1 = __fadd_rn(h1, T ? 0.f : u.y);
+  h1 = __fadd_rn(h1, (T || R1) ? 0.f : ur);
+  h1 = __fadd_rn(h1, L1 ? 0.f : c.x);
+  h1 = __fadd_rn(h1, R1 ? 0.f : cr);
+  h1 = __fadd_rn(h1, (B || L1) ? 0.f : d.x);
+  h1 = __fadd_rn(h1, B ? 0.f : d.y);
+  h1 = __fadd_rn(h1, (B || R1) ? 0.f : dr);
+  return f2(h0, h1);
+}
+
+template <bool EDGE>
+__device__ __forceinline__ void lbf_pair(const LbRowF& U, const LbRowF& C, const LbRowF& D, const LbStrip& S, int row,
+                                         int gy, bool own_row, float& acc_u, float& acc_v) {
+  const int o = row * LB_RW + S.c0;
+  const float* sc = S.sc;
+  const float2 IIx = *reinterpret_cast<const float2*>(sc + o);
+  const float2 IIy = *reinterpret_cast<const float2*>(sc + LB_PL + o);
+  const float2 II = *reinterpret_cast<const float2*>(sc + 2 * LB_PL + o);
+  // vertical differences and sums at the pair and at the outer columns
+  const float2 vdu = psub(D.cu, U.cu), vsu = padd(U.cu, D.cu);
+  const float2 vdv = psub(D.cv, U.cv), vsv = padd(U.cv, D.cv);
+  const float2 vdo_u = psub(f2(D.lu, D.ru), f2(U.lu, U.ru));  // (left column, right column)
+  const float2 vdo_v = psub(f2(D.lv, D.rv), f2(U.lv, U.rv));
+  const float2 mdu = psub(f2(vdu.y, vdo_u.y), f2(vdo_u.x, vdu.x));  // 4 M
+  const float2 mdv = psub(f2(vdv.y, vdo_v.y), f2(vdo_v.x, vdv.x));
+  // centre-row neighbours of the pair
+  const float2 Lu = f2(C.lu, C.cu.x), Ru = f2(C.cu.y, C.ru);
+  const float2 Lv = f2(C.lv, C.cv.x), Rv = f2(C.cv.y, C.rv);
+  const float2 dtu = psub(Ru, Lu), dtv = psub(Rv, Lv);  // 2 D^T
+  const float2 hsv = padd(Lv, Rv);                       // F^T
+  float2 Hu, Hv;
+  if (EDGE) {
+    const bool T = gy == 0, B = gy == S.H - 1;
+    const bool L0 = S.gx0 == 0, R0 = S.gx0 == S.W - 1, L1 = S.gx0 + 1 == 0, R1 = S.gx0 + 1 == S.W - 1;
+    Hu = lbf_hsum_edge(U, C, D, T, B, L0, R0, L1, R1, false);
+    Hv = lbf_hsum_edge(U, C, D, T, B, L0, R0, L1, R1, true);
+  } else {
+    const float2 vso_u = padd(f2(U.lu, U.ru), f2(D.lu, D.ru));
+    const float2 vso_v = padd(f2(U.lv, U.rv), f2(D.lv, D.rv));
+    Hu = padd(padd(vso_u, f2s(__fadd_rn(vsu.x, vsu.y))), padd(Lu, Ru));
+    Hv = padd(padd(vso_v, f2s(__fadd_rn(vsv.x, vsv.y))), hsv);
+  }
+  const float2 a2 = pmul(IIx, f2s(0.5f)), a3 = pmul(IIy, f2s(0.5f)), a5 = pmul(II, f2s(0.25f));
+  const float2 h2 = f2s(S.h);
+  // bu = 2 IIx D u + IIx D^T v + IIy D v + II F u + II M v + h H u + Ixt
+  float2 bu = *reinterpret_cast<const float2*>(sc + 3 * LB_PL + o);
+  bu = pfma(h2, Hu, bu);
+  bu = pfma(a5, mdv, bu);
+  bu = pfma(II, vsu, bu);
+  bu = pfma(a3, vdv, bu);
+  bu = pfma(a2, dtv, bu);
+  bu = pfma(IIx, vdu, bu);
+  // bv = IIy D u + IIx D^T u + 2 IIy D^T v + II M u + II F^T v + h H v + Iyt
+  float2 bv = *reinterpret_cast<const float2*>(sc + 4 * LB_PL + o);
+  bv = pfma(h2, Hv, bv);
+  bv = pfma(a5, mdu, bv);
+  bv = pfma(II, hsv, bv);
+  bv = pfma(IIy, dtv, bv);
+  bv = pfma(a2, dtu, bv);
+  bv = pfma(a3, vdu, bv);
+  const float2 B11 = *reinterpret_cast<const float2*>(sc + 5 * LB_PL + o);
+  const float2 B12 = *reinterpret_cast<const float2*>(sc + 6 * LB_PL + o);
+  const float2 B22 = *reinterpret_cast<const float2*>(sc + 7 * LB_PL + o);
+  const float2 m1 = f2s(-1.0f);
+  const float2 nu = pmul(pfma(B11, bu, pmul(B12, bv)), m1);
+  const float2 nv = pmul(pfma(B12, bu, pmul(B22, bv)), m1);
+  const bool in0 = S.gx0 < S.W, in1 = S.gx0 + 1 < S.W;
+  if (S.ou) {
+    *reinterpret_cast<float2*>(&S.ou[row][S.c0]) = nu;
+    *reinterpret_cast<float2*>(&S.ov[row][S.c0]) = nv;
+  } else if (own_row && S.own_col) {
+    const size_t gi = (size_t)row * S.pitch;
+    if (in1) {
+      *reinterpret_cast<float2*>(S.gu + gi) = nu;
+      *reinterpret_cast<float2*>(S.gv + gi) = nv;
+    } else if (in0) {
+      S.gu[gi] = nu.x;
+      S.gv[gi] = nv.x;
+    }
+  }
+  if (own_row && S.own_col) {
+    const float2 eu = psub(nu, C.cu), ev = psub(nv, C.cv);
+    const float eu0 = in0 ? eu.x : 0.0f, ev0 = in0 ? ev.x : 0.0f;
+    const float eu1 = in1 ? eu.y : 0.0f, ev1 = in1 ? ev.y : 0.0f;
+    acc_u = __fmaf_rn(eu0, eu0, __fmaf_rn(eu1, eu1, acc_u));
+    acc_v = __fmaf_rn(ev0, ev0, __fmaf_rn(ev1, ev1, acc_v));
+  }
+}
+
+template <bool EDGE>
+__device__ __forceinline__ void lbf_strip(const LbPlane* su, const LbPlane* sv, const LbStrip& S, const LbCols& cols,
+                                          int r0, int n, int rlo, int rhi, double& acc_u, double& acc_v) {
+  LbRowF A, B, C;
+  float au = 0.f, av = 0.f;
+#define LB_ROW(r) (EDGE ? clampi((r), rlo, rhi) : (r))
+#define LB_OWN(row) ((row) >= LB_T && (row) < LB_T + LB_TH)
+  lbf_load<EDGE>(A, su, sv, LB_ROW(r0 - 1), cols);
+  lbf_load<EDGE>(B, su, sv, r0, cols);
+#pragma unroll 1
+  for (int r = 0; r < n; r += 3) {
+    const int row = r0 + r;
+    lbf_load<EDGE>(C, su, sv, LB_ROW(row + 1), cols);
+    lbf_pair<EDGE>(A, B, C, S, row, S.gy0 + r, LB_OWN(row), au, av);
+    if (r + 1 < n) {
+      lbf_load<EDGE>(A, su, sv, LB_ROW(row + 2), cols);
+      lbf_pair<EDGE>(B, C, A, S, row + 1, S.gy0 + r + 1, LB_OWN(row + 1), au, av);
+    }
+    if (r + 2 < n) {
+      lbf_load<EDGE>(B, su, sv, LB_ROW(row + 3), cols);
+      lbf_pair<EDGE>(C, A, B, S, row + 2, S.gy0 + r + 2, LB_OWN(row + 2), au, av);
+    }
+  }
+#undef LB_OWN
+#undef LB_ROW
+  acc_u += (double)au;
+  acc_v += (double)av;
+}
+
+template <bool FAST>
 __global__ void __launch_bounds__(32 * LB_WARPS, 2) ls_pass_kernel(const __grid_constant__ CUtensorMap tm_coef,
                                                          const __grid_constant__ CUtensorMap tm_u0,
                                                          const __grid_constant__ CUtensorMap tm_v0,
@@ -582,10 +747,17 @@ __global__ void __launch_bounds__(32 * LB_WARPS, 2) ls_pass_kernel(const __grid_
       S.gu = un + ((ptrdiff_t)(y0 - LB_T) * pitch + S.gx0);
       S.gv = vn + ((ptrdiff_t)(y0 - LB_T) * pitch + S.gx0);
       S.gy0 = y0 - LB_T + ra;
-      if (edge)
-        lb_strip<true>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
-      else
-        lb_strip<false>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
+      if (FAST) {
+        if (edge)
+          lbf_strip<true>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
+        else
+          lbf_strip<false>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
+      } else {
+        if (edge)
+          lb_strip<true>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
+        else
+          lb_strip<false>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
+      }
     }
     if (!rollback) {
       for (int o = 16; o > 0; o >>= 1) {
@@ -688,10 +860,12 @@ extern "C" size_t of_ls_workspace_size(int H, int W, int pitch, int maxnum) {
   return s.off;
 }
 
-extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float h,
-                           int maxnum, double tol, int* iters_out, double* err_out, void* workspace,
-                           size_t workspace_bytes, void* stream) {
+extern "C" int of_ls_solve_mode(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float h,
+                                int maxnum, double tol, int mode, int* iters_out, double* err_out, void* workspace,
+                                size_t workspace_bytes, void* stream) {
   OF_REQUIRE(!bad_plane(I0, H, W, pitch) && I1 && U && V, "of_ls_solve: bad plane");
+  OF_REQUIRE(mode == OF_LS_EXACT || mode == OF_LS_FAST, "of_ls_solve: mode must be OF_LS_EXACT or OF_LS_FAST");
+  const bool fast = mode == OF_LS_FAST;
   OF_REQUIRE(maxnum >= 0 && maxnum <= 100000, "of_ls_solve: maxnum out of range");
   size_t need = of_ls_workspace_size(H, W, pitch, maxnum);
   if (!workspace || workspace_bytes < need)
@@ -728,7 +902,7 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
     }
   }
   {
-    cudaError_t e = OF_SMEM_OPT_IN(ls_pass_kernel, LB_SMEM);
+    cudaError_t e = fast ? OF_SMEM_OPT_IN(ls_pass_kernel<true>, LB_SMEM) : OF_SMEM_OPT_IN(ls_pass_kernel<false>, LB_SMEM);
     if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_ls_solve: %s", cudaGetErrorString(e));
   }
   // control block, flags, counters, redo counts and sums are contiguous: one memset
@@ -755,8 +929,9 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
     cfg.stream = st;
     cfg.attrs = dependent ? pdl : nullptr;
     cfg.numAttrs = dependent ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, ls_pass_kernel, tm_coef, tm_u[0], tm_v[0], tm_u[1], tm_v[1], ub[0], vb[0], ub[1],
-                              vb[1], H, W, P, h, PP, ctrl, ss, run, done, redo, inv_n, tol, err_flag, 1.0f);
+    return cudaLaunchKernelEx(&cfg, fast ? ls_pass_kernel<true> : ls_pass_kernel<false>, tm_coef, tm_u[0], tm_v[0],
+                              tm_u[1], tm_v[1], ub[0], vb[0], ub[1], vb[1], H, W, P, h, PP, ctrl, ss, run, done, redo,
+                              inv_n, tol, err_flag, 1.0f);
   };
   for (; k0 < maxnum; k0 += LB_T, p++) {
     LbPass P0{k0, maxnum - k0 < LB_T ? maxnum - k0 : LB_T, p, 0};
@@ -773,6 +948,13 @@ extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V,
   ls_count_kernel<<<1, 1, 0, st>>>(ctrl, ss, inv_n, err_flag, iters_out, err_out);
   ls_finalize_kernel<<<rg, 256, 0, st>>>(ub[0], vb[0], ub[1], vb[1], V, U, W, P, pitch, ctrl);
   return check_launch("of_ls_solve", nl + 1);
+}
+
+extern "C" int of_ls_solve(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float h,
+                           int maxnum, double tol, int* iters_out, double* err_out, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  return of_ls_solve_mode(I0, I1, U, V, H, W, pitch, h, maxnum, tol, OF_LS_EXACT, iters_out, err_out, workspace,
+                          workspace_bytes, stream);
 }
 
 // ---------------------------------------------------------------------------------------

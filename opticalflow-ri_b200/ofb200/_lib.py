@@ -60,6 +60,7 @@ _SIGS = {
     "of_ls_workspace_size": ([_I, _I, _I, _I], _Z),
     "of_ls_solve": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P, _Z, _P], _I),
     "of_ls_solve_noalloc": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P], _I),
+    "of_ls_solve_mode": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _I, _P, _P, _P, _Z, _P], _I),
     "of_warp_liushen_workspace_size": ([_I, _I], _Z),
     "of_warp_liushen_scatter": ([_P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P, _Z, _P], _I),
     "of_warp_liushen_ofe": ([_P, _P, _P, _P, _I, _I, _I, _P], _I),

@@ -9,6 +9,7 @@ libofb200.so.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -231,15 +232,29 @@ def ls_coefficients(I1n, Et, h: float):
          float(np.float32(h)), stream_ptr())
     return coef.view(8, H, W)
 
-def ls_solve(I0, I1, U, V, h: float, maxnum: int = 60, tol: float = 1e-8, iters=None, err=None):
+LS_ARITHMETICS = ("fast", "exact")
+
+
+def ls_arithmetic(arithmetic=None) -> str:
+    """The Liu-Shen sweep's arithmetic: 'fast' (float32 with fused multiply-adds, within
+    float32 rounding of the reference) or 'exact' (bit-exact with the reference's float32
+    fields).  None reads OFB_LS_ARITHMETIC, default 'fast'."""
+    a = arithmetic if arithmetic is not None else os.environ.get("OFB_LS_ARITHMETIC", "fast")
+    if a not in LS_ARITHMETICS:
+        raise ValueError(f"Liu-Shen arithmetic must be one of {LS_ARITHMETICS}, not {a!r}")
+    return a
+
+
+def ls_solve(I0, I1, U, V, h: float, maxnum: int = 60, tol: float = 1e-8, iters=None, err=None, arithmetic=None):
     """Liu-Shen in place on U (x) and V (y).  Returns (U, V, iters, err) (device scalars)."""
     p = _same_pitch(I0, I1, U, V)
     H, W = I0.shape
+    mode = 1 if ls_arithmetic(arithmetic) == "fast" else 0  # OF_LS_FAST / OF_LS_EXACT
     iters = torch.empty((), dtype=torch.int32, device=I0.device) if iters is None else iters
     err = torch.empty((), dtype=torch.float64, device=I0.device) if err is None else err
     ws, wn = workspace(lib().of_ls_workspace_size(H, W, p, int(maxnum)), "ls")
-    call("of_ls_solve", _plane(I0, "I0")[0], _plane(I1, "I1")[0], _plane(U, "U")[0], _plane(V, "V")[0], H, W, p,
-         float(np.float32(h)), int(maxnum), float(tol), ctypes.c_void_p(iters.data_ptr()),
+    call("of_ls_solve_mode", _plane(I0, "I0")[0], _plane(I1, "I1")[0], _plane(U, "U")[0], _plane(V, "V")[0], H, W, p,
+         float(np.float32(h)), int(maxnum), float(tol), mode, ctypes.c_void_p(iters.data_ptr()),
          ctypes.c_void_p(err.data_ptr()), ws, wn, stream_ptr())
     return U, V, iters, err
 

@@ -3,6 +3,11 @@ import sys
 
 import pytest
 
+# The parity suites compare the Liu-Shen solver bit for bit, which only its 'exact'
+# arithmetic promises; the float32 'fast' arithmetic (the library default) is tested on its
+# own, explicitly, in test_gpu_ls_fast.py.
+os.environ["OFB_LS_ARITHMETIC"] = "exact"
+
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(REPO, "opticalflow-ri_b200")
 for p in (PKG, os.path.join(REPO, "oracle"), REPO):
