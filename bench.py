@@ -11,8 +11,13 @@ noise 2 DN).  One step = `--pairs` frame pairs through the whole pipeline, sprea
           aggregated over all ranks (pairs / max-over-ranks time).
   e2e   : pairs/s through the reference-facing API (genericPyramidalOpticalFlow with
           numpy float32 frames in and numpy U, V out: host<->device copies inside).
-  roofline : the Liu-Shen solve at 1024^2 (the dominant kernel), algorithmic bytes =
-          (24 B x sweeps + 8 B) per pixel, against the measured HBM copy bandwidth.
+  roofline : the Liu-Shen solves of one step (the dominant kernel): --pairs solves at
+          1024^2 running concurrently on --streams streams, as they do in the step (their
+          working set, 60 MB each, exceeds the 126 MB L2), algorithmic bytes = (24 B x
+          sweeps + 8 B) per pixel per solve, against the measured HBM copy bandwidth.
+  configs : the other workloads, each with its own device-timed pairs/s, roofline and CPU
+          baseline: Horn-Schunck 256^2 (600 sweeps), dense LK pyr2 512^2, and the batch of
+          256 uneven pairs (128^2-2048^2, four methods; --no-batch skips it).
   cpu_baseline : the CPU oracle (C restatement of the reference, 1 thread) on one pair.
 
 --impl reference: the CPU restatement of the reference's path (the reference itself needs
@@ -43,7 +48,7 @@ L2_BYTES = 126 * 2 ** 20
 REF_BUDGET_S = 90.0
 # DRAM bytes (read + write) of one 60-sweep Liu-Shen solve at 1024^2, summed over its
 # launches from one ncu capture (profiles/ls_solve_traffic_1024.txt; cold cache per launch)
-NCU_LS_TRAFFIC = {1024: 663.48e6}
+NCU_LS_TRAFFIC = {("exact", 1024): 663.48e6}
 
 
 def parse():
@@ -60,6 +65,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
+    p.add_argument("--no-configs", action="store_true", help="skip the HS 256^2 / LK 512^2 / batch workloads")
+    p.add_argument("--no-batch", action="store_true", help="skip the 256-pair batch inside the configs block")
     p.add_argument("--learned-weights", default=None, help="weights + calibration .npz (default: packaged)")
     p.add_argument("--batch-pairs", type=int, default=256, help="--mode batch: pairs in the manifest")
     p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn", "fb", "e2e"],
@@ -311,35 +318,9 @@ def run_ours(args, rank, world, local_rank):
     total_ms = float(t.item())
     barrier()
 
-    # roofline of the dominant kernel: the Liu-Shen solve at full size, graph-replayed alone
-    from gaussian_filter import prepareGaussianKernel
-    from ofb200 import graph as _graph
-    a = ops.u8_to_f32(frames[0][0])
-    b = ops.u8_to_f32(frames[0][1])
-    taps = prepareGaussianKernel(0.48, 5)
-    fa, fb = ops.prefilter(a, taps), ops.prefilter(b, taps)
-    U0 = torch.zeros_like(fa)
-
-    def ls_fn(x, y, u0):
-        U, V = u0.clone(), u0.clone()
-        return ops.ls_solve(x, y, U, V, 10.0)
-
-    ls_ms, iters = [], None
-    for r in range(6):
-        flush.zero_()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        _, _, it, _ = _graph.CACHE.run(("bench-ls", args.size), ls_fn, [fa, fb, U0])
-        e1.record()
-        e1.synchronize()
-        if r > 1:
-            ls_ms.append(e0.elapsed_time(e1))
-        iters = int(it.item())
-    ls_ms = float(np.mean(ls_ms))
-    alg_bytes = (24.0 * iters + 8.0) * N
-    peak, peak_kind = peaks()
-    achieved = alg_bytes / (ls_ms * 1e-3) / 1e9
+    # roofline of the dominant kernel: the step's Liu-Shen solves (--pairs of them at full
+    # size, concurrently on --streams streams, as in the step), graph-replayed
+    roof = ls_step_roofline(args, frames, flush)
 
     # end to end through the reference-facing API, host buffers
     e2e = None
@@ -365,6 +346,7 @@ def run_ours(args, rank, world, local_rank):
 
     learned = None if args.no_learned else run_learned(args, step_frames, pairs, dev, flush, world,
                                                            pairs_total_ms=total_ms)
+    configs = None if args.no_configs else run_configs(args, rank, world, dev, flush)
     if rank != 0:
         return None
     pairs_total = args.pairs * args.steps * world
@@ -376,16 +358,240 @@ def run_ours(args, rank, world, local_rank):
                    "unique_pairs": args.unique, "streams": args.streams,
                    "l2": "flushed between steps (256 MB write)",
                    "parallelism": f"pairs sharded over {world} rank(s)"},
-        "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "learned": learned,
-        "roofline": {"kernel": "Liu-Shen solve 1024^2 (setup + sweeps)", "bound": "hbm",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind,
-                     "traffic": NCU_LS_TRAFFIC.get(args.size) if iters == 60 else None, "sweeps": iters, "ms": ls_ms,
-                     "algorithmic_bytes": alg_bytes},
+        "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "learned": learned, "roofline": roof,
     }
+    if configs is not None:
+        line["configs"] = configs
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pairs[0])
     return line
+
+
+def _graph_of(fn):
+    """fn (enqueues work on the current stream, may fork to other streams and join) run once
+    eagerly, then captured into a CUDA graph.  Returns (graph, outputs of the capture)."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.graph(g, stream=side):
+        out = fn()
+    torch.cuda.synchronize()
+    return g, out
+
+
+def _time_graph(g, flush, reps, warm=2):
+    """Mean CUDA-event time (ms) of g.replay() with L2 flushed before each replay."""
+    import torch
+    ms = []
+    for r in range(warm + reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        e1.synchronize()
+        if r >= warm:
+            ms.append(e0.elapsed_time(e1))
+    return float(np.mean(ms))
+
+
+def _fork_join(streams, jobs):
+    """Runs jobs[i]() on streams[i % len(streams)] after the current stream's work, and
+    makes the current stream wait for all of them (capturable)."""
+    import torch
+    cur = torch.cuda.current_stream()
+    for st in streams:
+        st.wait_stream(cur)
+    outs = []
+    for i, job in enumerate(jobs):
+        with torch.cuda.stream(streams[i % len(streams)]):
+            outs.append(job())
+    for st in streams:
+        cur.wait_stream(st)
+    return outs
+
+
+def ls_step_roofline(args, frames, flush):
+    """The step's Liu-Shen solves alone: --pairs prefiltered 1024^2 pairs solved concurrently
+    on --streams streams (one CUDA graph), L2 flushed before each replay."""
+    import torch
+    from gaussian_filter import prepareGaussianKernel
+    from ofb200 import ops
+    taps = prepareGaussianKernel(0.48, 5)
+    N = args.size * args.size
+    pre = []
+    for i in range(args.pairs):
+        a8, b8 = frames[i % len(frames)]
+        pre.append((ops.prefilter(ops.u8_to_f32(a8), taps), ops.prefilter(ops.u8_to_f32(b8), taps)))
+    zero = torch.zeros_like(pre[0][0])
+    streams = [torch.cuda.Stream() for _ in range(max(1, args.streams))]
+    arith = ops.ls_arithmetic()
+
+    def solve(fa, fb):
+        return lambda: ops.ls_solve(fa, fb, zero.clone(), zero.clone(), 10.0, arithmetic=arith)
+
+    g, outs = _graph_of(lambda: _fork_join(streams, [solve(fa, fb) for fa, fb in pre]))
+    ms = _time_graph(g, flush, reps=5)
+    iters = [int(o[2].item()) for o in outs]
+    alg = float(sum((24.0 * k + 8.0) * N for k in iters))
+    peak, peak_kind = peaks()
+    achieved = alg / (ms * 1e-3) / 1e9
+    per_solve = NCU_LS_TRAFFIC.get((arith, args.size))
+    del g
+    return {"kernel": f"Liu-Shen solve {args.size}^2 (set-up + sweeps), {args.pairs} concurrent on {len(streams)} "
+                      f"streams as in the step, working set {args.pairs * 60} MB > L2",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_kind": peak_kind, "traffic": per_solve * args.pairs if per_solve and set(iters) == {60} else None,
+            "traffic_note": "ncu DRAM bytes of one solve's launches (cold cache per launch) x solves",
+            "sweeps": iters[0] if len(set(iters)) == 1 else iters, "ms": ms, "solves": args.pairs,
+            "algorithmic_bytes": alg, "arithmetic": arith}
+
+
+FP32_LANES_PER_SM = 128
+
+
+def _fp32_peak_tflops(clk):
+    """Nominal FP32 rate at the sampled max SM clock: 148 SMs x 128 lanes x 2 flop."""
+    mhz = (clk or {}).get("sm_max_mhz") or 1965.0
+    return 148 * FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12
+
+
+def _pair_throughput(spec_fn, frames, nstreams, flush, reps=5):
+    """Device pairs/s of a list of uint8 frame pairs through PairBatch (one CUDA graph)."""
+    from ofb200.batch import PairBatch
+    batch = PairBatch([spec_fn() for _ in frames], streams=nstreams)
+    for _ in range(3):
+        batch.run(frames)
+    import torch
+    ms = []
+    for r in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.run(frames)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return len(frames) / (float(np.mean(ms)) * 1e-3), float(np.mean(ms))
+
+
+def _oracle_cfg(args):
+    cfg, size = args
+    O = _oracle()
+    from ofb200 import synthetic as S
+    a8, b8, _, _ = S.config_pair(cfg, seed=7, size=size)
+    a, b = a8.astype(np.float32), b8.astype(np.float32)
+    t0 = time.perf_counter()
+    if cfg == "hs256":
+        O.pyramid(a, b, 3.4, O.HS([21], 600), 1, 1, None)
+    else:
+        O.pyramid(a, b, 2, O.LK(5, 13), 2, 1, 0.48, None, warping=False)
+    return time.perf_counter() - t0
+
+
+def run_configs(args, rank, world, dev, flush):
+    """Configs 1, 2 and 4 with their own device-timed numbers (each rank runs its own pairs:
+    weak scaling; pairs/s summed over ranks)."""
+    import torch
+    import torch.distributed as dist
+    import denseLucasKanade_PyCL as LK
+    import HornSchunck as HS
+    from ofb200 import synthetic as S
+    from ofb200.batch import PairSpec
+    from ofb200.shard import max_over_ranks
+    out = {}
+    n_hs, n_lk, nst = 16, 8, 8
+    hs_frames, lk_frames = [], []
+    for i in range(n_hs):
+        a, b, _, _ = S.config_pair("hs256", seed=200 + 1000 * rank + i)
+        hs_frames.append((torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)))
+    for i in range(n_lk):
+        a, b, _, _ = S.config_pair("lk512", seed=300 + 1000 * rank + i)
+        lk_frames.append((torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)))
+    clocks = Clocks(dev.index) if rank == 0 else None
+    hs_spec = lambda: PairSpec(3.4, lambda: HS.HSOpticalFlowAlgoAdapter([21], 600), 1, 1, key=("hs",))  # noqa: E731
+    lk_spec = lambda: PairSpec(2.0, lambda: LK.denseLucasKanade_PyCl(Niter=5, halfWindow=13), 2, 1, 0.48,  # noqa
+                               key=("lk",))
+    _, hs_ms = _pair_throughput(hs_spec, hs_frames, nst, flush)
+    _, lk_ms = _pair_throughput(lk_spec, lk_frames, nst, flush)
+    clk = clocks.stop() if clocks else None
+    hs_ms, lk_ms = max_over_ranks(hs_ms, dev), max_over_ranks(lk_ms, dev)
+    peak, peak_kind = peaks()
+    hs_bytes = (600 * 24.0 + 20.0 + 8.0) * 256 * 256  # sweeps, derivatives, prefilter (per pair)
+    lk_px = 512 * 512 + 256 * 256
+    lk_flop = 7.0e4 * lk_px
+    fp32 = _fp32_peak_tflops(clk)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(2) as pool:
+            t_hs, t_lk = pool.map(_oracle_cfg, [("hs256", 256), ("lk512", 256)])
+        cpu = {"hs256": {"value": 1.0 / t_hs, "unit": "pairs/s", "cores": 1, "kind": "port",
+                         "sample": f"1 pair 256x256, full pipeline, {t_hs:.1f} s"},
+               "lk512": {"value": 0.25 / t_lk, "unit": "pairs/s", "cores": 1, "kind": "port",
+                         "sample": f"1 pair at 256x256 (a quarter of the pixels), full LK pyr2 pipeline, {t_lk:.1f} s; "
+                                   "pairs/s scaled by the pixel ratio"}}
+    out["hs256"] = {"workload": "PyHSchunck_Fs3_4 Horn-Schunck, 256x256 Poiseuille pairs, 600 sweeps",
+                    "value": n_hs * world / (hs_ms * 1e-3), "unit": "pairs/s", "ms_per_step": hs_ms,
+                    "pairs_per_step_per_gpu": n_hs, "streams": nst,
+                    "roofline": {"bound": "hbm", "achieved": n_hs * hs_bytes / (hs_ms * 1e-3) / 1e9, "peak": peak,
+                                 "unit": "GB/s", "frac": n_hs * hs_bytes / (hs_ms * 1e-3) / 1e9 / peak,
+                                 "peak_kind": peak_kind, "algorithmic_bytes_per_pair": hs_bytes},
+                    "cpu_baseline": cpu["hs256"] if cpu else None}
+    out["lk512"] = {"workload": "denseLK_Fs2_0_PyrLvls2 dense LK pyr2, 512x512 Lamb-Oseen pairs",
+                    "value": n_lk * world / (lk_ms * 1e-3), "unit": "pairs/s", "ms_per_step": lk_ms,
+                    "pairs_per_step_per_gpu": n_lk, "streams": nst,
+                    "roofline": {"bound": "fp32", "achieved": n_lk * lk_flop / (lk_ms * 1e-3) / 1e12, "peak": fp32,
+                                 "unit": "TFLOP/s", "frac": n_lk * lk_flop / (lk_ms * 1e-3) / 1e12 / fp32,
+                                 "peak_kind": "nominal (148 SMs x 128 FP32 lanes x 2 x max SM clock)",
+                                 "algorithmic_flop_per_pair": lk_flop,
+                                 "flop_model": "7e4 FP32 flop per pixel (27x27 window, 5 Newton steps), both levels"},
+                    "cpu_baseline": cpu["lk512"] if cpu else None}
+    out["clocks"] = clk
+    if not args.no_batch:
+        out["batch256"] = run_batch_inline(args, rank, world, dev, flush)
+    return out
+
+
+def run_batch_inline(args, rank, world, dev, flush):
+    """Config 4 inside the default bench: the seeded 256-pair manifest, autotuned over a
+    short candidate list, one timed pass (device events, L2 flushed before it)."""
+    import multiprocessing as mp
+    import torch
+    from ofb200.batch import autotune, config4_manifest, pair_cost_of, render_entry
+    from ofb200.shard import max_over_ranks, shard_by_cost
+    manifest = config4_manifest(args.batch_pairs, seed=0)
+    mine = shard_by_cost([pair_cost_of(e) for e in manifest], world)[rank]
+    entries = [manifest[i] for i in mine]
+    try:
+        ncores = len(os.sched_getaffinity(0))
+    except Exception:
+        ncores = os.cpu_count() or 1
+    with mp.get_context("spawn").Pool(max(1, min(32, ncores // world))) as pool:
+        rendered = pool.map(render_entry, entries)
+    frames = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _, _ in rendered]
+    runner, table = autotune(entries, frames, chunks=(64, 256), streams=(8,), reps=1)
+    ms = []
+    for _ in range(2):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        runner.run(frames)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = max_over_ranks(float(np.mean(ms)), dev)
+    del runner
+    return {"workload": f"{len(manifest)} pairs, sizes 128^2-2048^2, HS / LK pyr2 / FB pyr2 / FB pyr2 + LS, "
+                        "Poiseuille / Lamb-Oseen / random-Fourier, max 4 px",
+            "value": len(manifest) / (t * 1e-3), "unit": "pairs/s", "ms_per_pass": t, "scaling": "strong",
+            "autotuned": {f"{c}x{s}": round(v, 2) for (c, s), v in table.items()}}
 
 
 def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
