@@ -134,6 +134,48 @@ int of_hs_solve(const float* I0, const float* I1, float* U, float* V, int H, int
                 int niter, double* err_out, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------------
+ * Batches of frame pairs (the batched workload of uneven pairs).  Per-pair status words:
+ * bits ORed into a caller's DEVICE int array (zero it before the first call).
+ * ------------------------------------------------------------------------------- */
+#define OF_ST_NONFINITE_INPUT 0x1  /* a frame holds NaN or Inf */
+#define OF_ST_WAIT_TIMEOUT 0x2     /* a bounded device wait gave up; the pair's result is invalid */
+#define OF_ST_NOT_CONVERGED 0x4    /* an iterative solve used all its sweeps above its tolerance */
+#define OF_ST_SINGULAR 0x8         /* singular per-pixel systems (LK det < eps, LS det == 0) */
+#define OF_ST_NONFINITE_OUTPUT 0x10 /* the result holds NaN or Inf */
+
+/* Tuning of a batched launch: tile_shape indexes the kernel's table of (region width,
+ * region height, sweeps per pass) shapes, listed by of_hs_batch_shape(). */
+typedef struct OfTuning {
+  int tile_shape;
+  int streams;   /* host-side concurrency of callers that use streams; unused by the kernels */
+  int reserved[2];
+} OfTuning;
+
+/* One Horn-Schunck pair of a batch: DEVICE planes of H x W float32 with row pitch `pitch`;
+ * U, V hold the initial flow and receive the result. */
+typedef struct OfHsBatchPair {
+  const float* I0;
+  const float* I1;
+  float* U;
+  float* V;
+  int H, W, pitch;
+  float alpha;
+  int niter;
+} OfHsBatchPair;
+
+/* Horn-Schunck of n pairs (any sizes) in ONE persistent launch — replaces n calls of
+ * HSOpticalFlowAlgoAdapter.compute / HS (src/HornSchunck.py:34-104), bit-exact like
+ * of_hs_solve.  Work items (pass, pair, tile) come from a device queue; a pass of a pair
+ * waits for its previous pass with a bounded poll of at most `wait_limit` iterations, after
+ * which the pair gets OF_ST_WAIT_TIMEOUT and is skipped (the launch still ends).  The
+ * derivative pass sets OF_ST_NONFINITE_INPUT for frames with NaN / Inf, the last sweep pass
+ * OF_ST_NONFINITE_OUTPUT.  status: DEVICE int[n].  The HS error value is not computed. */
+int of_hs_batch_shape(int index, int* region_w, int* region_h, int* sweeps_per_pass);
+size_t of_hs_batch_workspace_size(const OfHsBatchPair* pairs, int n);
+int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tuning, int* status, long long wait_limit,
+                void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------
  * A8/A9 Liu-Shen physics-based optimiser — replaces LiuShenOpticalFlowAlgoAdapter.compute /
  * physicsBasedOpticalFlowLiuShen (src/PhysicsBasedOpticalFlowLiuShen.py:33-158).
  * Frames are normalised by their maxima; sweeps run while err > tol and k < maxnum

@@ -1,0 +1,416 @@
+// Horn-Schunck for one or many frame pairs in ONE persistent launch over a device work
+// queue (src/HornSchunck.py:51-126, bit-exact like hs.cu).
+//
+// Work items are (pass, pair, tile), handed out in that order by an atomic ticket
+// counter to CTAs that stay resident for the whole launch.  Pass 0 of a pair computes its
+// derivative planes (computeDerivatives, :106-126) and copies the initial U, V for a tile;
+// pass p >= 1 runs up to HQ_T Jacobi sweeps (HS_helper, :61-70) on the tile with a halo of
+// HQ_T cells staged in shared memory (the temporal blocking of hs_pass_kernel), reading
+// the previous pass's fields and writing the next buffer of a ping-pong pair.  An item of
+// pass p waits until every tile of pass p - 1 of the same pair is done (a per-pair counter
+// of finished items).  The ticket order makes this free of deadlock: an item only waits for
+// items with smaller tickets, which were handed out earlier to CTAs that are running and
+// never wait for later ones.  The wait is bounded: after `wait_limit` polls the item gives
+// up, sets OF_ST_WAIT_TIMEOUT in its pair's status word and the launch's error flag, and
+// every later item of that pair is skipped (counted done, so nothing waits on it).
+// Cross-CTA data goes through L2 only (ld.global.cg / st.global.cg), published by
+// __syncthreads + __threadfence + atomicAdd and consumed after the counter is observed.
+#include "common.cuh"
+
+namespace ofb {
+
+struct HsqPair {
+  const float* I0;   // frame at t0
+  const float* I1;   // frame at t1
+  float* U;          // initial flow in, result out
+  float* V;
+  float* fx;         // workspace planes (pitch `pitch`)
+  float* fy;
+  float* ft;
+  float* U0;         // the initial flow (kept for the reference's error)
+  float* V0;
+  float* Ub;         // ping-pong partner of U / V
+  float* Vb;
+  int H, W, pitch;
+  float a2;          // alpha^2
+  int niter;
+  int passes;        // 1 + ceil(niter / T): the derivative pass and the sweep passes
+  int tx, tiles;     // tiles per row, tiles per pass
+  unsigned int tile0;  // sum of tiles of the earlier pairs
+};
+
+__device__ __forceinline__ double hq_acc(double a, float v, double w) { return __fma_rn((double)v, w, a); }
+
+// Derivatives of one pixel (hs_deriv_kernel's arithmetic) and the copy of the initial flow.
+// Returns false when a frame sample of the pixel is not finite.
+__device__ __forceinline__ bool hq_deriv_px(const HsqPair& P, int y, int x) {
+  const int H = P.H, W = P.W, pitch = P.pitch;
+  int y1 = mirror1(y + 1, H), x1 = mirror1(x + 1, W);
+  size_t i00 = (size_t)y * pitch + x, i01 = (size_t)y * pitch + x1, i10 = (size_t)y1 * pitch + x,
+         i11 = (size_t)y1 * pitch + x1;
+  const float* f1 = P.I1;
+  const float* f0 = P.I0;
+  float a00 = f1[i00], a01 = f1[i01], a10 = f1[i10], a11 = f1[i11];
+  float b00 = f0[i00], b01 = f0[i01], b10 = f0[i10], b11 = f0[i11];
+  double t;
+  t = hq_acc(hq_acc(hq_acc(hq_acc(0.0, a00, 0.25), a01, -0.25), a10, 0.25), a11, -0.25);
+  float gx1 = (float)t;
+  t = hq_acc(hq_acc(hq_acc(hq_acc(0.0, b00, 0.25), b01, -0.25), b10, 0.25), b11, -0.25);
+  float gx0 = (float)t;
+  t = hq_acc(hq_acc(hq_acc(hq_acc(0.0, a00, 0.25), a01, 0.25), a10, -0.25), a11, -0.25);
+  float gy1 = (float)t;
+  t = hq_acc(hq_acc(hq_acc(hq_acc(0.0, b00, 0.25), b01, 0.25), b10, -0.25), b11, -0.25);
+  float gy0 = (float)t;
+  t = hq_acc(hq_acc(hq_acc(hq_acc(0.0, b00, 0.25), b01, 0.25), b10, 0.25), b11, 0.25);
+  float gt0 = (float)t;
+  t = hq_acc(hq_acc(hq_acc(hq_acc(0.0, a00, -0.25), a01, -0.25), a10, -0.25), a11, -0.25);
+  float gt1 = (float)t;
+  __stcg(P.fx + i00, __fadd_rn(gx1, gx0));
+  __stcg(P.fy + i00, __fadd_rn(gy1, gy0));
+  __stcg(P.ft + i00, __fadd_rn(gt0, gt1));
+  __stcg(P.U0 + i00, __ldcg(P.U + i00));
+  __stcg(P.V0 + i00, __ldcg(P.V + i00));
+  return isfinite(a00) && isfinite(b00);
+}
+
+// Up to T sweeps on one tile: region RW x RH = (TW + 2T) x (TH + 2T) in shared memory,
+// hb_sweep's arithmetic and border handling.
+template <int RW, int RH, int T>
+struct HqTile {
+  static constexpr int TW = RW - 2 * T, TH = RH - 2 * T, PL = RW * RH;
+  static constexpr size_t SMEM = 7 * (size_t)PL * sizeof(float);
+};
+
+template <int RW, int RH, int T, bool EDGE>
+__device__ __forceinline__ void hq_sweep(const float* __restrict__ sfx, const float* __restrict__ sfy,
+                                         const float* __restrict__ sft, const float* su, const float* sv, float* du,
+                                         float* dv, int s, int x0, int y0, int H, int W, float a2) {
+  const double wc = (double)(1.0f / 12.0f), we = (double)(1.0f / 6.0f);
+  for (int k = threadIdx.x; k < RW * RH; k += blockDim.x) {
+    const int r = k / RW, c = k - r * RW;
+    if (c < 1 + s || c >= RW - 1 - s || r < 1 + s || r >= RH - 1 - s) continue;
+    const int gx = x0 - T + c, gy = y0 - T + r;
+    if (EDGE && (gx < 0 || gx >= W || gy < 0 || gy >= H)) continue;
+    int cm = c - 1, cp = c + 1, rm = r - 1, rp = r + 1;
+    if (EDGE) {
+      cm = mirror1(gx - 1, W) - (x0 - T);
+      cp = mirror1(gx + 1, W) - (x0 - T);
+      rm = mirror1(gy - 1, H) - (y0 - T);
+      rp = mirror1(gy + 1, H) - (y0 - T);
+    }
+    const int om = rm * RW, o0 = r * RW, op = rp * RW;
+    double a = 0.0, b = 0.0;
+    a = __fma_rn((double)su[om + cm], wc, a); b = __fma_rn((double)sv[om + cm], wc, b);
+    a = __fma_rn((double)su[om + c], we, a);  b = __fma_rn((double)sv[om + c], we, b);
+    a = __fma_rn((double)su[om + cp], wc, a); b = __fma_rn((double)sv[om + cp], wc, b);
+    a = __fma_rn((double)su[o0 + cm], we, a); b = __fma_rn((double)sv[o0 + cm], we, b);
+    a = __fma_rn((double)su[o0 + cp], we, a); b = __fma_rn((double)sv[o0 + cp], we, b);
+    a = __fma_rn((double)su[op + cm], wc, a); b = __fma_rn((double)sv[op + cm], wc, b);
+    a = __fma_rn((double)su[op + c], we, a);  b = __fma_rn((double)sv[op + c], we, b);
+    a = __fma_rn((double)su[op + cp], wc, a); b = __fma_rn((double)sv[op + cp], wc, b);
+    const float ua = (float)a, va = (float)b;
+    const int i = o0 + c;
+    const float gxv = sfx[i], gyv = sfy[i];
+    const float num = __fadd_rn(__fadd_rn(__fmul_rn(gxv, ua), __fmul_rn(gyv, va)), sft[i]);
+    const float den = __fadd_rn(__fadd_rn(a2, __fmul_rn(gxv, gxv)), __fmul_rn(gyv, gyv));
+    const float der = __fdiv_rn(num, den);
+    du[i] = __fsub_rn(ua, __fmul_rn(gxv, der));
+    dv[i] = __fsub_rn(va, __fmul_rn(gyv, der));
+  }
+}
+
+// Returns false when a result of the last pass is not finite.
+template <int RW, int RH, int T>
+__device__ bool hq_sweep_item(const HsqPair& P, int pass, int tile, float* sm) {
+  using G = HqTile<RW, RH, T>;
+  const int ty = tile / P.tx, tx = tile - ty * P.tx;
+  const int x0 = tx * G::TW, y0 = ty * G::TH;
+  const int H = P.H, W = P.W, pitch = P.pitch;
+  const int np = P.passes - 1;   // sweep passes
+  const int p = pass - 1;        // this sweep pass
+  // pass p reads the initial flow (p == 0) or the previous pass's buffer and writes U, V when
+  // an even number of passes remain after it (so the last pass writes U, V)
+  const bool to_uv = ((np - 1 - p) & 1) == 0;
+  const float* srcu = p == 0 ? P.U0 : (to_uv ? P.Ub : P.U);
+  const float* srcv = p == 0 ? P.V0 : (to_uv ? P.Vb : P.V);
+  float* dstu = to_uv ? P.U : P.Ub;
+  float* dstv = to_uv ? P.V : P.Vb;
+  const int nsw = min(T, P.niter - p * T);
+  float* sfx = sm;
+  float* sfy = sfx + G::PL;
+  float* sft = sfy + G::PL;
+  float* const bu0 = sft + G::PL;
+  float* const bv0 = sft + 2 * G::PL;
+  float* const bu1 = sft + 3 * G::PL;
+  float* const bv1 = sft + 4 * G::PL;
+  for (int k = threadIdx.x; k < G::PL; k += blockDim.x) {
+    const int r = k / RW, c = k - r * RW;
+    const int gy = y0 - T + r, gx = x0 - T + c;
+    if (gy < 0 || gy >= H || gx < 0 || gx >= W) continue;  // never read
+    const size_t i = (size_t)gy * pitch + gx;
+    sfx[k] = __ldcg(P.fx + i);
+    sfy[k] = __ldcg(P.fy + i);
+    sft[k] = __ldcg(P.ft + i);
+    bu0[k] = __ldcg(srcu + i);
+    bv0[k] = __ldcg(srcv + i);
+  }
+  __syncthreads();
+  const bool edge = x0 < T || y0 < T || x0 + G::TW + T > W || y0 + G::TH + T > H;
+  for (int s = 0; s < nsw; s++) {
+    const bool q = s & 1;
+    float* iu = q ? bu1 : bu0;
+    float* iv = q ? bv1 : bv0;
+    float* ou = q ? bu0 : bu1;
+    float* ov = q ? bv0 : bv1;
+    if (edge)
+      hq_sweep<RW, RH, T, true>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
+    else
+      hq_sweep<RW, RH, T, false>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
+    __syncthreads();
+  }
+  const float* fu = (nsw & 1) ? bu1 : bu0;
+  const float* fv = (nsw & 1) ? bv1 : bv0;
+  bool finite = true;
+  for (int k = threadIdx.x; k < G::TW * G::TH; k += blockDim.x) {
+    const int r = k / G::TW, c = k - r * G::TW;
+    const int y = y0 + r, x = x0 + c;
+    if (y >= H || x >= W) continue;
+    const int o = (r + T) * RW + c + T;
+    __stcg(dstu + (size_t)y * pitch + x, fu[o]);
+    __stcg(dstv + (size_t)y * pitch + x, fv[o]);
+    finite = finite && isfinite(fu[o]) && isfinite(fv[o]);
+  }
+  return finite || p != np - 1;
+}
+
+template <int RW, int RH, int T>
+__global__ void __launch_bounds__(256) hsq_kernel(const HsqPair* __restrict__ pairs, int npairs,
+                                                  unsigned int tiles_total, int max_passes,
+                                                  unsigned long long* ticket, unsigned int* done, int* status,
+                                                  long long wait_limit, int* err_flag) {
+  extern __shared__ float hq_sm[];
+  __shared__ unsigned long long s_item;
+  __shared__ int s_run, s_pair;
+  const unsigned long long nitems = (unsigned long long)tiles_total * (unsigned long long)max_passes;
+  using G = HqTile<RW, RH, T>;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1ull);
+    __syncthreads();
+    const unsigned long long n = s_item;
+    if (n >= nitems) break;
+    const int pass = (int)(n / tiles_total);
+    const unsigned int r = (unsigned int)(n - (unsigned long long)pass * tiles_total);
+    if (threadIdx.x == 0) {  // the pair whose tiles hold ticket offset r (tile0 ascending)
+      int lo = 0, hi = npairs - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pairs[mid].tile0 <= r) lo = mid; else hi = mid - 1;
+      }
+      s_pair = lo;
+    }
+    __syncthreads();
+    const int i = s_pair;
+    const HsqPair& P = pairs[i];
+    const int tile = (int)(r - P.tile0);
+    if (threadIdx.x == 0) {
+      int run = pass < P.passes;
+      if (run && (((volatile int*)status)[i] & OF_ST_WAIT_TIMEOUT)) run = 0;  // the pair already failed
+      if (run && pass > 0) {
+        const unsigned int target = (unsigned int)pass * (unsigned int)P.tiles;
+        long long k = 0;
+        while (((volatile unsigned int*)done)[i] < target) {
+          if (++k > wait_limit) {
+            atomicOr(status + i, OF_ST_WAIT_TIMEOUT);
+            atomicExch(err_flag, 1);
+            run = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+        __threadfence();  // acquire: the previous pass's stores are visible from here on
+      }
+      s_run = run;
+    }
+    __syncthreads();
+    bool ok = true;
+    if (s_run) {
+      if (pass == 0) {
+        const int ty = tile / P.tx, tx = tile - ty * P.tx;
+        for (int k = threadIdx.x; k < G::TW * G::TH; k += blockDim.x) {
+          const int rr = k / G::TW, cc = k - rr * G::TW;
+          const int y = ty * G::TH + rr, x = tx * G::TW + cc;
+          if (y < P.H && x < P.W) ok = hq_deriv_px(P, y, x) && ok;
+        }
+      } else {
+        ok = hq_sweep_item<RW, RH, T>(P, pass, tile, hq_sm);
+      }
+    }
+    const int bad = __syncthreads_or(!ok);  // also: every store of the item is issued
+    if (threadIdx.x == 0 && bad) atomicOr(status + i, pass == 0 ? OF_ST_NONFINITE_INPUT : OF_ST_NONFINITE_OUTPUT);
+    if (threadIdx.x == 0 && pass < P.passes) {
+      __threadfence();  // release
+      atomicAdd(done + i, 1u);
+    }
+  }
+}
+
+// Pair descriptors travel as kernel parameters (captured by value in a CUDA graph), up to
+// HQ_DESC_CHUNK per launch of this copy kernel.
+constexpr int HQ_DESC_CHUNK = 24;  // 24 x 128 B, within the classic 4 KB of parameters
+struct HsqDescChunk {
+  HsqPair p[HQ_DESC_CHUNK];
+};
+__global__ void hsq_desc_kernel(const __grid_constant__ HsqDescChunk chunk, int n, HsqPair* dst) {
+  const int i = threadIdx.x;
+  if (i < n) dst[i] = chunk.p[i];
+}
+
+}  // namespace ofb
+
+using namespace ofb;
+
+namespace {
+// tile shapes (region width x height, sweeps per pass) the queue kernel is built for
+struct HsqShape {
+  int rw, rh, t;
+};
+constexpr HsqShape kHsqShapes[] = {{64, 40, 4}, {32, 24, 4}, {64, 24, 4}, {32, 32, 8}};
+constexpr int kHsqNumShapes = sizeof(kHsqShapes) / sizeof(kHsqShapes[0]);
+
+template <int RW, int RH, int T>
+cudaError_t hsq_launch(int grid, const HsqPair* pairs, int n, unsigned int tiles_total, int max_passes,
+                       unsigned long long* ticket, unsigned int* done, int* status, long long wait_limit,
+                       int* err_flag, cudaStream_t st) {
+  using G = HqTile<RW, RH, T>;
+  cudaError_t e = OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T>), G::SMEM);
+  if (e != cudaSuccess) return e;
+  hsq_kernel<RW, RH, T><<<grid, 256, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
+                                                     wait_limit, err_flag);
+  return cudaGetLastError();
+}
+
+template <int RW, int RH, int T>
+int hsq_resident(int* per_sm) {
+  using G = HqTile<RW, RH, T>;
+  cudaError_t e = OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T>), G::SMEM);
+  if (e != cudaSuccess) return -1;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, hsq_kernel<RW, RH, T>, 256, G::SMEM);
+  return e == cudaSuccess ? 0 : -1;
+}
+}  // namespace
+
+extern "C" size_t of_hs_batch_workspace_size(const OfHsBatchPair* pairs, int n) {
+  if (!pairs || n <= 0) return 0;
+  Sizer s;
+  s.take<HsqPair>((size_t)n);
+  s.take<unsigned long long>(1);
+  s.take<unsigned int>((size_t)n);
+  s.take<int>(1);
+  for (int i = 0; i < n; i++) {
+    size_t N = (size_t)pairs[i].H * (size_t)pairs[i].pitch;
+    for (int k = 0; k < 7; k++) s.take<float>(N);
+  }
+  return s.off;
+}
+
+extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tuning, int* status,
+                           long long wait_limit, void* workspace, size_t workspace_bytes, void* stream) {
+  OF_REQUIRE(pairs && n > 0 && n <= (1 << 20), "of_hs_batch: bad pair list");
+  OF_REQUIRE(status, "of_hs_batch: status (a device array of n ints) is required");
+  OF_REQUIRE(wait_limit > 0, "of_hs_batch: wait_limit must be positive");
+  int shape = tuning ? tuning->tile_shape : 0;
+  OF_REQUIRE(shape >= 0 && shape < kHsqNumShapes, "of_hs_batch: tile_shape must be in 0..%d", kHsqNumShapes - 1);
+  const HsqShape sh = kHsqShapes[shape];
+  const int TW = sh.rw - 2 * sh.t, TH = sh.rh - 2 * sh.t;
+  size_t need = of_hs_batch_workspace_size(pairs, n);
+  if (!workspace || workspace_bytes < need)
+    return set_error(OF_ERR_WORKSPACE, "of_hs_batch: workspace too small (%zu < %zu)", workspace_bytes, need);
+  cudaStream_t st = as_stream(stream);
+  Carver c(workspace, workspace_bytes);
+  HsqPair* dpairs = c.take<HsqPair>((size_t)n);
+  unsigned long long* ticket = c.take<unsigned long long>(1);
+  unsigned int* done = c.take<unsigned int>((size_t)n);
+  int* err_flag = c.take<int>(1);
+  // descriptors are built on the host and written to the workspace by kernels that take
+  // them as parameters (no host buffer outlives this call, and a graph capture holds copies)
+  HsqPair* hp = new HsqPair[n];
+  unsigned int tiles_total = 0;
+  int max_passes = 0;
+  for (int i = 0; i < n; i++) {
+    const OfHsBatchPair& q = pairs[i];
+    if (bad_plane(q.I0, q.H, q.W, q.pitch) || !q.I1 || !q.U || !q.V || q.niter < 0) {
+      delete[] hp;
+      return set_error(OF_ERR_INVALID, "of_hs_batch: pair %d: bad plane or niter", i);
+    }
+    HsqPair& P = hp[i];
+    P.I0 = q.I0;
+    P.I1 = q.I1;
+    P.U = q.U;
+    P.V = q.V;
+    size_t N = (size_t)q.H * q.pitch;
+    P.fx = c.take<float>(N);
+    P.fy = c.take<float>(N);
+    P.ft = c.take<float>(N);
+    P.U0 = c.take<float>(N);
+    P.V0 = c.take<float>(N);
+    P.Ub = c.take<float>(N);
+    P.Vb = c.take<float>(N);
+    P.H = q.H;
+    P.W = q.W;
+    P.pitch = q.pitch;
+    P.a2 = q.alpha * q.alpha;
+    P.niter = q.niter;
+    P.passes = 1 + (q.niter + sh.t - 1) / sh.t;
+    P.tx = (q.W + TW - 1) / TW;
+    P.tiles = P.tx * ((q.H + TH - 1) / TH);
+    P.tile0 = tiles_total;
+    tiles_total += (unsigned int)P.tiles;
+    if (P.passes > max_passes) max_passes = P.passes;
+  }
+  long long nl = 0;
+  for (int b = 0; b < n; b += HQ_DESC_CHUNK) {
+    HsqDescChunk chunk;
+    const int m = n - b < HQ_DESC_CHUNK ? n - b : HQ_DESC_CHUNK;
+    for (int k = 0; k < m; k++) chunk.p[k] = hp[b + k];
+    hsq_desc_kernel<<<1, HQ_DESC_CHUNK, 0, st>>>(chunk, m, dpairs + b);
+    nl++;
+  }
+  delete[] hp;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: descriptor kernel: %s", cudaGetErrorString(e));
+  // ticket, counters and the error flag are contiguous
+  e = cudaMemsetAsync(ticket, 0, (size_t)((char*)(err_flag + 1) - (char*)ticket), st);
+  if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: %s", cudaGetErrorString(e));
+  int dev = 0, sms = kNumSMs, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int rc;
+  switch (shape) {
+    case 0: rc = hsq_resident<64, 40, 4>(&per_sm); break;
+    case 1: rc = hsq_resident<32, 24, 4>(&per_sm); break;
+    case 2: rc = hsq_resident<64, 24, 4>(&per_sm); break;
+    default: rc = hsq_resident<32, 32, 8>(&per_sm); break;
+  }
+  if (rc != 0 || per_sm < 1) return set_error(OF_ERR_CUDA, "of_hs_batch: occupancy query failed");
+  // every CTA must be resident (items wait for items of running CTAs); no more CTAs than
+  // items of one pass are useful
+  long long grid = (long long)sms * per_sm;
+  if (grid > (long long)tiles_total) grid = tiles_total;
+  if (grid < 1) grid = 1;
+  switch (shape) {
+    case 0: e = hsq_launch<64, 40, 4>((int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    case 1: e = hsq_launch<32, 24, 4>((int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    case 2: e = hsq_launch<64, 24, 4>((int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    default: e = hsq_launch<32, 32, 8>((int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+  }
+  if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: launch: %s", cudaGetErrorString(e));
+  return check_launch("of_hs_batch", nl + 1);
+}
+
+extern "C" int of_hs_batch_shape(int index, int* region_w, int* region_h, int* sweeps_per_pass) {
+  if (index < 0 || index >= kHsqNumShapes) return OF_ERR_INVALID;
+  if (region_w) *region_w = kHsqShapes[index].rw;
+  if (region_h) *region_h = kHsqShapes[index].rh;
+  if (sweeps_per_pass) *sweeps_per_pass = kHsqShapes[index].t;
+  return OF_OK;
+}

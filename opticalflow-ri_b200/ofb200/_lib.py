@@ -21,6 +21,20 @@ class OfError(RuntimeError):
     """A C-ABI entry point returned a negative status."""
 
 
+class OfHsBatchPair(ctypes.Structure):
+    _fields_ = [("I0", ctypes.c_void_p), ("I1", ctypes.c_void_p), ("U", ctypes.c_void_p), ("V", ctypes.c_void_p),
+                ("H", ctypes.c_int), ("W", ctypes.c_int), ("pitch", ctypes.c_int), ("alpha", ctypes.c_float),
+                ("niter", ctypes.c_int)]
+
+
+class OfTuning(ctypes.Structure):
+    _fields_ = [("tile_shape", ctypes.c_int), ("streams", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
+
+
+# per-pair status bits (include/ofb200.h)
+ST_NONFINITE_INPUT, ST_WAIT_TIMEOUT, ST_NOT_CONVERGED, ST_SINGULAR, ST_NONFINITE_OUTPUT = 0x1, 0x2, 0x4, 0x8, 0x10
+
+
 class FbPolyConsts(ctypes.Structure):
     _fields_ = [("polyN", ctypes.c_int), ("g", ctypes.c_float * 8), ("xg", ctypes.c_float * 8),
                 ("xxg", ctypes.c_float * 8), ("ig", ctypes.c_float * 4)]
@@ -61,6 +75,9 @@ _SIGS = {
     "of_ls_solve": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P, _Z, _P], _I),
     "of_ls_solve_noalloc": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P], _I),
     "of_ls_solve_mode": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _I, _P, _P, _P, _Z, _P], _I),
+    "of_hs_batch_shape": ([_I, _P, _P, _P], _I),
+    "of_hs_batch_workspace_size": ([_P, _I], _Z),
+    "of_hs_batch": ([_P, _I, _P, _P, _L, _P, _Z, _P], _I),
     "of_warp_liushen_workspace_size": ([_I, _I], _Z),
     "of_warp_liushen_scatter": ([_P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P, _Z, _P], _I),
     "of_warp_liushen_ofe": ([_P, _P, _P, _P, _I, _I, _I, _P], _I),

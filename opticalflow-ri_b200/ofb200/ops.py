@@ -20,7 +20,7 @@ from ._lib import FbPolyConsts, call, lib
 __all__ = [
     "prefilter", "u8_to_f32", "resize", "spline_upsample", "spline_upsample_pair", "warp_pair", "accumulate", "scale", "hs_solve",
     "ls_solve", "lk_dense", "fb_blur", "fb_box5", "fb_polyexp", "fb_update_matrices", "fb_update_flow",
-    "fb_iteration", "workspace", "stream_ptr", "warp_liushen_scatter", "warp_liushen_ofe",
+    "fb_iteration", "workspace", "stream_ptr", "warp_liushen_scatter", "warp_liushen_ofe", "hs_batch", "hs_batch_shapes",
 ]
 
 _WS = {}
@@ -257,6 +257,43 @@ def ls_solve(I0, I1, U, V, h: float, maxnum: int = 60, tol: float = 1e-8, iters=
          float(np.float32(h)), int(maxnum), float(tol), mode, ctypes.c_void_p(iters.data_ptr()),
          ctypes.c_void_p(err.data_ptr()), ws, wn, stream_ptr())
     return U, V, iters, err
+
+
+def hs_batch_shapes():
+    """The persistent Horn-Schunck kernel's tile shapes: [(region_w, region_h, sweeps_per_pass)]."""
+    out = []
+    i = 0
+    while True:
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        if lib().of_hs_batch_shape(i, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)) != 0:
+            return out
+        out.append((a.value, b.value, c.value))
+        i += 1
+
+
+HS_WAIT_LIMIT = 1 << 24  # polls of a queue wait before a pair is given up (about a second)
+
+
+def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status=None):
+    """Horn-Schunck of many pairs in one persistent launch (of_hs_batch).  pairs: list of
+    (I0, I1, U, V, alpha, niter) with CUDA float32 planes; U, V are updated in place.
+    Returns the per-pair status words (device int32, bits of ofb200._lib.ST_*)."""
+    from ._lib import OfHsBatchPair, OfTuning
+    n = len(pairs)
+    arr = (OfHsBatchPair * n)()
+    dev = pairs[0][0].device
+    for k, (I0, I1, U, V, alpha, niter) in enumerate(pairs):
+        p = _same_pitch(I0, I1, U, V)
+        H, W = I0.shape
+        arr[k] = OfHsBatchPair(I0.data_ptr(), I1.data_ptr(), U.data_ptr(), V.data_ptr(), H, W, p,
+                               float(np.float32(alpha)), int(niter))
+    if status is None:
+        status = torch.zeros(n, dtype=torch.int32, device=dev)
+    tun = OfTuning(int(tile_shape), 0, (ctypes.c_int * 2)(0, 0))
+    ws, wn = workspace(lib().of_hs_batch_workspace_size(arr, n), "hs_batch")
+    call("of_hs_batch", arr, n, ctypes.byref(tun), ctypes.c_void_p(status.data_ptr()), int(wait_limit), ws, wn,
+         stream_ptr())
+    return status
 
 
 # --------------------------------------------------------------------------- A10/A11

@@ -1,0 +1,97 @@
+"""Horn-Schunck in one persistent launch over a device work queue (of_hs_batch).
+
+Bit-exact with the regular solver (of_hs_solve, itself bit-exact with the reference) for
+one pair and for a batch of uneven pairs, with every tile shape; per-pair status words for
+a NaN frame; and the bounded queue wait running out (a short wait limit) ends the launch
+with a timeout status instead of hanging, leaving the context usable."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(torch, H, W, seed):
+    from ofb200 import synthetic as S
+    a, b, _, _ = S.piv_pair(H, W, "poiseuille", seed=seed)
+    return torch.from_numpy(a.astype(np.float32)).cuda(), torch.from_numpy(b.astype(np.float32)).cuda()
+
+
+def _solve_ref(torch, a, b, U0, V0, alpha, niter):
+    from ofb200 import ops
+    U, V = U0.clone(), V0.clone()
+    ops.hs_solve(a, b, U, V, alpha, niter)
+    return U, V
+
+
+@pytest.mark.parametrize("shape_index", [0, 1, 2, 3])
+def test_single_pair_config1_bit_exact(cuda_ok, shape_index):
+    """256 x 256, alpha 21, 600 sweeps (the PyHSchunck_Fs3_4 calibration) in one launch."""
+    import torch
+    from ofb200 import ops
+    a, b = _pair(torch, 256, 256, 1)
+    z = torch.zeros_like(a)
+    Ur, Vr = _solve_ref(torch, a, b, z, z, 21.0, 600)
+    U, V = z.clone(), z.clone()
+    st = ops.hs_batch([(a, b, U, V, 21.0, 600)], tile_shape=shape_index)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    assert torch.equal(U, Ur) and torch.equal(V, Vr)
+
+
+def test_uneven_batch_bit_exact(cuda_ok):
+    import torch
+    from ofb200 import ops
+    shapes = [(128, 128, 600), (256, 256, 600), (64, 200, 37), (512, 384, 120), (17, 23, 9), (16, 16, 0)]
+    pairs, refs = [], []
+    g = torch.Generator().manual_seed(4)
+    for k, (H, W, n) in enumerate(shapes):
+        a, b = _pair(torch, H, W, 10 + k)
+        U0 = (torch.randn(H, W, generator=g) * 0.3).cuda()
+        V0 = (torch.randn(H, W, generator=g) * 0.3).cuda()
+        refs.append(_solve_ref(torch, a, b, U0, V0, 21.0 + k, n))
+        pairs.append((a, b, U0.clone(), V0.clone(), 21.0 + k, n))
+    st = ops.hs_batch(pairs, tile_shape=0)
+    torch.cuda.synchronize()
+    assert st.cpu().tolist() == [0] * len(shapes)
+    for (_, _, U, V, _, _), (Ur, Vr) in zip(pairs, refs):
+        assert torch.equal(U, Ur) and torch.equal(V, Vr)
+
+
+def test_nonfinite_frame_sets_status(cuda_ok):
+    import torch
+    from ofb200 import _lib, ops
+    a, b = _pair(torch, 64, 64, 3)
+    a2, b2 = _pair(torch, 64, 64, 4)
+    b2[10, 20] = float("nan")
+    z = torch.zeros_like(a)
+    pairs = [(a, b, z.clone(), z.clone(), 21.0, 40), (a2, b2, z.clone(), z.clone(), 21.0, 40)]
+    st = ops.hs_batch(pairs).cpu().tolist()
+    assert st[0] == 0
+    assert st[1] & _lib.ST_NONFINITE_INPUT and st[1] & _lib.ST_NONFINITE_OUTPUT
+
+
+def test_bounded_wait_runs_out_and_returns(cuda_ok):
+    """A wait limit of one poll: items that find their previous pass unfinished give up at
+    once.  The launch ends, the failed pairs carry OF_ST_WAIT_TIMEOUT, and the pairs that
+    report no error are bit-exact; afterwards the context works (a normal run follows)."""
+    import torch
+    from ofb200 import _lib, ops
+    pairs, refs = [], []
+    for k in range(4):
+        a, b = _pair(torch, 256, 256, 20 + k)
+        z = torch.zeros_like(a)
+        refs.append(_solve_ref(torch, a, b, z, z, 21.0, 200))
+        pairs.append((a, b, z.clone(), z.clone(), 21.0, 200))
+    st = ops.hs_batch(pairs, wait_limit=1).cpu().tolist()
+    assert any(s & _lib.ST_WAIT_TIMEOUT for s in st)
+    for s, (_, _, U, V, _, _), (Ur, Vr) in zip(st, pairs, refs):
+        assert s in (0, _lib.ST_WAIT_TIMEOUT)
+        if s == 0:
+            assert torch.equal(U, Ur) and torch.equal(V, Vr)
+    for p in pairs:
+        p[2].zero_()
+        p[3].zero_()
+    st = ops.hs_batch(pairs).cpu().tolist()
+    assert st == [0] * 4
+    for (_, _, U, V, _, _), (Ur, Vr) in zip(pairs, refs):
+        assert torch.equal(U, Ur) and torch.equal(V, Vr)
