@@ -171,6 +171,12 @@ typedef struct OfHsBatchPair {
  * derivative pass sets OF_ST_NONFINITE_INPUT for frames with NaN / Inf, the last sweep pass
  * OF_ST_NONFINITE_OUTPUT.  status: DEVICE int[n].  The HS error value is not computed. */
 int of_hs_batch_shape(int index, int* region_w, int* region_h, int* sweeps_per_pass);
+/* Status helpers for batches (no counterpart in the reference, which lets NaN propagate):
+ * of_check_finite ORs `bit` into *status (DEVICE int) when the plane holds NaN or Inf;
+ * of_ls_status ORs OF_ST_NOT_CONVERGED when a Liu-Shen solve's DEVICE sweep count reached
+ * maxnum with its last error above tol (or the solve failed). */
+int of_check_finite(const float* p, int H, int W, int pitch, int* status, int bit, void* stream);
+int of_ls_status(const int* iters, const double* err, int maxnum, double tol, int* status, void* stream);
 size_t of_hs_batch_workspace_size(const OfHsBatchPair* pairs, int n);
 int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tuning, int* status, long long wait_limit,
                 void* workspace, size_t workspace_bytes, void* stream);

@@ -29,7 +29,7 @@ class LiuShenOpticalFlowAlgoAdapter(object):
     def __init__(self, alpha, arithmetic=None):
         self.alpha = alpha
         self.arithmetic = ops.ls_arithmetic(arithmetic)
-        self.last_iterations = None
+        self.last_iterations = self.last_error = None
 
     def compute(self, im1, im2, U, V):
         [resV, resU, error] = physicsBasedOpticalFlowLiuShen(im1, im2, self.alpha, V, U, self.arithmetic)
@@ -40,7 +40,7 @@ class LiuShenOpticalFlowAlgoAdapter(object):
         sweep count of the last call is kept in self.last_iterations (device int32)."""
         U, V = U.clone(), V.clone()
         U, V, it, err = ops.ls_solve(im1, im2, U, V, self.alpha, MAXNUM, TOL, arithmetic=self.arithmetic)
-        self.last_iterations = it
+        self.last_iterations, self.last_error = it, err
         return U, V, err
 
     def _graph_key(self, n):

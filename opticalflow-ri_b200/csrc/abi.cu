@@ -150,3 +150,34 @@ extern "C" int of_scale(const float* src, float* dst, float s, int H, int W, int
   scale_kernel<<<grid, 256, 0, as_stream(stream)>>>(src, dst, s, pitch, W);
   return check_launch("of_scale");
 }
+
+namespace ofb {
+// ORs `bit` into *status when any sample of the plane is NaN or Inf (one atomic per block).
+__global__ void check_finite_kernel(const float* __restrict__ p, int H, int W, int pitch, int* status, int bit) {
+  int bad = 0;
+  for (int y = blockIdx.y; y < H; y += gridDim.y)
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x)
+      bad |= !isfinite(p[(size_t)y * pitch + x]);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(status, bit);
+}
+
+// Liu-Shen convergence: OF_ST_NOT_CONVERGED when the solve ran all `maxnum` sweeps and its
+// last error is still above `tol`, or when it failed (iters < 0).
+__global__ void ls_status_kernel(const int* iters, const double* err, int maxnum, double tol, int* status) {
+  const int k = *iters;
+  if (k < 0 || (k >= maxnum && !(*err <= tol))) atomicOr(status, OF_ST_NOT_CONVERGED);
+}
+}  // namespace ofb
+
+extern "C" int of_check_finite(const float* p, int H, int W, int pitch, int* status, int bit, void* stream) {
+  OF_REQUIRE(!bad_plane(p, H, W, pitch) && status, "of_check_finite: bad plane");
+  dim3 grid((W + 255) / 256 < 4 ? (W + 255) / 256 : 4, H < 64 ? H : 64);
+  check_finite_kernel<<<grid, 256, 0, as_stream(stream)>>>(p, H, W, pitch, status, bit);
+  return check_launch("of_check_finite");
+}
+
+extern "C" int of_ls_status(const int* iters, const double* err, int maxnum, double tol, int* status, void* stream) {
+  OF_REQUIRE(iters && err && status, "of_ls_status: null pointer");
+  ls_status_kernel<<<1, 1, 0, as_stream(stream)>>>(iters, err, maxnum, tol, status);
+  return check_launch("of_ls_status");
+}

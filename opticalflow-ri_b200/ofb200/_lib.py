@@ -76,6 +76,8 @@ _SIGS = {
     "of_ls_solve_noalloc": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P], _I),
     "of_ls_solve_mode": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _I, _P, _P, _P, _Z, _P], _I),
     "of_hs_batch_shape": ([_I, _P, _P, _P], _I),
+    "of_check_finite": ([_P, _I, _I, _I, _P, _I, _P], _I),
+    "of_ls_status": ([_P, _P, _I, _D, _P, _P], _I),
     "of_hs_batch_workspace_size": ([_P, _I], _Z),
     "of_hs_batch": ([_P, _I, _P, _P, _L, _P, _Z, _P], _I),
     "of_warp_liushen_workspace_size": ([_I, _I], _Z),

@@ -11,11 +11,13 @@ them by stream), so concurrent pairs never share scratch memory.
 """
 from __future__ import annotations
 
+import ctypes
 import threading
 from dataclasses import dataclass, field
 
 import torch
 
+from . import _lib
 from . import graph as _graph
 from . import ops
 
@@ -59,10 +61,15 @@ def _cfg_for(spec: PairSpec, main):
 class PairBatch:
     """Runs len(specs) pairs concurrently on `streams` CUDA streams (graph-captured)."""
 
-    def __init__(self, specs, streams=4, use_graph: bool = True):
+    def __init__(self, specs, streams=4, use_graph: bool = True, status: bool = False):
         """streams: a count, or a list of torch.cuda.Stream to share with other batches
-        (their workspaces are shared too: batches sharing streams must not overlap)."""
+        (their workspaces are shared too: batches sharing streams must not overlap).
+        status: also compute per-pair status words (self.status, device int32, bits
+        ofb200._lib.ST_*: non-finite frames, non-finite results, a Liu-Shen refine that
+        used all its sweeps above its tolerance), inside the same graph."""
         self.specs = list(specs)
+        self.want_status = status
+        self.status = None
         if isinstance(streams, (list, tuple)):
             self._streams, self.nstreams = list(streams), len(streams)
         else:
@@ -77,6 +84,10 @@ class PairBatch:
         if self._streams is None:
             self._streams = [torch.cuda.Stream() for _ in range(self.nstreams)]
         outs = [None] * len(frames)
+        if self.want_status:
+            if self.status is None or self.status.numel() != len(frames):
+                self.status = torch.zeros(len(frames), dtype=torch.int32, device=frames[0][0].device)
+            self.status.zero_()
         for s in self._streams:
             s.wait_stream(cur)
         for i, ((a, b), spec) in enumerate(zip(frames, self.specs)):
@@ -86,10 +97,26 @@ class PairBatch:
                 opt = spec.make_opt() if spec.make_opt is not None else None
                 if a.dtype in (torch.uint8, torch.uint16):
                     a, b = ops.u8_to_f32(a), ops.u8_to_f32(b)
+                elif self.want_status:
+                    self._check(a, i, _lib.ST_NONFINITE_INPUT)
+                    self._check(b, i, _lib.ST_NONFINITE_INPUT)
                 outs[i] = G._pyramid_dev(a, b, _cfg_for(spec, main), main, opt)
+                if self.want_status:
+                    self._check(outs[i][0], i, _lib.ST_NONFINITE_OUTPUT)
+                    self._check(outs[i][1], i, _lib.ST_NONFINITE_OUTPUT)
+                    if getattr(opt, "last_iterations", None) is not None:
+                        import PhysicsBasedOpticalFlowLiuShen as LS
+                        _lib.call("of_ls_status", ctypes.c_void_p(opt.last_iterations.data_ptr()),
+                                  ctypes.c_void_p(opt.last_error.data_ptr()), LS.MAXNUM, LS.TOL,
+                                  ctypes.c_void_p(self.status[i:].data_ptr()), ops.stream_ptr())
         for s in self._streams:
             cur.wait_stream(s)
         return outs
+
+    def _check(self, t, i, bit):
+        H, W = t.shape
+        _lib.call("of_check_finite", ctypes.c_void_p(t.data_ptr()), H, W, t.stride(0),
+                  ctypes.c_void_p(self.status[i:].data_ptr()), bit, ops.stream_ptr())
 
     def run(self, frames):
         """frames: list of (frame1, frame2) CUDA tensors (uint8 or float32) matching specs.

@@ -137,3 +137,33 @@ def test_u16_frames_convert_on_device(torch_cuda):
     a = np.random.default_rng(3).integers(0, 4096, (33, 70)).astype(np.uint16)
     got = ops.u8_to_f32(torch.from_numpy(a).cuda())
     assert np.array_equal(got.cpu().numpy(), a.astype(np.float32))
+
+
+def test_batch_status_words(cuda_ok):
+    """Per-pair status words inside the batch graph: a host-injected NaN frame is reported
+    (input and the NaN-polluted result), not a crash; clean pairs report only the Liu-Shen
+    refine's use of all its sweeps (when the reference's tolerance 1e-8 is not reached), and the
+    NaN pair does not disturb the other pairs' results."""
+    import torch
+    import Farneback_PyCL as FB
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    from ofb200 import _lib, ops, synthetic as S
+    from ofb200.batch import PairBatch, PairSpec
+    frames = []
+    for s in range(3):
+        a, b, _, _ = S.config_pair("fbls1024", seed=50 + s, size=128)
+        frames.append((ops.u8_to_f32(torch.from_numpy(a).cuda()), ops.u8_to_f32(torch.from_numpy(b).cuda())))
+    spec = PairSpec(0, lambda: FB.Farneback_PyCL(), 2, 1, 0.48, lambda: LS.LiuShenOpticalFlowAlgoAdapter(10),
+                    key=("fbls-status",))
+    clean = PairBatch([spec] * 3, streams=3).run([(a.clone(), b.clone()) for a, b in frames])
+    clean = [(U.clone(), V.clone()) for U, V in clean]
+    bad = [(a.clone(), b.clone()) for a, b in frames]
+    bad[1][1][40, 50] = float("nan")
+    pb = PairBatch([spec] * 3, streams=3, status=True)
+    for _ in range(2):  # eager capture run, then a graph replay
+        out = pb.run(bad)
+        st = pb.status.cpu().tolist()
+        assert st[1] & _lib.ST_NONFINITE_INPUT and st[1] & _lib.ST_NONFINITE_OUTPUT
+        for k in (0, 2):
+            assert st[k] & ~_lib.ST_NOT_CONVERGED == 0
+            assert torch.equal(out[k][0], clean[k][0]) and torch.equal(out[k][1], clean[k][1])
