@@ -477,7 +477,7 @@ class LearnedBatch:
         thr = self.ll.threshold
         if thr is None:
             return list(res), 0
-        bad = (errs > thr).nonzero().flatten().tolist()
+        bad = (~(errs <= thr)).nonzero().flatten().tolist()  # NaN norms fall back too
         out = list(res)
         for i in bad:
             A, B = _as_f32(frames[i][0]), _as_f32(frames[i][1])

@@ -80,3 +80,31 @@ def test_trained_start_gain(torch_cuda, trained):
     net.check()
     assert np.mean(e_learned) <= np.mean(e_plain), (e_learned, e_plain)
     assert np.mean(e_learned) < 0.5 * np.mean(e_zero), (e_learned, e_zero)
+
+
+def test_fallback_returns_the_plain_pyramid(torch_cuda, trained):
+    """A pair the network cannot start well (two unrelated frames: no displacement explains
+    the second) ends its reduced Liu-Shen stage with an update norm above the calibrated
+    threshold; fallback() then recomputes it with the plain pyramid, whose result is what
+    comes back, while an ordinary pair of the same batch keeps its learned result."""
+    torch = torch_cuda
+    import Farneback_PyCL as F
+    import GenericPyramidalOpticalFlow as G
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    from ofb200 import synthetic as S
+    from ofb200.warmstart import LearnedBatch
+    net, meta = trained
+    a, b, _, _ = S.config_pair("fbls1024", seed=HELD_OUT[0])
+    c, _, _, _ = S.config_pair("fbls1024", seed=HELD_OUT[1] + 77)
+    frames = [(_f32(torch, a), _f32(torch, b)), (_f32(torch, a), _f32(torch, c))]
+    lb = LearnedBatch(net, meta, 2, size=1024, streams=2)
+    res, errs = lb.run(frames)
+    e = errs.cpu().tolist()
+    assert e[0] <= meta["threshold"] and not e[1] <= meta["threshold"], e
+    learned0 = (res[0][0].clone(), res[0][1].clone())
+    out, nfb = lb.fallback(frames, res, errs.cpu())
+    assert nfb == 1
+    Up, Vp = G.genericPyramidalOpticalFlow(frames[1][0], frames[1][1], 0, F.Farneback_PyCL(), 2, 1, 0.48,
+                                           LS.LiuShenOpticalFlowAlgoAdapter(10))
+    assert torch.equal(out[1][0], Up) and torch.equal(out[1][1], Vp)
+    assert torch.equal(out[0][0], learned0[0]) and torch.equal(out[0][1], learned0[1])
