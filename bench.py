@@ -68,6 +68,8 @@ def parse():
     p.add_argument("--no-configs", action="store_true", help="skip the HS 256^2 / LK 512^2 / batch workloads")
     p.add_argument("--no-batch", action="store_true", help="skip the 256-pair batch inside the configs block")
     p.add_argument("--learned-weights", default=None, help="weights + calibration .npz (default: packaged)")
+    p.add_argument("--learned-pairs", type=int, default=64, help="pairs per step of the learned arm (batch)")
+    p.add_argument("--epe-pairs", type=int, default=32, help="distinct held-out pairs for the endpoint errors")
     p.add_argument("--batch-pairs", type=int, default=256, help="--mode batch: pairs in the manifest")
     p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn", "fb", "e2e"],
                    help="ls: only the Liu-Shen solve of one pair, --steps times (for profiling)")
@@ -594,27 +596,43 @@ def run_batch_inline(args, rank, world, dev, flush):
             "autotuned": {f"{c}x{s}": round(v, 2) for (c, s), v in table.items()}}
 
 
+def _render_eval(seed):
+    from ofb200 import synthetic as S
+    return S.config_pair("fbls1024", seed=seed)
+
+
 def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
-    """The learned warm start on the same frames: one network forward over the step's
-    pairs (at the network's level), Farneback at full size from that start, then the calibrated number
-    of Liu-Shen sweeps; pairs whose last update norm exceeds the calibrated threshold are
-    recomputed by the plain pyramid inside the timed region.  Endpoint errors of both arms
-    against the analytic ground truth (16 px interior) on the distinct pairs."""
+    """The learned warm start (config 5: batch --learned-pairs at 1024^2): one network
+    forward over the step's pairs (at the network's level), Farneback at full size from that
+    start, then the calibrated number of Liu-Shen sweeps; pairs whose last update norm exceeds
+    the calibrated threshold are recomputed by the plain pyramid inside the timed region.
+    The step's frames are --epe-pairs distinct held-out pairs (seeds outside the training and
+    calibration sets), cycled; the endpoint errors of all arms against the analytic ground
+    truth (16 px interior) are taken over those distinct pairs."""
+    import multiprocessing as mp
     import torch
     import torch.distributed as dist
     from ofb200 import ops, synthetic as S
     from ofb200.warmstart import LearnedBatch, load_trained
     net, meta = load_trained(**({"path": args.learned_weights} if args.learned_weights else {}), device=dev)
-    nu = min(len(pairs), args.pairs)
+    seeds = [960_000 + 1000 * (dist.get_rank() if world > 1 else 0) + i for i in range(args.epe_pairs)]
+    with mp.get_context("spawn").Pool(min(16, max(1, (os.cpu_count() or 2) // 2))) as pool:
+        evals = pool.map(_render_eval, seeds)
+    eval_frames = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _, _ in evals]
+    nb = args.learned_pairs
+    lframes = [eval_frames[i % len(eval_frames)] for i in range(nb)]
+    nu = min(len(eval_frames), nb)
     plain_value = args.pairs * args.steps * world / (pairs_total_ms * 1e-3)
     epe_p = []
     for i in range(nu):
-        a, b, Ug, Vg = pairs[i]
-        Up, Vp = pipeline_dev(ops.u8_to_f32(step_frames[i][0]), ops.u8_to_f32(step_frames[i][1]))
+        a, b, Ug, Vg = evals[i]
+        Up, Vp = pipeline_dev(ops.u8_to_f32(lframes[i][0]), ops.u8_to_f32(lframes[i][1]))
         epe_p.append(S.epe(Up.cpu().numpy(), Vp.cpu().numpy(), Ug, Vg, crop=16))
+    step_frames = lframes
+    pairs = evals
 
     def arm(start):
-        lb = LearnedBatch(net, meta, args.pairs, args.size, streams=args.streams, start=start)
+        lb = LearnedBatch(net, meta, nb, args.size, streams=args.streams, start=start)
 
         def step():
             res, errs = lb.run(step_frames)  # uint8 frames, converted inside the graph
@@ -645,7 +663,7 @@ def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
         out, _ = step()  # accuracy on the distinct pairs, outside the timed region
         epe = [S.epe(out[i][0].cpu().numpy(), out[i][1].cpu().numpy(), pairs[i][2], pairs[i][3], crop=16)
                for i in range(nu)]
-        value = args.pairs * args.steps * world / (total_ms * 1e-3)
+        value = nb * args.steps * world / (total_ms * 1e-3)
         ll = lb.ll
         return {"value": value, "unit": "pairs/s", "ms_per_step": total_ms / args.steps,
                 "speedup_vs_plain": value / plain_value, "fb_iters": ll.fb_iters if ll.mode == "fb" else 0,
@@ -655,7 +673,7 @@ def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
     ablation = arm("zero")
     net.check()
     learned.update({"mode": meta["mode"], "threshold": meta["threshold"], "epe_plain": float(np.mean(epe_p)),
-                    "epe_pairs": nu, "epe_crop_px": 16,
+                    "epe_pairs": nu, "epe_crop_px": 16, "pairs_per_step": nb,
                     "network": f"encoder-decoder CNN at the {meta.get('level', 512)}^2 level, 1.75M params, bf16 tcgen05 convs, "
                                "f32 accumulate",
                     "trained": {k: meta[k] for k in ("train_pairs", "steps", "batch", "crop", "level", "eval_pairs")},
