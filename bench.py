@@ -560,6 +560,11 @@ def run_configs(args, rank, world, dev, flush):
     return out
 
 
+def _cand(k):
+    """Autotune table key -> label: ('hs_shape', i) -> 'hs_shape_i', (chunk, streams) -> 'CxS'."""
+    return f"hs_shape_{k[1]}" if k[0] == "hs_shape" else f"{k[0]}x{k[1]}"
+
+
 def run_batch_inline(args, rank, world, dev, flush):
     """Config 4 inside the default bench: the seeded 256-pair manifest, autotuned over a
     short candidate list, one timed pass (device events, L2 flushed before it)."""
@@ -589,11 +594,13 @@ def run_batch_inline(args, rank, world, dev, flush):
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
     t = max_over_ranks(float(np.mean(ms)), dev)
+    runner_key, hs_shape = runner.key, runner.hs_shape
     del runner
     return {"workload": f"{len(manifest)} pairs, sizes 128^2-2048^2, HS / LK pyr2 / FB pyr2 / FB pyr2 + LS, "
                         "Poiseuille / Lamb-Oseen / random-Fourier, max 4 px",
             "value": len(manifest) / (t * 1e-3), "unit": "pairs/s", "ms_per_pass": t, "scaling": "strong",
-            "autotuned": {f"{c}x{s}": round(v, 2) for (c, s), v in table.items()}}
+            "autotuned": {"chunk": runner_key[0], "streams": runner_key[1], "hs_tile_shape": hs_shape,
+                          "candidates_ms": {_cand(k): round(v, 2) for k, v in table.items()}}}
 
 
 def _render_eval(seed):
@@ -744,8 +751,8 @@ def run_batch(args, rank, world, local_rank):
             "config": {"workload": f"{len(manifest)} pairs, sizes 128^2-2048^2, HS / LK pyr2 / FB pyr2 / FB pyr2 + LS, "
                                    "Poiseuille / Lamb-Oseen / random-Fourier, max 4 px",
                        "l2": "flushed between steps (256 MB write)", "parallelism": f"pairs sharded by cost over {world}",
-                       "autotuned": {"chunk": runner.key[0], "streams": runner.key[1],
-                                     "candidates_ms": {f"{c}x{s}": round(v, 2) for (c, s), v in table.items()}}},
+                       "autotuned": {"chunk": runner.key[0], "streams": runner.key[1], "hs_tile_shape": runner.hs_shape,
+                                     "candidates_ms": {_cand(k): round(v, 2) for k, v in table.items()}}},
             "clocks": clk, "epe_interior": epe}
 
 

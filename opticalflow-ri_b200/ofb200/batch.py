@@ -21,8 +21,8 @@ from . import _lib
 from . import graph as _graph
 from . import ops
 
-__all__ = ["PairSpec", "PairBatch", "method_spec", "config4_manifest", "render_entry", "pair_cost_of", "BatchRunner",
-           "autotune"]
+__all__ = ["PairSpec", "PairBatch", "HsGroup", "method_spec", "config4_manifest", "render_entry", "pair_cost_of",
+           "BatchRunner", "autotune", "tune_hs_shape"]
 
 
 @dataclass
@@ -202,16 +202,74 @@ def render_entry(e):
     return S.piv_pair(n, n, e["flow"], e["seed"], density=density, diameter=diameter, noise=2.0, **kw)
 
 
+class HsGroup:
+    """The Horn-Schunck pairs of a batch (one pyramid level, as method_spec("hs") sets them
+    up: prefilter, then the solve) with every solve in ONE persistent launch (of_hs_batch,
+    bit-exact with the per-pair path).  The prefilters, the launch and the accumulation into
+    the result are captured into one CUDA graph on the first run."""
+
+    def __init__(self, specs, tile_shape=0):
+        self.specs, self.tile_shape = list(specs), int(tile_shape)
+        for sp in self.specs:
+            if sp.pyramidalLevels != 1 or sp.kLevels != 1 or sp.make_opt is not None:
+                raise ValueError("HsGroup takes single-level Horn-Schunck pairs")
+        self._graph = None
+        self.status = None
+
+    def _pipelines(self, frames):
+        from gaussian_filter import prepareGaussianKernel
+        pairs, outs = [], []
+        for (a, b), sp in zip(frames, self.specs):
+            hs = sp.make_main()
+            if a.dtype in (torch.uint8, torch.uint16):
+                a, b = ops.u8_to_f32(a), ops.u8_to_f32(b)
+            if sp.FILTER > 1e-3:
+                taps = prepareGaussianKernel(sp.FILTER, 3)
+                a, b = ops.prefilter(a, taps), ops.prefilter(b, taps)
+            U, V = torch.zeros_like(a), torch.zeros_like(a)
+            pairs.append((a, b, U, V, hs.alphas[-1], hs.Niter))
+            outs.append((U, V))
+        self.status = ops.hs_batch(pairs, tile_shape=self.tile_shape)
+        # the driver's Uaccum = 0 + U (the sign of a zero result is the accumulation's)
+        return [(ops.accumulate(torch.zeros_like(U), U), ops.accumulate(torch.zeros_like(V), V)) for U, V in outs]
+
+    def run(self, frames):
+        if not _graph.ENABLED:
+            return self._pipelines(frames)
+        if self._graph is None:
+            static_in = [(a.clone(), b.clone()) for a, b in frames]
+            self._pipelines(static_in)
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.graph(g, stream=side):
+                static_out = self._pipelines(static_in)
+            self._graph = (g, static_in, static_out)
+        g, static_in, static_out = self._graph
+        torch._foreach_copy_([t for p in static_in for t in p], [t for p in frames for t in p])
+        g.replay()
+        _graph._replayed_kernels += 1
+        return static_out
+
+
 class BatchRunner:
     """A manifest in chunks of `chunk` pairs, ordered by decreasing cost, each chunk one
-    multi-stream CUDA graph (PairBatch) on `streams` shared streams.  run() replays the
-    chunks in turn and returns every pair's (U, V) in manifest order."""
+    multi-stream CUDA graph (PairBatch) on `streams` shared streams.  With hs_shape set,
+    the Horn-Schunck pairs leave the chunks and run as one persistent launch (HsGroup with
+    that tile shape) on a stream of their own, overlapping the chunks.  run() returns every
+    pair's (U, V) in manifest order."""
 
-    def __init__(self, entries, chunk=32, streams=4):
+    def __init__(self, entries, chunk=32, streams=4, hs_shape=None):
         self.entries = list(entries)
-        self.order = sorted(range(len(self.entries)), key=lambda i: (-pair_cost_of(self.entries[i]), i))
+        self.hs_shape = hs_shape
+        hs_idx = [i for i, e in enumerate(self.entries) if e["method"] == "hs"] if hs_shape is not None else []
+        rest = [i for i in range(len(self.entries)) if i not in set(hs_idx)]
+        self.order = sorted(rest, key=lambda i: (-pair_cost_of(self.entries[i]), i))
         self.chunk, self.nstreams = int(chunk), int(streams)
         self._streams = [torch.cuda.Stream() for _ in range(self.nstreams)]
+        self._hs = (hs_idx, HsGroup([method_spec("hs") for _ in hs_idx], hs_shape)) if hs_idx else None
+        self._hs_stream = torch.cuda.Stream() if hs_idx else None
         self._batches = []
         for c in range(0, len(self.order), self.chunk):
             idx = self.order[c:c + self.chunk]
@@ -220,31 +278,97 @@ class BatchRunner:
 
     def run(self, frames):
         outs = [None] * len(self.entries)
+        cur = torch.cuda.current_stream()
+        if self._hs is not None:
+            idx, grp = self._hs
+            self._hs_stream.wait_stream(cur)
+            with torch.cuda.stream(self._hs_stream):
+                res = grp.run([frames[i] for i in idx])
+            for i, r in zip(idx, res):
+                outs[i] = r
         for idx, pb in self._batches:
             res = pb.run([frames[i] for i in idx])
             for i, r in zip(idx, res):
                 outs[i] = r
+        if self._hs is not None:
+            cur.wait_stream(self._hs_stream)
         return outs
 
 
-def autotune(entries, frames, chunks=(16, 64, 256), streams=(2, 4, 8), reps=2, log=None):
+def _time_runner(r, frames, reps):
+    r.run(frames)  # capture
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        r.run(frames)
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _cache_path():
+    import os
+    return os.environ.get("OFB_AUTOTUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "ofb200",
+                                                             "autotune.json"))
+
+
+def tune_hs_shape(frames_hs, reps=2, log=None, use_cache=True):
+    """The persistent Horn-Schunck kernel's tile shape (region and sweeps per pass) for a set
+    of Horn-Schunck pairs: every shape of ops.hs_batch_shapes() timed on them; the choice is
+    cached per (GPU, method, sizes) in a JSON file (OFB_AUTOTUNE_CACHE, default
+    ~/.cache/ofb200/autotune.json).  Returns (shape index, {shape: ms})."""
+    import json
+    import os
+    key = "|".join([torch.cuda.get_device_name(), "hs", ",".join(sorted(f"{a.shape[0]}x{a.shape[1]}"
+                                                                         for a, _ in frames_hs))])
+    path = _cache_path()
+    cache = {}
+    if use_cache and os.path.exists(path):
+        try:
+            with open(path) as f:
+                cache = json.load(f)
+        except (OSError, ValueError):
+            cache = {}
+    if key in cache:
+        return int(cache[key]["shape"]), {int(k): v for k, v in cache[key]["ms"].items()}
+    specs = [method_spec("hs") for _ in frames_hs]
+    table = {}
+    for k in range(len(ops.hs_batch_shapes())):
+        g = HsGroup(specs, tile_shape=k)
+        table[k] = _time_runner(g, frames_hs, reps)
+        if log:
+            log(f"hs tile shape {k} {ops.hs_batch_shapes()[k]}: {table[k]:.2f} ms")
+        del g
+    best = min(table, key=table.get)
+    if use_cache:
+        cache[key] = {"shape": best, "ms": table}
+        try:
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            with open(path, "w") as f:
+                json.dump(cache, f, indent=1)
+        except OSError:
+            pass
+    return best, table
+
+
+def autotune(entries, frames, chunks=(16, 64, 256), streams=(2, 4, 8), reps=2, log=None, hs_persistent=True):
     """Times every (chunk, streams) candidate on the manifest (after its capture run) and
-    returns (best runner, {candidate: ms})."""
+    returns (best runner, {candidate: ms}).  With hs_persistent, the Horn-Schunck pairs run
+    in one persistent launch whose tile shape is tuned first (tune_hs_shape)."""
     import gc
     best, table = None, {}
+    hs_shape = None
+    if hs_persistent:
+        hs = [frames[i] for i, e in enumerate(entries) if e["method"] == "hs"]
+        if hs:
+            hs_shape, hs_table = tune_hs_shape(hs, reps=reps, log=log)
+            table.update({("hs_shape", k): v for k, v in hs_table.items()})
     for c in chunks:
         for s in streams:
-            r = BatchRunner(entries, chunk=min(c, len(entries)), streams=s)
+            r = BatchRunner(entries, chunk=min(c, len(entries)), streams=s, hs_shape=hs_shape)
             r.key = (c, s)
-            r.run(frames)  # capture
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(reps):
-                r.run(frames)
-            e1.record()
-            e1.synchronize()
-            ms = e0.elapsed_time(e1) / reps
+            ms = _time_runner(r, frames, reps)
             table[(c, s)] = ms
             if log:
                 log(f"chunk {c} streams {s}: {ms:.1f} ms")

@@ -95,3 +95,21 @@ def test_bounded_wait_runs_out_and_returns(cuda_ok):
     assert st == [0] * 4
     for (_, _, U, V, _, _), (Ur, Vr) in zip(pairs, refs):
         assert torch.equal(U, Ur) and torch.equal(V, Vr)
+
+
+def test_batch_runner_hs_group_equals_per_pair_graphs(cuda_ok):
+    """The batched workload with its Horn-Schunck pairs in one persistent launch gives the
+    same fields as with every pair in its own per-pair pipeline."""
+    import torch
+    from ofb200.batch import BatchRunner, config4_manifest, render_entry
+    entries = [e for e in config4_manifest(40, seed=3) if e["size"] <= 512][:12]
+    assert any(e["method"] == "hs" for e in entries)
+    frames = []
+    for e in entries:
+        a, b, _, _ = render_entry(e)
+        frames.append((torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()))
+    ref = [(U.clone(), V.clone()) for U, V in BatchRunner(entries, chunk=8, streams=4).run(frames)]
+    for shape in (0, 1):
+        got = BatchRunner(entries, chunk=8, streams=4, hs_shape=shape).run(frames)
+        for (U, V), (Ur, Vr) in zip(got, ref):
+            assert torch.equal(U, Ur) and torch.equal(V, Vr)
