@@ -20,6 +20,11 @@ namespace ofb {
 constexpr int LK_PT = 8;            // pixel tile edge
 constexpr int LK_G = LK_PT + 31;    // gradient positions per axis
 constexpr int LK_I = LK_G + 2;      // intensity positions per axis
+// J region staged per CTA for the Newton steps: LK_JR x LK_JR texels centred on the tile's
+// mean displaced window, row stride LK_JP (72: the 4 rows a warp reads at once fall in
+// distinct banks).  Texels hold clamped-coordinate values, so a bilinear footprint inside
+// the region reads exactly what the clamped global path reads.
+constexpr int LK_JR = 64, LK_JP = 72;
 
 struct LkParams {
   int ws, hw, aL, aR, aT, aB, niter;
@@ -61,6 +66,38 @@ __device__ __forceinline__ float lk_bilinear(const float* __restrict__ J, int H,
   return r;
 }
 
+// The same bilinear sample from the staged region when its 2 x 2 footprint lies inside it
+// (rx, ry: footprint origin relative to the region), else from global memory.
+__device__ __forceinline__ float lk_bilinear_s(const float* __restrict__ sJ, const float* __restrict__ J, int H, int W,
+                                               int pitch, float x, float y, int ox, int oy) {
+  float xs = __fsub_rn(x, 0.5f), ys = __fsub_rn(y, 0.5f);
+  float fx0 = floorf(xs), fy0 = floorf(ys);
+  float a = __fsub_rn(xs, fx0), b = __fsub_rn(ys, fy0);
+  int i0 = (int)fx0, j0 = (int)fy0;
+  const int rx = i0 - ox, ry = j0 - oy;
+  float t00, t10, t01, t11;
+  if ((unsigned)rx <= (unsigned)(LK_JR - 2) && (unsigned)ry <= (unsigned)(LK_JR - 2)) {
+    const float* q = sJ + ry * LK_JP + rx;
+    t00 = q[0];
+    t10 = q[1];
+    t01 = q[LK_JP];
+    t11 = q[LK_JP + 1];
+  } else {
+    int xa = clampi(i0, 0, W - 1), xb = clampi(i0 + 1, 0, W - 1);
+    int ya = clampi(j0, 0, H - 1), yb = clampi(j0 + 1, 0, H - 1);
+    t00 = __ldg(J + (size_t)ya * pitch + xa);
+    t10 = __ldg(J + (size_t)ya * pitch + xb);
+    t01 = __ldg(J + (size_t)yb * pitch + xa);
+    t11 = __ldg(J + (size_t)yb * pitch + xb);
+  }
+  float oa = __fsub_rn(1.f, a), ob = __fsub_rn(1.f, b);
+  float r = __fmul_rn(__fmul_rn(oa, ob), t00);
+  r = __fmaf_rn(__fmul_rn(a, ob), t10, r);
+  r = __fmaf_rn(__fmul_rn(oa, b), t01, r);
+  r = __fmaf_rn(__fmul_rn(a, b), t11, r);
+  return r;
+}
+
 // the reference's reduce tree: (t, t+32) in-lane, then 16, 8, 4, (0+1)+(2+3)
 __device__ __forceinline__ float lk_tree(float lo, float hi) {
   float q = __fadd_rn(lo, hi);
@@ -94,6 +131,34 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
     sDy[t] = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(1, -1), P(1, 1)), P(-1, -1)), P(-1, 1)), 3.0f,
                        __fmul_rn(__fsub_rn(P(1, 0), P(-1, 0)), 10.0f));
 #undef P
+  }
+  // J region: centred on the tile centre displaced by the mean initial flow of the tile
+  __shared__ float sJ[LK_JR * LK_JP];
+  __shared__ float red_u[8], red_v[8];
+  {
+    float su = 0.f, sv = 0.f;
+    if (threadIdx.x < LK_PT * LK_PT) {
+      const int yy = min(i0 + (int)(threadIdx.x >> 3), H - 1), xx = min(j0 + (int)(threadIdx.x & 7), W - 1);
+      su = U[(size_t)yy * pitch + xx];
+      sv = V[(size_t)yy * pitch + xx];
+      su = isfinite(su) ? fminf(fmaxf(su, -1e6f), 1e6f) : 0.f;
+      sv = isfinite(sv) ? fminf(fmaxf(sv, -1e6f), 1e6f) : 0.f;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      su += __shfl_down_sync(0xffffffffu, su, o);
+      sv += __shfl_down_sync(0xffffffffu, sv, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      red_u[threadIdx.x >> 5] = su;
+      red_v[threadIdx.x >> 5] = sv;
+    }
+  }
+  __syncthreads();
+  const float mu = (red_u[0] + red_u[1]) * (1.f / 64.f), mv = (red_v[0] + red_v[1]) * (1.f / 64.f);
+  const int jox = j0 + LK_PT / 2 + (int)floorf(mu) - LK_JR / 2, joy = i0 + LK_PT / 2 + (int)floorf(mv) - LK_JR / 2;
+  for (int t = threadIdx.x; t < LK_JR * LK_JR; t += blockDim.x) {
+    const int ly = t / LK_JR, lx = t - ly * LK_JR;
+    sJ[ly * LK_JP + lx] = __ldg(J + (size_t)clampi(joy + ly, 0, H - 1) * pitch + clampi(jox + lx, 0, W - 1));
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -171,7 +236,7 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
             if (w == 0.f) continue;
             int g = (gyb + ty * 8 + yy) * LK_G + gxb + tx * 8 + xid;
             float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_I + gxb + tx * 8 + xid + 1];
-            float Jv = lk_bilinear(J, H, W, pitch, lx[tx], ly[v][ty]);
+            float Jv = lk_bilinear_s(sJ, J, H, W, pitch, lx[tx], ly[v][ty], jox, joy);
             float diff = __fmul_rn(__fsub_rn(Jv, Iv), w);
             b1[v] = __fmaf_rn(diff, __fmul_rn(sDx[g], w), b1[v]);
             b2[v] = __fmaf_rn(diff, __fmul_rn(sDy[g], w), b2[v]);
@@ -209,7 +274,7 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
           if ((gb & 8) && !(by[1] < p.ws)) continue;
           float w = __fmul_rn(wx[tx], wy[ty]);
           float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_I + gxb + tx * 8 + xid + 1];
-          float Jv = lk_bilinear(J, H, W, pitch, lx[tx], ly[v][ty]);
+          float Jv = lk_bilinear_s(sJ, J, H, W, pitch, lx[tx], ly[v][ty], jox, joy);
           float d = __fmul_rn(__fsub_rn(__fdiv_rn(__fmaf_rn(Jv, 16384.f, 256.f), 512.f),
                                         __fdiv_rn(__fmaf_rn(Iv, 16384.f, 256.f), 512.f)),
                               w);
