@@ -187,7 +187,9 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
           float w = __fmul_rn(wx[tx], wy[ty]);
           if (w == 0.f) continue;
           int g = (gyb + ty * 8 + yy) * LK_G + gxb + tx * 8 + xid;
-          float dx = __fmul_rn(sDx[g], w), dy = __fmul_rn(sDy[g], w);
+          // w is 1 here (the tile weights are products of 0 / 1 values and w == 0 is
+          // skipped), so the reference's multiplications by w are exact identities
+          float dx = sDx[g], dy = sDy[g];
           a11[v] = __fmaf_rn(dx, dx, a11[v]);
           a12[v] = __fmaf_rn(dx, dy, a12[v]);
           a22[v] = __fmaf_rn(dy, dy, a22[v]);
@@ -237,9 +239,9 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
             int g = (gyb + ty * 8 + yy) * LK_G + gxb + tx * 8 + xid;
             float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_I + gxb + tx * 8 + xid + 1];
             float Jv = lk_bilinear_s(sJ, J, H, W, pitch, lx[tx], ly[v][ty], jox, joy);
-            float diff = __fmul_rn(__fsub_rn(Jv, Iv), w);
-            b1[v] = __fmaf_rn(diff, __fmul_rn(sDx[g], w), b1[v]);
-            b2[v] = __fmaf_rn(diff, __fmul_rn(sDy[g], w), b2[v]);
+            float diff = __fsub_rn(Jv, Iv);  // (Jv - Iv) * w with w == 1
+            b1[v] = __fmaf_rn(diff, sDx[g], b1[v]);
+            b2[v] = __fmaf_rn(diff, sDy[g], b2[v]);
           }
       }
       float B1 = lk_tree(b1[0], b1[1]), B2 = lk_tree(b2[0], b2[1]);
@@ -308,6 +310,9 @@ extern "C" int of_lk_dense(const float* I, const float* J, float* U, float* V, i
   p.aR = asym ? asym[1] : 0;
   p.aT = asym ? asym[2] : 0;
   p.aB = asym ? asym[3] : 0;
+  // the reference's window masks are 0 / 1 (denseLucasKanade_PyCL.py:75-92); the kernel's
+  // tile weights rely on it
+  OF_REQUIRE(((p.aL | p.aR | p.aT | p.aB) & ~1) == 0, "of_lk_dense: asym entries must be 0 or 1");
   p.niter = niter;
   dim3 grid((W + LK_PT - 1) / LK_PT, (H + LK_PT - 1) / LK_PT);
   lk_dense_kernel<<<grid, 256, 0, as_stream(stream)>>>(I, J, U, V, H, W, pitch, p, status, err);
