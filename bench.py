@@ -71,7 +71,7 @@ def parse():
     p.add_argument("--learned-pairs", type=int, default=64, help="pairs per step of the learned arm (batch)")
     p.add_argument("--epe-pairs", type=int, default=32, help="distinct held-out pairs for the endpoint errors")
     p.add_argument("--batch-pairs", type=int, default=256, help="--mode batch: pairs in the manifest")
-    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn", "fb", "e2e"],
+    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn", "fb", "e2e", "hs", "lk"],
                    help="ls: only the Liu-Shen solve of one pair, --steps times (for profiling)")
     return p.parse_args()
 
@@ -96,6 +96,75 @@ def run_ls_only(args):
         if r >= args.warmup:
             ms.append(e0.elapsed_time(e1))
     print(json.dumps({"mode": "ls", "size": args.size, "sweeps": int(it.item()), "ms": float(np.mean(ms))}))
+
+
+def run_hs_only(args):
+    """Horn-Schunck, 600 sweeps at --size: the multi-launch solver (of_hs_solve) against the
+    persistent one-launch solver (of_hs_batch) with every tile shape, one pair; CUDA events."""
+    import torch
+    from ofb200 import ops, synthetic as S
+    a8, b8, _, _ = S.config_pair("hs256", seed=1, size=args.size)
+    a = torch.from_numpy(a8.astype(np.float32)).cuda()
+    b = torch.from_numpy(b8.astype(np.float32)).cuda()
+    z = torch.zeros_like(a)
+
+    def timeit(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    out = {"mode": "hs", "size": args.size, "sweeps": 600}
+    U, V = z.clone(), z.clone()
+    out["of_hs_solve_ms"] = timeit(lambda: ops.hs_solve(a, b, U.zero_(), V.zero_(), 21.0, 600))
+    for k, shp in enumerate(ops.hs_batch_shapes()):
+        U2, V2 = z.clone(), z.clone()
+        out[f"of_hs_batch_shape{k}_{shp[0]}x{shp[1]}t{shp[2]}_ms"] = timeit(
+            lambda: ops.hs_batch([(a, b, U2.zero_(), V2.zero_(), 21.0, 600)], tile_shape=k))
+        out[f"shape{k}_equal"] = bool(torch.equal(U2, U) and torch.equal(V2, V))
+    print(json.dumps(out))
+
+
+def run_lk_only(args):
+    """Dense LK (27 x 27 window, 5 Newton steps) on one --size pair from zero flow, and the
+    LK pyr2 pipeline, --steps times after --warmup; CUDA events."""
+    import torch
+    import denseLucasKanade_PyCL as LK
+    import GenericPyramidalOpticalFlow as G
+    from ofb200 import ops, synthetic as S
+    a8, b8, _, _ = S.config_pair("lk512", seed=1, size=args.size)
+    I = torch.from_numpy(a8.astype(np.float32)).cuda()
+    J = torch.from_numpy(b8.astype(np.float32)).cuda()
+    U, V = torch.zeros_like(I), torch.zeros_like(I)
+    ms = []
+    for r in range(args.warmup + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ops.lk_dense(I, J, U.zero_(), V.zero_())
+        e1.record()
+        e1.synchronize()
+        if r >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+    pm = []
+    for r in range(args.warmup + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        G.genericPyramidalOpticalFlow(I, J, 2, LK.denseLucasKanade_PyCl(Niter=5, halfWindow=13), 2, 1, 0.48, None,
+                                      warping=False)
+        e1.record()
+        e1.synchronize()
+        if r >= args.warmup:
+            pm.append(e0.elapsed_time(e1))
+    px = args.size * args.size
+    t = float(np.mean(ms))
+    print(json.dumps({"mode": "lk", "size": args.size, "lk_dense_ms": t, "pyr2_pipeline_ms": float(np.mean(pm)),
+                      "tflops_at_7e4_flop_per_px": 7e4 * px / (t * 1e-3) / 1e12}))
 
 
 def run_e2e_only(args):
@@ -832,6 +901,12 @@ def main():
         return
     if args.mode == "e2e":
         run_e2e_only(args)
+        return
+    if args.mode == "hs":
+        run_hs_only(args)
+        return
+    if args.mode == "lk":
+        run_lk_only(args)
         return
     if args.mode == "batch":
         if world > 1:

@@ -226,7 +226,7 @@ int of_ls_solve_noalloc(const float* I0, const float* I1, float* U, float* V, in
  * (src/pyrlkDenseLargeW.cl:304-669): per pixel, Scharr gradients over a
  * (2*half_win+1)^2 window (half_win <= 15), <= niter Newton steps on a bilinear J
  * (float32 weights), stop at |delta| < 0.01.  asym: {left,right,top,bottom} window
- * masks (HOST array, may be NULL = all 0).  status (uint8, optional): 1 = tracked,
+ * masks (HOST array of 0 / 1 values, may be NULL = all 0).  status (uint8, optional): 1 = tracked,
  * 0 = singular / left the image.  err (float, optional): the kernel's mean |J-I|.
  * Pixels with a singular gradient matrix keep their input U, V.
  * ------------------------------------------------------------------------------- */
