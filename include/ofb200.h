@@ -346,6 +346,63 @@ int of_cnn_flow_up(const float* flow, int h, int w, int factor, float* U, float*
 /* (h, w, 2) interleaved f32 flow -> u, v planes (row pitch `pitch`). */
 int of_cnn_split_flow(const float* flow, int h, int w, float* u, float* v, int pitch, void* stream);
 
+/* ---------------------------------------------------------------------------------
+ * Batches through the whole pyramid — of_batch_run replaces genericPyramidalOpticalFlow
+ * (src/GenericPyramidalOpticalFlow.py:237-415) called once per pair with the HS, LK or
+ * Farneback adapter (+ the optional Liu-Shen refine), bilinear warp and kLevels = 1; the
+ * same kernels run with the same arguments as the Python drop-in, so results are equal.
+ * Host constants the reference computes in Python come with the descriptor: the prefilter
+ * taps (prepareGaussianKernel, src/gaussian_filter.py:47-52) and the Farneback kernels and
+ * polynomial constants (src/Farneback_PyCL.py:123-208).  Pairs run in stream order on
+ * `stream`; single-level Horn-Schunck pairs are gathered into one persistent launch
+ * (of_hs_batch, with tuning->tile_shape).  status (DEVICE int[n], optional): the OF_ST_*
+ * words of each pair (cleared by the call).
+ * ------------------------------------------------------------------------------- */
+#define OF_METHOD_HS 0
+#define OF_METHOD_LK 1
+#define OF_METHOD_FB 2
+#define OF_FB_MAX_LEVELS 8
+
+/* Farneback_PyCL(windowSize, Niters, polyN, polySigma, useGaussian, pyrScale, pyramidalLevels) */
+typedef struct OfFbParams {
+  int window_size, niters, use_gaussian, levels;
+  double pyr_scale;
+  of_fb_poly_consts poly;
+  const float* window_taps; /* half kernel (centre first) of getGaussianKernelBitExact(windowSize, windowSize/2*0.3) */
+  int window_kh;
+  const float* level_taps[OF_FB_MAX_LEVELS]; /* per internal level k (0 = full size): the frame blur's half kernel */
+  int level_kh[OF_FB_MAX_LEVELS];
+} OfFbParams;
+
+typedef struct OfPairDesc {
+  int method;                  /* OF_METHOD_* */
+  int frame_u8;                /* 1: I0, I1 are uint8 planes, 0: float32 */
+  const void* I0;              /* DEVICE frames H x W, row pitch in_pitch elements */
+  const void* I1;
+  int in_pitch;
+  float* U;                    /* DEVICE result (float32 H x W, row pitch out_pitch) */
+  float* V;
+  int out_pitch;
+  int H, W;
+  float filter;                /* FILTER; > 1e-3 prefilters with filter_taps (3 taps, HOST) */
+  const float* filter_taps;
+  int levels;                  /* pyramidalLevels */
+  int refine_ls;               /* the Liu-Shen refine (optionalOFlowAlgoAdapter) */
+  float filter_opt;            /* FILTER_OPT; > 1e-3 prefilters the refine's frames (5 taps, HOST) */
+  const float* filter_opt_taps;
+  float ls_h;                  /* LiuShenOpticalFlowAlgoAdapter(alpha) */
+  int ls_arithmetic;           /* OF_LS_EXACT or OF_LS_FAST */
+  int warping, intermediate_scaling, scaling;  /* -1: the main adapter's pyramid defaults */
+  float hs_alphas[8];          /* HSOpticalFlowAlgoAdapter(alphas, Niter): popped from the end */
+  int hs_nalphas, hs_niter;
+  int lk_half_win, lk_niter;   /* denseLucasKanade_PyCl(Niter, halfWindow) */
+  const OfFbParams* fb;        /* HOST, for OF_METHOD_FB */
+} OfPairDesc;
+
+size_t of_batch_workspace_size(const OfPairDesc* descs, int n, const OfTuning* tuning);
+int of_batch_run(const OfPairDesc* descs, int n, const OfTuning* tuning, int* status, void* workspace,
+                 size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -167,6 +167,12 @@ __global__ void ls_status_kernel(const int* iters, const double* err, int maxnum
   const int k = *iters;
   if (k < 0 || (k >= maxnum && !(*err <= tol))) atomicOr(status, OF_ST_NOT_CONVERGED);
 }
+__global__ void status_or_kernel(const int* src, int* dst) { atomicOr(dst, *src); }
+
+int status_or(const int* src, int* dst, cudaStream_t stream) {
+  status_or_kernel<<<1, 1, 0, stream>>>(src, dst);
+  return check_launch("status_or");
+}
 }  // namespace ofb
 
 extern "C" int of_check_finite(const float* p, int H, int W, int pitch, int* status, int bit, void* stream) {

@@ -19,6 +19,8 @@ int set_error(int code, const char* fmt, ...);
 // Reports the first launch error of an entry point; `nlaunch` kernel launches are added
 // to the process-wide counter behind of_launch_count().
 int check_launch(const char* what, long long nlaunch = 1);
+// *dst |= *src on the device (status words), one launch.
+int status_or(const int* src, int* dst, cudaStream_t stream);
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 

@@ -40,6 +40,29 @@ class FbPolyConsts(ctypes.Structure):
                 ("xxg", ctypes.c_float * 8), ("ig", ctypes.c_float * 4)]
 
 
+OF_FB_MAX_LEVELS = 8
+OF_METHOD_HS, OF_METHOD_LK, OF_METHOD_FB = 0, 1, 2
+
+
+class OfFbParams(ctypes.Structure):
+    _fields_ = [("window_size", ctypes.c_int), ("niters", ctypes.c_int), ("use_gaussian", ctypes.c_int),
+                ("levels", ctypes.c_int), ("pyr_scale", ctypes.c_double), ("poly", FbPolyConsts),
+                ("window_taps", ctypes.c_void_p), ("window_kh", ctypes.c_int),
+                ("level_taps", ctypes.c_void_p * OF_FB_MAX_LEVELS), ("level_kh", ctypes.c_int * OF_FB_MAX_LEVELS)]
+
+
+class OfPairDesc(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int), ("frame_u8", ctypes.c_int), ("I0", ctypes.c_void_p),
+                ("I1", ctypes.c_void_p), ("in_pitch", ctypes.c_int), ("U", ctypes.c_void_p), ("V", ctypes.c_void_p),
+                ("out_pitch", ctypes.c_int), ("H", ctypes.c_int), ("W", ctypes.c_int), ("filter", ctypes.c_float),
+                ("filter_taps", ctypes.c_void_p), ("levels", ctypes.c_int), ("refine_ls", ctypes.c_int),
+                ("filter_opt", ctypes.c_float), ("filter_opt_taps", ctypes.c_void_p), ("ls_h", ctypes.c_float),
+                ("ls_arithmetic", ctypes.c_int), ("warping", ctypes.c_int), ("intermediate_scaling", ctypes.c_int),
+                ("scaling", ctypes.c_int), ("hs_alphas", ctypes.c_float * 8), ("hs_nalphas", ctypes.c_int),
+                ("hs_niter", ctypes.c_int), ("lk_half_win", ctypes.c_int), ("lk_niter", ctypes.c_int),
+                ("fb", ctypes.c_void_p)]
+
+
 _lib = None
 
 _P = ctypes.c_void_p
@@ -76,6 +99,8 @@ _SIGS = {
     "of_ls_solve_noalloc": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P], _I),
     "of_ls_solve_mode": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _I, _P, _P, _P, _Z, _P], _I),
     "of_hs_batch_shape": ([_I, _P, _P, _P], _I),
+    "of_batch_workspace_size": ([_P, _I, _P], _Z),
+    "of_batch_run": ([_P, _I, _P, _P, _P, _Z, _P], _I),
     "of_check_finite": ([_P, _I, _I, _I, _P, _I, _P], _I),
     "of_ls_status": ([_P, _P, _I, _D, _P, _P], _I),
     "of_hs_batch_workspace_size": ([_P, _I], _Z),

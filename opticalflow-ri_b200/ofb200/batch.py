@@ -22,7 +22,7 @@ from . import graph as _graph
 from . import ops
 
 __all__ = ["PairSpec", "PairBatch", "HsGroup", "method_spec", "config4_manifest", "render_entry", "pair_cost_of",
-           "BatchRunner", "autotune", "tune_hs_shape"]
+           "BatchRunner", "autotune", "tune_hs_shape", "pair_descriptors", "run_c"]
 
 
 @dataclass
@@ -378,3 +378,96 @@ def autotune(entries, frames, chunks=(16, 64, 256), streams=(2, 4, 8), reps=2, l
                 del r
                 gc.collect()
     return best, table
+
+
+# ----------------------------------------------------------------------------- C driver
+def pair_descriptors(specs, frames, outs, keep):
+    """OfPairDesc entries for of_batch_run from PairSpecs (this package's HS / LK / Farneback
+    adapters, optional Liu-Shen refine), CUDA frames (uint8 or float32) and output planes.
+    Host constants (taps, Farneback kernels) are appended to `keep`, which must outlive the
+    call."""
+    import numpy as np
+    import denseLucasKanade_PyCL as LKm
+    import Farneback_PyCL as FBm
+    import HornSchunck as HSm
+    import PhysicsBasedOpticalFlowLiuShen as LSm
+    from gaussian_filter import prepareGaussianKernel
+    arr = (_lib.OfPairDesc * len(specs))()
+
+    def host(a):
+        a = np.ascontiguousarray(a, np.float32)
+        keep.append(a)
+        return a.ctypes.data
+
+    for k, (sp, (a, b), (U, V)) in enumerate(zip(specs, frames, outs)):
+        main = sp.make_main()
+        opt = sp.make_opt() if sp.make_opt is not None else None
+        FILTER, L, kL, FOPT, warping, biLinear, inter, last = _cfg_for(sp, main)
+        if kL != 1 or not biLinear:
+            raise ValueError("of_batch_run takes kLevels = 1 and the bilinear warp")
+        d = arr[k]
+        d.frame_u8 = int(a.dtype == torch.uint8)
+        d.I0, d.I1, d.in_pitch = a.data_ptr(), b.data_ptr(), a.stride(0)
+        d.U, d.V, d.out_pitch = U.data_ptr(), V.data_ptr(), U.stride(0)
+        d.H, d.W = a.shape
+        d.filter = FILTER
+        d.filter_taps = host(prepareGaussianKernel(FILTER, 3)) if FILTER > 1e-3 else None
+        d.levels = L
+        d.warping, d.intermediate_scaling, d.scaling = int(warping), int(inter), int(last)
+        if opt is not None:
+            if not isinstance(opt, LSm.LiuShenOpticalFlowAlgoAdapter):
+                raise ValueError("of_batch_run refines with Liu-Shen only")
+            d.refine_ls = 1
+            d.filter_opt = float(FOPT) if FOPT is not None else 0.0
+            d.filter_opt_taps = host(prepareGaussianKernel(FOPT, 5)) if FOPT is not None and FOPT > 1e-3 else None
+            d.ls_h = float(np.float32(opt.alpha))
+            d.ls_arithmetic = 1 if opt.arithmetic == "fast" else 0
+        if isinstance(main, HSm.HSOpticalFlowAlgoAdapter):
+            d.method = _lib.OF_METHOD_HS
+            al = list(main.alphas)[-8:]
+            for i, x in enumerate(al):
+                d.hs_alphas[i] = float(np.float32(x))
+            d.hs_nalphas, d.hs_niter = len(al), int(main.Niter)
+        elif isinstance(main, LKm.denseLucasKanade_PyCl):
+            if main.enableVorticityEnhancement:
+                raise ValueError("of_batch_run: no vorticity-enhanced windows")
+            d.method = _lib.OF_METHOD_LK
+            d.lk_half_win, d.lk_niter = int(main.windowHalfWidth), int(main.Niter)
+        elif isinstance(main, FBm.Farneback_PyCL):
+            d.method = _lib.OF_METHOD_FB
+            p = _lib.OfFbParams()
+            p.window_size, p.niters, p.use_gaussian = int(main.windowSize), int(main.numIters), int(main.useGaussianFilter)
+            p.levels, p.pyr_scale, p.poly = int(main.pyramidalLevels) + 1, float(main.pyrScale), main._poly
+            main.setGaussianBlurKernel(main.windowSize, main.windowSize / 2 * 0.3)
+            p.window_taps, p.window_kh = host(main.matrixGKernel[0]), len(main.matrixGKernel[0]) - 1
+            scale = 1.0
+            for lev in range(_lib.OF_FB_MAX_LEVELS):
+                sigma = (1.0 / scale - 1.0) * 0.5
+                smooth = max(int(round(sigma * 5)) | 1, 3)
+                main.setGaussianBlurKernel(smooth, sigma)
+                p.level_taps[lev], p.level_kh[lev] = host(main.matrixGKernel[0]), smooth // 2
+                scale *= main.pyrScale
+            keep.append(p)
+            d.fb = ctypes.addressof(p)
+        else:
+            raise ValueError("of_batch_run: unsupported main adapter")
+    return arr
+
+
+def run_c(specs, frames, tile_shape: int = 0, status: bool = True):
+    """The pairs through the C driver of_batch_run (one call, the current stream).  Returns
+    ([(U, V)], status words or None)."""
+    outs = [(torch.empty(a.shape, dtype=torch.float32, device=a.device),
+             torch.empty(a.shape, dtype=torch.float32, device=a.device)) for a, _ in frames]
+    keep = []
+    arr = pair_descriptors(specs, frames, outs, keep)
+    n = len(specs)
+    tun = _lib.OfTuning(int(tile_shape), 0, (ctypes.c_int * 2)(0, 0))
+    st = torch.zeros(n, dtype=torch.int32, device=frames[0][0].device) if status else None
+    need = _lib.lib().of_batch_workspace_size(arr, n, ctypes.byref(tun))
+    if need == 0:
+        raise ValueError("of_batch_run: invalid descriptors")
+    ws, wn = ops.workspace(need, "batch_c")
+    _lib.call("of_batch_run", arr, n, ctypes.byref(tun), ctypes.c_void_p(st.data_ptr()) if st is not None else None,
+              ws, wn, ops.stream_ptr())
+    return outs, st
