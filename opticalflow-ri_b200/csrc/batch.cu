@@ -220,9 +220,10 @@ int run_pair(Arena& A, const OfPairDesc& d, int index, int* status, std::vector<
       } else if (lscale) {
         CALL(of_scale(Ua.p, us.p, sx, h, w, us.pitch, st));
         CALL(of_scale(Va.p, vs.p, sy, h, w, vs.pitch, st));
-      } else {
-        us = Ua;
-        vs = Va;
+      } else {  // a copy: the mains update their initial field in place
+        if (copy_plane(A, Ua.p, Ua.pitch, us.p, us.pitch, h, w, st) ||
+            copy_plane(A, Va.p, Va.pitch, vs.p, vs.pitch, h, w, st))
+          return OF_ERR_CUDA;
       }
       U = new_plane(A, h, w);
       V = new_plane(A, h, w);
