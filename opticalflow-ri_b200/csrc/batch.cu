@@ -431,7 +431,7 @@ extern "C" int of_batch_run(const OfPairDesc* descs, int n, const OfTuning* tuni
     if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_batch_run: %s", cudaGetErrorString(e));
     OfTuning tun{};
     if (tuning) tun = *tuning;
-    int rc = of_hs_batch(hp.data(), (int)hp.size(), &tun, hs_status, 1ll << 24, ws, wn, stream);
+    int rc = of_hs_batch(hp.data(), (int)hp.size(), &tun, hs_status, 1ll << 20, ws, wn, stream);
     if (rc != OF_OK) return rc;
     for (size_t k = 0; k < defer.size(); k++) {
       const Deferred& q = defer[k];

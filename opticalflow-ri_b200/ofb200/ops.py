@@ -271,7 +271,7 @@ def hs_batch_shapes():
         i += 1
 
 
-HS_WAIT_LIMIT = 1 << 24  # polls of a queue wait before a pair is given up (about a second)
+HS_WAIT_LIMIT = 1 << 20  # polls of a queue wait before a pair is given up (under a second)
 
 
 def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status=None):
