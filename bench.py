@@ -124,10 +124,11 @@ def run_hs_only(args):
     U, V = z.clone(), z.clone()
     out["of_hs_solve_ms"] = timeit(lambda: ops.hs_solve(a, b, U.zero_(), V.zero_(), 21.0, 600))
     for k, shp in enumerate(ops.hs_batch_shapes()):
-        U2, V2 = z.clone(), z.clone()
-        out[f"of_hs_batch_shape{k}_{shp[0]}x{shp[1]}t{shp[2]}_ms"] = timeit(
-            lambda: ops.hs_batch([(a, b, U2.zero_(), V2.zero_(), 21.0, 600)], tile_shape=k))
-        out[f"shape{k}_equal"] = bool(torch.equal(U2, U) and torch.equal(V2, V))
+        for ar in ("exact", "fast"):
+            U2, V2 = z.clone(), z.clone()
+            out[f"of_hs_batch_{ar}_shape{k}_{shp[0]}x{shp[1]}t{shp[2]}_ms"] = timeit(
+                lambda: ops.hs_batch([(a, b, U2.zero_(), V2.zero_(), 21.0, 600)], tile_shape=k, arithmetic=ar))
+            out[f"{ar}_shape{k}_maxdiff"] = float(max((U2 - U).abs().max().item(), (V2 - V).abs().max().item()))
     print(json.dumps(out))
 
 

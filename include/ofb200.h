@@ -148,8 +148,11 @@ int of_hs_solve(const float* I0, const float* I1, float* U, float* V, int H, int
 typedef struct OfTuning {
   int tile_shape;
   int streams;   /* host-side concurrency of callers that use streams; unused by the kernels */
-  int reserved[2];
+  int hs_arithmetic; /* OF_HS_EXACT (bit-exact with the reference) or OF_HS_FAST (float32 averaging) */
+  int reserved;
 } OfTuning;
+#define OF_HS_EXACT 0
+#define OF_HS_FAST 1
 
 /* One Horn-Schunck pair of a batch: DEVICE planes of H x W float32 with row pitch `pitch`;
  * U, V hold the initial flow and receive the result. */
@@ -169,7 +172,9 @@ typedef struct OfHsBatchPair {
  * waits for its previous pass with a bounded poll of at most `wait_limit` iterations, after
  * which the pair gets OF_ST_WAIT_TIMEOUT and is skipped (the launch still ends).  The
  * derivative pass sets OF_ST_NONFINITE_INPUT for frames with NaN / Inf, the last sweep pass
- * OF_ST_NONFINITE_OUTPUT.  status: DEVICE int[n].  The HS error value is not computed. */
+ * OF_ST_NONFINITE_OUTPUT.  status: DEVICE int[n].  The HS error value is not computed.
+ * tuning->hs_arithmetic OF_HS_FAST averages in float32 (corner and edge sums, two
+ * multiply-adds) instead of the reference's float64 sum: within float32 rounding. */
 int of_hs_batch_shape(int index, int* region_w, int* region_h, int* sweeps_per_pass);
 /* Status helpers for batches (no counterpart in the reference, which lets NaN propagate):
  * of_check_finite ORs `bit` into *status (DEVICE int) when the plane holds NaN or Inf;

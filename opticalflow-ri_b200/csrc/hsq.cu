@@ -81,7 +81,7 @@ struct HqTile {
   static constexpr size_t SMEM = 7 * (size_t)PL * sizeof(float);
 };
 
-template <int RW, int RH, int T, bool EDGE>
+template <int RW, int RH, int T, bool EDGE, bool FAST>
 __device__ __forceinline__ void hq_sweep(const float* __restrict__ sfx, const float* __restrict__ sfy,
                                          const float* __restrict__ sft, const float* su, const float* sv, float* du,
                                          float* dv, int s, int x0, int y0, int H, int W, float a2) {
@@ -99,16 +99,28 @@ __device__ __forceinline__ void hq_sweep(const float* __restrict__ sfx, const fl
       rp = mirror1(gy + 1, H) - (y0 - T);
     }
     const int om = rm * RW, o0 = r * RW, op = rp * RW;
-    double a = 0.0, b = 0.0;
-    a = __fma_rn((double)su[om + cm], wc, a); b = __fma_rn((double)sv[om + cm], wc, b);
-    a = __fma_rn((double)su[om + c], we, a);  b = __fma_rn((double)sv[om + c], we, b);
-    a = __fma_rn((double)su[om + cp], wc, a); b = __fma_rn((double)sv[om + cp], wc, b);
-    a = __fma_rn((double)su[o0 + cm], we, a); b = __fma_rn((double)sv[o0 + cm], we, b);
-    a = __fma_rn((double)su[o0 + cp], we, a); b = __fma_rn((double)sv[o0 + cp], we, b);
-    a = __fma_rn((double)su[op + cm], wc, a); b = __fma_rn((double)sv[op + cm], wc, b);
-    a = __fma_rn((double)su[op + c], we, a);  b = __fma_rn((double)sv[op + c], we, b);
-    a = __fma_rn((double)su[op + cp], wc, a); b = __fma_rn((double)sv[op + cp], wc, b);
-    const float ua = (float)a, va = (float)b;
+    float ua, va;
+    if (FAST) {  // float32 averaging: corner and edge sums, one multiply-add each
+      const float wcf = 1.0f / 12.0f, wef = 1.0f / 6.0f;
+      const float cu = __fadd_rn(__fadd_rn(su[om + cm], su[om + cp]), __fadd_rn(su[op + cm], su[op + cp]));
+      const float eu = __fadd_rn(__fadd_rn(su[om + c], su[op + c]), __fadd_rn(su[o0 + cm], su[o0 + cp]));
+      const float cv = __fadd_rn(__fadd_rn(sv[om + cm], sv[om + cp]), __fadd_rn(sv[op + cm], sv[op + cp]));
+      const float ev = __fadd_rn(__fadd_rn(sv[om + c], sv[op + c]), __fadd_rn(sv[o0 + cm], sv[o0 + cp]));
+      ua = __fmaf_rn(cu, wcf, __fmul_rn(eu, wef));
+      va = __fmaf_rn(cv, wcf, __fmul_rn(ev, wef));
+    } else {
+      double a = 0.0, b = 0.0;
+      a = __fma_rn((double)su[om + cm], wc, a); b = __fma_rn((double)sv[om + cm], wc, b);
+      a = __fma_rn((double)su[om + c], we, a);  b = __fma_rn((double)sv[om + c], we, b);
+      a = __fma_rn((double)su[om + cp], wc, a); b = __fma_rn((double)sv[om + cp], wc, b);
+      a = __fma_rn((double)su[o0 + cm], we, a); b = __fma_rn((double)sv[o0 + cm], we, b);
+      a = __fma_rn((double)su[o0 + cp], we, a); b = __fma_rn((double)sv[o0 + cp], we, b);
+      a = __fma_rn((double)su[op + cm], wc, a); b = __fma_rn((double)sv[op + cm], wc, b);
+      a = __fma_rn((double)su[op + c], we, a);  b = __fma_rn((double)sv[op + c], we, b);
+      a = __fma_rn((double)su[op + cp], wc, a); b = __fma_rn((double)sv[op + cp], wc, b);
+      ua = (float)a;
+      va = (float)b;
+    }
     const int i = o0 + c;
     const float gxv = sfx[i], gyv = sfy[i];
     const float num = __fadd_rn(__fadd_rn(__fmul_rn(gxv, ua), __fmul_rn(gyv, va)), sft[i]);
@@ -120,7 +132,7 @@ __device__ __forceinline__ void hq_sweep(const float* __restrict__ sfx, const fl
 }
 
 // Returns false when a result of the last pass is not finite.
-template <int RW, int RH, int T>
+template <int RW, int RH, int T, bool FAST>
 __device__ bool hq_sweep_item(const HsqPair& P, int pass, int tile, float* sm) {
   using G = HqTile<RW, RH, T>;
   const int ty = tile / P.tx, tx = tile - ty * P.tx;
@@ -163,9 +175,9 @@ __device__ bool hq_sweep_item(const HsqPair& P, int pass, int tile, float* sm) {
     float* ou = q ? bu0 : bu1;
     float* ov = q ? bv0 : bv1;
     if (edge)
-      hq_sweep<RW, RH, T, true>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
+      hq_sweep<RW, RH, T, true, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
     else
-      hq_sweep<RW, RH, T, false>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
+      hq_sweep<RW, RH, T, false, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
     __syncthreads();
   }
   const float* fu = (nsw & 1) ? bu1 : bu0;
@@ -183,7 +195,7 @@ __device__ bool hq_sweep_item(const HsqPair& P, int pass, int tile, float* sm) {
   return finite || p != np - 1;
 }
 
-template <int RW, int RH, int T>
+template <int RW, int RH, int T, bool FAST>
 __global__ void __launch_bounds__(256) hsq_kernel(const HsqPair* __restrict__ pairs, int npairs,
                                                   unsigned int tiles_total, int max_passes,
                                                   unsigned long long* ticket, unsigned int* done, int* status,
@@ -242,7 +254,7 @@ __global__ void __launch_bounds__(256) hsq_kernel(const HsqPair* __restrict__ pa
           if (y < P.H && x < P.W) ok = hq_deriv_px(P, y, x) && ok;
         }
       } else {
-        ok = hq_sweep_item<RW, RH, T>(P, pass, tile, hq_sm);
+        ok = hq_sweep_item<RW, RH, T, FAST>(P, pass, tile, hq_sm);
       }
     }
     const int bad = __syncthreads_or(!ok);  // also: every store of the item is issued
@@ -278,23 +290,30 @@ constexpr HsqShape kHsqShapes[] = {{64, 40, 4}, {32, 24, 4}, {64, 24, 4}, {32, 3
 constexpr int kHsqNumShapes = sizeof(kHsqShapes) / sizeof(kHsqShapes[0]);
 
 template <int RW, int RH, int T>
-cudaError_t hsq_launch(int grid, const HsqPair* pairs, int n, unsigned int tiles_total, int max_passes,
+cudaError_t hsq_launch(bool fast, int grid, const HsqPair* pairs, int n, unsigned int tiles_total, int max_passes,
                        unsigned long long* ticket, unsigned int* done, int* status, long long wait_limit,
                        int* err_flag, cudaStream_t st) {
   using G = HqTile<RW, RH, T>;
-  cudaError_t e = OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T>), G::SMEM);
+  cudaError_t e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true>), G::SMEM)
+                       : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false>), G::SMEM);
   if (e != cudaSuccess) return e;
-  hsq_kernel<RW, RH, T><<<grid, 256, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
-                                                     wait_limit, err_flag);
+  if (fast)
+    hsq_kernel<RW, RH, T, true><<<grid, 256, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
+                                                            wait_limit, err_flag);
+  else
+    hsq_kernel<RW, RH, T, false><<<grid, 256, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
+                                                             wait_limit, err_flag);
   return cudaGetLastError();
 }
 
 template <int RW, int RH, int T>
-int hsq_resident(int* per_sm) {
+int hsq_resident(bool fast, int* per_sm) {
   using G = HqTile<RW, RH, T>;
-  cudaError_t e = OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T>), G::SMEM);
+  cudaError_t e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true>), G::SMEM)
+                       : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false>), G::SMEM);
   if (e != cudaSuccess) return -1;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, hsq_kernel<RW, RH, T>, 256, G::SMEM);
+  e = fast ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, hsq_kernel<RW, RH, T, true>, 256, G::SMEM)
+           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, hsq_kernel<RW, RH, T, false>, 256, G::SMEM);
   return e == cudaSuccess ? 0 : -1;
 }
 }  // namespace
@@ -319,6 +338,9 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
   OF_REQUIRE(status, "of_hs_batch: status (a device array of n ints) is required");
   OF_REQUIRE(wait_limit > 0, "of_hs_batch: wait_limit must be positive");
   int shape = tuning ? tuning->tile_shape : 0;
+  const int arith = tuning ? tuning->hs_arithmetic : OF_HS_EXACT;
+  OF_REQUIRE(arith == OF_HS_EXACT || arith == OF_HS_FAST, "of_hs_batch: hs_arithmetic must be OF_HS_EXACT or OF_HS_FAST");
+  const bool fast = arith == OF_HS_FAST;
   OF_REQUIRE(shape >= 0 && shape < kHsqNumShapes, "of_hs_batch: tile_shape must be in 0..%d", kHsqNumShapes - 1);
   const HsqShape sh = kHsqShapes[shape];
   const int TW = sh.rw - 2 * sh.t, TH = sh.rh - 2 * sh.t;
@@ -386,10 +408,10 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int rc;
   switch (shape) {
-    case 0: rc = hsq_resident<64, 40, 4>(&per_sm); break;
-    case 1: rc = hsq_resident<32, 24, 4>(&per_sm); break;
-    case 2: rc = hsq_resident<64, 24, 4>(&per_sm); break;
-    default: rc = hsq_resident<32, 32, 8>(&per_sm); break;
+    case 0: rc = hsq_resident<64, 40, 4>(fast, &per_sm); break;
+    case 1: rc = hsq_resident<32, 24, 4>(fast, &per_sm); break;
+    case 2: rc = hsq_resident<64, 24, 4>(fast, &per_sm); break;
+    default: rc = hsq_resident<32, 32, 8>(fast, &per_sm); break;
   }
   if (rc != 0 || per_sm < 1) return set_error(OF_ERR_CUDA, "of_hs_batch: occupancy query failed");
   // every CTA must be resident (items wait for items of running CTAs); no more CTAs than
@@ -398,10 +420,10 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
   if (grid > (long long)tiles_total) grid = tiles_total;
   if (grid < 1) grid = 1;
   switch (shape) {
-    case 0: e = hsq_launch<64, 40, 4>((int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    case 1: e = hsq_launch<32, 24, 4>((int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    case 2: e = hsq_launch<64, 24, 4>((int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    default: e = hsq_launch<32, 32, 8>((int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    case 0: e = hsq_launch<64, 40, 4>(fast, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    case 1: e = hsq_launch<32, 24, 4>(fast, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    case 2: e = hsq_launch<64, 24, 4>(fast, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    default: e = hsq_launch<32, 32, 8>(fast, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
   }
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: launch: %s", cudaGetErrorString(e));
   return check_launch("of_hs_batch", nl + 1);

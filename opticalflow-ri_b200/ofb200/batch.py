@@ -462,7 +462,7 @@ def run_c(specs, frames, tile_shape: int = 0, status: bool = True):
     keep = []
     arr = pair_descriptors(specs, frames, outs, keep)
     n = len(specs)
-    tun = _lib.OfTuning(int(tile_shape), 0, (ctypes.c_int * 2)(0, 0))
+    tun = _lib.OfTuning(int(tile_shape), 0, 0, 0)
     st = torch.zeros(n, dtype=torch.int32, device=frames[0][0].device) if status else None
     need = _lib.lib().of_batch_workspace_size(arr, n, ctypes.byref(tun))
     if need == 0:

@@ -274,10 +274,13 @@ def hs_batch_shapes():
 HS_WAIT_LIMIT = 1 << 20  # polls of a queue wait before a pair is given up (under a second)
 
 
-def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status=None):
+def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status=None, arithmetic: str = "exact"):
     """Horn-Schunck of many pairs in one persistent launch (of_hs_batch).  pairs: list of
     (I0, I1, U, V, alpha, niter) with CUDA float32 planes; U, V are updated in place.
+    arithmetic: 'exact' (bit-exact with the reference) or 'fast' (float32 averaging).
     Returns the per-pair status words (device int32, bits of ofb200._lib.ST_*)."""
+    if arithmetic not in ("exact", "fast"):
+        raise ValueError("arithmetic must be 'exact' or 'fast'")
     from ._lib import OfHsBatchPair, OfTuning
     n = len(pairs)
     arr = (OfHsBatchPair * n)()
@@ -289,7 +292,7 @@ def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status
                                float(np.float32(alpha)), int(niter))
     if status is None:
         status = torch.zeros(n, dtype=torch.int32, device=dev)
-    tun = OfTuning(int(tile_shape), 0, (ctypes.c_int * 2)(0, 0))
+    tun = OfTuning(int(tile_shape), 0, 1 if arithmetic == "fast" else 0, 0)
     ws, wn = workspace(lib().of_hs_batch_workspace_size(arr, n), "hs_batch")
     call("of_hs_batch", arr, n, ctypes.byref(tun), ctypes.c_void_p(status.data_ptr()), int(wait_limit), ws, wn,
          stream_ptr())

@@ -113,3 +113,18 @@ def test_batch_runner_hs_group_equals_per_pair_graphs(cuda_ok):
         got = BatchRunner(entries, chunk=8, streams=4, hs_shape=shape).run(frames)
         for (U, V), (Ur, Vr) in zip(got, ref):
             assert torch.equal(U, Ur) and torch.equal(V, Vr)
+
+
+def test_fast_arithmetic_within_float32_rounding(cuda_ok):
+    """OF_HS_FAST (float32 averaging) stays within 1e-4 px of the bit-exact solver after
+    600 sweeps at 256^2 (the reference's float64 answer is within a few 1e-6 px of both)."""
+    import torch
+    from ofb200 import ops
+    a, b = _pair(torch, 256, 256, 1)
+    z = torch.zeros_like(a)
+    Ur, Vr = _solve_ref(torch, a, b, z, z, 21.0, 600)
+    for shape in range(len(ops.hs_batch_shapes())):
+        U, V = z.clone(), z.clone()
+        st = ops.hs_batch([(a, b, U, V, 21.0, 600)], tile_shape=shape, arithmetic="fast")
+        assert int(st.item()) == 0
+        assert max((U - Ur).abs().max().item(), (V - Vr).abs().max().item()) <= 1e-4
