@@ -12,6 +12,8 @@
 // previous sweep's error from device memory, so the host enqueues maxnum sweeps with no
 // synchronisation and the sequence can be captured in a CUDA graph.
 // Inside the solver u is the row (y) component and v the column (x) component (:38-39).
+#include <stdlib.h>
+
 #include "common.cuh"
 #include "tma.cuh"
 
@@ -622,8 +624,8 @@ __device__ __forceinline__ void lbf_strip(const LbPlane* su, const LbPlane* sv, 
   acc_v += (double)av;
 }
 
-template <bool FAST>
-__global__ void __launch_bounds__(32 * LB_WARPS, 2) ls_pass_kernel(const __grid_constant__ CUtensorMap tm_coef,
+template <bool FAST, int NW>
+__global__ void __launch_bounds__(32 * NW, 2) ls_pass_kernel(const __grid_constant__ CUtensorMap tm_coef,
                                                          const __grid_constant__ CUtensorMap tm_u0,
                                                          const __grid_constant__ CUtensorMap tm_v0,
                                                          const __grid_constant__ CUtensorMap tm_u1,
@@ -726,7 +728,7 @@ __global__ void __launch_bounds__(32 * LB_WARPS, 2) ls_pass_kernel(const __grid_
   S.h = h;
   S.one = one;
   S.own_col = c0 >= LB_T && c0 < LB_T + LB_TW;
-  __shared__ double red[LB_T][2][LB_WARPS];
+  __shared__ double red[LB_T][2][NW];
   __syncthreads();
 #pragma unroll 1
   for (int s = 0; s < nsw; s++) {
@@ -737,7 +739,7 @@ __global__ void __launch_bounds__(32 * LB_WARPS, 2) ls_pass_kernel(const __grid_
     // others) that lie in the image, split evenly over the warps
     const int lo = max(1 + s, rlo), hi = min(LB_RH - 1 - s, rhi + 1);
     const int n = hi - lo;
-    const int ra = lo + (n * warp) / LB_WARPS, rb = lo + (n * (warp + 1)) / LB_WARPS;
+    const int ra = lo + (n * warp) / NW, rb = lo + (n * (warp + 1)) / NW;
     if (rb > ra) {
       S.su = LB_U(in);
       S.sv = LB_V(in);
@@ -776,7 +778,7 @@ __global__ void __launch_bounds__(32 * LB_WARPS, 2) ls_pass_kernel(const __grid_
   if (t == 0) {
     for (int s = 0; s < nsw; s++) {
       double a = 0.0, b = 0.0;
-      for (int w = 0; w < LB_WARPS; w++) {
+      for (int w = 0; w < NW; w++) {
         a += red[s][0][w];
         b += red[s][1][w];
       }
@@ -902,7 +904,9 @@ extern "C" int of_ls_solve_mode(const float* I0, const float* I1, float* U, floa
     }
   }
   {
-    cudaError_t e = fast ? OF_SMEM_OPT_IN(ls_pass_kernel<true>, LB_SMEM) : OF_SMEM_OPT_IN(ls_pass_kernel<false>, LB_SMEM);
+    cudaError_t e = OF_SMEM_OPT_IN((ls_pass_kernel<false, LB_WARPS>), LB_SMEM);
+    if (e == cudaSuccess) e = OF_SMEM_OPT_IN((ls_pass_kernel<true, 6>), LB_SMEM);
+    if (e == cudaSuccess) e = OF_SMEM_OPT_IN((ls_pass_kernel<true, 8>), LB_SMEM);
     if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_ls_solve: %s", cudaGetErrorString(e));
   }
   // control block, flags, counters, redo counts and sums are contiguous: one memset
@@ -913,7 +917,14 @@ extern "C" int of_ls_solve_mode(const float* I0, const float* I1, float* U, floa
   ls_prep_kernel<<<dim3((W + 31) / 32, (H + 7) / 8), 256, 0, st>>>(I0, I1, pitch, ctrl->maxkey, V, U, coef, N,
                                                                  ub[0], vb[0], H, W, P, h);
   double inv_n = 1.0 / ((double)H * (double)W);
-  dim3 pgrd((W + LB_TW - 1) / LB_TW, (H + LB_TH - 1) / LB_TH), pblk(32, LB_WARPS);
+  // warps per CTA: 6 for the float64 pass (its registers allow 2 CTAs of 6); the float32
+  // pass defaults to 8 (OFB_LS_FAST_WARPS=6 selects 6)
+  static const int fast_nw = [] {
+    const char* e = getenv("OFB_LS_FAST_WARPS");
+    return (e && atoi(e) == 6) ? 6 : 8;
+  }();
+  const int nw = fast ? fast_nw : LB_WARPS;
+  dim3 pgrd((W + LB_TW - 1) / LB_TW, (H + LB_TH - 1) / LB_TH), pblk(32, nw);
   long long nl = 3;
   int p = 0, k0 = 0;
   // pass 0 waits for the set-up in stream order; later passes (and the rollback launch)
@@ -929,7 +940,9 @@ extern "C" int of_ls_solve_mode(const float* I0, const float* I1, float* U, floa
     cfg.stream = st;
     cfg.attrs = dependent ? pdl : nullptr;
     cfg.numAttrs = dependent ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, fast ? ls_pass_kernel<true> : ls_pass_kernel<false>, tm_coef, tm_u[0], tm_v[0],
+    return cudaLaunchKernelEx(&cfg, !fast ? ls_pass_kernel<false, LB_WARPS> : nw == 6 ? ls_pass_kernel<true, 6>
+                                                                               : ls_pass_kernel<true, 8>,
+                              tm_coef, tm_u[0], tm_v[0],
                               tm_u[1], tm_v[1], ub[0], vb[0], ub[1], vb[1], H, W, P, h, PP, ctrl, ss, run, done, redo,
                               inv_n, tol, err_flag, 1.0f);
   };
