@@ -7,12 +7,16 @@
 // pass p >= 1 runs up to HQ_T Jacobi sweeps (HS_helper, :61-70) on the tile with a halo of
 // HQ_T cells staged in shared memory (the temporal blocking of hs_pass_kernel), reading
 // the previous pass's fields and writing the next buffer of a ping-pong pair.  An item of
-// pass p waits until every tile of pass p - 1 of the same pair is done (a per-pair counter
-// of finished items).  The ticket order makes this free of deadlock: an item only waits for
-// items with smaller tickets, which were handed out earlier to CTAs that are running and
-// never wait for later ones.  The wait is bounded: after `wait_limit` polls the item gives
-// up, sets OF_ST_WAIT_TIMEOUT in its pair's status word and the launch's error flag, and
-// every later item of that pair is skipped (counted done, so nothing waits on it).
+// pass p waits only for its own tile and its (up to) 8 neighbouring tiles to have finished
+// pass p - 1 (a counter of finished passes per tile): the halo of T cells lies inside those
+// tiles, and since the neighbourhood is symmetric the same wait also guarantees that no
+// neighbour still reads (at pass p - 1) the buffer this item overwrites.  Passes therefore
+// overlap as a wavefront instead of meeting at a per-pass barrier.  The ticket order makes
+// this free of deadlock: an item only waits for items with smaller tickets, which were
+// handed out earlier to CTAs that are running and never wait for later ones.  The wait is
+// bounded: after `wait_limit` polls the item gives up, sets OF_ST_WAIT_TIMEOUT in its pair's
+// status word and the launch's error flag, and every later item of that pair is skipped
+// (still counted, so nothing waits on it).
 // Cross-CTA data goes through L2 only (ld.global.cg / st.global.cg), published by
 // __syncthreads + __threadfence + atomicAdd and consumed after the counter is observed.
 #include "common.cuh"
@@ -228,18 +232,25 @@ __global__ void __launch_bounds__(256) hsq_kernel(const HsqPair* __restrict__ pa
       int run = pass < P.passes;
       if (run && (((volatile int*)status)[i] & OF_ST_WAIT_TIMEOUT)) run = 0;  // the pair already failed
       if (run && pass > 0) {
-        const unsigned int target = (unsigned int)pass * (unsigned int)P.tiles;
+        // this tile and its neighbours must have finished pass - 1 (counters of passes done)
+        const int ty = tile / P.tx, tx = tile - ty * P.tx, nty = P.tiles / P.tx;
         long long k = 0;
-        while (((volatile unsigned int*)done)[i] < target) {
-          if (++k > wait_limit) {
-            atomicOr(status + i, OF_ST_WAIT_TIMEOUT);
-            atomicExch(err_flag, 1);
-            run = 0;
-            break;
+        for (int dy = -1; dy <= 1 && run; dy++)
+          for (int dx = -1; dx <= 1 && run; dx++) {
+            const int yy = ty + dy, xx = tx + dx;
+            if (yy < 0 || yy >= nty || xx < 0 || xx >= P.tx) continue;
+            const unsigned int* c = done + P.tile0 + yy * P.tx + xx;
+            while (*(volatile const unsigned int*)c < (unsigned int)pass) {
+              if (++k > wait_limit) {
+                atomicOr(status + i, OF_ST_WAIT_TIMEOUT);
+                atomicExch(err_flag, 1);
+                run = 0;
+                break;
+              }
+              __nanosleep(64);
+            }
           }
-          __nanosleep(64);
-        }
-        __threadfence();  // acquire: the previous pass's stores are visible from here on
+        __threadfence();  // acquire: the neighbours' stores are visible from here on
       }
       s_run = run;
     }
@@ -261,7 +272,7 @@ __global__ void __launch_bounds__(256) hsq_kernel(const HsqPair* __restrict__ pa
     if (threadIdx.x == 0 && bad) atomicOr(status + i, pass == 0 ? OF_ST_NONFINITE_INPUT : OF_ST_NONFINITE_OUTPUT);
     if (threadIdx.x == 0 && pass < P.passes) {
       __threadfence();  // release
-      atomicAdd(done + i, 1u);
+      atomicAdd(done + P.tile0 + tile, 1u);
     }
   }
 }
@@ -318,12 +329,27 @@ int hsq_resident(bool fast, int* per_sm) {
 }
 }  // namespace
 
+// tiles of a pair under the tile shape that cuts it finest (sizes the per-tile counters)
+static size_t hsq_max_tiles(const OfHsBatchPair* pairs, int n) {
+  size_t total = 0;
+  for (int i = 0; i < n; i++) {
+    size_t best = 0;
+    for (int k = 0; k < kHsqNumShapes; k++) {
+      const int TW = kHsqShapes[k].rw - 2 * kHsqShapes[k].t, TH = kHsqShapes[k].rh - 2 * kHsqShapes[k].t;
+      const size_t t = (size_t)((pairs[i].W + TW - 1) / TW) * (size_t)((pairs[i].H + TH - 1) / TH);
+      if (t > best) best = t;
+    }
+    total += best;
+  }
+  return total;
+}
+
 extern "C" size_t of_hs_batch_workspace_size(const OfHsBatchPair* pairs, int n) {
   if (!pairs || n <= 0) return 0;
   Sizer s;
   s.take<HsqPair>((size_t)n);
   s.take<unsigned long long>(1);
-  s.take<unsigned int>((size_t)n);
+  s.take<unsigned int>(hsq_max_tiles(pairs, n));
   s.take<int>(1);
   for (int i = 0; i < n; i++) {
     size_t N = (size_t)pairs[i].H * (size_t)pairs[i].pitch;
@@ -351,7 +377,7 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
   Carver c(workspace, workspace_bytes);
   HsqPair* dpairs = c.take<HsqPair>((size_t)n);
   unsigned long long* ticket = c.take<unsigned long long>(1);
-  unsigned int* done = c.take<unsigned int>((size_t)n);
+  unsigned int* done = c.take<unsigned int>(hsq_max_tiles(pairs, n));  // passes finished, per tile
   int* err_flag = c.take<int>(1);
   // descriptors are built on the host and written to the workspace by kernels that take
   // them as parameters (no host buffer outlives this call, and a graph capture holds copies)
