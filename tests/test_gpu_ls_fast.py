@@ -59,12 +59,16 @@ def test_fast_piv_1024(cuda_ok):
     assert ef == pytest.approx(ee, rel=1e-3)
 
 
-@pytest.mark.parametrize("tol", [1e-3, 3e-5])
-def test_fast_stop_rule(cuda_ok, tol):
+@pytest.mark.parametrize("factor", [30.0, 3.0])
+def test_fast_stop_rule(cuda_ok, factor):
+    """With a tolerance the solve reaches before its 60th sweep (a multiple of the error
+    left after 60 sweeps), both arithmetics stop early and within one sweep of each other."""
     import torch
     fa, fb = _frames(torch, 256, seed=5)
-    _, _, ie, _ = _solve(torch, fa, fb, "exact", tol=tol)
-    _, _, i_f, _ = _solve(torch, fa, fb, "fast", tol=tol)
+    _, _, n60, e60 = _solve(torch, fa, fb, "exact", tol=0.0)
+    assert n60 == 60
+    _, _, ie, _ = _solve(torch, fa, fb, "exact", tol=factor * e60)
+    _, _, i_f, _ = _solve(torch, fa, fb, "fast", tol=factor * e60)
     assert ie < 60 and abs(ie - i_f) <= 1
 
 
