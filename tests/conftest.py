@@ -7,6 +7,10 @@ import pytest
 # arithmetic promises; the float32 'fast' arithmetic (the library default) is tested on its
 # own, explicitly, in test_gpu_ls_fast.py.
 os.environ["OFB_LS_ARITHMETIC"] = "exact"
+# autotuning choices made by tests go to a scratch file, not the user's cache
+import tempfile  # noqa: E402
+
+os.environ.setdefault("OFB_AUTOTUNE_CACHE", os.path.join(tempfile.mkdtemp(prefix="ofb200-tune-"), "autotune.json"))
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(REPO, "opticalflow-ri_b200")

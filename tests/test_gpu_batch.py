@@ -101,6 +101,11 @@ def test_batch_rejects_count_mismatch(torch_cuda):
         PairBatch(specs).run([])
 
 
+def ops_shapes():
+    from ofb200 import ops
+    return ops.hs_batch_shapes()
+
+
 def test_config4_runner_matches_single_pairs(torch_cuda):
     """A small mixed manifest (all four methods, three sizes) through the chunked,
     autotuned runner gives each pair's single-call result."""
@@ -115,7 +120,9 @@ def test_config4_runner_matches_single_pairs(torch_cuda):
     rendered = [render_entry(e) for e in entries]
     frames = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b, _, _ in rendered]
     runner, table = autotune(entries, frames, chunks=(2, 6), streams=(1, 3), reps=1)
-    assert len(table) == 4
+    # chunk x streams candidates, plus the persistent Horn-Schunck kernel's tile shapes
+    assert len([k for k in table if k[0] != "hs_shape"]) == 4
+    assert len([k for k in table if k[0] == "hs_shape"]) == len(ops_shapes())
     outs = runner.run(frames)
     torch.cuda.synchronize()
     graph.ENABLED = False
