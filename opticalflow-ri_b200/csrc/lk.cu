@@ -168,6 +168,14 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
   lk_weights(xid, p.ws, p.aL, p.aR, wx, bx);
   lk_weights(yid, p.ws, p.aT, p.aB, wy0, by0);
   lk_weights(yid + 4, p.ws, p.aT, p.aB, wy1, by1);
+  unsigned act = 0;  // bit 16 v + 4 ty + tx: the sample's tile weight is not 0
+#pragma unroll
+  for (int v = 0; v < 2; v++)
+#pragma unroll
+    for (int ty = 0; ty < 4; ty++)
+#pragma unroll
+      for (int tx = 0; tx < 4; tx++)
+        act |= (unsigned)(__fmul_rn(wx[tx], (v ? wy1 : wy0)[ty]) != 0.f) << (16 * v + 4 * ty + tx);
   const float hw = (float)p.hw;
   const int i = i0 + warp;
   if (i >= H) return;
@@ -225,20 +233,58 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
         st = 0;
         break;
       }
+      // The bilinear sample positions of a Newton step: x parts per column tile, y parts per
+      // row tile (the same float32 operations as lk_bilinear_s, computed once per step)
+      float xa[4], xoa[4], yb[2][4], yob[2][4];
+      int xr[4], yr[2][4];
+      unsigned inx = 0, iny = 0;
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        const float xs = __fsub_rn(lx[t], 0.5f), fx0 = floorf(xs);
+        xa[t] = __fsub_rn(xs, fx0);
+        xoa[t] = __fsub_rn(1.f, xa[t]);
+        xr[t] = (int)fx0 - jox;
+        inx |= ((unsigned)xr[t] <= (unsigned)(LK_JR - 2)) << t;
+#pragma unroll
+        for (int v = 0; v < 2; v++) {
+          const float ys = __fsub_rn(ly[v][t], 0.5f), fy0 = floorf(ys);
+          yb[v][t] = __fsub_rn(ys, fy0);
+          yob[v][t] = __fsub_rn(1.f, yb[v][t]);
+          yr[v][t] = (int)fy0 - joy;
+          iny |= ((unsigned)yr[v][t] <= (unsigned)(LK_JR - 2)) << (4 * v + t);
+        }
+      }
       float b1[2] = {0.f, 0.f}, b2[2] = {0.f, 0.f};
 #pragma unroll
       for (int v = 0; v < 2; v++) {
-        const float* wy = v ? wy1 : wy0;
         const int yy = yid + 4 * v;
 #pragma unroll
         for (int ty = 0; ty < 4; ty++)
 #pragma unroll
           for (int tx = 0; tx < 4; tx++) {
-            float w = __fmul_rn(wx[tx], wy[ty]);
-            if (w == 0.f) continue;
+            if (!((act >> (16 * v + 4 * ty + tx)) & 1u)) continue;  // tile weight 0
             int g = (gyb + ty * 8 + yy) * LK_G + gxb + tx * 8 + xid;
             float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_I + gxb + tx * 8 + xid + 1];
-            float Jv = lk_bilinear_s(sJ, J, H, W, pitch, lx[tx], ly[v][ty], jox, joy);
+            float t00, t10, t01, t11;
+            if (((inx >> tx) & (iny >> (4 * v + ty))) & 1u) {
+              const float* q = sJ + yr[v][ty] * LK_JP + xr[tx];
+              t00 = q[0];
+              t10 = q[1];
+              t01 = q[LK_JP];
+              t11 = q[LK_JP + 1];
+            } else {  // outside the staged region: clamped global reads
+              const int i0 = xr[tx] + jox, j0 = yr[v][ty] + joy;
+              const int xa0 = clampi(i0, 0, W - 1), xb0 = clampi(i0 + 1, 0, W - 1);
+              const int ya0 = clampi(j0, 0, H - 1), yb0 = clampi(j0 + 1, 0, H - 1);
+              t00 = __ldg(J + (size_t)ya0 * pitch + xa0);
+              t10 = __ldg(J + (size_t)ya0 * pitch + xb0);
+              t01 = __ldg(J + (size_t)yb0 * pitch + xa0);
+              t11 = __ldg(J + (size_t)yb0 * pitch + xb0);
+            }
+            float Jv = __fmul_rn(__fmul_rn(xoa[tx], yob[v][ty]), t00);
+            Jv = __fmaf_rn(__fmul_rn(xa[tx], yob[v][ty]), t10, Jv);
+            Jv = __fmaf_rn(__fmul_rn(xoa[tx], yb[v][ty]), t01, Jv);
+            Jv = __fmaf_rn(__fmul_rn(xa[tx], yb[v][ty]), t11, Jv);
             float diff = __fsub_rn(Jv, Iv);  // (Jv - Iv) * w with w == 1
             b1[v] = __fmaf_rn(diff, sDx[g], b1[v]);
             b2[v] = __fmaf_rn(diff, sDy[g], b2[v]);

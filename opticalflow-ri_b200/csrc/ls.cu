@@ -489,7 +489,12 @@ __device__ __forceinline__ void lbf_load(LbRowF& R, const LbPlane* su, const LbP
   R.rv = sv[row][c.k[3]];
 }
 
-__device__ __forceinline__ float2 psub(float2 a, float2 b) { return padd(a, pmul(b, f2s(-1.0f))); }
+// Packed float32 arithmetic of the float32 pass: sm_100's builtins (the compiler pairs the
+// registers itself; contraction is welcome here).  a - b is one fused multiply-add.
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 
 // 8-neighbour sum of the pair with out-of-image neighbours as 0 (H's 'constant' border)
 __device__ __forceinline__ float2 lbf_hsum_edge(const LbRowF& U, const LbRowF& C, const LbRowF& D, bool T, bool B,
@@ -525,17 +530,17 @@ __device__ __forceinline__ void lbf_pair(const LbRowF& U, const LbRowF& C, const
   const float2 IIy = *reinterpret_cast<const float2*>(sc + LB_PL + o);
   const float2 II = *reinterpret_cast<const float2*>(sc + 2 * LB_PL + o);
   // vertical differences and sums at the pair and at the outer columns
-  const float2 vdu = psub(D.cu, U.cu), vsu = padd(U.cu, D.cu);
-  const float2 vdv = psub(D.cv, U.cv), vsv = padd(U.cv, D.cv);
-  const float2 vdo_u = psub(f2(D.lu, D.ru), f2(U.lu, U.ru));  // (left column, right column)
-  const float2 vdo_v = psub(f2(D.lv, D.rv), f2(U.lv, U.rv));
-  const float2 mdu = psub(f2(vdu.y, vdo_u.y), f2(vdo_u.x, vdu.x));  // 4 M
-  const float2 mdv = psub(f2(vdv.y, vdo_v.y), f2(vdo_v.x, vdv.x));
+  const float2 vdu = fsub2(D.cu, U.cu), vsu = fadd2(U.cu, D.cu);
+  const float2 vdv = fsub2(D.cv, U.cv), vsv = fadd2(U.cv, D.cv);
+  const float2 vdo_u = fsub2(f2(D.lu, D.ru), f2(U.lu, U.ru));  // (left column, right column)
+  const float2 vdo_v = fsub2(f2(D.lv, D.rv), f2(U.lv, U.rv));
+  const float2 mdu = fsub2(f2(vdu.y, vdo_u.y), f2(vdo_u.x, vdu.x));  // 4 M
+  const float2 mdv = fsub2(f2(vdv.y, vdo_v.y), f2(vdo_v.x, vdv.x));
   // centre-row neighbours of the pair
   const float2 Lu = f2(C.lu, C.cu.x), Ru = f2(C.cu.y, C.ru);
   const float2 Lv = f2(C.lv, C.cv.x), Rv = f2(C.cv.y, C.rv);
-  const float2 dtu = psub(Ru, Lu), dtv = psub(Rv, Lv);  // 2 D^T
-  const float2 hsv = padd(Lv, Rv);                       // F^T
+  const float2 dtu = fsub2(Ru, Lu), dtv = fsub2(Rv, Lv);  // 2 D^T
+  const float2 hsv = fadd2(Lv, Rv);                       // F^T
   float2 Hu, Hv;
   if (EDGE) {
     const bool T = gy == 0, B = gy == S.H - 1;
@@ -543,35 +548,35 @@ __device__ __forceinline__ void lbf_pair(const LbRowF& U, const LbRowF& C, const
     Hu = lbf_hsum_edge(U, C, D, T, B, L0, R0, L1, R1, false);
     Hv = lbf_hsum_edge(U, C, D, T, B, L0, R0, L1, R1, true);
   } else {
-    const float2 vso_u = padd(f2(U.lu, U.ru), f2(D.lu, D.ru));
-    const float2 vso_v = padd(f2(U.lv, U.rv), f2(D.lv, D.rv));
-    Hu = padd(padd(vso_u, f2s(__fadd_rn(vsu.x, vsu.y))), padd(Lu, Ru));
-    Hv = padd(padd(vso_v, f2s(__fadd_rn(vsv.x, vsv.y))), hsv);
+    const float2 vso_u = fadd2(f2(U.lu, U.ru), f2(D.lu, D.ru));
+    const float2 vso_v = fadd2(f2(U.lv, U.rv), f2(D.lv, D.rv));
+    Hu = fadd2(fadd2(vso_u, f2s(__fadd_rn(vsu.x, vsu.y))), fadd2(Lu, Ru));
+    Hv = fadd2(fadd2(vso_v, f2s(__fadd_rn(vsv.x, vsv.y))), hsv);
   }
-  const float2 a2 = pmul(IIx, f2s(0.5f)), a3 = pmul(IIy, f2s(0.5f)), a5 = pmul(II, f2s(0.25f));
+  const float2 a2 = fmul2(IIx, f2s(0.5f)), a3 = fmul2(IIy, f2s(0.5f)), a5 = fmul2(II, f2s(0.25f));
   const float2 h2 = f2s(S.h);
   // bu = 2 IIx D u + IIx D^T v + IIy D v + II F u + II M v + h H u + Ixt
   float2 bu = *reinterpret_cast<const float2*>(sc + 3 * LB_PL + o);
-  bu = pfma(h2, Hu, bu);
-  bu = pfma(a5, mdv, bu);
-  bu = pfma(II, vsu, bu);
-  bu = pfma(a3, vdv, bu);
-  bu = pfma(a2, dtv, bu);
-  bu = pfma(IIx, vdu, bu);
+  bu = ffma2(h2, Hu, bu);
+  bu = ffma2(a5, mdv, bu);
+  bu = ffma2(II, vsu, bu);
+  bu = ffma2(a3, vdv, bu);
+  bu = ffma2(a2, dtv, bu);
+  bu = ffma2(IIx, vdu, bu);
   // bv = IIy D u + IIx D^T u + 2 IIy D^T v + II M u + II F^T v + h H v + Iyt
   float2 bv = *reinterpret_cast<const float2*>(sc + 4 * LB_PL + o);
-  bv = pfma(h2, Hv, bv);
-  bv = pfma(a5, mdu, bv);
-  bv = pfma(II, hsv, bv);
-  bv = pfma(IIy, dtv, bv);
-  bv = pfma(a2, dtu, bv);
-  bv = pfma(a3, vdu, bv);
+  bv = ffma2(h2, Hv, bv);
+  bv = ffma2(a5, mdu, bv);
+  bv = ffma2(II, hsv, bv);
+  bv = ffma2(IIy, dtv, bv);
+  bv = ffma2(a2, dtu, bv);
+  bv = ffma2(a3, vdu, bv);
   const float2 B11 = *reinterpret_cast<const float2*>(sc + 5 * LB_PL + o);
   const float2 B12 = *reinterpret_cast<const float2*>(sc + 6 * LB_PL + o);
   const float2 B22 = *reinterpret_cast<const float2*>(sc + 7 * LB_PL + o);
   const float2 m1 = f2s(-1.0f);
-  const float2 nu = pmul(pfma(B11, bu, pmul(B12, bv)), m1);
-  const float2 nv = pmul(pfma(B12, bu, pmul(B22, bv)), m1);
+  const float2 nu = fmul2(ffma2(B11, bu, fmul2(B12, bv)), m1);
+  const float2 nv = fmul2(ffma2(B12, bu, fmul2(B22, bv)), m1);
   const bool in0 = S.gx0 < S.W, in1 = S.gx0 + 1 < S.W;
   if (S.ou) {
     *reinterpret_cast<float2*>(&S.ou[row][S.c0]) = nu;
@@ -587,7 +592,7 @@ __device__ __forceinline__ void lbf_pair(const LbRowF& U, const LbRowF& C, const
     }
   }
   if (own_row && S.own_col) {
-    const float2 eu = psub(nu, C.cu), ev = psub(nv, C.cv);
+    const float2 eu = fsub2(nu, C.cu), ev = fsub2(nv, C.cv);
     const float eu0 = in0 ? eu.x : 0.0f, ev0 = in0 ? ev.x : 0.0f;
     const float eu1 = in1 ? eu.y : 0.0f, ev1 = in1 ? ev.y : 0.0f;
     acc_u = __fmaf_rn(eu0, eu0, __fmaf_rn(eu1, eu1, acc_u));
