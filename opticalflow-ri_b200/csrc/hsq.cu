@@ -85,16 +85,21 @@ struct HqTile {
   static constexpr size_t SMEM = 7 * (size_t)PL * sizeof(float);
 };
 
+constexpr int HQ_THREADS = 256;  // threads per CTA of the queue kernel
+
+// One cell of sweep s (region index k); the loop over a thread's cells is unrolled so the
+// cells' independent arithmetic chains interleave.
 template <int RW, int RH, int T, bool EDGE, bool FAST>
-__device__ __forceinline__ void hq_sweep(const float* __restrict__ sfx, const float* __restrict__ sfy,
-                                         const float* __restrict__ sft, const float* su, const float* sv, float* du,
-                                         float* dv, int s, int x0, int y0, int H, int W, float a2) {
+__device__ __forceinline__ void hq_cell(int k, const float* __restrict__ sfx, const float* __restrict__ sfy,
+                                        const float* __restrict__ sft, const float* su, const float* sv, float* du,
+                                        float* dv, int s, int x0, int y0, int H, int W, float a2) {
   const double wc = (double)(1.0f / 12.0f), we = (double)(1.0f / 6.0f);
-  for (int k = threadIdx.x; k < RW * RH; k += blockDim.x) {
+  {
+    if (k >= RW * RH) return;
     const int r = k / RW, c = k - r * RW;
-    if (c < 1 + s || c >= RW - 1 - s || r < 1 + s || r >= RH - 1 - s) continue;
+    if (c < 1 + s || c >= RW - 1 - s || r < 1 + s || r >= RH - 1 - s) return;
     const int gx = x0 - T + c, gy = y0 - T + r;
-    if (EDGE && (gx < 0 || gx >= W || gy < 0 || gy >= H)) continue;
+    if (EDGE && (gx < 0 || gx >= W || gy < 0 || gy >= H)) return;
     int cm = c - 1, cp = c + 1, rm = r - 1, rp = r + 1;
     if (EDGE) {
       cm = mirror1(gx - 1, W) - (x0 - T);
@@ -133,6 +138,16 @@ __device__ __forceinline__ void hq_sweep(const float* __restrict__ sfx, const fl
     du[i] = __fsub_rn(ua, __fmul_rn(gxv, der));
     dv[i] = __fsub_rn(va, __fmul_rn(gyv, der));
   }
+}
+
+template <int RW, int RH, int T, bool EDGE, bool FAST>
+__device__ __forceinline__ void hq_sweep(const float* __restrict__ sfx, const float* __restrict__ sfy,
+                                         const float* __restrict__ sft, const float* su, const float* sv, float* du,
+                                         float* dv, int s, int x0, int y0, int H, int W, float a2) {
+#pragma unroll 4
+  for (int it = 0; it < (RW * RH + HQ_THREADS - 1) / HQ_THREADS; it++)
+    hq_cell<RW, RH, T, EDGE, FAST>(it * HQ_THREADS + (int)threadIdx.x, sfx, sfy, sft, su, sv, du, dv, s, x0, y0, H,
+                                   W, a2);
 }
 
 // Returns false when a result of the last pass is not finite.
@@ -200,7 +215,7 @@ __device__ bool hq_sweep_item(const HsqPair& P, int pass, int tile, float* sm) {
 }
 
 template <int RW, int RH, int T, bool FAST>
-__global__ void __launch_bounds__(256) hsq_kernel(const HsqPair* __restrict__ pairs, int npairs,
+__global__ void __launch_bounds__(HQ_THREADS) hsq_kernel(const HsqPair* __restrict__ pairs, int npairs,
                                                   unsigned int tiles_total, int max_passes,
                                                   unsigned long long* ticket, unsigned int* done, int* status,
                                                   long long wait_limit, int* err_flag) {
@@ -309,10 +324,10 @@ cudaError_t hsq_launch(bool fast, int grid, const HsqPair* pairs, int n, unsigne
                        : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false>), G::SMEM);
   if (e != cudaSuccess) return e;
   if (fast)
-    hsq_kernel<RW, RH, T, true><<<grid, 256, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
+    hsq_kernel<RW, RH, T, true><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
                                                             wait_limit, err_flag);
   else
-    hsq_kernel<RW, RH, T, false><<<grid, 256, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
+    hsq_kernel<RW, RH, T, false><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
                                                              wait_limit, err_flag);
   return cudaGetLastError();
 }
@@ -323,8 +338,8 @@ int hsq_resident(bool fast, int* per_sm) {
   cudaError_t e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true>), G::SMEM)
                        : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false>), G::SMEM);
   if (e != cudaSuccess) return -1;
-  e = fast ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, hsq_kernel<RW, RH, T, true>, 256, G::SMEM)
-           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, hsq_kernel<RW, RH, T, false>, 256, G::SMEM);
+  e = fast ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, hsq_kernel<RW, RH, T, true>, HQ_THREADS, G::SMEM)
+           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, hsq_kernel<RW, RH, T, false>, HQ_THREADS, G::SMEM);
   return e == cudaSuccess ? 0 : -1;
 }
 }  // namespace
