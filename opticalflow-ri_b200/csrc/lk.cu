@@ -20,6 +20,10 @@ namespace ofb {
 constexpr int LK_PT = 8;            // pixel tile edge
 constexpr int LK_G = LK_PT + 31;    // gradient positions per axis
 constexpr int LK_I = LK_G + 2;      // intensity positions per axis
+// Row strides of the staged patches: a warp reads 4 rows of 8 consecutive columns at once,
+// so a stride of 8 or 24 (mod 32) banks puts the 4 rows in disjoint banks.
+constexpr int LK_IP = 56, LK_GP = 40;
+static_assert(LK_IP >= LK_I && LK_GP >= LK_G && LK_IP % 32 == 24 && LK_GP % 32 == 8, "patch strides");
 // J region staged per CTA for the Newton steps: LK_JR x LK_JR texels centred on the tile's
 // mean displaced window, row stride LK_JP (72: the 4 rows a warp reads at once fall in
 // distinct banks).  Texels hold clamped-coordinate values, so a bilinear footprint inside
@@ -113,22 +117,22 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
                                                        float* __restrict__ U, float* __restrict__ V, int H, int W,
                                                        int pitch, LkParams p, uint8_t* __restrict__ status,
                                                        float* __restrict__ err) {
-  __shared__ float sI[LK_I * LK_I];
-  __shared__ float sDx[LK_G * LK_G], sDy[LK_G * LK_G];
+  __shared__ float sI[LK_I * LK_IP];
+  __shared__ float sDx[LK_G * LK_GP], sDy[LK_G * LK_GP];
   const int i0 = blockIdx.y * LK_PT, j0 = blockIdx.x * LK_PT;
   const int oy = i0 - p.hw - 1, ox = j0 - p.hw - 1;  // image position of sI[0][0]
   for (int t = threadIdx.x; t < LK_I * LK_I; t += blockDim.x) {
     int ly = t / LK_I, lx = t - ly * LK_I;
-    sI[t] = I[(size_t)clampi(oy + ly, 0, H - 1) * pitch + clampi(ox + lx, 0, W - 1)];
+    sI[ly * LK_IP + lx] = I[(size_t)clampi(oy + ly, 0, H - 1) * pitch + clampi(ox + lx, 0, W - 1)];
   }
   __syncthreads();
   for (int t = threadIdx.x; t < LK_G * LK_G; t += blockDim.x) {
     int gy = t / LK_G, gx = t - gy * LK_G;
-    const float* c = sI + (gy + 1) * LK_I + gx + 1;
-#define P(dy, dx) c[(dy) * LK_I + (dx)]
-    sDx[t] = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(-1, 1), P(1, 1)), P(-1, -1)), P(1, -1)), 3.0f,
+    const float* c = sI + (gy + 1) * LK_IP + gx + 1;
+#define P(dy, dx) c[(dy) * LK_IP + (dx)]
+    sDx[gy * LK_GP + gx] = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(-1, 1), P(1, 1)), P(-1, -1)), P(1, -1)), 3.0f,
                        __fmul_rn(__fsub_rn(P(0, 1), P(0, -1)), 10.0f));
-    sDy[t] = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(1, -1), P(1, 1)), P(-1, -1)), P(-1, 1)), 3.0f,
+    sDy[gy * LK_GP + gx] = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(1, -1), P(1, 1)), P(-1, -1)), P(-1, 1)), 3.0f,
                        __fmul_rn(__fsub_rn(P(1, 0), P(-1, 0)), 10.0f));
 #undef P
   }
@@ -194,7 +198,7 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
         for (int tx = 0; tx < 4; tx++) {
           float w = __fmul_rn(wx[tx], wy[ty]);
           if (w == 0.f) continue;
-          int g = (gyb + ty * 8 + yy) * LK_G + gxb + tx * 8 + xid;
+          int g = (gyb + ty * 8 + yy) * LK_GP + gxb + tx * 8 + xid;
           // w is 1 here (the tile weights are products of 0 / 1 values and w == 0 is
           // skipped), so the reference's multiplications by w are exact identities
           float dx = sDx[g], dy = sDy[g];
@@ -263,8 +267,8 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
 #pragma unroll
           for (int tx = 0; tx < 4; tx++) {
             if (!((act >> (16 * v + 4 * ty + tx)) & 1u)) continue;  // tile weight 0
-            int g = (gyb + ty * 8 + yy) * LK_G + gxb + tx * 8 + xid;
-            float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_I + gxb + tx * 8 + xid + 1];
+            int g = (gyb + ty * 8 + yy) * LK_GP + gxb + tx * 8 + xid;
+            float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_IP + gxb + tx * 8 + xid + 1];
             float t00, t10, t01, t11;
             if (((inx >> tx) & (iny >> (4 * v + ty))) & 1u) {
               const float* q = sJ + yr[v][ty] * LK_JP + xr[tx];
@@ -321,7 +325,7 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
           if ((gb & 4) && !(bx[1] < p.ws)) continue;
           if ((gb & 8) && !(by[1] < p.ws)) continue;
           float w = __fmul_rn(wx[tx], wy[ty]);
-          float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_I + gxb + tx * 8 + xid + 1];
+          float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_IP + gxb + tx * 8 + xid + 1];
           float Jv = lk_bilinear_s(sJ, J, H, W, pitch, lx[tx], ly[v][ty], jox, joy);
           float d = __fmul_rn(__fsub_rn(__fdiv_rn(__fmaf_rn(Jv, 16384.f, 256.f), 512.f),
                                         __fdiv_rn(__fmaf_rn(Iv, 16384.f, 256.f), 512.f)),
