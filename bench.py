@@ -532,10 +532,14 @@ def _fp32_peak_tflops(clk):
     return 148 * FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12
 
 
-def _pair_throughput(spec_fn, frames, nstreams, flush, reps=5):
-    """Device pairs/s of a list of uint8 frame pairs through PairBatch (one CUDA graph)."""
-    from ofb200.batch import PairBatch
-    batch = PairBatch([spec_fn() for _ in frames], streams=nstreams)
+def _pair_throughput(spec_fn, frames, nstreams, flush, reps=5, hs_shape=None):
+    """Device pairs/s of a list of uint8 frame pairs through PairBatch (one CUDA graph), or,
+    with hs_shape, through HsGroup (every Horn-Schunck solve in one persistent launch)."""
+    from ofb200.batch import HsGroup, PairBatch
+    if hs_shape is None:
+        batch = PairBatch([spec_fn() for _ in frames], streams=nstreams)
+    else:
+        batch = HsGroup([spec_fn() for _ in frames], tile_shape=hs_shape)
     for _ in range(3):
         batch.run(frames)
     import torch
@@ -589,10 +593,16 @@ def run_configs(args, rank, world, dev, flush):
     hs_spec = lambda: PairSpec(3.4, lambda: HS.HSOpticalFlowAlgoAdapter([21], 600), 1, 1, key=("hs",))  # noqa: E731
     lk_spec = lambda: PairSpec(2.0, lambda: LK.denseLucasKanade_PyCl(Niter=5, halfWindow=13), 2, 1, 0.48,  # noqa
                                key=("lk",))
-    _, hs_ms = _pair_throughput(hs_spec, hs_frames, nst, flush)
+    # Horn-Schunck: the batch runner's path (every solve in one persistent launch, tile shape
+    # tuned on these pairs), beside per-pair graphs on 8 streams for comparison
+    from ofb200.batch import tune_hs_shape
+    hs_shape, _ = tune_hs_shape(hs_frames, reps=2)
+    _, hs_ms = _pair_throughput(hs_spec, hs_frames, nst, flush, hs_shape=hs_shape)
+    _, hs_graph_ms = _pair_throughput(hs_spec, hs_frames, nst, flush)
     _, lk_ms = _pair_throughput(lk_spec, lk_frames, nst, flush)
     clk = clocks.stop() if clocks else None
     hs_ms, lk_ms = max_over_ranks(hs_ms, dev), max_over_ranks(lk_ms, dev)
+    hs_graph_ms = max_over_ranks(hs_graph_ms, dev)
     peak, peak_kind = peaks()
     hs_bytes = (600 * 24.0 + 20.0 + 8.0) * 256 * 256  # sweeps, derivatives, prefilter (per pair)
     lk_px = 512 * 512 + 256 * 256
@@ -610,7 +620,8 @@ def run_configs(args, rank, world, dev, flush):
                                    "pairs/s scaled by the pixel ratio"}}
     out["hs256"] = {"workload": "PyHSchunck_Fs3_4 Horn-Schunck, 256x256 Poiseuille pairs, 600 sweeps",
                     "value": n_hs * world / (hs_ms * 1e-3), "unit": "pairs/s", "ms_per_step": hs_ms,
-                    "pairs_per_step_per_gpu": n_hs, "streams": nst,
+                    "pairs_per_step_per_gpu": n_hs, "path": f"one persistent launch (tile shape {hs_shape})",
+                    "per_pair_graphs_8_streams": {"value": n_hs * world / (hs_graph_ms * 1e-3), "ms_per_step": hs_graph_ms},
                     "roofline": {"bound": "hbm", "achieved": n_hs * hs_bytes / (hs_ms * 1e-3) / 1e9, "peak": peak,
                                  "unit": "GB/s", "frac": n_hs * hs_bytes / (hs_ms * 1e-3) / 1e9 / peak,
                                  "peak_kind": peak_kind, "algorithmic_bytes_per_pair": hs_bytes},
