@@ -9,8 +9,11 @@ noise 2 DN).  One step = `--pairs` frame pairs through the whole pipeline, sprea
 
   value : pairs/s with the frames already resident in HBM (device-timed, CUDA events),
           aggregated over all ranks (pairs / max-over-ranks time).
-  e2e   : pairs/s through the reference-facing API (genericPyramidalOpticalFlow with
-          numpy float32 frames in and numpy U, V out: host<->device copies inside).
+  e2e   : pairs/s from host memory to host memory: the step's pairs as pinned uint8 frames
+          through ofb200.batch.HostBatch (uploads, the batch graph and the downloads of U, V
+          into pinned buffers, two steps in flight), wall clock; e2e.single_call is the
+          one-pair drop-in call (genericPyramidalOpticalFlow, numpy float32 frames in, numpy
+          U, V out) back to back.
   roofline : the Liu-Shen solves of one step (the dominant kernel): --pairs solves at
           1024^2 running concurrently on --streams streams, as they do in the step (their
           working set, 60 MB each, exceeds the 126 MB L2), algorithmic bytes = (24 B x
@@ -47,8 +50,9 @@ WORKLOAD = "LiuSE_Farneback_Fs0_0_PyrLvls2 1024x1024 random-Fourier PIV pairs"
 L2_BYTES = 126 * 2 ** 20
 REF_BUDGET_S = 90.0
 # DRAM bytes (read + write) of one 60-sweep Liu-Shen solve at 1024^2, summed over its
-# launches from one ncu capture (profiles/ls_solve_traffic_1024.txt; cold cache per launch)
-NCU_LS_TRAFFIC = {("exact", 1024): 663.48e6}
+# launches from one ncu capture per arithmetic (profiles/ls_solve_traffic_1024.txt; cold cache
+# per launch)
+NCU_LS_TRAFFIC = {("exact", 1024): 663.48e6, ("fast", 1024): 663.49e6}
 
 
 def parse():
@@ -123,12 +127,14 @@ def run_hs_only(args):
     out = {"mode": "hs", "size": args.size, "sweeps": 600}
     U, V = z.clone(), z.clone()
     out["of_hs_solve_ms"] = timeit(lambda: ops.hs_solve(a, b, U.zero_(), V.zero_(), 21.0, 600))
-    for k, shp in enumerate(ops.hs_batch_shapes()):
-        for ar in ("exact", "fast"):
-            U2, V2 = z.clone(), z.clone()
-            out[f"of_hs_batch_{ar}_shape{k}_{shp[0]}x{shp[1]}t{shp[2]}_ms"] = timeit(
-                lambda: ops.hs_batch([(a, b, U2.zero_(), V2.zero_(), 21.0, 600)], tile_shape=k, arithmetic=ar))
-            out[f"{ar}_shape{k}_maxdiff"] = float(max((U2 - U).abs().max().item(), (V2 - V).abs().max().item()))
+    for sched in ("queue", "resident"):
+        for k, shp in enumerate(ops.hs_batch_shapes()):
+            for ar in ("exact", "fast"):
+                U2, V2 = z.clone(), z.clone()
+                tag = f"{sched}_{ar}_shape{k}_{shp[0]}x{shp[1]}t{shp[2]}"
+                out[f"of_hs_batch_{tag}_ms"] = timeit(lambda: ops.hs_batch(
+                    [(a, b, U2.zero_(), V2.zero_(), 21.0, 600)], tile_shape=k, arithmetic=ar, schedule=sched))
+                out[f"{tag}_maxdiff"] = float(max((U2 - U).abs().max().item(), (V2 - V).abs().max().item()))
     print(json.dumps(out))
 
 
@@ -169,24 +175,16 @@ def run_lk_only(args):
 
 
 def run_e2e_only(args):
-    """The drop-in call alone (genericPyramidalOpticalFlow with numpy float32 frames in and
-    numpy U, V out), --warmup + --steps calls, wall clock per call."""
+    """The end-to-end figures alone: --pairs pairs per step through HostBatch (pinned uint8
+    frames in, numpy U, V out, two steps in flight) and the one-pair drop-in call
+    (genericPyramidalOpticalFlow, numpy float32 frames in and numpy U, V out); wall clock."""
     import torch
     pairs = make_pairs(args.unique, args.size)
     host = [(a.astype(np.float32), b.astype(np.float32)) for a, b, _, _ in pairs]
-    import Farneback_PyCL as F
-    import GenericPyramidalOpticalFlow as G
-    import PhysicsBasedOpticalFlowLiuShen as LS
-    ms = []
-    for r in range(args.warmup + args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        G.genericPyramidalOpticalFlow(*host[r % len(host)], 0, F.Farneback_PyCL(), 2, 1, 0.48,
-                                      LS.LiuShenOpticalFlowAlgoAdapter(10))
-        if r >= args.warmup:
-            ms.append((time.perf_counter() - t0) * 1e3)
-    print(json.dumps({"mode": "e2e", "size": args.size, "ms_per_call": float(np.mean(ms)),
-                      "pairs_per_s": 1e3 / float(np.mean(ms))}))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    hb = e2e_host_batch(args, pairs, dev, 1, lambda: None)
+    one = e2e_single_call(host, 1, lambda: None, calls=max(2, args.steps))
+    print(json.dumps({"mode": "e2e", "size": args.size, "host_batch": hb, "single_call": one}))
 
 
 def run_fb_only(args):
@@ -328,6 +326,68 @@ def pipeline_dev(a, b):
     return G.genericPyramidalOpticalFlow(a, b, 0, F.Farneback_PyCL(), 2, 1, 0.48, LS.LiuShenOpticalFlowAlgoAdapter(10))
 
 
+def e2e_host_batch(args, pairs, dev, world, barrier):
+    """pairs/s of --steps steps of --pairs pairs from pinned host uint8 frames to numpy U, V
+    through ofb200.batch.HostBatch, wall clock, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    import Farneback_PyCL as F
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    from ofb200.batch import HostBatch, PairSpec
+    spec = PairSpec(0, lambda: F.Farneback_PyCL(), 2, 1, 0.48, lambda: LS.LiuShenOpticalFlowAlgoAdapter(10),
+                    key=("fbls",))
+    hb = HostBatch([spec] * args.pairs, streams=max(1, args.streams), depth=2)
+    pinned = [(torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()) for a, b, _, _ in pairs]
+    step_host = [pinned[i % len(pinned)] for i in range(args.pairs)]
+    for _ in range(max(3, args.warmup)):
+        hb.run(step_host)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    prev = None
+    for _ in range(args.steps):
+        t = hb.submit(step_host)
+        if prev is not None:
+            hb.result(prev)
+        prev = t
+    hb.result(prev)
+    dt = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(dt, op=dist.ReduceOp.MAX)
+    N = args.size * args.size
+    return {"value": args.pairs * args.steps * world / float(dt.item()), "unit": "pairs/s",
+            "h2d_bytes_per_step": sum(a.numel() + b.numel() for a, b in step_host),
+            "d2h_bytes_per_step": 2 * N * 4 * args.pairs,
+            "api": "ofb200.batch.HostBatch: pinned uint8 frames in, numpy float32 U, V out, 2 steps in flight",
+            "timing": "wall clock over the steps, max over ranks"}
+
+
+def e2e_single_call(host_frames, world, barrier, calls):
+    """pairs/s of the one-pair drop-in call (genericPyramidalOpticalFlow with numpy float32
+    frames in and numpy U, V out), called back to back, wall clock."""
+    import torch
+    import torch.distributed as dist
+    import Farneback_PyCL as F
+    import GenericPyramidalOpticalFlow as G
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    for i in range(2):
+        G.genericPyramidalOpticalFlow(*host_frames[i % len(host_frames)], 0, F.Farneback_PyCL(), 2, 1, 0.48,
+                                      LS.LiuShenOpticalFlowAlgoAdapter(10))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(calls):
+        G.genericPyramidalOpticalFlow(*host_frames[i % len(host_frames)], 0, F.Farneback_PyCL(), 2, 1, 0.48,
+                                      LS.LiuShenOpticalFlowAlgoAdapter(10))
+    dt = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=torch.cuda.current_device())
+    if world > 1:
+        dist.all_reduce(dt, op=dist.ReduceOp.MAX)
+    N = host_frames[0][0].size
+    return {"value": calls * world / float(dt.item()), "unit": "pairs/s", "h2d_bytes_per_call": 2 * N * 4,
+            "d2h_bytes_per_call": 2 * N * 4,
+            "api": "GenericPyramidalOpticalFlow.genericPyramidalOpticalFlow, numpy float32 frames in, numpy out"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -394,28 +454,13 @@ def run_ours(args, rank, world, local_rank):
     # size, concurrently on --streams streams, as in the step), graph-replayed
     roof = ls_step_roofline(args, frames, flush)
 
-    # end to end through the reference-facing API, host buffers
+    # end to end from host buffers to host results: the step's pairs as pinned uint8 frames
+    # through HostBatch (frames up on one copy stream, the batch graph, U and V down into
+    # pinned buffers on another; two steps in flight), wall clock over --steps steps
     e2e = None
     if not args.no_e2e:
-        import Farneback_PyCL as F
-        import GenericPyramidalOpticalFlow as G
-        import PhysicsBasedOpticalFlowLiuShen as LS
-        for i in range(2):
-            G.genericPyramidalOpticalFlow(*host_frames[i % len(host_frames)], 0, F.Farneback_PyCL(), 2, 1, 0.48,
-                                          LS.LiuShenOpticalFlowAlgoAdapter(10))
-        barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        n_e2e = max(2, args.pairs)
-        for i in range(n_e2e):
-            U, V = G.genericPyramidalOpticalFlow(*host_frames[i % len(host_frames)], 0, F.Farneback_PyCL(), 2, 1,
-                                                 0.48, LS.LiuShenOpticalFlowAlgoAdapter(10))
-        dt = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(dt, op=dist.ReduceOp.MAX)
-        e2e = {"value": n_e2e * world / float(dt.item()), "unit": "pairs/s",
-               "h2d_bytes_per_step": 2 * N * 4 * args.pairs, "d2h_bytes_per_step": 2 * N * 4 * args.pairs}
-
+        e2e = e2e_host_batch(args, pairs, dev, world, barrier)
+        e2e["single_call"] = e2e_single_call(host_frames, world, barrier, calls=max(2, args.pairs))
     learned = None if args.no_learned else run_learned(args, step_frames, pairs, dev, flush, world,
                                                            pairs_total_ms=total_ms)
     configs = None if args.no_configs else run_configs(args, rank, world, dev, flush)

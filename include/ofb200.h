@@ -149,10 +149,18 @@ typedef struct OfTuning {
   int tile_shape;
   int streams;   /* host-side concurrency of callers that use streams; unused by the kernels */
   int hs_arithmetic; /* OF_HS_EXACT (bit-exact with the reference) or OF_HS_FAST (float32 averaging) */
-  int reserved;
+  int hs_schedule;   /* OF_HS_SCHED_*: how the persistent Horn-Schunck launch hands out its tiles */
 } OfTuning;
 #define OF_HS_EXACT 0
 #define OF_HS_FAST 1
+/* AUTO: RESIDENT when every tile of the launch can have a resident CTA of its own, else
+ * QUEUE.  QUEUE: (pass, pair, tile) items from a device ticket counter.  RESIDENT: one CTA
+ * per tile for the whole solve, its derivative planes and flow kept in shared memory, only
+ * the halo ring exchanged through global memory (OF_ERR_INVALID when the tiles outnumber
+ * the resident CTAs).  The schedules give identical results. */
+#define OF_HS_SCHED_AUTO 0
+#define OF_HS_SCHED_QUEUE 1
+#define OF_HS_SCHED_RESIDENT 2
 
 /* One Horn-Schunck pair of a batch: DEVICE planes of H x W float32 with row pitch `pitch`;
  * U, V hold the initial flow and receive the result. */

@@ -45,9 +45,9 @@ struct HsqPair {
 
 __device__ __forceinline__ double hq_acc(double a, float v, double w) { return __fma_rn((double)v, w, a); }
 
-// Derivatives of one pixel (hs_deriv_kernel's arithmetic) and the copy of the initial flow.
-// Returns false when a frame sample of the pixel is not finite.
-__device__ __forceinline__ bool hq_deriv_px(const HsqPair& P, int y, int x) {
+// Derivatives of one pixel (hs_deriv_kernel's arithmetic).  Returns false when a frame
+// sample of the pixel is not finite.
+__device__ __forceinline__ bool hq_deriv(const HsqPair& P, int y, int x, float& fx, float& fy, float& ft) {
   const int H = P.H, W = P.W, pitch = P.pitch;
   int y1 = mirror1(y + 1, H), x1 = mirror1(x + 1, W);
   size_t i00 = (size_t)y * pitch + x, i01 = (size_t)y * pitch + x1, i10 = (size_t)y1 * pitch + x,
@@ -69,12 +69,61 @@ __device__ __forceinline__ bool hq_deriv_px(const HsqPair& P, int y, int x) {
   float gt0 = (float)t;
   t = hq_acc(hq_acc(hq_acc(hq_acc(0.0, a00, -0.25), a01, -0.25), a10, -0.25), a11, -0.25);
   float gt1 = (float)t;
-  __stcg(P.fx + i00, __fadd_rn(gx1, gx0));
-  __stcg(P.fy + i00, __fadd_rn(gy1, gy0));
-  __stcg(P.ft + i00, __fadd_rn(gt0, gt1));
+  fx = __fadd_rn(gx1, gx0);
+  fy = __fadd_rn(gy1, gy0);
+  ft = __fadd_rn(gt0, gt1);
+  return isfinite(a00) && isfinite(b00);
+}
+
+// The derivative planes of one pixel into the workspace, and the copy of its initial flow.
+__device__ __forceinline__ bool hq_deriv_px(const HsqPair& P, int y, int x) {
+  float fx, fy, ft;
+  const bool ok = hq_deriv(P, y, x, fx, fy, ft);
+  const size_t i00 = (size_t)y * P.pitch + x;
+  __stcg(P.fx + i00, fx);
+  __stcg(P.fy + i00, fy);
+  __stcg(P.ft + i00, ft);
   __stcg(P.U0 + i00, __ldcg(P.U + i00));
   __stcg(P.V0 + i00, __ldcg(P.V + i00));
-  return isfinite(a00) && isfinite(b00);
+  return ok;
+}
+
+// Called by all of warp 0: lanes 0-8 poll, in parallel, the finished-stage counters of the
+// tile and its (up to) 8 neighbours until each reaches `need`; lane 9 reads the pair's status
+// word.  Every poll gives up after `wait_limit` rounds, which marks the pair
+// (OF_ST_WAIT_TIMEOUT) and the launch's error flag.  Returns 1 when the item may run: no
+// wait gave up and the pair had not failed before.  Lane 0 issues the acquire fence.
+__device__ __forceinline__ int hq_wait(const unsigned int* done, unsigned int tile0, int tile, int ntx, int nty,
+                                       unsigned int need, long long wait_limit, int* status_i, int* err_flag) {
+  const int lane = threadIdx.x & 31;
+  bool gave_up = false, failed_before = false;
+  if (lane < 9) {
+    const int ty = tile / ntx, tx = tile - ty * ntx;
+    const int yy = ty + lane / 3 - 1, xx = tx + lane % 3 - 1;
+    if (need > 0 && yy >= 0 && yy < nty && xx >= 0 && xx < ntx) {
+      const volatile unsigned int* c = done + tile0 + yy * ntx + xx;
+      long long k = 0;
+      while (*c < need) {
+        if (++k > wait_limit) {
+          gave_up = true;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+  } else if (lane == 9) {
+    failed_before = (*(volatile int*)status_i & OF_ST_WAIT_TIMEOUT) != 0;
+  }
+  const bool timeout = __any_sync(0xffffffffu, gave_up);
+  const bool before = __any_sync(0xffffffffu, failed_before);
+  if (lane == 0) {
+    if (timeout && !before) {
+      atomicOr(status_i, OF_ST_WAIT_TIMEOUT);
+      atomicExch(err_flag, 1);
+    }
+    __threadfence();  // acquire: the neighbours' stores are visible from here on
+  }
+  return !(timeout || before);
 }
 
 // Up to T sweeps on one tile: region RW x RH = (TW + 2T) x (TH + 2T) in shared memory,
@@ -214,6 +263,16 @@ __device__ bool hq_sweep_item(const HsqPair& P, int pass, int tile, float* sm) {
   return finite || p != np - 1;
 }
 
+// The pair whose tiles hold global tile index r (tile0 ascending).
+__device__ __forceinline__ int hq_pair_of(const HsqPair* __restrict__ pairs, int npairs, unsigned int r) {
+  int lo = 0, hi = npairs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pairs[mid].tile0 <= r) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 template <int RW, int RH, int T, bool FAST>
 __global__ void __launch_bounds__(HQ_THREADS) hsq_kernel(const HsqPair* __restrict__ pairs, int npairs,
                                                   unsigned int tiles_total, int max_passes,
@@ -224,50 +283,31 @@ __global__ void __launch_bounds__(HQ_THREADS) hsq_kernel(const HsqPair* __restri
   __shared__ int s_run, s_pair;
   const unsigned long long nitems = (unsigned long long)tiles_total * (unsigned long long)max_passes;
   using G = HqTile<RW, RH, T>;
+  // thread 0 holds the next ticket while the current item runs (its atomic's latency is
+  // hidden); an item still only waits for items with smaller tickets
+  unsigned long long next = 0;
+  if (threadIdx.x == 0) next = atomicAdd(ticket, 1ull);
   for (;;) {
-    if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1ull);
+    if (threadIdx.x == 0) {
+      s_item = next;
+      if (next < nitems) next = atomicAdd(ticket, 1ull);
+    }
     __syncthreads();
     const unsigned long long n = s_item;
     if (n >= nitems) break;
     const int pass = (int)(n / tiles_total);
     const unsigned int r = (unsigned int)(n - (unsigned long long)pass * tiles_total);
-    if (threadIdx.x == 0) {  // the pair whose tiles hold ticket offset r (tile0 ascending)
-      int lo = 0, hi = npairs - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (pairs[mid].tile0 <= r) lo = mid; else hi = mid - 1;
-      }
-      s_pair = lo;
-    }
+    if (threadIdx.x == 0) s_pair = hq_pair_of(pairs, npairs, r);
     __syncthreads();
     const int i = s_pair;
     const HsqPair& P = pairs[i];
     const int tile = (int)(r - P.tile0);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+      // this tile and its neighbours must have finished pass - 1 (counters of passes done)
       int run = pass < P.passes;
-      if (run && (((volatile int*)status)[i] & OF_ST_WAIT_TIMEOUT)) run = 0;  // the pair already failed
-      if (run && pass > 0) {
-        // this tile and its neighbours must have finished pass - 1 (counters of passes done)
-        const int ty = tile / P.tx, tx = tile - ty * P.tx, nty = P.tiles / P.tx;
-        long long k = 0;
-        for (int dy = -1; dy <= 1 && run; dy++)
-          for (int dx = -1; dx <= 1 && run; dx++) {
-            const int yy = ty + dy, xx = tx + dx;
-            if (yy < 0 || yy >= nty || xx < 0 || xx >= P.tx) continue;
-            const unsigned int* c = done + P.tile0 + yy * P.tx + xx;
-            while (*(volatile const unsigned int*)c < (unsigned int)pass) {
-              if (++k > wait_limit) {
-                atomicOr(status + i, OF_ST_WAIT_TIMEOUT);
-                atomicExch(err_flag, 1);
-                run = 0;
-                break;
-              }
-              __nanosleep(64);
-            }
-          }
-        __threadfence();  // acquire: the neighbours' stores are visible from here on
-      }
-      s_run = run;
+      if (run) run = hq_wait(done, P.tile0, tile, P.tx, P.tiles / P.tx, (unsigned int)pass, wait_limit, status + i,
+                             err_flag);
+      if (threadIdx.x == 0) s_run = run;
     }
     __syncthreads();
     bool ok = true;
@@ -288,6 +328,124 @@ __global__ void __launch_bounds__(HQ_THREADS) hsq_kernel(const HsqPair* __restri
     if (threadIdx.x == 0 && pass < P.passes) {
       __threadfence();  // release
       atomicAdd(done + P.tile0 + tile, 1u);
+    }
+  }
+}
+
+// The resident schedule, for launches where every tile gets a CTA of its own (all CTAs
+// resident): CTA b owns global tile b for the whole solve and keeps its region on chip.
+// Stage 0 computes the derivative planes of the WHOLE region (owned tile and halo: they
+// depend on the frames only) and loads the region's initial flow; both stay in shared
+// memory.  Stage s >= 1 runs up to T sweeps as a queue item of pass s does, but only the
+// halo ring comes from global memory (the neighbours' results of stage s - 1); the owned
+// part is already in shared memory, where the previous stage's T (even) sweeps left it.
+// The owned tile is published every stage.  Waits and counters are the queue kernel's: a
+// stage waits for its own and its neighbours' counters to reach s, which also orders every
+// overwrite of a ping-pong buffer (or of the initial U, V at stage 1) after the neighbours'
+// reads of it.
+template <int RW, int RH, int T, bool FAST>
+__global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restrict__ pairs, int npairs,
+                                                  unsigned int* done, int* status, long long wait_limit,
+                                                  int* err_flag) {
+  static_assert(T % 2 == 0, "a full stage must leave its result in the first buffer");
+  extern __shared__ float hq_sm[];
+  __shared__ int s_pair, s_run;
+  using G = HqTile<RW, RH, T>;
+  const unsigned int gtile = blockIdx.x;
+  if (threadIdx.x == 0) s_pair = hq_pair_of(pairs, npairs, gtile);
+  __syncthreads();
+  const int i = s_pair;
+  const HsqPair& P = pairs[i];
+  const int tile = (int)(gtile - P.tile0);
+  const int ty = tile / P.tx, tx = tile - ty * P.tx;
+  const int x0 = tx * G::TW, y0 = ty * G::TH;
+  const int H = P.H, W = P.W, pitch = P.pitch, np = P.passes - 1, nty = P.tiles / P.tx;
+  float* sfx = hq_sm;
+  float* sfy = sfx + G::PL;
+  float* sft = sfy + G::PL;
+  float* const bu0 = sft + G::PL;
+  float* const bv0 = sft + 2 * G::PL;
+  float* const bu1 = sft + 3 * G::PL;
+  float* const bv1 = sft + 4 * G::PL;
+  const bool edge = x0 < T || y0 < T || x0 + G::TW + T > W || y0 + G::TH + T > H;
+  // stage 0
+  bool ok = true;
+  for (int k = threadIdx.x; k < G::PL; k += blockDim.x) {
+    const int r = k / RW, c = k - r * RW;
+    const int gy = y0 - T + r, gx = x0 - T + c;
+    if (gy < 0 || gy >= H || gx < 0 || gx >= W) continue;  // never read
+    float fx, fy, ft;
+    const bool f = hq_deriv(P, gy, gx, fx, fy, ft);
+    sfx[k] = fx;
+    sfy[k] = fy;
+    sft[k] = ft;
+    const size_t gi = (size_t)gy * pitch + gx;
+    bu0[k] = __ldcg(P.U + gi);
+    bv0[k] = __ldcg(P.V + gi);
+    if (r >= T && r < T + G::TH && c >= T && c < T + G::TW) ok = ok && f;  // each pixel checked once
+  }
+  int bad = __syncthreads_or(!ok);
+  if (threadIdx.x == 0) {
+    if (bad) atomicOr(status + i, OF_ST_NONFINITE_INPUT);
+    __threadfence();  // release: this tile's reads of the initial U, V are done
+    atomicAdd(done + gtile, 1u);
+  }
+  for (int p = 0; p < np; p++) {
+    const int stage = p + 1;
+    if (threadIdx.x < 32) {
+      const int run = hq_wait(done, P.tile0, tile, P.tx, nty, (unsigned int)stage, wait_limit, status + i, err_flag);
+      if (threadIdx.x == 0) s_run = run;
+    }
+    __syncthreads();
+    ok = true;
+    if (s_run) {
+      const bool to_uv = ((np - 1 - p) & 1) == 0;  // the last stage writes U, V
+      float* dstu = to_uv ? P.U : P.Ub;
+      float* dstv = to_uv ? P.V : P.Vb;
+      if (p > 0) {  // halo ring: the neighbours' results of the previous stage
+        const float* srcu = to_uv ? P.Ub : P.U;
+        const float* srcv = to_uv ? P.Vb : P.V;
+        for (int k = threadIdx.x; k < G::PL; k += blockDim.x) {
+          const int r = k / RW, c = k - r * RW;
+          if (r >= T && r < T + G::TH && c >= T && c < T + G::TW) continue;  // owned: on chip
+          const int gy = y0 - T + r, gx = x0 - T + c;
+          if (gy < 0 || gy >= H || gx < 0 || gx >= W) continue;
+          const size_t gi = (size_t)gy * pitch + gx;
+          bu0[k] = __ldcg(srcu + gi);
+          bv0[k] = __ldcg(srcv + gi);
+        }
+        __syncthreads();
+      }
+      const int nsw = min(T, P.niter - p * T);
+      for (int s = 0; s < nsw; s++) {
+        const bool q = s & 1;
+        float* iu = q ? bu1 : bu0;
+        float* iv = q ? bv1 : bv0;
+        float* ou = q ? bu0 : bu1;
+        float* ov = q ? bv0 : bv1;
+        if (edge)
+          hq_sweep<RW, RH, T, true, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
+        else
+          hq_sweep<RW, RH, T, false, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
+        __syncthreads();
+      }
+      const float* fu = (nsw & 1) ? bu1 : bu0;
+      const float* fv = (nsw & 1) ? bv1 : bv0;
+      for (int k = threadIdx.x; k < G::TW * G::TH; k += blockDim.x) {
+        const int r = k / G::TW, c = k - r * G::TW;
+        const int y = y0 + r, x = x0 + c;
+        if (y >= H || x >= W) continue;
+        const int o = (r + T) * RW + c + T;
+        __stcg(dstu + (size_t)y * pitch + x, fu[o]);
+        __stcg(dstv + (size_t)y * pitch + x, fv[o]);
+        if (p == np - 1) ok = ok && isfinite(fu[o]) && isfinite(fv[o]);
+      }
+    }
+    bad = __syncthreads_or(!ok);  // also: every store of the stage is issued
+    if (threadIdx.x == 0) {
+      if (bad) atomicOr(status + i, OF_ST_NONFINITE_OUTPUT);
+      __threadfence();  // release
+      atomicAdd(done + gtile, 1u);
     }
   }
 }
@@ -315,32 +473,46 @@ struct HsqShape {
 constexpr HsqShape kHsqShapes[] = {{64, 40, 4}, {32, 24, 4}, {64, 24, 4}, {32, 32, 8}};
 constexpr int kHsqNumShapes = sizeof(kHsqShapes) / sizeof(kHsqShapes[0]);
 
+template <int RW, int RH, int T, bool FAST>
+void* hsq_kernel_ptr(bool resident) {
+  return resident ? (void*)hsr_kernel<RW, RH, T, FAST> : (void*)hsq_kernel<RW, RH, T, FAST>;
+}
+
+// Opts the chosen kernel into its shared memory and reports how many of its CTAs fit on an SM.
 template <int RW, int RH, int T>
-cudaError_t hsq_launch(bool fast, int grid, const HsqPair* pairs, int n, unsigned int tiles_total, int max_passes,
-                       unsigned long long* ticket, unsigned int* done, int* status, long long wait_limit,
-                       int* err_flag, cudaStream_t st) {
+int hsq_resident(bool fast, bool resident, int* per_sm) {
   using G = HqTile<RW, RH, T>;
-  cudaError_t e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true>), G::SMEM)
-                       : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false>), G::SMEM);
-  if (e != cudaSuccess) return e;
-  if (fast)
-    hsq_kernel<RW, RH, T, true><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
-                                                            wait_limit, err_flag);
+  cudaError_t e;
+  if (resident)
+    e = fast ? OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, true>), G::SMEM)
+             : OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, false>), G::SMEM);
   else
-    hsq_kernel<RW, RH, T, false><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
-                                                             wait_limit, err_flag);
-  return cudaGetLastError();
+    e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true>), G::SMEM)
+             : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false>), G::SMEM);
+  if (e != cudaSuccess) return -1;
+  const void* k = fast ? hsq_kernel_ptr<RW, RH, T, true>(resident) : hsq_kernel_ptr<RW, RH, T, false>(resident);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, HQ_THREADS, G::SMEM);
+  return e == cudaSuccess ? 0 : -1;
 }
 
 template <int RW, int RH, int T>
-int hsq_resident(bool fast, int* per_sm) {
+cudaError_t hsq_launch(bool fast, bool resident, int grid, const HsqPair* pairs, int n, unsigned int tiles_total,
+                       int max_passes, unsigned long long* ticket, unsigned int* done, int* status,
+                       long long wait_limit, int* err_flag, cudaStream_t st) {
   using G = HqTile<RW, RH, T>;
-  cudaError_t e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true>), G::SMEM)
-                       : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false>), G::SMEM);
-  if (e != cudaSuccess) return -1;
-  e = fast ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, hsq_kernel<RW, RH, T, true>, HQ_THREADS, G::SMEM)
-           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, hsq_kernel<RW, RH, T, false>, HQ_THREADS, G::SMEM);
-  return e == cudaSuccess ? 0 : -1;
+  if (resident) {
+    if (fast)
+      hsr_kernel<RW, RH, T, true><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, done, status, wait_limit, err_flag);
+    else
+      hsr_kernel<RW, RH, T, false><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, done, status, wait_limit, err_flag);
+  } else if (fast) {
+    hsq_kernel<RW, RH, T, true><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done,
+                                                                 status, wait_limit, err_flag);
+  } else {
+    hsq_kernel<RW, RH, T, false><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done,
+                                                                  status, wait_limit, err_flag);
+  }
+  return cudaGetLastError();
 }
 }  // namespace
 
@@ -382,6 +554,9 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
   const int arith = tuning ? tuning->hs_arithmetic : OF_HS_EXACT;
   OF_REQUIRE(arith == OF_HS_EXACT || arith == OF_HS_FAST, "of_hs_batch: hs_arithmetic must be OF_HS_EXACT or OF_HS_FAST");
   const bool fast = arith == OF_HS_FAST;
+  const int sched = tuning ? tuning->hs_schedule : OF_HS_SCHED_AUTO;
+  OF_REQUIRE(sched == OF_HS_SCHED_AUTO || sched == OF_HS_SCHED_QUEUE || sched == OF_HS_SCHED_RESIDENT,
+             "of_hs_batch: hs_schedule must be OF_HS_SCHED_AUTO, _QUEUE or _RESIDENT");
   OF_REQUIRE(shape >= 0 && shape < kHsqNumShapes, "of_hs_batch: tile_shape must be in 0..%d", kHsqNumShapes - 1);
   const HsqShape sh = kHsqShapes[shape];
   const int TW = sh.rw - 2 * sh.t, TH = sh.rh - 2 * sh.t;
@@ -444,27 +619,41 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
   // ticket, counters and the error flag are contiguous
   e = cudaMemsetAsync(ticket, 0, (size_t)((char*)(err_flag + 1) - (char*)ticket), st);
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: %s", cudaGetErrorString(e));
-  int dev = 0, sms = kNumSMs, per_sm = 1;
+  int dev = 0, sms = kNumSMs;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int rc;
-  switch (shape) {
-    case 0: rc = hsq_resident<64, 40, 4>(fast, &per_sm); break;
-    case 1: rc = hsq_resident<32, 24, 4>(fast, &per_sm); break;
-    case 2: rc = hsq_resident<64, 24, 4>(fast, &per_sm); break;
-    default: rc = hsq_resident<32, 32, 8>(fast, &per_sm); break;
+  // every CTA must be resident (items wait for items of running CTAs)
+  auto capacity = [&](bool resident, long long* cap) {
+    int per_sm = 0, rc;
+    switch (shape) {
+      case 0: rc = hsq_resident<64, 40, 4>(fast, resident, &per_sm); break;
+      case 1: rc = hsq_resident<32, 24, 4>(fast, resident, &per_sm); break;
+      case 2: rc = hsq_resident<64, 24, 4>(fast, resident, &per_sm); break;
+      default: rc = hsq_resident<32, 32, 8>(fast, resident, &per_sm); break;
+    }
+    *cap = (long long)sms * per_sm;
+    return rc == 0 && per_sm >= 1;
+  };
+  long long cap_r = 0, cap_q = 0;
+  bool resident = false;
+  if (sched != OF_HS_SCHED_QUEUE) {
+    if (!capacity(true, &cap_r)) return set_error(OF_ERR_CUDA, "of_hs_batch: occupancy query failed");
+    resident = (long long)tiles_total <= cap_r;
+    if (sched == OF_HS_SCHED_RESIDENT && !resident)
+      return set_error(OF_ERR_INVALID, "of_hs_batch: %u tiles exceed the %lld resident CTAs of the resident schedule",
+                       tiles_total, cap_r);
   }
-  if (rc != 0 || per_sm < 1) return set_error(OF_ERR_CUDA, "of_hs_batch: occupancy query failed");
-  // every CTA must be resident (items wait for items of running CTAs); no more CTAs than
-  // items of one pass are useful
-  long long grid = (long long)sms * per_sm;
-  if (grid > (long long)tiles_total) grid = tiles_total;
+  long long grid = tiles_total;  // resident: one CTA per tile
+  if (!resident) {
+    if (!capacity(false, &cap_q)) return set_error(OF_ERR_CUDA, "of_hs_batch: occupancy query failed");
+    grid = cap_q < (long long)tiles_total ? cap_q : (long long)tiles_total;  // no more CTAs than items of a pass
+  }
   if (grid < 1) grid = 1;
   switch (shape) {
-    case 0: e = hsq_launch<64, 40, 4>(fast, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    case 1: e = hsq_launch<32, 24, 4>(fast, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    case 2: e = hsq_launch<64, 24, 4>(fast, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    default: e = hsq_launch<32, 32, 8>(fast, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    case 0: e = hsq_launch<64, 40, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    case 1: e = hsq_launch<32, 24, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    case 2: e = hsq_launch<64, 24, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    default: e = hsq_launch<32, 32, 8>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
   }
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: launch: %s", cudaGetErrorString(e));
   return check_launch("of_hs_batch", nl + 1);

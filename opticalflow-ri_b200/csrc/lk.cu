@@ -9,9 +9,15 @@
 // reference's 64->1 reduction tree is an in-lane add and the rest are warp shuffles in
 // the same pairing: A, b and the error are reduced in exactly the reference's order.
 // J is sampled with exact float32 bilinear weights (pixel-centre convention, clamp to
-// edge) through L1.  Compute bound: ~7e4 FP32 flops per pixel at a 27x27 window and
-// 5 Newton steps.
+// edge) from a 64x64 region staged per CTA around the tile's mean displaced window, stored
+// as (J[y][x], J[y][x+1]) pairs so a bilinear footprint is two 64-bit loads; the gradients
+// are stored as (dx, dy) pairs.  A warp whose every footprint of a Newton step lies in the
+// region runs the samples without per-sample region tests; others fall back per sample to
+// clamped global reads.  Issue bound: ~7e4 FP32 flops per pixel at a 27x27 window and
+// 5 Newton steps, about 7 shared-memory reads per sample.
 #include <float.h>
+
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -22,13 +28,16 @@ constexpr int LK_G = LK_PT + 31;    // gradient positions per axis
 constexpr int LK_I = LK_G + 2;      // intensity positions per axis
 // Row strides of the staged patches: a warp reads 4 rows of 8 consecutive columns at once,
 // so a stride of 8 or 24 (mod 32) banks puts the 4 rows in disjoint banks.
-constexpr int LK_IP = 56, LK_GP = 40;
-static_assert(LK_IP >= LK_I && LK_GP >= LK_G && LK_IP % 32 == 24 && LK_GP % 32 == 8, "patch strides");
+constexpr int LK_IP = 56, LK_GP = 40;  // LK_GP counts float2 (dx, dy) pairs
+static_assert(LK_IP >= LK_I && LK_GP >= LK_G && LK_IP % 32 == 24 && LK_GP % 16 == 8, "patch strides");
 // J region staged per CTA for the Newton steps: LK_JR x LK_JR texels centred on the tile's
 // mean displaced window, row stride LK_JP (72: the 4 rows a warp reads at once fall in
 // distinct banks).  Texels hold clamped-coordinate values, so a bilinear footprint inside
 // the region reads exactly what the clamped global path reads.
-constexpr int LK_JR = 64, LK_JP = 72;
+constexpr int LK_JR = 64, LK_JP = 72;  // LK_JP counts float2 texel pairs
+static_assert(LK_JP % 16 == 8, "J pair stride");
+// dynamic shared memory of the kernel: sJ2 pairs, sD2 pairs, sI
+constexpr size_t LK_SMEM = (size_t)LK_JR * LK_JP * 8 + (size_t)LK_G * LK_GP * 8 + (size_t)LK_I * LK_IP * 4;
 
 struct LkParams {
   int ws, hw, aL, aR, aT, aB, niter;
@@ -72,7 +81,7 @@ __device__ __forceinline__ float lk_bilinear(const float* __restrict__ J, int H,
 
 // The same bilinear sample from the staged region when its 2 x 2 footprint lies inside it
 // (rx, ry: footprint origin relative to the region), else from global memory.
-__device__ __forceinline__ float lk_bilinear_s(const float* __restrict__ sJ, const float* __restrict__ J, int H, int W,
+__device__ __forceinline__ float lk_bilinear_s(const float2* __restrict__ sJ, const float* __restrict__ J, int H, int W,
                                                int pitch, float x, float y, int ox, int oy) {
   float xs = __fsub_rn(x, 0.5f), ys = __fsub_rn(y, 0.5f);
   float fx0 = floorf(xs), fy0 = floorf(ys);
@@ -81,11 +90,11 @@ __device__ __forceinline__ float lk_bilinear_s(const float* __restrict__ sJ, con
   const int rx = i0 - ox, ry = j0 - oy;
   float t00, t10, t01, t11;
   if ((unsigned)rx <= (unsigned)(LK_JR - 2) && (unsigned)ry <= (unsigned)(LK_JR - 2)) {
-    const float* q = sJ + ry * LK_JP + rx;
-    t00 = q[0];
-    t10 = q[1];
-    t01 = q[LK_JP];
-    t11 = q[LK_JP + 1];
+    const float2 top = sJ[ry * LK_JP + rx], bot = sJ[(ry + 1) * LK_JP + rx];
+    t00 = top.x;
+    t10 = top.y;
+    t01 = bot.x;
+    t11 = bot.y;
   } else {
     int xa = clampi(i0, 0, W - 1), xb = clampi(i0 + 1, 0, W - 1);
     int ya = clampi(j0, 0, H - 1), yb = clampi(j0 + 1, 0, H - 1);
@@ -113,12 +122,14 @@ __device__ __forceinline__ float lk_tree(float lo, float hi) {
   return __shfl_sync(0xffffffffu, t, 0);
 }
 
-__global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__ I, const float* __restrict__ J,
+__global__ void __launch_bounds__(256, 2) lk_dense_kernel(const float* __restrict__ I, const float* __restrict__ J,
                                                        float* __restrict__ U, float* __restrict__ V, int H, int W,
                                                        int pitch, LkParams p, uint8_t* __restrict__ status,
                                                        float* __restrict__ err) {
-  __shared__ float sI[LK_I * LK_IP];
-  __shared__ float sDx[LK_G * LK_GP], sDy[LK_G * LK_GP];
+  extern __shared__ float4 lk_dyn[];
+  float2* const sJ = reinterpret_cast<float2*>(lk_dyn);  // (J[y][x], J[y][x + 1]) pairs
+  float2* const sD = sJ + LK_JR * LK_JP;                 // (dx, dy) pairs
+  float* const sI = reinterpret_cast<float*>(sD + LK_G * LK_GP);
   const int i0 = blockIdx.y * LK_PT, j0 = blockIdx.x * LK_PT;
   const int oy = i0 - p.hw - 1, ox = j0 - p.hw - 1;  // image position of sI[0][0]
   for (int t = threadIdx.x; t < LK_I * LK_I; t += blockDim.x) {
@@ -130,14 +141,15 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
     int gy = t / LK_G, gx = t - gy * LK_G;
     const float* c = sI + (gy + 1) * LK_IP + gx + 1;
 #define P(dy, dx) c[(dy) * LK_IP + (dx)]
-    sDx[gy * LK_GP + gx] = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(-1, 1), P(1, 1)), P(-1, -1)), P(1, -1)), 3.0f,
+    float ddx, ddy;
+    ddx = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(-1, 1), P(1, 1)), P(-1, -1)), P(1, -1)), 3.0f,
                        __fmul_rn(__fsub_rn(P(0, 1), P(0, -1)), 10.0f));
-    sDy[gy * LK_GP + gx] = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(1, -1), P(1, 1)), P(-1, -1)), P(-1, 1)), 3.0f,
+    ddy = __fmaf_rn(__fsub_rn(__fsub_rn(__fadd_rn(P(1, -1), P(1, 1)), P(-1, -1)), P(-1, 1)), 3.0f,
                        __fmul_rn(__fsub_rn(P(1, 0), P(-1, 0)), 10.0f));
 #undef P
+    sD[gy * LK_GP + gx] = make_float2(ddx, ddy);
   }
   // J region: centred on the tile centre displaced by the mean initial flow of the tile
-  __shared__ float sJ[LK_JR * LK_JP];
   __shared__ float red_u[8], red_v[8];
   {
     float su = 0.f, sv = 0.f;
@@ -162,24 +174,27 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
   const int jox = j0 + LK_PT / 2 + (int)floorf(mu) - LK_JR / 2, joy = i0 + LK_PT / 2 + (int)floorf(mv) - LK_JR / 2;
   for (int t = threadIdx.x; t < LK_JR * LK_JR; t += blockDim.x) {
     const int ly = t / LK_JR, lx = t - ly * LK_JR;
-    sJ[ly * LK_JP + lx] = __ldg(J + (size_t)clampi(joy + ly, 0, H - 1) * pitch + clampi(jox + lx, 0, W - 1));
+    const float* row = J + (size_t)clampi(joy + ly, 0, H - 1) * pitch;
+    sJ[ly * LK_JP + lx] = make_float2(__ldg(row + clampi(jox + lx, 0, W - 1)), __ldg(row + clampi(jox + lx + 1, 0, W - 1)));
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int xid = lane & 7, yid = lane >> 3;
-  float wx[4], wy0[4], wy1[4];
-  int bx[2], by0[2], by1[2];
-  lk_weights(xid, p.ws, p.aL, p.aR, wx, bx);
-  lk_weights(yid, p.ws, p.aT, p.aB, wy0, by0);
-  lk_weights(yid + 4, p.ws, p.aT, p.aB, wy1, by1);
   unsigned act = 0;  // bit 16 v + 4 ty + tx: the sample's tile weight is not 0
+  {
+    float wx[4], wy0[4], wy1[4];
+    int bx[2], by0[2], by1[2];
+    lk_weights(xid, p.ws, p.aL, p.aR, wx, bx);
+    lk_weights(yid, p.ws, p.aT, p.aB, wy0, by0);
+    lk_weights(yid + 4, p.ws, p.aT, p.aB, wy1, by1);
 #pragma unroll
-  for (int v = 0; v < 2; v++)
+    for (int v = 0; v < 2; v++)
 #pragma unroll
-    for (int ty = 0; ty < 4; ty++)
+      for (int ty = 0; ty < 4; ty++)
 #pragma unroll
-      for (int tx = 0; tx < 4; tx++)
-        act |= (unsigned)(__fmul_rn(wx[tx], (v ? wy1 : wy0)[ty]) != 0.f) << (16 * v + 4 * ty + tx);
+        for (int tx = 0; tx < 4; tx++)
+          act |= (unsigned)(__fmul_rn(wx[tx], (v ? wy1 : wy0)[ty]) != 0.f) << (16 * v + 4 * ty + tx);
+  }
   const float hw = (float)p.hw;
   const int i = i0 + warp;
   if (i >= H) return;
@@ -190,18 +205,17 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
     float a11[2] = {0.f, 0.f}, a12[2] = {0.f, 0.f}, a22[2] = {0.f, 0.f};
 #pragma unroll
     for (int v = 0; v < 2; v++) {
-      const float* wy = v ? wy1 : wy0;
       const int yy = yid + 4 * v;
 #pragma unroll
       for (int ty = 0; ty < 4; ty++)
 #pragma unroll
         for (int tx = 0; tx < 4; tx++) {
-          float w = __fmul_rn(wx[tx], wy[ty]);
-          if (w == 0.f) continue;
+          if (!((act >> (16 * v + 4 * ty + tx)) & 1u)) continue;  // tile weight 0
           int g = (gyb + ty * 8 + yy) * LK_GP + gxb + tx * 8 + xid;
           // w is 1 here (the tile weights are products of 0 / 1 values and w == 0 is
           // skipped), so the reference's multiplications by w are exact identities
-          float dx = sDx[g], dy = sDy[g];
+          const float2 d = sD[g];
+          const float dx = d.x, dy = d.y;
           a11[v] = __fmaf_rn(dx, dx, a11[v]);
           a12[v] = __fmaf_rn(dx, dy, a12[v]);
           a22[v] = __fmaf_rn(dy, dy, a22[v]);
@@ -259,41 +273,51 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
         }
       }
       float b1[2] = {0.f, 0.f}, b2[2] = {0.f, 0.f};
+      // The samples of the step; a warp whose every footprint lies inside the staged J
+      // region (the common case) runs the variant without the per-sample region test.
+      auto samples = [&](auto all_in) {
 #pragma unroll
-      for (int v = 0; v < 2; v++) {
-        const int yy = yid + 4 * v;
+        for (int v = 0; v < 2; v++) {
+          const int yy = yid + 4 * v;
 #pragma unroll
-        for (int ty = 0; ty < 4; ty++)
+          for (int ty = 0; ty < 4; ty++)
 #pragma unroll
-          for (int tx = 0; tx < 4; tx++) {
-            if (!((act >> (16 * v + 4 * ty + tx)) & 1u)) continue;  // tile weight 0
-            int g = (gyb + ty * 8 + yy) * LK_GP + gxb + tx * 8 + xid;
-            float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_IP + gxb + tx * 8 + xid + 1];
-            float t00, t10, t01, t11;
-            if (((inx >> tx) & (iny >> (4 * v + ty))) & 1u) {
-              const float* q = sJ + yr[v][ty] * LK_JP + xr[tx];
-              t00 = q[0];
-              t10 = q[1];
-              t01 = q[LK_JP];
-              t11 = q[LK_JP + 1];
-            } else {  // outside the staged region: clamped global reads
-              const int i0 = xr[tx] + jox, j0 = yr[v][ty] + joy;
-              const int xa0 = clampi(i0, 0, W - 1), xb0 = clampi(i0 + 1, 0, W - 1);
-              const int ya0 = clampi(j0, 0, H - 1), yb0 = clampi(j0 + 1, 0, H - 1);
-              t00 = __ldg(J + (size_t)ya0 * pitch + xa0);
-              t10 = __ldg(J + (size_t)ya0 * pitch + xb0);
-              t01 = __ldg(J + (size_t)yb0 * pitch + xa0);
-              t11 = __ldg(J + (size_t)yb0 * pitch + xb0);
+            for (int tx = 0; tx < 4; tx++) {
+              if (!((act >> (16 * v + 4 * ty + tx)) & 1u)) continue;  // tile weight 0
+              int g = (gyb + ty * 8 + yy) * LK_GP + gxb + tx * 8 + xid;
+              float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_IP + gxb + tx * 8 + xid + 1];
+              float t00, t10, t01, t11;
+              if (decltype(all_in)::value || (((inx >> tx) & (iny >> (4 * v + ty))) & 1u)) {
+                const float2* q = sJ + yr[v][ty] * LK_JP + xr[tx];
+                const float2 top = q[0], bot = q[LK_JP];
+                t00 = top.x;
+                t10 = top.y;
+                t01 = bot.x;
+                t11 = bot.y;
+              } else {  // outside the staged region: clamped global reads
+                const int i0 = xr[tx] + jox, j0 = yr[v][ty] + joy;
+                const int xa0 = clampi(i0, 0, W - 1), xb0 = clampi(i0 + 1, 0, W - 1);
+                const int ya0 = clampi(j0, 0, H - 1), yb0 = clampi(j0 + 1, 0, H - 1);
+                t00 = __ldg(J + (size_t)ya0 * pitch + xa0);
+                t10 = __ldg(J + (size_t)ya0 * pitch + xb0);
+                t01 = __ldg(J + (size_t)yb0 * pitch + xa0);
+                t11 = __ldg(J + (size_t)yb0 * pitch + xb0);
+              }
+              float Jv = __fmul_rn(__fmul_rn(xoa[tx], yob[v][ty]), t00);
+              Jv = __fmaf_rn(__fmul_rn(xa[tx], yob[v][ty]), t10, Jv);
+              Jv = __fmaf_rn(__fmul_rn(xoa[tx], yb[v][ty]), t01, Jv);
+              Jv = __fmaf_rn(__fmul_rn(xa[tx], yb[v][ty]), t11, Jv);
+              float diff = __fsub_rn(Jv, Iv);  // (Jv - Iv) * w with w == 1
+              const float2 d = sD[g];
+              b1[v] = __fmaf_rn(diff, d.x, b1[v]);
+              b2[v] = __fmaf_rn(diff, d.y, b2[v]);
             }
-            float Jv = __fmul_rn(__fmul_rn(xoa[tx], yob[v][ty]), t00);
-            Jv = __fmaf_rn(__fmul_rn(xa[tx], yob[v][ty]), t10, Jv);
-            Jv = __fmaf_rn(__fmul_rn(xoa[tx], yb[v][ty]), t01, Jv);
-            Jv = __fmaf_rn(__fmul_rn(xa[tx], yb[v][ty]), t11, Jv);
-            float diff = __fsub_rn(Jv, Iv);  // (Jv - Iv) * w with w == 1
-            b1[v] = __fmaf_rn(diff, sDx[g], b1[v]);
-            b2[v] = __fmaf_rn(diff, sDy[g], b2[v]);
-          }
-      }
+        }
+      };
+      if (__all_sync(0xffffffffu, inx == 0xFu && iny == 0xFFu))
+        samples(std::true_type());
+      else
+        samples(std::false_type());
       float B1 = lk_tree(b1[0], b1[1]), B2 = lk_tree(b2[0], b2[1]);
       float dx = __fmul_rn(__fmaf_rn(A12, B2, -__fmul_rn(A22, B1)), 32.0f);
       float dy = __fmul_rn(__fmaf_rn(A12, B1, -__fmul_rn(A11, B2)), 32.0f);
@@ -311,6 +335,11 @@ __global__ void __launch_bounds__(256) lk_dense_kernel(const float* __restrict__
       // GetError visiting order and guards (:620-653); bits: 1 xBase, 2 yBase, 4 xBase2, 8 yBase2
       const int ord[16] = {0x000, 0x010, 0x100, 0x110, 0x021, 0x121, 0x202, 0x212,
                            0x223, 0x034, 0x134, 0x234, 0x308, 0x318, 0x328, 0x33c};
+      float wx[4], wy0[4], wy1[4];  // recomputed here rather than kept live through the steps
+      int bx[2], by0[2], by1[2];
+      lk_weights(xid, p.ws, p.aL, p.aR, wx, bx);
+      lk_weights(yid, p.ws, p.aT, p.aB, wy0, by0);
+      lk_weights(yid + 4, p.ws, p.aT, p.aB, wy1, by1);
       float e[2] = {0.f, 0.f};
 #pragma unroll
       for (int v = 0; v < 2; v++) {
@@ -365,6 +394,8 @@ extern "C" int of_lk_dense(const float* I, const float* J, float* U, float* V, i
   OF_REQUIRE(((p.aL | p.aR | p.aT | p.aB) & ~1) == 0, "of_lk_dense: asym entries must be 0 or 1");
   p.niter = niter;
   dim3 grid((W + LK_PT - 1) / LK_PT, (H + LK_PT - 1) / LK_PT);
-  lk_dense_kernel<<<grid, 256, 0, as_stream(stream)>>>(I, J, U, V, H, W, pitch, p, status, err);
+  cudaError_t e = OF_SMEM_OPT_IN(lk_dense_kernel, LK_SMEM);
+  if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_lk_dense: %s", cudaGetErrorString(e));
+  lk_dense_kernel<<<grid, 256, LK_SMEM, as_stream(stream)>>>(I, J, U, V, H, W, pitch, p, status, err);
   return check_launch("of_lk_dense");
 }

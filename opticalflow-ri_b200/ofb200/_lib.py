@@ -29,7 +29,7 @@ class OfHsBatchPair(ctypes.Structure):
 
 class OfTuning(ctypes.Structure):
     _fields_ = [("tile_shape", ctypes.c_int), ("streams", ctypes.c_int), ("hs_arithmetic", ctypes.c_int),
-                ("reserved", ctypes.c_int)]
+                ("hs_schedule", ctypes.c_int)]
 
 
 # per-pair status bits (include/ofb200.h)

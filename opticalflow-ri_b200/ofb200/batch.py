@@ -21,7 +21,7 @@ from . import _lib
 from . import graph as _graph
 from . import ops
 
-__all__ = ["PairSpec", "PairBatch", "HsGroup", "method_spec", "config4_manifest", "render_entry", "pair_cost_of",
+__all__ = ["PairSpec", "PairBatch", "HostBatch", "HsGroup", "method_spec", "config4_manifest", "render_entry", "pair_cost_of",
            "BatchRunner", "autotune", "tune_hs_shape", "pair_descriptors", "run_c"]
 
 
@@ -125,29 +125,135 @@ class PairBatch:
             raise ValueError("one frame pair per spec")
         if not (self.use_graph and _graph.ENABLED):
             return self._pipelines(frames)
-        key = tuple((tuple(a.shape), a.dtype, s.key) for (a, _), s in zip(frames, self.specs))
         with self._lock:
-            e = self._graphs.get(key)
-            if e is None:
-                static_in = [(a.clone(), b.clone()) for a, b in frames]
-                self._pipelines(static_in)  # eager warm-up: sizes every stream's workspaces
-                torch.cuda.synchronize()
-                from ._lib import lib
-                n0 = lib().of_launch_count()
-                g = torch.cuda.CUDAGraph()
-                side = torch.cuda.Stream()
-                side.wait_stream(torch.cuda.current_stream())
-                with torch.cuda.graph(g, stream=side):
-                    static_out = self._pipelines(static_in)
-                nk = lib().of_launch_count() - n0
-                e = (g, static_in, static_out, nk)
-                self._graphs[key] = e
-            g, static_in, static_out, nk = e
+            g, static_in, static_out, nk = self._entry(frames)
             # all inputs into the graph's buffers with one multi-tensor copy
             torch._foreach_copy_([t for p in static_in for t in p], [t for p in frames for t in p])
             g.replay()
             _graph._replayed_kernels += nk
             return static_out
+
+    def _entry(self, frames):
+        """The graph for these frames' shapes, dtypes and settings, captured on first use
+        (frames: CUDA tensors whose values feed the eager warm-up run)."""
+        key = tuple((tuple(a.shape), a.dtype, s.key) for (a, _), s in zip(frames, self.specs))
+        e = self._graphs.get(key)
+        if e is None:
+            static_in = [(a.clone(), b.clone()) for a, b in frames]
+            self._pipelines(static_in)  # eager warm-up: sizes every stream's workspaces
+            torch.cuda.synchronize()
+            from ._lib import lib
+            n0 = lib().of_launch_count()
+            g = torch.cuda.CUDAGraph()
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.graph(g, stream=side):
+                static_out = self._pipelines(static_in)
+            nk = lib().of_launch_count() - n0
+            e = (g, static_in, static_out, nk)
+            self._graphs[key] = e
+        return e
+
+
+class HostBatch:
+    """Frame pairs from host memory to flow fields in host memory, `depth` batches in flight.
+
+    submit() copies a batch's frames host -> device on a copy stream, replays the batch's
+    graph (a PairBatch per slot, so that the batches in flight own distinct device buffers;
+    the slots share the compute streams and run one after another), then copies every U, V
+    device -> host into the slot's pinned buffers on the copy stream.  result() waits for
+    those copies and returns numpy views of the pinned buffers.  While the GPU computes
+    batch k the host prepares batch k+1, and batch k's results cross PCIe while batch k+1
+    computes.  A slot's results stay valid until its next submit, `depth` submits later.
+    Frames given as pinned CPU tensors are copied from directly (keep them unchanged until
+    their result is taken); other host arrays go through the slot's pinned staging first."""
+
+    def __init__(self, specs, streams=8, depth=2, status: bool = False):
+        self.specs = list(specs)
+        self.depth = max(1, int(depth))
+        shared = [torch.cuda.Stream() for _ in range(max(1, int(streams)))]
+        self._slots = [PairBatch(self.specs, streams=shared, status=status) for _ in range(self.depth)]
+        # separate copy streams: batch k+1's inputs go up while batch k computes and while
+        # batch k-1's results come down
+        self._up, self._down = torch.cuda.Stream(), torch.cuda.Stream()
+        self._state = [None] * self.depth
+        self._submitted = 0
+
+    @staticmethod
+    def _host(x):
+        return x if isinstance(x, torch.Tensor) else torch.from_numpy(x)
+
+    def _first_use(self, slot, frames):
+        dev = torch.device("cuda", torch.cuda.current_device())
+        pb = self._slots[slot]
+        d = [(self._host(a).to(dev), self._host(b).to(dev)) for a, b in frames]
+        g, static_in, static_out, nk = pb._entry(d)
+        pin = lambda t: torch.empty(t.shape, dtype=t.dtype, pin_memory=True)  # noqa: E731
+        st = {"entry": (g, static_in, static_out, nk),
+              "stage": [(pin(a), pin(b)) for a, b in static_in],
+              "out": [(pin(U), pin(V)) for U, V in static_out],
+              "status": pin(pb.status) if pb.status is not None else None,
+              "h2d": torch.cuda.Event(), "done": torch.cuda.Event(), "d2h": torch.cuda.Event(), "ticket": -1}
+        self._state[slot] = st
+        return st
+
+    def submit(self, frames):
+        """frames: list of (frame1, frame2) host arrays / CPU tensors (uint8, uint16 or
+        float32) matching the specs.  Returns a ticket for result()."""
+        if len(frames) != len(self.specs):
+            raise ValueError("one frame pair per spec")
+        ticket = self._submitted
+        slot = ticket % self.depth
+        st = self._state[slot] or self._first_use(slot, frames)
+        g, static_in, static_out, nk = st["entry"]
+        for (a, b), (sa, sb) in zip(frames, static_in):
+            if tuple(a.shape) != tuple(sa.shape) or tuple(b.shape) != tuple(sb.shape):
+                raise ValueError("HostBatch: frame shapes differ from the first batch's")
+        st["h2d"].synchronize()  # the staging buffers' previous copy has left the host
+        srcs = []
+        for (a, b), (pa, pb_) in zip(frames, st["stage"]):
+            for x, p in ((a, pa), (b, pb_)):
+                t = self._host(x)
+                if t.is_pinned() and t.dtype == p.dtype:
+                    srcs.append(t)
+                else:
+                    p.copy_(t)
+                    srcs.append(p)
+        cur, up, down = torch.cuda.current_stream(), self._up, self._down
+        up.wait_event(st["done"])  # the slot's previous replay has read its inputs
+        with torch.cuda.stream(up):
+            torch._foreach_copy_([t for p in static_in for t in p], srcs, non_blocking=True)
+        st["h2d"].record(up)
+        cur.wait_event(st["h2d"])
+        cur.wait_event(st["d2h"])  # the slot's previous results have left the device
+        g.replay()
+        _graph._replayed_kernels += nk
+        st["done"].record(cur)
+        down.wait_event(st["done"])
+        with torch.cuda.stream(down):
+            torch._foreach_copy_([t for p in st["out"] for t in p], [t for p in static_out for t in p],
+                                 non_blocking=True)
+            if st["status"] is not None:
+                st["status"].copy_(self._slots[slot].status, non_blocking=True)
+        st["d2h"].record(down)
+        st["ticket"] = ticket
+        self._submitted += 1
+        return ticket
+
+    def result(self, ticket):
+        """[(U, V)] numpy float32 views of the slot's pinned buffers for a submitted batch
+        (and, with status=True, self.last_status: the batch's status words)."""
+        st = self._state[ticket % self.depth] if 0 <= ticket < self._submitted else None
+        if st is None or st["ticket"] != ticket:
+            raise ValueError(f"HostBatch: ticket {ticket} is not in flight (its slot was reused)")
+        st["d2h"].synchronize()
+        if st["status"] is not None:
+            self.last_status = st["status"].numpy().copy()
+        return [(U.numpy(), V.numpy()) for U, V in st["out"]]
+
+    def run(self, frames):
+        """submit + result: one batch from host frames to host flow fields."""
+        return self.result(self.submit(frames))
 
 
 # ----------------------------------------------------------------------------- config 4
@@ -208,8 +314,11 @@ class HsGroup:
     bit-exact with the per-pair path).  The prefilters, the launch and the accumulation into
     the result are captured into one CUDA graph on the first run."""
 
-    def __init__(self, specs, tile_shape=0):
-        self.specs, self.tile_shape = list(specs), int(tile_shape)
+    def __init__(self, specs, tile_shape=0, schedule="auto"):
+        """schedule: ops.hs_batch's ('auto', 'queue' or 'resident').  The resident schedule
+        needs every tile's CTA resident at once: with other kernels running beside the
+        group (BatchRunner's chunks) use 'queue', whose items only wait for running CTAs."""
+        self.specs, self.tile_shape, self.schedule = list(specs), int(tile_shape), schedule
         for sp in self.specs:
             if sp.pyramidalLevels != 1 or sp.kLevels != 1 or sp.make_opt is not None:
                 raise ValueError("HsGroup takes single-level Horn-Schunck pairs")
@@ -229,7 +338,7 @@ class HsGroup:
             U, V = torch.zeros_like(a), torch.zeros_like(a)
             pairs.append((a, b, U, V, hs.alphas[-1], hs.Niter))
             outs.append((U, V))
-        self.status = ops.hs_batch(pairs, tile_shape=self.tile_shape)
+        self.status = ops.hs_batch(pairs, tile_shape=self.tile_shape, schedule=self.schedule)
         # the driver's Uaccum = 0 + U (the sign of a zero result is the accumulation's)
         return [(ops.accumulate(torch.zeros_like(U), U), ops.accumulate(torch.zeros_like(V), V)) for U, V in outs]
 
@@ -268,7 +377,7 @@ class BatchRunner:
         self.order = sorted(rest, key=lambda i: (-pair_cost_of(self.entries[i]), i))
         self.chunk, self.nstreams = int(chunk), int(streams)
         self._streams = [torch.cuda.Stream() for _ in range(self.nstreams)]
-        self._hs = (hs_idx, HsGroup([method_spec("hs") for _ in hs_idx], hs_shape)) if hs_idx else None
+        self._hs = (hs_idx, HsGroup([method_spec("hs") for _ in hs_idx], hs_shape, schedule="queue")) if hs_idx else None
         self._hs_stream = torch.cuda.Stream() if hs_idx else None
         self._batches = []
         for c in range(0, len(self.order), self.chunk):
@@ -313,15 +422,16 @@ def _cache_path():
                                                              "autotune.json"))
 
 
-def tune_hs_shape(frames_hs, reps=2, log=None, use_cache=True):
+def tune_hs_shape(frames_hs, reps=2, log=None, use_cache=True, schedule="auto"):
     """The persistent Horn-Schunck kernel's tile shape (region and sweeps per pass) for a set
-    of Horn-Schunck pairs: every shape of ops.hs_batch_shapes() timed on them; the choice is
-    cached per (GPU, method, sizes) in a JSON file (OFB_AUTOTUNE_CACHE, default
-    ~/.cache/ofb200/autotune.json).  Returns (shape index, {shape: ms})."""
+    of Horn-Schunck pairs under `schedule`: every shape of ops.hs_batch_shapes() timed on
+    them; the choice is cached per (GPU, method, schedule, sizes) in a JSON file
+    (OFB_AUTOTUNE_CACHE, default ~/.cache/ofb200/autotune.json).  Returns (shape index,
+    {shape: ms})."""
     import json
     import os
-    key = "|".join([torch.cuda.get_device_name(), "hs", ",".join(sorted(f"{a.shape[0]}x{a.shape[1]}"
-                                                                         for a, _ in frames_hs))])
+    key = "|".join([torch.cuda.get_device_name(), "hs", schedule,
+                    ",".join(sorted(f"{a.shape[0]}x{a.shape[1]}" for a, _ in frames_hs))])
     path = _cache_path()
     cache = {}
     if use_cache and os.path.exists(path):
@@ -335,7 +445,7 @@ def tune_hs_shape(frames_hs, reps=2, log=None, use_cache=True):
     specs = [method_spec("hs") for _ in frames_hs]
     table = {}
     for k in range(len(ops.hs_batch_shapes())):
-        g = HsGroup(specs, tile_shape=k)
+        g = HsGroup(specs, tile_shape=k, schedule=schedule)
         table[k] = _time_runner(g, frames_hs, reps)
         if log:
             log(f"hs tile shape {k} {ops.hs_batch_shapes()[k]}: {table[k]:.2f} ms")
@@ -362,7 +472,7 @@ def autotune(entries, frames, chunks=(16, 64, 256), streams=(2, 4, 8), reps=2, l
     if hs_persistent:
         hs = [frames[i] for i, e in enumerate(entries) if e["method"] == "hs"]
         if hs:
-            hs_shape, hs_table = tune_hs_shape(hs, reps=reps, log=log)
+            hs_shape, hs_table = tune_hs_shape(hs, reps=reps, log=log, schedule="queue")
             table.update({("hs_shape", k): v for k, v in hs_table.items()})
     for c in chunks:
         for s in streams:

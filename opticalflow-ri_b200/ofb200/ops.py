@@ -274,13 +274,21 @@ def hs_batch_shapes():
 HS_WAIT_LIMIT = 1 << 20  # polls of a queue wait before a pair is given up (under a second)
 
 
-def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status=None, arithmetic: str = "exact"):
+HS_SCHEDULES = ("auto", "queue", "resident")  # OF_HS_SCHED_AUTO / _QUEUE / _RESIDENT
+
+
+def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status=None, arithmetic: str = "exact",
+             schedule: str = "auto"):
     """Horn-Schunck of many pairs in one persistent launch (of_hs_batch).  pairs: list of
     (I0, I1, U, V, alpha, niter) with CUDA float32 planes; U, V are updated in place.
     arithmetic: 'exact' (bit-exact with the reference) or 'fast' (float32 averaging).
+    schedule: 'resident' (one CTA per tile, region kept on chip; needs every tile to get a
+    resident CTA), 'queue' (device work queue) or 'auto' (resident when it fits).
     Returns the per-pair status words (device int32, bits of ofb200._lib.ST_*)."""
     if arithmetic not in ("exact", "fast"):
         raise ValueError("arithmetic must be 'exact' or 'fast'")
+    if schedule not in HS_SCHEDULES:
+        raise ValueError(f"schedule must be one of {HS_SCHEDULES}")
     from ._lib import OfHsBatchPair, OfTuning
     n = len(pairs)
     arr = (OfHsBatchPair * n)()
@@ -292,7 +300,7 @@ def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status
                                float(np.float32(alpha)), int(niter))
     if status is None:
         status = torch.zeros(n, dtype=torch.int32, device=dev)
-    tun = OfTuning(int(tile_shape), 0, 1 if arithmetic == "fast" else 0, 0)
+    tun = OfTuning(int(tile_shape), 0, 1 if arithmetic == "fast" else 0, HS_SCHEDULES.index(schedule))
     ws, wn = workspace(lib().of_hs_batch_workspace_size(arr, n), "hs_batch")
     call("of_hs_batch", arr, n, ctypes.byref(tun), ctypes.c_void_p(status.data_ptr()), int(wait_limit), ws, wn,
          stream_ptr())

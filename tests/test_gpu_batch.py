@@ -174,3 +174,31 @@ def test_batch_status_words(cuda_ok):
         for k in (0, 2):
             assert st[k] & ~_lib.ST_NOT_CONVERGED == 0
             assert torch.equal(out[k][0], clean[k][0]) and torch.equal(out[k][1], clean[k][1])
+
+
+def test_host_batch_in_flight(torch_cuda):
+    """HostBatch: host frames (numpy and pinned tensors) to host U, V with two batches in
+    flight gives each batch's PairBatch result; a ticket whose slot was reused is refused."""
+    torch = torch_cuda
+    from ofb200.batch import HostBatch, PairBatch
+    specs, shapes = _specs()
+    batches = [[_pair(s, seed + 10 * k) for s, seed in shapes] for k in range(3)]
+    want = []
+    ref = PairBatch(specs, streams=2)
+    for fr in batches:
+        out = ref.run([(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in fr])
+        want.append([(U.cpu().numpy(), V.cpu().numpy()) for U, V in out])
+    hb = HostBatch(specs, streams=3, depth=2)
+    pinned = [(torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()) for a, b in batches[1]]
+    t0 = hb.submit(batches[0])
+    t1 = hb.submit(pinned)
+    got0 = [(U.copy(), V.copy()) for U, V in hb.result(t0)]
+    t2 = hb.submit(batches[2])
+    with pytest.raises(ValueError):
+        hb.result(t0)
+    got1, got2 = hb.result(t1), hb.result(t2)
+    for got, exp in zip((got0, got1, got2), want):
+        for (Ug, Vg), (Uw, Vw) in zip(got, exp):
+            assert np.array_equal(Ug, Uw) and np.array_equal(Vg, Vw)
+    with pytest.raises(ValueError):
+        hb.submit(batches[0][:2])

@@ -1,9 +1,10 @@
-"""Horn-Schunck in one persistent launch over a device work queue (of_hs_batch).
+"""Horn-Schunck in one persistent launch (of_hs_batch), under both schedules: the device
+work queue and the resident one (a CTA per tile for the whole solve, region on chip).
 
 Bit-exact with the regular solver (of_hs_solve, itself bit-exact with the reference) for
 one pair and for a batch of uneven pairs, with every tile shape; per-pair status words for
-a NaN frame; and the bounded queue wait running out (a short wait limit) ends the launch
-with a timeout status instead of hanging, leaving the context usable."""
+a NaN frame; and the bounded wait running out (a short wait limit) ends the launch with a
+timeout status instead of hanging, leaving the context usable."""
 import numpy as np
 import pytest
 
@@ -23,8 +24,12 @@ def _solve_ref(torch, a, b, U0, V0, alpha, niter):
     return U, V
 
 
+SCHEDULES = ["queue", "resident"]
+
+
+@pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("shape_index", [0, 1, 2, 3])
-def test_single_pair_config1_bit_exact(cuda_ok, shape_index):
+def test_single_pair_config1_bit_exact(cuda_ok, shape_index, schedule):
     """256 x 256, alpha 21, 600 sweeps (the PyHSchunck_Fs3_4 calibration) in one launch."""
     import torch
     from ofb200 import ops
@@ -32,13 +37,16 @@ def test_single_pair_config1_bit_exact(cuda_ok, shape_index):
     z = torch.zeros_like(a)
     Ur, Vr = _solve_ref(torch, a, b, z, z, 21.0, 600)
     U, V = z.clone(), z.clone()
-    st = ops.hs_batch([(a, b, U, V, 21.0, 600)], tile_shape=shape_index)
+    st = ops.hs_batch([(a, b, U, V, 21.0, 600)], tile_shape=shape_index, schedule=schedule)
     torch.cuda.synchronize()
     assert int(st.item()) == 0
     assert torch.equal(U, Ur) and torch.equal(V, Vr)
 
 
-def test_uneven_batch_bit_exact(cuda_ok):
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_uneven_batch_bit_exact(cuda_ok, schedule):
+    """Uneven sizes and sweep counts (600, 37, 9, 0: a last pass of fewer sweeps than the
+    shape's, and a pair with no sweep pass) in one launch."""
     import torch
     from ofb200 import ops
     shapes = [(128, 128, 600), (256, 256, 600), (64, 200, 37), (512, 384, 120), (17, 23, 9), (16, 16, 0)]
@@ -50,14 +58,15 @@ def test_uneven_batch_bit_exact(cuda_ok):
         V0 = (torch.randn(H, W, generator=g) * 0.3).cuda()
         refs.append(_solve_ref(torch, a, b, U0, V0, 21.0 + k, n))
         pairs.append((a, b, U0.clone(), V0.clone(), 21.0 + k, n))
-    st = ops.hs_batch(pairs, tile_shape=0)
+    st = ops.hs_batch(pairs, tile_shape=0, schedule=schedule)
     torch.cuda.synchronize()
     assert st.cpu().tolist() == [0] * len(shapes)
     for (_, _, U, V, _, _), (Ur, Vr) in zip(pairs, refs):
         assert torch.equal(U, Ur) and torch.equal(V, Vr)
 
 
-def test_nonfinite_frame_sets_status(cuda_ok):
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_nonfinite_frame_sets_status(cuda_ok, schedule):
     import torch
     from ofb200 import _lib, ops
     a, b = _pair(torch, 64, 64, 3)
@@ -65,12 +74,13 @@ def test_nonfinite_frame_sets_status(cuda_ok):
     b2[10, 20] = float("nan")
     z = torch.zeros_like(a)
     pairs = [(a, b, z.clone(), z.clone(), 21.0, 40), (a2, b2, z.clone(), z.clone(), 21.0, 40)]
-    st = ops.hs_batch(pairs).cpu().tolist()
+    st = ops.hs_batch(pairs, schedule=schedule).cpu().tolist()
     assert st[0] == 0
     assert st[1] & _lib.ST_NONFINITE_INPUT and st[1] & _lib.ST_NONFINITE_OUTPUT
 
 
-def test_bounded_wait_runs_out_and_returns(cuda_ok):
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_bounded_wait_runs_out_and_returns(cuda_ok, schedule):
     """A wait limit of one poll: items that find their previous pass unfinished give up at
     once.  The launch ends, the failed pairs carry OF_ST_WAIT_TIMEOUT, and the pairs that
     report no error are bit-exact; afterwards the context works (a normal run follows)."""
@@ -82,7 +92,7 @@ def test_bounded_wait_runs_out_and_returns(cuda_ok):
         z = torch.zeros_like(a)
         refs.append(_solve_ref(torch, a, b, z, z, 21.0, 200))
         pairs.append((a, b, z.clone(), z.clone(), 21.0, 200))
-    st = ops.hs_batch(pairs, wait_limit=1).cpu().tolist()
+    st = ops.hs_batch(pairs, wait_limit=1, schedule=schedule).cpu().tolist()
     assert any(s & _lib.ST_WAIT_TIMEOUT for s in st)
     for s, (_, _, U, V, _, _), (Ur, Vr) in zip(st, pairs, refs):
         assert s in (0, _lib.ST_WAIT_TIMEOUT)
@@ -91,7 +101,7 @@ def test_bounded_wait_runs_out_and_returns(cuda_ok):
     for p in pairs:
         p[2].zero_()
         p[3].zero_()
-    st = ops.hs_batch(pairs).cpu().tolist()
+    st = ops.hs_batch(pairs, schedule=schedule).cpu().tolist()
     assert st == [0] * 4
     for (_, _, U, V, _, _), (Ur, Vr) in zip(pairs, refs):
         assert torch.equal(U, Ur) and torch.equal(V, Vr)
@@ -128,3 +138,16 @@ def test_fast_arithmetic_within_float32_rounding(cuda_ok):
         st = ops.hs_batch([(a, b, U, V, 21.0, 600)], tile_shape=shape, arithmetic="fast")
         assert int(st.item()) == 0
         assert max((U - Ur).abs().max().item(), (V - Vr).abs().max().item()) <= 1e-4
+
+
+def test_resident_schedule_refuses_more_tiles_than_ctas(cuda_ok):
+    """A 2048^2 pair cut into 24 x 16 tiles has more tiles than resident CTAs: the resident
+    schedule is refused with an error, and the automatic choice falls back to the queue."""
+    import torch
+    from ofb200 import _lib, ops
+    a = torch.zeros(2048, 2048, device="cuda")
+    U, V = torch.zeros_like(a), torch.zeros_like(a)
+    with pytest.raises(_lib.OfError):
+        ops.hs_batch([(a, a, U, V, 21.0, 4)], tile_shape=1, schedule="resident")
+    st = ops.hs_batch([(a, a, U, V, 21.0, 4)], tile_shape=1, schedule="auto")
+    assert int(st.item()) == 0 and float(U.abs().max()) == 0.0
