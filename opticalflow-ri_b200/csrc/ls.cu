@@ -296,9 +296,17 @@ __device__ __forceinline__ float st_h(const double* U, const double* C, const do
 constexpr int LB_T = 4, LB_TW = 56, LB_TH = 23, LB_RW = LB_TW + 2 * LB_T, LB_RH = LB_TH + 2 * LB_T;  // 64 x 31
 constexpr int LB_PLANE = LB_RW * LB_RH * 4;                  // 7936 B, a multiple of 128 (TMA destinations)
 static_assert(LB_PLANE % 128 == 0, "each staged plane must start 128-byte aligned");
-constexpr int LB_PL = LB_RW * LB_RH;                         // floats per plane
-constexpr int LB_COEF_BYTES = 8 * LB_PLANE;
-constexpr size_t LB_SMEM = LB_COEF_BYTES + 4 * LB_PLANE + 128 + 128;  // coef + 2 x (u, v) + barrier + slack
+// The sweeps update region rows 1 .. LB_RH - 2 only, so the coefficient planes are staged
+// for those rows: LB_CH rows per plane.
+constexpr int LB_CH = LB_RH - 2;
+constexpr int LB_CPLANE = LB_RW * LB_CH * 4;                 // 7424 B
+static_assert(LB_CPLANE % 128 == 0, "the u, v planes after the coefficients must start 128-byte aligned");
+constexpr int LB_PL = LB_RW * LB_CH;                         // floats per coefficient plane
+constexpr int LB_COEF_BYTES = 8 * LB_CPLANE;
+// The float64-sum pass ping-pongs (u, v) between two buffers; the float32 pass updates one
+// buffer in place (each warp keeps the old values of its band's boundary rows in registers),
+// which brings it to 75.5 KB: 3 CTAs per SM.
+constexpr size_t lb_smem(bool fast) { return LB_COEF_BYTES + (fast ? 2 : 4) * LB_PLANE + 128 + 128; }
 #ifndef OF_LS_PASS_WARPS
 #define OF_LS_PASS_WARPS 6
 #endif
@@ -366,7 +374,7 @@ __device__ __forceinline__ void lb_pair(const LbRow& U, const LbRow& C, const Lb
                                         int gy, bool own_row, double& acc_u, double& acc_v) {
   const bool T = gy == 0, B = gy == S.H - 1;
   const bool L0 = S.gx0 == 0, R0 = S.gx0 == S.W - 1, L1 = S.gx0 + 1 == 0, R1 = S.gx0 + 1 == S.W - 1;
-  const int o = row * LB_RW + S.c0;
+  const int o = (row - 1) * LB_RW + S.c0;  // coefficient rows start at region row 1
   const float* sc = S.sc;
   const float2 a = *reinterpret_cast<const float2*>(sc + o);
   const float2 b = *reinterpret_cast<const float2*>(sc + LB_PL + o);
@@ -524,7 +532,7 @@ __device__ __forceinline__ float2 lbf_hsum_edge(const LbRowF& U, const LbRowF& C
 template <bool EDGE>
 __device__ __forceinline__ void lbf_pair(const LbRowF& U, const LbRowF& C, const LbRowF& D, const LbStrip& S, int row,
                                          int gy, bool own_row, float& acc_u, float& acc_v) {
-  const int o = row * LB_RW + S.c0;
+  const int o = (row - 1) * LB_RW + S.c0;  // coefficient rows start at region row 1
   const float* sc = S.sc;
   const float2 IIx = *reinterpret_cast<const float2*>(sc + o);
   const float2 IIy = *reinterpret_cast<const float2*>(sc + LB_PL + o);
@@ -579,6 +587,7 @@ __device__ __forceinline__ void lbf_pair(const LbRowF& U, const LbRowF& C, const
   const float2 nv = fmul2(ffma2(B12, bu, fmul2(B22, bv)), m1);
   const bool in0 = S.gx0 < S.W, in1 = S.gx0 + 1 < S.W;
   if (S.ou) {
+    __syncwarp();  // in place: every lane has read this row (as its window's next row) already
     *reinterpret_cast<float2*>(&S.ou[row][S.c0]) = nu;
     *reinterpret_cast<float2*>(&S.ov[row][S.c0]) = nv;
   } else if (own_row && S.own_col) {
@@ -600,37 +609,57 @@ __device__ __forceinline__ void lbf_pair(const LbRowF& U, const LbRowF& C, const
   }
 }
 
+// The old values a band needs from outside it, read before any warp of the CTA writes the
+// sweep's results in place: the row above the band and its first row (the window's start)
+// and the row below it.
+template <bool EDGE>
+__device__ __forceinline__ void lbf_edges(LbRowF& A, LbRowF& B, LbRowF& E, const LbPlane* su, const LbPlane* sv,
+                                          const LbCols& cols, int r0, int n, int rlo, int rhi) {
+  lbf_load<EDGE>(A, su, sv, EDGE ? clampi(r0 - 1, rlo, rhi) : r0 - 1, cols);
+  lbf_load<EDGE>(B, su, sv, r0, cols);
+  lbf_load<EDGE>(E, su, sv, EDGE ? clampi(r0 + n, rlo, rhi) : r0 + n, cols);
+}
+
+// One float32 sweep of a lane's band, rows [r0, r0 + n), in place: the window starts from
+// A, B (lbf_edges) and takes E for the row below the band; every other row is read from
+// shared memory before this warp overwrites it (the rows of the band belong to this warp).
 template <bool EDGE>
 __device__ __forceinline__ void lbf_strip(const LbPlane* su, const LbPlane* sv, const LbStrip& S, const LbCols& cols,
-                                          int r0, int n, int rlo, int rhi, double& acc_u, double& acc_v) {
-  LbRowF A, B, C;
+                                          int r0, int n, int rlo, int rhi, LbRowF& A, LbRowF& B, const LbRowF& E,
+                                          double& acc_u, double& acc_v) {
+  LbRowF C;
   float au = 0.f, av = 0.f;
-#define LB_ROW(r) (EDGE ? clampi((r), rlo, rhi) : (r))
+  const int rend = r0 + n;
 #define LB_OWN(row) ((row) >= LB_T && (row) < LB_T + LB_TH)
-  lbf_load<EDGE>(A, su, sv, LB_ROW(r0 - 1), cols);
-  lbf_load<EDGE>(B, su, sv, r0, cols);
+#define LB_NEXT(X, r)                                                     \
+  do {                                                                    \
+    if ((r) == rend)                                                      \
+      X = E;                                                              \
+    else                                                                  \
+      lbf_load<EDGE>(X, su, sv, EDGE ? clampi((r), rlo, rhi) : (r), cols); \
+  } while (0)
 #pragma unroll 1
   for (int r = 0; r < n; r += 3) {
     const int row = r0 + r;
-    lbf_load<EDGE>(C, su, sv, LB_ROW(row + 1), cols);
+    LB_NEXT(C, row + 1);
     lbf_pair<EDGE>(A, B, C, S, row, S.gy0 + r, LB_OWN(row), au, av);
     if (r + 1 < n) {
-      lbf_load<EDGE>(A, su, sv, LB_ROW(row + 2), cols);
+      LB_NEXT(A, row + 2);
       lbf_pair<EDGE>(B, C, A, S, row + 1, S.gy0 + r + 1, LB_OWN(row + 1), au, av);
     }
     if (r + 2 < n) {
-      lbf_load<EDGE>(B, su, sv, LB_ROW(row + 3), cols);
+      LB_NEXT(B, row + 3);
       lbf_pair<EDGE>(C, A, B, S, row + 2, S.gy0 + r + 2, LB_OWN(row + 2), au, av);
     }
   }
+#undef LB_NEXT
 #undef LB_OWN
-#undef LB_ROW
   acc_u += (double)au;
   acc_v += (double)av;
 }
 
 template <bool FAST, int NW>
-__global__ void __launch_bounds__(32 * NW, 2) ls_pass_kernel(const __grid_constant__ CUtensorMap tm_coef,
+__global__ void __launch_bounds__(32 * NW, (FAST && NW == 6) ? 3 : 2) ls_pass_kernel(const __grid_constant__ CUtensorMap tm_coef,
                                                          const __grid_constant__ CUtensorMap tm_u0,
                                                          const __grid_constant__ CUtensorMap tm_v0,
                                                          const __grid_constant__ CUtensorMap tm_u1,
@@ -652,7 +681,8 @@ __global__ void __launch_bounds__(32 * NW, 2) ls_pass_kernel(const __grid_consta
   // ping-pong buffer q: u at base + COEF + 2q planes, v right after it
 #define LB_U(q) reinterpret_cast<LbPlane*>(base + LB_COEF_BYTES + (2 * (q)) * LB_PLANE)
 #define LB_V(q) reinterpret_cast<LbPlane*>(base + LB_COEF_BYTES + (2 * (q) + 1) * LB_PLANE)
-  uint64_t* bar = reinterpret_cast<uint64_t*>(base + LB_COEF_BYTES + 4 * LB_PLANE);  // coefficients
+  // the barriers follow the (u, v) buffers: 2 planes in place (float32 pass), else 4
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + LB_COEF_BYTES + (FAST ? 2 : 4) * LB_PLANE);  // coefficients
   uint64_t* bar2 = bar + 1;                                                           // u, v
   const int x0 = blockIdx.x * LB_TW, y0 = blockIdx.y * LB_TH;
   const int lane = threadIdx.x, warp = threadIdx.y;
@@ -665,7 +695,7 @@ __global__ void __launch_bounds__(32 * NW, 2) ls_pass_kernel(const __grid_consta
   const bool pre = !P.last;  // the launch after the last pass only rolls back: no prefetch
   if (pre && t == 0) {
     mbar_expect_tx(bar, LB_COEF_BYTES);
-    tma_load_3d((void*)sc, &tm_coef, x0 - LB_T, y0 - LB_T, 0, bar);
+    tma_load_3d((void*)sc, &tm_coef, x0 - LB_T, y0 - LB_T + 1, 0, bar);
   }
   asm volatile("griddepcontrol.wait;" ::: "memory");
   // Pass p reads ping-pong buffer p & 1 and writes the other.  A pass that the stop rule
@@ -693,7 +723,7 @@ __global__ void __launch_bounds__(32 * NW, 2) ls_pass_kernel(const __grid_consta
   if (t == 0) {
     if (!pre) {
       mbar_expect_tx(bar, LB_COEF_BYTES);
-      tma_load_3d((void*)sc, &tm_coef, x0 - LB_T, y0 - LB_T, 0, bar);
+      tma_load_3d((void*)sc, &tm_coef, x0 - LB_T, y0 - LB_T + 1, 0, bar);
     }
     mbar_expect_tx(bar2, 2 * LB_PLANE);
     tma_load_2d(LB_U(0), tm_u, x0 - LB_T, y0 - LB_T, bar2);
@@ -737,7 +767,8 @@ __global__ void __launch_bounds__(32 * NW, 2) ls_pass_kernel(const __grid_consta
   __syncthreads();
 #pragma unroll 1
   for (int s = 0; s < nsw; s++) {
-    const int in = s & 1, out = in ^ 1;
+    // the float32 pass updates buffer 0 in place; the float64-sum pass ping-pongs
+    const int in = FAST ? 0 : s & 1, out = FAST ? 0 : in ^ 1;
     const bool last = s == nsw - 1;
     double au = 0.0, av = 0.0;
     // sweep s computes the rows at least s + 1 from the region's edge (later sweeps read no
@@ -745,6 +776,16 @@ __global__ void __launch_bounds__(32 * NW, 2) ls_pass_kernel(const __grid_consta
     const int lo = max(1 + s, rlo), hi = min(LB_RH - 1 - s, rhi + 1);
     const int n = hi - lo;
     const int ra = lo + (n * warp) / NW, rb = lo + (n * (warp + 1)) / NW;
+    LbRowF A, B, E;
+    if (FAST) {
+      if (rb > ra) {
+        if (edge)
+          lbf_edges<true>(A, B, E, LB_U(0), LB_V(0), cols, ra, rb - ra, rlo, rhi);
+        else
+          lbf_edges<false>(A, B, E, LB_U(0), LB_V(0), cols, ra, rb - ra, rlo, rhi);
+      }
+      if (!last) __syncthreads();  // every band's boundary rows are read before any row is rewritten
+    }
     if (rb > ra) {
       S.su = LB_U(in);
       S.sv = LB_V(in);
@@ -756,9 +797,9 @@ __global__ void __launch_bounds__(32 * NW, 2) ls_pass_kernel(const __grid_consta
       S.gy0 = y0 - LB_T + ra;
       if (FAST) {
         if (edge)
-          lbf_strip<true>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
+          lbf_strip<true>(LB_U(0), LB_V(0), S, cols, ra, rb - ra, rlo, rhi, A, B, E, au, av);
         else
-          lbf_strip<false>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
+          lbf_strip<false>(LB_U(0), LB_V(0), S, cols, ra, rb - ra, rlo, rhi, A, B, E, au, av);
       } else {
         if (edge)
           lb_strip<true>(LB_U(in), LB_V(in), S, cols, ra, rb - ra, rlo, rhi, au, av);
@@ -898,7 +939,7 @@ extern "C" int of_ls_solve_mode(const float* I0, const float* I1, float* U, floa
   CUtensorMap tm_coef, tm_u[2], tm_v[2];
   {
     uint64_t d3[3] = {(uint64_t)W, (uint64_t)H, 8}, s3[2] = {(uint64_t)P * 4, (uint64_t)N * 4};
-    uint32_t b3[3] = {LB_RW, LB_RH, 8};
+    uint32_t b3[3] = {LB_RW, LB_CH, 8};  // region rows 1 .. LB_RH - 2
     int rc = tmap_f32(&tm_coef, coef, 3, d3, s3, b3);
     if (rc) return rc;
     uint64_t d2[2] = {(uint64_t)W, (uint64_t)H}, s2[1] = {(uint64_t)P * 4};
@@ -909,9 +950,9 @@ extern "C" int of_ls_solve_mode(const float* I0, const float* I1, float* U, floa
     }
   }
   {
-    cudaError_t e = OF_SMEM_OPT_IN((ls_pass_kernel<false, LB_WARPS>), LB_SMEM);
-    if (e == cudaSuccess) e = OF_SMEM_OPT_IN((ls_pass_kernel<true, 6>), LB_SMEM);
-    if (e == cudaSuccess) e = OF_SMEM_OPT_IN((ls_pass_kernel<true, 8>), LB_SMEM);
+    cudaError_t e = OF_SMEM_OPT_IN((ls_pass_kernel<false, LB_WARPS>), lb_smem(false));
+    if (e == cudaSuccess) e = OF_SMEM_OPT_IN((ls_pass_kernel<true, 6>), lb_smem(true));
+    if (e == cudaSuccess) e = OF_SMEM_OPT_IN((ls_pass_kernel<true, 8>), lb_smem(true));
     if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_ls_solve: %s", cudaGetErrorString(e));
   }
   // control block, flags, counters, redo counts and sums are contiguous: one memset
@@ -922,11 +963,12 @@ extern "C" int of_ls_solve_mode(const float* I0, const float* I1, float* U, floa
   ls_prep_kernel<<<dim3((W + 31) / 32, (H + 7) / 8), 256, 0, st>>>(I0, I1, pitch, ctrl->maxkey, V, U, coef, N,
                                                                  ub[0], vb[0], H, W, P, h);
   double inv_n = 1.0 / ((double)H * (double)W);
-  // warps per CTA: 6 for the float64 pass (its registers allow 2 CTAs of 6); the float32
-  // pass defaults to 8 (OFB_LS_FAST_WARPS=6 selects 6)
+  // warps per CTA: 6 for the float64 pass (its registers allow 2 CTAs of 6); 6 for the
+  // float32 pass too (96 registers and 75.5 KB of shared memory: 3 CTAs per SM;
+  // OFB_LS_FAST_WARPS=8 selects 8 warps, 2 CTAs per SM)
   static const int fast_nw = [] {
     const char* e = getenv("OFB_LS_FAST_WARPS");
-    return (e && atoi(e) == 6) ? 6 : 8;
+    return (e && atoi(e) == 8) ? 8 : 6;
   }();
   const int nw = fast ? fast_nw : LB_WARPS;
   dim3 pgrd((W + LB_TW - 1) / LB_TW, (H + LB_TH - 1) / LB_TH), pblk(32, nw);
@@ -941,7 +983,7 @@ extern "C" int of_ls_solve_mode(const float* I0, const float* I1, float* U, floa
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = pgrd;
     cfg.blockDim = pblk;
-    cfg.dynamicSmemBytes = LB_SMEM;
+    cfg.dynamicSmemBytes = lb_smem(fast);
     cfg.stream = st;
     cfg.attrs = dependent ? pdl : nullptr;
     cfg.numAttrs = dependent ? 1 : 0;
