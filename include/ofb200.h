@@ -132,6 +132,15 @@ int of_hs_derivatives(const float* I0, const float* I1, float* fx, float* fy, fl
                       void* stream);
 int of_hs_solve(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float alpha,
                 int niter, double* err_out, void* workspace, size_t workspace_bytes, void* stream);
+/* The same solve in one persistent launch (of_hs_batch with one pair, device work queue):
+ * the same results bit for bit, for callers that solve one pair at a time (its latency is
+ * a chain of passes rather than a chain of launches).  Beside other launches on other
+ * streams it stays correct but gains nothing: there of_hs_solve, whose short launches
+ * interleave with the other streams' work, is the faster choice.  The workspace is
+ * of_hs_workspace_size's.  A bounded wait that gave up (OF_ST_WAIT_TIMEOUT) makes err_out NaN. */
+int of_hs_solve_persistent(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch,
+                           float alpha, int niter, double* err_out, void* workspace, size_t workspace_bytes,
+                           void* stream);
 
 /* ---------------------------------------------------------------------------------
  * Batches of frame pairs (the batched workload of uneven pairs).  Per-pair status words:

@@ -77,16 +77,17 @@ __global__ void hs_sweep_kernel(const float* __restrict__ fx, const float* __res
 // and out-of-image cells are neither computed nor read.  Each cell's arithmetic is
 // hs_sweep_kernel's: the averaging weights are float32 values (24-bit mantissas), so every
 // product with a float32 sample is exact in double and fma(v, w, acc) rounds exactly as
-// the separate multiply and add.
+// the separate multiply and add.  U and V sit in shared memory as float64 copies of their
+// float32 values, so the float64 sums read their operands without a conversion each.
 constexpr int HB_T = 4, HB_TW = 56, HB_TH = 32, HB_RW = HB_TW + 2 * HB_T, HB_RH = HB_TH + 2 * HB_T;  // 64 x 40
 constexpr int HB_PL = HB_RW * HB_RH;
-constexpr size_t HB_SMEM = 7 * (size_t)HB_PL * sizeof(float);  // fx, fy, ft, U x2, V x2: 70 KB
+constexpr size_t HB_SMEM = 3 * (size_t)HB_PL * sizeof(float) + 4 * (size_t)HB_PL * sizeof(double);  // 110 KB
 
 template <bool EDGE>
 __device__ __forceinline__ void hb_sweep(const float* __restrict__ sfx, const float* __restrict__ sfy,
-                                         const float* __restrict__ sft, const float* __restrict__ su,
-                                         const float* __restrict__ sv, float* __restrict__ du, float* __restrict__ dv,
-                                         int s, int x0, int y0, int H, int W, float a2) {
+                                         const float* __restrict__ sft, const double* __restrict__ su,
+                                         const double* __restrict__ sv, double* __restrict__ du,
+                                         double* __restrict__ dv, int s, int x0, int y0, int H, int W, float a2) {
   const double wc = (double)(1.0f / 12.0f), we = (double)(1.0f / 6.0f);
   const int c = threadIdx.x & (HB_RW - 1), g = threadIdx.x >> 6;
   if (c < 1 + s || c >= HB_RW - 1 - s) return;
@@ -107,22 +108,22 @@ __device__ __forceinline__ void hb_sweep(const float* __restrict__ sfx, const fl
     }
     const int om = rm * HB_RW, o0 = r * HB_RW, op = rp * HB_RW;
     double a = 0.0, b = 0.0;
-    a = __fma_rn((double)su[om + cm], wc, a); b = __fma_rn((double)sv[om + cm], wc, b);
-    a = __fma_rn((double)su[om + c], we, a);  b = __fma_rn((double)sv[om + c], we, b);
-    a = __fma_rn((double)su[om + cp], wc, a); b = __fma_rn((double)sv[om + cp], wc, b);
-    a = __fma_rn((double)su[o0 + cm], we, a); b = __fma_rn((double)sv[o0 + cm], we, b);
-    a = __fma_rn((double)su[o0 + cp], we, a); b = __fma_rn((double)sv[o0 + cp], we, b);
-    a = __fma_rn((double)su[op + cm], wc, a); b = __fma_rn((double)sv[op + cm], wc, b);
-    a = __fma_rn((double)su[op + c], we, a);  b = __fma_rn((double)sv[op + c], we, b);
-    a = __fma_rn((double)su[op + cp], wc, a); b = __fma_rn((double)sv[op + cp], wc, b);
+    a = __fma_rn(su[om + cm], wc, a); b = __fma_rn(sv[om + cm], wc, b);
+    a = __fma_rn(su[om + c], we, a);  b = __fma_rn(sv[om + c], we, b);
+    a = __fma_rn(su[om + cp], wc, a); b = __fma_rn(sv[om + cp], wc, b);
+    a = __fma_rn(su[o0 + cm], we, a); b = __fma_rn(sv[o0 + cm], we, b);
+    a = __fma_rn(su[o0 + cp], we, a); b = __fma_rn(sv[o0 + cp], we, b);
+    a = __fma_rn(su[op + cm], wc, a); b = __fma_rn(sv[op + cm], wc, b);
+    a = __fma_rn(su[op + c], we, a);  b = __fma_rn(sv[op + c], we, b);
+    a = __fma_rn(su[op + cp], wc, a); b = __fma_rn(sv[op + cp], wc, b);
     const float ua = (float)a, va = (float)b;
     const int i = o0 + c;
     const float gxv = sfx[i], gyv = sfy[i];
     const float num = __fadd_rn(__fadd_rn(__fmul_rn(gxv, ua), __fmul_rn(gyv, va)), sft[i]);
     const float den = __fadd_rn(__fadd_rn(a2, __fmul_rn(gxv, gxv)), __fmul_rn(gyv, gyv));
     const float der = __fdiv_rn(num, den);
-    du[i] = __fsub_rn(ua, __fmul_rn(gxv, der));
-    dv[i] = __fsub_rn(va, __fmul_rn(gyv, der));
+    du[i] = (double)__fsub_rn(ua, __fmul_rn(gxv, der));
+    dv[i] = (double)__fsub_rn(va, __fmul_rn(gyv, der));
   }
 }
 
@@ -135,9 +136,10 @@ __global__ void __launch_bounds__(256) hs_pass_kernel(const float* __restrict__ 
   float* sfx = hb_sm;
   float* sfy = sfx + HB_PL;
   float* sft = sfy + HB_PL;
-  // ping-pong buffer q: u at sft + (1 + 2q) planes, v right after it
-#define HB_U(q) (sft + (1 + 2 * (q)) * HB_PL)
-#define HB_V(q) (sft + (2 + 2 * (q)) * HB_PL)
+  // ping-pong buffer q (float64): u at plane 2q after the float planes, v right after it
+  double* const hb_uv = reinterpret_cast<double*>(sft + HB_PL);
+#define HB_U(q) (hb_uv + (2 * (q)) * HB_PL)
+#define HB_V(q) (hb_uv + (1 + 2 * (q)) * HB_PL)
   const int x0 = blockIdx.x * HB_TW, y0 = blockIdx.y * HB_TH;
   for (int k = threadIdx.x; k < HB_PL; k += 256) {
     const int r = k / HB_RW, c = k - r * HB_RW;
@@ -161,15 +163,15 @@ __global__ void __launch_bounds__(256) hs_pass_kernel(const float* __restrict__ 
       hb_sweep<false>(sfx, sfy, sft, HB_U(q), HB_V(q), HB_U(q ^ 1), HB_V(q ^ 1), s, x0, y0, H, W, a2);
     __syncthreads();
   }
-  const float* fu = HB_U(nsw & 1);
-  const float* fv = HB_V(nsw & 1);
+  const double* fu = HB_U(nsw & 1);
+  const double* fv = HB_V(nsw & 1);
   for (int k = threadIdx.x; k < HB_TW * HB_TH; k += 256) {
     const int r = k / HB_TW, c = k - r * HB_TW;
     const int y = y0 + r, x = x0 + c;
     if (y >= H || x >= W) continue;
     const int o = (r + HB_T) * HB_RW + c + HB_T;
-    Un[(size_t)y * pitch + x] = fu[o];
-    Vn[(size_t)y * pitch + x] = fv[o];
+    Un[(size_t)y * pitch + x] = (float)fu[o];
+    Vn[(size_t)y * pitch + x] = (float)fv[o];
   }
 #undef HB_U
 #undef HB_V
@@ -211,8 +213,11 @@ __global__ void sqdiff2_kernel(const float* __restrict__ a, const float* __restr
   }
 }
 
-__global__ void hs_err_kernel(const double* acc, double n, double* err_out) {
-  *err_out = (sqrt(acc[0]) + sqrt(acc[1])) / n;
+// status (optional): a persistent solve's status word; a solve whose bounded waits gave up
+// reports a NaN error
+__global__ void hs_err_kernel(const double* acc, double n, double* err_out, const int* status) {
+  const bool failed = status && (*status & OF_ST_WAIT_TIMEOUT);
+  *err_out = failed ? __longlong_as_double(0x7ff8000000000000ll) : (sqrt(acc[0]) + sqrt(acc[1])) / n;
 }
 
 }  // namespace ofb
@@ -227,12 +232,28 @@ extern "C" int of_hs_derivatives(const float* I0, const float* I1, float* fx, fl
   return check_launch("of_hs_derivatives");
 }
 
+// of_hs_solve_persistent: one pair through the persistent kernel of hsq.cu (of_hs_batch,
+// device work queue: items only wait for items of running CTAs, so it is correct beside any
+// other work on the GPU, if slower there).
+constexpr int kHsSolveShape = 3;  // of_hs_batch tile shape for one pair: 32 x 32 regions, 8 sweeps per pass
+
+static size_t hs_persistent_ws(int H, int W, int pitch) {
+  OfHsBatchPair q = {nullptr, nullptr, nullptr, nullptr, H, W, pitch, 0.f, 1};
+  return of_hs_batch_workspace_size(&q, 1);
+}
+
+// Covers both of_hs_solve and of_hs_solve_persistent.
 extern "C" size_t of_hs_workspace_size(int H, int W, int pitch) {
-  Sizer s;
   size_t N = (size_t)H * pitch;
+  Sizer s;  // of_hs_solve
   for (int i = 0; i < 7; i++) s.take<float>(N);
   s.take<double>(2);
-  return s.off;
+  Sizer q;  // of_hs_solve_persistent: initial flow (for the error), sums, status, batch workspace
+  q.take<float>(2 * N);
+  q.take<double>(2);
+  q.take<int>(1);
+  q.take<unsigned char>(hs_persistent_ws(H, W, pitch));
+  return s.off > q.off ? s.off : q.off;
 }
 
 extern "C" int of_hs_solve(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch, float alpha,
@@ -272,7 +293,7 @@ extern "C" int of_hs_solve(const float* I0, const float* I1, float* U, float* V,
       cudaMemsetAsync(acc, 0, 2 * sizeof(double), st);
       dim3 g2((W + 255) / 256 < 4 ? (W + 255) / 256 : 4, H < 256 ? H : 256);
       sqdiff2_kernel<<<g2, 256, 0, st>>>(U, U0, V, V0, H, W, pitch, acc);
-      hs_err_kernel<<<1, 1, 0, st>>>(acc, (double)H * (double)W, err_out);
+      hs_err_kernel<<<1, 1, 0, st>>>(acc, (double)H * (double)W, err_out, nullptr);
       n += 2;
     }
     return check_launch("of_hs_solve", n);
@@ -294,8 +315,46 @@ extern "C" int of_hs_solve(const float* I0, const float* I1, float* U, float* V,
     cudaMemsetAsync(acc, 0, 2 * sizeof(double), st);
     dim3 g2((W + 255) / 256 < 4 ? (W + 255) / 256 : 4, H < 256 ? H : 256);
     sqdiff2_kernel<<<g2, 256, 0, st>>>(U, U0, V, V0, H, W, pitch, acc);
-    hs_err_kernel<<<1, 1, 0, st>>>(acc, (double)H * (double)W, err_out);
+    hs_err_kernel<<<1, 1, 0, st>>>(acc, (double)H * (double)W, err_out, nullptr);
     n += 2;
   }
   return check_launch("of_hs_solve", n);
+}
+
+extern "C" int of_hs_solve_persistent(const float* I0, const float* I1, float* U, float* V, int H, int W, int pitch,
+                                      float alpha, int niter, double* err_out, void* workspace, size_t workspace_bytes,
+                                      void* stream) {
+  OF_REQUIRE(!bad_plane(I0, H, W, pitch) && I1 && U && V, "of_hs_solve_persistent: bad plane");
+  OF_REQUIRE(niter >= 0, "of_hs_solve_persistent: niter < 0");
+  if (!workspace || workspace_bytes < of_hs_workspace_size(H, W, pitch))
+    return set_error(OF_ERR_WORKSPACE, "of_hs_solve_persistent: workspace too small (%zu < %zu)", workspace_bytes,
+                     of_hs_workspace_size(H, W, pitch));
+  cudaStream_t st = as_stream(stream);
+  const size_t N = (size_t)H * pitch;
+  Carver c(workspace, workspace_bytes);
+  float* U0 = c.take<float>(2 * N);
+  float* V0 = U0 + N;
+  double* acc = c.take<double>(2);
+  int* status = c.take<int>(1);
+  const size_t bws = hs_persistent_ws(H, W, pitch);
+  void* bw = c.take<unsigned char>(bws);
+  long long n = 0;
+  if (err_out) {
+    copy2_kernel<<<dim3((W + 255) / 256, H), 256, 0, st>>>(U, V, U0, V0, W, pitch);
+    n++;
+  }
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), st);
+  if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_solve_persistent: %s", cudaGetErrorString(e));
+  OfHsBatchPair q = {I0, I1, U, V, H, W, pitch, alpha, niter};
+  OfTuning tun = {kHsSolveShape, 0, OF_HS_EXACT, OF_HS_SCHED_QUEUE};
+  const int rc = of_hs_batch(&q, 1, &tun, status, 1ll << 20, bw, bws, stream);
+  if (rc != OF_OK) return rc;
+  if (err_out) {
+    cudaMemsetAsync(acc, 0, 2 * sizeof(double), st);
+    dim3 g2((W + 255) / 256 < 4 ? (W + 255) / 256 : 4, H < 256 ? H : 256);
+    sqdiff2_kernel<<<g2, 256, 0, st>>>(U, U0, V, V0, H, W, pitch, acc);
+    hs_err_kernel<<<1, 1, 0, st>>>(acc, (double)H * (double)W, err_out, status);
+    n += 2;
+  }
+  return check_launch("of_hs_solve_persistent", n);
 }

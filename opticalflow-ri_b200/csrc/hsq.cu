@@ -5,7 +5,7 @@
 // counter to CTAs that stay resident for the whole launch.  Pass 0 of a pair computes its
 // derivative planes (computeDerivatives, :106-126) and copies the initial U, V for a tile;
 // pass p >= 1 runs up to HQ_T Jacobi sweeps (HS_helper, :61-70) on the tile with a halo of
-// HQ_T cells staged in shared memory (the temporal blocking of hs_pass_kernel), reading
+// HQ_T cells staged in shared memory (temporal blocking), reading
 // the previous pass's fields and writing the next buffer of a ping-pong pair.  An item of
 // pass p waits only for its own tile and its (up to) 8 neighbouring tiles to have finished
 // pass p - 1 (a counter of finished passes per tile): the halo of T cells lies inside those
@@ -19,6 +19,8 @@
 // (still counted, so nothing waits on it).
 // Cross-CTA data goes through L2 only (ld.global.cg / st.global.cg), published by
 // __syncthreads + __threadfence + atomicAdd and consumed after the counter is observed.
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace ofb {
@@ -126,13 +128,24 @@ __device__ __forceinline__ int hq_wait(const unsigned int* done, unsigned int ti
   return !(timeout || before);
 }
 
-// Up to T sweeps on one tile: region RW x RH = (TW + 2T) x (TH + 2T) in shared memory,
-// hb_sweep's arithmetic and border handling.
+// Up to T sweeps on one tile: region RW x RH = (TW + 2T) x (TH + 2T) in shared memory.
+// Sweep s computes the cells at least s + 1 from the region's edge, which after T sweeps
+// leaves exactly the owned cells exact.  On image borders every neighbour index goes
+// through hs_sweep_kernel's 'mirror' map (mapped neighbours stay within one row / column of
+// their cell, so inside the region), and out-of-image cells are neither computed nor read.
+// Each cell's arithmetic is hs_sweep_kernel's: the averaging weights are float32 values
+// (24-bit mantissas), so every product with a float32 sample is exact in double and
+// fma(v, w, acc) rounds exactly as the separate multiply and add.
+// Shared memory: the derivative planes as float32 and two (u, v) buffers, float64 for the
+// bit-exact arithmetic (the values are float32 results, held exactly, so the reference's
+// float64 stencil sums need no conversion per neighbour) and float32 for OF_HS_FAST.
 template <int RW, int RH, int T>
 struct HqTile {
   static constexpr int TW = RW - 2 * T, TH = RH - 2 * T, PL = RW * RH;
-  static constexpr size_t SMEM = 7 * (size_t)PL * sizeof(float);
+  static constexpr size_t smem(bool fast) { return 3 * (size_t)PL * 4 + 4 * (size_t)PL * (fast ? 4 : 8); }
 };
+template <bool FAST>
+using HqVal = typename std::conditional<FAST, float, double>::type;
 
 constexpr int HQ_THREADS = 256;  // threads per CTA of the queue kernel
 
@@ -140,8 +153,9 @@ constexpr int HQ_THREADS = 256;  // threads per CTA of the queue kernel
 // cells' independent arithmetic chains interleave.
 template <int RW, int RH, int T, bool EDGE, bool FAST>
 __device__ __forceinline__ void hq_cell(int k, const float* __restrict__ sfx, const float* __restrict__ sfy,
-                                        const float* __restrict__ sft, const float* su, const float* sv, float* du,
-                                        float* dv, int s, int x0, int y0, int H, int W, float a2) {
+                                        const float* __restrict__ sft, const HqVal<FAST>* su, const HqVal<FAST>* sv,
+                                        HqVal<FAST>* du, HqVal<FAST>* dv, int s, int x0, int y0, int H, int W,
+                                        float a2) {
   const double wc = (double)(1.0f / 12.0f), we = (double)(1.0f / 6.0f);
   {
     if (k >= RW * RH) return;
@@ -158,7 +172,7 @@ __device__ __forceinline__ void hq_cell(int k, const float* __restrict__ sfx, co
     }
     const int om = rm * RW, o0 = r * RW, op = rp * RW;
     float ua, va;
-    if (FAST) {  // float32 averaging: corner and edge sums, one multiply-add each
+    if constexpr (FAST) {  // float32 averaging: corner and edge sums, one multiply-add each
       const float wcf = 1.0f / 12.0f, wef = 1.0f / 6.0f;
       const float cu = __fadd_rn(__fadd_rn(su[om + cm], su[om + cp]), __fadd_rn(su[op + cm], su[op + cp]));
       const float eu = __fadd_rn(__fadd_rn(su[om + c], su[op + c]), __fadd_rn(su[o0 + cm], su[o0 + cp]));
@@ -167,15 +181,15 @@ __device__ __forceinline__ void hq_cell(int k, const float* __restrict__ sfx, co
       ua = __fmaf_rn(cu, wcf, __fmul_rn(eu, wef));
       va = __fmaf_rn(cv, wcf, __fmul_rn(ev, wef));
     } else {
-      double a = 0.0, b = 0.0;
-      a = __fma_rn((double)su[om + cm], wc, a); b = __fma_rn((double)sv[om + cm], wc, b);
-      a = __fma_rn((double)su[om + c], we, a);  b = __fma_rn((double)sv[om + c], we, b);
-      a = __fma_rn((double)su[om + cp], wc, a); b = __fma_rn((double)sv[om + cp], wc, b);
-      a = __fma_rn((double)su[o0 + cm], we, a); b = __fma_rn((double)sv[o0 + cm], we, b);
-      a = __fma_rn((double)su[o0 + cp], we, a); b = __fma_rn((double)sv[o0 + cp], we, b);
-      a = __fma_rn((double)su[op + cm], wc, a); b = __fma_rn((double)sv[op + cm], wc, b);
-      a = __fma_rn((double)su[op + c], we, a);  b = __fma_rn((double)sv[op + c], we, b);
-      a = __fma_rn((double)su[op + cp], wc, a); b = __fma_rn((double)sv[op + cp], wc, b);
+      double a = 0.0, b = 0.0;  // su, sv hold float32 values as float64: no conversions here
+      a = __fma_rn(su[om + cm], wc, a); b = __fma_rn(sv[om + cm], wc, b);
+      a = __fma_rn(su[om + c], we, a);  b = __fma_rn(sv[om + c], we, b);
+      a = __fma_rn(su[om + cp], wc, a); b = __fma_rn(sv[om + cp], wc, b);
+      a = __fma_rn(su[o0 + cm], we, a); b = __fma_rn(sv[o0 + cm], we, b);
+      a = __fma_rn(su[o0 + cp], we, a); b = __fma_rn(sv[o0 + cp], we, b);
+      a = __fma_rn(su[op + cm], wc, a); b = __fma_rn(sv[op + cm], wc, b);
+      a = __fma_rn(su[op + c], we, a);  b = __fma_rn(sv[op + c], we, b);
+      a = __fma_rn(su[op + cp], wc, a); b = __fma_rn(sv[op + cp], wc, b);
       ua = (float)a;
       va = (float)b;
     }
@@ -184,15 +198,16 @@ __device__ __forceinline__ void hq_cell(int k, const float* __restrict__ sfx, co
     const float num = __fadd_rn(__fadd_rn(__fmul_rn(gxv, ua), __fmul_rn(gyv, va)), sft[i]);
     const float den = __fadd_rn(__fadd_rn(a2, __fmul_rn(gxv, gxv)), __fmul_rn(gyv, gyv));
     const float der = __fdiv_rn(num, den);
-    du[i] = __fsub_rn(ua, __fmul_rn(gxv, der));
-    dv[i] = __fsub_rn(va, __fmul_rn(gyv, der));
+    du[i] = (HqVal<FAST>)__fsub_rn(ua, __fmul_rn(gxv, der));
+    dv[i] = (HqVal<FAST>)__fsub_rn(va, __fmul_rn(gyv, der));
   }
 }
 
 template <int RW, int RH, int T, bool EDGE, bool FAST>
 __device__ __forceinline__ void hq_sweep(const float* __restrict__ sfx, const float* __restrict__ sfy,
-                                         const float* __restrict__ sft, const float* su, const float* sv, float* du,
-                                         float* dv, int s, int x0, int y0, int H, int W, float a2) {
+                                         const float* __restrict__ sft, const HqVal<FAST>* su, const HqVal<FAST>* sv,
+                                         HqVal<FAST>* du, HqVal<FAST>* dv, int s, int x0, int y0, int H, int W,
+                                         float a2) {
 #pragma unroll 4
   for (int it = 0; it < (RW * RH + HQ_THREADS - 1) / HQ_THREADS; it++)
     hq_cell<RW, RH, T, EDGE, FAST>(it * HQ_THREADS + (int)threadIdx.x, sfx, sfy, sft, su, sv, du, dv, s, x0, y0, H,
@@ -219,10 +234,11 @@ __device__ bool hq_sweep_item(const HsqPair& P, int pass, int tile, float* sm) {
   float* sfx = sm;
   float* sfy = sfx + G::PL;
   float* sft = sfy + G::PL;
-  float* const bu0 = sft + G::PL;
-  float* const bv0 = sft + 2 * G::PL;
-  float* const bu1 = sft + 3 * G::PL;
-  float* const bv1 = sft + 4 * G::PL;
+  using V = HqVal<FAST>;
+  V* const bu0 = reinterpret_cast<V*>(sft + G::PL);  // 3 PL floats: 8-byte aligned for even PL
+  V* const bv0 = bu0 + G::PL;
+  V* const bu1 = bu0 + 2 * G::PL;
+  V* const bv1 = bu0 + 3 * G::PL;
   for (int k = threadIdx.x; k < G::PL; k += blockDim.x) {
     const int r = k / RW, c = k - r * RW;
     const int gy = y0 - T + r, gx = x0 - T + c;
@@ -238,26 +254,26 @@ __device__ bool hq_sweep_item(const HsqPair& P, int pass, int tile, float* sm) {
   const bool edge = x0 < T || y0 < T || x0 + G::TW + T > W || y0 + G::TH + T > H;
   for (int s = 0; s < nsw; s++) {
     const bool q = s & 1;
-    float* iu = q ? bu1 : bu0;
-    float* iv = q ? bv1 : bv0;
-    float* ou = q ? bu0 : bu1;
-    float* ov = q ? bv0 : bv1;
+    V* iu = q ? bu1 : bu0;
+    V* iv = q ? bv1 : bv0;
+    V* ou = q ? bu0 : bu1;
+    V* ov = q ? bv0 : bv1;
     if (edge)
       hq_sweep<RW, RH, T, true, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
     else
       hq_sweep<RW, RH, T, false, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
     __syncthreads();
   }
-  const float* fu = (nsw & 1) ? bu1 : bu0;
-  const float* fv = (nsw & 1) ? bv1 : bv0;
+  const V* fu = (nsw & 1) ? bu1 : bu0;
+  const V* fv = (nsw & 1) ? bv1 : bv0;
   bool finite = true;
   for (int k = threadIdx.x; k < G::TW * G::TH; k += blockDim.x) {
     const int r = k / G::TW, c = k - r * G::TW;
     const int y = y0 + r, x = x0 + c;
     if (y >= H || x >= W) continue;
     const int o = (r + T) * RW + c + T;
-    __stcg(dstu + (size_t)y * pitch + x, fu[o]);
-    __stcg(dstv + (size_t)y * pitch + x, fv[o]);
+    __stcg(dstu + (size_t)y * pitch + x, (float)fu[o]);
+    __stcg(dstv + (size_t)y * pitch + x, (float)fv[o]);
     finite = finite && isfinite(fu[o]) && isfinite(fv[o]);
   }
   return finite || p != np - 1;
@@ -363,10 +379,11 @@ __global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restri
   float* sfx = hq_sm;
   float* sfy = sfx + G::PL;
   float* sft = sfy + G::PL;
-  float* const bu0 = sft + G::PL;
-  float* const bv0 = sft + 2 * G::PL;
-  float* const bu1 = sft + 3 * G::PL;
-  float* const bv1 = sft + 4 * G::PL;
+  using V = HqVal<FAST>;
+  V* const bu0 = reinterpret_cast<V*>(sft + G::PL);  // 3 PL floats: 8-byte aligned for even PL
+  V* const bv0 = bu0 + G::PL;
+  V* const bu1 = bu0 + 2 * G::PL;
+  V* const bv1 = bu0 + 3 * G::PL;
   const bool edge = x0 < T || y0 < T || x0 + G::TW + T > W || y0 + G::TH + T > H;
   // stage 0
   bool ok = true;
@@ -419,25 +436,25 @@ __global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restri
       const int nsw = min(T, P.niter - p * T);
       for (int s = 0; s < nsw; s++) {
         const bool q = s & 1;
-        float* iu = q ? bu1 : bu0;
-        float* iv = q ? bv1 : bv0;
-        float* ou = q ? bu0 : bu1;
-        float* ov = q ? bv0 : bv1;
+        V* iu = q ? bu1 : bu0;
+        V* iv = q ? bv1 : bv0;
+        V* ou = q ? bu0 : bu1;
+        V* ov = q ? bv0 : bv1;
         if (edge)
           hq_sweep<RW, RH, T, true, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
         else
           hq_sweep<RW, RH, T, false, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
         __syncthreads();
       }
-      const float* fu = (nsw & 1) ? bu1 : bu0;
-      const float* fv = (nsw & 1) ? bv1 : bv0;
+      const V* fu = (nsw & 1) ? bu1 : bu0;
+      const V* fv = (nsw & 1) ? bv1 : bv0;
       for (int k = threadIdx.x; k < G::TW * G::TH; k += blockDim.x) {
         const int r = k / G::TW, c = k - r * G::TW;
         const int y = y0 + r, x = x0 + c;
         if (y >= H || x >= W) continue;
         const int o = (r + T) * RW + c + T;
-        __stcg(dstu + (size_t)y * pitch + x, fu[o]);
-        __stcg(dstv + (size_t)y * pitch + x, fv[o]);
+        __stcg(dstu + (size_t)y * pitch + x, (float)fu[o]);
+        __stcg(dstv + (size_t)y * pitch + x, (float)fv[o]);
         if (p == np - 1) ok = ok && isfinite(fu[o]) && isfinite(fv[o]);
       }
     }
@@ -470,7 +487,7 @@ namespace {
 struct HsqShape {
   int rw, rh, t;
 };
-constexpr HsqShape kHsqShapes[] = {{64, 40, 4}, {32, 24, 4}, {64, 24, 4}, {32, 32, 8}};
+constexpr HsqShape kHsqShapes[] = {{64, 40, 4}, {32, 24, 4}, {64, 24, 4}, {32, 32, 8}, {40, 40, 8}};
 constexpr int kHsqNumShapes = sizeof(kHsqShapes) / sizeof(kHsqShapes[0]);
 
 template <int RW, int RH, int T, bool FAST>
@@ -484,14 +501,14 @@ int hsq_resident(bool fast, bool resident, int* per_sm) {
   using G = HqTile<RW, RH, T>;
   cudaError_t e;
   if (resident)
-    e = fast ? OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, true>), G::SMEM)
-             : OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, false>), G::SMEM);
+    e = fast ? OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, true>), G::smem(true))
+             : OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, false>), G::smem(false));
   else
-    e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true>), G::SMEM)
-             : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false>), G::SMEM);
+    e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true>), G::smem(true))
+             : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false>), G::smem(false));
   if (e != cudaSuccess) return -1;
   const void* k = fast ? hsq_kernel_ptr<RW, RH, T, true>(resident) : hsq_kernel_ptr<RW, RH, T, false>(resident);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, HQ_THREADS, G::SMEM);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, HQ_THREADS, G::smem(fast));
   return e == cudaSuccess ? 0 : -1;
 }
 
@@ -502,14 +519,14 @@ cudaError_t hsq_launch(bool fast, bool resident, int grid, const HsqPair* pairs,
   using G = HqTile<RW, RH, T>;
   if (resident) {
     if (fast)
-      hsr_kernel<RW, RH, T, true><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, done, status, wait_limit, err_flag);
+      hsr_kernel<RW, RH, T, true><<<grid, HQ_THREADS, G::smem(fast), st>>>(pairs, n, done, status, wait_limit, err_flag);
     else
-      hsr_kernel<RW, RH, T, false><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, done, status, wait_limit, err_flag);
+      hsr_kernel<RW, RH, T, false><<<grid, HQ_THREADS, G::smem(fast), st>>>(pairs, n, done, status, wait_limit, err_flag);
   } else if (fast) {
-    hsq_kernel<RW, RH, T, true><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done,
+    hsq_kernel<RW, RH, T, true><<<grid, HQ_THREADS, G::smem(fast), st>>>(pairs, n, tiles_total, max_passes, ticket, done,
                                                                  status, wait_limit, err_flag);
   } else {
-    hsq_kernel<RW, RH, T, false><<<grid, HQ_THREADS, G::SMEM, st>>>(pairs, n, tiles_total, max_passes, ticket, done,
+    hsq_kernel<RW, RH, T, false><<<grid, HQ_THREADS, G::smem(fast), st>>>(pairs, n, tiles_total, max_passes, ticket, done,
                                                                   status, wait_limit, err_flag);
   }
   return cudaGetLastError();
@@ -629,7 +646,8 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
       case 0: rc = hsq_resident<64, 40, 4>(fast, resident, &per_sm); break;
       case 1: rc = hsq_resident<32, 24, 4>(fast, resident, &per_sm); break;
       case 2: rc = hsq_resident<64, 24, 4>(fast, resident, &per_sm); break;
-      default: rc = hsq_resident<32, 32, 8>(fast, resident, &per_sm); break;
+      case 3: rc = hsq_resident<32, 32, 8>(fast, resident, &per_sm); break;
+      default: rc = hsq_resident<40, 40, 8>(fast, resident, &per_sm); break;
     }
     *cap = (long long)sms * per_sm;
     return rc == 0 && per_sm >= 1;
@@ -653,7 +671,8 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
     case 0: e = hsq_launch<64, 40, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
     case 1: e = hsq_launch<32, 24, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
     case 2: e = hsq_launch<64, 24, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    default: e = hsq_launch<32, 32, 8>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    case 3: e = hsq_launch<32, 32, 8>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    default: e = hsq_launch<40, 40, 8>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
   }
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: launch: %s", cudaGetErrorString(e));
   return check_launch("of_hs_batch", nl + 1);

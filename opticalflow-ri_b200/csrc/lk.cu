@@ -111,6 +111,15 @@ __device__ __forceinline__ float lk_bilinear_s(const float2* __restrict__ sJ, co
   return r;
 }
 
+// floor(x) for |x| < 2^22, as a float and as an int, on the FMA pipe: x + 1.5 * 2^23 rounded
+// toward -inf is floor(x) + 1.5 * 2^23 (that binade's unit is 1), and its low mantissa bits
+// hold the integer.
+__device__ __forceinline__ float lk_floor(float x, int& i) {
+  const float t = __fadd_rd(x, 12582912.0f);
+  i = __float_as_int(t) - 0x4B400000;
+  return __fsub_rn(t, 12582912.0f);
+}
+
 // the reference's reduce tree: (t, t+32) in-lane, then 16, 8, 4, (0+1)+(2+3)
 __device__ __forceinline__ float lk_tree(float lo, float hi) {
   float q = __fadd_rn(lo, hi);
@@ -122,6 +131,17 @@ __device__ __forceinline__ float lk_tree(float lo, float hi) {
   return __shfl_sync(0xffffffffu, t, 0);
 }
 
+// Whether sample (v, ty, tx) of lane (xid, yid) has a non-zero tile weight.
+template <bool DEF>
+__device__ __forceinline__ bool lk_on(unsigned act, int v, int ty, int tx, int xid, int yid) {
+  if (DEF) return (tx < 3 || xid < 3) && (ty < 3 || (v == 0 && yid < 3));
+  return (act >> (16 * v + 4 * ty + tx)) & 1u;
+}
+
+// DEF: the default window (27 x 27, no asymmetric mask), whose tile-weight pattern is known
+// at compile time: lane (xid, yid)'s 4th column tile is used when xid < 3, its 4th row tile
+// of the first half when yid < 3, the 4th row tile of the second half never.
+template <bool DEF>
 __global__ void __launch_bounds__(256, 2) lk_dense_kernel(const float* __restrict__ I, const float* __restrict__ J,
                                                        float* __restrict__ U, float* __restrict__ V, int H, int W,
                                                        int pitch, LkParams p, uint8_t* __restrict__ status,
@@ -210,7 +230,7 @@ __global__ void __launch_bounds__(256, 2) lk_dense_kernel(const float* __restric
       for (int ty = 0; ty < 4; ty++)
 #pragma unroll
         for (int tx = 0; tx < 4; tx++) {
-          if (!((act >> (16 * v + 4 * ty + tx)) & 1u)) continue;  // tile weight 0
+          if (!lk_on<DEF>(act, v, ty, tx, xid, yid)) continue;  // tile weight 0
           int g = (gyb + ty * 8 + yy) * LK_GP + gxb + tx * 8 + xid;
           // w is 1 here (the tile weights are products of 0 / 1 values and w == 0 is
           // skipped), so the reference's multiplications by w are exact identities
@@ -258,17 +278,21 @@ __global__ void __launch_bounds__(256, 2) lk_dense_kernel(const float* __restric
       unsigned inx = 0, iny = 0;
 #pragma unroll
       for (int t = 0; t < 4; t++) {
-        const float xs = __fsub_rn(lx[t], 0.5f), fx0 = floorf(xs);
+        // positions here are within a window of the image (the step's range test), so
+        // |xs|, |ys| < 2^22 (the ABI caps H, W) and lk_floor is floorf
+        int ix;
+        const float xs = __fsub_rn(lx[t], 0.5f), fx0 = lk_floor(xs, ix);
         xa[t] = __fsub_rn(xs, fx0);
         xoa[t] = __fsub_rn(1.f, xa[t]);
-        xr[t] = (int)fx0 - jox;
+        xr[t] = ix - jox;
         inx |= ((unsigned)xr[t] <= (unsigned)(LK_JR - 2)) << t;
 #pragma unroll
         for (int v = 0; v < 2; v++) {
-          const float ys = __fsub_rn(ly[v][t], 0.5f), fy0 = floorf(ys);
+          int iy;
+          const float ys = __fsub_rn(ly[v][t], 0.5f), fy0 = lk_floor(ys, iy);
           yb[v][t] = __fsub_rn(ys, fy0);
           yob[v][t] = __fsub_rn(1.f, yb[v][t]);
-          yr[v][t] = (int)fy0 - joy;
+          yr[v][t] = iy - joy;
           iny |= ((unsigned)yr[v][t] <= (unsigned)(LK_JR - 2)) << (4 * v + t);
         }
       }
@@ -283,7 +307,7 @@ __global__ void __launch_bounds__(256, 2) lk_dense_kernel(const float* __restric
           for (int ty = 0; ty < 4; ty++)
 #pragma unroll
             for (int tx = 0; tx < 4; tx++) {
-              if (!((act >> (16 * v + 4 * ty + tx)) & 1u)) continue;  // tile weight 0
+              if (!lk_on<DEF>(act, v, ty, tx, xid, yid)) continue;  // tile weight 0
               int g = (gyb + ty * 8 + yy) * LK_GP + gxb + tx * 8 + xid;
               float Iv = sI[(gyb + ty * 8 + yy + 1) * LK_IP + gxb + tx * 8 + xid + 1];
               float t00, t10, t01, t11;
@@ -382,6 +406,7 @@ extern "C" int of_lk_dense(const float* I, const float* J, float* U, float* V, i
   OF_REQUIRE(!bad_plane(I, H, W, pitch) && J && U && V, "of_lk_dense: bad plane");
   OF_REQUIRE(half_win >= 1 && half_win <= 15, "of_lk_dense: half_win must be in 1..15");
   OF_REQUIRE(niter >= 0, "of_lk_dense: niter < 0");
+  OF_REQUIRE(H < (1 << 21) && W < (1 << 21), "of_lk_dense: H and W must be below 2^21");
   LkParams p;
   p.ws = 2 * half_win + 1;
   p.hw = (p.ws - 1) >> 1;
@@ -394,8 +419,12 @@ extern "C" int of_lk_dense(const float* I, const float* J, float* U, float* V, i
   OF_REQUIRE(((p.aL | p.aR | p.aT | p.aB) & ~1) == 0, "of_lk_dense: asym entries must be 0 or 1");
   p.niter = niter;
   dim3 grid((W + LK_PT - 1) / LK_PT, (H + LK_PT - 1) / LK_PT);
-  cudaError_t e = OF_SMEM_OPT_IN(lk_dense_kernel, LK_SMEM);
+  const bool def = p.ws == 27 && !(p.aL | p.aR | p.aT | p.aB);
+  cudaError_t e = def ? OF_SMEM_OPT_IN(lk_dense_kernel<true>, LK_SMEM) : OF_SMEM_OPT_IN(lk_dense_kernel<false>, LK_SMEM);
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_lk_dense: %s", cudaGetErrorString(e));
-  lk_dense_kernel<<<grid, 256, LK_SMEM, as_stream(stream)>>>(I, J, U, V, H, W, pitch, p, status, err);
+  if (def)
+    lk_dense_kernel<true><<<grid, 256, LK_SMEM, as_stream(stream)>>>(I, J, U, V, H, W, pitch, p, status, err);
+  else
+    lk_dense_kernel<false><<<grid, 256, LK_SMEM, as_stream(stream)>>>(I, J, U, V, H, W, pitch, p, status, err);
   return check_launch("of_lk_dense");
 }

@@ -11,6 +11,7 @@ them by stream), so concurrent pairs never share scratch memory.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import threading
 from dataclasses import dataclass, field
@@ -79,7 +80,6 @@ class PairBatch:
         self._lock = threading.Lock()
 
     def _pipelines(self, frames):
-        import GenericPyramidalOpticalFlow as G
         cur = torch.cuda.current_stream()
         if self._streams is None:
             self._streams = [torch.cuda.Stream() for _ in range(self.nstreams)]
@@ -90,6 +90,15 @@ class PairBatch:
             self.status.zero_()
         for s in self._streams:
             s.wait_stream(cur)
+        conc = ops.concurrent_streams() if self.nstreams > 1 else contextlib.nullcontext()
+        with conc:
+            self._enqueue(frames, outs)
+        for s in self._streams:
+            cur.wait_stream(s)
+        return outs
+
+    def _enqueue(self, frames, outs):
+        import GenericPyramidalOpticalFlow as G
         for i, ((a, b), spec) in enumerate(zip(frames, self.specs)):
             st = self._streams[i % self.nstreams]
             with torch.cuda.stream(st):
@@ -109,9 +118,6 @@ class PairBatch:
                         _lib.call("of_ls_status", ctypes.c_void_p(opt.last_iterations.data_ptr()),
                                   ctypes.c_void_p(opt.last_error.data_ptr()), LS.MAXNUM, LS.TOL,
                                   ctypes.c_void_p(self.status[i:].data_ptr()), ops.stream_ptr())
-        for s in self._streams:
-            cur.wait_stream(s)
-        return outs
 
     def _check(self, t, i, bit):
         H, W = t.shape

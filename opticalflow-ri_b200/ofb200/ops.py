@@ -8,8 +8,10 @@ libofb200.so.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import os
+import threading
 
 import numpy as np
 import torch
@@ -198,14 +200,39 @@ def scale(src: torch.Tensor, s: float, out=None) -> torch.Tensor:
 
 
 # --------------------------------------------------------------------------- A6/A7
-def hs_solve(I0, I1, U, V, alpha: float, niter: int, err: torch.Tensor | None = None):
-    """Horn-Schunck in place on U, V.  Returns (U, V, err) with err a device float64 scalar."""
+_conc = threading.local()
+
+
+@contextlib.contextmanager
+def concurrent_streams():
+    """Marks the work enqueued inside as running beside other streams' work (a multi-stream
+    batch): solvers with a one-launch persistent form use their multi-launch form there,
+    whose short launches interleave with the other streams."""
+    _conc.depth = getattr(_conc, "depth", 0) + 1
+    try:
+        yield
+    finally:
+        _conc.depth -= 1
+
+
+def in_concurrent_streams() -> bool:
+    return getattr(_conc, "depth", 0) > 0
+
+
+def hs_solve(I0, I1, U, V, alpha: float, niter: int, err: torch.Tensor | None = None, persistent=None):
+    """Horn-Schunck in place on U, V.  Returns (U, V, err) with err a device float64 scalar.
+    persistent: all sweeps in one launch (of_hs_solve_persistent) or one launch per pass of
+    4 sweeps (of_hs_solve); None picks the persistent form except inside
+    concurrent_streams().  Both give the same results bit for bit."""
     p = _same_pitch(I0, I1, U, V)
     H, W = I0.shape
+    if persistent is None:
+        persistent = not in_concurrent_streams()
     err = torch.empty((), dtype=torch.float64, device=I0.device) if err is None else err
     ws, wn = workspace(lib().of_hs_workspace_size(H, W, p), "hs")
-    call("of_hs_solve", _plane(I0, "I0")[0], _plane(I1, "I1")[0], _plane(U, "U")[0], _plane(V, "V")[0], H, W, p,
-         float(np.float32(alpha)), int(niter), ctypes.c_void_p(err.data_ptr()), ws, wn, stream_ptr())
+    call("of_hs_solve_persistent" if persistent else "of_hs_solve", _plane(I0, "I0")[0], _plane(I1, "I1")[0],
+         _plane(U, "U")[0], _plane(V, "V")[0], H, W, p, float(np.float32(alpha)), int(niter),
+         ctypes.c_void_p(err.data_ptr()), ws, wn, stream_ptr())
     return U, V, err
 
 

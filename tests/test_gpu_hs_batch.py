@@ -20,15 +20,35 @@ def _pair(torch, H, W, seed):
 def _solve_ref(torch, a, b, U0, V0, alpha, niter):
     from ofb200 import ops
     U, V = U0.clone(), V0.clone()
-    ops.hs_solve(a, b, U, V, alpha, niter)
+    ops.hs_solve(a, b, U, V, alpha, niter, persistent=False)  # one launch per pass
     return U, V
+
+
+@pytest.mark.parametrize("H,W,niter", [(256, 256, 600), (100, 300, 37), (17, 23, 9), (12, 40, 5), (64, 64, 0)])
+def test_persistent_single_solve_equals_multi_launch(cuda_ok, H, W, niter):
+    """of_hs_solve_persistent (the drop-in's single-pair form) against of_hs_solve: the
+    same U, V bit for bit, and the same error value, from a non-zero initial flow."""
+    import torch
+    from ofb200 import ops
+    a, b = _pair(torch, H, W, 31)
+    g = torch.Generator().manual_seed(H + W)
+    U0 = (torch.randn(H, W, generator=g) * 0.3).cuda()
+    V0 = (torch.randn(H, W, generator=g) * 0.3).cuda()
+    out = []
+    for persistent in (False, True):
+        U, V = U0.clone(), V0.clone()
+        _, _, err = ops.hs_solve(a, b, U, V, 21.0, niter, persistent=persistent)
+        out.append((U, V, float(err.item())))
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+    # the error's float64 sums are combined across CTAs by atomics (order-dependent last bit)
+    assert out[0][2] == pytest.approx(out[1][2], rel=1e-12, abs=0.0)
 
 
 SCHEDULES = ["queue", "resident"]
 
 
 @pytest.mark.parametrize("schedule", SCHEDULES)
-@pytest.mark.parametrize("shape_index", [0, 1, 2, 3])
+@pytest.mark.parametrize("shape_index", [0, 1, 2, 3, 4])
 def test_single_pair_config1_bit_exact(cuda_ok, shape_index, schedule):
     """256 x 256, alpha 21, 600 sweeps (the PyHSchunck_Fs3_4 calibration) in one launch."""
     import torch
