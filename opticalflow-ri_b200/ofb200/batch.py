@@ -471,7 +471,9 @@ def tune_hs_shape(frames_hs, reps=2, log=None, use_cache=True, schedule="auto"):
 def autotune(entries, frames, chunks=(16, 64, 256), streams=(2, 4, 8), reps=2, log=None, hs_persistent=True):
     """Times every (chunk, streams) candidate on the manifest (after its capture run) and
     returns (best runner, {candidate: ms}).  With hs_persistent, the Horn-Schunck pairs run
-    in one persistent launch whose tile shape is tuned first (tune_hs_shape)."""
+    in one persistent launch whose tile shape is tuned first (tune_hs_shape); the best
+    candidate is then timed once more with the Horn-Schunck pairs back in the chunks
+    (key ('hs_in_chunks', chunk, streams)), and the faster of the two is returned."""
     import gc
     best, table = None, {}
     hs_shape = None
@@ -493,6 +495,19 @@ def autotune(entries, frames, chunks=(16, 64, 256), streams=(2, 4, 8), reps=2, l
             else:
                 del r
                 gc.collect()
+    if hs_shape is not None:
+        c, s = best.key
+        r = BatchRunner(entries, chunk=min(c, len(entries)), streams=s, hs_shape=None)
+        r.key = ("hs_in_chunks", c, s)
+        ms = _time_runner(r, frames, reps)
+        table[r.key] = ms
+        if log:
+            log(f"chunk {c} streams {s}, Horn-Schunck in the chunks: {ms:.1f} ms")
+        if ms < table[best.key]:
+            best = r
+        else:
+            del r
+            gc.collect()
     return best, table
 
 

@@ -120,9 +120,11 @@ def test_config4_runner_matches_single_pairs(torch_cuda):
     rendered = [render_entry(e) for e in entries]
     frames = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b, _, _ in rendered]
     runner, table = autotune(entries, frames, chunks=(2, 6), streams=(1, 3), reps=1)
-    # chunk x streams candidates, plus the persistent Horn-Schunck kernel's tile shapes
-    assert len([k for k in table if k[0] != "hs_shape"]) == 4
+    # chunk x streams candidates, the persistent Horn-Schunck kernel's tile shapes, and the
+    # best candidate with the Horn-Schunck pairs back in the chunks
+    assert len([k for k in table if isinstance(k[0], int)]) == 4
     assert len([k for k in table if k[0] == "hs_shape"]) == len(ops_shapes())
+    assert len([k for k in table if k[0] == "hs_in_chunks"]) == 1
     outs = runner.run(frames)
     torch.cuda.synchronize()
     graph.ENABLED = False
