@@ -95,6 +95,12 @@ __device__ __forceinline__ bool hq_deriv_px(const HsqPair& P, int y, int x) {
 // word.  Every poll gives up after `wait_limit` rounds, which marks the pair
 // (OF_ST_WAIT_TIMEOUT) and the launch's error flag.  Returns 1 when the item may run: no
 // wait gave up and the pair had not failed before.  Lane 0 issues the acquire fence.
+__device__ __forceinline__ unsigned int hq_ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ int hq_wait(const unsigned int* done, unsigned int tile0, int tile, int ntx, int nty,
                                        unsigned int need, long long wait_limit, int* status_i, int* err_flag) {
   const int lane = threadIdx.x & 31;
@@ -103,14 +109,14 @@ __device__ __forceinline__ int hq_wait(const unsigned int* done, unsigned int ti
     const int ty = tile / ntx, tx = tile - ty * ntx;
     const int yy = ty + lane / 3 - 1, xx = tx + lane % 3 - 1;
     if (need > 0 && yy >= 0 && yy < nty && xx >= 0 && xx < ntx) {
-      const volatile unsigned int* c = done + tile0 + yy * ntx + xx;
+      const unsigned int* c = done + tile0 + yy * ntx + xx;
       long long k = 0;
-      while (*c < need) {
+      while (hq_ld_acquire(c) < need) {
         if (++k > wait_limit) {
           gave_up = true;
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
     }
   } else if (lane == 9) {
@@ -118,13 +124,12 @@ __device__ __forceinline__ int hq_wait(const unsigned int* done, unsigned int ti
   }
   const bool timeout = __any_sync(0xffffffffu, gave_up);
   const bool before = __any_sync(0xffffffffu, failed_before);
-  if (lane == 0) {
-    if (timeout && !before) {
-      atomicOr(status_i, OF_ST_WAIT_TIMEOUT);
-      atomicExch(err_flag, 1);
-    }
-    __threadfence();  // acquire: the neighbours' stores are visible from here on
+  if (lane == 0 && timeout && !before) {
+    atomicOr(status_i, OF_ST_WAIT_TIMEOUT);
+    atomicExch(err_flag, 1);
   }
+  // the polls are acquire loads: the neighbours' stores released before their counters are
+  // visible to this CTA after the barrier that follows
   return !(timeout || before);
 }
 
@@ -149,69 +154,109 @@ using HqVal = typename std::conditional<FAST, float, double>::type;
 
 constexpr int HQ_THREADS = 256;  // threads per CTA of the queue kernel
 
-// One cell of sweep s (region index k); the loop over a thread's cells is unrolled so the
-// cells' independent arithmetic chains interleave.
-template <int RW, int RH, int T, bool EDGE, bool FAST>
-__device__ __forceinline__ void hq_cell(int k, const float* __restrict__ sfx, const float* __restrict__ sfy,
-                                        const float* __restrict__ sft, const HqVal<FAST>* su, const HqVal<FAST>* sv,
-                                        HqVal<FAST>* du, HqVal<FAST>* dv, int s, int x0, int y0, int H, int W,
-                                        float a2) {
-  const double wc = (double)(1.0f / 12.0f), we = (double)(1.0f / 6.0f);
-  {
-    if (k >= RW * RH) return;
-    const int r = k / RW, c = k - r * RW;
-    if (c < 1 + s || c >= RW - 1 - s || r < 1 + s || r >= RH - 1 - s) return;
-    const int gx = x0 - T + c, gy = y0 - T + r;
-    if (EDGE && (gx < 0 || gx >= W || gy < 0 || gy >= H)) return;
-    int cm = c - 1, cp = c + 1, rm = r - 1, rp = r + 1;
-    if (EDGE) {
-      cm = mirror1(gx - 1, W) - (x0 - T);
-      cp = mirror1(gx + 1, W) - (x0 - T);
-      rm = mirror1(gy - 1, H) - (y0 - T);
-      rp = mirror1(gy + 1, H) - (y0 - T);
-    }
-    const int om = rm * RW, o0 = r * RW, op = rp * RW;
-    float ua, va;
-    if constexpr (FAST) {  // float32 averaging: corner and edge sums, one multiply-add each
-      const float wcf = 1.0f / 12.0f, wef = 1.0f / 6.0f;
-      const float cu = __fadd_rn(__fadd_rn(su[om + cm], su[om + cp]), __fadd_rn(su[op + cm], su[op + cp]));
-      const float eu = __fadd_rn(__fadd_rn(su[om + c], su[op + c]), __fadd_rn(su[o0 + cm], su[o0 + cp]));
-      const float cv = __fadd_rn(__fadd_rn(sv[om + cm], sv[om + cp]), __fadd_rn(sv[op + cm], sv[op + cp]));
-      const float ev = __fadd_rn(__fadd_rn(sv[om + c], sv[op + c]), __fadd_rn(sv[o0 + cm], sv[o0 + cp]));
-      ua = __fmaf_rn(cu, wcf, __fmul_rn(eu, wef));
-      va = __fmaf_rn(cv, wcf, __fmul_rn(ev, wef));
-    } else {
-      double a = 0.0, b = 0.0;  // su, sv hold float32 values as float64: no conversions here
-      a = __fma_rn(su[om + cm], wc, a); b = __fma_rn(sv[om + cm], wc, b);
-      a = __fma_rn(su[om + c], we, a);  b = __fma_rn(sv[om + c], we, b);
-      a = __fma_rn(su[om + cp], wc, a); b = __fma_rn(sv[om + cp], wc, b);
-      a = __fma_rn(su[o0 + cm], we, a); b = __fma_rn(sv[o0 + cm], we, b);
-      a = __fma_rn(su[o0 + cp], we, a); b = __fma_rn(sv[o0 + cp], we, b);
-      a = __fma_rn(su[op + cm], wc, a); b = __fma_rn(sv[op + cm], wc, b);
-      a = __fma_rn(su[op + c], we, a);  b = __fma_rn(sv[op + c], we, b);
-      a = __fma_rn(su[op + cp], wc, a); b = __fma_rn(sv[op + cp], wc, b);
-      ua = (float)a;
-      va = (float)b;
-    }
-    const int i = o0 + c;
-    const float gxv = sfx[i], gyv = sfy[i];
-    const float num = __fadd_rn(__fadd_rn(__fmul_rn(gxv, ua), __fmul_rn(gyv, va)), sft[i]);
-    const float den = __fadd_rn(__fadd_rn(a2, __fmul_rn(gxv, gxv)), __fmul_rn(gyv, gyv));
-    const float der = __fdiv_rn(num, den);
-    du[i] = (HqVal<FAST>)__fsub_rn(ua, __fmul_rn(gxv, der));
-    dv[i] = (HqVal<FAST>)__fsub_rn(va, __fmul_rn(gyv, der));
-  }
+// A thread's window row: the values of columns c - 1, c, c + 1 (mirrored on image borders)
+// of one region row, for u and v.
+template <bool FAST>
+struct HqRow {
+  HqVal<FAST> ul, um, ur, vl, vm, vr;
+};
+
+template <int RW, bool FAST>
+__device__ __forceinline__ void hq_load(HqRow<FAST>& R, const HqVal<FAST>* su, const HqVal<FAST>* sv, int row, int cm,
+                                        int c, int cp) {
+  const int o = row * RW;
+  R.ul = su[o + cm];
+  R.um = su[o + c];
+  R.ur = su[o + cp];
+  R.vl = sv[o + cm];
+  R.vm = sv[o + c];
+  R.vr = sv[o + cp];
 }
 
+// The update of region cell i from its window rows U (above), C and D (below):
+// hs_sweep_kernel's arithmetic, the 8 neighbours summed in its order.
+template <bool FAST>
+__device__ __forceinline__ void hq_update(const HqRow<FAST>& U, const HqRow<FAST>& C, const HqRow<FAST>& D, int i,
+                                          const float* __restrict__ sfx, const float* __restrict__ sfy,
+                                          const float* __restrict__ sft, HqVal<FAST>* du, HqVal<FAST>* dv,
+                                          float a2) {
+  float ua, va;
+  if constexpr (FAST) {  // float32 averaging: corner and edge sums, one multiply-add each
+    const float wcf = 1.0f / 12.0f, wef = 1.0f / 6.0f;
+    const float cu = __fadd_rn(__fadd_rn(U.ul, U.ur), __fadd_rn(D.ul, D.ur));
+    const float eu = __fadd_rn(__fadd_rn(U.um, D.um), __fadd_rn(C.ul, C.ur));
+    const float cv = __fadd_rn(__fadd_rn(U.vl, U.vr), __fadd_rn(D.vl, D.vr));
+    const float ev = __fadd_rn(__fadd_rn(U.vm, D.vm), __fadd_rn(C.vl, C.vr));
+    ua = __fmaf_rn(cu, wcf, __fmul_rn(eu, wef));
+    va = __fmaf_rn(cv, wcf, __fmul_rn(ev, wef));
+  } else {
+    const double wc = (double)(1.0f / 12.0f), we = (double)(1.0f / 6.0f);
+    double a = 0.0, b = 0.0;  // float32 values held as float64: no conversions here
+    a = __fma_rn(U.ul, wc, a); b = __fma_rn(U.vl, wc, b);
+    a = __fma_rn(U.um, we, a); b = __fma_rn(U.vm, we, b);
+    a = __fma_rn(U.ur, wc, a); b = __fma_rn(U.vr, wc, b);
+    a = __fma_rn(C.ul, we, a); b = __fma_rn(C.vl, we, b);
+    a = __fma_rn(C.ur, we, a); b = __fma_rn(C.vr, we, b);
+    a = __fma_rn(D.ul, wc, a); b = __fma_rn(D.vl, wc, b);
+    a = __fma_rn(D.um, we, a); b = __fma_rn(D.vm, we, b);
+    a = __fma_rn(D.ur, wc, a); b = __fma_rn(D.vr, wc, b);
+    ua = (float)a;
+    va = (float)b;
+  }
+  const float gxv = sfx[i], gyv = sfy[i];
+  const float num = __fadd_rn(__fadd_rn(__fmul_rn(gxv, ua), __fmul_rn(gyv, va)), sft[i]);
+  const float den = __fadd_rn(__fadd_rn(a2, __fmul_rn(gxv, gxv)), __fmul_rn(gyv, gyv));
+  const float der = __fdiv_rn(num, den);
+  du[i] = (HqVal<FAST>)__fsub_rn(ua, __fmul_rn(gxv, der));
+  dv[i] = (HqVal<FAST>)__fsub_rn(va, __fmul_rn(gyv, der));
+}
+
+// Sweep s of the region: thread t owns column t % RW and walks a band of the rows the sweep
+// computes (band t / RW of HQ_THREADS / RW) with a 3-row register window, so each row it
+// visits costs one row of loads.  On image borders the neighbour columns and the window's
+// outer rows go through the 'mirror' map; inside the image the mapped row is the row.
 template <int RW, int RH, int T, bool EDGE, bool FAST>
 __device__ __forceinline__ void hq_sweep(const float* __restrict__ sfx, const float* __restrict__ sfy,
                                          const float* __restrict__ sft, const HqVal<FAST>* su, const HqVal<FAST>* sv,
                                          HqVal<FAST>* du, HqVal<FAST>* dv, int s, int x0, int y0, int H, int W,
                                          float a2) {
-#pragma unroll 4
-  for (int it = 0; it < (RW * RH + HQ_THREADS - 1) / HQ_THREADS; it++)
-    hq_cell<RW, RH, T, EDGE, FAST>(it * HQ_THREADS + (int)threadIdx.x, sfx, sfy, sft, su, sv, du, dv, s, x0, y0, H,
-                                   W, a2);
+  static_assert(HQ_THREADS % RW == 0, "a whole number of bands");
+  constexpr int NB = HQ_THREADS / RW;
+  const int c = (int)threadIdx.x % RW, band = (int)threadIdx.x / RW;
+  if (c < 1 + s || c >= RW - 1 - s) return;
+  const int gx = x0 - T + c;
+  if (EDGE && (gx < 0 || gx >= W)) return;
+  int cm = c - 1, cp = c + 1;
+  if (EDGE) {
+    cm = mirror1(gx - 1, W) - (x0 - T);
+    cp = mirror1(gx + 1, W) - (x0 - T);
+  }
+  int lo = 1 + s, hi = RH - 1 - s;
+  if (EDGE) {  // rows in the image only
+    lo = max(lo, T - y0);
+    hi = min(hi, H + T - y0);
+  }
+  const int n = hi - lo;
+  if (n <= 0) return;
+  const int ra = lo + (n * band) / NB, rb = lo + (n * (band + 1)) / NB;
+  if (rb <= ra) return;
+  auto row_of = [&](int r) { return EDGE ? mirror1(y0 - T + r, H) - (y0 - T) : r; };
+  HqRow<FAST> A, B, C;
+  hq_load<RW, FAST>(A, su, sv, row_of(ra - 1), cm, c, cp);
+  hq_load<RW, FAST>(B, su, sv, ra, cm, c, cp);
+#pragma unroll 1
+  for (int r = ra; r < rb; r += 3) {
+    hq_load<RW, FAST>(C, su, sv, row_of(r + 1), cm, c, cp);
+    hq_update<FAST>(A, B, C, r * RW + c, sfx, sfy, sft, du, dv, a2);
+    if (r + 1 < rb) {
+      hq_load<RW, FAST>(A, su, sv, row_of(r + 2), cm, c, cp);
+      hq_update<FAST>(B, C, A, (r + 1) * RW + c, sfx, sfy, sft, du, dv, a2);
+    }
+    if (r + 2 < rb) {
+      hq_load<RW, FAST>(B, su, sv, row_of(r + 3), cm, c, cp);
+      hq_update<FAST>(C, A, B, (r + 2) * RW + c, sfx, sfy, sft, du, dv, a2);
+    }
+  }
 }
 
 // Returns false when a result of the last pass is not finite.
@@ -348,6 +393,17 @@ __global__ void __launch_bounds__(HQ_THREADS) hsq_kernel(const HsqPair* __restri
   }
 }
 
+constexpr unsigned int HQ_WARPS = HQ_THREADS / 32;
+
+// Each warp publishes its own part of a stage: its stores (or reads) are ordered before its
+// increment of the tile's counter, so a stage of a tile is complete when the counter has
+// grown by HQ_WARPS; no CTA barrier sits between the last store and the release.
+__device__ __forceinline__ void hq_release_warp(unsigned int* counter) {
+  __syncwarp();
+  __threadfence();
+  if ((threadIdx.x & 31) == 0) atomicAdd(counter, 1u);
+}
+
 // The resident schedule, for launches where every tile gets a CTA of its own (all CTAs
 // resident): CTA b owns global tile b for the whole solve and keeps its region on chip.
 // Stage 0 computes the derivative planes of the WHOLE region (owned tile and halo: they
@@ -355,10 +411,10 @@ __global__ void __launch_bounds__(HQ_THREADS) hsq_kernel(const HsqPair* __restri
 // memory.  Stage s >= 1 runs up to T sweeps as a queue item of pass s does, but only the
 // halo ring comes from global memory (the neighbours' results of stage s - 1); the owned
 // part is already in shared memory, where the previous stage's T (even) sweeps left it.
-// The owned tile is published every stage.  Waits and counters are the queue kernel's: a
-// stage waits for its own and its neighbours' counters to reach s, which also orders every
-// overwrite of a ping-pong buffer (or of the initial U, V at stage 1) after the neighbours'
-// reads of it.
+// The owned tile is published every stage.  Waits are the queue kernel's, the counters
+// count warps: a stage waits for its own and its neighbours' counters to reach s x
+// HQ_WARPS, which also orders every overwrite of a ping-pong buffer (or of the initial U, V
+// at stage 1) after the neighbours' reads of it.
 template <int RW, int RH, int T, bool FAST>
 __global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restrict__ pairs, int npairs,
                                                   unsigned int* done, int* status, long long wait_limit,
@@ -401,16 +457,14 @@ __global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restri
     bv0[k] = __ldcg(P.V + gi);
     if (r >= T && r < T + G::TH && c >= T && c < T + G::TW) ok = ok && f;  // each pixel checked once
   }
-  int bad = __syncthreads_or(!ok);
-  if (threadIdx.x == 0) {
-    if (bad) atomicOr(status + i, OF_ST_NONFINITE_INPUT);
-    __threadfence();  // release: this tile's reads of the initial U, V are done
-    atomicAdd(done + gtile, 1u);
-  }
+  const int bad0 = __syncthreads_or(!ok);
+  if (threadIdx.x == 0 && bad0) atomicOr(status + i, OF_ST_NONFINITE_INPUT);
+  hq_release_warp(done + gtile);  // this warp's reads of the initial U, V are done
   for (int p = 0; p < np; p++) {
     const int stage = p + 1;
     if (threadIdx.x < 32) {
-      const int run = hq_wait(done, P.tile0, tile, P.tx, nty, (unsigned int)stage, wait_limit, status + i, err_flag);
+      const int run = hq_wait(done, P.tile0, tile, P.tx, nty, (unsigned int)(stage * HQ_WARPS), wait_limit,
+                              status + i, err_flag);
       if (threadIdx.x == 0) s_run = run;
     }
     __syncthreads();
@@ -458,12 +512,11 @@ __global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restri
         if (p == np - 1) ok = ok && isfinite(fu[o]) && isfinite(fv[o]);
       }
     }
-    bad = __syncthreads_or(!ok);  // also: every store of the stage is issued
-    if (threadIdx.x == 0) {
-      if (bad) atomicOr(status + i, OF_ST_NONFINITE_OUTPUT);
-      __threadfence();  // release
-      atomicAdd(done + gtile, 1u);
+    if (p == np - 1) {
+      const int bad = __syncthreads_or(!ok);
+      if (threadIdx.x == 0 && bad) atomicOr(status + i, OF_ST_NONFINITE_OUTPUT);
     }
+    hq_release_warp(done + gtile);  // this warp's stores of the stage
   }
 }
 
@@ -487,7 +540,7 @@ namespace {
 struct HsqShape {
   int rw, rh, t;
 };
-constexpr HsqShape kHsqShapes[] = {{64, 40, 4}, {32, 24, 4}, {64, 24, 4}, {32, 32, 8}, {40, 40, 8}};
+constexpr HsqShape kHsqShapes[] = {{64, 40, 4}, {32, 24, 4}, {64, 24, 4}, {32, 32, 8}};
 constexpr int kHsqNumShapes = sizeof(kHsqShapes) / sizeof(kHsqShapes[0]);
 
 template <int RW, int RH, int T, bool FAST>
@@ -646,8 +699,7 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
       case 0: rc = hsq_resident<64, 40, 4>(fast, resident, &per_sm); break;
       case 1: rc = hsq_resident<32, 24, 4>(fast, resident, &per_sm); break;
       case 2: rc = hsq_resident<64, 24, 4>(fast, resident, &per_sm); break;
-      case 3: rc = hsq_resident<32, 32, 8>(fast, resident, &per_sm); break;
-      default: rc = hsq_resident<40, 40, 8>(fast, resident, &per_sm); break;
+      default: rc = hsq_resident<32, 32, 8>(fast, resident, &per_sm); break;
     }
     *cap = (long long)sms * per_sm;
     return rc == 0 && per_sm >= 1;
@@ -671,8 +723,7 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
     case 0: e = hsq_launch<64, 40, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
     case 1: e = hsq_launch<32, 24, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
     case 2: e = hsq_launch<64, 24, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    case 3: e = hsq_launch<32, 32, 8>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    default: e = hsq_launch<40, 40, 8>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
+    default: e = hsq_launch<32, 32, 8>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
   }
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: launch: %s", cudaGetErrorString(e));
   return check_launch("of_hs_batch", nl + 1);

@@ -48,7 +48,7 @@ SCHEDULES = ["queue", "resident"]
 
 
 @pytest.mark.parametrize("schedule", SCHEDULES)
-@pytest.mark.parametrize("shape_index", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("shape_index", [0, 1, 2, 3])
 def test_single_pair_config1_bit_exact(cuda_ok, shape_index, schedule):
     """256 x 256, alpha 21, 600 sweeps (the PyHSchunck_Fs3_4 calibration) in one launch."""
     import torch
