@@ -776,6 +776,48 @@ def _render_eval(seed):
     return S.config_pair("fbls1024", seed=seed)
 
 
+LARGE_DISP_PX = 12.0
+
+
+def _render_eval_large(seed):
+    """The workload's pairs with displacements up to LARGE_DISP_PX, where a zero start at
+    full size needs the pyramid's coarse level."""
+    from ofb200 import synthetic as S
+    return S.piv_pair(1024, 1024, "fourier", seed, density=0.05, diameter=(2.0, 3.0), noise=2.0,
+                      max_disp=LARGE_DISP_PX)
+
+
+def learned_large_disp(args, net, meta, dev, npairs=8):
+    """Interior EPE of the plain pyramid, the learned start and the no-network ablation on
+    held-out pairs with displacements up to LARGE_DISP_PX (accuracy only, not timed)."""
+    import multiprocessing as mp
+    import torch
+    from ofb200 import ops, synthetic as S
+    from ofb200.warmstart import LearnedBatch
+    seeds = [970_000 + i for i in range(npairs)]
+    with mp.get_context("spawn").Pool(min(8, max(1, (os.cpu_count() or 2) // 2))) as pool:
+        evals = pool.map(_render_eval_large, seeds)
+    frames = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _, _ in evals]
+    out = {"max_disp_px": LARGE_DISP_PX, "pairs": npairs, "crop_px": 16}
+    epe = []
+    for (a8, b8), (_, _, Ug, Vg) in zip(frames, evals):
+        Up, Vp = pipeline_dev(ops.u8_to_f32(a8), ops.u8_to_f32(b8))
+        epe.append(S.epe(Up.cpu().numpy(), Vp.cpu().numpy(), Ug, Vg, crop=16))
+    out["epe_plain"] = float(np.mean(epe))
+    for start, key in (("cnn", "learned"), ("zero", "no_network_ablation")):
+        lb = LearnedBatch(net, meta, npairs, args.size, streams=args.streams, start=start)
+        res, errs = lb.run(frames)
+        nfb = 0
+        if start == "cnn":
+            res, nfb = lb.fallback(frames, res, errs.cpu())
+        epe = [S.epe(U.cpu().numpy(), V.cpu().numpy(), e[2], e[3], crop=16) for (U, V), e in zip(res, evals)]
+        out[f"epe_{key}"] = float(np.mean(epe))
+        if start == "cnn":
+            out["learned_fallback_pairs"] = int(nfb)
+        del lb
+    return out
+
+
 def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
     """The learned warm start (config 5: batch --learned-pairs at 1024^2): one network
     forward over the step's pairs (at the network's level), Farneback at full size from that
@@ -846,13 +888,14 @@ def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
 
     learned = arm("cnn")
     ablation = arm("zero")
+    large = learned_large_disp(args, net, meta, dev)
     net.check()
     learned.update({"mode": meta["mode"], "threshold": meta["threshold"], "epe_plain": float(np.mean(epe_p)),
                     "epe_pairs": nu, "epe_crop_px": 16, "pairs_per_step": nb,
                     "network": f"encoder-decoder CNN at the {meta.get('level', 512)}^2 level, 1.75M params, bf16 tcgen05 convs, "
                                "f32 accumulate",
                     "trained": {k: meta[k] for k in ("train_pairs", "steps", "batch", "crop", "level", "eval_pairs")},
-                    "no_network_ablation": ablation})
+                    "no_network_ablation": ablation, "large_displacement": large})
     return learned
 
 

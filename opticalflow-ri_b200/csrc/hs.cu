@@ -8,6 +8,7 @@
 // 3 coefficient planes and the two 3x3 neighbourhoods (served by L1) and writes U, V:
 // 28 B per pixel of HBM/L2 traffic.
 #include "common.cuh"
+#include "hsweep.cuh"
 
 namespace ofb {
 
@@ -83,51 +84,7 @@ constexpr int HB_T = 4, HB_TW = 56, HB_TH = 32, HB_RW = HB_TW + 2 * HB_T, HB_RH 
 constexpr int HB_PL = HB_RW * HB_RH;
 constexpr size_t HB_SMEM = 3 * (size_t)HB_PL * sizeof(float) + 4 * (size_t)HB_PL * sizeof(double);  // 110 KB
 
-template <bool EDGE>
-__device__ __forceinline__ void hb_sweep(const float* __restrict__ sfx, const float* __restrict__ sfy,
-                                         const float* __restrict__ sft, const double* __restrict__ su,
-                                         const double* __restrict__ sv, double* __restrict__ du,
-                                         double* __restrict__ dv, int s, int x0, int y0, int H, int W, float a2) {
-  const double wc = (double)(1.0f / 12.0f), we = (double)(1.0f / 6.0f);
-  const int c = threadIdx.x & (HB_RW - 1), g = threadIdx.x >> 6;
-  if (c < 1 + s || c >= HB_RW - 1 - s) return;
-  const int gx = x0 - HB_T + c;
-  if (EDGE && (gx < 0 || gx >= W)) return;
-  int cm = c - 1, cp = c + 1;
-  if (EDGE) {
-    cm = mirror1(gx - 1, W) - (x0 - HB_T);
-    cp = mirror1(gx + 1, W) - (x0 - HB_T);
-  }
-  for (int r = 1 + s + g; r < HB_RH - 1 - s; r += 4) {
-    const int gy = y0 - HB_T + r;
-    if (EDGE && (gy < 0 || gy >= H)) continue;
-    int rm = r - 1, rp = r + 1;
-    if (EDGE) {
-      rm = mirror1(gy - 1, H) - (y0 - HB_T);
-      rp = mirror1(gy + 1, H) - (y0 - HB_T);
-    }
-    const int om = rm * HB_RW, o0 = r * HB_RW, op = rp * HB_RW;
-    double a = 0.0, b = 0.0;
-    a = __fma_rn(su[om + cm], wc, a); b = __fma_rn(sv[om + cm], wc, b);
-    a = __fma_rn(su[om + c], we, a);  b = __fma_rn(sv[om + c], we, b);
-    a = __fma_rn(su[om + cp], wc, a); b = __fma_rn(sv[om + cp], wc, b);
-    a = __fma_rn(su[o0 + cm], we, a); b = __fma_rn(sv[o0 + cm], we, b);
-    a = __fma_rn(su[o0 + cp], we, a); b = __fma_rn(sv[o0 + cp], we, b);
-    a = __fma_rn(su[op + cm], wc, a); b = __fma_rn(sv[op + cm], wc, b);
-    a = __fma_rn(su[op + c], we, a);  b = __fma_rn(sv[op + c], we, b);
-    a = __fma_rn(su[op + cp], wc, a); b = __fma_rn(sv[op + cp], wc, b);
-    const float ua = (float)a, va = (float)b;
-    const int i = o0 + c;
-    const float gxv = sfx[i], gyv = sfy[i];
-    const float num = __fadd_rn(__fadd_rn(__fmul_rn(gxv, ua), __fmul_rn(gyv, va)), sft[i]);
-    const float den = __fadd_rn(__fadd_rn(a2, __fmul_rn(gxv, gxv)), __fmul_rn(gyv, gyv));
-    const float der = __fdiv_rn(num, den);
-    du[i] = (double)__fsub_rn(ua, __fmul_rn(gxv, der));
-    dv[i] = (double)__fsub_rn(va, __fmul_rn(gyv, der));
-  }
-}
-
-__global__ void __launch_bounds__(256) hs_pass_kernel(const float* __restrict__ fx, const float* __restrict__ fy,
+__global__ void __launch_bounds__(HQ_THREADS) hs_pass_kernel(const float* __restrict__ fx, const float* __restrict__ fy,
                                                       const float* __restrict__ ft, const float* __restrict__ U,
                                                       const float* __restrict__ V, float* __restrict__ Un,
                                                       float* __restrict__ Vn, int H, int W, int pitch, float a2,
@@ -141,7 +98,7 @@ __global__ void __launch_bounds__(256) hs_pass_kernel(const float* __restrict__ 
 #define HB_U(q) (hb_uv + (2 * (q)) * HB_PL)
 #define HB_V(q) (hb_uv + (1 + 2 * (q)) * HB_PL)
   const int x0 = blockIdx.x * HB_TW, y0 = blockIdx.y * HB_TH;
-  for (int k = threadIdx.x; k < HB_PL; k += 256) {
+  for (int k = threadIdx.x; k < HB_PL; k += HQ_THREADS) {
     const int r = k / HB_RW, c = k - r * HB_RW;
     const int gy = y0 - HB_T + r, gx = x0 - HB_T + c;
     if (gy < 0 || gy >= H || gx < 0 || gx >= W) continue;  // never read
@@ -158,14 +115,16 @@ __global__ void __launch_bounds__(256) hs_pass_kernel(const float* __restrict__ 
   for (int s = 0; s < nsw; s++) {
     const int q = s & 1;
     if (edge)
-      hb_sweep<true>(sfx, sfy, sft, HB_U(q), HB_V(q), HB_U(q ^ 1), HB_V(q ^ 1), s, x0, y0, H, W, a2);
+      hq_sweep<HB_RW, HB_RH, HB_T, true, false>(sfx, sfy, sft, HB_U(q), HB_V(q), HB_U(q ^ 1), HB_V(q ^ 1), s, x0, y0,
+                                                H, W, a2);
     else
-      hb_sweep<false>(sfx, sfy, sft, HB_U(q), HB_V(q), HB_U(q ^ 1), HB_V(q ^ 1), s, x0, y0, H, W, a2);
+      hq_sweep<HB_RW, HB_RH, HB_T, false, false>(sfx, sfy, sft, HB_U(q), HB_V(q), HB_U(q ^ 1), HB_V(q ^ 1), s, x0,
+                                                 y0, H, W, a2);
     __syncthreads();
   }
   const double* fu = HB_U(nsw & 1);
   const double* fv = HB_V(nsw & 1);
-  for (int k = threadIdx.x; k < HB_TW * HB_TH; k += 256) {
+  for (int k = threadIdx.x; k < HB_TW * HB_TH; k += HQ_THREADS) {
     const int r = k / HB_TW, c = k - r * HB_TW;
     const int y = y0 + r, x = x0 + c;
     if (y >= H || x >= W) continue;
@@ -285,7 +244,7 @@ extern "C" int of_hs_solve(const float* I0, const float* I1, float* U, float* V,
       const float* su = p == 0 ? U0 : (to_uv ? Ub : U);
       const float* sv = p == 0 ? V0 : (to_uv ? Vb : V);
       const int nsw = niter - p * HB_T < HB_T ? niter - p * HB_T : HB_T;
-      hs_pass_kernel<<<pg, 256, HB_SMEM, st>>>(fx, fy, ft, su, sv, to_uv ? U : Ub, to_uv ? V : Vb, H, W, pitch, a2,
+      hs_pass_kernel<<<pg, HQ_THREADS, HB_SMEM, st>>>(fx, fy, ft, su, sv, to_uv ? U : Ub, to_uv ? V : Vb, H, W, pitch, a2,
                                               nsw);
     }
     long long n = 2 + np;
