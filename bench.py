@@ -787,34 +787,76 @@ def _render_eval_large(seed):
                       max_disp=LARGE_DISP_PX)
 
 
-def learned_large_disp(args, net, meta, dev, npairs=8):
-    """Interior EPE of the plain pyramid, the learned start and the no-network ablation on
-    held-out pairs with displacements up to LARGE_DISP_PX (accuracy only, not timed)."""
+def _events_ms(fn, flush, steps, warmup):
+    """Mean device time of fn() (CUDA events, L2 flushed before each timed call)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return float(np.mean(ms))
+
+
+def learned_large_disp(args, net, meta, dev, flush, npairs=8):
+    """Held-out pairs with displacements up to LARGE_DISP_PX: interior EPE of the plain
+    pyramid, of the packaged network's start (trained on max 4 px) and of the no-network
+    ablation; and, when the package holds a network trained on larger displacements
+    (warmstart_weights_12px.npz, calibrated on this kind of pair), that network's arm and
+    its ablation with pairs/s for each arm (CUDA events over --steps batches of the pairs)."""
     import multiprocessing as mp
     import torch
+    import Farneback_PyCL as F
+    import PhysicsBasedOpticalFlowLiuShen as LS
     from ofb200 import ops, synthetic as S
-    from ofb200.warmstart import LearnedBatch
+    from ofb200.batch import PairBatch, PairSpec
+    from ofb200.warmstart import WEIGHTS, LearnedBatch, load_trained
     seeds = [970_000 + i for i in range(npairs)]
     with mp.get_context("spawn").Pool(min(8, max(1, (os.cpu_count() or 2) // 2))) as pool:
         evals = pool.map(_render_eval_large, seeds)
     frames = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _, _ in evals]
-    out = {"max_disp_px": LARGE_DISP_PX, "pairs": npairs, "crop_px": 16}
-    epe = []
-    for (a8, b8), (_, _, Ug, Vg) in zip(frames, evals):
-        Up, Vp = pipeline_dev(ops.u8_to_f32(a8), ops.u8_to_f32(b8))
-        epe.append(S.epe(Up.cpu().numpy(), Vp.cpu().numpy(), Ug, Vg, crop=16))
-    out["epe_plain"] = float(np.mean(epe))
-    for start, key in (("cnn", "learned"), ("zero", "no_network_ablation")):
-        lb = LearnedBatch(net, meta, npairs, args.size, streams=args.streams, start=start)
-        res, errs = lb.run(frames)
-        nfb = 0
-        if start == "cnn":
-            res, nfb = lb.fallback(frames, res, errs.cpu())
-        epe = [S.epe(U.cpu().numpy(), V.cpu().numpy(), e[2], e[3], crop=16) for (U, V), e in zip(res, evals)]
-        out[f"epe_{key}"] = float(np.mean(epe))
-        if start == "cnn":
-            out["learned_fallback_pairs"] = int(nfb)
-        del lb
+    epe_of = lambda res: float(np.mean([S.epe(U.cpu().numpy(), V.cpu().numpy(), e[2], e[3], crop=16)  # noqa: E731
+                                        for (U, V), e in zip(res, evals)]))
+    spec = PairSpec(0, lambda: F.Farneback_PyCL(), 2, 1, 0.48, lambda: LS.LiuShenOpticalFlowAlgoAdapter(10),
+                    key=("fbls",))
+    pb = PairBatch([spec] * npairs, streams=max(1, args.streams))
+    out = {"max_disp_px": LARGE_DISP_PX, "pairs": npairs, "crop_px": 16,
+           "epe_plain": epe_of(pb.run(frames)),
+           "plain_pairs_per_s": npairs / (_events_ms(lambda: pb.run(frames), flush, args.steps, 2) * 1e-3)}
+    del pb
+
+    def arms(net_, meta_, tag, timed):
+        for start, key in (("cnn", "learned"), ("zero", "no_network_ablation")):
+            lb = LearnedBatch(net_, meta_, npairs, args.size, streams=args.streams, start=start)
+            res, errs = lb.run(frames)
+            if start == "cnn":
+                out[f"{tag}epe_learned_before_fallback"] = epe_of(res)
+                res, nfb = lb.fallback(frames, res, errs.cpu())
+                out[f"{tag}learned_fallback_pairs"] = int(nfb)
+            out[f"{tag}epe_{key}"] = epe_of(res)
+            if timed:
+                def step():
+                    r, e = lb.run(frames)
+                    if start == "cnn":
+                        lb.fallback(frames, r, e.cpu())
+                out[f"{tag}{key}_pairs_per_s"] = npairs / (_events_ms(step, flush, args.steps, 2) * 1e-3)
+            del lb
+
+    arms(net, meta, "", False)
+    large = os.path.join(os.path.dirname(WEIGHTS), "warmstart_weights_12px.npz")
+    if os.path.exists(large):
+        net2, meta2 = load_trained(path=large, device=dev)
+        out["large_network"] = {k: meta2.get(k) for k in ("train_max_disp", "eval_max_disp", "mode", "fb_iters",
+                                                           "sweeps", "zero_fb_iters", "zero_sweeps", "train_pairs")}
+        arms(net2, meta2, "large_network_", True)
+        net2.check()
     return out
 
 
@@ -888,7 +930,7 @@ def run_learned(args, step_frames, pairs, dev, flush, world, pairs_total_ms):
 
     learned = arm("cnn")
     ablation = arm("zero")
-    large = learned_large_disp(args, net, meta, dev)
+    large = learned_large_disp(args, net, meta, dev, flush)
     net.check()
     learned.update({"mode": meta["mode"], "threshold": meta["threshold"], "epe_plain": float(np.mean(epe_p)),
                     "epe_pairs": nu, "epe_crop_px": 16, "pairs_per_step": nb,

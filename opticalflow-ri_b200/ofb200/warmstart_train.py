@@ -3,15 +3,16 @@
     python -m ofb200.warmstart_train --pairs 2000 --steps 3000 --out warmstart.npz
 
 1. Training pairs (1024^2, seeded; random-Fourier or Lamb-Oseen flow with a random core
-   radius, 0.02-0.1 particles/px, noise sigma 0-5 DN, diameter 2-3 px, max 4 px) are
-   rendered on the host cores by a spawn process pool.
+   radius, 0.02-0.1 particles/px, noise sigma 0-5 DN, diameter 2-3 px, max displacement
+   4 px or drawn from --max-disp) are rendered on the host cores by a spawn process pool.
 2. Each pair is labelled by the plain pipeline on the GPU (Farneback pyr2 + Liu-Shen h = 10,
    the package's converged output); frames and label are taken to the --level size (the
    pyramid's bicubic downsample; the label scaled by level / 1024 in magnitude).  The
    packaged weights: --level 128 --crop 128.
 3. The network is trained on random --crop crops (Adam, mean squared flow error) with the
    package's own forward / backward kernels.
-4. On held-out pairs of the 1024^2 benchmark workload (disjoint seeds) the plain pipeline,
+4. On held-out pairs of the 1024^2 benchmark workload (disjoint seeds; with
+   --eval-max-disp, the same flows scaled to that maximum displacement) the plain pipeline,
    the network's start followed by each full-size stage (Liu-Shen alone with K sweeps, or
    Farneback with 1-5 iterations then K sweeps), and the same stages from a zero field
    (the no-network ablation) are compared by interior endpoint error against the analytic
@@ -24,6 +25,7 @@ Weights, the configuration, the threshold and the evaluation table go to one .np
 from __future__ import annotations
 
 import argparse
+import functools
 import json
 import multiprocessing as mp
 import os
@@ -43,19 +45,24 @@ LEVEL = 512
 CROP = 256
 
 
-def _train_pair(seed):
+def _train_pair(seed, disp=(4.0, 4.0)):
+    """disp: the range the pair's maximum displacement is drawn from (px)."""
     from ofb200 import synthetic as S
     rng = np.random.default_rng(seed)
     kind = "fourier" if rng.uniform() < 0.5 else "lamb_oseen"
     kw = {"core_radius": float(rng.uniform(40, 160))} if kind == "lamb_oseen" else {}
+    md = float(rng.uniform(disp[0], disp[1])) if disp[1] > disp[0] else float(disp[0])
     a, b, U, V = S.piv_pair(1024, 1024, kind, seed=seed, density=float(rng.uniform(0.02, 0.1)), diameter=(2.0, 3.0),
-                            noise=float(rng.uniform(0.0, 5.0)), **kw)
+                            noise=float(rng.uniform(0.0, 5.0)), max_disp=md, **kw)
     return a, b
 
 
-def _eval_pair(seed):
+def _eval_pair(seed, max_disp=4.0):
+    """The benchmark workload's pairs (max 4 px), or the same flows scaled to max_disp."""
     from ofb200 import synthetic as S
-    return S.config_pair("fbls1024", seed=seed)
+    if max_disp == 4.0:
+        return S.config_pair("fbls1024", seed=seed)
+    return S.piv_pair(1024, 1024, "fourier", seed, density=0.05, diameter=(2.0, 3.0), noise=2.0, max_disp=max_disp)
 
 
 def generate(fn, seeds, workers):
@@ -202,7 +209,8 @@ def evaluate(net, pairs, sweeps_list, dev, log=print, level=LEVEL):
 def calibrate_only(args):
     """New calibration (configuration, threshold, table) for existing weights."""
     workers = args.workers or max(1, min(64, len(os.sched_getaffinity(0))))
-    eval_pairs = generate(_eval_pair, [EVAL_SEED0 + i for i in range(args.eval)], workers)
+    eval_pairs = generate(functools.partial(_eval_pair, max_disp=args.eval_max_disp),
+                          [EVAL_SEED0 + i for i in range(args.eval)], workers)
     import torch
     from ofb200.warmstart import WarmStartNet
     d = np.load(args.calibrate)
@@ -229,6 +237,9 @@ def main():
     ap.add_argument("--calibrate", default=None, help="recalibrate the weights in this .npz (no training)")
     ap.add_argument("--level", type=int, default=LEVEL, help="size the network runs at (1024 / 2^k)")
     ap.add_argument("--crop", type=int, default=CROP, help="training crop (<= level)")
+    ap.add_argument("--max-disp", default="4,4", help="range of the training pairs' maximum displacement (px)")
+    ap.add_argument("--eval-max-disp", type=float, default=4.0,
+                    help="maximum displacement of the calibration pairs (4: the benchmark workload)")
     args = ap.parse_args()
     if args.calibrate:
         return calibrate_only(args)
@@ -241,8 +252,10 @@ def main():
     t0 = time.time()
     # host rendering first, in spawned workers, before this process touches CUDA
     mine = [TRAIN_SEED0 + i for i in shard_range(args.pairs, rank, world)]
-    train_pairs = generate(_train_pair, mine, workers)
-    eval_pairs = generate(_eval_pair, [EVAL_SEED0 + i for i in range(args.eval)], workers) if rank == 0 else []
+    disp = tuple(float(x) for x in args.max_disp.split(","))
+    train_pairs = generate(functools.partial(_train_pair, disp=disp), mine, workers)
+    eval_pairs = (generate(functools.partial(_eval_pair, max_disp=args.eval_max_disp),
+                           [EVAL_SEED0 + i for i in range(args.eval)], workers) if rank == 0 else [])
     print(f"rank {rank}: generated {len(train_pairs)} + {len(eval_pairs)} pairs on {workers} workers in "
           f"{time.time() - t0:.0f}s", flush=True)
     import torch
@@ -273,6 +286,7 @@ def main():
     sel, table, rows = evaluate(net, eval_pairs, sweeps, dev, log=lambda m: print(m, flush=True), level=args.level)
     meta = {**sel, "table": table, "train_pairs": args.pairs, "steps": args.steps, "ranks": world,
             "batch": args.batch, "crop": min(args.crop, args.level), "level": args.level, "eval_pairs": args.eval,
+            "train_max_disp": list(disp), "eval_max_disp": args.eval_max_disp,
             "train_seed0": TRAIN_SEED0, "eval_seed0": EVAL_SEED0, "loss_history": hist}
     np.savez(args.out, meta=json.dumps(meta), **net.state())
     print(json.dumps({k: v for k, v in meta.items() if k != "loss_history"}), flush=True)
