@@ -69,6 +69,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm-start arm")
+    p.add_argument("--no-roofline", action="store_true", help="skip the Liu-Shen roofline block (profiling runs)")
     p.add_argument("--no-configs", action="store_true", help="skip the HS 256^2 / LK 512^2 / batch workloads")
     p.add_argument("--no-batch", action="store_true", help="skip the 256-pair batch inside the configs block")
     p.add_argument("--learned-weights", default=None, help="weights + calibration .npz (default: packaged)")
@@ -452,7 +453,7 @@ def run_ours(args, rank, world, local_rank):
 
     # roofline of the dominant kernel: the step's Liu-Shen solves (--pairs of them at full
     # size, concurrently on --streams streams, as in the step), graph-replayed
-    roof = ls_step_roofline(args, frames, flush)
+    roof = None if args.no_roofline else ls_step_roofline(args, frames, flush)
 
     # end to end from host buffers to host results: the step's pairs as pinned uint8 frames
     # through HostBatch (frames up on one copy stream, the batch graph, U and V down into

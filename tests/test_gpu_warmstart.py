@@ -108,3 +108,38 @@ def test_fallback_returns_the_plain_pyramid(torch_cuda, trained):
                                            LS.LiuShenOpticalFlowAlgoAdapter(10))
     assert torch.equal(out[1][0], Up) and torch.equal(out[1][1], Vp)
     assert torch.equal(out[0][0], learned0[0]) and torch.equal(out[0][1], learned0[1])
+
+
+def test_large_displacement_network(torch_cuda):
+    """The network trained on 2-16 px flows (warmstart_weights_12px.npz), on held-out pairs
+    with displacements up to 12 px: with its calibrated stage (one Farneback iteration and
+    a few Liu-Shen sweeps) it is at least as accurate as the plain pyramid, while the same
+    stage from a zero start, with the calibration's most expensive zero-start stage, is far
+    off: at these displacements the start needs the coarse level, and the network gives it."""
+    torch = torch_cuda
+    import os
+    import Farneback_PyCL as F
+    import GenericPyramidalOpticalFlow as G
+    import PhysicsBasedOpticalFlowLiuShen as LS
+    from ofb200 import synthetic as S
+    from ofb200.warmstart import WEIGHTS, LearnedLiuShen, load_trained
+    net, meta = load_trained(path=os.path.join(os.path.dirname(WEIGHTS), "warmstart_weights_12px.npz"))
+    assert meta["eval_max_disp"] == 12.0
+    ll = LearnedLiuShen.from_meta(net, meta)
+    llz = LearnedLiuShen.from_meta(net, meta, "zero")
+    e_plain, e_learned, e_zero = [], [], []
+    for seed in (975_000, 975_001):
+        a, b, Ug, Vg = S.piv_pair(1024, 1024, "fourier", seed, density=0.05, diameter=(2.0, 3.0), noise=2.0,
+                                  max_disp=12.0)
+        A, B = _f32(torch, a), _f32(torch, b)
+        Up, Vp = G.genericPyramidalOpticalFlow(A, B, 0, F.Farneback_PyCL(), 2, 1, 0.48,
+                                               LS.LiuShenOpticalFlowAlgoAdapter(10))
+        e_plain.append(S.epe(Up.cpu().numpy(), Vp.cpu().numpy(), Ug, Vg, crop=16))
+        U, V, _, err = ll.run(A, B)
+        e_learned.append(S.epe(U.cpu().numpy(), V.cpu().numpy(), Ug, Vg, crop=16))
+        Z = torch.zeros_like(A)
+        Uz, Vz, _, _ = llz.refine(A, B, Z, Z.clone())
+        e_zero.append(S.epe(Uz.cpu().numpy(), Vz.cpu().numpy(), Ug, Vg, crop=16))
+    net.check()
+    assert np.mean(e_learned) <= np.mean(e_plain), (e_learned, e_plain)
+    assert np.mean(e_zero) > 3 * np.mean(e_plain), (e_zero, e_plain)
