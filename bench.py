@@ -1040,7 +1040,7 @@ def run_reference(args, rank, world):
         ncores = len(os.sched_getaffinity(0))
     except Exception:
         ncores = os.cpu_count() or 1
-    pairs = make_pairs(min(args.unique, 2), args.size)
+    pairs = make_pairs(args.unique, args.size)  # the same distinct pairs as the GPU arm's step
     work = [(p[0].astype(np.float32), p[1].astype(np.float32)) for p in pairs]
     ctx = mp.get_context("spawn")
     per_step = ncores
@@ -1058,7 +1058,9 @@ def run_reference(args, rank, world):
     return {"metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "pairs_per_step": per_step, "size": args.size},
+            "config": {"workload": WORKLOAD, "pairs_per_step": per_step, "size": args.size,
+                       "unique_pairs": args.unique,
+                       "parallelism": f"one pair per host process, {per_step} processes"},
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": ncores, "kind": "port",
                              "sample": f"{per_step} pairs per step, one per process, {steps} of "
                                        f"{args.steps} steps (capped at {REF_BUDGET_S:.0f} s)"},
