@@ -25,8 +25,8 @@ struct HqRow {
 };
 
 template <int RW, bool FAST>
-__device__ __forceinline__ void hq_load(HqRow<FAST>& R, const HqVal<FAST>* su, const HqVal<FAST>* sv, int row, int cm,
-                                        int c, int cp) {
+__device__ __forceinline__ void hq_load(HqRow<FAST>& R, const HqVal<FAST>* __restrict__ su,
+                                        const HqVal<FAST>* __restrict__ sv, int row, int cm, int c, int cp) {
   const int o = row * RW;
   R.ul = su[o + cm];
   R.um = su[o + c];
@@ -41,8 +41,8 @@ __device__ __forceinline__ void hq_load(HqRow<FAST>& R, const HqVal<FAST>* su, c
 template <bool FAST>
 __device__ __forceinline__ void hq_update(const HqRow<FAST>& U, const HqRow<FAST>& C, const HqRow<FAST>& D, int i,
                                           const float* __restrict__ sfx, const float* __restrict__ sfy,
-                                          const float* __restrict__ sft, HqVal<FAST>* du, HqVal<FAST>* dv,
-                                          float a2) {
+                                          const float* __restrict__ sft, HqVal<FAST>* __restrict__ du,
+                                          HqVal<FAST>* __restrict__ dv, float a2) {
   float ua, va;
   if constexpr (FAST) {  // float32 averaging: corner and edge sums, one multiply-add each
     const float wcf = 1.0f / 12.0f, wef = 1.0f / 6.0f;
@@ -76,12 +76,15 @@ __device__ __forceinline__ void hq_update(const HqRow<FAST>& U, const HqRow<FAST
 
 // Sweep s of the region: thread t owns column t % RW and walks a band of the rows the sweep
 // computes (band t / RW of HQ_THREADS / RW) with a 3-row register window, so each row it
-// visits costs one row of loads.  On image borders the neighbour columns and the window's
+// visits costs one row of loads.  The input and output buffers are distinct (ping-pong), so
+// the pointers are restrict: the loads of the next rows may move ahead of this row's
+// stores and the rows' float64 chains overlap.  On image borders the neighbour columns and the window's
 // outer rows go through the 'mirror' map; inside the image the mapped row is the row.
 template <int RW, int RH, int T, bool EDGE, bool FAST>
 __device__ __forceinline__ void hq_sweep(const float* __restrict__ sfx, const float* __restrict__ sfy,
-                                         const float* __restrict__ sft, const HqVal<FAST>* su, const HqVal<FAST>* sv,
-                                         HqVal<FAST>* du, HqVal<FAST>* dv, int s, int x0, int y0, int H, int W,
+                                         const float* __restrict__ sft, const HqVal<FAST>* __restrict__ su,
+                                         const HqVal<FAST>* __restrict__ sv, HqVal<FAST>* __restrict__ du,
+                                         HqVal<FAST>* __restrict__ dv, int s, int x0, int y0, int H, int W,
                                          float a2) {
   static_assert(HQ_THREADS % RW == 0, "a whole number of bands");
   constexpr int NB = HQ_THREADS / RW;
