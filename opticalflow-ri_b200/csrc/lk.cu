@@ -139,10 +139,10 @@ __device__ __forceinline__ bool lk_on(unsigned act, int v, int ty, int tx, int x
 }
 
 // DEF: the default window (27 x 27, no asymmetric mask), whose tile-weight pattern is known
-// at compile time: lane (xid, yid)'s 4th column tile is used when xid < 3, its 4th row tile
+// at compile time (and whose registers fit 3 CTAs per SM, 80 per thread): lane (xid, yid)'s 4th column tile is used when xid < 3, its 4th row tile
 // of the first half when yid < 3, the 4th row tile of the second half never.
 template <bool DEF>
-__global__ void __launch_bounds__(256, 2) lk_dense_kernel(const float* __restrict__ I, const float* __restrict__ J,
+__global__ void __launch_bounds__(256, DEF ? 3 : 2) lk_dense_kernel(const float* __restrict__ I, const float* __restrict__ J,
                                                        float* __restrict__ U, float* __restrict__ V, int H, int W,
                                                        int pitch, LkParams p, uint8_t* __restrict__ status,
                                                        float* __restrict__ err) {
