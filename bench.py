@@ -128,6 +128,14 @@ def run_hs_only(args):
     out = {"mode": "hs", "size": args.size, "sweeps": 600}
     U, V = z.clone(), z.clone()
     out["of_hs_solve_ms"] = timeit(lambda: ops.hs_solve(a, b, U.zero_(), V.zero_(), 21.0, 600))
+    Um, Vm = z.clone(), z.clone()
+    out["of_hs_solve_multilaunch_ms"] = timeit(lambda: ops.hs_solve(a, b, Um.zero_(), Vm.zero_(), 21.0, 600,
+                                                                    persistent=False))
+    for ar in ("exact", "fast"):  # one thread-block cluster (the tile shapes do not apply)
+        U2, V2 = z.clone(), z.clone()
+        out[f"of_hs_batch_cluster_{ar}_ms"] = timeit(lambda: ops.hs_batch(
+            [(a, b, U2.zero_(), V2.zero_(), 21.0, 600)], arithmetic=ar, schedule="cluster"))
+        out[f"cluster_{ar}_maxdiff"] = float(max((U2 - U).abs().max().item(), (V2 - V).abs().max().item()))
     for sched in ("queue", "resident"):
         for k, shp in enumerate(ops.hs_batch_shapes()):
             for ar in ("exact", "fast"):

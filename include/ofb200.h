@@ -163,13 +163,21 @@ typedef struct OfTuning {
 #define OF_HS_EXACT 0
 #define OF_HS_FAST 1
 /* AUTO: RESIDENT when every tile of the launch can have a resident CTA of its own, else
- * QUEUE.  QUEUE: (pass, pair, tile) items from a device ticket counter.  RESIDENT: one CTA
- * per tile for the whole solve, its derivative planes and flow kept in shared memory, only
- * the halo ring exchanged through global memory (OF_ERR_INVALID when the tiles outnumber
- * the resident CTAs).  The schedules give identical results. */
+ * QUEUE.
+ * QUEUE: (pass, pair, tile) items from a device ticket counter.
+ * RESIDENT: one CTA per tile for the whole solve, its derivative planes and flow kept in
+ * shared memory, only the halo ring exchanged through global memory (OF_ERR_INVALID when
+ * the tiles outnumber the resident CTAs).
+ * CLUSTER: one pair of at most 16 tiles of 64 x 64 (256 x 256 and smaller) on one
+ * thread-block cluster, the halo exchanged through distributed shared memory with one
+ * cluster barrier per sweep (OF_ERR_INVALID for other batches, OF_ERR_UNSUPPORTED where
+ * the device cannot hold the cluster).  At 256 x 256 its per-sweep cluster barrier makes
+ * it slower than RESIDENT; AUTO does not pick it.
+ * The schedules give identical results. */
 #define OF_HS_SCHED_AUTO 0
 #define OF_HS_SCHED_QUEUE 1
 #define OF_HS_SCHED_RESIDENT 2
+#define OF_HS_SCHED_CLUSTER 3
 
 /* One Horn-Schunck pair of a batch: DEVICE planes of H x W float32 with row pitch `pitch`;
  * U, V hold the initial flow and receive the result. */

@@ -19,6 +19,8 @@
 // (still counted, so nothing waits on it).
 // Cross-CTA data goes through L2 only (ld.global.cg / st.global.cg), published by
 // __syncthreads + __threadfence + atomicAdd and consumed after the counter is observed.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "hsweep.cuh"
 
@@ -411,6 +413,205 @@ __global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restri
   }
 }
 
+// ---- One pair on one thread-block cluster ------------------------------------------------
+// For images that one cluster of at most 16 CTAs covers with tiles of at most HC_T x HC_T
+// cells (256 x 256 and smaller).  CTA (cx, cy) owns a tile and holds the tile plus a
+// one-cell halo ring of (u, v) in shared memory, in two buffers, with the tile's derivative
+// planes.  A sweep reads its input buffer (all local), writes the owned cells of the output
+// buffer, and every cell that a halo ring shows (a neighbouring tile's ring, or a mirrored
+// position on the image border) is also stored there, in that CTA's shared memory
+// (distributed shared memory).  One cluster barrier per sweep publishes the sweep: no
+// global memory and no polling between sweeps.  Each halo position has exactly one source
+// cell, so no position is written twice; a CTA only reads its input buffer while its
+// neighbours write its output buffer.  Cell arithmetic: hq_update, bit for bit.
+constexpr int HC_T = 64;              // largest tile edge
+constexpr int HC_RS = HC_T + 2;       // region row stride: tile + halo ring
+constexpr int HC_PL = HC_RS * HC_RS;  // cells per region plane
+constexpr int HC_THREADS = 512;
+constexpr int HC_MAX_CTAS = 16;
+static_assert((3 * HC_PL * 4) % 8 == 0, "the float64 planes after the float planes stay 8-byte aligned");
+
+template <bool FAST>
+constexpr size_t hc_smem() {
+  return 3 * (size_t)HC_PL * sizeof(float) + 4 * (size_t)HC_PL * sizeof(HqVal<FAST>);
+}
+
+struct HcGeom {
+  int CX, CY;  // tiles per row / column (the cluster's shape)
+  int TW, TH;  // tile size (the last column / row of tiles may be smaller)
+};
+
+// Tiles of one axis whose region (tile plus the halo ring) contains position p (-1 .. n):
+// the tile p lies in (or the nearest one, for -1 and n) and, on a tile edge, its neighbour.
+__device__ __forceinline__ int hc_tiles_of(int p, int n, int T, int ntiles, int t[2]) {
+  const int own = clampi(p < 0 ? 0 : p / T, 0, ntiles - 1);
+  const int lo = own * T, hi = min(lo + T, n) - 1;  // the tile's cells
+  int k = 0;
+  t[k++] = own;
+  if (p == lo && own > 0) t[k++] = own - 1;          // the previous tile's last halo row
+  if (p == hi && own < ntiles - 1) t[k++] = own + 1;  // the next tile's first halo row
+  return k;
+}
+
+// The other positions a halo ring shows cell (gy, gx) at, as (CTA rank << 16 | region
+// offset) entries: mirror images on the image border (index -1 shows 1, H shows H - 2) and
+// the neighbouring tiles' rings.  Returns the count (at most HC_MAX_TARGETS).
+constexpr int HC_MAX_TARGETS = 8;
+__device__ __forceinline__ int hc_targets(int gy, int gx, int H, int W, const HcGeom& g, int cx, int cy,
+                                          int* tgt) {
+  int ys[2], xs[2], ny = 1, nx = 1, n = 0;
+  ys[0] = gy;
+  xs[0] = gx;
+  if (gy == 1) ys[ny++] = -1;
+  else if (gy == H - 2) ys[ny++] = H;
+  if (gx == 1) xs[nx++] = -1;
+  else if (gx == W - 2) xs[nx++] = W;
+  for (int a = 0; a < ny; a++) {
+    int ty[2];
+    const int nty = hc_tiles_of(ys[a], H, g.TH, g.CY, ty);
+    for (int b = 0; b < nx; b++) {
+      int tx[2];
+      const int ntx = hc_tiles_of(xs[b], W, g.TW, g.CX, tx);
+      for (int i = 0; i < nty; i++)
+        for (int j = 0; j < ntx; j++) {
+          if (a == 0 && b == 0 && ty[i] == cy && tx[j] == cx) continue;  // the cell itself
+          if (n == HC_MAX_TARGETS) return n;
+          const int o = (ys[a] - ty[i] * g.TH + 1) * HC_RS + (xs[b] - tx[j] * g.TW + 1);
+          tgt[n++] = ((tx[j] + ty[i] * g.CX) << 16) | o;  // rank, region offset (< 2^16)
+        }
+    }
+  }
+  return n;
+}
+
+template <bool FAST>
+__global__ void __launch_bounds__(HC_THREADS, 1) hsc_kernel(const HsqPair P, const HcGeom g, int* status) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) float hc_sm[];
+  using V = HqVal<FAST>;
+  float* const sfx = hc_sm;
+  float* const sfy = sfx + HC_PL;
+  float* const sft = sfy + HC_PL;
+  V* const bu0 = reinterpret_cast<V*>(sft + HC_PL);
+  V* const bv0 = bu0 + HC_PL;
+  V* const bu1 = bu0 + 2 * HC_PL;
+  V* const bv1 = bu0 + 3 * HC_PL;
+  const int cx = blockIdx.x, cy = blockIdx.y;
+  const int H = P.H, W = P.W, pitch = P.pitch;
+  const int x0 = cx * g.TW, y0 = cy * g.TH;
+  const int tw = min(g.TW, W - x0), th = min(g.TH, H - y0);
+  // region cell (ry, rx) <-> image cell (y0 - 1 + ry, x0 - 1 + rx); the ring mirrors the
+  // image border like the stencil's neighbour map
+  bool ok = true;
+  for (int k = threadIdx.x; k < (th + 2) * (tw + 2); k += HC_THREADS) {
+    const int ry = k / (tw + 2), rx = k - ry * (tw + 2);
+    const int o = ry * HC_RS + rx;
+    const size_t gi = (size_t)mirror1(y0 - 1 + ry, H) * pitch + mirror1(x0 - 1 + rx, W);
+    bu0[o] = (V)P.U[gi];
+    bv0[o] = (V)P.V[gi];
+    if (ry >= 1 && ry <= th && rx >= 1 && rx <= tw) {
+      float fx, fy, ft;
+      ok = hq_deriv(P, y0 - 1 + ry, x0 - 1 + rx, fx, fy, ft) && ok;
+      sfx[o] = fx;
+      sfy[o] = fy;
+      sft[o] = ft;
+    }
+  }
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(status, OF_ST_NONFINITE_INPUT);
+  cl.sync();  // every CTA of the cluster runs and holds its initial region
+  // the thread's halo source: candidate t among the tile's edge rows and columns and the
+  // rows / columns the image border mirrors (4 rows x tw + 4 columns x th <= HC_THREADS),
+  // with the positions it is copied to after each sweep
+  int hsrc = -1, ntg = 0, tgt[HC_MAX_TARGETS];
+  {
+    const int t = threadIdx.x;
+    const int rset[4] = {1, th, 2 - y0, H - 1 - y0};  // region rows of gy = y0, y0 + th - 1, 1, H - 2
+    const int cset[4] = {1, tw, 2 - x0, W - 1 - x0};
+    auto in_rset = [&](int r, int upto) {
+      for (int j = 0; j < upto; j++)
+        if (rset[j] == r) return true;
+      return false;
+    };
+    int r = -1, cc = -1;
+    bool valid = false;
+    if (t < 4 * tw) {
+      const int k = t / tw;
+      r = rset[k];
+      cc = t - k * tw + 1;
+      valid = r >= 1 && r <= th && !in_rset(r, k);
+    } else if (t < 4 * tw + 4 * th) {
+      const int u = t - 4 * tw, k = u / th;
+      cc = cset[k];
+      r = u - k * th + 1;
+      bool dup = false;
+      for (int j = 0; j < k; j++) dup = dup || cset[j] == cc;
+      for (int j = 0; j < 4; j++) dup = dup || (rset[j] == r && rset[j] >= 1 && rset[j] <= th);
+      valid = cc >= 1 && cc <= tw && !dup;
+    }
+    if (valid) {
+      ntg = hc_targets(y0 - 1 + r, x0 - 1 + cc, H, W, g, cx, cy, tgt);
+      if (ntg > 0) hsrc = r * HC_RS + cc;
+    }
+  }
+  // compute: owned column c of the tile, a band of its rows
+  constexpr int NB = HC_THREADS / HC_T;
+  const int c = (int)threadIdx.x % HC_T, band = (int)threadIdx.x / HC_T;
+  const int ra = 1 + (th * band) / NB, rb = 1 + (th * (band + 1)) / NB;  // region rows
+  const int rc = c + 1;                                                // region column
+  const bool on = c < tw && rb > ra;
+  for (int s = 0; s < P.niter; s++) {
+    const bool q = s & 1;
+    const V* su = q ? bu1 : bu0;
+    const V* sv = q ? bv1 : bv0;
+    V* du = q ? bu0 : bu1;
+    V* dv = q ? bv0 : bv1;
+    if (on) {
+      HqRow<FAST> A, B, C;
+      hq_load<HC_RS, FAST>(A, su, sv, ra - 1, rc - 1, rc, rc + 1);
+      hq_load<HC_RS, FAST>(B, su, sv, ra, rc - 1, rc, rc + 1);
+#pragma unroll 1
+      for (int r = ra; r < rb; r += 3) {
+        hq_load<HC_RS, FAST>(C, su, sv, r + 1, rc - 1, rc, rc + 1);
+        hq_update<FAST>(A, B, C, r * HC_RS + rc, sfx, sfy, sft, du, dv, P.a2);
+        if (r + 1 < rb) {
+          hq_load<HC_RS, FAST>(A, su, sv, r + 2, rc - 1, rc, rc + 1);
+          hq_update<FAST>(B, C, A, (r + 1) * HC_RS + rc, sfx, sfy, sft, du, dv, P.a2);
+        }
+        if (r + 2 < rb) {
+          hq_load<HC_RS, FAST>(B, su, sv, r + 3, rc - 1, rc, rc + 1);
+          hq_update<FAST>(C, A, B, (r + 2) * HC_RS + rc, sfx, sfy, sft, du, dv, P.a2);
+        }
+      }
+    }
+    __syncthreads();  // the tile's cells of this sweep are in shared memory
+    if (hsrc >= 0) {  // copies on the halo rings (this CTA's and its neighbours')
+      const V u = du[hsrc], v = dv[hsrc];
+#pragma unroll
+      for (int k = 0; k < HC_MAX_TARGETS; k++)
+        if (k < ntg) {
+          const unsigned int rank = (unsigned int)tgt[k] >> 16;
+          const int o = tgt[k] & 0xffff;
+          *cl.map_shared_rank(du + o, rank) = u;
+          *cl.map_shared_rank(dv + o, rank) = v;
+        }
+    }
+    cl.sync();  // the sweep, rings included, is visible cluster-wide
+  }
+  const V* fu = (P.niter & 1) ? bu1 : bu0;
+  const V* fv = (P.niter & 1) ? bv1 : bv0;
+  ok = true;
+  for (int k = threadIdx.x; k < th * tw; k += HC_THREADS) {
+    const int r = k / tw, cc = k - r * tw;
+    const int o = (r + 1) * HC_RS + cc + 1;
+    const size_t gi = (size_t)(y0 + r) * pitch + x0 + cc;
+    P.U[gi] = (float)fu[o];
+    P.V[gi] = (float)fv[o];
+    ok = ok && isfinite(fu[o]) && isfinite(fv[o]);
+  }
+  if (__syncthreads_or(!ok) && threadIdx.x == 0 && P.niter > 0) atomicOr(status, OF_ST_NONFINITE_OUTPUT);
+}
+
 // Pair descriptors travel as kernel parameters (captured by value in a CUDA graph), up to
 // HQ_DESC_CHUNK per launch of this copy kernel.
 constexpr int HQ_DESC_CHUNK = 24;  // 24 x 128 B, within the classic 4 KB of parameters
@@ -477,6 +678,70 @@ cudaError_t hsq_launch(bool fast, bool resident, int grid, const HsqPair* pairs,
 }
 }  // namespace
 
+// The cluster schedule's geometry for an H x W image: at most HC_MAX_CTAS tiles of at most
+// HC_T x HC_T cells.
+static bool hc_geometry(int H, int W, HcGeom* g) {
+  if (H < 16 || W < 16) return false;
+  g->CX = (W + HC_T - 1) / HC_T;
+  g->CY = (H + HC_T - 1) / HC_T;
+  if (g->CX * g->CY > HC_MAX_CTAS) return false;
+  g->TW = (W + g->CX - 1) / g->CX;
+  g->TH = (H + g->CY - 1) / g->CY;
+  return true;
+}
+
+template <bool FAST>
+static cudaError_t hsc_config(const HcGeom& g, cudaStream_t st, cudaLaunchConfig_t* cfg, cudaLaunchAttribute* attr) {
+  cudaError_t e = cudaFuncSetAttribute(hsc_kernel<FAST>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e == cudaSuccess) e = OF_SMEM_OPT_IN(hsc_kernel<FAST>, hc_smem<FAST>());
+  *cfg = cudaLaunchConfig_t{};
+  cfg->gridDim = dim3(g.CX, g.CY, 1);
+  cfg->blockDim = dim3(HC_THREADS, 1, 1);
+  cfg->dynamicSmemBytes = hc_smem<FAST>();
+  cfg->stream = st;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = g.CX;
+  attr[0].val.clusterDim.y = g.CY;
+  attr[0].val.clusterDim.z = 1;
+  cfg->attrs = attr;
+  cfg->numAttrs = 1;
+  return e;
+}
+
+// Whether the device can hold a cluster of this shape (all its CTAs at once).
+static bool hsc_schedulable(bool fast, const HcGeom& g) {
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute attr[1];
+  int n = 0;
+  cudaError_t e;
+  if (fast) {
+    e = hsc_config<true>(g, nullptr, &cfg, attr);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&n, hsc_kernel<true>, &cfg);
+  } else {
+    e = hsc_config<false>(g, nullptr, &cfg, attr);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&n, hsc_kernel<false>, &cfg);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // clear: a refused shape only means the other schedules run
+    return false;
+  }
+  return n >= 1;
+}
+
+static cudaError_t hsc_launch(bool fast, const HsqPair& P, const HcGeom& g, int* status, cudaStream_t st) {
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute attr[1];
+  cudaError_t e;
+  if (fast) {
+    e = hsc_config<true>(g, st, &cfg, attr);
+    if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, hsc_kernel<true>, P, g, status);
+  } else {
+    e = hsc_config<false>(g, st, &cfg, attr);
+    if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, hsc_kernel<false>, P, g, status);
+  }
+  return e;
+}
+
 // tiles of a pair under the tile shape that cuts it finest (sizes the per-tile counters)
 static size_t hsq_max_tiles(const OfHsBatchPair* pairs, int n) {
   size_t total = 0;
@@ -516,8 +781,9 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
   OF_REQUIRE(arith == OF_HS_EXACT || arith == OF_HS_FAST, "of_hs_batch: hs_arithmetic must be OF_HS_EXACT or OF_HS_FAST");
   const bool fast = arith == OF_HS_FAST;
   const int sched = tuning ? tuning->hs_schedule : OF_HS_SCHED_AUTO;
-  OF_REQUIRE(sched == OF_HS_SCHED_AUTO || sched == OF_HS_SCHED_QUEUE || sched == OF_HS_SCHED_RESIDENT,
-             "of_hs_batch: hs_schedule must be OF_HS_SCHED_AUTO, _QUEUE or _RESIDENT");
+  OF_REQUIRE(sched == OF_HS_SCHED_AUTO || sched == OF_HS_SCHED_QUEUE || sched == OF_HS_SCHED_RESIDENT ||
+                 sched == OF_HS_SCHED_CLUSTER,
+             "of_hs_batch: hs_schedule must be OF_HS_SCHED_AUTO, _QUEUE, _RESIDENT or _CLUSTER");
   OF_REQUIRE(shape >= 0 && shape < kHsqNumShapes, "of_hs_batch: tile_shape must be in 0..%d", kHsqNumShapes - 1);
   const HsqShape sh = kHsqShapes[shape];
   const int TW = sh.rw - 2 * sh.t, TH = sh.rh - 2 * sh.t;
@@ -565,6 +831,23 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
     P.tile0 = tiles_total;
     tiles_total += (unsigned int)P.tiles;
     if (P.passes > max_passes) max_passes = P.passes;
+  }
+  // the cluster schedule (one pair that one cluster covers); it needs neither the
+  // descriptors in memory nor the counters
+  if (sched == OF_HS_SCHED_CLUSTER) {
+    HcGeom hg;
+    const bool fits = n == 1 && hc_geometry(pairs[0].H, pairs[0].W, &hg);
+    const HsqPair P = hp[0];
+    delete[] hp;
+    if (!fits)
+      return set_error(OF_ERR_INVALID, "of_hs_batch: the cluster schedule takes one pair of at most %d tiles of %d x %d",
+                       HC_MAX_CTAS, HC_T, HC_T);
+    if (!hsc_schedulable(fast, hg))
+      return set_error(OF_ERR_UNSUPPORTED, "of_hs_batch: the device cannot hold a %d x %d cluster of this kernel",
+                       hg.CX, hg.CY);
+    cudaError_t e = hsc_launch(fast, P, hg, status, st);
+    if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: cluster launch: %s", cudaGetErrorString(e));
+    return check_launch("of_hs_batch", 1);
   }
   long long nl = 0;
   for (int b = 0; b < n; b += HQ_DESC_CHUNK) {

@@ -301,7 +301,7 @@ def hs_batch_shapes():
 HS_WAIT_LIMIT = 1 << 20  # polls of a queue wait before a pair is given up (under a second)
 
 
-HS_SCHEDULES = ("auto", "queue", "resident")  # OF_HS_SCHED_AUTO / _QUEUE / _RESIDENT
+HS_SCHEDULES = ("auto", "queue", "resident", "cluster")  # OF_HS_SCHED_AUTO / _QUEUE / _RESIDENT / _CLUSTER
 
 
 def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status=None, arithmetic: str = "exact",
@@ -309,8 +309,10 @@ def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status
     """Horn-Schunck of many pairs in one persistent launch (of_hs_batch).  pairs: list of
     (I0, I1, U, V, alpha, niter) with CUDA float32 planes; U, V are updated in place.
     arithmetic: 'exact' (bit-exact with the reference) or 'fast' (float32 averaging).
-    schedule: 'resident' (one CTA per tile, region kept on chip; needs every tile to get a
-    resident CTA), 'queue' (device work queue) or 'auto' (resident when it fits).
+    schedule: 'cluster' (one pair of at most 256 x 256 on one thread-block cluster, halos
+    through distributed shared memory), 'resident' (one CTA per tile, region kept on chip;
+    needs every tile to get a resident CTA), 'queue' (device work queue) or 'auto' (resident
+    when it fits, else queue).
     Returns the per-pair status words (device int32, bits of ofb200._lib.ST_*)."""
     if arithmetic not in ("exact", "fast"):
         raise ValueError("arithmetic must be 'exact' or 'fast'")

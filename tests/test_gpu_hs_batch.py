@@ -47,7 +47,7 @@ def test_persistent_single_solve_equals_multi_launch(cuda_ok, H, W, niter):
 SCHEDULES = ["queue", "resident"]
 
 
-@pytest.mark.parametrize("schedule", SCHEDULES)
+@pytest.mark.parametrize("schedule", SCHEDULES + ["cluster"])
 @pytest.mark.parametrize("shape_index", [0, 1, 2, 3])
 def test_single_pair_config1_bit_exact(cuda_ok, shape_index, schedule):
     """256 x 256, alpha 21, 600 sweeps (the PyHSchunck_Fs3_4 calibration) in one launch."""
@@ -171,3 +171,43 @@ def test_resident_schedule_refuses_more_tiles_than_ctas(cuda_ok):
         ops.hs_batch([(a, a, U, V, 21.0, 4)], tile_shape=1, schedule="resident")
     st = ops.hs_batch([(a, a, U, V, 21.0, 4)], tile_shape=1, schedule="auto")
     assert int(st.item()) == 0 and float(U.abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("H,W,niter", [(256, 256, 601), (200, 130, 37), (64, 17, 9), (16, 16, 2), (100, 255, 0)])
+def test_cluster_schedule_shapes(cuda_ok, H, W, niter):
+    """The cluster schedule (one thread-block cluster, halos through distributed shared
+    memory) on uneven tilings, odd sweep counts and the smallest images, from a non-zero
+    initial flow, bit for bit against the multi-launch solver; float32 averaging within 1e-4."""
+    import torch
+    from ofb200 import ops
+    a, b = _pair(torch, H, W, 41)
+    g = torch.Generator().manual_seed(H * W)
+    U0 = (torch.randn(H, W, generator=g) * 0.3).cuda()
+    V0 = (torch.randn(H, W, generator=g) * 0.3).cuda()
+    Ur, Vr = _solve_ref(torch, a, b, U0, V0, 21.0, niter)
+    U, V = U0.clone(), V0.clone()
+    st = ops.hs_batch([(a, b, U, V, 21.0, niter)], schedule="cluster")
+    assert int(st.item()) == 0
+    assert torch.equal(U, Ur) and torch.equal(V, Vr)
+    U, V = U0.clone(), V0.clone()
+    st = ops.hs_batch([(a, b, U, V, 21.0, niter)], schedule="cluster", arithmetic="fast")
+    assert int(st.item()) == 0
+    assert max((U - Ur).abs().max().item(), (V - Vr).abs().max().item()) <= 1e-4
+
+
+def test_cluster_schedule_refusals_and_status(cuda_ok):
+    """Two pairs, or an image beyond 16 tiles of 64 x 64, are refused; a NaN frame sets the
+    status bits."""
+    import torch
+    from ofb200 import _lib, ops
+    a, b = _pair(torch, 64, 64, 5)
+    z = torch.zeros_like(a)
+    with pytest.raises(_lib.OfError):
+        ops.hs_batch([(a, b, z.clone(), z.clone(), 21.0, 4)] * 2, schedule="cluster")
+    big = torch.zeros(300, 300, device="cuda")
+    with pytest.raises(_lib.OfError):
+        ops.hs_batch([(big, big, big.clone(), big.clone(), 21.0, 4)], schedule="cluster")
+    b2 = b.clone()
+    b2[10, 20] = float("nan")
+    st = int(ops.hs_batch([(a, b2, z.clone(), z.clone(), 21.0, 40)], schedule="cluster").item())
+    assert st & _lib.ST_NONFINITE_INPUT and st & _lib.ST_NONFINITE_OUTPUT
