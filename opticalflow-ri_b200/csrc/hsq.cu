@@ -443,7 +443,7 @@ struct HcGeom {
 
 // Tiles of one axis whose region (tile plus the halo ring) contains position p (-1 .. n):
 // the tile p lies in (or the nearest one, for -1 and n) and, on a tile edge, its neighbour.
-__device__ __forceinline__ int hc_tiles_of(int p, int n, int T, int ntiles, int t[2]) {
+__device__ __forceinline__ int hc_tiles_of(int p, int n, int T, int ntiles, int t[3]) {
   const int own = clampi(p < 0 ? 0 : p / T, 0, ntiles - 1);
   const int lo = own * T, hi = min(lo + T, n) - 1;  // the tile's cells
   int k = 0;
@@ -467,10 +467,10 @@ __device__ __forceinline__ int hc_targets(int gy, int gx, int H, int W, const Hc
   if (gx == 1) xs[nx++] = -1;
   else if (gx == W - 2) xs[nx++] = W;
   for (int a = 0; a < ny; a++) {
-    int ty[2];
+    int ty[3];
     const int nty = hc_tiles_of(ys[a], H, g.TH, g.CY, ty);
     for (int b = 0; b < nx; b++) {
-      int tx[2];
+      int tx[3];
       const int ntx = hc_tiles_of(xs[b], W, g.TW, g.CX, tx);
       for (int i = 0; i < nty; i++)
         for (int j = 0; j < ntx; j++) {
