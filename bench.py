@@ -192,8 +192,10 @@ def run_e2e_only(args):
     host = [(a.astype(np.float32), b.astype(np.float32)) for a, b, _, _ in pairs]
     dev = torch.device("cuda", torch.cuda.current_device())
     hb = e2e_host_batch(args, pairs, dev, 1, lambda: None)
+    hb32 = e2e_host_batch(args, pairs, dev, 1, lambda: None, dtype=np.float32)
     one = e2e_single_call(host, 1, lambda: None, calls=max(2, args.steps))
-    print(json.dumps({"mode": "e2e", "size": args.size, "host_batch": hb, "single_call": one}))
+    print(json.dumps({"mode": "e2e", "size": args.size, "host_batch": hb, "host_batch_float32": hb32,
+                      "single_call": one}))
 
 
 def run_fb_only(args):
@@ -335,9 +337,10 @@ def pipeline_dev(a, b):
     return G.genericPyramidalOpticalFlow(a, b, 0, F.Farneback_PyCL(), 2, 1, 0.48, LS.LiuShenOpticalFlowAlgoAdapter(10))
 
 
-def e2e_host_batch(args, pairs, dev, world, barrier):
-    """pairs/s of --steps steps of --pairs pairs from pinned host uint8 frames to numpy U, V
-    through ofb200.batch.HostBatch, wall clock, max over ranks."""
+def e2e_host_batch(args, pairs, dev, world, barrier, dtype=np.uint8):
+    """pairs/s of --steps steps of --pairs pairs from pinned host frames (uint8, the camera's
+    format, or float32 as the reference's examples cast them) to numpy U, V through
+    ofb200.batch.HostBatch, wall clock, max over ranks."""
     import torch
     import torch.distributed as dist
     import Farneback_PyCL as F
@@ -346,7 +349,8 @@ def e2e_host_batch(args, pairs, dev, world, barrier):
     spec = PairSpec(0, lambda: F.Farneback_PyCL(), 2, 1, 0.48, lambda: LS.LiuShenOpticalFlowAlgoAdapter(10),
                     key=("fbls",))
     hb = HostBatch([spec] * args.pairs, streams=max(1, args.streams), depth=2)
-    pinned = [(torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()) for a, b, _, _ in pairs]
+    pinned = [(torch.from_numpy(a.astype(dtype)).pin_memory(), torch.from_numpy(b.astype(dtype)).pin_memory())
+              for a, b, _, _ in pairs]
     step_host = [pinned[i % len(pinned)] for i in range(args.pairs)]
     for _ in range(max(3, args.warmup)):
         hb.run(step_host)
@@ -364,10 +368,11 @@ def e2e_host_batch(args, pairs, dev, world, barrier):
     if world > 1:
         dist.all_reduce(dt, op=dist.ReduceOp.MAX)
     N = args.size * args.size
+    name = np.dtype(dtype).name
     return {"value": args.pairs * args.steps * world / float(dt.item()), "unit": "pairs/s",
-            "h2d_bytes_per_step": sum(a.numel() + b.numel() for a, b in step_host),
+            "h2d_bytes_per_step": sum(a.numel() * a.element_size() + b.numel() * b.element_size() for a, b in step_host),
             "d2h_bytes_per_step": 2 * N * 4 * args.pairs,
-            "api": "ofb200.batch.HostBatch: pinned uint8 frames in, numpy float32 U, V out, 2 steps in flight",
+            "api": f"ofb200.batch.HostBatch: pinned {name} frames in, numpy float32 U, V out, 2 steps in flight",
             "timing": "wall clock over the steps, max over ranks"}
 
 
@@ -469,6 +474,7 @@ def run_ours(args, rank, world, local_rank):
     e2e = None
     if not args.no_e2e:
         e2e = e2e_host_batch(args, pairs, dev, world, barrier)
+        e2e["float32_frames"] = e2e_host_batch(args, pairs, dev, world, barrier, dtype=np.float32)
         e2e["single_call"] = e2e_single_call(host_frames, world, barrier, calls=max(2, args.pairs))
     learned = None if args.no_learned else run_learned(args, step_frames, pairs, dev, flush, world,
                                                            pairs_total_ms=total_ms)
