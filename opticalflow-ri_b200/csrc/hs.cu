@@ -84,7 +84,7 @@ constexpr int HB_T = 4, HB_TW = 56, HB_TH = 32, HB_RW = HB_TW + 2 * HB_T, HB_RH 
 constexpr int HB_PL = HB_RW * HB_RH;
 constexpr size_t HB_SMEM = 3 * (size_t)HB_PL * sizeof(float) + 4 * (size_t)HB_PL * sizeof(double);  // 110 KB
 
-__global__ void __launch_bounds__(HQ_THREADS) hs_pass_kernel(const float* __restrict__ fx, const float* __restrict__ fy,
+__global__ void __launch_bounds__(HQ_THREADS, 2) hs_pass_kernel(const float* __restrict__ fx, const float* __restrict__ fy,
                                                       const float* __restrict__ ft, const float* __restrict__ U,
                                                       const float* __restrict__ V, float* __restrict__ Un,
                                                       float* __restrict__ Vn, int H, int W, int pitch, float a2,
@@ -115,11 +115,11 @@ __global__ void __launch_bounds__(HQ_THREADS) hs_pass_kernel(const float* __rest
   for (int s = 0; s < nsw; s++) {
     const int q = s & 1;
     if (edge)
-      hq_sweep<HB_RW, HB_RH, HB_T, true, false>(sfx, sfy, sft, HB_U(q), HB_V(q), HB_U(q ^ 1), HB_V(q ^ 1), s, x0, y0,
-                                                H, W, a2);
+      hq_sweep2<HB_RW, HB_RH, HB_T, true, false, HQ_THREADS, false>(sfx, sfy, sft, nullptr, HB_U(q), HB_V(q),
+                                                                   HB_U(q ^ 1), HB_V(q ^ 1), s, x0, y0, H, W, a2);
     else
-      hq_sweep<HB_RW, HB_RH, HB_T, false, false>(sfx, sfy, sft, HB_U(q), HB_V(q), HB_U(q ^ 1), HB_V(q ^ 1), s, x0,
-                                                 y0, H, W, a2);
+      hq_sweep2<HB_RW, HB_RH, HB_T, false, false, HQ_THREADS, false>(sfx, sfy, sft, nullptr, HB_U(q), HB_V(q),
+                                                                    HB_U(q ^ 1), HB_V(q ^ 1), s, x0, y0, H, W, a2);
     __syncthreads();
   }
   const double* fu = HB_U(nsw & 1);

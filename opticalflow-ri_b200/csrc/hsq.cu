@@ -145,15 +145,43 @@ __device__ __forceinline__ int hq_wait(const unsigned int* done, unsigned int ti
 // Shared memory: the derivative planes as float32 and two (u, v) buffers, float64 for the
 // bit-exact arithmetic (the values are float32 results, held exactly, so the reference's
 // float64 stencil sums need no conversion per neighbour) and float32 for OF_HS_FAST.
+// RD: after the (u, v) buffers, each cell's float64 reciprocal of its denominator (hq_div,
+// the branch-free quotient); left out of the largest region, whose two CTAs per SM it
+// would not leave room for (that shape divides with __fdiv_rn).
 template <int RW, int RH, int T>
 struct HqTile {
   static constexpr int TW = RW - 2 * T, TH = RH - 2 * T, PL = RW * RH;
-  static constexpr size_t smem(bool fast) { return 3 * (size_t)PL * 4 + 4 * (size_t)PL * (fast ? 4 : 8); }
+  static constexpr bool RD = PL <= 2048;
+  static_assert(PL % 2 == 0, "the float64 planes stay 8-byte aligned");
+  static constexpr size_t smem(bool fast) {
+    return 3 * (size_t)PL * 4 + 4 * (size_t)PL * (fast ? 4 : 8) + (RD ? (size_t)PL * 8 : 0);
+  }
 };
 
+// The sweeps of one pass on the region (nsw <= T of them), ping-pong from buffer 0, so an
+// even count leaves the result in buffer 0.
+template <int RW, int RH, int T, bool FAST, int NT>
+__device__ __forceinline__ void hq_sweeps(const float* sfx, const float* sfy, const float* sft, const double* srd,
+                                          HqVal<FAST>* bu0, HqVal<FAST>* bv0, HqVal<FAST>* bu1, HqVal<FAST>* bv1,
+                                          int nsw, bool edge, int x0, int y0, int H, int W, float a2) {
+#pragma unroll 1
+  for (int s = 0; s < nsw; s++) {
+    const bool q = s & 1;
+    HqVal<FAST>* iu = q ? bu1 : bu0;
+    HqVal<FAST>* iv = q ? bv1 : bv0;
+    HqVal<FAST>* ou = q ? bu0 : bu1;
+    HqVal<FAST>* ov = q ? bv0 : bv1;
+    constexpr bool RD = HqTile<RW, RH, T>::RD;
+    if (edge)
+      hq_sweep2<RW, RH, T, true, FAST, NT, RD>(sfx, sfy, sft, srd, iu, iv, ou, ov, s, x0, y0, H, W, a2);
+    else
+      hq_sweep2<RW, RH, T, false, FAST, NT, RD>(sfx, sfy, sft, srd, iu, iv, ou, ov, s, x0, y0, H, W, a2);
+    __syncthreads();
+  }
+}
 
 // Returns false when a result of the last pass is not finite.
-template <int RW, int RH, int T, bool FAST>
+template <int RW, int RH, int T, bool FAST, int NT>
 __device__ bool hq_sweep_item(const HsqPair& P, int pass, int tile, float* sm) {
   using G = HqTile<RW, RH, T>;
   const int ty = tile / P.tx, tx = tile - ty * P.tx;
@@ -177,35 +205,27 @@ __device__ bool hq_sweep_item(const HsqPair& P, int pass, int tile, float* sm) {
   V* const bv0 = bu0 + G::PL;
   V* const bu1 = bu0 + 2 * G::PL;
   V* const bv1 = bu0 + 3 * G::PL;
-  for (int k = threadIdx.x; k < G::PL; k += blockDim.x) {
+  double* const srd = reinterpret_cast<double*>(bu0 + 4 * G::PL);
+  for (int k = threadIdx.x; k < G::PL; k += NT) {
     const int r = k / RW, c = k - r * RW;
     const int gy = y0 - T + r, gx = x0 - T + c;
     if (gy < 0 || gy >= H || gx < 0 || gx >= W) continue;  // never read
     const size_t i = (size_t)gy * pitch + gx;
-    sfx[k] = __ldcg(P.fx + i);
-    sfy[k] = __ldcg(P.fy + i);
+    const float gxv = __ldcg(P.fx + i), gyv = __ldcg(P.fy + i);
+    sfx[k] = gxv;
+    sfy[k] = gyv;
     sft[k] = __ldcg(P.ft + i);
+    if (G::RD) srd[k] = hq_recip_den(gxv, gyv, P.a2);
     bu0[k] = __ldcg(srcu + i);
     bv0[k] = __ldcg(srcv + i);
   }
   __syncthreads();
   const bool edge = x0 < T || y0 < T || x0 + G::TW + T > W || y0 + G::TH + T > H;
-  for (int s = 0; s < nsw; s++) {
-    const bool q = s & 1;
-    V* iu = q ? bu1 : bu0;
-    V* iv = q ? bv1 : bv0;
-    V* ou = q ? bu0 : bu1;
-    V* ov = q ? bv0 : bv1;
-    if (edge)
-      hq_sweep<RW, RH, T, true, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
-    else
-      hq_sweep<RW, RH, T, false, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
-    __syncthreads();
-  }
+  hq_sweeps<RW, RH, T, FAST, NT>(sfx, sfy, sft, srd, bu0, bv0, bu1, bv1, nsw, edge, x0, y0, H, W, P.a2);
   const V* fu = (nsw & 1) ? bu1 : bu0;
   const V* fv = (nsw & 1) ? bv1 : bv0;
   bool finite = true;
-  for (int k = threadIdx.x; k < G::TW * G::TH; k += blockDim.x) {
+  for (int k = threadIdx.x; k < G::TW * G::TH; k += NT) {
     const int r = k / G::TW, c = k - r * G::TW;
     const int y = y0 + r, x = x0 + c;
     if (y >= H || x >= W) continue;
@@ -227,8 +247,8 @@ __device__ __forceinline__ int hq_pair_of(const HsqPair* __restrict__ pairs, int
   return lo;
 }
 
-template <int RW, int RH, int T, bool FAST>
-__global__ void __launch_bounds__(HQ_THREADS) hsq_kernel(const HsqPair* __restrict__ pairs, int npairs,
+template <int RW, int RH, int T, bool FAST, int NT>
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) hsq_kernel(const HsqPair* __restrict__ pairs, int npairs,
                                                   unsigned int tiles_total, int max_passes,
                                                   unsigned long long* ticket, unsigned int* done, int* status,
                                                   long long wait_limit, int* err_flag) {
@@ -268,13 +288,13 @@ __global__ void __launch_bounds__(HQ_THREADS) hsq_kernel(const HsqPair* __restri
     if (s_run) {
       if (pass == 0) {
         const int ty = tile / P.tx, tx = tile - ty * P.tx;
-        for (int k = threadIdx.x; k < G::TW * G::TH; k += blockDim.x) {
+        for (int k = threadIdx.x; k < G::TW * G::TH; k += NT) {
           const int rr = k / G::TW, cc = k - rr * G::TW;
           const int y = ty * G::TH + rr, x = tx * G::TW + cc;
           if (y < P.H && x < P.W) ok = hq_deriv_px(P, y, x) && ok;
         }
       } else {
-        ok = hq_sweep_item<RW, RH, T, FAST>(P, pass, tile, hq_sm);
+        ok = hq_sweep_item<RW, RH, T, FAST, NT>(P, pass, tile, hq_sm);
       }
     }
     const int bad = __syncthreads_or(!ok);  // also: every store of the item is issued
@@ -286,11 +306,28 @@ __global__ void __launch_bounds__(HQ_THREADS) hsq_kernel(const HsqPair* __restri
   }
 }
 
-constexpr unsigned int HQ_WARPS = HQ_THREADS / 32;
+// Cell k of a region's halo ring (the region minus its owned tile): the top T rows, the
+// bottom T rows, then the T columns left and right of the tile in each tile row.
+template <int RW, int RH, int T>
+__device__ __forceinline__ void hq_ring_cell(int k, int& r, int& c) {
+  constexpr int TW = RW - 2 * T, BAND = T * RW;
+  if (k < BAND) {
+    r = k / RW;
+    c = k - r * RW;
+  } else if (k < 2 * BAND) {
+    const int q = k - BAND;
+    r = RH - T + q / RW;
+    c = q - (q / RW) * RW;
+  } else {
+    const int m = k - 2 * BAND, cc = m % (2 * T);
+    r = T + m / (2 * T);
+    c = cc < T ? cc : cc + TW;
+  }
+}
 
 // Each warp publishes its own part of a stage: its stores (or reads) are ordered before its
 // increment of the tile's counter, so a stage of a tile is complete when the counter has
-// grown by HQ_WARPS; no CTA barrier sits between the last store and the release.
+// grown by the CTA's warp count; no CTA barrier sits between the last store and the release.
 __device__ __forceinline__ void hq_release_warp(unsigned int* counter) {
   __syncwarp();
   __threadfence();
@@ -305,11 +342,12 @@ __device__ __forceinline__ void hq_release_warp(unsigned int* counter) {
 // halo ring comes from global memory (the neighbours' results of stage s - 1); the owned
 // part is already in shared memory, where the previous stage's T (even) sweeps left it.
 // The owned tile is published every stage.  Waits are the queue kernel's, the counters
-// count warps: a stage waits for its own and its neighbours' counters to reach s x
-// HQ_WARPS, which also orders every overwrite of a ping-pong buffer (or of the initial U, V
-// at stage 1) after the neighbours' reads of it.
-template <int RW, int RH, int T, bool FAST>
-__global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restrict__ pairs, int npairs,
+// count warps: a stage waits for its own and its neighbours' counters to reach s x (NT /
+// 32), which also orders every overwrite of a ping-pong buffer (or of the initial U, V at
+// stage 1) after the neighbours' reads of it.  The halo ring of a stage is gathered with
+// every thread's loads in flight at once (one L2 round trip), then written to shared memory.
+template <int RW, int RH, int T, bool FAST, int NT>
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) hsr_kernel(const HsqPair* __restrict__ pairs, int npairs,
                                                   unsigned int* done, int* status, long long wait_limit,
                                                   int* err_flag) {
   static_assert(T % 2 == 0, "a full stage must leave its result in the first buffer");
@@ -333,10 +371,11 @@ __global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restri
   V* const bv0 = bu0 + G::PL;
   V* const bu1 = bu0 + 2 * G::PL;
   V* const bv1 = bu0 + 3 * G::PL;
+  double* const srd = reinterpret_cast<double*>(bu0 + 4 * G::PL);
   const bool edge = x0 < T || y0 < T || x0 + G::TW + T > W || y0 + G::TH + T > H;
   // stage 0
   bool ok = true;
-  for (int k = threadIdx.x; k < G::PL; k += blockDim.x) {
+  for (int k = threadIdx.x; k < G::PL; k += NT) {
     const int r = k / RW, c = k - r * RW;
     const int gy = y0 - T + r, gx = x0 - T + c;
     if (gy < 0 || gy >= H || gx < 0 || gx >= W) continue;  // never read
@@ -345,6 +384,7 @@ __global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restri
     sfx[k] = fx;
     sfy[k] = fy;
     sft[k] = ft;
+    if (G::RD) srd[k] = hq_recip_den(fx, fy, P.a2);
     const size_t gi = (size_t)gy * pitch + gx;
     bu0[k] = __ldcg(P.U + gi);
     bv0[k] = __ldcg(P.V + gi);
@@ -356,7 +396,7 @@ __global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restri
   for (int p = 0; p < np; p++) {
     const int stage = p + 1;
     if (threadIdx.x < 32) {
-      const int run = hq_wait(done, P.tile0, tile, P.tx, nty, (unsigned int)(stage * HQ_WARPS), wait_limit,
+      const int run = hq_wait(done, P.tile0, tile, P.tx, nty, (unsigned int)(stage * (NT / 32)), wait_limit,
                               status + i, err_flag);
       if (threadIdx.x == 0) s_run = run;
     }
@@ -369,33 +409,36 @@ __global__ void __launch_bounds__(HQ_THREADS) hsr_kernel(const HsqPair* __restri
       if (p > 0) {  // halo ring: the neighbours' results of the previous stage
         const float* srcu = to_uv ? P.Ub : P.U;
         const float* srcv = to_uv ? P.Vb : P.V;
-        for (int k = threadIdx.x; k < G::PL; k += blockDim.x) {
-          const int r = k / RW, c = k - r * RW;
-          if (r >= T && r < T + G::TH && c >= T && c < T + G::TW) continue;  // owned: on chip
+        constexpr int RING = G::PL - G::TW * G::TH, NK = (RING + NT - 1) / NT;
+        float hu[NK], hv[NK];
+        int ho[NK];
+#pragma unroll
+        for (int j = 0; j < NK; j++) {
+          int r, c;
+          hq_ring_cell<RW, RH, T>((int)threadIdx.x + j * NT, r, c);
           const int gy = y0 - T + r, gx = x0 - T + c;
-          if (gy < 0 || gy >= H || gx < 0 || gx >= W) continue;
-          const size_t gi = (size_t)gy * pitch + gx;
-          bu0[k] = __ldcg(srcu + gi);
-          bv0[k] = __ldcg(srcv + gi);
+          ho[j] = -1;
+          if ((int)threadIdx.x + j * NT < RING && gy >= 0 && gy < H && gx >= 0 && gx < W) {
+            const size_t gi = (size_t)gy * pitch + gx;
+            hu[j] = __ldcg(srcu + gi);
+            hv[j] = __ldcg(srcv + gi);
+            ho[j] = r * RW + c;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < NK; j++) {
+          if (ho[j] >= 0) {
+            bu0[ho[j]] = hu[j];
+            bv0[ho[j]] = hv[j];
+          }
         }
         __syncthreads();
       }
       const int nsw = min(T, P.niter - p * T);
-      for (int s = 0; s < nsw; s++) {
-        const bool q = s & 1;
-        V* iu = q ? bu1 : bu0;
-        V* iv = q ? bv1 : bv0;
-        V* ou = q ? bu0 : bu1;
-        V* ov = q ? bv0 : bv1;
-        if (edge)
-          hq_sweep<RW, RH, T, true, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
-        else
-          hq_sweep<RW, RH, T, false, FAST>(sfx, sfy, sft, iu, iv, ou, ov, s, x0, y0, H, W, P.a2);
-        __syncthreads();
-      }
+      hq_sweeps<RW, RH, T, FAST, NT>(sfx, sfy, sft, srd, bu0, bv0, bu1, bv1, nsw, edge, x0, y0, H, W, P.a2);
       const V* fu = (nsw & 1) ? bu1 : bu0;
       const V* fv = (nsw & 1) ? bv1 : bv0;
-      for (int k = threadIdx.x; k < G::TW * G::TH; k += blockDim.x) {
+      for (int k = threadIdx.x; k < G::TW * G::TH; k += NT) {
         const int r = k / G::TW, c = k - r * G::TW;
         const int y = y0 + r, x = x0 + c;
         if (y >= H || x >= W) continue;
@@ -628,53 +671,65 @@ __global__ void hsq_desc_kernel(const __grid_constant__ HsqDescChunk chunk, int 
 using namespace ofb;
 
 namespace {
-// tile shapes (region width x height, sweeps per pass) the queue kernel is built for
+// tile shapes (region width x height, sweeps per pass, threads per CTA) the persistent
+// kernels are built for; hsq_with_shape maps an index to the same shape at compile time
 struct HsqShape {
-  int rw, rh, t;
+  int rw, rh, t, nt;
 };
-constexpr HsqShape kHsqShapes[] = {{64, 40, 4}, {32, 24, 4}, {64, 24, 4}, {32, 32, 8}};
+constexpr HsqShape kHsqShapes[] = {{64, 40, 4, 256}, {32, 24, 4, 256}, {64, 24, 4, 256}, {32, 32, 8, 256},
+                                   {32, 48, 8, 512}};
 constexpr int kHsqNumShapes = sizeof(kHsqShapes) / sizeof(kHsqShapes[0]);
 
-template <int RW, int RH, int T, bool FAST>
+template <int RW_, int RH_, int T_, int NT_>
+struct HsqShapeT {
+  static constexpr int RW = RW_, RH = RH_, T = T_, NT = NT_;
+};
+
+template <class F>
+cudaError_t hsq_with_shape(int shape, F&& f) {
+  switch (shape) {
+    case 0: return f(HsqShapeT<64, 40, 4, 256>{});
+    case 1: return f(HsqShapeT<32, 24, 4, 256>{});
+    case 2: return f(HsqShapeT<64, 24, 4, 256>{});
+    case 3: return f(HsqShapeT<32, 32, 8, 256>{});
+    case 4: return f(HsqShapeT<32, 48, 8, 512>{});
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <class S, bool FAST>
 void* hsq_kernel_ptr(bool resident) {
-  return resident ? (void*)hsr_kernel<RW, RH, T, FAST> : (void*)hsq_kernel<RW, RH, T, FAST>;
+  return resident ? (void*)hsr_kernel<S::RW, S::RH, S::T, FAST, S::NT>
+                  : (void*)hsq_kernel<S::RW, S::RH, S::T, FAST, S::NT>;
 }
 
 // Opts the chosen kernel into its shared memory and reports how many of its CTAs fit on an SM.
-template <int RW, int RH, int T>
-int hsq_resident(bool fast, bool resident, int* per_sm) {
+template <class S>
+cudaError_t hsq_resident(bool fast, bool resident, int* per_sm) {
+  constexpr int RW = S::RW, RH = S::RH, T = S::T, NT = S::NT;
   using G = HqTile<RW, RH, T>;
   cudaError_t e;
   if (resident)
-    e = fast ? OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, true>), G::smem(true))
-             : OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, false>), G::smem(false));
+    e = fast ? OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, true, NT>), G::smem(true))
+             : OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, false, NT>), G::smem(false));
   else
-    e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true>), G::smem(true))
-             : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false>), G::smem(false));
-  if (e != cudaSuccess) return -1;
-  const void* k = fast ? hsq_kernel_ptr<RW, RH, T, true>(resident) : hsq_kernel_ptr<RW, RH, T, false>(resident);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, HQ_THREADS, G::smem(fast));
-  return e == cudaSuccess ? 0 : -1;
+    e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true, NT>), G::smem(true))
+             : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false, NT>), G::smem(false));
+  if (e != cudaSuccess) return e;
+  const void* k = fast ? hsq_kernel_ptr<S, true>(resident) : hsq_kernel_ptr<S, false>(resident);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, NT, G::smem(fast));
 }
 
-template <int RW, int RH, int T>
-cudaError_t hsq_launch(bool fast, bool resident, int grid, const HsqPair* pairs, int n, unsigned int tiles_total,
-                       int max_passes, unsigned long long* ticket, unsigned int* done, int* status,
-                       long long wait_limit, int* err_flag, cudaStream_t st) {
-  using G = HqTile<RW, RH, T>;
-  if (resident) {
-    if (fast)
-      hsr_kernel<RW, RH, T, true><<<grid, HQ_THREADS, G::smem(fast), st>>>(pairs, n, done, status, wait_limit, err_flag);
-    else
-      hsr_kernel<RW, RH, T, false><<<grid, HQ_THREADS, G::smem(fast), st>>>(pairs, n, done, status, wait_limit, err_flag);
-  } else if (fast) {
-    hsq_kernel<RW, RH, T, true><<<grid, HQ_THREADS, G::smem(fast), st>>>(pairs, n, tiles_total, max_passes, ticket, done,
-                                                                 status, wait_limit, err_flag);
-  } else {
-    hsq_kernel<RW, RH, T, false><<<grid, HQ_THREADS, G::smem(fast), st>>>(pairs, n, tiles_total, max_passes, ticket, done,
-                                                                  status, wait_limit, err_flag);
-  }
-  return cudaGetLastError();
+template <class S, bool FAST>
+void hsq_launch_as(bool resident, int grid, const HsqPair* pairs, int n, unsigned int tiles_total, int max_passes,
+                   unsigned long long* ticket, unsigned int* done, int* status, long long wait_limit, int* err_flag,
+                   cudaStream_t st) {
+  const size_t smem = HqTile<S::RW, S::RH, S::T>::smem(FAST);
+  if (resident)
+    hsr_kernel<S::RW, S::RH, S::T, FAST, S::NT><<<grid, S::NT, smem, st>>>(pairs, n, done, status, wait_limit, err_flag);
+  else
+    hsq_kernel<S::RW, S::RH, S::T, FAST, S::NT><<<grid, S::NT, smem, st>>>(pairs, n, tiles_total, max_passes, ticket,
+                                                                          done, status, wait_limit, err_flag);
 }
 }  // namespace
 
@@ -868,15 +923,11 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // every CTA must be resident (items wait for items of running CTAs)
   auto capacity = [&](bool resident, long long* cap) {
-    int per_sm = 0, rc;
-    switch (shape) {
-      case 0: rc = hsq_resident<64, 40, 4>(fast, resident, &per_sm); break;
-      case 1: rc = hsq_resident<32, 24, 4>(fast, resident, &per_sm); break;
-      case 2: rc = hsq_resident<64, 24, 4>(fast, resident, &per_sm); break;
-      default: rc = hsq_resident<32, 32, 8>(fast, resident, &per_sm); break;
-    }
+    int per_sm = 0;
+    const cudaError_t rc =
+        hsq_with_shape(shape, [&](auto S) { return hsq_resident<decltype(S)>(fast, resident, &per_sm); });
     *cap = (long long)sms * per_sm;
-    return rc == 0 && per_sm >= 1;
+    return rc == cudaSuccess && per_sm >= 1;
   };
   long long cap_r = 0, cap_q = 0;
   bool resident = false;
@@ -893,12 +944,16 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
     grid = cap_q < (long long)tiles_total ? cap_q : (long long)tiles_total;  // no more CTAs than items of a pass
   }
   if (grid < 1) grid = 1;
-  switch (shape) {
-    case 0: e = hsq_launch<64, 40, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    case 1: e = hsq_launch<32, 24, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    case 2: e = hsq_launch<64, 24, 4>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-    default: e = hsq_launch<32, 32, 8>(fast, resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag, st); break;
-  }
+  e = hsq_with_shape(shape, [&](auto S) {
+    using Sh = decltype(S);
+    if (fast)
+      hsq_launch_as<Sh, true>(resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status,
+                              wait_limit, err_flag, st);
+    else
+      hsq_launch_as<Sh, false>(resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status,
+                               wait_limit, err_flag, st);
+    return cudaGetLastError();
+  });
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: launch: %s", cudaGetErrorString(e));
   return check_launch("of_hs_batch", nl + 1);
 }

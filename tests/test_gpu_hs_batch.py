@@ -48,7 +48,7 @@ SCHEDULES = ["queue", "resident"]
 
 
 @pytest.mark.parametrize("schedule", SCHEDULES + ["cluster"])
-@pytest.mark.parametrize("shape_index", [0, 1, 2, 3])
+@pytest.mark.parametrize("shape_index", [0, 1, 2, 3, 4])
 def test_single_pair_config1_bit_exact(cuda_ok, shape_index, schedule):
     """256 x 256, alpha 21, 600 sweeps (the PyHSchunck_Fs3_4 calibration) in one launch."""
     import torch
@@ -63,10 +63,11 @@ def test_single_pair_config1_bit_exact(cuda_ok, shape_index, schedule):
     assert torch.equal(U, Ur) and torch.equal(V, Vr)
 
 
-@pytest.mark.parametrize("schedule", SCHEDULES)
-def test_uneven_batch_bit_exact(cuda_ok, schedule):
+@pytest.mark.parametrize("schedule,shape_index", [("queue", 0), ("resident", 0), ("queue", 4)])
+def test_uneven_batch_bit_exact(cuda_ok, schedule, shape_index):
     """Uneven sizes and sweep counts (600, 37, 9, 0: a last pass of fewer sweeps than the
-    shape's, and a pair with no sweep pass) in one launch."""
+    shape's, and a pair with no sweep pass) in one launch, with 256- and 512-thread CTAs
+    (the 573 tiles of shape 4 are more than the resident schedule's one CTA per SM)."""
     import torch
     from ofb200 import ops
     shapes = [(128, 128, 600), (256, 256, 600), (64, 200, 37), (512, 384, 120), (17, 23, 9), (16, 16, 0)]
@@ -78,7 +79,7 @@ def test_uneven_batch_bit_exact(cuda_ok, schedule):
         V0 = (torch.randn(H, W, generator=g) * 0.3).cuda()
         refs.append(_solve_ref(torch, a, b, U0, V0, 21.0 + k, n))
         pairs.append((a, b, U0.clone(), V0.clone(), 21.0 + k, n))
-    st = ops.hs_batch(pairs, tile_shape=0, schedule=schedule)
+    st = ops.hs_batch(pairs, tile_shape=shape_index, schedule=schedule)
     torch.cuda.synchronize()
     assert st.cpu().tolist() == [0] * len(shapes)
     for (_, _, U, V, _, _), (Ur, Vr) in zip(pairs, refs):
