@@ -162,8 +162,10 @@ typedef struct OfTuning {
 } OfTuning;
 #define OF_HS_EXACT 0
 #define OF_HS_FAST 1
-/* AUTO: RESIDENT when every tile of the launch can have a resident CTA of its own, else
- * QUEUE.
+/* AUTO: when the device can hold one CTA per tile, a launch of one CTA per tile that runs
+ * the RESIDENT schedule if all its CTAs get an SM at once and the QUEUE otherwise (the CTAs
+ * decide at their start, within a bounded poll: other work holding SMs only costs speed);
+ * else QUEUE.  of_hs_batch_schedule reports which one ran.
  * QUEUE: (pass, pair, tile) items from a device ticket counter.
  * RESIDENT: one CTA per tile for the whole solve, its derivative planes and flow kept in
  * shared memory, only the halo ring exchanged through global memory (OF_ERR_INVALID when
@@ -210,6 +212,11 @@ int of_ls_status(const int* iters, const double* err, int maxnum, double tol, in
 size_t of_hs_batch_workspace_size(const OfHsBatchPair* pairs, int n);
 int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tuning, int* status, long long wait_limit,
                 void* workspace, size_t workspace_bytes, void* stream);
+/* The schedule the last AUTO launch of of_hs_batch over this pair list and workspace ran:
+ * OF_HS_SCHED_RESIDENT or OF_HS_SCHED_QUEUE into *schedule (OF_HS_SCHED_AUTO when that launch
+ * chose statically: an explicit schedule, or tiles beyond one CTA each).  Waits for `stream`. */
+int of_hs_batch_schedule(const OfHsBatchPair* pairs, int n, const void* workspace, size_t workspace_bytes,
+                         int* schedule, void* stream);
 
 /* ---------------------------------------------------------------------------------
  * A8/A9 Liu-Shen physics-based optimiser — replaces LiuShenOpticalFlowAlgoAdapter.compute /

@@ -191,9 +191,10 @@ extern "C" int of_hs_derivatives(const float* I0, const float* I1, float* fx, fl
   return check_launch("of_hs_derivatives");
 }
 
-// of_hs_solve_persistent: one pair through the persistent kernel of hsq.cu (of_hs_batch,
-// device work queue: items only wait for items of running CTAs, so it is correct beside any
-// other work on the GPU, if slower there).
+// of_hs_solve_persistent: one pair through the persistent kernels of hsq.cu (of_hs_batch,
+// automatic schedule: the resident schedule when all the launch's CTAs run at once, else the
+// device work queue, whose items only wait for items of running CTAs, so it is correct
+// beside any other work on the GPU, if slower there).
 constexpr int kHsSolveShape = 3;  // of_hs_batch tile shape for one pair: 32 x 32 regions, 8 sweeps per pass
 
 static size_t hs_persistent_ws(int H, int W, int pitch) {
@@ -305,7 +306,7 @@ extern "C" int of_hs_solve_persistent(const float* I0, const float* I1, float* U
   cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), st);
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_solve_persistent: %s", cudaGetErrorString(e));
   OfHsBatchPair q = {I0, I1, U, V, H, W, pitch, alpha, niter};
-  OfTuning tun = {kHsSolveShape, 0, OF_HS_EXACT, OF_HS_SCHED_QUEUE};
+  OfTuning tun = {kHsSolveShape, 0, OF_HS_EXACT, OF_HS_SCHED_AUTO};
   const int rc = of_hs_batch(&q, 1, &tun, status, 1ll << 20, bw, bws, stream);
   if (rc != OF_OK) return rc;
   if (err_out) {

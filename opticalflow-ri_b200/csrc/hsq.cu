@@ -248,10 +248,9 @@ __device__ __forceinline__ int hq_pair_of(const HsqPair* __restrict__ pairs, int
 }
 
 template <int RW, int RH, int T, bool FAST, int NT>
-__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) hsq_kernel(const HsqPair* __restrict__ pairs, int npairs,
-                                                  unsigned int tiles_total, int max_passes,
-                                                  unsigned long long* ticket, unsigned int* done, int* status,
-                                                  long long wait_limit, int* err_flag) {
+__device__ __forceinline__ void hsq_body(const HsqPair* __restrict__ pairs, int npairs, unsigned int tiles_total,
+                                         int max_passes, unsigned long long* ticket, unsigned int* done, int* status,
+                                         long long wait_limit, int* err_flag) {
   extern __shared__ float hq_sm[];
   __shared__ unsigned long long s_item;
   __shared__ int s_run, s_pair;
@@ -347,9 +346,8 @@ __device__ __forceinline__ void hq_release_warp(unsigned int* counter) {
 // stage 1) after the neighbours' reads of it.  The halo ring of a stage is gathered with
 // every thread's loads in flight at once (one L2 round trip), then written to shared memory.
 template <int RW, int RH, int T, bool FAST, int NT>
-__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) hsr_kernel(const HsqPair* __restrict__ pairs, int npairs,
-                                                  unsigned int* done, int* status, long long wait_limit,
-                                                  int* err_flag) {
+__device__ __forceinline__ void hsr_body(const HsqPair* __restrict__ pairs, int npairs, unsigned int* done,
+                                         int* status, long long wait_limit, int* err_flag) {
   static_assert(T % 2 == 0, "a full stage must leave its result in the first buffer");
   extern __shared__ float hq_sm[];
   __shared__ int s_pair, s_run;
@@ -454,6 +452,71 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) hsr_kernel(const HsqPai
     }
     hq_release_warp(done + gtile);  // this warp's stores of the stage
   }
+}
+
+template <int RW, int RH, int T, bool FAST, int NT>
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2)
+    hsq_kernel(const HsqPair* __restrict__ pairs, int npairs, unsigned int tiles_total, int max_passes,
+               unsigned long long* ticket, unsigned int* done, int* status, long long wait_limit, int* err_flag) {
+  hsq_body<RW, RH, T, FAST, NT>(pairs, npairs, tiles_total, max_passes, ticket, done, status, wait_limit, err_flag);
+}
+
+template <int RW, int RH, int T, bool FAST, int NT>
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2)
+    hsr_kernel(const HsqPair* __restrict__ pairs, int npairs, unsigned int* done, int* status, long long wait_limit,
+               int* err_flag) {
+  hsr_body<RW, RH, T, FAST, NT>(pairs, npairs, done, status, wait_limit, err_flag);
+}
+
+// The adaptive schedule (one CTA per tile launched): the resident schedule when every CTA of
+// the launch runs at once, the queue otherwise, decided by the CTAs themselves at the start.
+// Each CTA counts itself into `arrived` and polls; the first to see all gridDim.x CTAs
+// arrived (all are running, and a running CTA runs to its end) sets the mode word to
+// RESIDENT, the first to give up after HQ_ARRIVE_POLLS polls (CTAs still waiting for an SM
+// that other work holds) sets it to QUEUE; the word is set once (compare-and-swap) and every
+// CTA follows it.  The queue is correct with any number of CTAs running, so neither outcome
+// waits on a CTA that may never start.
+constexpr int HQ_MODE_UNDECIDED = OF_HS_SCHED_AUTO, HQ_MODE_RESIDENT = OF_HS_SCHED_RESIDENT,
+              HQ_MODE_QUEUE = OF_HS_SCHED_QUEUE;
+constexpr int HQ_ARRIVE_POLLS = 256;
+
+__device__ __forceinline__ int hq_ld_acquire_i(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int hq_decide_mode(unsigned int* arrived, int* mode) {
+  __shared__ int s_mode;
+  if (threadIdx.x == 0) {
+    atomicAdd(arrived, 1u);
+    int m;
+    for (int k = 0;; k++) {  // at most HQ_ARRIVE_POLLS + 2 rounds: a give-up sets the word
+      m = hq_ld_acquire_i(mode);
+      if (m != HQ_MODE_UNDECIDED) break;
+      if (hq_ld_acquire(arrived) >= gridDim.x)
+        atomicCAS(mode, HQ_MODE_UNDECIDED, HQ_MODE_RESIDENT);
+      else if (k >= HQ_ARRIVE_POLLS)
+        atomicCAS(mode, HQ_MODE_UNDECIDED, HQ_MODE_QUEUE);
+      else
+        __nanosleep(128);
+    }
+    s_mode = m;
+  }
+  __syncthreads();
+  return s_mode;
+}
+
+template <int RW, int RH, int T, bool FAST, int NT>
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2)
+    hsa_kernel(const HsqPair* __restrict__ pairs, int npairs, unsigned int tiles_total, int max_passes,
+               unsigned long long* ticket, unsigned int* done, int* status, long long wait_limit, int* err_flag,
+               unsigned int* arrived, int* mode) {
+  if (hq_decide_mode(arrived, mode) == HQ_MODE_RESIDENT)
+    hsr_body<RW, RH, T, FAST, NT>(pairs, npairs, done, status, wait_limit, err_flag);
+  else
+    hsq_body<RW, RH, T, FAST, NT>(pairs, npairs, tiles_total, max_passes, ticket, done, status, wait_limit,
+                                  err_flag);
 }
 
 // ---- One pair on one thread-block cluster ------------------------------------------------
@@ -697,39 +760,51 @@ cudaError_t hsq_with_shape(int shape, F&& f) {
   }
 }
 
+// which persistent kernel a launch uses
+enum HqKind { HQ_QUEUE, HQ_RESIDENT, HQ_ADAPTIVE };
+
 template <class S, bool FAST>
-void* hsq_kernel_ptr(bool resident) {
-  return resident ? (void*)hsr_kernel<S::RW, S::RH, S::T, FAST, S::NT>
-                  : (void*)hsq_kernel<S::RW, S::RH, S::T, FAST, S::NT>;
+const void* hsq_kernel_ptr(HqKind kind) {
+  constexpr int RW = S::RW, RH = S::RH, T = S::T, NT = S::NT;
+  return kind == HQ_RESIDENT ? (const void*)hsr_kernel<RW, RH, T, FAST, NT>
+         : kind == HQ_QUEUE  ? (const void*)hsq_kernel<RW, RH, T, FAST, NT>
+                             : (const void*)hsa_kernel<RW, RH, T, FAST, NT>;
 }
 
 // Opts the chosen kernel into its shared memory and reports how many of its CTAs fit on an SM.
 template <class S>
-cudaError_t hsq_resident(bool fast, bool resident, int* per_sm) {
+cudaError_t hsq_resident(bool fast, HqKind kind, int* per_sm) {
   constexpr int RW = S::RW, RH = S::RH, T = S::T, NT = S::NT;
   using G = HqTile<RW, RH, T>;
   cudaError_t e;
-  if (resident)
+  if (kind == HQ_RESIDENT)
     e = fast ? OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, true, NT>), G::smem(true))
              : OF_SMEM_OPT_IN((hsr_kernel<RW, RH, T, false, NT>), G::smem(false));
-  else
+  else if (kind == HQ_QUEUE)
     e = fast ? OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, true, NT>), G::smem(true))
              : OF_SMEM_OPT_IN((hsq_kernel<RW, RH, T, false, NT>), G::smem(false));
+  else
+    e = fast ? OF_SMEM_OPT_IN((hsa_kernel<RW, RH, T, true, NT>), G::smem(true))
+             : OF_SMEM_OPT_IN((hsa_kernel<RW, RH, T, false, NT>), G::smem(false));
   if (e != cudaSuccess) return e;
-  const void* k = fast ? hsq_kernel_ptr<S, true>(resident) : hsq_kernel_ptr<S, false>(resident);
+  const void* k = fast ? hsq_kernel_ptr<S, true>(kind) : hsq_kernel_ptr<S, false>(kind);
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, NT, G::smem(fast));
 }
 
 template <class S, bool FAST>
-void hsq_launch_as(bool resident, int grid, const HsqPair* pairs, int n, unsigned int tiles_total, int max_passes,
+void hsq_launch_as(HqKind kind, int grid, const HsqPair* pairs, int n, unsigned int tiles_total, int max_passes,
                    unsigned long long* ticket, unsigned int* done, int* status, long long wait_limit, int* err_flag,
-                   cudaStream_t st) {
-  const size_t smem = HqTile<S::RW, S::RH, S::T>::smem(FAST);
-  if (resident)
-    hsr_kernel<S::RW, S::RH, S::T, FAST, S::NT><<<grid, S::NT, smem, st>>>(pairs, n, done, status, wait_limit, err_flag);
+                   unsigned int* arrived, int* mode, cudaStream_t st) {
+  constexpr int RW = S::RW, RH = S::RH, T = S::T, NT = S::NT;
+  const size_t smem = HqTile<RW, RH, T>::smem(FAST);
+  if (kind == HQ_RESIDENT)
+    hsr_kernel<RW, RH, T, FAST, NT><<<grid, NT, smem, st>>>(pairs, n, done, status, wait_limit, err_flag);
+  else if (kind == HQ_QUEUE)
+    hsq_kernel<RW, RH, T, FAST, NT><<<grid, NT, smem, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
+                                                           wait_limit, err_flag);
   else
-    hsq_kernel<S::RW, S::RH, S::T, FAST, S::NT><<<grid, S::NT, smem, st>>>(pairs, n, tiles_total, max_passes, ticket,
-                                                                          done, status, wait_limit, err_flag);
+    hsa_kernel<RW, RH, T, FAST, NT><<<grid, NT, smem, st>>>(pairs, n, tiles_total, max_passes, ticket, done, status,
+                                                           wait_limit, err_flag, arrived, mode);
 }
 }  // namespace
 
@@ -812,12 +887,51 @@ static size_t hsq_max_tiles(const OfHsBatchPair* pairs, int n) {
   return total;
 }
 
+// The launch-control part at the start of the workspace: descriptors, ticket, per-tile
+// counters, error flag, the adaptive schedule's arrival count and mode word.
+struct HsqControl {
+  HsqPair* dpairs;
+  unsigned long long* ticket;
+  unsigned int* done;  // passes (queue) or warp stages (resident) finished, per tile
+  int* err_flag;
+  unsigned int* arrived;
+  int* mode;
+};
+
+static HsqControl hsq_carve_control(Carver& c, const OfHsBatchPair* pairs, int n) {
+  HsqControl k;
+  k.dpairs = c.take<HsqPair>((size_t)n);
+  k.ticket = c.take<unsigned long long>(1);
+  k.done = c.take<unsigned int>(hsq_max_tiles(pairs, n));
+  k.err_flag = c.take<int>(1);
+  k.arrived = c.take<unsigned int>(1);
+  k.mode = c.take<int>(1);
+  return k;
+}
+
+extern "C" int of_hs_batch_schedule(const OfHsBatchPair* pairs, int n, const void* workspace, size_t workspace_bytes,
+                                    int* schedule, void* stream) {
+  OF_REQUIRE(pairs && n > 0 && n <= (1 << 20) && schedule, "of_hs_batch_schedule: bad arguments");
+  Carver c(const_cast<void*>(workspace), workspace_bytes);
+  const HsqControl ctl = hsq_carve_control(c, pairs, n);
+  OF_REQUIRE(workspace && c.ok(), "of_hs_batch_schedule: workspace too small");
+  cudaStream_t st = as_stream(stream);
+  int m = 0;
+  cudaError_t e = cudaMemcpyAsync(&m, ctl.mode, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch_schedule: %s", cudaGetErrorString(e));
+  *schedule = m;
+  return OF_OK;
+}
+
 extern "C" size_t of_hs_batch_workspace_size(const OfHsBatchPair* pairs, int n) {
   if (!pairs || n <= 0) return 0;
   Sizer s;
   s.take<HsqPair>((size_t)n);
   s.take<unsigned long long>(1);
   s.take<unsigned int>(hsq_max_tiles(pairs, n));
+  s.take<int>(1);
+  s.take<unsigned int>(1);
   s.take<int>(1);
   for (int i = 0; i < n; i++) {
     size_t N = (size_t)pairs[i].H * (size_t)pairs[i].pitch;
@@ -847,10 +961,13 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
     return set_error(OF_ERR_WORKSPACE, "of_hs_batch: workspace too small (%zu < %zu)", workspace_bytes, need);
   cudaStream_t st = as_stream(stream);
   Carver c(workspace, workspace_bytes);
-  HsqPair* dpairs = c.take<HsqPair>((size_t)n);
-  unsigned long long* ticket = c.take<unsigned long long>(1);
-  unsigned int* done = c.take<unsigned int>(hsq_max_tiles(pairs, n));  // passes finished, per tile
-  int* err_flag = c.take<int>(1);
+  const HsqControl ctl = hsq_carve_control(c, pairs, n);
+  HsqPair* dpairs = ctl.dpairs;
+  unsigned long long* ticket = ctl.ticket;
+  unsigned int* done = ctl.done;
+  int* err_flag = ctl.err_flag;
+  unsigned int* arrived = ctl.arrived;
+  int* mode = ctl.mode;
   // descriptors are built on the host and written to the workspace by kernels that take
   // them as parameters (no host buffer outlives this call, and a graph capture holds copies)
   HsqPair* hp = new HsqPair[n];
@@ -900,7 +1017,8 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
     if (!hsc_schedulable(fast, hg))
       return set_error(OF_ERR_UNSUPPORTED, "of_hs_batch: the device cannot hold a %d x %d cluster of this kernel",
                        hg.CX, hg.CY);
-    cudaError_t e = hsc_launch(fast, P, hg, status, st);
+    cudaError_t e = cudaMemsetAsync(mode, 0, sizeof(int), st);  // no adaptive decision
+    if (e == cudaSuccess) e = hsc_launch(fast, P, hg, status, st);
     if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: cluster launch: %s", cudaGetErrorString(e));
     return check_launch("of_hs_batch", 1);
   }
@@ -915,43 +1033,48 @@ extern "C" int of_hs_batch(const OfHsBatchPair* pairs, int n, const OfTuning* tu
   delete[] hp;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: descriptor kernel: %s", cudaGetErrorString(e));
-  // ticket, counters and the error flag are contiguous
-  e = cudaMemsetAsync(ticket, 0, (size_t)((char*)(err_flag + 1) - (char*)ticket), st);
+  // ticket, counters, error flag, arrival count and mode word are contiguous
+  e = cudaMemsetAsync(ticket, 0, (size_t)((char*)(mode + 1) - (char*)ticket), st);
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: %s", cudaGetErrorString(e));
   int dev = 0, sms = kNumSMs;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // every CTA must be resident (items wait for items of running CTAs)
-  auto capacity = [&](bool resident, long long* cap) {
+  auto capacity = [&](HqKind kind, long long* cap) {
     int per_sm = 0;
     const cudaError_t rc =
-        hsq_with_shape(shape, [&](auto S) { return hsq_resident<decltype(S)>(fast, resident, &per_sm); });
+        hsq_with_shape(shape, [&](auto S) { return hsq_resident<decltype(S)>(fast, kind, &per_sm); });
     *cap = (long long)sms * per_sm;
     return rc == cudaSuccess && per_sm >= 1;
   };
-  long long cap_r = 0, cap_q = 0;
-  bool resident = false;
-  if (sched != OF_HS_SCHED_QUEUE) {
-    if (!capacity(true, &cap_r)) return set_error(OF_ERR_CUDA, "of_hs_batch: occupancy query failed");
-    resident = (long long)tiles_total <= cap_r;
-    if (sched == OF_HS_SCHED_RESIDENT && !resident)
+  // RESIDENT: one CTA per tile, all of them running at once (refused when the device cannot
+  // hold them); AUTO: the adaptive kernel with one CTA per tile when the device can hold them
+  // (it falls back to the queue itself when they do not all get an SM), else the queue
+  HqKind kind = HQ_QUEUE;
+  long long cap = 0;
+  if (sched == OF_HS_SCHED_RESIDENT || sched == OF_HS_SCHED_AUTO) {
+    const HqKind k = sched == OF_HS_SCHED_RESIDENT ? HQ_RESIDENT : HQ_ADAPTIVE;
+    if (!capacity(k, &cap)) return set_error(OF_ERR_CUDA, "of_hs_batch: occupancy query failed");
+    if ((long long)tiles_total <= cap)
+      kind = k;
+    else if (sched == OF_HS_SCHED_RESIDENT)
       return set_error(OF_ERR_INVALID, "of_hs_batch: %u tiles exceed the %lld resident CTAs of the resident schedule",
-                       tiles_total, cap_r);
+                       tiles_total, cap);
   }
-  long long grid = tiles_total;  // resident: one CTA per tile
-  if (!resident) {
-    if (!capacity(false, &cap_q)) return set_error(OF_ERR_CUDA, "of_hs_batch: occupancy query failed");
-    grid = cap_q < (long long)tiles_total ? cap_q : (long long)tiles_total;  // no more CTAs than items of a pass
+  long long grid = tiles_total;  // resident and adaptive: one CTA per tile
+  if (kind == HQ_QUEUE) {
+    if (!capacity(HQ_QUEUE, &cap)) return set_error(OF_ERR_CUDA, "of_hs_batch: occupancy query failed");
+    grid = cap < (long long)tiles_total ? cap : (long long)tiles_total;  // no more CTAs than items of a pass
   }
   if (grid < 1) grid = 1;
   e = hsq_with_shape(shape, [&](auto S) {
     using Sh = decltype(S);
     if (fast)
-      hsq_launch_as<Sh, true>(resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status,
-                              wait_limit, err_flag, st);
+      hsq_launch_as<Sh, true>(kind, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit,
+                              err_flag, arrived, mode, st);
     else
-      hsq_launch_as<Sh, false>(resident, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status,
-                               wait_limit, err_flag, st);
+      hsq_launch_as<Sh, false>(kind, (int)grid, dpairs, n, tiles_total, max_passes, ticket, done, status, wait_limit,
+                               err_flag, arrived, mode, st);
     return cudaGetLastError();
   });
   if (e != cudaSuccess) return set_error(OF_ERR_CUDA, "of_hs_batch: launch: %s", cudaGetErrorString(e));

@@ -101,6 +101,7 @@ _SIGS = {
     "of_ls_solve_noalloc": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _P, _P, _P], _I),
     "of_ls_solve_mode": ([_P, _P, _P, _P, _I, _I, _I, _F, _I, _D, _I, _P, _P, _P, _Z, _P], _I),
     "of_hs_batch_shape": ([_I, _P, _P, _P], _I),
+    "of_hs_batch_schedule": ([_P, _I, _P, _Z, _P, _P], _I),
     "of_batch_workspace_size": ([_P, _I, _P], _Z),
     "of_batch_run": ([_P, _I, _P, _P, _P, _Z, _P], _I),
     "of_check_finite": ([_P, _I, _I, _I, _P, _I, _P], _I),

@@ -22,7 +22,7 @@ from ._lib import FbPolyConsts, call, lib
 __all__ = [
     "prefilter", "u8_to_f32", "resize", "spline_upsample", "spline_upsample_pair", "warp_pair", "accumulate", "scale", "hs_solve",
     "ls_solve", "lk_dense", "fb_blur", "fb_box5", "fb_polyexp", "fb_update_matrices", "fb_update_flow",
-    "fb_iteration", "workspace", "stream_ptr", "warp_liushen_scatter", "warp_liushen_ofe", "hs_batch", "hs_batch_shapes",
+    "fb_iteration", "workspace", "stream_ptr", "warp_liushen_scatter", "warp_liushen_ofe", "hs_batch", "hs_batch_shapes", "hs_batch_schedule",
 ]
 
 _WS = {}
@@ -311,8 +311,9 @@ def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status
     arithmetic: 'exact' (bit-exact with the reference) or 'fast' (float32 averaging).
     schedule: 'cluster' (one pair of at most 256 x 256 on one thread-block cluster, halos
     through distributed shared memory), 'resident' (one CTA per tile, region kept on chip;
-    needs every tile to get a resident CTA), 'queue' (device work queue) or 'auto' (resident
-    when it fits, else queue).
+    needs every tile to get a resident CTA), 'queue' (device work queue) or 'auto' (one CTA
+    per tile when the device holds them, resident if they all run at once and the queue if
+    not, decided on the device; else the queue; hs_batch_schedule tells which ran).
     Returns the per-pair status words (device int32, bits of ofb200._lib.ST_*)."""
     if arithmetic not in ("exact", "fast"):
         raise ValueError("arithmetic must be 'exact' or 'fast'")
@@ -334,6 +335,27 @@ def hs_batch(pairs, tile_shape: int = 0, wait_limit: int = HS_WAIT_LIMIT, status
     call("of_hs_batch", arr, n, ctypes.byref(tun), ctypes.c_void_p(status.data_ptr()), int(wait_limit), ws, wn,
          stream_ptr())
     return status
+
+
+def _hs_batch_pairs(pairs):
+    from ._lib import OfHsBatchPair
+    arr = (OfHsBatchPair * len(pairs))()
+    for k, (I0, I1, U, V, alpha, niter) in enumerate(pairs):
+        H, W = I0.shape
+        arr[k] = OfHsBatchPair(I0.data_ptr(), I1.data_ptr(), U.data_ptr(), V.data_ptr(), H, W, I0.stride(0),
+                               float(np.float32(alpha)), int(niter))
+    return arr
+
+
+def hs_batch_schedule(pairs) -> str:
+    """Which schedule the last hs_batch(pairs, schedule='auto') on this stream ran: 'resident'
+    or 'queue' as its CTAs decided, or 'auto' when the launch chose statically (an explicit
+    schedule, or more tiles than the device holds CTAs).  Synchronises the stream."""
+    arr = _hs_batch_pairs(pairs)
+    ws, wn = workspace(lib().of_hs_batch_workspace_size(arr, len(pairs)), "hs_batch")
+    out = ctypes.c_int(-1)
+    call("of_hs_batch_schedule", arr, len(pairs), ws, wn, ctypes.byref(out), stream_ptr())
+    return HS_SCHEDULES[out.value]
 
 
 # --------------------------------------------------------------------------- A10/A11

@@ -212,3 +212,89 @@ def test_cluster_schedule_refusals_and_status(cuda_ok):
     b2[10, 20] = float("nan")
     st = int(ops.hs_batch([(a, b2, z.clone(), z.clone(), 21.0, 40)], schedule="cluster").item())
     assert st & _lib.ST_NONFINITE_INPUT and st & _lib.ST_NONFINITE_OUTPUT
+
+
+@pytest.mark.parametrize("shape_index", [3, 4])
+def test_auto_schedule_runs_resident_on_an_idle_device(cuda_ok, shape_index):
+    """The automatic schedule launches one CTA per tile; with the device to itself every CTA
+    runs at once and they choose the resident schedule: bit-exact, and reported as such."""
+    import torch
+    from ofb200 import ops
+    a, b = _pair(torch, 256, 256, 1)
+    z = torch.zeros_like(a)
+    Ur, Vr = _solve_ref(torch, a, b, z, z, 21.0, 600)
+    pairs = [(a, b, z.clone(), z.clone(), 21.0, 600)]
+    st = ops.hs_batch(pairs, tile_shape=shape_index, schedule="auto")
+    assert int(st.item()) == 0
+    assert torch.equal(pairs[0][2], Ur) and torch.equal(pairs[0][3], Vr)
+    assert ops.hs_batch_schedule(pairs) == "resident"
+    ops.hs_batch(pairs, tile_shape=shape_index, schedule="queue")
+    assert ops.hs_batch_schedule(pairs) == "auto"  # an explicit schedule makes no decision
+
+
+_OCCUPY_SRC = rb"""
+extern "C" __global__ void occupy(unsigned long long ns) {
+  extern __shared__ volatile int held[];
+  unsigned long long t0, t = 0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (int k = 0; k < 200000; k++) {  // ends after ns, or after 200000 short sleeps
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 > ns) break;
+    __nanosleep(1000);
+  }
+  if (threadIdx.x == 0) held[0] = (int)(t - t0);
+}
+"""
+
+
+def _occupy(torch, stream, ctas, smem_bytes, ns):
+    """Launches `ctas` CTAs of one warp that each hold `smem_bytes` of shared memory (so an SM
+    takes one) for about `ns` nanoseconds, on `stream`: other kernels find those SMs taken."""
+    from cuda.bindings import driver, nvrtc
+    err, prog = nvrtc.nvrtcCreateProgram(_OCCUPY_SRC, b"occupy.cu", 0, [], [])
+    assert err == nvrtc.nvrtcResult.NVRTC_SUCCESS
+    (err,) = nvrtc.nvrtcCompileProgram(prog, 1, [b"--gpu-architecture=sm_100a"])
+    assert err == nvrtc.nvrtcResult.NVRTC_SUCCESS
+    err, n = nvrtc.nvrtcGetCUBINSize(prog)
+    cubin = b" " * n
+    (err,) = nvrtc.nvrtcGetCUBIN(prog, cubin)
+    assert err == nvrtc.nvrtcResult.NVRTC_SUCCESS
+    err, mod = driver.cuModuleLoadData(cubin)
+    assert err == driver.CUresult.CUDA_SUCCESS
+    err, fn = driver.cuModuleGetFunction(mod, b"occupy")
+    assert err == driver.CUresult.CUDA_SUCCESS
+    (err,) = driver.cuFuncSetAttribute(fn, driver.CUfunction_attribute.CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
+                                       smem_bytes)
+    assert err == driver.CUresult.CUDA_SUCCESS
+    arg = np.array([ns], dtype=np.uint64)
+    params = np.array([arg.ctypes.data], dtype=np.uint64)
+    (err,) = driver.cuLaunchKernel(fn, ctas, 1, 1, 32, 1, 1, smem_bytes, driver.CUstream(stream.cuda_stream),
+                                   params.ctypes.data, 0)
+    assert err == driver.CUresult.CUDA_SUCCESS
+    return mod, arg, params
+
+
+def test_auto_schedule_falls_back_to_the_queue_when_sms_are_taken(cuda_ok):
+    """Another kernel holds all but 20 SMs for a few milliseconds when the automatic launch
+    starts: its 256 CTAs cannot all run, they give up the resident schedule within their
+    bounded poll and run the queue instead, and the result is still bit-exact."""
+    import time
+    import torch
+    from ofb200 import ops
+    a, b = _pair(torch, 256, 256, 1)
+    z = torch.zeros_like(a)
+    Ur, Vr = _solve_ref(torch, a, b, z, z, 21.0, 600)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    side, main = torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.synchronize()
+    held = _occupy(torch, side, sms - 20, 200 * 1024, 5_000_000)
+    time.sleep(0.001)  # the occupying CTAs are on their SMs
+    with torch.cuda.stream(main):
+        pairs = [(a, b, z.clone(), z.clone(), 21.0, 600)]
+        st = ops.hs_batch(pairs, tile_shape=3, schedule="auto")
+        mode = ops.hs_batch_schedule(pairs)
+    torch.cuda.synchronize()
+    del held
+    assert int(st.item()) == 0
+    assert torch.equal(pairs[0][2], Ur) and torch.equal(pairs[0][3], Vr)
+    assert mode == "queue"
