@@ -290,6 +290,13 @@ int of_fb_box5(const float* src, float* dst, int H, int W, int pitch, int kh, vo
 /* polynomialExpansion (:72-133): src H x W -> dst 5H x W. consts: HOST struct. */
 int of_fb_polyexp(const float* src, float* dst, int H, int W, int pitch, const of_fb_poly_consts* consts,
                   void* stream);
+/* gaussianBlur with a 3-tap kernel (kh = 1, reflect-101) followed by polynomialExpansion
+ * (:160-253 then :72-133), as the full-size level of Farneback_PyCL.compute runs them
+ * (src/Farneback_PyCL.py:562-583, no resize between): one launch, the blurred frame never
+ * stored.  Equals of_fb_blur(src, tmp, ..., 1, gk, 1) then of_fb_polyexp(tmp, dst, ...)
+ * bit for bit.  gk: HOST array of 2 taps (centre first); polyN 5 or 7; H, W >= 3. */
+int of_fb_polyexp_blurred(const float* src, float* dst, int H, int W, int pitch, const float* gk,
+                          const of_fb_poly_consts* consts, void* stream);
 /* updateMatrices (:256-348): M from the flow and the two expansions. */
 int of_fb_update_matrices(const float* flowx, const float* flowy, const float* R0, const float* R1, float* M, int H,
                           int W, int pitch, void* stream);

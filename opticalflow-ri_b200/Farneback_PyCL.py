@@ -166,18 +166,24 @@ class Farneback_PyCL(object):
             smoothSize = max(int(round(sigma * 5)) | 1, 3)
             width, height = int(round(size[1] * scale)), int(round(size[0] * scale))
             if prev is None:
-                cx = ops.scale(ops.resize(U, (width, height), bicubic=False), scale)
-                cy = ops.scale(ops.resize(V, (width, height), bicubic=False), scale)
+                cx = _scaled(ops.resize(U, (width, height), bicubic=False), scale)
+                cy = _scaled(ops.resize(V, (width, height), bicubic=False), scale)
             else:
-                cx = ops.scale(ops.resize(prev[0], (width, height), bicubic=False), 1.0 / self.pyrScale)
-                cy = ops.scale(ops.resize(prev[1], (width, height), bicubic=False), 1.0 / self.pyrScale)
+                cx = _scaled(ops.resize(prev[0], (width, height), bicubic=False), 1.0 / self.pyrScale)
+                cy = _scaled(ops.resize(prev[1], (width, height), bicubic=False), 1.0 / self.pyrScale)
             self.setGaussianBlurKernel(smoothSize, sigma)
             gk = self.matrixGKernel[0]
-            # the blurred frame is only read by the expansion: no copy at the full-size level
-            RA = ops.fb_polyexp(ops.resize(ops.fb_blur(im1, gk, 1), (width, height), bicubic=False, copy=False),
-                                self._poly)
-            RB = ops.fb_polyexp(ops.resize(ops.fb_blur(im2, gk, 1), (width, height), bicubic=False, copy=False),
-                                self._poly)
+            if ((height, width) == tuple(size) and len(gk) == 2 and min(size) >= 3 and im1.is_contiguous()
+                    and im2.is_contiguous()):
+                # full-size level, 3-tap blur: blur and expansion in one launch
+                RA = ops.fb_polyexp_blurred(im1, gk, self._poly)
+                RB = ops.fb_polyexp_blurred(im2, gk, self._poly)
+            else:
+                # the blurred frame is only read by the expansion: no copy at the full-size level
+                RA = ops.fb_polyexp(ops.resize(ops.fb_blur(im1, gk, 1), (width, height), bicubic=False, copy=False),
+                                    self._poly)
+                RB = ops.fb_polyexp(ops.resize(ops.fb_blur(im2, gk, 1), (width, height), bicubic=False, copy=False),
+                                    self._poly)
             M = ops.fb_update_matrices(cx, cy, RA, RB)
             if self.useGaussianFilter:
                 self.setGaussianBlurKernel(self.windowSize, self.windowSize / 2 * 0.3)
@@ -224,6 +230,12 @@ class Farneback_PyCL(object):
 
     def getGenericPyramidalDefaults(self):
         return {'warping': False, 'scaling': True}
+
+
+def _scaled(t, s):
+    """t * s in float32 (src/Farneback_PyCL.py:530-539); a factor of exactly 1 (the
+    full-size level) changes no value, so the multiplication is skipped there."""
+    return t if float(np.float32(s)) == 1.0 else ops.scale(t, s)
 
 
 def torch_empty_like(t):

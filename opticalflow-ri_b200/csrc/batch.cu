@@ -117,14 +117,25 @@ int farneback(Arena& A, const OfFbParams& fb, const Plane& im1, const Plane& im2
     Plane rx = new_plane(A, h, w), ry = new_plane(A, h, w);
     if (resize_to(A, sx, rx, OF_FILTER_BILINEAR, st) || resize_to(A, sy, ry, OF_FILTER_BILINEAR, st))
       return OF_ERR_CUDA;
-    CALL(of_scale(rx.p, nx.p, s, h, w, nx.pitch, st));
-    CALL(of_scale(ry.p, ny.p, s, h, w, ny.pitch, st));
-    cx = nx;
-    cy = ny;
+    if (s != 1.0f) {  // x * 1 is x: the full-size level keeps the resized copies
+      CALL(of_scale(rx.p, nx.p, s, h, w, nx.pitch, st));
+      CALL(of_scale(ry.p, ny.p, s, h, w, ny.pitch, st));
+      cx = nx;
+      cy = ny;
+    } else {
+      cx = rx;
+      cy = ry;
+    }
     Plane RA = new_plane(A, 5 * h, w), RB = new_plane(A, 5 * h, w);
     RA.H = RB.H = h;
+    const bool fused = h == Hs && w == Ws && fb.level_kh[k] == 1 && (fb.poly.polyN == 5 || fb.poly.polyN == 7) &&
+                       h >= 3 && w >= 3 && im1.pitch == RA.pitch && im2.pitch == RA.pitch;
     for (int f = 0; f < 2; f++) {
       const Plane& src = f ? im2 : im1;
+      if (fused) {  // blur and expansion in one launch at the full-size level
+        CALL(of_fb_polyexp_blurred(src.p, (f ? RB : RA).p, h, w, RA.pitch, fb.level_taps[k], &fb.poly, st));
+        continue;
+      }
       Plane bl = new_plane(A, Hs, Ws);
       CALL(of_fb_blur(src.p, bl.p, Hs, Ws, bl.pitch, 1, fb.level_taps[k], fb.level_kh[k], st));
       Plane lv = bl;

@@ -175,21 +175,69 @@ __global__ void __launch_bounds__(FBP_T) fb_polyexp_kernel(const float* __restri
 // outputs of one row with a register window along the row.  The arithmetic of every
 // output is the row kernel's, in the same order.  The moment rows are padded by one float
 // per 8 columns, so the 8-column segments of a warp's lanes fall in distinct banks.
+//
+// BLUR = true fuses the level's 3-tap frame blur in front (gaussianBlur with kh = 1 and
+// reflect-101 borders, :160-253, then the expansion of the blurred frame, as at the
+// pyramid's full-size level where no resize lies between them).  The CTA first computes
+// the vertical blur V of its rows for the CW + 2 columns around its window into shared
+// memory (the storage the moments use later), then each thread forms the blurred samples
+// of its column from V and its two reflect-101 neighbours.  Every blurred value is the
+// blur kernel's, operation for operation, so the result equals of_fb_blur followed by
+// of_fb_polyexp.  Needs H, W >= 3.
 constexpr int FBQ_OW = 240, FBQ_R = 8, FBQ_SEG = 8;
 __device__ __forceinline__ int fbq_col(int c) { return c + (c >> 3); }
-template <int N>
+template <int N, bool BLUR>
 __global__ void __launch_bounds__(256) fb_polyexp_tile_kernel(const float* __restrict__ src, float* __restrict__ dst,
-                                                              int H, int W, int pitch, FbPoly P, int vec) {
+                                                              int H, int W, int pitch, FbPoly P, int vec, float bg0,
+                                                              float bg1) {
   constexpr int CW = FBQ_OW + 2 * N;          // columns that get vertical moments
   constexpr int CWP = CW + (CW >> 3) + 1;     // padded row length
   constexpr int WIN = FBQ_SEG + 2 * N;
+  constexpr int NR = FBQ_R + 2 * N;           // rows of the vertical window
+  static_assert(CW + 2 <= 256 && NR * 256 <= 3 * FBQ_R * CWP, "blur rows must fit the moment storage");
   __shared__ float mom[3][FBQ_R][CWP];
   const int x0 = blockIdx.x * FBQ_OW, y0 = blockIdx.y * FBQ_R, tx = threadIdx.x;
-  if (tx < CW) {
-    const int xw = clampi(x0 - N + tx, 0, W - 1);
-    float c[FBQ_R + 2 * N];
+  float c[NR];
+  if (BLUR) {
+    // V(y, x) = g1 (src[y-1] + src[y+1]) + g0 src[y] at the window's clamped rows y, for
+    // the columns clamp(x0 - N - 1 + j), j <= CW + 1
+    float (*vs)[256] = reinterpret_cast<float (*)[256]>(&mom[0][0][0]);
+    if (tx < CW + 2) {
+      const float* col = src + clampi(x0 - N - 1 + tx, 0, W - 1);
+      if (y0 - N - 1 >= 0 && y0 + FBQ_R + N < H) {  // rows y0-N-1 .. y0+R+N, all inside
+        float r[NR + 2];
 #pragma unroll
-    for (int q = 0; q < FBQ_R + 2 * N; q++) c[q] = src[(size_t)clampi(y0 - N + q, 0, H - 1) * pitch + xw];
+        for (int q = 0; q < NR + 2; q++) r[q] = col[(size_t)(y0 - N - 1 + q) * pitch];
+#pragma unroll
+        for (int q = 0; q < NR; q++) vs[q][tx] = __fmaf_rn(__fadd_rn(r[q], r[q + 2]), bg1, __fmul_rn(r[q + 1], bg0));
+      } else {
+#pragma unroll
+        for (int q = 0; q < NR; q++) {
+          const int y = clampi(y0 - N + q, 0, H - 1);
+          const float up = col[(size_t)fb_row(y - 1, H) * pitch], mid = col[(size_t)y * pitch],
+                      dn = col[(size_t)fb_row(y + 1, H) * pitch];
+          vs[q][tx] = __fmaf_rn(__fadd_rn(up, dn), bg1, __fmul_rn(mid, bg0));
+        }
+      }
+    }
+    __syncthreads();
+    if (tx < CW) {
+      // column u = x0 - N + tx, clamped to xw; V's column j holds clamp(x0 - N - 1 + j)
+      const int u = x0 - N + tx;
+      int jl = tx, jr = tx + 2;  // xw - 1 and xw + 1 inside the image
+      if (u <= 0) jl = jr = N + 2 - x0;           // xw = 0: both reflect-101 neighbours are column 1
+      else if (u >= W - 1) jl = jr = W - 1 - x0 + N;  // xw = W - 1: both are column W - 2
+#pragma unroll
+      for (int q = 0; q < NR; q++) c[q] = __fmaf_rn(__fadd_rn(vs[q][jl], vs[q][jr]), bg1, __fmul_rn(vs[q][tx + 1], bg0));
+    }
+    __syncthreads();  // V is overwritten by the moments below
+  }
+  if (tx < CW) {
+    if (!BLUR) {
+      const int xw = clampi(x0 - N + tx, 0, W - 1);
+#pragma unroll
+      for (int q = 0; q < NR; q++) c[q] = src[(size_t)clampi(y0 - N + q, 0, H - 1) * pitch + xw];
+    }
 #pragma unroll
     for (int r = 0; r < FBQ_R; r++) {
       float r0 = __fmul_rn(c[r + N], P.g[0]), r1 = 0.f, r2 = 0.f;
@@ -622,14 +670,36 @@ extern "C" int of_fb_polyexp(const float* src, float* dst, int H, int W, int pit
     const int vec = (pitch % 4) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
     dim3 grid((W + FBQ_OW - 1) / FBQ_OW, (H + FBQ_R - 1) / FBQ_R);
     if (P.n == 7)
-      fb_polyexp_tile_kernel<7><<<grid, 256, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P, vec);
+      fb_polyexp_tile_kernel<7, false><<<grid, 256, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P, vec, 0.f, 0.f);
     else
-      fb_polyexp_tile_kernel<5><<<grid, 256, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P, vec);
+      fb_polyexp_tile_kernel<5, false><<<grid, 256, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P, vec, 0.f, 0.f);
     return check_launch("of_fb_polyexp");
   }
   dim3 grid((W + (FBP_T - 2 * P.n) - 1) / (FBP_T - 2 * P.n), H);
   fb_polyexp_kernel<<<grid, FBP_T, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P);
   return check_launch("of_fb_polyexp");
+}
+
+extern "C" int of_fb_polyexp_blurred(const float* src, float* dst, int H, int W, int pitch, const float* gk,
+                                     const of_fb_poly_consts* c, void* stream) {
+  OF_REQUIRE(!bad_plane(src, H, W, pitch) && dst && c && gk, "of_fb_polyexp_blurred: bad plane");
+  OF_REQUIRE(c->polyN == 5 || c->polyN == 7, "of_fb_polyexp_blurred: polyN must be 5 or 7");
+  OF_REQUIRE(H >= 3 && W >= 3, "of_fb_polyexp_blurred: the frame must be at least 3 x 3");
+  FbPoly P{};
+  P.n = c->polyN;
+  for (int k = 0; k <= P.n; k++) {
+    P.g[k] = c->g[k];
+    P.xg[k] = c->xg[k];
+    P.xxg[k] = c->xxg[k];
+  }
+  for (int k = 0; k < 4; k++) P.ig[k] = c->ig[k];
+  const int vec = (pitch % 4) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
+  dim3 grid((W + FBQ_OW - 1) / FBQ_OW, (H + FBQ_R - 1) / FBQ_R);
+  if (P.n == 7)
+    fb_polyexp_tile_kernel<7, true><<<grid, 256, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P, vec, gk[0], gk[1]);
+  else
+    fb_polyexp_tile_kernel<5, true><<<grid, 256, 0, as_stream(stream)>>>(src, dst, H, W, pitch, P, vec, gk[0], gk[1]);
+  return check_launch("of_fb_polyexp_blurred");
 }
 
 extern "C" int of_fb_update_matrices(const float* flowx, const float* flowy, const float* R0, const float* R1, float* M,

@@ -35,29 +35,45 @@ __device__ __forceinline__ float key2f(unsigned int k) {
   return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
-__global__ void ls_max_kernel(const float* __restrict__ a, const float* __restrict__ b, int H, int W, int pitch,
-                              unsigned int* keys) {
+// The largest value of each frame (as order-preserving keys): one CTA per row, rows
+// strided over the grid, float4 loads when the rows are 16-byte aligned.  max is exact and
+// order-free, so the traversal does not change the result.
+__global__ void __launch_bounds__(256) ls_max_kernel(const float* __restrict__ a, const float* __restrict__ b, int H,
+                                                     int W, int pitch, int vec, unsigned int* keys) {
   unsigned int ka = 0, kb = 0;
-  for (int y = blockIdx.y; y < H; y += gridDim.y)
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < W; x += gridDim.x * blockDim.x) {
-      size_t i = (size_t)y * pitch + x;
-      ka = max(ka, f2key(a[i]));
-      kb = max(kb, f2key(b[i]));
+  for (int y = blockIdx.x; y < H; y += gridDim.x) {
+    const float* ra = a + (size_t)y * pitch;
+    const float* rb = b + (size_t)y * pitch;
+    int x = threadIdx.x;
+    if (vec) {
+      const int W4 = W >> 2;
+      for (; x < W4; x += blockDim.x) {
+        const float4 va = __ldg(reinterpret_cast<const float4*>(ra) + x);
+        const float4 vb = __ldg(reinterpret_cast<const float4*>(rb) + x);
+        ka = max(ka, max(max(f2key(va.x), f2key(va.y)), max(f2key(va.z), f2key(va.w))));
+        kb = max(kb, max(max(f2key(vb.x), f2key(vb.y)), max(f2key(vb.z), f2key(vb.w))));
+      }
+      x = 4 * W4 + threadIdx.x;
     }
+    for (; x < W; x += blockDim.x) {
+      ka = max(ka, f2key(ra[x]));
+      kb = max(kb, f2key(rb[x]));
+    }
+  }
   for (int o = 16; o > 0; o >>= 1) {
     ka = max(ka, __shfl_down_sync(0xffffffffu, ka, o));
     kb = max(kb, __shfl_down_sync(0xffffffffu, kb, o));
   }
-  __shared__ unsigned int ra[8], rb[8];
+  __shared__ unsigned int sa[8], sb[8];
   if ((threadIdx.x & 31) == 0) {
-    ra[threadIdx.x >> 5] = ka;
-    rb[threadIdx.x >> 5] = kb;
+    sa[threadIdx.x >> 5] = ka;
+    sb[threadIdx.x >> 5] = kb;
   }
   __syncthreads();
   if (threadIdx.x == 0) {  // one atomic per block
     for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
-      ka = max(ka, ra[w]);
-      kb = max(kb, rb[w]);
+      ka = max(ka, sa[w]);
+      kb = max(kb, sb[w]);
     }
     atomicMax(keys, ka);
     atomicMax(keys + 1, kb);
@@ -957,8 +973,10 @@ extern "C" int of_ls_solve_mode(const float* I0, const float* I1, float* U, floa
   }
   // control block, flags, counters, redo counts and sums are contiguous: one memset
   cudaMemsetAsync(ctrl, 0, (size_t)((char*)(ss + 2 * (size_t)(maxnum > 0 ? maxnum : 1)) - (char*)ctrl), st);
-  dim3 mg((W + 255) / 256 < 2 ? (W + 255) / 256 : 2, H < 148 ? H : 148);
-  ls_max_kernel<<<mg, 256, 0, st>>>(I0, I1, H, W, pitch, ctrl->maxkey);
+  {
+    const int vec = (pitch % 4) == 0 && ((reinterpret_cast<uintptr_t>(I0) | reinterpret_cast<uintptr_t>(I1)) & 15) == 0;
+    ls_max_kernel<<<H < 4 * 148 ? H : 4 * 148, 256, 0, st>>>(I0, I1, H, W, pitch, vec, ctrl->maxkey);
+  }
   dim3 rg((W + 255) / 256, H);
   ls_prep_kernel<<<dim3((W + 31) / 32, (H + 7) / 8), 256, 0, st>>>(I0, I1, pitch, ctrl->maxkey, V, U, coef, N,
                                                                  ub[0], vb[0], H, W, P, h);

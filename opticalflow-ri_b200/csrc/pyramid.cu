@@ -79,19 +79,23 @@ __global__ void resize_coeff_kernel(int inSize, int outSize, int bicubic, int ks
 
 // Fused passes for kernels of up to RZ_MAXK taps: a CTA computes the weights it needs into
 // shared memory (the horizontal pass: its 128 output columns; the vertical pass: its
-// RZ_RB output rows) and applies them to a band of RZ_RB rows, so a resize is two
-// launches, not four.  Same weights and sums as the table path.
-constexpr int RZ_MAXK = 32, RZ_RB = 16;
+// `rb` output rows) and applies them to a band of rb <= RZ_RB rows, so a resize is two
+// launches, not four.  Same weights and sums as the table path.  RZ_MAXK = 40 covers
+// Pillow's bicubic support up to a factor of 9.5 (33 taps at 8x: 1024 -> 128) and its
+// bilinear support up to 19x.  The band height is picked per launch (rz_band) so that
+// small outputs still spread over the SMs.
+constexpr int RZ_MAXK = 40, RZ_RB = 16;
 __global__ void __launch_bounds__(128) resize_hf_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst,
-                                                        int dp, int Hs, int Ws, int Wd, int bicubic, int ksize) {
+                                                        int dp, int Hs, int Ws, int Wd, int bicubic, int ksize,
+                                                        int rb) {
   __shared__ double kk[RZ_MAXK * 128];
   const int xx = blockIdx.x * 128 + threadIdx.x;
   if (xx >= Wd) return;  // no barrier below: every thread uses only its own column's weights
   int xmin, xcnt;
   resize_coeff_at(Ws, Wd, bicubic, ksize, xx, &xmin, &xcnt, kk + threadIdx.x, 128);
   const double* k = kk + threadIdx.x;
-  const int y1 = min(Hs, (blockIdx.y + 1) * RZ_RB);
-  for (int y = blockIdx.y * RZ_RB; y < y1; y++) {
+  const int y1 = min(Hs, (blockIdx.y + 1) * rb);
+  for (int y = blockIdx.y * rb; y < y1; y++) {
     const float* row = src + (size_t)y * sp + xmin;
     double ss = 0.0;
     for (int x = 0; x < xcnt; x++) ss = __dadd_rn(ss, __dmul_rn((double)row[x], k[x * 128]));
@@ -100,17 +104,18 @@ __global__ void __launch_bounds__(128) resize_hf_kernel(const float* __restrict_
 }
 
 __global__ void __launch_bounds__(128) resize_vf_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst,
-                                                        int dp, int Hs, int Hd, int Wd, int bicubic, int ksize) {
+                                                        int dp, int Hs, int Hd, int Wd, int bicubic, int ksize,
+                                                        int rb) {
   __shared__ double kk[RZ_RB * RZ_MAXK];
   __shared__ int bnd[RZ_RB][2];
-  const int yy0 = blockIdx.y * RZ_RB;
-  if (threadIdx.x < RZ_RB && yy0 + threadIdx.x < Hd)
+  const int yy0 = blockIdx.y * rb;
+  if (threadIdx.x < rb && yy0 + threadIdx.x < Hd)
     resize_coeff_at(Hs, Hd, bicubic, ksize, yy0 + threadIdx.x, &bnd[threadIdx.x][0], &bnd[threadIdx.x][1],
                     kk + threadIdx.x * RZ_MAXK, 1);
   __syncthreads();
   const int x = blockIdx.x * 128 + threadIdx.x;
   if (x >= Wd) return;
-  const int n = min(RZ_RB, Hd - yy0);
+  const int n = min(rb, Hd - yy0);
   for (int r = 0; r < n; r++) {
     const int ymin = bnd[r][0], ymax = bnd[r][1];
     const double* k = kk + r * RZ_MAXK;
@@ -118,6 +123,14 @@ __global__ void __launch_bounds__(128) resize_vf_kernel(const float* __restrict_
     for (int y = 0; y < ymax; y++) ss = __dadd_rn(ss, __dmul_rn((double)src[(size_t)(y + ymin) * sp + x], k[y]));
     dst[(size_t)(yy0 + r) * dp + x] = (float)ss;
   }
+}
+
+// Rows per CTA of a fused pass: RZ_RB, halved while the grid would cover fewer than two
+// CTAs per SM of a 148-SM part (a 128 x 128 output has one column block).
+static int rz_band(int col_blocks, int rows) {
+  int rb = RZ_RB;
+  while (rb > 1 && (long long)col_blocks * ((rows + rb - 1) / rb) < 2 * 148) rb >>= 1;
+  return rb;
 }
 
 __global__ void resize_h_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst, int dp, int Hs, int Wd,
@@ -599,12 +612,16 @@ extern "C" int of_resize(const float* src, int Hs, int Ws, int src_pitch, float*
   if (kh <= RZ_MAXK && kv <= RZ_MAXK) {  // the fused passes
     float* mid = need_v ? tmp : dst;
     const int mp = need_v ? Wd : dst_pitch;
-    if (need_h)
-      resize_hf_kernel<<<dim3((Wd + 127) / 128, (Hs + RZ_RB - 1) / RZ_RB), 128, 0, st>>>(src, src_pitch, mid, mp, Hs,
-                                                                                          Ws, Wd, bic, kh);
-    if (need_v)
-      resize_vf_kernel<<<dim3((Wd + 127) / 128, (Hd + RZ_RB - 1) / RZ_RB), 128, 0, st>>>(
-          need_h ? tmp : src, need_h ? Wd : src_pitch, dst, dst_pitch, Hs, Hd, Wd, bic, kv);
+    const int cb = (Wd + 127) / 128;
+    if (need_h) {
+      const int rb = rz_band(cb, Hs);
+      resize_hf_kernel<<<dim3(cb, (Hs + rb - 1) / rb), 128, 0, st>>>(src, src_pitch, mid, mp, Hs, Ws, Wd, bic, kh, rb);
+    }
+    if (need_v) {
+      const int rb = rz_band(cb, Hd);
+      resize_vf_kernel<<<dim3(cb, (Hd + rb - 1) / rb), 128, 0, st>>>(need_h ? tmp : src, need_h ? Wd : src_pitch, dst,
+                                                                     dst_pitch, Hs, Hd, Wd, bic, kv, rb);
+    }
     return check_launch("of_resize", (int)need_h + (int)need_v);
   }
   const float* cur = src;

@@ -130,6 +130,7 @@ _SIGS = {
     "of_fb_blur": ([_P, _P, _I, _I, _I, _I, _P, _I, _P], _I),
     "of_fb_box5": ([_P, _P, _I, _I, _I, _I, _P], _I),
     "of_fb_polyexp": ([_P, _P, _I, _I, _I, ctypes.POINTER(FbPolyConsts), _P], _I),
+    "of_fb_polyexp_blurred": ([_P, _P, _I, _I, _I, _P, ctypes.POINTER(FbPolyConsts), _P], _I),
     "of_fb_update_matrices": ([_P, _P, _P, _P, _P, _I, _I, _I, _P], _I),
     "of_fb_update_flow": ([_P, _P, _P, _I, _I, _I, _P], _I),
     "of_fb_iteration": ([_P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _I, _I, _P], _I),

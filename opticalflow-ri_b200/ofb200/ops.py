@@ -21,7 +21,7 @@ from ._lib import FbPolyConsts, call, lib
 
 __all__ = [
     "prefilter", "u8_to_f32", "resize", "spline_upsample", "spline_upsample_pair", "warp_pair", "accumulate", "scale", "hs_solve",
-    "ls_solve", "lk_dense", "fb_blur", "fb_box5", "fb_polyexp", "fb_update_matrices", "fb_update_flow",
+    "ls_solve", "lk_dense", "fb_blur", "fb_box5", "fb_polyexp", "fb_polyexp_blurred", "fb_update_matrices", "fb_update_flow",
     "fb_iteration", "workspace", "stream_ptr", "warp_liushen_scatter", "warp_liushen_ofe", "hs_batch", "hs_batch_shapes", "hs_batch_schedule",
 ]
 
@@ -410,6 +410,20 @@ def fb_polyexp(src: torch.Tensor, consts: FbPolyConsts, out=None) -> torch.Tenso
     if out.stride(0) != p:
         raise ValueError("fb_polyexp: out must share the source pitch")
     call("of_fb_polyexp", s, _plane(out, "fb_polyexp.out")[0], H, W, p, ctypes.byref(consts), stream_ptr())
+    return out
+
+
+def fb_polyexp_blurred(src: torch.Tensor, half_kernel, consts: FbPolyConsts, out=None) -> torch.Tensor:
+    """fb_polyexp(fb_blur(src, half_kernel, 1)) for a 3-tap blur, in one launch."""
+    hk = np.ascontiguousarray(half_kernel, dtype=np.float32)
+    if hk.shape != (2,):
+        raise ValueError("fb_polyexp_blurred: the blur must have 3 taps (half kernel of 2)")
+    s, H, W, p = _plane(src, "fb_polyexp_blurred.src")
+    out = torch.empty((5 * H, W), dtype=torch.float32, device=src.device) if out is None else out
+    if out.stride(0) != p:
+        raise ValueError("fb_polyexp_blurred: out must share the source pitch")
+    call("of_fb_polyexp_blurred", s, _plane(out, "fb_polyexp_blurred.out")[0], H, W, p, hk.ctypes.data,
+         ctypes.byref(consts), stream_ptr())
     return out
 
 

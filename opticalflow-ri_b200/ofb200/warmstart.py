@@ -422,17 +422,27 @@ class LearnedBatch:
         cur = torch.cuda.current_stream()
         if self._streams is None:
             self._streams = [torch.cuda.Stream() for _ in range(self.nstreams)]
-        frames = [(_as_f32(A), _as_f32(B)) for A, B in frames]  # uint8 / uint16 frames converted in the graph
-        out = None
-        if self.start == "cnn":
-            b = self.net.buffers(self.n, self.size // self.ll.factor)
-            for i, (A, B) in enumerate(frames):
-                self.ll.pack(b, i, A, B)
-            out = self.net.forward(b)
-        errs = torch.empty(self.n, dtype=torch.float64, device=frames[0][0].device)
-        res = [None] * self.n
+        # per pair, on its stream: uint8 / uint16 frames converted inside the graph, and the
+        # network's input (the frames resized to its level) packed into the batch
+        b = self.net.buffers(self.n, self.size // self.ll.factor) if self.start == "cnn" else None
         for s in self._streams:
             s.wait_stream(cur)
+        conv = [None] * self.n
+        for i, (A, B) in enumerate(frames):
+            with torch.cuda.stream(self._streams[i % self.nstreams]):
+                conv[i] = (_as_f32(A), _as_f32(B))
+                if b is not None:
+                    self.ll.pack(b, i, *conv[i])
+        frames = conv
+        out = None
+        if b is not None:
+            for s in self._streams:
+                cur.wait_stream(s)
+            out = self.net.forward(b)
+            for s in self._streams:
+                s.wait_stream(cur)
+        errs = torch.empty(self.n, dtype=torch.float64, device=frames[0][0].device)
+        res = [None] * self.n
         for i, (A, B) in enumerate(frames):
             with torch.cuda.stream(self._streams[i % self.nstreams]):
                 if out is not None:

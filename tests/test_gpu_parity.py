@@ -86,7 +86,8 @@ def test_resize_golden(torch_cuda):
 
 @pytest.mark.parametrize("src,dst", [((1024, 1024), (512, 512)), ((2048, 2048), (1024, 1024)), ((128, 96), (64, 48)),
                                      ((37, 41), (19, 20)), ((64, 64), (32, 64)), ((40, 128), (40, 64)),
-                                     ((64, 96), (128, 150)), ((512, 512), (16, 16))])
+                                     ((64, 96), (128, 150)), ((512, 512), (16, 16)), ((1024, 1024), (128, 128)),
+                                     ((1000, 760), (100, 95)), ((96, 1024), (12, 120))])
 @pytest.mark.parametrize("bicubic", [True, False])
 def test_resize_vs_oracle(torch_cuda, src, dst, bicubic):
     from ofb200 import ops
@@ -331,6 +332,25 @@ def test_fb_polyexp_shapes_vs_oracle(torch_cuda, shape, polyN, sigma):
     g, xg, xxg, ig = O.farneback_poly_consts(polyN, sigma)
     R = ops.fb_polyexp(dev(torch_cuda, a), ops.poly_consts(g, xg, xxg, ig, polyN))
     assert np.array_equal(host(R), O.fb_polyexp(a, polyN, sigma))
+
+
+@pytest.mark.parametrize("shape,polyN,sigma", [((37, 250), 7, 1.5), ((130, 491), 7, 1.5), ((257, 480), 5, 1.1),
+                                               ((9, 1000), 5, 1.1), ((3, 17), 7, 1.5), ((3, 3), 5, 1.1),
+                                               ((24, 254), 7, 1.5), ((25, 481), 7, 1.5), ((1024, 1024), 7, 1.5)])
+def test_fb_polyexp_blurred_vs_two_launches(torch_cuda, shape, polyN, sigma):
+    """Blur (3 taps, reflect-101) fused into the expansion equals the blur kernel followed
+    by the expansion kernel, and the oracle's blur then expansion, bit for bit: tiles whose
+    rows lie inside the image and border tiles, the left, right, top and bottom reflections,
+    widths at and beside the 240-column tile edge."""
+    from ofb200 import ops
+    a = rng(shape[0] * 5 + shape[1]).uniform(0, 255, shape).astype(np.float32)
+    hk = O.fb_half_kernel(3, 0.0)
+    g, xg, xxg, ig = O.farneback_poly_consts(polyN, sigma)
+    pc = ops.poly_consts(g, xg, xxg, ig, polyN)
+    d = dev(torch_cuda, a)
+    fused = host(ops.fb_polyexp_blurred(d, hk, pc))
+    assert np.array_equal(fused, host(ops.fb_polyexp(ops.fb_blur(d, hk), pc)))
+    assert np.array_equal(fused, O.fb_polyexp(O.fb_blur(a, hk), polyN, sigma))
 
 
 @pytest.mark.parametrize("kw", [{}, {"useGaussian": False}, {"polyN": 5, "polySigma": 1.1},
