@@ -76,7 +76,8 @@ def parse():
     p.add_argument("--learned-pairs", type=int, default=64, help="pairs per step of the learned arm (batch)")
     p.add_argument("--epe-pairs", type=int, default=32, help="distinct held-out pairs for the endpoint errors")
     p.add_argument("--batch-pairs", type=int, default=256, help="--mode batch: pairs in the manifest")
-    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn", "fb", "e2e", "hs", "lk"],
+    p.add_argument("--mode", default="pipeline", choices=["pipeline", "ls", "batch", "cnn", "fb", "e2e", "hs", "lk",
+                                                          "learned"],
                    help="ls: only the Liu-Shen solve of one pair, --steps times (for profiling)")
     return p.parse_args()
 
@@ -225,6 +226,31 @@ def run_fb_only(args):
     px = args.size * args.size
     print(json.dumps({"mode": "fb", "size": args.size, "ms": float(np.mean(ms)),
                       "gbs_88B_per_px": 88.0 * px / (float(np.mean(ms)) * 1e-3) / 1e9}))
+
+
+def run_learned_only(args):
+    """The learned warm-start step alone (profiling): --learned-pairs pairs at --size through
+    one LearnedBatch graph on --streams streams (the packaged network, its calibrated
+    Farneback iterations and sweeps), four seeded pairs cycled; --warmup + --steps replays,
+    CUDA events, no fallback pass."""
+    import torch
+    from ofb200.warmstart import LearnedBatch, load_trained
+    net, meta = load_trained(**({"path": args.learned_weights} if args.learned_weights else {}), device="cuda")
+    fr = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b, _, _ in make_pairs(4, args.size)]
+    frames = [fr[i % len(fr)] for i in range(args.learned_pairs)]
+    lb = LearnedBatch(net, meta, args.learned_pairs, args.size, streams=args.streams)
+    for _ in range(args.warmup):
+        lb.run(frames)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        lb.run(frames)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / max(1, args.steps)
+    print(json.dumps({"mode": "learned", "size": args.size, "pairs": args.learned_pairs, "ms_per_step": ms,
+                      "pairs_per_s": args.learned_pairs / (ms * 1e-3)}))
 
 
 def run_cnn(args):
@@ -1108,6 +1134,9 @@ def main():
         return
     if args.mode == "lk":
         run_lk_only(args)
+        return
+    if args.mode == "learned":
+        run_learned_only(args)
         return
     if args.mode == "batch":
         if world > 1:

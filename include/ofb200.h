@@ -83,6 +83,17 @@ int of_u16_to_f32(const uint16_t* src, int src_pitch, float* dst, int dst_pitch,
 size_t of_resize_workspace_size(int Hs, int Ws, int Hd, int Wd, int filter);
 int of_resize(const float* src, int Hs, int Ws, int src_pitch, float* dst, int Hd, int Wd, int dst_pitch, int filter,
               void* workspace, size_t workspace_bytes, void* stream);
+/* The same resize from weight tables the caller computed once per (size, filter) and keeps
+ * (same results bit for bit): of_resize_table fills one axis's table (in -> out samples,
+ * of_resize_table_size bytes, DEVICE memory); of_resize_tabled takes the horizontal
+ * (Ws -> Wd) and vertical (Hs -> Hd) tables (either may be NULL when that axis keeps its
+ * size) and, when both axes change, a workspace of Hs * Wd floats.  Worth it for strong
+ * downscales, whose many taps per output make the weights the dominant cost. */
+size_t of_resize_table_size(int in, int out, int filter);
+int of_resize_table(int in, int out, int filter, void* table, size_t table_bytes, void* stream);
+int of_resize_tabled(const float* src, int Hs, int Ws, int src_pitch, float* dst, int Hd, int Wd, int dst_pitch,
+                     int filter, const void* table_h, const void* table_v, void* workspace, size_t workspace_bytes,
+                     void* stream);
 
 /* ---------------------------------------------------------------------------------
  * A3 flow upsample — replaces the RectBivariateSpline branch of updateNextPyramidalLevel

@@ -143,8 +143,10 @@ class Farneback_PyCL(object):
         raise Exception('Fast Pyramids not supported yet... Check ocl_pyrDown and ocl_pyrUp, pyrDown, pyrUp in OpenCV')
 
     # ---------------------------------------------------------------- driver
-    def _compute_dev(self, im1, im2, U, V):
-        """src/Farneback_PyCL.py:461-603 on device tensors; returns (U, V, 'Unknown')."""
+    def _compute_dev(self, im1, im2, U, V, consume_init=False):
+        """src/Farneback_PyCL.py:461-603 on device tensors; returns (U, V, 'Unknown').
+        consume_init: the caller hands U, V over (it does not read them afterwards), so a
+        full-size first level iterates on them in place instead of on copies."""
         assert self.polyN == 5 or self.polyN == 7
         assert im1.shape == im2.shape and self.pyrScale < 1
         assert U.shape == im1.shape and V.shape == im1.shape
@@ -166,8 +168,8 @@ class Farneback_PyCL(object):
             smoothSize = max(int(round(sigma * 5)) | 1, 3)
             width, height = int(round(size[1] * scale)), int(round(size[0] * scale))
             if prev is None:
-                cx = _scaled(ops.resize(U, (width, height), bicubic=False), scale)
-                cy = _scaled(ops.resize(V, (width, height), bicubic=False), scale)
+                cx = _scaled(ops.resize(U, (width, height), bicubic=False, copy=not consume_init), scale)
+                cy = _scaled(ops.resize(V, (width, height), bicubic=False, copy=not consume_init), scale)
             else:
                 cx = _scaled(ops.resize(prev[0], (width, height), bicubic=False), 1.0 / self.pyrScale)
                 cy = _scaled(ops.resize(prev[1], (width, height), bicubic=False), 1.0 / self.pyrScale)

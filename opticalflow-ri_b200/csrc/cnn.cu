@@ -515,6 +515,58 @@ __global__ void avgpool2_kernel(const bf16* __restrict__ x, int xct, int xco, in
   y[(((size_t)img * h + oy) * w + ox) * yct + yco + c] = __float2bfloat16_rn(__fmul_rn(s, 0.25f));
 }
 
+// The same two kernels on 8 channels (16 bytes) per thread, one output row per blockIdx.y
+// (image * rows + row) and 32-bit index arithmetic: used when the channel counts, channel
+// offsets and row strides are multiples of 8 and the bases 16-byte aligned (every layer of
+// the network).  Per channel the arithmetic is the scalar kernels'.
+__device__ __forceinline__ float2 bf2f(unsigned int u) {
+  return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
+}
+__device__ __forceinline__ unsigned int f2bf(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const unsigned int*>(&h);
+}
+
+__global__ void avgpool2_v8_kernel(const bf16* __restrict__ x, int xct, int xco, int H, int W, int C,
+                                   bf16* __restrict__ y, int yct, int yco) {
+  const int h = H / 2, w = W / 2, c8 = C / 8;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= w * c8) return;
+  const int ox = t / c8, c = 8 * (t - ox * c8);
+  const int img = blockIdx.y / h, oy = blockIdx.y - img * h;
+  const bf16* b = x + (((size_t)img * H + 2 * oy) * W + 2 * ox) * xct + xco + c;
+  const uint4 p0 = *reinterpret_cast<const uint4*>(b), p1 = *reinterpret_cast<const uint4*>(b + xct);
+  const uint4 p2 = *reinterpret_cast<const uint4*>(b + (size_t)W * xct);
+  const uint4 p3 = *reinterpret_cast<const uint4*>(b + (size_t)W * xct + xct);
+  const unsigned int a0[4] = {p0.x, p0.y, p0.z, p0.w}, a1[4] = {p1.x, p1.y, p1.z, p1.w};
+  const unsigned int a2[4] = {p2.x, p2.y, p2.z, p2.w}, a3[4] = {p3.x, p3.y, p3.z, p3.w};
+  unsigned int o[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const float2 v0 = bf2f(a0[k]), v1 = bf2f(a1[k]), v2 = bf2f(a2[k]), v3 = bf2f(a3[k]);
+    const float sx = __fadd_rn(__fadd_rn(v0.x, v1.x), __fadd_rn(v2.x, v3.x));
+    const float sy = __fadd_rn(__fadd_rn(v0.y, v1.y), __fadd_rn(v2.y, v3.y));
+    o[k] = f2bf(__fmul_rn(sx, 0.25f), __fmul_rn(sy, 0.25f));
+  }
+  *reinterpret_cast<uint4*>(y + (((size_t)img * h + oy) * w + ox) * yct + yco + c) = make_uint4(o[0], o[1], o[2], o[3]);
+}
+
+__global__ void upsample2_v8_kernel(const bf16* __restrict__ x, int xct, int xco, int h, int w, int C,
+                                    bf16* __restrict__ y, int yct, int yco) {
+  const int H = 2 * h, W = 2 * w, c8 = C / 8;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= W * c8) return;
+  const int xx = t / c8, c = 8 * (t - xx * c8);
+  const int img = blockIdx.y / H, yy = blockIdx.y - img * H;
+  *reinterpret_cast<uint4*>(y + (((size_t)img * H + yy) * W + xx) * yct + yco + c) =
+      *reinterpret_cast<const uint4*>(x + (((size_t)img * h + yy / 2) * w + xx / 2) * xct + xco + c);
+}
+
+static bool v8_ok(const void* x, int xct, int xco, const void* y, int yct, int yco, int C) {
+  return C % 8 == 0 && xct % 8 == 0 && xco % 8 == 0 && yct % 8 == 0 && yco % 8 == 0 &&
+         ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
+}
+
 // dx (fine) = dy (coarse parent) / 4, added to dx when accumulate
 __global__ void avgpool2_bwd_kernel(const bf16* __restrict__ dy, int dct, int dco, int n, int H, int W, int C,
                                     bf16* __restrict__ dx, int xct, int xco, int accumulate) {
@@ -772,6 +824,11 @@ extern "C" int of_cnn_pack_pair(const float* I0, const float* I1, int H, int W, 
 extern "C" int of_cnn_avgpool2(const void* x, int x_ctot, int x_coff, int n, int H, int W, int C, void* y, int y_ctot,
                                int y_coff, void* stream) {
   OF_REQUIRE(x && y && H % 2 == 0 && W % 2 == 0 && C > 0, "of_cnn_avgpool2: bad arguments");
+  if (v8_ok(x, x_ctot, x_coff, y, y_ctot, y_coff, C) && (long long)n * (H / 2) <= 65535) {
+    avgpool2_v8_kernel<<<dim3(blocks_for((long long)(W / 2) * (C / 8)), n * (H / 2)), 256, 0, as_stream(stream)>>>(
+        static_cast<const bf16*>(x), x_ctot, x_coff, H, W, C, static_cast<bf16*>(y), y_ctot, y_coff);
+    return check_launch("of_cnn_avgpool2");
+  }
   long long tot = (long long)n * (H / 2) * (W / 2) * C;
   avgpool2_kernel<<<blocks_for(tot), 256, 0, as_stream(stream)>>>(static_cast<const bf16*>(x), x_ctot, x_coff, n, H,
                                                                    W, C, static_cast<bf16*>(y), y_ctot, y_coff);
@@ -790,6 +847,11 @@ extern "C" int of_cnn_avgpool2_bwd(const void* dy, int dy_ctot, int dy_coff, int
 extern "C" int of_cnn_upsample2(const void* x, int x_ctot, int x_coff, int n, int h, int w, int C, void* y, int y_ctot,
                                 int y_coff, void* stream) {
   OF_REQUIRE(x && y && h > 0 && w > 0 && C > 0, "of_cnn_upsample2: bad arguments");
+  if (v8_ok(x, x_ctot, x_coff, y, y_ctot, y_coff, C) && (long long)n * 2 * h <= 65535) {
+    upsample2_v8_kernel<<<dim3(blocks_for((long long)(2 * w) * (C / 8)), n * 2 * h), 256, 0, as_stream(stream)>>>(
+        static_cast<const bf16*>(x), x_ctot, x_coff, h, w, C, static_cast<bf16*>(y), y_ctot, y_coff);
+    return check_launch("of_cnn_upsample2");
+  }
   long long tot = (long long)n * 4 * h * w * C;
   upsample2_kernel<<<blocks_for(tot), 256, 0, as_stream(stream)>>>(static_cast<const bf16*>(x), x_ctot, x_coff, n, h,
                                                                     w, C, static_cast<bf16*>(y), y_ctot, y_coff);

@@ -70,11 +70,100 @@ __device__ __forceinline__ void resize_coeff_at(int inSize, int outSize, int bic
   *pcnt = xmax;
 }
 
+// sum over j < n of (double)a(j) * w(j), accumulated in the order j = 0, 1, ... (Pillow's);
+// the loads go in groups of 8 ahead of the group's adds, so a thread waits on one memory
+// latency per 8 taps instead of one per tap.
+template <class A, class Wt>
+__device__ __forceinline__ double rz_dot(int n, const A& a, const Wt& w) {
+  double ss = 0.0;
+  int j = 0;
+  for (; j + 8 <= n; j += 8) {
+    float v[8];
+    double k[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      v[q] = a(j + q);
+      k[q] = w(j + q);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) ss = __dadd_rn(ss, __dmul_rn((double)v[q], k[q]));
+  }
+  for (; j < n; j++) ss = __dadd_rn(ss, __dmul_rn((double)a(j), w(j)));
+  return ss;
+}
+
 __global__ void resize_coeff_kernel(int inSize, int outSize, int bicubic, int ksize, int* bounds, double* kk) {
   int xx = blockIdx.x * blockDim.x + threadIdx.x;
   if (xx >= outSize) return;
   resize_coeff_at(inSize, outSize, bicubic, ksize, xx, &bounds[2 * xx], &bounds[2 * xx + 1], kk + (size_t)xx * ksize,
                   1);
+}
+
+// The same weights tap-major (kk[tap * outSize + xx]), the layout of the caller-kept tables:
+// the outputs of a warp read consecutive words of one tap.
+__global__ void resize_coeff_t_kernel(int inSize, int outSize, int bicubic, int ksize, int* bounds, double* kk) {
+  int xx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (xx >= outSize) return;
+  resize_coeff_at(inSize, outSize, bicubic, ksize, xx, &bounds[2 * xx], &bounds[2 * xx + 1], kk + xx, outSize);
+}
+
+// Horizontal pass from a tap-major table: a CTA takes 128 output columns of `rb` rows; per
+// row it stages the source span those columns read into shared memory with coalesced loads
+// (index i stored at i + i / 32, so outputs 8 samples apart, as at a downscale by 8, fall in
+// distinct banks), then each thread sums its taps from there.  Same sums as resize_h_kernel.
+__device__ __forceinline__ int rz_pad(int i) { return i + (i >> 5); }
+__global__ void __launch_bounds__(128) resize_ht_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst,
+                                                        int dp, int Hs, int Wd, const int* __restrict__ bounds,
+                                                        const double* __restrict__ kk, int rb) {
+  extern __shared__ float seg[];
+  const int xb = blockIdx.x * 128, xl = min(Wd, xb + 128) - 1;
+  const int lo = bounds[2 * xb], n = bounds[2 * xl] + bounds[2 * xl + 1] - lo;  // window ends never decrease
+  const int xx = xb + (int)threadIdx.x;
+  const bool act = xx < Wd;
+  const int xmin = act ? bounds[2 * xx] - lo : 0, cnt = act ? bounds[2 * xx + 1] : 0;
+  const double* k = kk + xx;
+  const int y1 = min(Hs, (int)(blockIdx.y + 1) * rb);
+  for (int y = blockIdx.y * rb; y < y1; y++) {
+    const float* row = src + (size_t)y * sp + lo;
+    __syncthreads();  // the previous row's span is no longer read
+    for (int i = threadIdx.x; i < n; i += 128) seg[rz_pad(i)] = row[i];
+    __syncthreads();
+    if (act) {
+      const double ss = rz_dot(cnt, [&](int x) { return seg[rz_pad(xmin + x)]; },
+                               [&](int x) { return k[(size_t)x * Wd]; });
+      dst[(size_t)y * dp + xx] = (float)ss;
+    }
+  }
+}
+
+// The horizontal pass from a tap-major table with the source read from global memory (one
+// row per CTA), for spans too long to stage.
+__global__ void __launch_bounds__(128) resize_htg_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst,
+                                                         int dp, int Wd, const int* __restrict__ bounds,
+                                                         const double* __restrict__ kk) {
+  const int xx = blockIdx.x * 128 + threadIdx.x, y = blockIdx.y;
+  if (xx >= Wd) return;
+  const float* row = src + (size_t)y * sp + bounds[2 * xx];
+  const double* k = kk + xx;
+  const double ss = rz_dot(bounds[2 * xx + 1], [&](int x) { return row[x]; }, [&](int x) { return k[(size_t)x * Wd]; });
+  dst[(size_t)y * dp + xx] = (float)ss;
+}
+
+// Vertical pass from a tap-major table: a thread sums its column for `rb` output rows
+// (the row's weights are read by every thread at once).
+__global__ void __launch_bounds__(128) resize_vt_kernel(const float* __restrict__ src, int sp, float* __restrict__ dst,
+                                                        int dp, int Hd, int Wd, const int* __restrict__ bounds,
+                                                        const double* __restrict__ kk, int rb) {
+  const int x = blockIdx.x * 128 + threadIdx.x;
+  if (x >= Wd) return;
+  const int y1 = min(Hd, (int)(blockIdx.y + 1) * rb);
+  for (int yy = blockIdx.y * rb; yy < y1; yy++) {
+    const int ymin = bounds[2 * yy], ymax = bounds[2 * yy + 1];
+    const float* col = src + (size_t)ymin * sp + x;
+    const double ss = rz_dot(ymax, [&](int y) { return col[(size_t)y * sp]; },
+                             [&](int y) { return kk[(size_t)y * Hd + yy]; });
+    dst[(size_t)yy * dp + x] = (float)ss;
+  }
 }
 
 // Fused passes for kernels of up to RZ_MAXK taps: a CTA computes the weights it needs into
@@ -97,8 +186,7 @@ __global__ void __launch_bounds__(128) resize_hf_kernel(const float* __restrict_
   const int y1 = min(Hs, (blockIdx.y + 1) * rb);
   for (int y = blockIdx.y * rb; y < y1; y++) {
     const float* row = src + (size_t)y * sp + xmin;
-    double ss = 0.0;
-    for (int x = 0; x < xcnt; x++) ss = __dadd_rn(ss, __dmul_rn((double)row[x], k[x * 128]));
+    const double ss = rz_dot(xcnt, [&](int x) { return row[x]; }, [&](int x) { return k[x * 128]; });
     dst[(size_t)y * dp + xx] = (float)ss;
   }
 }
@@ -119,8 +207,8 @@ __global__ void __launch_bounds__(128) resize_vf_kernel(const float* __restrict_
   for (int r = 0; r < n; r++) {
     const int ymin = bnd[r][0], ymax = bnd[r][1];
     const double* k = kk + r * RZ_MAXK;
-    double ss = 0.0;
-    for (int y = 0; y < ymax; y++) ss = __dadd_rn(ss, __dmul_rn((double)src[(size_t)(y + ymin) * sp + x], k[y]));
+    const float* col = src + (size_t)ymin * sp + x;
+    const double ss = rz_dot(ymax, [&](int y) { return col[(size_t)y * sp]; }, [&](int y) { return k[y]; });
     dst[(size_t)(yy0 + r) * dp + x] = (float)ss;
   }
 }
@@ -140,8 +228,7 @@ __global__ void resize_h_kernel(const float* __restrict__ src, int sp, float* __
   int xmin = bounds[2 * xx], xmax = bounds[2 * xx + 1];
   const double* k = kk + (size_t)xx * ksize;
   const float* row = src + (size_t)y * sp + xmin;
-  double ss = 0.0;
-  for (int x = 0; x < xmax; x++) ss = __dadd_rn(ss, __dmul_rn((double)row[x], k[x]));
+  const double ss = rz_dot(xmax, [&](int x) { return row[x]; }, [&](int x) { return k[x]; });
   dst[(size_t)y * dp + xx] = (float)ss;
 }
 
@@ -151,8 +238,8 @@ __global__ void resize_v_kernel(const float* __restrict__ src, int sp, float* __
   if (x >= Wd) return;
   int ymin = bounds[2 * yy], ymax = bounds[2 * yy + 1];
   const double* k = kk + (size_t)yy * ksize;
-  double ss = 0.0;
-  for (int y = 0; y < ymax; y++) ss = __dadd_rn(ss, __dmul_rn((double)src[(size_t)(y + ymin) * sp + x], k[y]));
+  const float* col = src + (size_t)ymin * sp + x;
+  const double ss = rz_dot(ymax, [&](int y) { return col[(size_t)y * sp]; }, [&](int y) { return k[y]; });
   dst[(size_t)yy * dp + x] = (float)ss;
 }
 
@@ -639,6 +726,84 @@ extern "C" int of_resize(const float* src, int Hs, int Ws, int src_pitch, float*
     resize_v_kernel<<<dim3((Wd + 127) / 128, Hd), 128, 0, st>>>(cur, cur_pitch, dst, dst_pitch, Wd, bv, kkv, kv);
   }
   return check_launch("of_resize", 2 * (int)need_h + 2 * (int)need_v);
+}
+
+// Weight tables of one axis, computed once and kept by the caller (a downscale by 8 has 33
+// bicubic taps per output, whose weights cost more than the resize's sums when every CTA of
+// a fused pass recomputes them).  Layout: int bounds[2 * out], then (256-byte aligned)
+// double weights[out][ksize], as the table path of of_resize builds them.
+extern "C" size_t of_resize_table_size(int in, int out, int filter) {
+  if (in <= 0 || out <= 0) return 0;
+  Sizer s;
+  s.take<int>(2 * (size_t)out);
+  s.take<double>((size_t)ksize_of(in, out, filter == OF_FILTER_BICUBIC) * out);
+  return s.off;
+}
+
+extern "C" int of_resize_table(int in, int out, int filter, void* table, size_t table_bytes, void* stream) {
+  OF_REQUIRE(in > 0 && out > 0 && table, "of_resize_table: bad arguments");
+  OF_REQUIRE(filter == OF_FILTER_BILINEAR || filter == OF_FILTER_BICUBIC, "of_resize_table: unknown filter");
+  const size_t need = of_resize_table_size(in, out, filter);
+  if (table_bytes < need)
+    return set_error(OF_ERR_WORKSPACE, "of_resize_table: table too small (%zu < %zu)", table_bytes, need);
+  const int bic = filter == OF_FILTER_BICUBIC, k = ksize_of(in, out, bic);
+  Carver c(table, table_bytes);
+  int* b = c.take<int>(2 * (size_t)out);
+  double* kk = c.take<double>((size_t)k * out);
+  resize_coeff_t_kernel<<<(out + 127) / 128, 128, 0, as_stream(stream)>>>(in, out, bic, k, b, kk);
+  return check_launch("of_resize_table");
+}
+
+extern "C" int of_resize_tabled(const float* src, int Hs, int Ws, int src_pitch, float* dst, int Hd, int Wd,
+                                int dst_pitch, int filter, const void* table_h, const void* table_v, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+  OF_REQUIRE(!bad_plane(src, Hs, Ws, src_pitch) && !bad_plane(dst, Hd, Wd, dst_pitch), "of_resize_tabled: bad plane");
+  OF_REQUIRE(filter == OF_FILTER_BILINEAR || filter == OF_FILTER_BICUBIC, "of_resize_tabled: unknown filter");
+  cudaStream_t st = as_stream(stream);
+  if (Hs == Hd && Ws == Wd) {
+    copy_plane_kernel<<<dim3((Wd + 255) / 256, Hd), 256, 0, st>>>(src, src_pitch, dst, dst_pitch, Wd);
+    return check_launch("of_resize_tabled");
+  }
+  const bool need_h = Wd != Ws, need_v = Hd != Hs;
+  OF_REQUIRE((!need_h || table_h) && (!need_v || table_v), "of_resize_tabled: missing weight table");
+  const int bic = filter == OF_FILTER_BICUBIC;
+  const int kh = need_h ? ksize_of(Ws, Wd, bic) : 0, kv = need_v ? ksize_of(Hs, Hd, bic) : 0;
+  float* tmp = nullptr;
+  if (need_h && need_v) {
+    if (!workspace || workspace_bytes < (size_t)Hs * Wd * sizeof(float))
+      return set_error(OF_ERR_WORKSPACE, "of_resize_tabled: workspace too small (%zu < %zu)", workspace_bytes,
+                       (size_t)Hs * Wd * sizeof(float));
+    tmp = static_cast<float*>(workspace);
+  }
+  const float* cur = src;
+  int cur_pitch = src_pitch;
+  if (need_h) {
+    Carver c(const_cast<void*>(table_h), of_resize_table_size(Ws, Wd, filter));
+    const int* bh = c.take<int>(2 * (size_t)Wd);
+    const double* kkh = c.take<double>((size_t)kh * Wd);
+    float* out = need_v ? tmp : dst;
+    const int op = need_v ? Wd : dst_pitch;
+    // a CTA's source span: its 128 columns' windows (at most 128 input steps plus one window)
+    const long long span = (long long)ceil(128.0 * Ws / Wd) + kh + 2;
+    const int cb = (Wd + 127) / 128;
+    if (span <= 8192) {
+      const size_t smem = sizeof(float) * (size_t)(span + (span >> 5) + 1);
+      const int rb = rz_band(cb, Hs);
+      resize_ht_kernel<<<dim3(cb, (Hs + rb - 1) / rb), 128, smem, st>>>(src, src_pitch, out, op, Hs, Wd, bh, kkh, rb);
+    } else {  // very strong downscales: the span does not fit a CTA's default shared memory
+      resize_htg_kernel<<<dim3(cb, Hs), 128, 0, st>>>(src, src_pitch, out, op, Wd, bh, kkh);
+    }
+    cur = out;
+    cur_pitch = op;
+  }
+  if (need_v) {
+    Carver c(const_cast<void*>(table_v), of_resize_table_size(Hs, Hd, filter));
+    const int* bv = c.take<int>(2 * (size_t)Hd);
+    const double* kkv = c.take<double>((size_t)kv * Hd);
+    const int cb = (Wd + 127) / 128, rb = rz_band(cb, Hd);
+    resize_vt_kernel<<<dim3(cb, (Hd + rb - 1) / rb), 128, 0, st>>>(cur, cur_pitch, dst, dst_pitch, Hd, Wd, bv, kkv, rb);
+  }
+  return check_launch("of_resize_tabled", (int)need_h + (int)need_v);
 }
 
 extern "C" size_t of_spline_workspace_size(int h, int w, int H, int W) {

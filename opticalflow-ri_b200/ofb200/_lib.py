@@ -84,6 +84,9 @@ _SIGS = {
     "of_u16_to_f32": ([_P, _I, _P, _I, _I, _I, _P], _I),
     "of_resize_workspace_size": ([_I, _I, _I, _I, _I], _Z),
     "of_resize": ([_P, _I, _I, _I, _P, _I, _I, _I, _I, _P, _Z, _P], _I),
+    "of_resize_table_size": ([_I, _I, _I], _Z),
+    "of_resize_table": ([_I, _I, _I, _P, _Z, _P], _I),
+    "of_resize_tabled": ([_P, _I, _I, _I, _P, _I, _I, _I, _I, _P, _P, _P, _Z, _P], _I),
     "of_spline_workspace_size": ([_I, _I, _I, _I], _Z),
     "of_spline_upsample": ([_P, _I, _I, _I, _P, _I, _I, _I, _F, _P, _Z, _P], _I),
     "of_spline_upsample_pair": ([_P, _P, _I, _I, _I, _P, _P, _I, _I, _I, _F, _F, _P, _Z, _P], _I),

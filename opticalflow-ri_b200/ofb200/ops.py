@@ -110,9 +110,52 @@ def resize(src: torch.Tensor, size_wh, bicubic: bool, out: torch.Tensor | None =
     out = _new(Hd, Wd, src) if out is None else out
     d, _, _, dp = _plane(out, "resize.out")
     f = _lib.OF_FILTER_BICUBIC if bicubic else _lib.OF_FILTER_BILINEAR
+    if max(_resize_taps(Ws, Wd, bicubic), _resize_taps(Hs, Hd, bicubic)) > RESIZE_TABLE_TAPS:
+        th = _resize_table(Ws, Wd, f) if Wd != Ws else None
+        tv = _resize_table(Hs, Hd, f) if Hd != Hs else None
+        if (th is not None or Wd == Ws) and (tv is not None or Hd == Hs):
+            ws, wn = workspace(4 * Hs * Wd, "resize")
+            call("of_resize_tabled", s, Hs, Ws, sp, d, Hd, Wd, dp, f, None if th is None else _p(th),
+                 None if tv is None else _p(tv), ws, wn, stream_ptr())
+            return out
     ws, wn = workspace(lib().of_resize_workspace_size(Hs, Ws, Hd, Wd, f), "resize")
     call("of_resize", s, Hs, Ws, sp, d, Hd, Wd, dp, f, ws, wn, stream_ptr())
     return out
+
+
+# Resizes with more taps per output than this (downscales by more than 4 with the bicubic
+# filter, by more than 8 with the bilinear one) take their weights from tables computed
+# once per (device, sizes, filter) and kept (of_resize_table), instead of recomputing them
+# in every CTA.
+RESIZE_TABLE_TAPS = 16
+_RZ_TABLES = {}
+
+
+def _resize_taps(n_in, n_out, bicubic):
+    """Pillow's taps per output sample along one axis (the kernel's ksize)."""
+    support = (2.0 if bicubic else 1.0) * max(n_in / n_out, 1.0)
+    return int(np.ceil(support)) * 2 + 1
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _resize_table(n_in, n_out, f):
+    """The weight table of one axis on the current device (None while a stream is being
+    captured and the table does not exist yet: the caller then resizes without it)."""
+    dev = torch.cuda.current_device()
+    key = (dev, n_in, n_out, f)
+    t = _RZ_TABLES.get(key)
+    if t is None:
+        if torch.cuda.is_current_stream_capturing():
+            return None
+        nb = lib().of_resize_table_size(n_in, n_out, f)
+        t = torch.empty(nb, dtype=torch.uint8, device=f"cuda:{dev}")
+        call("of_resize_table", n_in, n_out, f, _p(t), nb, stream_ptr())
+        torch.cuda.current_stream().synchronize()  # later calls read it from any stream
+        _RZ_TABLES[key] = t
+    return t
 
 
 def spline_upsample(src: torch.Tensor, H: int, W: int, scale: float = 1.0, out=None) -> torch.Tensor:

@@ -367,10 +367,11 @@ class LearnedLiuShen:
         return self.upsample(self.net.forward(b)[0], H, W)
 
     def refine(self, I0, I1, U, V):
-        """The full-size stage from the initial field: (Farneback,) then Liu-Shen."""
+        """The full-size stage from the initial field: (Farneback,) then Liu-Shen.  U, V are
+        handed over: the Farneback stage iterates on them in place."""
         if self.mode == "fb":
             import Farneback_PyCL as F
-            U, V, _ = F.Farneback_PyCL(Niters=self.fb_iters)._compute_dev(I0, I1, U, V)
+            U, V, _ = F.Farneback_PyCL(Niters=self.fb_iters)._compute_dev(I0, I1, U, V, consume_init=True)
         f0 = ops.prefilter(I0, self.taps)
         f1 = ops.prefilter(I1, self.taps)
         return ops.ls_solve(f0, f1, U, V, self.h, self.sweeps, 1e-8)

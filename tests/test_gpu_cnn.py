@@ -167,6 +167,26 @@ def test_weight_gradient(torch_cuda, cin, cout, coff):
     assert np.max(np.abs(db.cpu().numpy() - wb)) <= 1e-4 * np.max(np.abs(wb))
 
 
+def test_pool_and_upsample_any_channel_layout(torch_cuda):
+    """Channel counts and offsets that are not multiples of 8 take the one-channel-per-thread
+    kernels; multiples of 8 the 8-channel ones: both equal the oracle."""
+    import cnn_oracle as C
+    from ofb200._lib import call
+    torch = torch_cuda
+    rng = np.random.default_rng(9)
+    n, H, W = 3, 10, 14
+    x = C.bf16(rng.normal(0, 1, (n, H, W, 24)))
+    xt = _bf(torch, x)
+    for c0, cn in ((4, 12), (2, 5), (8, 8), (0, 16)):
+        p = torch.empty((n, H // 2, W // 2, cn), dtype=torch.bfloat16, device="cuda")
+        call("of_cnn_avgpool2", _P(xt), 24, c0, n, H, W, cn, _P(p), cn, 0, _sp())
+        up = torch.zeros((n, 2 * H, 2 * W, cn), dtype=torch.bfloat16, device="cuda")
+        call("of_cnn_upsample2", _P(xt), 24, c0, n, H, W, cn, _P(up), cn, 0, _sp())
+        torch.cuda.synchronize()
+        assert np.array_equal(_f(p), C.bf16(C.avgpool2(x[..., c0:c0 + cn]))), (c0, cn)
+        assert np.array_equal(_f(up), C.upsample2(x[..., c0:c0 + cn])), (c0, cn)
+
+
 def test_elementwise_kernels_bit_exact(torch_cuda):
     import cnn_oracle as C
     from ofb200._lib import call
