@@ -487,6 +487,22 @@ __global__ void frame_max_kernel(const float* __restrict__ I, int H, int W, int 
   if ((threadIdx.x & 31) == 0) atomicMax(mx, __float_as_uint(m));  // non-negative floats order as integers
 }
 
+// One pixel of the network input: (a, b, 0, ...) over cpad channels; 16-byte stores when
+// cpad is a multiple of 8 and the pixel's channels start 16-byte aligned.
+__device__ __forceinline__ void pack_store(bf16* o, int cpad, float a, float b) {
+  if ((cpad & 7) == 0 && (reinterpret_cast<uintptr_t>(o) & 15) == 0) {
+    const __nv_bfloat162 ab = __floats2bfloat162_rn(a, b);
+    uint4 v = make_uint4(*reinterpret_cast<const unsigned int*>(&ab), 0u, 0u, 0u);
+    reinterpret_cast<uint4*>(o)[0] = v;
+    v.x = 0u;
+    for (int c = 8; c < cpad; c += 8) reinterpret_cast<uint4*>(o + c)[0] = v;
+    return;
+  }
+  o[0] = __float2bfloat16_rn(a);
+  o[1] = __float2bfloat16_rn(b);
+  for (int c = 2; c < cpad; c++) o[c] = __float2bfloat16_rn(0.f);
+}
+
 __global__ void pack_pair_kernel(const float* __restrict__ I0, const float* __restrict__ I1, int H, int W, int pitch,
                                  const unsigned* __restrict__ mx, bf16* __restrict__ out, int cpad) {
   long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -495,10 +511,50 @@ __global__ void pack_pair_kernel(const float* __restrict__ I0, const float* __re
   float m0 = __uint_as_float(mx[0]), m1 = __uint_as_float(mx[1]);
   float a = m0 > 0.f ? __fdiv_rn(I0[(size_t)y * pitch + x], m0) : 0.f;
   float b = m1 > 0.f ? __fdiv_rn(I1[(size_t)y * pitch + x], m1) : 0.f;
-  bf16* o = out + (size_t)e * cpad;
-  o[0] = __float2bfloat16_rn(a);
-  o[1] = __float2bfloat16_rn(b);
-  for (int c = 2; c < cpad; c++) o[c] = __float2bfloat16_rn(0.f);
+  pack_store(out + (size_t)e * cpad, cpad, a, b);
+}
+
+// Both maxima and the packing in one CTA, for the small frames the network runs on (up to
+// 64 K pixels): the maxima are the same (max is exact and order-free, NaN-free through
+// fmaxf as in frame_max_kernel) and the packing is pack_pair_kernel's per pixel.
+constexpr int PK1_THREADS = 1024;
+__global__ void __launch_bounds__(PK1_THREADS) pack_pair_one_kernel(const float* __restrict__ I0,
+                                                                     const float* __restrict__ I1, int H, int W,
+                                                                     int pitch, unsigned* __restrict__ mx,
+                                                                     bf16* __restrict__ out, int cpad) {
+  __shared__ float r0[32], r1[32];
+  const int n = H * W;
+  float m0 = 0.f, m1 = 0.f;
+  for (int e = threadIdx.x; e < n; e += PK1_THREADS) {
+    const int y = e / W, x = e - y * W;
+    m0 = fmaxf(m0, I0[(size_t)y * pitch + x]);
+    m1 = fmaxf(m1, I1[(size_t)y * pitch + x]);
+  }
+  for (int o = 16; o; o >>= 1) {
+    m0 = fmaxf(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+    m1 = fmaxf(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    r0[threadIdx.x >> 5] = m0;
+    r1[threadIdx.x >> 5] = m1;
+  }
+  __syncthreads();
+  m0 = r0[0];
+  m1 = r1[0];
+  for (int w = 1; w < PK1_THREADS / 32; w++) {
+    m0 = fmaxf(m0, r0[w]);
+    m1 = fmaxf(m1, r1[w]);
+  }
+  if (threadIdx.x == 0) {
+    mx[0] = __float_as_uint(m0);
+    mx[1] = __float_as_uint(m1);
+  }
+  for (int e = threadIdx.x; e < n; e += PK1_THREADS) {
+    const int y = e / W, x = e - y * W;
+    const float a = m0 > 0.f ? __fdiv_rn(I0[(size_t)y * pitch + x], m0) : 0.f;
+    const float b = m1 > 0.f ? __fdiv_rn(I1[(size_t)y * pitch + x], m1) : 0.f;
+    pack_store(out + (size_t)e * cpad, cpad, a, b);
+  }
 }
 
 __global__ void avgpool2_kernel(const bf16* __restrict__ x, int xct, int xco, int n, int H, int W, int C,
@@ -812,6 +868,10 @@ extern "C" int of_cnn_pack_pair(const float* I0, const float* I1, int H, int W, 
                                 int cpad, void* stream) {
   OF_REQUIRE(I0 && I1 && max2 && out && H > 0 && W > 0 && pitch >= W && cpad >= 2, "of_cnn_pack_pair: bad arguments");
   cudaStream_t st = as_stream(stream);
+  if ((long long)H * W <= 65536) {
+    pack_pair_one_kernel<<<1, PK1_THREADS, 0, st>>>(I0, I1, H, W, pitch, max2, static_cast<bf16*>(out), cpad);
+    return check_launch("of_cnn_pack_pair");
+  }
   cudaMemsetAsync(max2, 0, 2 * sizeof(unsigned), st);
   int g = blocks_for((long long)H * W);
   int gm = g < 4 * kNumSMs ? g : 4 * kNumSMs;

@@ -221,21 +221,26 @@ def test_elementwise_kernels_bit_exact(torch_cuda):
     assert np.array_equal(_f(gt), np.where(_f(up) > 0, g, 0))
 
 
-def test_pack_pair_and_split_flow(torch_cuda):
+@pytest.mark.parametrize("H,W", [(24, 40), (300, 260)])
+def test_pack_pair_and_split_flow(torch_cuda, H, W):
+    """The network input: one CTA for small frames, the multi-block maxima above 64 K pixels."""
     import cnn_oracle as C
     from ofb200._lib import call
     torch = torch_cuda
     rng = np.random.default_rng(8)
-    a = rng.uniform(0, 200, (24, 40)).astype(np.float32)
-    b = rng.uniform(0, 250, (24, 40)).astype(np.float32)
+    a = rng.uniform(0, 200, (H, W)).astype(np.float32)
+    b = rng.uniform(0, 250, (H, W)).astype(np.float32)
     at, bt = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
-    mx = torch.zeros(2, dtype=torch.int32, device="cuda")
-    out = torch.empty((24, 40, 16), dtype=torch.bfloat16, device="cuda")
-    call("of_cnn_pack_pair", _P(at), _P(bt), 24, 40, 40, _P(mx), _P(out), 16, _sp())
+    mx = torch.full((2,), 7, dtype=torch.int32, device="cuda")  # stale contents are overwritten
+    out = torch.empty((H, W, 16), dtype=torch.bfloat16, device="cuda")
+    call("of_cnn_pack_pair", _P(at), _P(bt), H, W, W, _P(mx), _P(out), 16, _sp())
     torch.cuda.synchronize()
     o = _f(out)
     assert np.array_equal(o[..., 0], C.bf16(a / a.max())) and np.array_equal(o[..., 1], C.bf16(b / b.max()))
     assert not o[..., 2:].any()
+    assert mx.cpu().numpy().view(np.float32).tolist() == [a.max(), b.max()]
+    if (H, W) != (24, 40):
+        return
     f = rng.normal(0, 1, (24, 40, 2)).astype(np.float32)
     ft = torch.from_numpy(f).cuda()
     u = torch.empty((24, 48), dtype=torch.float32, device="cuda")[:, :40]
