@@ -1073,6 +1073,11 @@ def cpu_baseline(pair):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the oracle (the reference's path restated in C, one thread per
+    pair) on the GPU arm's workload, --pairs pairs per step, on every host core.  Steps are
+    handed to a pool of one process per core in groups of cores // pairs steps, so every core
+    works while a step's pairs run in parallel; the run stops after REF_BUDGET_S seconds
+    (whole groups), and value = pairs done / time."""
     if rank != 0:
         return None
     import multiprocessing as mp
@@ -1083,24 +1088,26 @@ def run_reference(args, rank, world):
     pairs = make_pairs(args.unique, args.size)  # the same distinct pairs as the GPU arm's step
     work = [(p[0].astype(np.float32), p[1].astype(np.float32)) for p in pairs]
     ctx = mp.get_context("spawn")
-    per_step = ncores
+    per_step = args.pairs
+    group = max(1, ncores // per_step)  # steps per pool call
     steps = 0
     with ctx.Pool(ncores) as pool:
         for _ in range(min(args.warmup, 1)):
-            pool.map(_oracle_pair, [work[i % len(work)] for i in range(per_step)])
+            pool.map(_oracle_pair, [work[i % len(work)] for i in range(min(ncores, per_step * group))])
         t0 = time.perf_counter()
         # a step takes several seconds of CPU time: stop after REF_BUDGET_S so the run stays short
         while steps < args.steps and (steps == 0 or time.perf_counter() - t0 < REF_BUDGET_S):
-            pool.map(_oracle_pair, [work[i % len(work)] for i in range(per_step)])
-            steps += 1
+            g = min(group, args.steps - steps)
+            pool.map(_oracle_pair, [work[i % len(work)] for i in range(per_step * g)])
+            steps += g
         dt = time.perf_counter() - t0
     v = per_step * steps / dt
     return {"metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "pairs_per_step": per_step, "size": args.size,
+            "config": {"workload": WORKLOAD, "pairs_per_step_per_gpu": per_step, "size": args.size,
                        "unique_pairs": args.unique,
-                       "parallelism": f"one pair per host process, {per_step} processes"},
+                       "parallelism": f"one pair per host process, {ncores} processes, {group} step(s) at a time"},
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": ncores, "kind": "port",
                              "sample": f"{per_step} pairs per step, one per process, {steps} of "
                                        f"{args.steps} steps (capped at {REF_BUDGET_S:.0f} s)"},
