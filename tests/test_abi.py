@@ -94,3 +94,29 @@ def test_spline_pair_argument_checks_without_gpu():
     need = 2 * L.of_spline_workspace_size(8, 8, 16, 16)
     rc = L.of_spline_upsample_pair(fake, fake, 8, 8, 8, fake, other, 16, 16, 16, 1.0, 1.0, fake, need - 8, None)
     assert rc == -3 and "workspace" in _lib.last_error()
+
+
+def test_resize_table_sizes_without_gpu():
+    """The drop-in's estimate of Pillow's taps per output (which decides when a resize uses
+    kept weight tables) is the library's kernel width: of_resize_table_size holds 2 ints and
+    that many doubles per output sample.  The tabled resize rejects a missing table and a
+    small workspace on the host."""
+    if not os.path.exists(LIB):
+        pytest.skip("libofb200.so not built")
+    from ofb200 import _lib, ops
+    L = _lib.lib()
+
+    def up256(x):
+        return (x + 255) // 256 * 256
+
+    for n_in, n_out in ((1024, 128), (1024, 512), (512, 16), (37, 19), (64, 128), (1000, 95), (8192, 128)):
+        for bic, f in ((True, _lib.OF_FILTER_BICUBIC), (False, _lib.OF_FILTER_BILINEAR)):
+            k = ops._resize_taps(n_in, n_out, bic)
+            assert L.of_resize_table_size(n_in, n_out, f) == up256(8 * n_out) + 8 * k * n_out, (n_in, n_out, bic)
+    assert L.of_resize_table_size(0, 4, _lib.OF_FILTER_BICUBIC) == 0
+    fake = ctypes.c_void_p(4096)  # never dereferenced: the checks fail first
+    rc = L.of_resize_tabled(fake, 64, 64, 64, fake, 8, 8, 8, _lib.OF_FILTER_BICUBIC, None, fake, fake, 1 << 20, None)
+    assert rc == -1 and "table" in _lib.last_error()
+    rc = L.of_resize_tabled(fake, 64, 64, 64, fake, 8, 8, 8, _lib.OF_FILTER_BICUBIC, fake, fake, fake, 4 * 64 * 8 - 4,
+                            None)
+    assert rc == -3 and "workspace" in _lib.last_error()
