@@ -129,6 +129,7 @@ def resize(src: torch.Tensor, size_wh, bicubic: bool, out: torch.Tensor | None =
 # in every CTA.
 RESIZE_TABLE_TAPS = 16
 _RZ_TABLES = {}
+_RZ_LOCK = threading.Lock()  # a table is built once even when host threads resize at once
 
 
 def _resize_taps(n_in, n_out, bicubic):
@@ -150,11 +151,14 @@ def _resize_table(n_in, n_out, f):
     if t is None:
         if torch.cuda.is_current_stream_capturing():
             return None
-        nb = lib().of_resize_table_size(n_in, n_out, f)
-        t = torch.empty(nb, dtype=torch.uint8, device=f"cuda:{dev}")
-        call("of_resize_table", n_in, n_out, f, _p(t), nb, stream_ptr())
-        torch.cuda.current_stream().synchronize()  # later calls read it from any stream
-        _RZ_TABLES[key] = t
+        with _RZ_LOCK:
+            t = _RZ_TABLES.get(key)
+            if t is None:
+                nb = lib().of_resize_table_size(n_in, n_out, f)
+                t = torch.empty(nb, dtype=torch.uint8, device=f"cuda:{dev}")
+                call("of_resize_table", n_in, n_out, f, _p(t), nb, stream_ptr())
+                torch.cuda.current_stream().synchronize()  # later calls read it from any stream
+                _RZ_TABLES[key] = t
     return t
 
 
