@@ -88,7 +88,7 @@ def test_resize_golden(torch_cuda):
                                      ((37, 41), (19, 20)), ((64, 64), (32, 64)), ((40, 128), (40, 64)),
                                      ((64, 96), (128, 150)), ((512, 512), (16, 16)), ((1024, 1024), (128, 128)),
                                      ((1000, 760), (100, 95)), ((96, 1024), (12, 120)), ((8, 8192), (8, 128)),
-                                     ((300, 40), (9, 40))])
+                                     ((300, 40), (9, 40)), ((1024, 2048), (128, 256)), ((600, 1800), (60, 180))])
 @pytest.mark.parametrize("bicubic", [True, False])
 def test_resize_vs_oracle(torch_cuda, src, dst, bicubic):
     from ofb200 import ops
