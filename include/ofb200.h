@@ -87,8 +87,9 @@ int of_resize(const float* src, int Hs, int Ws, int src_pitch, float* dst, int H
  * (same results bit for bit): of_resize_table fills one axis's table (in -> out samples,
  * of_resize_table_size bytes, DEVICE memory); of_resize_tabled takes the horizontal
  * (Ws -> Wd) and vertical (Hs -> Hd) tables (either may be NULL when that axis keeps its
- * size) and, when both axes change, a workspace of Hs * Wd floats.  Worth it for strong
- * downscales, whose many taps per output make the weights the dominant cost. */
+ * size) and, when both axes change, a workspace of Hs * Wd floats.  Each table must be
+ * the one built for that axis's (in, out, filter): the kernels trust its contents.  Worth
+ * it for strong downscales, whose many taps per output make the weights the dominant cost. */
 size_t of_resize_table_size(int in, int out, int filter);
 int of_resize_table(int in, int out, int filter, void* table, size_t table_bytes, void* stream);
 int of_resize_tabled(const float* src, int Hs, int Ws, int src_pitch, float* dst, int Hd, int Wd, int dst_pitch,
