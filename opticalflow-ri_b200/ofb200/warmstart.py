@@ -34,7 +34,7 @@ import numpy as np
 import torch
 
 from . import ops
-from ._lib import call, lib
+from ._lib import call
 
 __all__ = ["LAYERS", "WarmStartNet", "LearnedLiuShen", "LearnedBatch", "load_trained", "n_params"]
 
